@@ -1,0 +1,275 @@
+"""B200-native SQP inner loop for 7-DOF iiwa end-effector tracking.
+
+Python front end of libgpt.so (the C ABI in include/gpt.h).  It mirrors the
+reference's host interface for this path (gpu-pcg-tracking toplevel.cuh
+sqpSolve and the kernels it launches) on torch CUDA tensors; torch only
+supplies device memory and streams.  There is no CPU implementation: if the
+CUDA library is missing or no GPU is visible, every call raises.
+
+The directory name contains hyphens, so import it with
+``importlib.import_module("gpu-pcg-tracking_b200")``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from dataclasses import dataclass, field
+from typing import List, Optional, Sequence
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libgpt.so")
+
+GPT_OK = 0
+STATUS_NAMES = {0: "OK", 1: "BAD_ARG", 2: "CUDA", 3: "NO_DEVICE", 4: "CAPACITY", 5: "NONFINITE", 6: "FACTOR"}
+EXIT_RHO_MAX, EXIT_PCG_MAXITER, EXIT_NONFINITE, EXIT_ITER_LIMIT = 1, 2, 4, 8
+
+STATE_SIZE, CONTROL_SIZE = 14, 7
+
+# The C-ABI entry points include/gpt.h declares (checked by the CPU tests).
+EXPORTED = [
+    "gpt_default_problem_config", "gpt_default_solver_config", "gpt_create", "gpt_destroy",
+    "gpt_set_solver_config", "gpt_last_error", "gpt_version", "gpt_sqp_solve", "gpt_sqp_solve_batched",
+    "gpt_form_kkt", "gpt_form_schur", "gpt_form_schur_csc", "gpt_prep_csr", "gpt_pcg", "gpt_compute_dz",
+    "gpt_compute_merit", "gpt_ls_compute_merit", "gpt_set_profiling", "gpt_get_phase_stats",
+]
+PHASES = ["init", "kkt", "schur", "pcg", "dz", "merit", "accept"]
+
+
+class ProblemConfig(C.Structure):
+    """gpt_problem_config (include/gpt.h)."""
+    _fields_ = [("state_size", C.c_uint32), ("control_size", C.c_uint32), ("max_knot_points", C.c_uint32),
+                ("max_batch", C.c_uint32), ("timestep", C.c_float), ("integrator", C.c_uint32),
+                ("q_ee", C.c_float), ("qd_cost", C.c_float), ("r_cost", C.c_float), ("mu", C.c_float),
+                ("ref_terminal", C.c_uint32)]
+
+
+class SolverConfig(C.Structure):
+    """gpt_solver_config (include/gpt.h)."""
+    _fields_ = [("sqp_max_iter", C.c_uint32), ("pcg_max_iter", C.c_uint32), ("pcg_exit_tol", C.c_float),
+                ("pcg_exit_mode", C.c_uint32), ("rho_factor", C.c_float), ("rho_max", C.c_float),
+                ("rho_min", C.c_float)]
+
+
+class SqpStats(C.Structure):
+    """gpt_sqp_stats (include/gpt.h)."""
+    _fields_ = [("sqp_iters", C.c_uint32), ("exit_flags", C.c_uint32), ("pcg_iters_total", C.c_uint32),
+                ("pcg_maxiter_count", C.c_uint32), ("ls_fail_count", C.c_uint32), ("merit_initial", C.c_float),
+                ("merit_final", C.c_float), ("rho_final", C.c_float)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class GptError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"gpt {STATUS_NAMES.get(status, status)}: {msg}")
+        self.status = status
+
+
+def build(force: bool = False) -> str:
+    """Compile libgpt.so for sm_100a with nvcc (csrc/Makefile)."""
+    args = ["make", "-s", "-j8", "-C", os.path.join(HERE, "csrc")]
+    if force:
+        subprocess.run(args + ["clean"], check=True)
+    subprocess.run(args, check=True)
+    return LIB_PATH
+
+
+_LIB = None
+
+
+def lib():
+    """The loaded CUDA library; raises if it was not built."""
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with csrc/Makefile (nvcc, sm_100a)")
+        L = C.CDLL(LIB_PATH)
+        _declare(L)
+        _LIB = L
+    return _LIB
+
+
+def _declare(L):
+    vp, u32, f32 = C.c_void_p, C.c_uint32, C.c_float
+    P = C.POINTER
+    sig = {
+        "gpt_default_problem_config": ([P(ProblemConfig)], None),
+        "gpt_default_solver_config": ([P(SolverConfig)], None),
+        "gpt_create": ([P(ProblemConfig), P(SolverConfig), P(vp)], C.c_int),
+        "gpt_destroy": ([vp], C.c_int),
+        "gpt_set_solver_config": ([vp, P(SolverConfig)], C.c_int),
+        "gpt_last_error": ([], C.c_char_p),
+        "gpt_version": ([], C.c_char_p),
+        "gpt_sqp_solve": ([vp, u32, vp, vp, vp, P(f32), f32, P(SqpStats), vp, vp, vp], C.c_int),
+        "gpt_sqp_solve_batched": ([vp, u32, vp, vp, vp, vp, vp, f32, vp, vp], C.c_int),
+        "gpt_form_kkt": ([vp, u32, vp, vp, vp, vp, vp, vp, vp, vp], C.c_int),
+        "gpt_form_schur": ([vp, u32, f32, vp, vp, vp, vp, vp, vp, vp, vp, vp], C.c_int),
+        "gpt_form_schur_csc": ([vp, u32, f32, vp, vp, vp, vp, vp, vp, vp, vp], C.c_int),
+        "gpt_prep_csr": ([u32, vp, vp], C.c_int),
+        "gpt_pcg": ([vp, u32, vp, vp, vp, vp, u32, f32, u32, P(u32), P(C.c_uint8), vp], C.c_int),
+        "gpt_compute_dz": ([vp, u32, vp, vp, vp, vp, vp, vp], C.c_int),
+        "gpt_compute_merit": ([vp, u32, vp, vp, vp, vp], C.c_int),
+        "gpt_ls_compute_merit": ([vp, u32, vp, vp, vp, vp, vp, vp], C.c_int),
+        "gpt_set_profiling": ([vp, C.c_int], C.c_int),
+        "gpt_get_phase_stats": ([vp, vp, vp, C.c_int], C.c_int),
+    }
+    for name, (args, res) in sig.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = res
+
+
+def _check(st: int):
+    if st != GPT_OK:
+        raise GptError(st, lib().gpt_last_error().decode())
+
+
+def default_problem_config(**kw) -> ProblemConfig:
+    pc = ProblemConfig()
+    lib().gpt_default_problem_config(C.byref(pc))
+    for k, v in kw.items():
+        setattr(pc, k, v)
+    return pc
+
+
+def default_solver_config(**kw) -> SolverConfig:
+    sc = SolverConfig()
+    lib().gpt_default_solver_config(C.byref(sc))
+    for k, v in kw.items():
+        setattr(sc, k, v)
+    return sc
+
+
+def _ptr(t):
+    if t is None:
+        return None
+    if not t.is_cuda:
+        raise ValueError("expected a CUDA tensor")
+    if not t.is_contiguous():
+        raise ValueError("expected a contiguous tensor")
+    return C.c_void_p(t.data_ptr())
+
+
+def _stream(stream):
+    import torch
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return C.c_void_p(s.cuda_stream)
+
+
+@dataclass
+class SqpResult:
+    """What sqpSolve returns (toplevel.cuh:502) plus the device-side stats."""
+    pcg_iters: List[int]
+    pcg_exit: List[bool]
+    sqp_iters: int
+    rho: float
+    stats: dict = field(default_factory=dict)
+
+
+class Solver:
+    """A gpt_handle: workspace for max_batch x max_knot_points, preallocated."""
+
+    def __init__(self, problem: Optional[ProblemConfig] = None, solver: Optional[SolverConfig] = None, **kw):
+        pkw = {k: v for k, v in kw.items() if k in dict(ProblemConfig._fields_)}
+        skw = {k: v for k, v in kw.items() if k in dict(SolverConfig._fields_)}
+        unknown = set(kw) - set(pkw) - set(skw)
+        if unknown:
+            raise TypeError(f"unknown config keys {sorted(unknown)}")
+        self.problem = problem or default_problem_config(**pkw)
+        self.solver = solver or default_solver_config(**skw)
+        h = C.c_void_p()
+        _check(lib().gpt_create(C.byref(self.problem), C.byref(self.solver), C.byref(h)))
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().gpt_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_solver(self, **kw):
+        for k, v in kw.items():
+            setattr(self.solver, k, v)
+        _check(lib().gpt_set_solver_config(self._h, C.byref(self.solver)))
+
+    def set_profiling(self, enable: bool):
+        _check(lib().gpt_set_profiling(self._h, int(bool(enable))))
+
+    def phase_stats(self, reset: bool = False):
+        """{phase: (device ms, launches)} accumulated while profiling was on."""
+        ms = (C.c_double * len(PHASES))()
+        n = (C.c_uint64 * len(PHASES))()
+        _check(lib().gpt_get_phase_stats(self._h, C.cast(ms, C.c_void_p), C.cast(n, C.c_void_p), int(reset)))
+        return {p: (ms[i], n[i]) for i, p in enumerate(PHASES)}
+
+    # ---- the SQP solve (toplevel.cuh:24-503) ----
+    def sqp_solve(self, knot_points: int, eePos_traj, lam, xu, rho: float, rho_reset: float = 1e-3,
+                  stream=None) -> SqpResult:
+        r = C.c_float(rho)
+        st = SqpStats()
+        n = self.solver.sqp_max_iter
+        iters = (C.c_uint32 * n)()
+        ex = (C.c_uint8 * n)()
+        _check(lib().gpt_sqp_solve(self._h, knot_points, _ptr(eePos_traj), _ptr(lam), _ptr(xu), C.byref(r),
+                                   rho_reset, C.byref(st), C.cast(iters, C.c_void_p), C.cast(ex, C.c_void_p),
+                                   _stream(stream)))
+        k = st.sqp_iters
+        return SqpResult(list(iters)[:k], [bool(x) for x in list(ex)[:k]], k, r.value, st.as_dict())
+
+    def sqp_solve_batched(self, knot_points: Sequence[int], eePos_traj, lam, xu, rho: Sequence[float],
+                          rho_reset: float = 1e-3, stream=None):
+        B = len(knot_points)
+        Ns = (C.c_uint32 * B)(*knot_points)
+        rr = (C.c_float * B)(*rho)
+        sts = (SqpStats * B)()
+        _check(lib().gpt_sqp_solve_batched(self._h, B, C.cast(Ns, C.c_void_p), _ptr(eePos_traj), _ptr(lam),
+                                           _ptr(xu), C.cast(rr, C.c_void_p), rho_reset, C.cast(sts, C.c_void_p),
+                                           _stream(stream)))
+        return list(rr), [s.as_dict() for s in sts]
+
+    # ---- the reference's kernels, one instance ----
+    def form_kkt(self, N, xu, eePos, xs, G, Cm, g, c, stream=None):
+        _check(lib().gpt_form_kkt(self._h, N, _ptr(xu), _ptr(eePos), _ptr(xs), _ptr(G), _ptr(Cm), _ptr(g), _ptr(c),
+                                  _stream(stream)))
+
+    def form_schur(self, N, rho, G, Cm, g, c, S, Pinv, gamma, Ginv, stream=None):
+        _check(lib().gpt_form_schur(self._h, N, rho, _ptr(G), _ptr(Cm), _ptr(g), _ptr(c), _ptr(S), _ptr(Pinv),
+                                    _ptr(gamma), _ptr(Ginv), _stream(stream)))
+
+    def form_schur_csc(self, N, rho, G, Cm, g, c, val, gamma, Ginv, stream=None):
+        _check(lib().gpt_form_schur_csc(self._h, N, rho, _ptr(G), _ptr(Cm), _ptr(g), _ptr(c), _ptr(val),
+                                        _ptr(gamma), _ptr(Ginv), _stream(stream)))
+
+    def pcg(self, N, S, Pinv, gamma, lam, max_iter, exit_tol, exit_mode=0, stream=None):
+        it = C.c_uint32(0)
+        mx = C.c_uint8(0)
+        _check(lib().gpt_pcg(self._h, N, _ptr(S), _ptr(Pinv), _ptr(gamma), _ptr(lam), max_iter, exit_tol, exit_mode,
+                             C.byref(it), C.byref(mx), _stream(stream)))
+        return it.value, bool(mx.value)
+
+    def compute_dz(self, N, Ginv, Cm, g, lam, dz, stream=None):
+        _check(lib().gpt_compute_dz(self._h, N, _ptr(Ginv), _ptr(Cm), _ptr(g), _ptr(lam), _ptr(dz), _stream(stream)))
+
+    def compute_merit(self, N, xu, eePos, out, stream=None):
+        _check(lib().gpt_compute_merit(self._h, N, _ptr(xu), _ptr(eePos), _ptr(out), _stream(stream)))
+
+    def ls_compute_merit(self, N, xs, xu, eePos, dz, out, stream=None):
+        _check(lib().gpt_ls_compute_merit(self._h, N, _ptr(xs), _ptr(xu), _ptr(eePos), _ptr(dz), _ptr(out),
+                                          _stream(stream)))
+
+
+def prep_csr(N: int):
+    """CSC pattern of the Schur matrix's upper triangle (prep_csr, utils.cuh:84-118)."""
+    import numpy as np
+    nnz = 196 * (N - 1) + 105 * N
+    cp = np.zeros(14 * N + 1, np.int32)
+    ri = np.zeros(nnz, np.int32)
+    _check(lib().gpt_prep_csr(N, cp.ctypes.data_as(C.c_void_p), ri.ctypes.data_as(C.c_void_p)))
+    return cp, ri

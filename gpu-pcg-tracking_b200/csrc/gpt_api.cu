@@ -1,0 +1,540 @@
+// gpt_api.cu -- the C ABI (include/gpt.h): handle, preallocated workspace,
+// the reference's kernels as single-instance entry points, and the SQP loop
+// (toplevel.cuh:24-503) driven from the host with every decision on the device.
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/gpt.h"
+#include "gpt_common.cuh"
+#include "gpt_internal.h"
+
+using namespace gpt;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+gpt_status set_err(gpt_status st, const std::string &msg)
+{
+    g_last_error = msg;
+    return st;
+}
+gpt_status cuda_err(cudaError_t e, const char *where)
+{
+    return set_err(GPT_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+#define GPT_CUDA(call)                                        \
+    do {                                                      \
+        cudaError_t e_ = (call);                              \
+        if (e_ != cudaSuccess) return cuda_err(e_, #call);    \
+    } while (0)
+
+}  // namespace
+
+struct gpt_handle {
+    gpt_problem_config pc;
+    gpt_solver_config sc;
+    int device = 0;
+    int num_sms = 148;
+    size_t cap_knots = 0;  // max_batch * max_knot_points
+    // workspace
+    float *G = nullptr, *C = nullptr, *g = nullptr, *c = nullptr, *S = nullptr, *Pinv = nullptr,
+          *gamma = nullptr, *Ginv = nullptr, *dz = nullptr, *xs = nullptr, *knot_merit = nullptr,
+          *merits = nullptr;
+    InstState *st = nullptr;
+    int *knot_off = nullptr, *knot_inst = nullptr;
+    uint32_t *pcg_log = nullptr, *pcg_out = nullptr, *d_active = nullptr;
+    // pinned host staging
+    uint32_t *h_active = nullptr;
+    InstState *h_st = nullptr;
+    uint32_t *h_pcg_out = nullptr;
+    uint32_t *h_pcg_log = nullptr;
+    // cached batch layout
+    std::vector<int> off_cache;
+    cudaEvent_t ev = nullptr;
+    // optional per-phase CUDA-event timing of the SQP loop's launches
+    int profile = 0;
+    std::vector<cudaEvent_t> ev_pool;
+    std::vector<int> ev_phase;
+    size_t ev_used = 0;
+    double phase_ms[GPT_NUM_PHASES] = {0};
+    uint64_t phase_launches[GPT_NUM_PHASES] = {0};
+};
+
+namespace {
+
+ProblemParams to_params(const gpt_problem_config &pc)
+{
+    ProblemParams P;
+    P.dt = pc.timestep;
+    P.integrator = (int)pc.integrator;
+    P.q_ee = pc.q_ee;
+    P.qd_cost = pc.qd_cost;
+    P.r_cost = pc.r_cost;
+    P.mu = pc.mu;
+    P.ref_terminal = (int)pc.ref_terminal;
+    return P;
+}
+SolverParams to_solver(const gpt_solver_config &sc)
+{
+    SolverParams S;
+    S.sqp_max_iter = sc.sqp_max_iter;
+    S.pcg_max_iter = sc.pcg_max_iter;
+    S.pcg_tol = sc.pcg_exit_tol;
+    S.pcg_exit_mode = sc.pcg_exit_mode;
+    S.rho_factor = sc.rho_factor;
+    S.rho_max = sc.rho_max;
+    S.rho_min = sc.rho_min;
+    return S;
+}
+BatchView single_view(uint32_t N)
+{
+    BatchView bv;
+    bv.B = 1;
+    bv.total_knots = (int)N;
+    bv.knot_off = nullptr;
+    bv.knot_inst = nullptr;
+    bv.st = nullptr;
+    return bv;
+}
+bool check_n(const gpt_handle *h, uint32_t N) { return N >= 2 && N <= h->pc.max_knot_points; }
+
+template <typename T>
+cudaError_t dalloc(T **p, size_t n)
+{
+    return cudaMalloc((void **)p, sizeof(T) * (n ? n : 1));
+}
+
+}  // namespace
+
+extern "C" {
+
+void gpt_default_problem_config(gpt_problem_config *o)
+{
+    if (!o) return;
+    o->state_size = 14;
+    o->control_size = 7;
+    o->max_knot_points = 128;
+    o->max_batch = 1;
+    o->timestep = 1.0f / 64.0f;
+    o->integrator = 0;
+    o->q_ee = 1.0f;
+    o->qd_cost = 1e-4f;
+    o->r_cost = 1e-4f;
+    o->mu = 10.0f;
+    o->ref_terminal = 1;
+}
+
+void gpt_default_solver_config(gpt_solver_config *o)
+{
+    if (!o) return;
+    o->sqp_max_iter = 40;
+    o->pcg_max_iter = 167;
+    o->pcg_exit_tol = 1e-5f;
+    o->pcg_exit_mode = 0;
+    o->rho_factor = 1.2f;
+    o->rho_max = 10.0f;
+    o->rho_min = 1e-3f;
+}
+
+const char *gpt_last_error(void) { return g_last_error.c_str(); }
+const char *gpt_version(void) { return "gpt-b200 0.1 (sm_100a)"; }
+
+gpt_status gpt_set_solver_config(gpt_handle *h, const gpt_solver_config *sc)
+{
+    if (!h || !sc) return set_err(GPT_ERR_BAD_ARG, "null argument");
+    if (sc->sqp_max_iter == 0 || sc->sqp_max_iter > 4096) return set_err(GPT_ERR_BAD_ARG, "sqp_max_iter out of range");
+    if (!(sc->rho_factor > 1.0f) || !(sc->rho_min > 0.0f)) return set_err(GPT_ERR_BAD_ARG, "rho schedule out of range");
+    if (sc->sqp_max_iter > h->sc.sqp_max_iter && h->pcg_log) {
+        // pcg log is sized at creation
+        return set_err(GPT_ERR_CAPACITY, "sqp_max_iter larger than at creation");
+    }
+    h->sc = *sc;
+    return GPT_OK;
+}
+
+gpt_status gpt_create(const gpt_problem_config *pc, const gpt_solver_config *sc, gpt_handle **out)
+{
+    if (!pc || !sc || !out) return set_err(GPT_ERR_BAD_ARG, "null argument");
+    *out = nullptr;
+    if (pc->state_size != 14 || pc->control_size != 7)
+        return set_err(GPT_ERR_BAD_ARG, "state_size must be 14 and control_size 7 (iiwa14)");
+    if (pc->max_knot_points < 2 || pc->max_knot_points > (uint32_t)MAX_PCG_KNOTS)
+        return set_err(GPT_ERR_BAD_ARG, "max_knot_points must be in [2, 512]");
+    if (pc->max_batch < 1 || pc->max_batch > 65536) return set_err(GPT_ERR_BAD_ARG, "max_batch out of range");
+    if (!(pc->timestep > 0.f) || pc->integrator > 1) return set_err(GPT_ERR_BAD_ARG, "bad timestep/integrator");
+    if (sc->sqp_max_iter == 0 || sc->sqp_max_iter > 4096) return set_err(GPT_ERR_BAD_ARG, "sqp_max_iter out of range");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return set_err(GPT_ERR_NO_DEVICE, "no CUDA device");
+    }
+    gpt_handle *h = new gpt_handle();
+    h->pc = *pc;
+    h->sc = *sc;
+    cudaGetDevice(&h->device);
+    cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, h->device);
+    const size_t T = (size_t)pc->max_batch * pc->max_knot_points;
+    const size_t B = pc->max_batch;
+    h->cap_knots = T;
+    cudaError_t e = cudaSuccess;
+#define ALLOC(p, n) \
+    if (e == cudaSuccess) e = dalloc(&h->p, (n))
+    ALLOC(G, G_STRIDE * T);
+    ALLOC(C, C_STRIDE * T);
+    ALLOC(g, NX * T);
+    ALLOC(c, NS * T);
+    ALLOC(S, S_STRIDE * T);
+    ALLOC(Pinv, SS * T);
+    ALLOC(gamma, NS * T);
+    ALLOC(Ginv, G_STRIDE * T);
+    ALLOC(dz, NX * T);
+    ALLOC(xs, NS * B);
+    ALLOC(knot_merit, NUM_ALPHAS * T);
+    ALLOC(merits, NUM_ALPHAS * B);
+    ALLOC(st, B);
+    ALLOC(knot_off, B + 1);
+    ALLOC(knot_inst, T);
+    ALLOC(pcg_log, B * sc->sqp_max_iter);
+    ALLOC(pcg_out, 2 * B);
+    ALLOC(d_active, 1);
+#undef ALLOC
+    if (e == cudaSuccess) e = cudaMallocHost((void **)&h->h_active, sizeof(uint32_t));
+    if (e == cudaSuccess) e = cudaMallocHost((void **)&h->h_st, sizeof(InstState) * B);
+    if (e == cudaSuccess) e = cudaMallocHost((void **)&h->h_pcg_out, sizeof(uint32_t) * 2 * B);
+    if (e == cudaSuccess) e = cudaMallocHost((void **)&h->h_pcg_log, sizeof(uint32_t) * B * sc->sqp_max_iter);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->ev, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaMemset(h->Pinv, 0, sizeof(float) * SS * T);
+    if (e == cudaSuccess) e = cudaMemset(h->dz, 0, sizeof(float) * NX * T);
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) {
+        gpt_destroy(h);
+        return cuda_err(e, "gpt_create workspace");
+    }
+    *out = h;
+    return GPT_OK;
+}
+
+gpt_status gpt_set_profiling(gpt_handle *h, int enable)
+{
+    if (!h) return set_err(GPT_ERR_BAD_ARG, "null handle");
+    h->profile = enable ? 1 : 0;
+    return GPT_OK;
+}
+
+gpt_status gpt_get_phase_stats(gpt_handle *h, double *h_ms, uint64_t *h_launches, int reset)
+{
+    if (!h) return set_err(GPT_ERR_BAD_ARG, "null handle");
+    for (int i = 0; i < GPT_NUM_PHASES; ++i) {
+        if (h_ms) h_ms[i] = h->phase_ms[i];
+        if (h_launches) h_launches[i] = h->phase_launches[i];
+        if (reset) {
+            h->phase_ms[i] = 0.0;
+            h->phase_launches[i] = 0;
+        }
+    }
+    return GPT_OK;
+}
+
+gpt_status gpt_destroy(gpt_handle *h)
+{
+    if (!h) return GPT_OK;
+    for (cudaEvent_t e : h->ev_pool) cudaEventDestroy(e);
+    cudaFree(h->G); cudaFree(h->C); cudaFree(h->g); cudaFree(h->c); cudaFree(h->S); cudaFree(h->Pinv);
+    cudaFree(h->gamma); cudaFree(h->Ginv); cudaFree(h->dz); cudaFree(h->xs); cudaFree(h->knot_merit);
+    cudaFree(h->merits); cudaFree(h->st); cudaFree(h->knot_off); cudaFree(h->knot_inst); cudaFree(h->pcg_log);
+    cudaFree(h->pcg_out); cudaFree(h->d_active);
+    cudaFreeHost(h->h_active); cudaFreeHost(h->h_st); cudaFreeHost(h->h_pcg_out); cudaFreeHost(h->h_pcg_log);
+    if (h->ev) cudaEventDestroy(h->ev);
+    delete h;
+    return GPT_OK;
+}
+
+// ---------------------------------------------------------------------------
+// single-instance kernels
+// ---------------------------------------------------------------------------
+
+gpt_status gpt_form_kkt(gpt_handle *h, uint32_t N, const float *d_xu, const float *d_goal, const float *d_xs,
+                        float *d_G, float *d_C, float *d_g, float *d_c, gpt_stream_t stream)
+{
+    if (!h || !d_xu || !d_goal || !d_xs || !d_G || !d_C || !d_g || !d_c) return set_err(GPT_ERR_BAD_ARG, "null argument");
+    if (!check_n(h, N)) return set_err(GPT_ERR_BAD_ARG, "knot_points out of range");
+    GPT_CUDA(launch_kkt(single_view(N), to_params(h->pc), d_xu, d_goal, d_xs, d_G, d_C, d_g, d_c, h->num_sms,
+                        (cudaStream_t)stream));
+    return GPT_OK;
+}
+
+gpt_status gpt_form_schur(gpt_handle *h, uint32_t N, float rho, const float *d_G, const float *d_C, const float *d_g,
+                          const float *d_c, float *d_S, float *d_Pinv, float *d_gamma, float *d_Ginv,
+                          gpt_stream_t stream)
+{
+    if (!h || !d_G || !d_C || !d_g || !d_c || !d_S || !d_Pinv || !d_gamma || !d_Ginv)
+        return set_err(GPT_ERR_BAD_ARG, "null argument");
+    if (!check_n(h, N)) return set_err(GPT_ERR_BAD_ARG, "knot_points out of range");
+    GPT_CUDA(launch_schur(0, single_view(N), rho, d_G, d_C, d_g, d_c, d_S, d_Pinv, d_gamma, d_Ginv, nullptr,
+                          h->num_sms, (cudaStream_t)stream));
+    return GPT_OK;
+}
+
+gpt_status gpt_form_schur_csc(gpt_handle *h, uint32_t N, float rho, const float *d_G, const float *d_C,
+                              const float *d_g, const float *d_c, float *d_val, float *d_gamma, float *d_Ginv,
+                              gpt_stream_t stream)
+{
+    if (!h || !d_G || !d_C || !d_g || !d_c || !d_val || !d_gamma || !d_Ginv)
+        return set_err(GPT_ERR_BAD_ARG, "null argument");
+    if (!check_n(h, N)) return set_err(GPT_ERR_BAD_ARG, "knot_points out of range");
+    GPT_CUDA(launch_schur(2, single_view(N), rho, d_G, d_C, d_g, d_c, nullptr, nullptr, d_gamma, d_Ginv, d_val,
+                          h->num_sms, (cudaStream_t)stream));
+    return GPT_OK;
+}
+
+gpt_status gpt_prep_csr(uint32_t N, int32_t *cp, int32_t *ri)
+{
+    if (!cp || !ri || N < 1) return set_err(GPT_ERR_BAD_ARG, "bad argument");
+    const int tri = (NS + 1) * NS / 2, brow = SS + tri;
+    cp[0] = 0;
+    for (uint32_t b = 0; b < N; ++b)
+        for (int r = 0; r < NS; ++r) {
+            const int bb = (int)b;
+            const int off = (bb > 0) * tri + (bb > 0) * (bb - 1) * brow + (bb > 0) * r * NS + (r + 1) * r / 2;
+            const int len = (bb > 0) * NS + r + 1;
+            cp[bb * NS + r + 1] = off + len;
+            for (int k = 0; k < len; ++k) ri[off + k] = (bb > 0) * (bb - 1) * NS + k;
+        }
+    return GPT_OK;
+}
+
+gpt_status gpt_pcg(gpt_handle *h, uint32_t N, const float *d_S, const float *d_Pinv, const float *d_gamma,
+                   float *d_lambda, uint32_t max_iter, float tol, uint32_t exit_mode, uint32_t *h_iters,
+                   uint8_t *h_maxit, gpt_stream_t stream)
+{
+    if (!h || !d_S || !d_Pinv || !d_gamma || !d_lambda) return set_err(GPT_ERR_BAD_ARG, "null argument");
+    if (!check_n(h, N) || exit_mode > 1) return set_err(GPT_ERR_BAD_ARG, "knot_points/exit_mode out of range");
+    cudaStream_t s = (cudaStream_t)stream;
+    GPT_CUDA(launch_pcg(single_view(N), (int)N, d_S, d_Pinv, S_STRIDE, SS, d_gamma, d_lambda, (int)max_iter, tol,
+                        (int)exit_mode, h->pcg_out, nullptr, 0, h->num_sms, s));
+    GPT_CUDA(cudaMemcpyAsync(h->h_pcg_out, h->pcg_out, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    GPT_CUDA(cudaStreamSynchronize(s));
+    if (h_iters) *h_iters = h->h_pcg_out[0];
+    if (h_maxit) *h_maxit = (uint8_t)(h->h_pcg_out[1] & 1u);
+    if (h->h_pcg_out[1] & 2u) return set_err(GPT_ERR_NONFINITE, "non-finite value in PCG");
+    return GPT_OK;
+}
+
+gpt_status gpt_compute_dz(gpt_handle *h, uint32_t N, const float *d_Ginv, const float *d_C, const float *d_g,
+                          const float *d_lambda, float *d_dz, gpt_stream_t stream)
+{
+    if (!h || !d_Ginv || !d_C || !d_g || !d_lambda || !d_dz) return set_err(GPT_ERR_BAD_ARG, "null argument");
+    if (!check_n(h, N)) return set_err(GPT_ERR_BAD_ARG, "knot_points out of range");
+    GPT_CUDA(launch_dz(single_view(N), d_Ginv, d_C, d_g, d_lambda, d_dz, h->num_sms, (cudaStream_t)stream));
+    return GPT_OK;
+}
+
+gpt_status gpt_compute_merit(gpt_handle *h, uint32_t N, const float *d_xu, const float *d_goal, float *d_merit,
+                             gpt_stream_t stream)
+{
+    if (!h || !d_xu || !d_goal || !d_merit) return set_err(GPT_ERR_BAD_ARG, "null argument");
+    if (!check_n(h, N)) return set_err(GPT_ERR_BAD_ARG, "knot_points out of range");
+    cudaStream_t s = (cudaStream_t)stream;
+    BatchView bv = single_view(N);
+    GPT_CUDA(launch_merit(bv, to_params(h->pc), 1, d_xu, nullptr, d_goal, nullptr, h->knot_merit, h->num_sms, s));
+    GPT_CUDA(launch_accept(bv, 0, to_solver(h->sc), h->knot_merit, nullptr, nullptr, h->merits, nullptr, h->num_sms, s));
+    GPT_CUDA(cudaMemcpyAsync(d_merit, h->merits, sizeof(float), cudaMemcpyDeviceToDevice, s));
+    return GPT_OK;
+}
+
+gpt_status gpt_ls_compute_merit(gpt_handle *h, uint32_t N, const float *d_xs, const float *d_xu, const float *d_goal,
+                                const float *d_dz, float *d_merits, gpt_stream_t stream)
+{
+    if (!h || !d_xs || !d_xu || !d_goal || !d_dz || !d_merits) return set_err(GPT_ERR_BAD_ARG, "null argument");
+    if (!check_n(h, N)) return set_err(GPT_ERR_BAD_ARG, "knot_points out of range");
+    cudaStream_t s = (cudaStream_t)stream;
+    BatchView bv = single_view(N);
+    GPT_CUDA(launch_merit(bv, to_params(h->pc), NUM_ALPHAS, d_xu, d_dz, d_goal, d_xs, h->knot_merit, h->num_sms, s));
+    GPT_CUDA(launch_accept(bv, 2, to_solver(h->sc), h->knot_merit, nullptr, nullptr, h->merits, nullptr, h->num_sms, s));
+    GPT_CUDA(cudaMemcpyAsync(d_merits, h->merits, NUM_ALPHAS * sizeof(float), cudaMemcpyDeviceToDevice, s));
+    return GPT_OK;
+}
+
+// ---------------------------------------------------------------------------
+// SQP loop
+// ---------------------------------------------------------------------------
+
+// Brackets one phase launch with a pair of events when profiling is on.
+struct PhaseTimer {
+    gpt_handle *h;
+    cudaStream_t s;
+    int phase;
+    size_t slot = (size_t)-1;
+    PhaseTimer(gpt_handle *h_, cudaStream_t s_, int phase_) : h(h_), s(s_), phase(phase_)
+    {
+        if (!h->profile) return;
+        if (h->ev_used + 2 > h->ev_pool.size()) {
+            for (int i = 0; i < 64; ++i) {
+                cudaEvent_t e;
+                if (cudaEventCreate(&e) != cudaSuccess) return;
+                h->ev_pool.push_back(e);
+                h->ev_phase.push_back(0);
+            }
+        }
+        slot = h->ev_used;
+        h->ev_used += 2;
+        h->ev_phase[slot] = phase;
+        cudaEventRecord(h->ev_pool[slot], s);
+    }
+    ~PhaseTimer()
+    {
+        if (slot != (size_t)-1) cudaEventRecord(h->ev_pool[slot + 1], s);
+    }
+};
+
+// After the stream synchronised: fold the recorded event pairs into the per-phase totals.
+static void collect_phase_times(gpt_handle *h)
+{
+    for (size_t i = 0; i + 1 < h->ev_used; i += 2) {
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, h->ev_pool[i], h->ev_pool[i + 1]) == cudaSuccess) {
+            h->phase_ms[h->ev_phase[i]] += ms;
+            h->phase_launches[h->ev_phase[i]] += 1;
+        }
+    }
+    h->ev_used = 0;
+}
+
+static gpt_status sqp_run(gpt_handle *h, uint32_t B, const uint32_t *Ns, const float *d_goal, float *d_lambda,
+                          float *d_xu, float *h_rho, float rho_reset, gpt_sqp_stats *h_stats, uint32_t *h_pcg_iters,
+                          uint8_t *h_pcg_exit, cudaStream_t s)
+{
+    if (B == 0 || B > h->pc.max_batch) return set_err(GPT_ERR_CAPACITY, "batch exceeds handle capacity");
+    // batch layout
+    std::vector<int> off(B + 1, 0);
+    for (uint32_t b = 0; b < B; ++b) {
+        if (!check_n(h, Ns[b])) return set_err(GPT_ERR_BAD_ARG, "knot_points out of range");
+        off[b + 1] = off[b] + (int)Ns[b];
+    }
+    const int total = off[B];
+    if ((size_t)total > h->cap_knots) return set_err(GPT_ERR_CAPACITY, "total knots exceed workspace");
+    int maxN = 0;
+    for (uint32_t b = 0; b < B; ++b) maxN = Ns[b] > (uint32_t)maxN ? (int)Ns[b] : maxN;
+    if (off != h->off_cache) {
+        std::vector<int> inst(total);
+        for (uint32_t b = 0; b < B; ++b)
+            for (int k = off[b]; k < off[b + 1]; ++k) inst[k] = (int)b;
+        GPT_CUDA(cudaMemcpy(h->knot_off, off.data(), sizeof(int) * (B + 1), cudaMemcpyHostToDevice));
+        GPT_CUDA(cudaMemcpy(h->knot_inst, inst.data(), sizeof(int) * total, cudaMemcpyHostToDevice));
+        h->off_cache = off;
+    }
+    for (uint32_t b = 0; b < B; ++b) {
+        InstState &st = h->h_st[b];
+        std::memset(&st, 0, sizeof(st));
+        st.rho = h_rho ? h_rho[b] : 1e-3f;
+        st.drho = 1.0f;
+        st.rho_reset = rho_reset;
+        st.active = 1;
+    }
+    GPT_CUDA(cudaMemcpyAsync(h->st, h->h_st, sizeof(InstState) * B, cudaMemcpyHostToDevice, s));
+    BatchView bv;
+    bv.B = (int)B;
+    bv.total_knots = total;
+    bv.knot_off = h->knot_off;
+    bv.knot_inst = h->knot_inst;
+    bv.st = h->st;
+    const ProblemParams P = to_params(h->pc);
+    const SolverParams SP = to_solver(h->sc);
+    const int ns = h->num_sms;
+
+    {
+        PhaseTimer t(h, s, GPT_PHASE_INIT);
+        GPT_CUDA(launch_init(bv, d_xu, h->xs, ns, s));
+        GPT_CUDA(launch_merit(bv, P, 1, d_xu, nullptr, d_goal, h->xs, h->knot_merit, ns, s));
+        GPT_CUDA(launch_accept(bv, 0, SP, h->knot_merit, nullptr, nullptr, nullptr, nullptr, ns, s));
+    }
+    for (uint32_t it = 0; it < SP.sqp_max_iter; ++it) {
+        {
+            PhaseTimer t(h, s, GPT_PHASE_KKT);
+            GPT_CUDA(launch_kkt(bv, P, d_xu, d_goal, h->xs, h->G, h->C, h->g, h->c, ns, s));
+        }
+        {
+            PhaseTimer t(h, s, GPT_PHASE_SCHUR);
+            GPT_CUDA(launch_schur(1, bv, 0.f, h->G, h->C, h->g, h->c, h->S, h->Pinv, h->gamma, h->Ginv, nullptr, ns, s));
+        }
+        {
+            PhaseTimer t(h, s, GPT_PHASE_PCG);
+            GPT_CUDA(launch_pcg(bv, maxN, h->S, h->Pinv, SS, 0, h->gamma, d_lambda, (int)SP.pcg_max_iter, SP.pcg_tol,
+                                (int)SP.pcg_exit_mode, nullptr, h->pcg_log, (int)SP.sqp_max_iter, ns, s));
+        }
+        {
+            PhaseTimer t(h, s, GPT_PHASE_DZ);
+            GPT_CUDA(launch_dz(bv, h->Ginv, h->C, h->g, d_lambda, h->dz, ns, s));
+        }
+        {
+            PhaseTimer t(h, s, GPT_PHASE_MERIT);
+            GPT_CUDA(launch_merit(bv, P, NUM_ALPHAS, d_xu, h->dz, d_goal, h->xs, h->knot_merit, ns, s));
+        }
+        GPT_CUDA(cudaMemsetAsync(h->d_active, 0, sizeof(uint32_t), s));
+        {
+            PhaseTimer t(h, s, GPT_PHASE_ACCEPT);
+            GPT_CUDA(launch_accept(bv, 1, SP, h->knot_merit, h->dz, d_xu, nullptr, h->d_active, ns, s));
+        }
+        GPT_CUDA(cudaMemcpyAsync(h->h_active, h->d_active, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+        GPT_CUDA(cudaEventRecord(h->ev, s));
+        GPT_CUDA(cudaEventSynchronize(h->ev));
+        if (*h->h_active == 0) break;
+    }
+    GPT_CUDA(cudaMemcpyAsync(h->h_st, h->st, sizeof(InstState) * B, cudaMemcpyDeviceToHost, s));
+    if (h_pcg_iters || h_pcg_exit)
+        GPT_CUDA(cudaMemcpyAsync(h->h_pcg_log, h->pcg_log, sizeof(uint32_t) * SP.sqp_max_iter, cudaMemcpyDeviceToHost, s));
+    GPT_CUDA(cudaStreamSynchronize(s));
+    if (h->profile) collect_phase_times(h);
+    bool nonfinite = false;
+    for (uint32_t b = 0; b < B; ++b) {
+        const InstState &st = h->h_st[b];
+        if (h_rho) h_rho[b] = st.rho;
+        if (st.exit_flags & 4u) nonfinite = true;
+        if (h_stats) {
+            gpt_sqp_stats &o = h_stats[b];
+            o.sqp_iters = st.sqp_iters;
+            o.exit_flags = st.exit_flags | (st.pcg_maxiter_count ? GPT_EXIT_PCG_MAXITER : 0u);
+            o.pcg_iters_total = st.pcg_iters_total;
+            o.pcg_maxiter_count = st.pcg_maxiter_count;
+            o.ls_fail_count = st.ls_fail_count;
+            o.merit_initial = st.merit_init;
+            o.merit_final = st.merit0;
+            o.rho_final = st.rho;
+        }
+    }
+    if (h_pcg_iters || h_pcg_exit) {
+        const uint32_t n = h->h_st[0].sqp_iters;
+        for (uint32_t i = 0; i < SP.sqp_max_iter; ++i) {
+            const uint32_t v = (i < n) ? h->h_pcg_log[i] : 0u;
+            if (h_pcg_iters) h_pcg_iters[i] = v & 0x7fffffffu;
+            if (h_pcg_exit) h_pcg_exit[i] = (uint8_t)(v >> 31);
+        }
+    }
+    if (nonfinite) return set_err(GPT_ERR_NONFINITE, "non-finite merit or PCG reduction in at least one instance");
+    return GPT_OK;
+}
+
+gpt_status gpt_sqp_solve(gpt_handle *h, uint32_t N, const float *d_goal, float *d_lambda, float *d_xu, float *h_rho,
+                         float rho_reset, gpt_sqp_stats *h_stats, uint32_t *h_pcg_iters, uint8_t *h_pcg_exit,
+                         gpt_stream_t stream)
+{
+    if (!h || !d_goal || !d_lambda || !d_xu || !h_rho) return set_err(GPT_ERR_BAD_ARG, "null argument");
+    return sqp_run(h, 1, &N, d_goal, d_lambda, d_xu, h_rho, rho_reset, h_stats, h_pcg_iters, h_pcg_exit,
+                   (cudaStream_t)stream);
+}
+
+gpt_status gpt_sqp_solve_batched(gpt_handle *h, uint32_t B, const uint32_t *h_N, const float *d_goal, float *d_lambda,
+                                 float *d_xu, float *h_rho, float rho_reset, gpt_sqp_stats *h_stats,
+                                 gpt_stream_t stream)
+{
+    if (!h || !h_N || !d_goal || !d_lambda || !d_xu) return set_err(GPT_ERR_BAD_ARG, "null argument");
+    return sqp_run(h, B, h_N, d_goal, d_lambda, d_xu, h_rho, rho_reset, h_stats, nullptr, nullptr,
+                   (cudaStream_t)stream);
+}
+
+}  // extern "C"

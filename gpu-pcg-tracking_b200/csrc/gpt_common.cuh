@@ -1,0 +1,83 @@
+// gpt_common.cuh -- layouts, batch descriptors and small device helpers shared
+// by the kernels of the SQP inner loop.
+//
+// Buffers keep the reference's per-knot block layouts (toplevel.cuh:42-50,
+// utils.cuh:121-187) so single-instance calls accept reference-sized buffers.
+// A batch concatenates instances knot by knot: knot j of the batch belongs to
+// instance b = knot_inst[j], local index k = j - knot_off[b], and every
+// per-knot block of every buffer sits at (stride * j).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace gpt {
+
+constexpr int NQ = 7;            // joints
+constexpr int NS = 14;           // state size (settings.cuh:4)
+constexpr int NC = 7;            // control size
+constexpr int NX = NS + NC;      // 21 floats of xu per knot
+constexpr int SS = NS * NS;      // 196
+constexpr int SC = NS * NC;      // 98
+constexpr int CC = NC * NC;      // 49
+constexpr int G_STRIDE = SS + CC;        // 245 (toplevel.cuh:46)
+constexpr int C_STRIDE = SS + SC;        // 294 (toplevel.cuh:47)
+constexpr int S_STRIDE = 3 * SS;         // 588 (toplevel.cuh:103)
+constexpr int NUM_ALPHAS = 8;            // toplevel.cuh:55
+constexpr int MAX_KNOTS = 1024;          // per-instance horizon limit of this build
+
+// Per-instance SQP state kept on the device across the phases of one solve.
+struct InstState {
+    float rho, drho, merit0, merit_init;
+    float rho_reset;
+    uint32_t active;          // 1 while the SQP loop of this instance runs
+    uint32_t sqp_iters;
+    uint32_t exit_flags;      // GPT_EXIT_* bits (include/gpt.h)
+    uint32_t pcg_iters_total;
+    uint32_t pcg_maxiter_count;
+    uint32_t ls_fail_count;
+    uint32_t last_pcg_iters;
+    uint32_t last_pcg_exit;
+    uint32_t pad[3];
+};
+
+struct BatchView {
+    int B;                   // instances
+    int total_knots;         // sum of horizons
+    const int *knot_off;     // [B+1] prefix offsets, nullptr => single instance of total_knots
+    const int *knot_inst;    // [total_knots] owning instance, nullptr => single instance
+    InstState *st;           // [B] or nullptr (always active)
+
+    __device__ __forceinline__ int inst(int j) const { return knot_inst ? knot_inst[j] : 0; }
+    __device__ __forceinline__ int off(int b) const { return knot_off ? knot_off[b] : 0; }
+    __device__ __forceinline__ int N(int b) const
+    {
+        return knot_off ? knot_off[b + 1] - knot_off[b] : total_knots;
+    }
+    __device__ __forceinline__ bool active(int b) const { return st == nullptr || st[b].active != 0; }
+};
+
+// Physical problem parameters (the reference's compile-time macros, runtime here).
+struct ProblemParams {
+    float dt;          // timestep (runme.cu:65)
+    int integrator;    // 0 explicit Euler, 1 semi-implicit Euler (integrator.cuh:25-126)
+    float q_ee;        // end-effector position weight
+    float qd_cost;     // QD_COST
+    float r_cost;      // R_COST
+    float mu;          // merit penalty (toplevel.cuh:54)
+    int ref_terminal;  // 1: terminal Q,q at x_{N-2} like iiwa_eepos_plant.cuh:399
+};
+
+__device__ __forceinline__ float warp_sum(float v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+__device__ __forceinline__ double warp_sum(double v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+}  // namespace gpt

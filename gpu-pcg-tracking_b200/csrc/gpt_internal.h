@@ -1,0 +1,40 @@
+// gpt_internal.h -- launchers shared between the kernel files and the C-ABI.
+#pragma once
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "gpt_common.cuh"
+
+namespace gpt {
+
+constexpr int MAX_PCG_KNOTS = 512;  // one thread block per instance holds 2 x 14 N floats
+
+// SQP control constants (settings.cuh:31-50 and the -D flags of perform_experiment.sh:42-58)
+struct SolverParams {
+    uint32_t sqp_max_iter;
+    uint32_t pcg_max_iter;
+    float pcg_tol;
+    uint32_t pcg_exit_mode;
+    float rho_factor, rho_max, rho_min;
+};
+
+cudaError_t launch_kkt(const BatchView &bv, const ProblemParams &P, const float *xu, const float *goal,
+                       const float *xs, float *G, float *C, float *g, float *c, int num_sms, cudaStream_t s);
+cudaError_t launch_schur(int mode, const BatchView &bv, float rho_scalar, const float *G, const float *C,
+                         const float *g, const float *c, float *S, float *Pinv, float *gamma, float *Ginv,
+                         float *csc_val, int num_sms, cudaStream_t s);
+size_t pcg_smem_bytes(int max_n_knots);
+cudaError_t launch_pcg(const BatchView &bv, int max_n_knots, const float *S, const float *Pinv, int pinv_stride,
+                       int pinv_off, const float *gamma, float *lambda, int max_iter, float tol, int exit_mode,
+                       uint32_t *out_iters, uint32_t *pcg_log, int log_stride, int num_sms, cudaStream_t s);
+cudaError_t launch_dz(const BatchView &bv, const float *Ginv, const float *C, const float *g, const float *lambda,
+                      float *dz, int num_sms, cudaStream_t s);
+cudaError_t launch_merit(const BatchView &bv, const ProblemParams &P, int n_alpha, const float *xu, const float *dz,
+                         const float *goal, const float *xs, float *knot_merit, int num_sms, cudaStream_t s);
+cudaError_t launch_accept(const BatchView &bv, int mode, const SolverParams &SP, const float *knot_merit,
+                          const float *dz, float *xu, float *merits_out, uint32_t *active_count, int num_sms,
+                          cudaStream_t s);
+cudaError_t launch_init(const BatchView &bv, const float *xu, float *xs, int num_sms, cudaStream_t s);
+
+}  // namespace gpt

@@ -1,0 +1,262 @@
+// gpt_kkt.cu -- KKT formation: one warp per knot.
+//
+// Replaces gato_form_kkt (schur.cuh:391-524) with the per-knot pieces it
+// calls: integratorAndGradient (integrator.cuh:159-183), the plant's
+// forwardDynamicsAndGradient (rbdfiles/iiwa_eepos_plant.cuh:126-156) and
+// trackingCostGradientAndHessian[_lastblock] (iiwa_eepos_plant.cuh:295-401).
+//
+// Per knot k < N-1 the warp computes, with no block-wide barrier:
+//   lanes 0..6   M(q) e_j  (inverse dynamics with qd = 0, qdd = e_j)
+//   lane  7      c(q, qd)  (bias force)
+//   lanes 0..7   FP64 Cholesky of M: Minv columns and qdd = Minv (u - c)
+//   lanes 0..13  d ID(q, qd, qdd) / d(q_j | qd_j)  (forward-mode RNEA tangent)
+//   all lanes    df/du = [-Minv dID/dx, Minv], A_k, B_k, defect, cost terms
+// and writes the reference blocks G_k = {Q_k, R_k}, C_k = {-A_k, -B_k},
+// g_k = {q_k, r_k}, c_{k+1}.  The warp of knot N-2 also writes the terminal
+// Q_{N-1}, q_{N-1} and c_0 = x_0 - x_s (schur.cuh:429-479).
+#include "gpt_common.cuh"
+#include "gpt_dyn.cuh"
+#include "gpt_internal.h"
+
+namespace gpt {
+
+struct KktWarpSmem {
+    float x[NS], u[NC], xn[NS];
+    float goal[12];
+    float M[CC];
+    float cbias[NQ];
+    float Minv[CC];
+    float qdd[NQ];
+    float dc[NQ * NS];     // dID/dx, col-major 7x14
+    float dfdu[NQ * NX];   // [dqdd/dq dqdd/dqd dqdd/du], col-major 7x21
+    float ee[2][3];
+    float J[2][21];
+    float qv[2][NS];
+};
+
+constexpr int KKT_WARPS = 4;
+
+__global__ void __launch_bounds__(32 * KKT_WARPS) kkt_kernel(BatchView bv, ProblemParams P, const float *__restrict__ xu,
+                                                           const float *__restrict__ goal,
+                                                           const float *__restrict__ xs, float *__restrict__ G,
+                                                           float *__restrict__ Cm, float *__restrict__ g,
+                                                           float *__restrict__ c)
+{
+    __shared__ KktWarpSmem smem_all[KKT_WARPS];
+    const int lane = threadIdx.x & 31;
+    KktWarpSmem &sm = smem_all[threadIdx.x >> 5];
+    const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+
+    for (int j = gw; j < bv.total_knots; j += nw) {
+        const int b = bv.inst(j);
+        const int N = bv.N(b);
+        const int k = j - bv.off(b);
+        if (k >= N - 1 || !bv.active(b)) continue;
+        const bool terminal = (k == N - 2);
+
+        // ---- stage x_k, u_k, x_{k+1}, goal_k, goal_{k+1}
+        const float *xk = xu + (size_t)NX * j;
+        for (int i = lane; i < NX + NS; i += 32) {
+            float v = xk[i];
+            if (i < NS) sm.x[i] = v;
+            else if (i < NX) sm.u[i - NS] = v;
+            else sm.xn[i - NX] = v;
+        }
+        if (lane < 12) sm.goal[lane] = goal[(size_t)6 * j + lane];
+        __syncwarp();
+
+        JointTrig trig;
+        joint_trig(sm.x, trig);
+
+        // ---- mass-matrix columns and bias force
+        {
+            float qd[NQ], qdd[NQ], tau[NQ];
+#pragma unroll
+            for (int i = 0; i < NQ; ++i) {
+                qd[i] = (lane == 7) ? sm.x[NQ + i] : 0.f;
+                qdd[i] = (lane == i) ? 1.f : 0.f;
+            }
+            rnea<false>(trig, qd, qdd, -1, -1, tau, nullptr);
+            if (lane < NQ) {
+#pragma unroll
+                for (int r = 0; r < NQ; ++r) sm.M[NQ * lane + r] = tau[r];
+            } else if (lane == NQ) {
+#pragma unroll
+                for (int r = 0; r < NQ; ++r) sm.cbias[r] = tau[r];
+            }
+        }
+        __syncwarp();
+
+        // ---- Minv columns (lanes 0..6) and qdd (lane 7), FP64 Cholesky
+        if (lane <= NQ) {
+            double L[CC], rhs[NQ], sol[NQ];
+            chol7_factor(sm.M, L);
+#pragma unroll
+            for (int i = 0; i < NQ; ++i)
+                rhs[i] = (lane < NQ) ? (double)(lane == i) : (double)sm.u[i] - (double)sm.cbias[i];
+            chol7_solve(L, rhs, sol);
+            if (lane < NQ) {
+#pragma unroll
+                for (int i = 0; i < NQ; ++i) sm.Minv[NQ * lane + i] = (float)sol[i];
+            } else {
+#pragma unroll
+                for (int i = 0; i < NQ; ++i) sm.qdd[i] = (float)sol[i];
+            }
+        }
+        __syncwarp();
+
+        // ---- dID/dq_j, dID/dqd_j at (q, qd, qdd), lanes 0..13
+        {
+            float qd[NQ], qdd[NQ], tau[NQ], dtau[NQ];
+#pragma unroll
+            for (int i = 0; i < NQ; ++i) {
+                qd[i] = sm.x[NQ + i];
+                qdd[i] = sm.qdd[i];
+            }
+            const int dq_dir = (lane < NQ) ? lane : -1;
+            const int dqd_dir = (lane >= NQ && lane < NS) ? lane - NQ : -1;
+            rnea<true>(trig, qd, qdd, dq_dir, dqd_dir, tau, dtau);
+            if (lane < NS) {
+#pragma unroll
+                for (int r = 0; r < NQ; ++r) sm.dc[NQ * lane + r] = dtau[r];
+            }
+        }
+        // ---- end-effector position and Jacobian (lane 0 at x_k, lane 1 at the terminal state)
+        if (lane == 0) {
+            fk_lane<true>(trig, sm.ee[0], sm.J[0]);
+        } else if (lane == 1 && terminal && !P.ref_terminal) {
+            JointTrig t2;
+            joint_trig(sm.xn, t2);
+            fk_lane<true>(t2, sm.ee[1], sm.J[1]);
+        }
+        __syncwarp();
+
+        // ---- df/du (iiwa_eepos_plant.cuh:142-155)
+        for (int e = lane; e < NQ * NX; e += 32) {
+            float v;
+            if (e < NQ * NS) {
+                const int col = e / NQ, r = e - NQ * col;
+                float acc = 0.f;
+#pragma unroll
+                for (int t = 0; t < NQ; ++t) acc += sm.Minv[r + NQ * t] * sm.dc[NQ * col + t];
+                v = -acc;
+            } else {
+                v = sm.Minv[e - NQ * NS];
+            }
+            sm.dfdu[e] = v;
+        }
+        // ---- cost gradient (iiwa_eepos_plant.cuh:329-354)
+        if (lane < NS) {
+            const int which = 0;
+            float v;
+            if (lane < NQ) {
+                const float *J = sm.J[which];
+                v = P.q_ee * (J[3 * lane] * (sm.ee[which][0] - sm.goal[0]) +
+                              J[3 * lane + 1] * (sm.ee[which][1] - sm.goal[1]) +
+                              J[3 * lane + 2] * (sm.ee[which][2] - sm.goal[2]));
+            } else {
+                v = P.qd_cost * sm.x[lane];
+            }
+            sm.qv[0][lane] = v;
+        } else if (terminal && lane >= 16 && lane < 16 + NS) {
+            const int i = lane - 16;
+            const int which = P.ref_terminal ? 0 : 1;
+            const float *xt = P.ref_terminal ? sm.x : sm.xn;
+            float v;
+            if (i < NQ) {
+                const float *J = sm.J[which];
+                v = P.q_ee * (J[3 * i] * (sm.ee[which][0] - sm.goal[6]) + J[3 * i + 1] * (sm.ee[which][1] - sm.goal[7]) +
+                              J[3 * i + 2] * (sm.ee[which][2] - sm.goal[8]));
+            } else {
+                v = P.qd_cost * xt[i];
+            }
+            sm.qv[1][i] = v;
+        }
+        __syncwarp();
+
+        // ---- C_k = {-A_k, -B_k} (integrator.cuh:85-126, sign from schur.cuh:519-520)
+        float *Ck = Cm + (size_t)C_STRIDE * j;
+        const float dt = P.dt;
+        for (int e = lane; e < C_STRIDE; e += 32) {
+            float val;
+            if (e < SS) {
+                const int col = e / NS, r = e - NS * col;
+                if (P.integrator == 0) {
+                    val = (float)(r == col);
+                    if (r < NQ && r == col - NQ) val += dt;
+                    if (r >= NQ) val += dt * sm.dfdu[col * NQ + r - NQ];
+                } else {
+                    const int rq = r % NQ;
+                    const float dtv = (r == rq) ? dt : 1.f;
+                    val = (float)(r == col) + dt * (float)(r == col - NQ) + dt * sm.dfdu[col * NQ + rq] * dtv;
+                }
+            } else {
+                const int e2 = e - SS, col = e2 / NS, r = e2 - NS * col;
+                if (P.integrator == 0) {
+                    val = (r >= NQ) ? dt * sm.dfdu[(NS + col) * NQ + r - NQ] : 0.f;
+                } else {
+                    const int rq = r % NQ;
+                    const float dtv = (r == rq) ? dt : 1.f;
+                    val = dt * sm.dfdu[SC + col * NQ + rq] * dtv;
+                }
+            }
+            Ck[e] = -val;
+        }
+        // ---- defect c_{k+1} = x_{k+1} - f(x_k, u_k)  (integrator.cuh:25-83)
+        if (lane < NQ) {
+            const float q = sm.x[lane], qd = sm.x[NQ + lane], a = sm.qdd[lane];
+            float nq, nqd;
+            if (P.integrator == 0) {
+                nq = q + dt * qd;
+                nqd = qd + dt * a;
+            } else {
+                nqd = qd + dt * a;
+                nq = q + dt * nqd;
+            }
+            float *cn = c + (size_t)NS * (j + 1);
+            cn[lane] = sm.xn[lane] - nq;
+            cn[NQ + lane] = sm.xn[NQ + lane] - nqd;
+        }
+        // ---- G_k = {Q_k, R_k}, g_k = {q_k, r_k}
+        float *Gk = G + (size_t)G_STRIDE * j;
+        for (int e = lane; e < G_STRIDE; e += 32) {
+            float v;
+            if (e < SS) {
+                const int i = e / NS, jj = e - NS * i;
+                v = (i < NQ && jj < NQ) ? sm.qv[0][i] * sm.qv[0][jj] : ((i == jj) ? P.qd_cost : 0.f);
+            } else {
+                v = ((e - SS) % (NC + 1) == 0) ? P.r_cost : 0.f;
+            }
+            Gk[e] = v;
+        }
+        if (lane < NX) g[(size_t)NX * j + lane] = (lane < NS) ? sm.qv[0][lane] : P.r_cost * sm.u[lane - NS];
+        if (terminal) {
+            float *Gt = G + (size_t)G_STRIDE * (j + 1);
+            for (int e = lane; e < SS; e += 32) {
+                const int i = e / NS, jj = e - NS * i;
+                Gt[e] = (i < NQ && jj < NQ) ? sm.qv[1][i] * sm.qv[1][jj] : ((i == jj) ? P.qd_cost : 0.f);
+            }
+            if (lane < NS) {
+                g[(size_t)NX * (j + 1) + lane] = sm.qv[1][lane];
+                const int j0 = j - k;
+                c[(size_t)NS * j0 + lane] = xu[(size_t)NX * j0 + lane] - xs[(size_t)NS * b + lane];
+            }
+        }
+        __syncwarp();
+    }
+}
+
+cudaError_t launch_kkt(const BatchView &bv, const ProblemParams &P, const float *xu, const float *goal,
+                       const float *xs, float *G, float *C, float *g, float *c, int num_sms, cudaStream_t s)
+{
+    if (bv.total_knots <= 0) return cudaSuccess;
+    int warps = bv.total_knots;
+    int blocks = (warps + KKT_WARPS - 1) / KKT_WARPS;
+    const int cap = num_sms * 16;
+    if (blocks > cap) blocks = cap;
+    kkt_kernel<<<blocks, 32 * KKT_WARPS, 0, s>>>(bv, P, xu, goal, xs, G, C, g, c);
+    return cudaGetLastError();
+}
+
+}  // namespace gpt

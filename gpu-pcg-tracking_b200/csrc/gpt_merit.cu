@@ -1,0 +1,359 @@
+// gpt_merit.cu -- primal step recovery, merit / line search and the SQP
+// accept-and-update step, all on the device.
+//
+//   dz_kernel      oldschur.cuh:966-1105 (compute_dz), one warp per knot
+//   merit_kernel   merit.cuh:16-94 (ls_gato_compute_merit, all 8 step sizes in
+//                  one launch) and merit.cuh:99-145 (compute_merit, alpha = 0);
+//                  one warp per knot, lanes = (step size, mass-matrix column)
+//   accept_kernel  toplevel.cuh:377-444: argmin merit, rho schedule, the
+//                  saxpy xu += alpha dz (cuBLAS in the reference) -- one block
+//                  per instance, deterministic fixed-order merit sums
+#include "gpt_common.cuh"
+#include "gpt_dyn.cuh"
+#include "gpt_internal.h"
+
+namespace gpt {
+
+constexpr int DZ_WARPS = 4;
+
+__global__ void __launch_bounds__(32 * DZ_WARPS)
+    dz_kernel(BatchView bv, const float *__restrict__ Ginv, const float *__restrict__ Cm,
+              const float *__restrict__ g, const float *__restrict__ lambda, float *__restrict__ dz)
+{
+    __shared__ float s_all[DZ_WARPS][NX];
+    const int lane = threadIdx.x & 31;
+    float *s = s_all[threadIdx.x >> 5];
+    const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    for (int j = gw; j < bv.total_knots; j += nw) {
+        const int b = bv.inst(j);
+        if (!bv.active(b)) continue;
+        const int N = bv.N(b), k = j - bv.off(b);
+        const bool last = (k == N - 1);
+        const float *Cj = Cm + (size_t)C_STRIDE * j;
+        const float *ln = lambda + (size_t)NS * (j + 1);
+        if (lane < NS) {
+            // q_k - (lambda_k + (-A_k)^T lambda_{k+1})
+            float a = 0.f;
+            if (!last) {
+#pragma unroll
+                for (int t = 0; t < NS; ++t) a = fmaf(Cj[lane * NS + t], ln[t], a);
+            }
+            s[lane] = g[(size_t)NX * j + lane] - (lambda[(size_t)NS * j + lane] + a);
+        } else if (lane < NX && !last) {
+            // r_k - (-B_k)^T lambda_{k+1}
+            const int i = lane - NS;
+            float a = 0.f;
+#pragma unroll
+            for (int t = 0; t < NS; ++t) a = fmaf(Cj[SS + i * NS + t], ln[t], a);
+            s[lane] = g[(size_t)NX * j + lane] - a;
+        }
+        __syncwarp();
+        const float *Gi = Ginv + (size_t)G_STRIDE * j;
+        if (lane < NS) {
+            float a = 0.f;
+#pragma unroll
+            for (int t = 0; t < NS; ++t) a = fmaf(Gi[lane + NS * t], s[t], a);
+            dz[(size_t)NX * j + lane] = a;
+        } else if (lane < NX && !last) {
+            const int i = lane - NS;
+            float a = 0.f;
+#pragma unroll
+            for (int t = 0; t < NC; ++t) a = fmaf(Gi[SS + i + NC * t], s[NS + t], a);
+            dz[(size_t)NX * j + lane] = a;
+        }
+        __syncwarp();
+    }
+}
+
+cudaError_t launch_dz(const BatchView &bv, const float *Ginv, const float *C, const float *g, const float *lambda,
+                      float *dz, int num_sms, cudaStream_t s)
+{
+    if (bv.total_knots <= 0) return cudaSuccess;
+    int blocks = (bv.total_knots + DZ_WARPS - 1) / DZ_WARPS;
+    if (blocks > num_sms * 16) blocks = num_sms * 16;
+    dz_kernel<<<blocks, 32 * DZ_WARPS, 0, s>>>(bv, Ginv, C, g, lambda, dz);
+    return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------------
+// merit
+// ------------------------------------------------------------------------
+
+struct MeritWarpSmem {
+    float x[NX + NS];    // x_k, u_k, x_{k+1}
+    float d[NX + NS];    // dz_k, dz_{k+1}
+    float goal[3];
+    float M[NUM_ALPHAS][CC];
+    float cb[NUM_ALPHAS][NQ];
+    float defect[NUM_ALPHAS];
+    float cost[NUM_ALPHAS];
+};
+
+constexpr int MERIT_WARPS = 4;
+
+__device__ __forceinline__ float alpha_of(int a, int n_alpha)
+{
+    return n_alpha == 1 ? 0.f : -1.f / (float)(1 << a);  // toplevel.cuh:409, merit.cuh:47
+}
+
+// n_alpha = 8: line search (last knot adds ||x_0 + alpha dz_0 - x_s||_1);
+// n_alpha = 1: merit at the current iterate (last knot defect 0).
+__global__ void __launch_bounds__(32 * MERIT_WARPS)
+    merit_kernel(BatchView bv, ProblemParams P, int n_alpha, const float *__restrict__ xu,
+                 const float *__restrict__ dz, const float *__restrict__ goal, const float *__restrict__ xs,
+                 float *__restrict__ knot_merit)
+{
+    __shared__ MeritWarpSmem smem_all[MERIT_WARPS];
+    const int lane = threadIdx.x & 31;
+    MeritWarpSmem &sm = smem_all[threadIdx.x >> 5];
+    const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    for (int j = gw; j < bv.total_knots; j += nw) {
+        const int b = bv.inst(j);
+        if (!bv.active(b)) continue;
+        const int N = bv.N(b), k = j - bv.off(b);
+        const bool last = (k == N - 1);
+        const int len = last ? NS : NX + NS;
+        for (int i = lane; i < len; i += 32) {
+            sm.x[i] = xu[(size_t)NX * j + i];
+            sm.d[i] = (n_alpha > 1) ? dz[(size_t)NX * j + i] : 0.f;
+        }
+        if (lane < 3) sm.goal[lane] = goal[(size_t)6 * j + lane];
+        __syncwarp();
+
+        if (!last) {
+            // mass-matrix columns (m < 7) and bias force (m == 7) per step size
+            const int rounds = (n_alpha * 8 + 31) / 32;
+            for (int rd = 0; rd < rounds; ++rd) {
+                const int a = 4 * rd + (lane >> 3), m = lane & 7;
+                const int aa = (a < n_alpha) ? a : 0;
+                const float al = alpha_of(aa, n_alpha);
+                float q[NQ], qd[NQ], qdd[NQ], tau[NQ];
+#pragma unroll
+                for (int i = 0; i < NQ; ++i) {
+                    q[i] = fmaf(al, sm.d[i], sm.x[i]);
+                    qd[i] = (m == 7) ? fmaf(al, sm.d[NQ + i], sm.x[NQ + i]) : 0.f;
+                    qdd[i] = (m == i) ? 1.f : 0.f;
+                }
+                JointTrig t;
+                joint_trig(q, t);
+                rnea<false>(t, qd, qdd, -1, -1, tau, nullptr);
+                if (a < n_alpha) {
+                    if (m < 7) {
+#pragma unroll
+                        for (int r = 0; r < NQ; ++r) sm.M[a][NQ * m + r] = tau[r];
+                    } else {
+#pragma unroll
+                        for (int r = 0; r < NQ; ++r) sm.cb[a][r] = tau[r];
+                    }
+                }
+            }
+            __syncwarp();
+        }
+        if (lane < n_alpha) {
+            // defect ||x_{k+1} - f(x_k, u_k)||_1 at xu + alpha dz (integrator.cuh:187-219)
+            const int a = lane;
+            const float al = alpha_of(a, n_alpha);
+            float dsum = 0.f;
+            if (!last) {
+                double L[CC], rhs[NQ], qdd[NQ];
+                chol7_factor(sm.M[a], L);
+#pragma unroll
+                for (int i = 0; i < NQ; ++i)
+                    rhs[i] = (double)fmaf(al, sm.d[NS + i], sm.x[NS + i]) - (double)sm.cb[a][i];
+                chol7_solve(L, rhs, qdd);
+#pragma unroll
+                for (int i = 0; i < NQ; ++i) {
+                    const float q = fmaf(al, sm.d[i], sm.x[i]), qd = fmaf(al, sm.d[NQ + i], sm.x[NQ + i]);
+                    const float qn = fmaf(al, sm.d[NX + i], sm.x[NX + i]);
+                    const float qdn = fmaf(al, sm.d[NX + NQ + i], sm.x[NX + NQ + i]);
+                    float nq, nqd;
+                    if (P.integrator == 0) {
+                        nq = q + P.dt * qd;
+                        nqd = qd + P.dt * (float)qdd[i];
+                    } else {
+                        nqd = qd + P.dt * (float)qdd[i];
+                        nq = q + P.dt * nqd;
+                    }
+                    dsum += fabsf(qn - nq) + fabsf(qdn - nqd);
+                }
+            } else if (n_alpha > 1) {
+                const int j0 = j - k;
+#pragma unroll
+                for (int i = 0; i < NS; ++i)
+                    dsum += fabsf(fmaf(al, dz[(size_t)NX * j0 + i], xu[(size_t)NX * j0 + i]) - xs[(size_t)NS * b + i]);
+            }
+            sm.defect[a] = dsum;
+        } else if (lane >= 16 && lane < 16 + n_alpha) {
+            // tracking cost (iiwa_eepos_plant.cuh:240-290)
+            const int a = lane - 16;
+            const float al = alpha_of(a, n_alpha);
+            float q[NQ], p[3];
+            float J = 0.f;
+#pragma unroll
+            for (int i = 0; i < NQ; ++i) {
+                q[i] = fmaf(al, sm.d[i], sm.x[i]);
+                const float qd = fmaf(al, sm.d[NQ + i], sm.x[NQ + i]);
+                J += 0.5f * (P.qd_cost * qd * qd);
+            }
+            if (!last) {
+#pragma unroll
+                for (int i = 0; i < NC; ++i) {
+                    const float u = fmaf(al, sm.d[NS + i], sm.x[NS + i]);
+                    J += 0.5f * (P.r_cost * u * u);
+                }
+            }
+            JointTrig t;
+            joint_trig(q, t);
+            fk_lane<false>(t, p, nullptr);
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                const float e = p[d] - sm.goal[d];
+                J += 0.5f * P.q_ee * e * e;
+            }
+            sm.cost[a] = J;
+        }
+        __syncwarp();
+        if (lane < n_alpha) knot_merit[(size_t)NUM_ALPHAS * j + lane] = sm.cost[lane] + P.mu * sm.defect[lane];
+        __syncwarp();
+    }
+}
+
+cudaError_t launch_merit(const BatchView &bv, const ProblemParams &P, int n_alpha, const float *xu, const float *dz,
+                         const float *goal, const float *xs, float *knot_merit, int num_sms, cudaStream_t s)
+{
+    if (bv.total_knots <= 0) return cudaSuccess;
+    int blocks = (bv.total_knots + MERIT_WARPS - 1) / MERIT_WARPS;
+    if (blocks > num_sms * 16) blocks = num_sms * 16;
+    merit_kernel<<<blocks, 32 * MERIT_WARPS, 0, s>>>(bv, P, n_alpha, xu, dz, goal, xs, knot_merit);
+    return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------------
+// merit reduction + accept
+// ------------------------------------------------------------------------
+
+constexpr int ACC_THREADS = 256;
+
+// Fixed-order sum of knot_merit[8 (kb + k) + a] over k for all a; result in out[a] (all threads).
+__device__ void merit_sums(const float *km, int kb, int N, int n_alpha, float *out, double *scratch)
+{
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    constexpr int NW = ACC_THREADS / 32;
+    for (int a = 0; a < n_alpha; ++a) {
+        double v = 0.0;
+        for (int k = tid; k < N; k += ACC_THREADS) v += (double)km[(size_t)NUM_ALPHAS * (kb + k) + a];
+        v = warp_sum(v);
+        if (lane == 0) scratch[a * NW + warp] = v;
+    }
+    __syncthreads();
+    if (tid < n_alpha) {
+        double t = 0.0;
+        for (int w = 0; w < NW; ++w) t += scratch[tid * NW + w];
+        scratch[NUM_ALPHAS * NW + tid] = t;
+    }
+    __syncthreads();
+    for (int a = 0; a < n_alpha; ++a) out[a] = (float)scratch[NUM_ALPHAS * NW + a];
+    __syncthreads();
+}
+
+// mode 0: initial merit of the iterate (merit0, toplevel.cuh:235-244)
+// mode 1: line-search decision and step (toplevel.cuh:384-444)
+__global__ void __launch_bounds__(ACC_THREADS)
+    accept_kernel(BatchView bv, int mode, SolverParams SP, const float *__restrict__ knot_merit,
+                  const float *__restrict__ dz, float *__restrict__ xu, float *__restrict__ merits_out,
+                  uint32_t *__restrict__ active_count)
+{
+    __shared__ double scratch[NUM_ALPHAS * (ACC_THREADS / 32) + NUM_ALPHAS];
+    __shared__ float s_alpha;
+    for (int b = blockIdx.x; b < bv.B; b += gridDim.x) {
+        if (!bv.active(b)) continue;
+        const int N = bv.N(b), kb = bv.off(b);
+        float m[NUM_ALPHAS];
+        merit_sums(knot_merit, kb, N, mode == 0 ? 1 : NUM_ALPHAS, m, scratch);
+        if (threadIdx.x == 0) {
+            float alpha = 0.f;
+            if (merits_out) {
+                for (int a = 0; a < (mode == 0 ? 1 : NUM_ALPHAS); ++a) merits_out[NUM_ALPHAS * b + a] = m[a];
+            }
+            if (bv.st) {
+                InstState &s = bv.st[b];
+                if (mode == 0) {
+                    s.merit0 = m[0];
+                    s.merit_init = m[0];
+                    if (!isfinite(m[0])) { s.exit_flags |= 4u; s.active = 0; }
+                } else {
+                    float minm = s.merit0;
+                    int best = 0;
+                    for (int a = 0; a < NUM_ALPHAS; ++a)
+                        if (m[a] < minm) { minm = m[a]; best = a; }
+                    const float f = SP.rho_factor;
+                    if (minm == s.merit0) {
+                        s.drho = fmaxf(s.drho * f, f);
+                        s.rho = fmaxf(s.rho * s.drho, SP.rho_min);
+                        s.sqp_iters++;
+                        s.ls_fail_count++;
+                        if (s.rho > SP.rho_max) {
+                            s.exit_flags |= 1u;
+                            s.rho = s.rho_reset;
+                            s.active = 0;
+                        }
+                    } else {
+                        alpha = -1.f / (float)(1 << best);
+                        s.drho = fminf(s.drho / f, 1.f / f);
+                        s.rho = fmaxf(s.rho * s.drho, SP.rho_min);
+                        s.sqp_iters++;
+                        s.merit0 = minm;
+                    }
+                    if (s.active && s.sqp_iters >= SP.sqp_max_iter) {
+                        s.active = 0;
+                        s.exit_flags |= 8u;
+                    }
+                }
+                if (active_count && s.active) atomicAdd(active_count, 1u);
+            }
+            s_alpha = alpha;
+        }
+        __syncthreads();
+        const float alpha = s_alpha;
+        if (alpha != 0.f) {
+            const int len = NX * N - NC;
+            float *xb = xu + (size_t)NX * kb;
+            const float *db = dz + (size_t)NX * kb;
+            for (int i = threadIdx.x; i < len; i += ACC_THREADS) xb[i] = fmaf(alpha, db[i], xb[i]);
+        }
+        __syncthreads();
+    }
+}
+
+cudaError_t launch_accept(const BatchView &bv, int mode, const SolverParams &SP, const float *knot_merit,
+                          const float *dz, float *xu, float *merits_out, uint32_t *active_count, int num_sms,
+                          cudaStream_t s)
+{
+    if (bv.B <= 0) return cudaSuccess;
+    int blocks = bv.B;
+    if (blocks > num_sms * 8) blocks = num_sms * 8;
+    accept_kernel<<<blocks, ACC_THREADS, 0, s>>>(bv, mode, SP, knot_merit, dz, xu, merits_out, active_count);
+    return cudaGetLastError();
+}
+
+// Per-instance start of a solve: x_s = x_0 (toplevel.cuh:110), state from the host image.
+__global__ void init_kernel(BatchView bv, const float *__restrict__ xu, float *__restrict__ xs)
+{
+    for (int b = blockIdx.x; b < bv.B; b += gridDim.x) {
+        const int kb = bv.off(b);
+        if (threadIdx.x < NS) xs[(size_t)NS * b + threadIdx.x] = xu[(size_t)NX * kb + threadIdx.x];
+    }
+}
+
+cudaError_t launch_init(const BatchView &bv, const float *xu, float *xs, int num_sms, cudaStream_t s)
+{
+    if (bv.B <= 0) return cudaSuccess;
+    int blocks = bv.B;
+    if (blocks > num_sms * 8) blocks = num_sms * 8;
+    init_kernel<<<blocks, 32, 0, s>>>(bv, xu, xs);
+    return cudaGetLastError();
+}
+
+}  // namespace gpt

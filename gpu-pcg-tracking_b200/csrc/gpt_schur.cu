@@ -1,0 +1,275 @@
+// gpt_schur.cu -- Schur complement, block-Jacobi preconditioner and the CSC
+// values of the Schur matrix: one warp per block row.
+//
+// Replaces gato_form_schur_jacobi / gato_form_schur_jacobi_inner
+// (schur.cuh:12-54, oldschur.cuh:518-963) and form_schur_qdl_kernel
+// (schur.cuh:57-383 with store_block_csr_lowertri, utils.cuh:55-81).
+//
+// Block row k >= 1 (A, B = dynamics Jacobians of knot k-1; C stores -A, -B):
+//   phi_k   = (-A) Qt_{k-1}^{-1}                     Qt = Q + rho I, Rt = R + rho I
+//   theta_k = phi_k (-A)^T + Qt_k^{-1} + (-B) Rt^{-1} (-B)^T
+//   gamma_k = Qt_k^{-1} q_k - c_k + phi_k q_{k-1} + (-B) Rt^{-1} r_{k-1}
+//   S[k] = [-phi_k, -theta_k, .], S[k-1].right = -phi_k^T,
+//   Pinv[k].diag = -theta_k^{-1}, gamma_out[k] = -gamma_k
+// Block row 0: S[0].diag = -Qt_0^{-1}, Pinv[0].diag = -Qt_0, gamma_out[0] = -Qt_0^{-1} q_0.
+// Inverses (Qt, Rt, theta) are Gauss-Jordan in FP64 with the augmented
+// columns spread over the lanes; the products are FP32 from shared memory.
+// The inverses Qt_k^{-1}, Rt_k^{-1} go to a separate Ginv buffer (the
+// reference overwrites G in place, which races with the neighbouring block's
+// read of the same slot, oldschur.cuh:700 vs :751).
+#include "gpt_common.cuh"
+#include "gpt_internal.h"
+
+namespace gpt {
+
+// FP64 Gauss-Jordan inverse of the n x n matrix (A + shift I) held column-major
+// in A (global or shared).  Lanes 0..2n-1 hold the columns of [A | I]; the
+// inverse is written column-major (float) to Ainv.
+template <int n>
+__device__ __forceinline__ void warp_inverse(const float *A, float shift, float *Ainv, int lane)
+{
+    double col[n];
+    const bool left = lane < n, right = (lane >= n) && (lane < 2 * n);
+#pragma unroll
+    for (int r = 0; r < n; ++r) {
+        double v = 0.0;
+        if (left) v = (double)A[r + n * lane] + ((r == lane) ? (double)shift : 0.0);
+        else if (right) v = (r == lane - n) ? 1.0 : 0.0;
+        col[r] = v;
+    }
+#pragma unroll
+    for (int p = 0; p < n; ++p) {
+        double pc[n];
+#pragma unroll
+        for (int r = 0; r < n; ++r) pc[r] = __shfl_sync(0xffffffffu, col[r], p);
+        const double prow = col[p] / pc[p];
+#pragma unroll
+        for (int r = 0; r < n; ++r) col[r] = (r == p) ? prow : fma(-pc[r], prow, col[r]);
+    }
+    if (right) {
+#pragma unroll
+        for (int r = 0; r < n; ++r) Ainv[r + n * (lane - n)] = (float)col[r];
+    }
+}
+
+// out (14 x NCOL, col-major) = A (14 x K, col-major) * op(B)
+//   op(B) = B (K x NCOL, ld 14 or 7) or B^T with B (NCOL x K, ld 14)
+template <int K, int NCOL, bool TRANS_B>
+__device__ __forceinline__ void warp_mm(const float *A, const float *B, int ldb, float *out, int lane)
+{
+    if (lane < 2 * NCOL) {
+        const int col = lane % NCOL, r0 = (lane / NCOL) * 7;
+        float acc[7];
+#pragma unroll
+        for (int i = 0; i < 7; ++i) acc[i] = 0.f;
+#pragma unroll
+        for (int t = 0; t < K; ++t) {
+            const float bv = TRANS_B ? B[col + ldb * t] : B[t + ldb * col];
+#pragma unroll
+            for (int i = 0; i < 7; ++i) acc[i] = fmaf(A[r0 + i + NS * t], bv, acc[i]);
+        }
+#pragma unroll
+        for (int i = 0; i < 7; ++i) out[r0 + i + NS * col] = acc[i];
+    }
+}
+
+struct SchurWarpSmem {
+    float A[SS], B[SC];
+    float Qki[SS], Qkp1i[SS], Rki[CC];
+    float phi[SS], BRi[SC], theta[SS], tmp[SS], thetai[SS];
+    float qk[NS], qkp1[NS], rk[NC], ck[NS];
+};
+
+constexpr int SCHUR_WARPS = 4;
+
+// MODE 0: S, Pinv (reference 3-block layout, off-diagonal Pinv blocks zero), gamma, Ginv
+// MODE 1: S, compact Pinv (diagonal block only, stride 196), gamma, Ginv
+// MODE 2: CSC values of the upper triangle (utils.cuh:55-118 layout), gamma, Ginv
+template <int MODE>
+__global__ void __launch_bounds__(32 * SCHUR_WARPS)
+    schur_kernel(BatchView bv, float rho_scalar, const float *__restrict__ G,
+                 const float *__restrict__ Cm, const float *__restrict__ g, const float *__restrict__ c,
+                 float *__restrict__ S, float *__restrict__ Pinv, float *__restrict__ gamma,
+                 float *__restrict__ Ginv, float *__restrict__ csc_val)
+{
+    extern __shared__ float4 schur_dyn_smem[];
+    SchurWarpSmem *smem_all = reinterpret_cast<SchurWarpSmem *>(schur_dyn_smem);
+    const int lane = threadIdx.x & 31;
+    SchurWarpSmem &sm = smem_all[threadIdx.x >> 5];
+    const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+
+    for (int j = gw; j < bv.total_knots; j += nw) {
+        const int b = bv.inst(j);
+        if (!bv.active(b)) continue;
+        const int N = bv.N(b);
+        const int k = j - bv.off(b);
+        const float rho = bv.st ? bv.st[b].rho : rho_scalar;
+        float *Srow = S ? S + (size_t)S_STRIDE * j : nullptr;
+
+        if (k == 0) {
+            const float *Q0 = G + (size_t)G_STRIDE * j;
+            warp_inverse<NS>(Q0, rho, sm.Qki, lane);
+            if (lane < NS) sm.qk[lane] = g[(size_t)NX * j + lane];
+            __syncwarp();
+            if (lane < NS) {
+                float acc = 0.f;
+#pragma unroll
+                for (int t = 0; t < NS; ++t) acc = fmaf(sm.Qki[lane + NS * t], sm.qk[t], acc);
+                gamma[(size_t)NS * j + lane] = -acc;
+            }
+            for (int e = lane; e < SS; e += 32) {
+                const float qv = Q0[e] + ((e % (NS + 1)) == 0 ? rho : 0.f);
+                if (MODE == 0) {
+                    Pinv[(size_t)S_STRIDE * j + e] = 0.f;
+                    Pinv[(size_t)S_STRIDE * j + SS + e] = -qv;
+                    Srow[e] = 0.f;
+                    Srow[SS + e] = -sm.Qki[e];
+                } else if (MODE == 1) {
+                    Pinv[(size_t)SS * j + e] = -qv;
+                    Srow[e] = 0.f;
+                    Srow[SS + e] = -sm.Qki[e];
+                }
+                if (N == 1) Ginv[(size_t)G_STRIDE * j + e] = sm.Qki[e];
+            }
+            if (MODE == 2) {
+                // first block row: lower triangle of -Qt_0^{-1}, row r holds cols 0..r
+                const size_t base = 0;
+                for (int e = lane; e < SS; e += 32) {
+                    const int r = e / NS, cc = e - NS * r;
+                    if (cc <= r) csc_val[base + (r * (r + 1)) / 2 + cc] = -sm.Qki[r + NS * cc];
+                }
+            }
+            if (MODE == 0) {
+                for (int e = lane; e < SS; e += 32) {
+                    Pinv[(size_t)S_STRIDE * j + 2 * SS + e] = 0.f;
+                    if (N == 1) Srow[2 * SS + e] = 0.f;
+                }
+            } else if (MODE == 1 && N == 1) {
+                for (int e = lane; e < SS; e += 32) Srow[2 * SS + e] = 0.f;
+            }
+            __syncwarp();
+            continue;
+        }
+
+        // ---- rows k >= 1
+        const float *Ck = Cm + (size_t)C_STRIDE * (j - 1);
+        for (int e = lane; e < C_STRIDE; e += 32) {
+            const float v = Ck[e];
+            if (e < SS) sm.A[e] = v;
+            else sm.B[e - SS] = v;
+        }
+        if (lane < NS) {
+            sm.qk[lane] = g[(size_t)NX * (j - 1) + lane];
+            sm.qkp1[lane] = g[(size_t)NX * j + lane];
+            sm.ck[lane] = c[(size_t)NS * j + lane];
+        } else if (lane < NS + NC) {
+            sm.rk[lane - NS] = g[(size_t)NX * (j - 1) + lane];
+        }
+        const float *Gkm1 = G + (size_t)G_STRIDE * (j - 1);
+        const float *Gk = G + (size_t)G_STRIDE * j;
+        warp_inverse<NS>(Gkm1, rho, sm.Qki, lane);
+        warp_inverse<NS>(Gk, rho, sm.Qkp1i, lane);
+        warp_inverse<NC>(Gkm1 + SS, rho, sm.Rki, lane);
+        __syncwarp();
+        // Ginv slots (schur.cuh:236-256): Qt_{k-1}^{-1}, Rt_{k-1}^{-1}; the last row also Qt_{N-1}^{-1}
+        {
+            float *Gi = Ginv + (size_t)G_STRIDE * (j - 1);
+            for (int e = lane; e < G_STRIDE; e += 32) Gi[e] = (e < SS) ? sm.Qki[e] : sm.Rki[e - SS];
+            if (k == N - 1) {
+                float *Gl = Ginv + (size_t)G_STRIDE * j;
+                for (int e = lane; e < SS; e += 32) Gl[e] = sm.Qkp1i[e];
+            }
+        }
+        warp_mm<NS, NS, false>(sm.A, sm.Qki, NS, sm.phi, lane);   // phi = (-A) Qt^{-1}
+        warp_mm<NC, NC, false>(sm.B, sm.Rki, NC, sm.BRi, lane);   // (-B) Rt^{-1}
+        __syncwarp();
+        warp_mm<NS, NS, true>(sm.phi, sm.A, NS, sm.theta, lane);  // phi (-A)^T
+        warp_mm<NC, NS, true>(sm.BRi, sm.B, NS, sm.tmp, lane);    // (-B) Rt^{-1} (-B)^T
+        if (lane < NS) {
+            float a1 = 0.f, a2 = 0.f, a3 = 0.f;
+#pragma unroll
+            for (int t = 0; t < NS; ++t) {
+                a1 = fmaf(sm.Qkp1i[lane + NS * t], sm.qkp1[t], a1);
+                a2 = fmaf(sm.phi[lane + NS * t], sm.qk[t], a2);
+            }
+#pragma unroll
+            for (int t = 0; t < NC; ++t) a3 = fmaf(sm.BRi[lane + NS * t], sm.rk[t], a3);
+            gamma[(size_t)NS * j + lane] = -((a1 - sm.ck[lane]) + (a3 + a2));
+        }
+        __syncwarp();
+        for (int e = lane; e < SS; e += 32) sm.theta[e] = (sm.theta[e] + sm.Qkp1i[e]) + sm.tmp[e];
+        __syncwarp();
+        warp_inverse<NS>(sm.theta, 0.f, sm.thetai, lane);
+        __syncwarp();
+        if (MODE != 2) {
+            float *Sprev_right = S + (size_t)S_STRIDE * (j - 1) + 2 * SS;
+            for (int e = lane; e < SS; e += 32) {
+                const int r = e % NS, cc = e / NS;
+                Srow[e] = -sm.phi[e];
+                Srow[SS + e] = -sm.theta[e];
+                Sprev_right[e] = -sm.phi[cc + NS * r];
+                if (MODE == 0) {
+                    Pinv[(size_t)S_STRIDE * j + e] = 0.f;
+                    Pinv[(size_t)S_STRIDE * j + SS + e] = -sm.thetai[e];
+                    Pinv[(size_t)S_STRIDE * j + 2 * SS + e] = 0.f;
+                } else {
+                    Pinv[(size_t)SS * j + e] = -sm.thetai[e];
+                }
+                if (k == N - 1) Srow[2 * SS + e] = 0.f;
+            }
+        } else {
+            // block row k of the CSC (utils.cuh:55-81): row r holds 14 left entries then r+1 diagonal entries
+            const int tri = (NS + 1) * NS / 2, brow = SS + tri;
+            const size_t base = (size_t)tri + (size_t)(k - 1) * brow;
+            for (int e = lane; e < SS; e += 32) {
+                const int r = e / NS, cc = e - NS * r;
+                const size_t off = base + (size_t)r * NS + (r * (r + 1)) / 2;
+                csc_val[off + cc] = -sm.phi[r + NS * cc];
+                if (cc <= r) csc_val[off + NS + cc] = -sm.theta[r + NS * cc];
+            }
+        }
+        __syncwarp();
+    }
+}
+
+cudaError_t launch_schur(int mode, const BatchView &bv, float rho_scalar, const float *G,
+                         const float *C, const float *g, const float *c, float *S, float *Pinv, float *gamma,
+                         float *Ginv, float *csc_val, int num_sms, cudaStream_t s)
+{
+    if (bv.total_knots <= 0) return cudaSuccess;
+    const size_t smem = sizeof(SchurWarpSmem) * SCHUR_WARPS;
+    int blocks = (bv.total_knots + SCHUR_WARPS - 1) / SCHUR_WARPS;
+    const int cap = num_sms * 16;
+    if (blocks > cap) blocks = cap;
+    static bool attr_done[3] = {false, false, false};
+    switch (mode) {
+    case 0:
+        if (!attr_done[0]) {
+            cudaFuncSetAttribute(schur_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            attr_done[0] = true;
+        }
+        schur_kernel<0><<<blocks, 32 * SCHUR_WARPS, smem, s>>>(bv, rho_scalar, G, C, g, c, S, Pinv, gamma,
+                                                               Ginv, csc_val);
+        break;
+    case 1:
+        if (!attr_done[1]) {
+            cudaFuncSetAttribute(schur_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            attr_done[1] = true;
+        }
+        schur_kernel<1><<<blocks, 32 * SCHUR_WARPS, smem, s>>>(bv, rho_scalar, G, C, g, c, S, Pinv, gamma,
+                                                               Ginv, csc_val);
+        break;
+    default:
+        if (!attr_done[2]) {
+            cudaFuncSetAttribute(schur_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            attr_done[2] = true;
+        }
+        schur_kernel<2><<<blocks, 32 * SCHUR_WARPS, smem, s>>>(bv, rho_scalar, G, C, g, c, S, Pinv, gamma,
+                                                               Ginv, csc_val);
+        break;
+    }
+    return cudaGetLastError();
+}
+
+}  // namespace gpt

@@ -1,0 +1,194 @@
+/*
+ * gpt.h -- C ABI of the B200-native SQP inner loop for 7-DOF iiwa
+ * end-effector tracking (a drop-in for gpu-pcg-tracking's sqpSolve path).
+ *
+ * Every entry point takes plain pointers, sizes and a CUDA stream, never
+ * exits, and returns a gpt_status.  Device pointers are named d_*, host
+ * pointers h_*.  All floating-point buffers are float32 in the reference's
+ * layouts (column-major blocks, knots contiguous):
+ *
+ *   xu        [21N-7]      x_0 u_0 x_1 u_1 ... x_{N-1}      (toplevel.cuh:512)
+ *   eePos     [6N]         goal xyz + rpy per knot           (runme.cu:153-157)
+ *   lambda    [14N]        Schur-system multipliers (warm start, in/out)
+ *   G         [245N-49]    {Q_k, R_k}           (toplevel.cuh:46)
+ *   C         [294(N-1)]   {-A_k, -B_k}         (toplevel.cuh:47)
+ *   g         [21N-7]      {q_k, r_k}           (toplevel.cuh:48)
+ *   c         [14N]        defects              (toplevel.cuh:49)
+ *   S, Pinv   [588N]       3 blocks per row     (toplevel.cuh:103,124)
+ *   gamma     [14N]
+ *   dz        [21N-7]                           (toplevel.cuh:50)
+ *
+ * Batched calls concatenate instances knot by knot: instance b with horizon
+ * N_b starts at knot K_b = N_0 + ... + N_{b-1}, i.e. at float offset 21 K_b
+ * of xu (slot of 21 N_b floats, the last 7 unused), 6 K_b of eePos and
+ * 14 K_b of lambda.
+ */
+#ifndef GPT_H
+#define GPT_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st *gpt_stream_t; /* same type as cudaStream_t */
+typedef struct gpt_handle gpt_handle;
+
+typedef enum gpt_status {
+    GPT_OK = 0,
+    GPT_ERR_BAD_ARG = 1,     /* null pointer, size out of range, wrong state/control size */
+    GPT_ERR_CUDA = 2,        /* a CUDA runtime call failed; see gpt_last_error() */
+    GPT_ERR_NO_DEVICE = 3,   /* no CUDA device / library built without a usable GPU */
+    GPT_ERR_CAPACITY = 4,    /* request exceeds the handle's preallocated workspace */
+    GPT_ERR_NONFINITE = 5,   /* a NaN/Inf appeared (reported per instance in gpt_sqp_stats) */
+    GPT_ERR_FACTOR = 6       /* a factorisation failed (matrix not definite) */
+} gpt_status;
+
+/* gpt_sqp_stats.exit_flags bits */
+#define GPT_EXIT_RHO_MAX 1u      /* line search failed until rho > rho_max (toplevel.cuh:396-405) */
+#define GPT_EXIT_PCG_MAXITER 2u  /* at least one PCG solve hit its iteration limit */
+#define GPT_EXIT_NONFINITE 4u    /* NaN/Inf in a merit or a PCG reduction */
+#define GPT_EXIT_ITER_LIMIT 8u   /* SQP_MAX_ITER iterations done (toplevel.cuh:254) */
+
+/* Problem description; the reference's compile-time macros become fields.
+ * Replaces settings.cuh and the -D flags of perform_experiment.sh:42-58. */
+typedef struct gpt_problem_config {
+    uint32_t state_size;       /* must be 14 (settings.cuh:4) */
+    uint32_t control_size;     /* must be 7 (grid::NUM_JOINTS) */
+    uint32_t max_knot_points;  /* capacity: largest horizon N (2..512) */
+    uint32_t max_batch;        /* capacity: instances per batched call */
+    float timestep;            /* runme.cu:65 uses 1/64 */
+    uint32_t integrator;       /* 0 explicit Euler (reference default), 1 semi-implicit */
+    float q_ee;                /* end-effector position weight (1 in the reference) */
+    float qd_cost;             /* QD_COST */
+    float r_cost;              /* R_COST */
+    float mu;                  /* merit penalty, 10 in toplevel.cuh:54 */
+    uint32_t ref_terminal;     /* 1: terminal Q,q at x_{N-2} (iiwa_eepos_plant.cuh:399); 0: at x_{N-1} */
+} gpt_problem_config;
+
+/* SQP / PCG controls (settings.cuh:31-50; pcg_config of GPU-PCG, toplevel.cuh:573-576) */
+typedef struct gpt_solver_config {
+    uint32_t sqp_max_iter;     /* SQP_MAX_ITER, 40 */
+    uint32_t pcg_max_iter;     /* PCG_MAX_ITER */
+    float pcg_exit_tol;        /* PCG_EXIT_TOL */
+    uint32_t pcg_exit_mode;    /* 0: ||r||_2 <= tol ||gamma||_2; 1: |r^T Pinv r| < tol */
+    float rho_factor;          /* RHO_FACTOR */
+    float rho_max;             /* RHO_MAX */
+    float rho_min;             /* RHO_MIN */
+} gpt_solver_config;
+
+/* One sqpSolve's outcome (the reference returns a tuple, toplevel.cuh:502) */
+typedef struct gpt_sqp_stats {
+    uint32_t sqp_iters;          /* sqp_iter */
+    uint32_t exit_flags;         /* GPT_EXIT_* */
+    uint32_t pcg_iters_total;
+    uint32_t pcg_maxiter_count;  /* number of PCG solves that stopped at pcg_max_iter */
+    uint32_t ls_fail_count;
+    float merit_initial;
+    float merit_final;
+    float rho_final;
+} gpt_sqp_stats;
+
+/* Default configs: the reference's logged experiment settings (dt 1/64, Euler,
+ * QD = R = 1e-4, RHO_FACTOR 1.2, RHO_MAX 10, RHO_MIN 1e-3, SQP_MAX_ITER 40). */
+void gpt_default_problem_config(gpt_problem_config *out);
+void gpt_default_solver_config(gpt_solver_config *out);
+
+/* Handle with a workspace sized for max_batch x max_knot_points; no
+ * allocation happens inside the solve calls.  Replaces the per-call
+ * cudaMalloc/cublasCreate of sqpSolve (toplevel.cuh:67-141) and
+ * gato_plant::initializeDynamicsConstMem (rbdfiles/iiwa_eepos_plant.cuh:66-70). */
+gpt_status gpt_create(const gpt_problem_config *problem, const gpt_solver_config *solver, gpt_handle **out);
+gpt_status gpt_destroy(gpt_handle *h);
+gpt_status gpt_set_solver_config(gpt_handle *h, const gpt_solver_config *solver);
+const char *gpt_last_error(void);
+const char *gpt_version(void);
+
+/*
+ * One SQP solve of one instance: replaces
+ *   sqpSolve<T>(state_size, control_size, knot_points, timestep, d_eePos_traj, d_lambda, d_xu,
+ *               d_dynMem_const, pcg_config&, T& rho, T rho_reset)      (toplevel.cuh:24-25)
+ * d_xu and d_lambda are updated in place; *h_rho is in/out like the
+ * reference's T& rho.  h_pcg_iters / h_pcg_exit (optional, length
+ * sqp_max_iter) receive the per-iteration PCG iteration counts and max-iter
+ * flags (the tuple's pcg_iter_vec / pcg_exit_vec).  Stream-ordered; returns
+ * after the solve completed (the stats are host values).
+ */
+gpt_status gpt_sqp_solve(gpt_handle *h, uint32_t knot_points, const float *d_eePos_traj, float *d_lambda,
+                         float *d_xu, float *h_rho, float rho_reset, gpt_sqp_stats *h_stats,
+                         uint32_t *h_pcg_iters, uint8_t *h_pcg_exit, gpt_stream_t stream);
+
+/* Many independent instances of uneven horizon in one call (no reference
+ * counterpart; the reference solves one instance per sqpSolve).  h_rho and
+ * h_stats have `batch` entries. */
+gpt_status gpt_sqp_solve_batched(gpt_handle *h, uint32_t batch, const uint32_t *h_knot_points,
+                                 const float *d_eePos_traj, float *d_lambda, float *d_xu, float *h_rho,
+                                 float rho_reset, gpt_sqp_stats *h_stats, gpt_stream_t stream);
+
+/* ---- the reference's kernels, one instance, device buffers, stream-ordered ---- */
+
+/* gato_form_kkt (schur.cuh:391-524); d_xs = x_s (14) */
+gpt_status gpt_form_kkt(gpt_handle *h, uint32_t knot_points, const float *d_xu, const float *d_eePos_traj,
+                        const float *d_xs, float *d_G, float *d_C, float *d_g, float *d_c, gpt_stream_t stream);
+
+/* form_schur -> gato_form_schur_jacobi (schur.cuh:545-559, oldschur.cuh:518-963).
+ * d_Ginv (245N-49) receives (Q+rho I)^-1 and (R+rho I)^-1, which the reference
+ * writes over d_G (schur.cuh:236-256). */
+gpt_status gpt_form_schur(gpt_handle *h, uint32_t knot_points, float rho, const float *d_G, const float *d_C,
+                          const float *d_g, const float *d_c, float *d_S, float *d_Pinv, float *d_gamma,
+                          float *d_Ginv, gpt_stream_t stream);
+
+/* form_schur_qdl (schur.cuh:528-542): upper-triangle CSC values (nnz = 196(N-1)+105N) */
+gpt_status gpt_form_schur_csc(gpt_handle *h, uint32_t knot_points, float rho, const float *d_G, const float *d_C,
+                              const float *d_g, const float *d_c, float *d_val, float *d_gamma, float *d_Ginv,
+                              gpt_stream_t stream);
+
+/* prep_csr (utils.cuh:84-118): CSC column pointers [14N+1] and row indices [nnz] (host arrays) */
+gpt_status gpt_prep_csr(uint32_t knot_points, int32_t *h_col_ptr, int32_t *h_row_ind);
+
+/* GPU-PCG pcg<T,STATE_SIZE,KNOT_POINTS> launch (toplevel.cuh:135-157,292-294):
+ * solves S lambda = gamma from the warm start in d_lambda. */
+gpt_status gpt_pcg(gpt_handle *h, uint32_t knot_points, const float *d_S, const float *d_Pinv,
+                   const float *d_gamma, float *d_lambda, uint32_t max_iter, float exit_tol, uint32_t exit_mode,
+                   uint32_t *h_iters, uint8_t *h_maxiter_exit, gpt_stream_t stream);
+
+/* compute_dz (schur.cuh:562-566, oldschur.cuh:966-1105) from Ginv */
+gpt_status gpt_compute_dz(gpt_handle *h, uint32_t knot_points, const float *d_Ginv, const float *d_C,
+                          const float *d_g, const float *d_lambda, float *d_dz, gpt_stream_t stream);
+
+/* compute_merit (merit.cuh:99-145): merit of d_xu -> *d_merit (one float) */
+gpt_status gpt_compute_merit(gpt_handle *h, uint32_t knot_points, const float *d_xu, const float *d_eePos_traj,
+                             float *d_merit, gpt_stream_t stream);
+
+/* ls_gato_compute_merit x 8 (merit.cuh:16-94, toplevel.cuh:357-374): merits of
+ * d_xu + alpha_p d_dz, alpha_p = -2^-p, p = 0..7 -> d_merits[8] */
+gpt_status gpt_ls_compute_merit(gpt_handle *h, uint32_t knot_points, const float *d_xs, const float *d_xu,
+                                const float *d_eePos_traj, const float *d_dz, float *d_merits,
+                                gpt_stream_t stream);
+
+/* ---- instrumentation (no reference counterpart; the reference times with
+ * clock_gettime around host syncs, toplevel.cuh:36-38,219-222,286-303) ---- */
+
+/* SQP-loop phases timed with CUDA events on the launch stream */
+#define GPT_PHASE_INIT 0   /* x_s copy + merit of the initial iterate */
+#define GPT_PHASE_KKT 1    /* KKT formation */
+#define GPT_PHASE_SCHUR 2  /* Schur complement + preconditioner */
+#define GPT_PHASE_PCG 3    /* PCG solve */
+#define GPT_PHASE_DZ 4     /* dz recovery */
+#define GPT_PHASE_MERIT 5  /* 8-step line-search merits */
+#define GPT_PHASE_ACCEPT 6 /* merit reduction, rho schedule, step update */
+#define GPT_NUM_PHASES 7
+
+/* When enabled, every SQP-loop launch is bracketed by CUDA events. */
+gpt_status gpt_set_profiling(gpt_handle *h, int enable);
+/* Accumulated device milliseconds and launch counts per phase (arrays of
+ * GPT_NUM_PHASES); reset != 0 clears them. */
+gpt_status gpt_get_phase_stats(gpt_handle *h, double *h_ms, uint64_t *h_launches, int reset);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GPT_H */

@@ -1,0 +1,265 @@
+"""Parity of the CUDA kernels (through the C ABI) against the CPU oracle.
+
+Every kernel is fed the same inputs as the oracle; the oracle runs in FP64
+unless noted.  Tolerances are written next to each check: FP32 kernels vs an
+FP64 restatement, scaled by the magnitude of the compared block.
+"""
+import numpy as np
+import pytest
+
+from conftest import ref_problem
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+
+
+def dev(a):
+    return torch.as_tensor(np.ascontiguousarray(a, np.float32), device="cuda")
+
+
+def host(t):
+    torch.cuda.synchronize()
+    return t.detach().cpu().numpy().astype(np.float64)
+
+
+def close(got, want, rtol, what, scale=None):
+    """|got - want| <= rtol * scale elementwise, scale = max|want| by default."""
+    s = np.abs(want).max() if scale is None else scale
+    err = np.abs(got - want).max()
+    assert err <= rtol * max(s, 1e-30), f"{what}: max err {err:.3e} vs scale {s:.3e} (rtol {rtol})"
+
+
+REF_CFG = dict(timestep=1.0 / 64, integrator=0, qd_cost=1e-4, r_cost=1e-4)
+SPEC_CFG = dict(timestep=0.01, integrator=1, qd_cost=1e-2, r_cost=1e-4)
+
+
+def problems(golden, problem_mod):
+    out = []
+    for N in (2, 3, 32, 128):
+        out.append(("ref", N, REF_CFG, ref_problem(golden, N)))
+    for N in (4, 64):
+        out.append(("spec", N, SPEC_CFG, problem_mod.make_problem(N, 7, dt=0.01)))
+    return out
+
+
+def oracle_params(oracle, cfg, ref_terminal=1):
+    return oracle.make_params(dt=cfg["timestep"], integrator=cfg["integrator"], qd_cost=cfg["qd_cost"],
+                              r_cost=cfg["r_cost"], ref_terminal=ref_terminal)
+
+
+@pytest.fixture(scope="module")
+def solvers(gpt):
+    cache = {}
+
+    def get(cfg, **extra):
+        key = tuple(sorted(cfg.items())) + tuple(sorted(extra.items()))
+        if key not in cache:
+            cache[key] = gpt.Solver(max_knot_points=512, **cfg, **extra)
+        return cache[key]
+    yield get
+    for s in cache.values():
+        s.close()
+
+
+def kkt_gpu(sv, N, p):
+    G, Cm, g, c = (torch.zeros(n, device="cuda") for n in (245 * N - 49, 294 * (N - 1), 21 * N - 7, 14 * N))
+    sv.form_kkt(N, dev(p["xu"]), dev(p["goal"]), dev(p["xs"]), G, Cm, g, c)
+    return host(G), host(Cm), host(g), host(c)
+
+
+@pytest.mark.parametrize("ref_terminal", [1, 0])
+def test_form_kkt(gpt, oracle, golden, problem_mod, solvers, ref_terminal):
+    for kind, N, cfg, p in problems(golden, problem_mod):
+        sv = solvers(cfg, ref_terminal=ref_terminal)
+        G, Cm, g, c = kkt_gpu(sv, N, p)
+        oG, oC, og, oc = oracle.form_kkt(oracle_params(oracle, cfg, ref_terminal), N, p["xu"], p["goal"], p["xs"])
+        for k in range(N):
+            # Q_k holds q q^T (the reference's Hessian, iiwa_eepos_plant.cuh:362-373): relative 2e-5 of its block
+            close(G[245 * k:245 * k + 196], oG[245 * k:245 * k + 196], 2e-5, f"{kind} N={N} Q_{k}")
+        close(G, oG, 2e-5, f"{kind} N={N} G")
+        for k in range(N - 1):
+            close(Cm[294 * k:294 * k + 294], oC[294 * k:294 * k + 294], 2e-5, f"{kind} N={N} C_{k}")
+        close(g, og, 2e-5, f"{kind} N={N} g")
+        # defects are differences of nearby states: absolute 1e-5 of the state scale
+        close(c, oc, 1e-5, f"{kind} N={N} c", scale=max(1.0, np.abs(p["xu"]).max()))
+
+
+def test_form_schur(gpt, oracle, golden, problem_mod, solvers):
+    for kind, N, cfg, p in problems(golden, problem_mod):
+        sv = solvers(cfg)
+        oG, oC, og, oc = oracle.form_kkt(oracle_params(oracle, cfg), N, p["xu"], p["goal"], p["xs"])
+        for rho in (1e-3, 0.5):
+            # inputs rounded to float32 once; the oracle works on the same rounded values
+            f = [x.astype(np.float32).astype(np.float64) for x in (oG, oC, og, oc)]
+            S, Pv, gam, Gi = (torch.zeros(n, device="cuda") for n in (588 * N, 588 * N, 14 * N, 245 * N - 49))
+            sv.form_schur(N, rho, *(dev(x) for x in f), S, Pv, gam, Gi)
+            S, Pv, gam, Gi = map(host, (S, Pv, gam, Gi))
+            wS, wP, wg, wGi = oracle.form_schur(N, rho, *f)
+            for k in range(N):
+                for b in range(3):
+                    if (k == 0 and b == 0) or (k == N - 1 and b == 2):
+                        assert np.abs(S[588 * k + 196 * b:588 * k + 196 * (b + 1)]).max() == 0.0
+                        continue
+                    blk = slice(588 * k + 196 * b, 588 * k + 196 * (b + 1))
+                    close(S[blk], wS[blk], 1e-4, f"{kind} N={N} rho={rho} S[{k}][{b}]")
+                Sd = S[588 * k + 196:588 * k + 392].reshape(14, 14, order="F")
+                Pd = Pv[588 * k + 196:588 * k + 392].reshape(14, 14, order="F")
+                # Pinv diag = (S diag)^{-1} (theta inverted in FP64): residual test
+                assert np.abs(Sd @ Pd - np.eye(14)).max() < 1e-3, (kind, N, rho, k)
+                assert np.abs(Pv[588 * k:588 * k + 196]).max() == 0 and np.abs(Pv[588 * k + 392:588 * k + 588]).max() == 0
+            close(gam, wg, 1e-4, f"{kind} N={N} gamma")
+            close(Gi, wGi, 1e-4, f"{kind} N={N} Ginv")
+
+
+def test_form_schur_csc_matches_block_layout(gpt, oracle, golden, solvers):
+    N = 16
+    p = ref_problem(golden, N)
+    sv = solvers(REF_CFG)
+    f = [x.astype(np.float32) for x in oracle.form_kkt(oracle_params(oracle, REF_CFG), N, p["xu"], p["goal"], p["xs"])]
+    S, Pv, gam, Gi = (torch.zeros(n, device="cuda") for n in (588 * N, 588 * N, 14 * N, 245 * N - 49))
+    sv.form_schur(N, 1e-3, *(dev(x) for x in f), S, Pv, gam, Gi)
+    val = torch.zeros(196 * (N - 1) + 105 * N, device="cuda")
+    gam2, Gi2 = torch.zeros_like(gam), torch.zeros_like(Gi)
+    sv.form_schur_csc(N, 1e-3, *(dev(x) for x in f), val, gam2, Gi2)
+    # the CSC values are exactly the block matrix's upper triangle (same arithmetic)
+    np.testing.assert_array_equal(host(val), oracle.csc_values(N, host(S)))
+    np.testing.assert_array_equal(host(gam2), host(gam))
+
+
+@pytest.mark.parametrize("exit_mode", [0, 1])
+def test_pcg_reaches_tolerance(gpt, oracle, golden, problem_mod, solvers, exit_mode):
+    for kind, N, cfg, p in problems(golden, problem_mod):
+        sv = solvers(cfg)
+        oG, oC, og, oc = oracle.form_kkt(oracle_params(oracle, cfg), N, p["xu"], p["goal"], p["xs"])
+        S, Pv, gam, _ = oracle.form_schur(N, 1e-1, *(x.astype(np.float32) for x in (oG, oC, og, oc)))
+        S, Pv, gam = (x.astype(np.float32) for x in (S, Pv, gam))
+        lam_star = oracle.banded_cholesky(N, S, gam)
+        tol = 1e-6 if exit_mode == 0 else 1e-9 * float(np.abs(gam).max()) ** 2
+        lam = torch.zeros(14 * N, device="cuda")
+        it, maxed = sv.pcg(N, dev(S), dev(Pv), dev(gam), lam, 20000, tol, exit_mode)
+        lam = host(lam)
+        M = S.astype(np.float64)
+        r = gam - np.concatenate([
+            sum(M[588 * k + 196 * b:588 * k + 196 * (b + 1)].reshape(14, 14, order="F") @ lam[14 * kk:14 * kk + 14]
+                for b, kk in ((0, k - 1), (1, k), (2, k + 1)) if 0 <= kk < N) for k in range(N)])
+        relres = np.linalg.norm(r) / np.linalg.norm(gam)
+        assert not maxed, (kind, N, it)
+        assert it > 0
+        if exit_mode == 0:
+            # the recursively updated residual met 1e-6; the true FP64 residual within 10x of it
+            assert relres < 1e-5, (kind, N, relres, it)
+        # warm start from the solution: converges immediately
+        lam2 = torch.as_tensor(lam_star.astype(np.float32), device="cuda")
+        it2, _ = sv.pcg(N, dev(S), dev(Pv), dev(gam), lam2, 20000, max(tol, 1e-4) if exit_mode == 0 else tol * 1e6,
+                        exit_mode)
+        assert it2 <= max(2, it // 4), (kind, N, it2, it)
+
+
+def test_compute_dz(gpt, oracle, golden, problem_mod, solvers):
+    for kind, N, cfg, p in problems(golden, problem_mod):
+        sv = solvers(cfg)
+        oG, oC, og, oc = oracle.form_kkt(oracle_params(oracle, cfg), N, p["xu"], p["goal"], p["xs"])
+        f = [x.astype(np.float32).astype(np.float64) for x in (oG, oC, og, oc)]
+        S, Pv, gam, Gi = oracle.form_schur(N, 1e-2, *f)
+        lam = oracle.banded_cholesky(N, S, gam).astype(np.float32).astype(np.float64)
+        Gi = Gi.astype(np.float32).astype(np.float64)
+        dz = torch.zeros(21 * N - 7, device="cuda")
+        sv.compute_dz(N, dev(Gi), dev(f[1]), dev(f[2]), dev(lam), dz)
+        want = oracle.compute_dz(N, Gi, f[1], f[2], lam)
+        for k in range(N):
+            close(host(dz)[21 * k:21 * k + 14], want[21 * k:21 * k + 14], 1e-4, f"{kind} N={N} dz_x{k}",
+                  scale=np.abs(want).max())
+
+
+def test_merits(gpt, oracle, golden, problem_mod, solvers):
+    for kind, N, cfg, p in problems(golden, problem_mod):
+        sv = solvers(cfg)
+        par = oracle_params(oracle, cfg)
+        m = torch.zeros(1, device="cuda")
+        sv.compute_merit(N, dev(p["xu"]), dev(p["goal"]), m)
+        want, _ = oracle.merit(par, N, p["xu"].astype(np.float64), None, 0.0, p["goal"], p["xs"], 0)
+        assert abs(host(m)[0] - want) <= 2e-5 * abs(want) + 1e-6, (kind, N, host(m)[0], want)
+        rng = np.random.default_rng(N)
+        dz = (rng.normal(0, 0.05, 21 * N - 7)).astype(np.float32)
+        xs = (p["xs"] + rng.normal(0, 0.01, 14)).astype(np.float32)
+        ms = torch.zeros(8, device="cuda")
+        sv.ls_compute_merit(N, dev(xs), dev(p["xu"]), dev(p["goal"]), dev(dz), ms)
+        got = host(ms)
+        for a in range(8):
+            w, _ = oracle.merit(par, N, p["xu"], dz, -1.0 / (1 << a), p["goal"], xs, 1)
+            assert abs(got[a] - w) <= 5e-5 * abs(w) + 1e-5, (kind, N, a, got[a], w)
+
+
+def test_sqp_first_iterate_matches_oracle(gpt, oracle, golden, problem_mod, solvers):
+    """One SQP iteration (KKT, Schur, PCG to 1e-7, dz, line search, step) vs the
+    oracle's iteration with the exact FP64 Cholesky solve: the new iterate xu
+    agrees to 1e-4 relative (per-iterate primal parity)."""
+    for kind, N, cfg, p in problems(golden, problem_mod):
+        if N > 64:
+            continue
+        sv = solvers(cfg)
+        sv.set_solver(sqp_max_iter=1, pcg_max_iter=20000, pcg_exit_tol=1e-7, pcg_exit_mode=0)
+        xu = dev(p["xu"])
+        lam = dev(p["lam"])
+        res = sv.sqp_solve(N, dev(p["goal"]), lam, xu, 1e-3)
+        sv.set_solver(sqp_max_iter=40, pcg_max_iter=167, pcg_exit_tol=1e-5)
+        sol = oracle.make_solver(linsys=2, sqp_max_iter=1)
+        oxu, olam, orho, ost, _ = oracle.sqp_solve(oracle_params(oracle, cfg), sol, N, p["goal"], p["lam"], p["xu"], 1e-3)
+        assert res.sqp_iters == 1 and ost.sqp_iters == 1
+        gxu = host(xu)
+        step_g = gxu - p["xu"]
+        step_o = oxu - p["xu"]
+        assert np.linalg.norm(step_g - step_o) <= 1e-4 * max(np.linalg.norm(step_o), 1e-6) + 1e-5, (
+            kind, N, np.linalg.norm(step_g - step_o), np.linalg.norm(step_o))
+        assert abs(res.rho - orho) <= 1e-6 * orho
+
+
+def test_sqp_solve_full_reduces_merit_like_oracle(gpt, oracle, golden, problem_mod, solvers):
+    for kind, N, cfg, p in problems(golden, problem_mod):
+        if N not in (32, 64):
+            continue
+        sv = solvers(cfg)
+        sv.set_solver(sqp_max_iter=10, pcg_max_iter=4000, pcg_exit_tol=1e-6)
+        res = sv.sqp_solve(N, dev(p["goal"]), dev(p["lam"]), dev(p["xu"]), 1e-3)
+        sv.set_solver(sqp_max_iter=40, pcg_max_iter=167, pcg_exit_tol=1e-5)
+        sol = oracle.make_solver(linsys=2, sqp_max_iter=10)
+        oxu, olam, orho, ost, _ = oracle.sqp_solve(oracle_params(oracle, cfg), sol, N, p["goal"], p["lam"], p["xu"], 1e-3)
+        m0 = res.stats["merit_initial"]
+        assert res.stats["merit_final"] < m0
+        # both descend to within 5% of each other's merit after 10 iterations
+        assert abs(res.stats["merit_final"] - ost.merit_final) <= 0.05 * abs(m0 - ost.merit_final) + 1e-4, (
+            kind, N, res.stats, ost.merit_final)
+
+
+def test_batched_equals_plain(gpt, problem_mod, solvers):
+    Ns = [8, 16, 5, 32]
+    batch = problem_mod.make_batch(Ns, seed0=11)
+    sv = gpt.Solver(max_knot_points=64, max_batch=8, **SPEC_CFG)
+    sv.set_solver(sqp_max_iter=6, pcg_max_iter=500, pcg_exit_tol=1e-5)
+    xu = dev(batch["xu"])
+    lam = dev(batch["lam"])
+    rho, stats = sv.sqp_solve_batched(Ns, dev(batch["goal"]), lam, xu, [1e-3] * len(Ns))
+    gxu = host(xu)
+    off = 0
+    for b, N in enumerate(Ns):
+        p = problem_mod.make_problem(N, 11 + b)
+        xu1 = dev(p["xu"])
+        r1 = sv.sqp_solve(N, dev(p["goal"]), dev(p["lam"]), xu1, 1e-3)
+        np.testing.assert_array_equal(gxu[21 * off:21 * off + 21 * N - 7], host(xu1))
+        assert r1.sqp_iters == stats[b]["sqp_iters"]
+        assert abs(r1.rho - rho[b]) == 0.0
+        off += N
+    sv.close()
+
+
+def test_bad_arguments_are_rejected_without_launch(gpt, solvers):
+    sv = solvers(REF_CFG)
+    t = torch.zeros(1000, device="cuda")
+    with pytest.raises(gpt.GptError) as e:
+        sv.form_kkt(1, t, t, t, t, t, t, t)  # N < 2
+    assert e.value.status == 1
+    with pytest.raises(gpt.GptError):
+        sv.pcg(600, t, t, t, t, 10, 1e-5)  # N above the handle's capacity
+    with pytest.raises(ValueError):
+        sv.form_kkt(4, t.cpu(), t, t, t, t, t, t)
