@@ -42,7 +42,7 @@ struct gpt_handle {
     int num_sms = 148;
     size_t cap_knots = 0;  // max_batch * max_knot_points
     // workspace
-    float *G = nullptr, *C = nullptr, *g = nullptr, *c = nullptr, *S = nullptr, *Pinv = nullptr,
+    float *G = nullptr, *C = nullptr, *g = nullptr, *c = nullptr, *S = nullptr,
           *gamma = nullptr, *Ginv = nullptr, *dz = nullptr, *xs = nullptr, *knot_merit = nullptr,
           *merits = nullptr;
     InstState *st = nullptr;
@@ -89,6 +89,7 @@ SolverParams to_solver(const gpt_solver_config &sc)
     S.rho_factor = sc.rho_factor;
     S.rho_max = sc.rho_max;
     S.rho_min = sc.rho_min;
+    S.pcg_cluster_size = sc.pcg_cluster_size;
     return S;
 }
 BatchView single_view(uint32_t N)
@@ -139,6 +140,7 @@ void gpt_default_solver_config(gpt_solver_config *o)
     o->rho_factor = 1.2f;
     o->rho_max = 10.0f;
     o->rho_min = 1e-3f;
+    o->pcg_cluster_size = 0;
 }
 
 const char *gpt_last_error(void) { return g_last_error.c_str(); }
@@ -149,6 +151,8 @@ gpt_status gpt_set_solver_config(gpt_handle *h, const gpt_solver_config *sc)
     if (!h || !sc) return set_err(GPT_ERR_BAD_ARG, "null argument");
     if (sc->sqp_max_iter == 0 || sc->sqp_max_iter > 4096) return set_err(GPT_ERR_BAD_ARG, "sqp_max_iter out of range");
     if (!(sc->rho_factor > 1.0f) || !(sc->rho_min > 0.0f)) return set_err(GPT_ERR_BAD_ARG, "rho schedule out of range");
+    if (sc->pcg_cluster_size & (sc->pcg_cluster_size - 1) || sc->pcg_cluster_size > 16)
+        return set_err(GPT_ERR_BAD_ARG, "pcg_cluster_size must be 0, 1, 2, 4, 8 or 16");
     if (sc->sqp_max_iter > h->sc.sqp_max_iter && h->pcg_log) {
         // pcg log is sized at creation
         return set_err(GPT_ERR_CAPACITY, "sqp_max_iter larger than at creation");
@@ -188,8 +192,7 @@ gpt_status gpt_create(const gpt_problem_config *pc, const gpt_solver_config *sc,
     ALLOC(C, C_STRIDE * T);
     ALLOC(g, NX * T);
     ALLOC(c, NS * T);
-    ALLOC(S, S_STRIDE * T);
-    ALLOC(Pinv, SS * T);
+    ALLOC(S, PK * T);
     ALLOC(gamma, NS * T);
     ALLOC(Ginv, G_STRIDE * T);
     ALLOC(dz, NX * T);
@@ -208,7 +211,7 @@ gpt_status gpt_create(const gpt_problem_config *pc, const gpt_solver_config *sc,
     if (e == cudaSuccess) e = cudaMallocHost((void **)&h->h_pcg_out, sizeof(uint32_t) * 2 * B);
     if (e == cudaSuccess) e = cudaMallocHost((void **)&h->h_pcg_log, sizeof(uint32_t) * B * sc->sqp_max_iter);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->ev, cudaEventDisableTiming);
-    if (e == cudaSuccess) e = cudaMemset(h->Pinv, 0, sizeof(float) * SS * T);
+    if (e == cudaSuccess) e = cudaMemset(h->S, 0, sizeof(float) * PK * T);
     if (e == cudaSuccess) e = cudaMemset(h->dz, 0, sizeof(float) * NX * T);
     if (e == cudaSuccess) e = cudaDeviceSynchronize();
     if (e != cudaSuccess) {
@@ -244,7 +247,7 @@ gpt_status gpt_destroy(gpt_handle *h)
 {
     if (!h) return GPT_OK;
     for (cudaEvent_t e : h->ev_pool) cudaEventDestroy(e);
-    cudaFree(h->G); cudaFree(h->C); cudaFree(h->g); cudaFree(h->c); cudaFree(h->S); cudaFree(h->Pinv);
+    cudaFree(h->G); cudaFree(h->C); cudaFree(h->g); cudaFree(h->c); cudaFree(h->S);
     cudaFree(h->gamma); cudaFree(h->Ginv); cudaFree(h->dz); cudaFree(h->xs); cudaFree(h->knot_merit);
     cudaFree(h->merits); cudaFree(h->st); cudaFree(h->knot_off); cudaFree(h->knot_inst); cudaFree(h->pcg_log);
     cudaFree(h->pcg_out); cudaFree(h->d_active);
@@ -315,8 +318,8 @@ gpt_status gpt_pcg(gpt_handle *h, uint32_t N, const float *d_S, const float *d_P
     if (!h || !d_S || !d_Pinv || !d_gamma || !d_lambda) return set_err(GPT_ERR_BAD_ARG, "null argument");
     if (!check_n(h, N) || exit_mode > 1) return set_err(GPT_ERR_BAD_ARG, "knot_points/exit_mode out of range");
     cudaStream_t s = (cudaStream_t)stream;
-    GPT_CUDA(launch_pcg(single_view(N), (int)N, d_S, d_Pinv, S_STRIDE, SS, d_gamma, d_lambda, (int)max_iter, tol,
-                        (int)exit_mode, h->pcg_out, nullptr, 0, h->num_sms, s));
+    GPT_CUDA(launch_pcg(single_view(N), (int)N, (int)N, 0, d_S, d_Pinv, d_gamma, d_lambda, (int)max_iter, tol,
+                        (int)exit_mode, h->pcg_out, nullptr, 0, (int)h->sc.pcg_cluster_size, h->num_sms, s));
     GPT_CUDA(cudaMemcpyAsync(h->h_pcg_out, h->pcg_out, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
     GPT_CUDA(cudaStreamSynchronize(s));
     if (h_iters) *h_iters = h->h_pcg_out[0];
@@ -418,8 +421,11 @@ static gpt_status sqp_run(gpt_handle *h, uint32_t B, const uint32_t *Ns, const f
     }
     const int total = off[B];
     if ((size_t)total > h->cap_knots) return set_err(GPT_ERR_CAPACITY, "total knots exceed workspace");
-    int maxN = 0;
-    for (uint32_t b = 0; b < B; ++b) maxN = Ns[b] > (uint32_t)maxN ? (int)Ns[b] : maxN;
+    int maxN = 0, minN = 1 << 30;
+    for (uint32_t b = 0; b < B; ++b) {
+        maxN = Ns[b] > (uint32_t)maxN ? (int)Ns[b] : maxN;
+        minN = Ns[b] < (uint32_t)minN ? (int)Ns[b] : minN;
+    }
     if (off != h->off_cache) {
         std::vector<int> inst(total);
         for (uint32_t b = 0; b < B; ++b)
@@ -460,12 +466,13 @@ static gpt_status sqp_run(gpt_handle *h, uint32_t B, const uint32_t *Ns, const f
         }
         {
             PhaseTimer t(h, s, GPT_PHASE_SCHUR);
-            GPT_CUDA(launch_schur(1, bv, 0.f, h->G, h->C, h->g, h->c, h->S, h->Pinv, h->gamma, h->Ginv, nullptr, ns, s));
+            GPT_CUDA(launch_schur(1, bv, 0.f, h->G, h->C, h->g, h->c, h->S, nullptr, h->gamma, h->Ginv, nullptr, ns, s));
         }
         {
             PhaseTimer t(h, s, GPT_PHASE_PCG);
-            GPT_CUDA(launch_pcg(bv, maxN, h->S, h->Pinv, SS, 0, h->gamma, d_lambda, (int)SP.pcg_max_iter, SP.pcg_tol,
-                                (int)SP.pcg_exit_mode, nullptr, h->pcg_log, (int)SP.sqp_max_iter, ns, s));
+            GPT_CUDA(launch_pcg(bv, maxN, minN, 1, h->S, nullptr, h->gamma, d_lambda, (int)SP.pcg_max_iter, SP.pcg_tol,
+                                (int)SP.pcg_exit_mode, nullptr, h->pcg_log, (int)SP.sqp_max_iter,
+                                (int)SP.pcg_cluster_size, ns, s));
         }
         {
             PhaseTimer t(h, s, GPT_PHASE_DZ);

@@ -8,7 +8,8 @@
 
 namespace gpt {
 
-constexpr int MAX_PCG_KNOTS = 512;  // one thread block per instance holds 2 x 14 N floats
+constexpr int MAX_PCG_KNOTS = 512;  // horizon limit of this build (16-CTA cluster x 32 knots)
+constexpr int PCG_KPC_MAX = 128;    // knots per CTA held in shared memory by the PCG
 
 // SQP control constants (settings.cuh:31-50 and the -D flags of perform_experiment.sh:42-58)
 struct SolverParams {
@@ -17,6 +18,7 @@ struct SolverParams {
     float pcg_tol;
     uint32_t pcg_exit_mode;
     float rho_factor, rho_max, rho_min;
+    uint32_t pcg_cluster_size;  // 0: chosen from N and the batch size
 };
 
 cudaError_t launch_kkt(const BatchView &bv, const ProblemParams &P, const float *xu, const float *goal,
@@ -24,10 +26,13 @@ cudaError_t launch_kkt(const BatchView &bv, const ProblemParams &P, const float 
 cudaError_t launch_schur(int mode, const BatchView &bv, float rho_scalar, const float *G, const float *C,
                          const float *g, const float *c, float *S, float *Pinv, float *gamma, float *Ginv,
                          float *csc_val, int num_sms, cudaStream_t s);
-size_t pcg_smem_bytes(int max_n_knots);
-cudaError_t launch_pcg(const BatchView &bv, int max_n_knots, const float *S, const float *Pinv, int pinv_stride,
-                       int pinv_off, const float *gamma, float *lambda, int max_iter, float tol, int exit_mode,
-                       uint32_t *out_iters, uint32_t *pcg_log, int log_stride, int num_sms, cudaStream_t s);
+size_t pcg_cluster_smem_bytes(int kpc);
+int pcg_pick_cluster(int maxN, int B, int num_sms, int requested);
+// fmt 0: S and Pinv in the reference 3-block layout; fmt 1: packed rows (PK floats per knot) in S
+cudaError_t launch_pcg(const BatchView &bv, int max_n_knots, int min_n_knots, int fmt, const float *S,
+                       const float *Pinv, const float *gamma, float *lambda, int max_iter, float tol, int exit_mode,
+                       uint32_t *out_iters, uint32_t *pcg_log, int log_stride, int cluster_size, int num_sms,
+                       cudaStream_t s);
 cudaError_t launch_dz(const BatchView &bv, const float *Ginv, const float *C, const float *g, const float *lambda,
                       float *dz, int num_sms, cudaStream_t s);
 cudaError_t launch_merit(const BatchView &bv, const ProblemParams &P, int n_alpha, const float *xu, const float *dz,

@@ -83,7 +83,8 @@ struct SchurWarpSmem {
 constexpr int SCHUR_WARPS = 4;
 
 // MODE 0: S, Pinv (reference 3-block layout, off-diagonal Pinv blocks zero), gamma, Ginv
-// MODE 1: S, compact Pinv (diagonal block only, stride 196), gamma, Ginv
+// MODE 1: packed rows for the PCG (PK = 408 floats per knot: left block, lower
+//         triangle of the diagonal block, lower triangle of Pinv, 2 pad), gamma, Ginv
 // MODE 2: CSC values of the upper triangle (utils.cuh:55-118 layout), gamma, Ginv
 template <int MODE>
 __global__ void __launch_bounds__(32 * SCHUR_WARPS)
@@ -105,7 +106,7 @@ __global__ void __launch_bounds__(32 * SCHUR_WARPS)
         const int N = bv.N(b);
         const int k = j - bv.off(b);
         const float rho = bv.st ? bv.st[b].rho : rho_scalar;
-        float *Srow = S ? S + (size_t)S_STRIDE * j : nullptr;
+        float *Srow = (MODE == 0) ? S + (size_t)S_STRIDE * j : nullptr;
 
         if (k == 0) {
             const float *Q0 = G + (size_t)G_STRIDE * j;
@@ -126,9 +127,15 @@ __global__ void __launch_bounds__(32 * SCHUR_WARPS)
                     Srow[e] = 0.f;
                     Srow[SS + e] = -sm.Qki[e];
                 } else if (MODE == 1) {
-                    Pinv[(size_t)SS * j + e] = -qv;
-                    Srow[e] = 0.f;
-                    Srow[SS + e] = -sm.Qki[e];
+                    float *Pk = S + (size_t)PK * j;
+                    const int r = e % NS, cc = e / NS;
+                    Pk[e] = 0.f;  // no left block in row 0
+                    if (r >= cc) {
+                        const int t = ((r * (r + 1)) >> 1) + cc;
+                        Pk[SS + t] = -sm.Qki[e];
+                        Pk[SS + 105 + t] = -qv;
+                    }
+                    if (e < PK - SS - 210) Pk[SS + 210 + e] = 0.f;
                 }
                 if (N == 1) Ginv[(size_t)G_STRIDE * j + e] = sm.Qki[e];
             }
@@ -145,8 +152,6 @@ __global__ void __launch_bounds__(32 * SCHUR_WARPS)
                     Pinv[(size_t)S_STRIDE * j + 2 * SS + e] = 0.f;
                     if (N == 1) Srow[2 * SS + e] = 0.f;
                 }
-            } else if (MODE == 1 && N == 1) {
-                for (int e = lane; e < SS; e += 32) Srow[2 * SS + e] = 0.f;
             }
             __syncwarp();
             continue;
@@ -202,21 +207,30 @@ __global__ void __launch_bounds__(32 * SCHUR_WARPS)
         __syncwarp();
         warp_inverse<NS>(sm.theta, 0.f, sm.thetai, lane);
         __syncwarp();
-        if (MODE != 2) {
+        if (MODE == 0) {
             float *Sprev_right = S + (size_t)S_STRIDE * (j - 1) + 2 * SS;
             for (int e = lane; e < SS; e += 32) {
                 const int r = e % NS, cc = e / NS;
                 Srow[e] = -sm.phi[e];
                 Srow[SS + e] = -sm.theta[e];
                 Sprev_right[e] = -sm.phi[cc + NS * r];
-                if (MODE == 0) {
-                    Pinv[(size_t)S_STRIDE * j + e] = 0.f;
-                    Pinv[(size_t)S_STRIDE * j + SS + e] = -sm.thetai[e];
-                    Pinv[(size_t)S_STRIDE * j + 2 * SS + e] = 0.f;
-                } else {
-                    Pinv[(size_t)SS * j + e] = -sm.thetai[e];
-                }
+                Pinv[(size_t)S_STRIDE * j + e] = 0.f;
+                Pinv[(size_t)S_STRIDE * j + SS + e] = -sm.thetai[e];
+                Pinv[(size_t)S_STRIDE * j + 2 * SS + e] = 0.f;
                 if (k == N - 1) Srow[2 * SS + e] = 0.f;
+            }
+        } else if (MODE == 1) {
+            // packed row: left block, lower triangles of the diagonal block and of Pinv
+            float *Pk = S + (size_t)PK * j;
+            for (int e = lane; e < SS; e += 32) {
+                const int r = e % NS, cc = e / NS;
+                Pk[e] = -sm.phi[e];
+                if (r >= cc) {
+                    const int t = ((r * (r + 1)) >> 1) + cc;
+                    Pk[SS + t] = -sm.theta[e];
+                    Pk[SS + 105 + t] = -sm.thetai[e];
+                }
+                if (e < PK - SS - 210) Pk[SS + 210 + e] = 0.f;
             }
         } else {
             // block row k of the CSC (utils.cuh:55-81): row r holds 14 left entries then r+1 diagonal entries

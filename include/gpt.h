@@ -77,6 +77,7 @@ typedef struct gpt_solver_config {
     float rho_factor;          /* RHO_FACTOR */
     float rho_max;             /* RHO_MAX */
     float rho_min;             /* RHO_MIN */
+    uint32_t pcg_cluster_size; /* CTAs per instance in the PCG (1,2,4,8,16); 0 = chosen by the library */
 } gpt_solver_config;
 
 /* One sqpSolve's outcome (the reference returns a tuple, toplevel.cuh:502) */
