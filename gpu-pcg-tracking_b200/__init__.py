@@ -108,7 +108,7 @@ def _declare(L):
         "gpt_form_schur": ([vp, u32, f32, vp, vp, vp, vp, vp, vp, vp, vp, vp], C.c_int),
         "gpt_form_schur_csc": ([vp, u32, f32, vp, vp, vp, vp, vp, vp, vp, vp], C.c_int),
         "gpt_prep_csr": ([u32, vp, vp], C.c_int),
-        "gpt_pcg": ([vp, u32, vp, vp, vp, vp, u32, f32, u32, P(u32), P(C.c_uint8), vp], C.c_int),
+        "gpt_pcg": ([vp, u32, vp, vp, vp, vp, vp, u32, f32, u32, P(u32), P(C.c_uint8), vp], C.c_int),
         "gpt_compute_dz": ([vp, u32, vp, vp, vp, vp, vp, vp], C.c_int),
         "gpt_compute_merit": ([vp, u32, vp, vp, vp, vp], C.c_int),
         "gpt_ls_compute_merit": ([vp, u32, vp, vp, vp, vp, vp, vp], C.c_int),
@@ -247,11 +247,11 @@ class Solver:
         _check(lib().gpt_form_schur_csc(self._h, N, rho, _ptr(G), _ptr(Cm), _ptr(g), _ptr(c), _ptr(val),
                                         _ptr(gamma), _ptr(Ginv), _stream(stream)))
 
-    def pcg(self, N, S, Pinv, gamma, lam, max_iter, exit_tol, exit_mode=0, stream=None):
+    def pcg(self, N, S, Pinv, gamma, lam, max_iter, exit_tol, exit_mode=0, lam64=None, stream=None):
         it = C.c_uint32(0)
         mx = C.c_uint8(0)
-        _check(lib().gpt_pcg(self._h, N, _ptr(S), _ptr(Pinv), _ptr(gamma), _ptr(lam), max_iter, exit_tol, exit_mode,
-                             C.byref(it), C.byref(mx), _stream(stream)))
+        _check(lib().gpt_pcg(self._h, N, _ptr(S), _ptr(Pinv), _ptr(gamma), _ptr(lam), _ptr(lam64), max_iter,
+                             exit_tol, exit_mode, C.byref(it), C.byref(mx), _stream(stream)))
         return it.value, bool(mx.value)
 
     def compute_dz(self, N, Ginv, Cm, g, lam, dz, stream=None):

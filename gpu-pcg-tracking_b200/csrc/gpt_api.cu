@@ -48,6 +48,8 @@ struct gpt_handle {
     InstState *st = nullptr;
     int *knot_off = nullptr, *knot_inst = nullptr;
     uint32_t *pcg_log = nullptr, *pcg_out = nullptr, *d_active = nullptr;
+    double *lam64 = nullptr;   // FP64 multipliers from the PCG, consumed by dz
+    uint32_t cap_sqp_iter = 0;  // pcg_log rows allocated at creation
     // pinned host staging
     uint32_t *h_active = nullptr;
     InstState *h_st = nullptr;
@@ -153,7 +155,7 @@ gpt_status gpt_set_solver_config(gpt_handle *h, const gpt_solver_config *sc)
     if (!(sc->rho_factor > 1.0f) || !(sc->rho_min > 0.0f)) return set_err(GPT_ERR_BAD_ARG, "rho schedule out of range");
     if (sc->pcg_cluster_size & (sc->pcg_cluster_size - 1) || sc->pcg_cluster_size > 16)
         return set_err(GPT_ERR_BAD_ARG, "pcg_cluster_size must be 0, 1, 2, 4, 8 or 16");
-    if (sc->sqp_max_iter > h->sc.sqp_max_iter && h->pcg_log) {
+    if (sc->sqp_max_iter > h->cap_sqp_iter) {
         // pcg log is sized at creation
         return set_err(GPT_ERR_CAPACITY, "sqp_max_iter larger than at creation");
     }
@@ -185,6 +187,7 @@ gpt_status gpt_create(const gpt_problem_config *pc, const gpt_solver_config *sc,
     const size_t T = (size_t)pc->max_batch * pc->max_knot_points;
     const size_t B = pc->max_batch;
     h->cap_knots = T;
+    h->cap_sqp_iter = sc->sqp_max_iter;
     cudaError_t e = cudaSuccess;
 #define ALLOC(p, n) \
     if (e == cudaSuccess) e = dalloc(&h->p, (n))
@@ -205,6 +208,7 @@ gpt_status gpt_create(const gpt_problem_config *pc, const gpt_solver_config *sc,
     ALLOC(pcg_log, B * sc->sqp_max_iter);
     ALLOC(pcg_out, 2 * B);
     ALLOC(d_active, 1);
+    ALLOC(lam64, NS * T);
 #undef ALLOC
     if (e == cudaSuccess) e = cudaMallocHost((void **)&h->h_active, sizeof(uint32_t));
     if (e == cudaSuccess) e = cudaMallocHost((void **)&h->h_st, sizeof(InstState) * B);
@@ -250,7 +254,7 @@ gpt_status gpt_destroy(gpt_handle *h)
     cudaFree(h->G); cudaFree(h->C); cudaFree(h->g); cudaFree(h->c); cudaFree(h->S);
     cudaFree(h->gamma); cudaFree(h->Ginv); cudaFree(h->dz); cudaFree(h->xs); cudaFree(h->knot_merit);
     cudaFree(h->merits); cudaFree(h->st); cudaFree(h->knot_off); cudaFree(h->knot_inst); cudaFree(h->pcg_log);
-    cudaFree(h->pcg_out); cudaFree(h->d_active);
+    cudaFree(h->pcg_out); cudaFree(h->d_active); cudaFree(h->lam64);
     cudaFreeHost(h->h_active); cudaFreeHost(h->h_st); cudaFreeHost(h->h_pcg_out); cudaFreeHost(h->h_pcg_log);
     if (h->ev) cudaEventDestroy(h->ev);
     delete h;
@@ -312,13 +316,13 @@ gpt_status gpt_prep_csr(uint32_t N, int32_t *cp, int32_t *ri)
 }
 
 gpt_status gpt_pcg(gpt_handle *h, uint32_t N, const float *d_S, const float *d_Pinv, const float *d_gamma,
-                   float *d_lambda, uint32_t max_iter, float tol, uint32_t exit_mode, uint32_t *h_iters,
-                   uint8_t *h_maxit, gpt_stream_t stream)
+                   float *d_lambda, double *d_lambda64, uint32_t max_iter, float tol, uint32_t exit_mode,
+                   uint32_t *h_iters, uint8_t *h_maxit, gpt_stream_t stream)
 {
     if (!h || !d_S || !d_Pinv || !d_gamma || !d_lambda) return set_err(GPT_ERR_BAD_ARG, "null argument");
     if (!check_n(h, N) || exit_mode > 1) return set_err(GPT_ERR_BAD_ARG, "knot_points/exit_mode out of range");
     cudaStream_t s = (cudaStream_t)stream;
-    GPT_CUDA(launch_pcg(single_view(N), (int)N, (int)N, 0, d_S, d_Pinv, d_gamma, d_lambda, (int)max_iter, tol,
+    GPT_CUDA(launch_pcg(single_view(N), (int)N, (int)N, 0, d_S, d_Pinv, d_gamma, d_lambda, d_lambda64, (int)max_iter, tol,
                         (int)exit_mode, h->pcg_out, nullptr, 0, (int)h->sc.pcg_cluster_size, h->num_sms, s));
     GPT_CUDA(cudaMemcpyAsync(h->h_pcg_out, h->pcg_out, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
     GPT_CUDA(cudaStreamSynchronize(s));
@@ -333,7 +337,7 @@ gpt_status gpt_compute_dz(gpt_handle *h, uint32_t N, const float *d_Ginv, const 
 {
     if (!h || !d_Ginv || !d_C || !d_g || !d_lambda || !d_dz) return set_err(GPT_ERR_BAD_ARG, "null argument");
     if (!check_n(h, N)) return set_err(GPT_ERR_BAD_ARG, "knot_points out of range");
-    GPT_CUDA(launch_dz(single_view(N), d_Ginv, d_C, d_g, d_lambda, d_dz, h->num_sms, (cudaStream_t)stream));
+    GPT_CUDA(launch_dz(single_view(N), d_Ginv, d_C, d_g, d_lambda, nullptr, d_dz, h->num_sms, (cudaStream_t)stream));
     return GPT_OK;
 }
 
@@ -470,13 +474,13 @@ static gpt_status sqp_run(gpt_handle *h, uint32_t B, const uint32_t *Ns, const f
         }
         {
             PhaseTimer t(h, s, GPT_PHASE_PCG);
-            GPT_CUDA(launch_pcg(bv, maxN, minN, 1, h->S, nullptr, h->gamma, d_lambda, (int)SP.pcg_max_iter, SP.pcg_tol,
+            GPT_CUDA(launch_pcg(bv, maxN, minN, 1, h->S, nullptr, h->gamma, d_lambda, h->lam64, (int)SP.pcg_max_iter, SP.pcg_tol,
                                 (int)SP.pcg_exit_mode, nullptr, h->pcg_log, (int)SP.sqp_max_iter,
                                 (int)SP.pcg_cluster_size, ns, s));
         }
         {
             PhaseTimer t(h, s, GPT_PHASE_DZ);
-            GPT_CUDA(launch_dz(bv, h->Ginv, h->C, h->g, d_lambda, h->dz, ns, s));
+            GPT_CUDA(launch_dz(bv, h->Ginv, h->C, h->g, d_lambda, h->lam64, h->dz, ns, s));
         }
         {
             PhaseTimer t(h, s, GPT_PHASE_MERIT);

@@ -30,11 +30,12 @@ size_t pcg_cluster_smem_bytes(int kpc);
 int pcg_pick_cluster(int maxN, int B, int num_sms, int requested);
 // fmt 0: S and Pinv in the reference 3-block layout; fmt 1: packed rows (PK floats per knot) in S
 cudaError_t launch_pcg(const BatchView &bv, int max_n_knots, int min_n_knots, int fmt, const float *S,
-                       const float *Pinv, const float *gamma, float *lambda, int max_iter, float tol, int exit_mode,
-                       uint32_t *out_iters, uint32_t *pcg_log, int log_stride, int cluster_size, int num_sms,
-                       cudaStream_t s);
+                       const float *Pinv, const float *gamma, float *lambda, double *lambda64, int max_iter,
+                       float tol, int exit_mode, uint32_t *out_iters, uint32_t *pcg_log, int log_stride,
+                       int cluster_size, int num_sms, cudaStream_t s);
+// lambda64 (optional) replaces lambda when given
 cudaError_t launch_dz(const BatchView &bv, const float *Ginv, const float *C, const float *g, const float *lambda,
-                      float *dz, int num_sms, cudaStream_t s);
+                      const double *lambda64, float *dz, int num_sms, cudaStream_t s);
 cudaError_t launch_merit(const BatchView &bv, const ProblemParams &P, int n_alpha, const float *xu, const float *dz,
                          const float *goal, const float *xs, float *knot_merit, int num_sms, cudaStream_t s);
 cudaError_t launch_accept(const BatchView &bv, int mode, const SolverParams &SP, const float *knot_merit,

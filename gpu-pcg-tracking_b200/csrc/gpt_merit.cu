@@ -16,13 +16,19 @@ namespace gpt {
 
 constexpr int DZ_WARPS = 4;
 
+// dz from lambda (FP32 or, when lambda64 is given, FP64).  The right-hand sides
+// q_k - lambda_k - (-A_k)^T lambda_{k+1} and r_k - (-B_k)^T lambda_{k+1} cancel
+// heavily, so they are accumulated in FP64 before the FP32-stored inverses apply.
 __global__ void __launch_bounds__(32 * DZ_WARPS)
     dz_kernel(BatchView bv, const float *__restrict__ Ginv, const float *__restrict__ Cm,
-              const float *__restrict__ g, const float *__restrict__ lambda, float *__restrict__ dz)
+              const float *__restrict__ g, const float *__restrict__ lambda, const double *__restrict__ lambda64,
+              float *__restrict__ dz)
 {
-    __shared__ float s_all[DZ_WARPS][NX];
+    __shared__ double s_all[DZ_WARPS][NX];
+    __shared__ double l_all[DZ_WARPS][2 * NS];
     const int lane = threadIdx.x & 31;
-    float *s = s_all[threadIdx.x >> 5];
+    double *s = s_all[threadIdx.x >> 5];
+    double *lv = l_all[threadIdx.x >> 5];
     const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nw = (gridDim.x * blockDim.x) >> 5;
     for (int j = gw; j < bv.total_knots; j += nw) {
@@ -31,48 +37,50 @@ __global__ void __launch_bounds__(32 * DZ_WARPS)
         const int N = bv.N(b), k = j - bv.off(b);
         const bool last = (k == N - 1);
         const float *Cj = Cm + (size_t)C_STRIDE * j;
-        const float *ln = lambda + (size_t)NS * (j + 1);
+        const int nl = last ? NS : 2 * NS;
+        if (lane < nl) lv[lane] = lambda64 ? lambda64[(size_t)NS * j + lane] : (double)lambda[(size_t)NS * j + lane];
+        __syncwarp();
         if (lane < NS) {
             // q_k - (lambda_k + (-A_k)^T lambda_{k+1})
-            float a = 0.f;
+            double a = 0.0;
             if (!last) {
 #pragma unroll
-                for (int t = 0; t < NS; ++t) a = fmaf(Cj[lane * NS + t], ln[t], a);
+                for (int t = 0; t < NS; ++t) a = fma((double)Cj[lane * NS + t], lv[NS + t], a);
             }
-            s[lane] = g[(size_t)NX * j + lane] - (lambda[(size_t)NS * j + lane] + a);
+            s[lane] = (double)g[(size_t)NX * j + lane] - (lv[lane] + a);
         } else if (lane < NX && !last) {
             // r_k - (-B_k)^T lambda_{k+1}
             const int i = lane - NS;
-            float a = 0.f;
+            double a = 0.0;
 #pragma unroll
-            for (int t = 0; t < NS; ++t) a = fmaf(Cj[SS + i * NS + t], ln[t], a);
-            s[lane] = g[(size_t)NX * j + lane] - a;
+            for (int t = 0; t < NS; ++t) a = fma((double)Cj[SS + i * NS + t], lv[NS + t], a);
+            s[lane] = (double)g[(size_t)NX * j + lane] - a;
         }
         __syncwarp();
         const float *Gi = Ginv + (size_t)G_STRIDE * j;
         if (lane < NS) {
-            float a = 0.f;
+            double a = 0.0;
 #pragma unroll
-            for (int t = 0; t < NS; ++t) a = fmaf(Gi[lane + NS * t], s[t], a);
-            dz[(size_t)NX * j + lane] = a;
+            for (int t = 0; t < NS; ++t) a = fma((double)Gi[lane + NS * t], s[t], a);
+            dz[(size_t)NX * j + lane] = (float)a;
         } else if (lane < NX && !last) {
             const int i = lane - NS;
-            float a = 0.f;
+            double a = 0.0;
 #pragma unroll
-            for (int t = 0; t < NC; ++t) a = fmaf(Gi[SS + i + NC * t], s[NS + t], a);
-            dz[(size_t)NX * j + lane] = a;
+            for (int t = 0; t < NC; ++t) a = fma((double)Gi[SS + i + NC * t], s[NS + t], a);
+            dz[(size_t)NX * j + lane] = (float)a;
         }
         __syncwarp();
     }
 }
 
 cudaError_t launch_dz(const BatchView &bv, const float *Ginv, const float *C, const float *g, const float *lambda,
-                      float *dz, int num_sms, cudaStream_t s)
+                      const double *lambda64, float *dz, int num_sms, cudaStream_t s)
 {
     if (bv.total_knots <= 0) return cudaSuccess;
     int blocks = (bv.total_knots + DZ_WARPS - 1) / DZ_WARPS;
     if (blocks > num_sms * 16) blocks = num_sms * 16;
-    dz_kernel<<<blocks, 32 * DZ_WARPS, 0, s>>>(bv, Ginv, C, g, lambda, dz);
+    dz_kernel<<<blocks, 32 * DZ_WARPS, 0, s>>>(bv, Ginv, C, g, lambda, lambda64, dz);
     return cudaGetLastError();
 }
 

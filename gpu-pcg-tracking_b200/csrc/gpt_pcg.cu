@@ -20,9 +20,11 @@
 // barrier each.  No grid-wide synchronisation: clusters never wait on each
 // other.
 //
-// Exit test: mode 0 ||r||_2 <= tol ||gamma||_2 on the true residual
-// (recomputed with FP64 accumulation when the recursive residual passes;
-// up to two residual-replacement restarts); mode 1 |r^T Pinv r| < tol.
+// Precision: S, Pinv, the search direction p and z = Pinv r are FP32; the
+// iterate lambda, the residual r, the products S p and every dot product are
+// FP64.  Exit test: mode 0 ||r||_2 <= tol ||gamma||_2 on the true residual
+// (recomputed with FP64 accumulation when the recursive residual passes; up
+// to two residual-replacement restarts); mode 1 |r^T Pinv r| < tol.
 #include <cooperative_groups.h>
 
 #include "gpt_common.cuh"
@@ -145,9 +147,9 @@ __device__ __forceinline__ float pinv_row(const float *Sp, const float *rv, int 
 template <int CS, int FMT>
 __global__ void __launch_bounds__(PCG_THREADS, 1)
     pcg_cluster_kernel(BatchView bv, int kpc_max, const float *__restrict__ S, const float *__restrict__ Pinv,
-                       const float *__restrict__ gamma, float *__restrict__ lambda, int max_iter, float tol,
-                       int exit_mode, uint32_t *__restrict__ out_iters, uint32_t *__restrict__ pcg_log,
-                       int log_stride)
+                       const float *__restrict__ gamma, float *__restrict__ lambda, double *__restrict__ lambda64,
+                       int max_iter, float tol, int exit_mode, uint32_t *__restrict__ out_iters,
+                       uint32_t *__restrict__ pcg_log, int log_stride)
 {
     extern __shared__ float4 pcg_dyn_smem[];
     float *base = reinterpret_cast<float *>(pcg_dyn_smem);
@@ -201,17 +203,22 @@ __global__ void __launch_bounds__(PCG_THREADS, 1)
     }
     __syncthreads();
 
-    float lam[PCG_RPT], rr_[PCG_RPT], zz[PCG_RPT], pp[PCG_RPT], gv[PCG_RPT];
+    // lambda and the residual in FP64 (an FP32 lambda cannot represent a solution whose relative
+    // residual is below ~eps32 ||S|| ||lambda|| / ||gamma||, which exceeds 1e-5 at N = 128); the
+    // matrix, the preconditioned residual z and the search direction p stay FP32.
+    double lam[PCG_RPT], rr_[PCG_RPT];
+    float zz[PCG_RPT], pp[PCG_RPT], gv[PCG_RPT];
     double acc[3] = {0.0, 0.0, 0.0};
 #pragma unroll
     for (int q = 0; q < PCG_RPT; ++q) {
         const int i = tid + q * PCG_THREADS;
-        lam[q] = rr_[q] = zz[q] = pp[q] = gv[q] = 0.f;
+        lam[q] = rr_[q] = 0.0;
+        zz[q] = pp[q] = gv[q] = 0.f;
         if (i < nloc) {
             const int kl = i / NS, r = i - NS * kl;
             gv[q] = gb[i];
             lam[q] = c.pv[NS + i];
-            rr_[q] = (float)((double)gv[q] - schur_row<double>(c.Sp, c.left_next, c.pv, kl, r, k0 + kl, N, kpc));
+            rr_[q] = (double)gv[q] - schur_row<double>(c.Sp, c.left_next, c.pv, kl, r, k0 + kl, N, kpc);
             acc[0] += (double)gv[q] * gv[q];
         }
     }
@@ -225,7 +232,7 @@ __global__ void __launch_bounds__(PCG_THREADS, 1)
 #pragma unroll
         for (int q = 0; q < PCG_RPT; ++q) {
             const int i = tid + q * PCG_THREADS;
-            if (i < nloc) c.rv[i] = rr_[q];
+            if (i < nloc) c.rv[i] = (float)rr_[q];
         }
         __syncthreads();
         double a3[3] = {with_gg ? acc[0] : 0.0, 0.0, 0.0};
@@ -237,8 +244,8 @@ __global__ void __launch_bounds__(PCG_THREADS, 1)
                 zz[q] = pinv_row(c.Sp, c.rv, kl, r);
                 pp[q] = zz[q];
                 c.pv[NS + i] = pp[q];
-                a3[1] += (double)rr_[q] * zz[q];
-                a3[2] += (double)rr_[q] * rr_[q];
+                a3[1] += rr_[q] * (double)zz[q];
+                a3[2] += rr_[q] * rr_[q];
                 if constexpr (CS > 1) {
                     cg::cluster_group cl = cg::this_cluster();
                     if (kl == 0 && rank > 0) cl.map_shared_rank(c.zh_r, rank - 1)[r] = zz[q];
@@ -267,43 +274,60 @@ __global__ void __launch_bounds__(PCG_THREADS, 1)
     bool conv = converged(eta, rr2), bad = false, checked = false;
     while (true) {
         if (conv && exit_mode == 0 && !checked) {
-            // true residual gamma - S lambda with FP64 accumulation
-            __syncthreads();
+            // true residual gamma - S lambda, FP64 accumulation; lambda (FP64) enters as hi + lo floats
+            double t1[1] = {0.0};
+            double sl[PCG_RPT];
 #pragma unroll
-            for (int q = 0; q < PCG_RPT; ++q) {
-                const int i = tid + q * PCG_THREADS;
-                if (i < nloc) c.rv[i] = lam[q];
-            }
-            if constexpr (CS > 1) {
-                cg::cluster_group cl = cg::this_cluster();
+            for (int q = 0; q < PCG_RPT; ++q) sl[q] = 0.0;
+#pragma unroll
+            for (int part = 0; part < 2; ++part) {
+                __syncthreads();
+#pragma unroll
+                for (int q = 0; q < PCG_RPT; ++q) {
+                    const int i = tid + q * PCG_THREADS;
+                    if (i < nloc) {
+                        const float hi = (float)lam[q];
+                        c.pv[NS + i] = part == 0 ? hi : (float)(lam[q] - (double)hi);
+                    }
+                }
+                if constexpr (CS > 1) {
+                    cg::cluster_group cl = cg::this_cluster();
+#pragma unroll
+                    for (int q = 0; q < PCG_RPT; ++q) {
+                        const int i = tid + q * PCG_THREADS;
+                        if (i < nloc) {
+                            const int kl = i / NS, r = i - NS * kl;
+                            const float hi = (float)lam[q];
+                            const float v = part == 0 ? hi : (float)(lam[q] - (double)hi);
+                            if (kl == 0 && rank > 0) cl.map_shared_rank(c.lh_r, rank - 1)[r] = v;
+                            if (kl == kpc - 1 && rank < CS - 1) cl.map_shared_rank(c.lh_l, rank + 1)[r] = v;
+                        }
+                    }
+                    cl.sync();
+                } else {
+                    __syncthreads();
+                }
+                if (tid < NS) {
+                    c.pv[tid] = (k0 > 0) ? (CS > 1 ? c.lh_l[tid] : 0.f) : 0.f;
+                    c.pv[NS * (kpc + 1) + tid] = (k1 < N) ? (CS > 1 ? c.lh_r[tid] : 0.f) : 0.f;
+                }
+                __syncthreads();
 #pragma unroll
                 for (int q = 0; q < PCG_RPT; ++q) {
                     const int i = tid + q * PCG_THREADS;
                     if (i < nloc) {
                         const int kl = i / NS, r = i - NS * kl;
-                        if (kl == 0 && rank > 0) cl.map_shared_rank(c.lh_r, rank - 1)[r] = lam[q];
-                        if (kl == kpc - 1 && rank < CS - 1) cl.map_shared_rank(c.lh_l, rank + 1)[r] = lam[q];
+                        sl[q] += schur_row<double>(c.Sp, c.left_next, c.pv, kl, r, k0 + kl, N, kpc);
                     }
                 }
-                cl.sync();
-            } else {
-                __syncthreads();
+                if constexpr (CS > 1) cg::this_cluster().sync();  // halos are rewritten by the next part
             }
-            // assemble lambda with halos in pv (p no longer needed unless we restart, which rebuilds it)
-            for (int i = tid; i < nloc; i += PCG_THREADS) c.pv[NS + i] = c.rv[i];
-            if (tid < NS) {
-                c.pv[tid] = (k0 > 0) ? (CS > 1 ? c.lh_l[tid] : 0.f) : 0.f;
-                c.pv[NS * (kpc + 1) + tid] = (k1 < N) ? (CS > 1 ? c.lh_r[tid] : 0.f) : 0.f;
-            }
-            __syncthreads();
-            double t1[1] = {0.0};
 #pragma unroll
             for (int q = 0; q < PCG_RPT; ++q) {
                 const int i = tid + q * PCG_THREADS;
                 if (i < nloc) {
-                    const int kl = i / NS, r = i - NS * kl;
-                    const double tr = (double)gv[q] - schur_row<double>(c.Sp, c.left_next, c.pv, kl, r, k0 + kl, N, kpc);
-                    rr_[q] = (float)tr;
+                    const double tr = (double)gv[q] - sl[q];
+                    rr_[q] = tr;
                     t1[0] += tr * tr;
                 }
             }
@@ -324,14 +348,14 @@ __global__ void __launch_bounds__(PCG_THREADS, 1)
         if (conv || it >= max_iter) break;
         // v = S p
         double d1[1] = {0.0};
-        float vv[PCG_RPT];
+        double vv[PCG_RPT];
 #pragma unroll
         for (int q = 0; q < PCG_RPT; ++q) {
             const int i = tid + q * PCG_THREADS;
-            vv[q] = 0.f;
+            vv[q] = 0.0;
             if (i < nloc) {
                 const int kl = i / NS, r = i - NS * kl;
-                vv[q] = schur_row<float>(c.Sp, c.left_next, c.pv, kl, r, k0 + kl, N, kpc);
+                vv[q] = schur_row<double>(c.Sp, c.left_next, c.pv, kl, r, k0 + kl, N, kpc);
                 d1[0] += (double)pp[q] * vv[q];
             }
         }
@@ -343,14 +367,13 @@ __global__ void __launch_bounds__(PCG_THREADS, 1)
             conv = false;
             break;
         }
-        const float alpha = (float)alpha_d;
 #pragma unroll
         for (int q = 0; q < PCG_RPT; ++q) {
             const int i = tid + q * PCG_THREADS;
             if (i < nloc) {
-                lam[q] = fmaf(alpha, pp[q], lam[q]);
-                rr_[q] = fmaf(-alpha, vv[q], rr_[q]);
-                c.rv[i] = rr_[q];
+                lam[q] = fma(alpha_d, (double)pp[q], lam[q]);
+                rr_[q] = fma(-alpha_d, vv[q], rr_[q]);
+                c.rv[i] = (float)rr_[q];
             }
         }
         __syncthreads();
@@ -361,8 +384,8 @@ __global__ void __launch_bounds__(PCG_THREADS, 1)
             if (i < nloc) {
                 const int kl = i / NS, r = i - NS * kl;
                 zz[q] = pinv_row(c.Sp, c.rv, kl, r);
-                d2[0] += (double)rr_[q] * zz[q];
-                d2[1] += (double)rr_[q] * rr_[q];
+                d2[0] += rr_[q] * (double)zz[q];
+                d2[1] += rr_[q] * rr_[q];
                 if constexpr (CS > 1) {
                     cg::cluster_group cl = cg::this_cluster();
                     if (kl == 0 && rank > 0) cl.map_shared_rank(c.zh_r, rank - 1)[r] = zz[q];
@@ -401,7 +424,10 @@ __global__ void __launch_bounds__(PCG_THREADS, 1)
 #pragma unroll
     for (int q = 0; q < PCG_RPT; ++q) {
         const int i = tid + q * PCG_THREADS;
-        if (i < nloc) lb[i] = lam[q];
+        if (i < nloc) {
+            lb[i] = (float)lam[q];
+            if (lambda64) lambda64[(size_t)NS * (kb + k0) + i] = lam[q];
+        }
     }
     if (tid == 0 && rank == 0) {
         const uint32_t maxit = conv ? 0u : 1u;
@@ -441,8 +467,8 @@ int pcg_pick_cluster(int maxN, int B, int num_sms, int requested)
 
 template <int CS, int FMT>
 static cudaError_t launch_pcg_cs(const BatchView &bv, int kpc_max, const float *S, const float *Pinv,
-                                 const float *gamma, float *lambda, int max_iter, float tol, int exit_mode,
-                                 uint32_t *out_iters, uint32_t *pcg_log, int log_stride, cudaStream_t s)
+                                 const float *gamma, float *lambda, double *lambda64, int max_iter, float tol,
+                                 int exit_mode, uint32_t *out_iters, uint32_t *pcg_log, int log_stride, cudaStream_t s)
 {
     auto kern = pcg_cluster_kernel<CS, FMT>;
     const size_t smem = pcg_cluster_smem_bytes(kpc_max);
@@ -468,14 +494,14 @@ static cudaError_t launch_pcg_cs(const BatchView &bv, int kpc_max, const float *
     attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, kern, bv, kpc_max, S, Pinv, gamma, lambda, max_iter, tol, exit_mode, out_iters,
-                              pcg_log, log_stride);
+    return cudaLaunchKernelEx(&cfg, kern, bv, kpc_max, S, Pinv, gamma, lambda, lambda64, max_iter, tol, exit_mode,
+                              out_iters, pcg_log, log_stride);
 }
 
 cudaError_t launch_pcg(const BatchView &bv, int max_n_knots, int min_n_knots, int fmt, const float *S,
-                       const float *Pinv, const float *gamma, float *lambda, int max_iter, float tol, int exit_mode,
-                       uint32_t *out_iters, uint32_t *pcg_log, int log_stride, int cluster_size, int num_sms,
-                       cudaStream_t s)
+                       const float *Pinv, const float *gamma, float *lambda, double *lambda64, int max_iter,
+                       float tol, int exit_mode, uint32_t *out_iters, uint32_t *pcg_log, int log_stride,
+                       int cluster_size, int num_sms, cudaStream_t s)
 {
     if (bv.B <= 0) return cudaSuccess;
     if (max_n_knots > MAX_PCG_KNOTS) return cudaErrorInvalidValue;
@@ -485,10 +511,10 @@ cudaError_t launch_pcg(const BatchView &bv, int max_n_knots, int min_n_knots, in
     if (kpc_max > PCG_KPC_MAX) return cudaErrorInvalidValue;
 #define GPT_PCG_CASE(CSV)                                                                                      \
     case CSV:                                                                                                  \
-        return fmt ? launch_pcg_cs<CSV, 1>(bv, kpc_max, S, Pinv, gamma, lambda, max_iter, tol, exit_mode,      \
-                                           out_iters, pcg_log, log_stride, s)                                  \
-                   : launch_pcg_cs<CSV, 0>(bv, kpc_max, S, Pinv, gamma, lambda, max_iter, tol, exit_mode,      \
-                                           out_iters, pcg_log, log_stride, s);
+        return fmt ? launch_pcg_cs<CSV, 1>(bv, kpc_max, S, Pinv, gamma, lambda, lambda64, max_iter, tol,       \
+                                           exit_mode, out_iters, pcg_log, log_stride, s)                       \
+                   : launch_pcg_cs<CSV, 0>(bv, kpc_max, S, Pinv, gamma, lambda, lambda64, max_iter, tol,       \
+                                           exit_mode, out_iters, pcg_log, log_stride, s);
     switch (cs) {
         GPT_PCG_CASE(1)
         GPT_PCG_CASE(2)

@@ -150,10 +150,12 @@ gpt_status gpt_form_schur_csc(gpt_handle *h, uint32_t knot_points, float rho, co
 gpt_status gpt_prep_csr(uint32_t knot_points, int32_t *h_col_ptr, int32_t *h_row_ind);
 
 /* GPU-PCG pcg<T,STATE_SIZE,KNOT_POINTS> launch (toplevel.cuh:135-157,292-294):
- * solves S lambda = gamma from the warm start in d_lambda. */
+ * solves S lambda = gamma from the warm start in d_lambda (updated in place,
+ * FP32).  d_lambda64 (optional, 14N doubles) receives the FP64 iterate; at
+ * N >= ~64 only it can carry a relative residual near 1e-5. */
 gpt_status gpt_pcg(gpt_handle *h, uint32_t knot_points, const float *d_S, const float *d_Pinv,
-                   const float *d_gamma, float *d_lambda, uint32_t max_iter, float exit_tol, uint32_t exit_mode,
-                   uint32_t *h_iters, uint8_t *h_maxiter_exit, gpt_stream_t stream);
+                   const float *d_gamma, float *d_lambda, double *d_lambda64, uint32_t max_iter, float exit_tol,
+                   uint32_t exit_mode, uint32_t *h_iters, uint8_t *h_maxiter_exit, gpt_stream_t stream);
 
 /* compute_dz (schur.cuh:562-566, oldschur.cuh:966-1105) from Ginv */
 gpt_status gpt_compute_dz(gpt_handle *h, uint32_t knot_points, const float *d_Ginv, const float *d_C,

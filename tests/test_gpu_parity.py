@@ -150,14 +150,20 @@ def test_pcg_reaches_tolerance(gpt, oracle, golden, problem_mod, solvers, cluste
         S, Pv, gam = (x.astype(np.float32) for x in (S, Pv, gam))
         tol = 1e-5
         lam = torch.zeros(14 * N, device="cuda")
-        it, maxed = sv.pcg(N, dev(S), dev(Pv), dev(gam), lam, 20000, tol, 0)
-        relres = schur_residual(S, host(lam), gam.astype(np.float64), N)
+        lam64 = torch.zeros(14 * N, device="cuda", dtype=torch.float64)
+        it, maxed = sv.pcg(N, dev(S), dev(Pv), dev(gam), lam, 20000, tol, 0, lam64=lam64)
+        torch.cuda.synchronize()
+        l64 = lam64.cpu().numpy()
+        relres = schur_residual(S, l64, gam.astype(np.float64), N)
         assert not maxed, (kind, N, cluster, it, relres)
         # the kernel's FP64 true residual and this host evaluation agree to rounding
         assert relres <= 1.02 * tol, (kind, N, cluster, relres, it)
+        # the FP32 copy is the FP64 iterate rounded
+        np.testing.assert_array_equal(host(lam).astype(np.float32), l64.astype(np.float32))
+        # warm start from the FP32 copy: the FP32 rounding floor may need a few iterations, no more
         lam2 = lam.clone()
         it2, maxed2 = sv.pcg(N, dev(S), dev(Pv), dev(gam), lam2, 20000, tol, 0)
-        assert it2 == 0 and not maxed2, (kind, N, cluster, it2)
+        assert not maxed2 and it2 <= max(5, it // 10), (kind, N, cluster, it2, it)
         # eta-based exit (|r^T Pinv r| < tol) runs and stops
         lam3 = torch.zeros(14 * N, device="cuda")
         it3, maxed3 = sv.pcg(N, dev(S), dev(Pv), dev(gam), lam3, 20000, 1e-12 * float(np.abs(gam).max()) ** 2, 1)
@@ -179,8 +185,10 @@ def test_pcg_cluster_sizes_agree(gpt, oracle, problem_mod, solvers):
     for cs in (1, 2, 4, 8, 16):
         sv.set_solver(pcg_cluster_size=cs)
         lam = torch.zeros(14 * N, device="cuda")
-        sv.pcg(N, dev(S), dev(Pv), dev(gam), lam, 50000, 1e-5, 0)
-        sols[cs] = host(lam)
+        lam64 = torch.zeros(14 * N, device="cuda", dtype=torch.float64)
+        sv.pcg(N, dev(S), dev(Pv), dev(gam), lam, 50000, 1e-5, 0, lam64=lam64)
+        torch.cuda.synchronize()
+        sols[cs] = lam64.cpu().numpy()
     sv.set_solver(pcg_cluster_size=0)
     ref = np.linalg.norm(lam_star)
     errs = {cs: np.linalg.norm(v - lam_star) / ref for cs, v in sols.items()}
@@ -189,6 +197,9 @@ def test_pcg_cluster_sizes_agree(gpt, oracle, problem_mod, solvers):
 
 
 def test_compute_dz(gpt, oracle, golden, problem_mod, solvers):
+    """dz from lambda (FP32 inputs).  The right-hand sides cancel heavily, so the
+    bound is componentwise: |dz - dz64| <= 4e-6 * |Ginv| (|g| + |lambda_k| + |C|^T |lambda_{k+1}|)
+    (FP32 storage of the inputs, FP64 accumulation inside the kernel)."""
     for kind, N, cfg, p in problems(golden, problem_mod):
         sv = solvers(cfg)
         oG, oC, og, oc = oracle.form_kkt(oracle_params(oracle, cfg), N, p["xu"], p["goal"], p["xs"])
@@ -198,10 +209,22 @@ def test_compute_dz(gpt, oracle, golden, problem_mod, solvers):
         Gi = Gi.astype(np.float32).astype(np.float64)
         dz = torch.zeros(21 * N - 7, device="cuda")
         sv.compute_dz(N, dev(Gi), dev(f[1]), dev(f[2]), dev(lam), dz)
+        got = host(dz)
         want = oracle.compute_dz(N, Gi, f[1], f[2], lam)
+        bound = np.zeros(21 * N - 7)
         for k in range(N):
-            close(host(dz)[21 * k:21 * k + 14], want[21 * k:21 * k + 14], 1e-4, f"{kind} N={N} dz_x{k}",
-                  scale=np.abs(want).max())
+            Gq = np.abs(Gi[245 * k:245 * k + 196]).reshape(14, 14, order="F")
+            sx = np.abs(f[2][21 * k:21 * k + 14]) + np.abs(lam[14 * k:14 * k + 14])
+            if k < N - 1:
+                mA = np.abs(f[1][294 * k:294 * k + 196]).reshape(14, 14, order="F")
+                mB = np.abs(f[1][294 * k + 196:294 * k + 294]).reshape(14, 7, order="F")
+                ln = np.abs(lam[14 * (k + 1):14 * (k + 2)])
+                sx = sx + mA.T @ ln
+                Gr = np.abs(Gi[245 * k + 196:245 * k + 245]).reshape(7, 7, order="F")
+                bound[21 * k + 14:21 * k + 21] = Gr @ (np.abs(f[2][21 * k + 14:21 * k + 21]) + mB.T @ ln)
+            bound[21 * k:21 * k + 14] = Gq @ sx
+        err = np.abs(got - want)
+        assert (err <= 4e-6 * bound + 1e-12).all(), (kind, N, float((err / (bound + 1e-30)).max()))
 
 
 def test_merits(gpt, oracle, golden, problem_mod, solvers):
@@ -211,7 +234,10 @@ def test_merits(gpt, oracle, golden, problem_mod, solvers):
         m = torch.zeros(1, device="cuda")
         sv.compute_merit(N, dev(p["xu"]), dev(p["goal"]), m)
         want, _ = oracle.merit(par, N, p["xu"].astype(np.float64), None, 0.0, p["goal"], p["xs"], 0)
-        assert abs(host(m)[0] - want) <= 2e-5 * abs(want) + 1e-6, (kind, N, host(m)[0], want)
+        # cost terms: relative 2e-5; defect terms are differences of states: mu * 14 (N-1) * 2 eps32 |x|
+        xmax = max(1.0, float(np.abs(p["xu"]).max()))
+        dtol = 10.0 * 14 * (N - 1) * 2.4e-7 * xmax
+        assert abs(host(m)[0] - want) <= 2e-5 * abs(want) + dtol, (kind, N, host(m)[0], want)
         rng = np.random.default_rng(N)
         dz = (rng.normal(0, 0.05, 21 * N - 7)).astype(np.float32)
         xs = (p["xs"] + rng.normal(0, 0.01, 14)).astype(np.float32)
@@ -220,7 +246,7 @@ def test_merits(gpt, oracle, golden, problem_mod, solvers):
         got = host(ms)
         for a in range(8):
             w, _ = oracle.merit(par, N, p["xu"], dz, -1.0 / (1 << a), p["goal"], xs, 1)
-            assert abs(got[a] - w) <= 5e-5 * abs(w) + 1e-5, (kind, N, a, got[a], w)
+            assert abs(got[a] - w) <= 5e-5 * abs(w) + dtol + 1e-5, (kind, N, a, got[a], w)
 
 
 def test_sqp_first_iterate_matches_oracle(gpt, oracle, golden, problem_mod, solvers):
