@@ -250,14 +250,15 @@ def test_merits(gpt, oracle, golden, problem_mod, solvers):
 
 
 def test_sqp_first_iterate_matches_oracle(gpt, oracle, golden, problem_mod, solvers):
-    """One SQP iteration (KKT, Schur, PCG to 1e-7, dz, line search, step) vs the
-    oracle's iteration with the exact FP64 Cholesky solve: the new iterate xu
-    agrees to 1e-4 relative (per-iterate primal parity)."""
+    """One SQP iteration (KKT, Schur, PCG to relative residual 1e-10, dz, line
+    search, step) vs the oracle's iteration with the exact FP64 Cholesky solve:
+    the new iterate xu agrees to 1e-4 relative (per-iterate primal parity).  A
+    tight PCG tolerance is needed because cond(S) reaches 1e7 at these sizes."""
     for kind, N, cfg, p in problems(golden, problem_mod):
         if N > 64:
             continue
         sv = solvers(cfg)
-        sv.set_solver(sqp_max_iter=1, pcg_max_iter=20000, pcg_exit_tol=1e-7, pcg_exit_mode=0)
+        sv.set_solver(sqp_max_iter=1, pcg_max_iter=50000, pcg_exit_tol=1e-10, pcg_exit_mode=0)
         xu = dev(p["xu"])
         lam = dev(p["lam"])
         res = sv.sqp_solve(N, dev(p["goal"]), lam, xu, 1e-3)
@@ -294,7 +295,8 @@ def test_batched_equals_plain(gpt, problem_mod, solvers):
     Ns = [8, 16, 5, 32]
     batch = problem_mod.make_batch(Ns, seed0=11)
     sv = gpt.Solver(max_knot_points=64, max_batch=8, **SPEC_CFG)
-    sv.set_solver(sqp_max_iter=6, pcg_max_iter=500, pcg_exit_tol=1e-5)
+    # same CTA split for both calls, so the reductions run in the same order
+    sv.set_solver(sqp_max_iter=6, pcg_max_iter=500, pcg_exit_tol=1e-5, pcg_cluster_size=1)
     xu = dev(batch["xu"])
     lam = dev(batch["lam"])
     rho, stats = sv.sqp_solve_batched(Ns, dev(batch["goal"]), lam, xu, [1e-3] * len(Ns))
