@@ -9,22 +9,25 @@
 //
 // Layout: an instance's N knots are split into CS contiguous chunks, one per
 // CTA of a cluster (CS = 1..16).  Each CTA copies its chunk of the packed
-// Schur matrix (per knot: left block 196, lower triangle of the diagonal
-// block 105, lower triangle of the Pinv block 105, pad 2 = 408 floats) into
-// shared memory once and iterates on it: no global traffic inside the loop.
-// The right block of row k is the transpose of the left block of row k+1 (the
-// reference stores exactly that, oldschur.cuh:945-958), so only left blocks
-// are kept.  Neighbouring chunks exchange one knot of the search direction
-// through distributed shared memory; the two dot products per iteration are
-// reduced in FP64, in a fixed order, across the cluster with one cluster
-// barrier each.  No grid-wide synchronisation: clusters never wait on each
-// other.
+// Schur matrix (per knot: left block 196 column-major, lower triangle of the
+// diagonal block 105, lower triangle of the Pinv block 105, pad 2 = 408
+// floats) into shared memory once and iterates on it: no global traffic
+// inside the loop.  The right block of row k is the transpose of the left
+// block of row k+1 (the reference stores exactly that, oldschur.cuh:945-958),
+// so only left blocks are kept.  Thread (r, g) owns row r of knots g, g+TK,
+// g+2TK, g+3TK, so its triangle offsets are computed once and its rows give
+// independent accumulation chains.  Neighbouring chunks exchange one knot of
+// the search direction through distributed shared memory; the dot products
+// are reduced in FP64, in a fixed order, across the cluster with one cluster
+// barrier per reduction.  Clusters never wait on each other.
 //
-// Precision: S, Pinv, the search direction p and z = Pinv r are FP32; the
-// iterate lambda, the residual r, the products S p and every dot product are
-// FP64.  Exit test: mode 0 ||r||_2 <= tol ||gamma||_2 on the true residual
-// (recomputed with FP64 accumulation when the recursive residual passes; up
-// to two residual-replacement restarts); mode 1 |r^T Pinv r| < tol.
+// Precision: S, Pinv, the search direction p, z = Pinv r and the product S p
+// are FP32; the iterate lambda, the residual r and every dot product are
+// FP64.  Every RR_PERIOD iterations, and whenever the recursive residual
+// passes the exit test, r is replaced by the true residual gamma - S lambda
+// evaluated with FP64 accumulation (lambda split into two floats), so the
+// exit test always holds for the true residual.
+// Exit test: mode 0 ||r||_2 <= tol ||gamma||_2; mode 1 |r^T Pinv r| < tol.
 #include <cooperative_groups.h>
 
 #include "gpt_common.cuh"
@@ -35,32 +38,28 @@ namespace cg = cooperative_groups;
 namespace gpt {
 
 constexpr int PK_LEFT = 0, PK_DIAG = SS, PK_PINV = SS + 105;
-constexpr int PCG_THREADS = 512;
+constexpr int PCG_TK = 36;                       // knot groups per CTA
+constexpr int PCG_THREADS = 512;                 // 14 * 36 = 504 workers
+constexpr int PCG_WORKERS = NS * PCG_TK;
 constexpr int PCG_NWARP = PCG_THREADS / 32;
-constexpr int PCG_RPT = 4;  // rows per thread: 14 * PCG_KPC_MAX <= 512 * 4
-constexpr int PCG_MAX_RESTARTS = 2;
+constexpr int PCG_KPT = (PCG_KPC_MAX + PCG_TK - 1) / PCG_TK;  // knots per thread (4)
+constexpr int RR_PERIOD = 32;
 constexpr int SLOT_CS = 16;
-
-__device__ __forceinline__ int tri_idx(int r, int c)
-{
-    return r >= c ? ((r * (r + 1)) >> 1) + c : ((c * (c + 1)) >> 1) + r;
-}
 
 size_t pcg_cluster_smem_bytes(int kpc)
 {
-    return sizeof(float) * ((size_t)kpc * PK + SS + (size_t)NS * kpc + (size_t)NS * (kpc + 2) + 2 * NS + 2 * NS) +
+    return sizeof(float) * ((size_t)kpc * PK + SS + 2 * (size_t)NS * (kpc + 2) + 2 * NS) +
            sizeof(double) * (2 * SLOT_CS * 4 + PCG_NWARP * 4) + 16;
 }
 
-template <int CS>
 struct PcgCtx {
-    float *Sp, *left_next, *rv, *pv, *zh_l, *zh_r, *lh_l, *lh_r;
+    float *Sp, *left_next, *rv, *pv, *zh_l, *zh_r;
     double *slots, *red;
 };
 
 // Fixed-order reduction of NV doubles over the cluster; every thread gets the totals.
 template <int CS, int NV>
-__device__ __forceinline__ void cluster_sum(double (&v)[NV], const PcgCtx<CS> &c, int set)
+__device__ __forceinline__ void cluster_sum(double (&v)[NV], const PcgCtx &c, int set)
 {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
@@ -106,40 +105,77 @@ __device__ __forceinline__ void cluster_sum(double (&v)[NV], const PcgCtx<CS> &c
     }
 }
 
-// One row of S x with x in pv (halo knot at local index 0 and kpc+1); FP32 or FP64 accumulation.
-template <typename ACC>
-__device__ __forceinline__ ACC schur_row(const float *Sp, const float *left_next, const float *x, int kl, int r, int k,
-                                         int N, int kpc)
-{
-    const float *blk = Sp + (size_t)kl * PK;
-    ACC a = 0;
-    if (k > 0) {
-        const float *xp = x + kl * NS;
-#pragma unroll
-        for (int cc = 0; cc < NS; ++cc) a += (ACC)blk[PK_LEFT + r + NS * cc] * (ACC)xp[cc];
-    }
+// Triangle offsets of row r: element (r, c) of a packed lower triangle.
+struct RowOffsets {
+    int o[NS];
+    __device__ __forceinline__ explicit RowOffsets(int r)
     {
-        const float *xk = x + (kl + 1) * NS;
 #pragma unroll
-        for (int cc = 0; cc < NS; ++cc) a += (ACC)blk[PK_DIAG + tri_idx(r, cc)] * (ACC)xk[cc];
+        for (int cc = 0; cc < NS; ++cc) o[cc] = (cc <= r) ? ((r * (r + 1)) >> 1) + cc : ((cc * (cc + 1)) >> 1) + r;
     }
-    if (k < N - 1) {
-        const float *ln = (kl + 1 < kpc) ? blk + PK : left_next;
-        const float *xn = x + (kl + 2) * NS;
+};
+
+__device__ __forceinline__ float2 lds2(const float *p) { return *reinterpret_cast<const float2 *>(p); }
+
+// Row r of (S x)_k, FP32; x points at knot k-1's block of a halo-padded vector.
+__device__ __forceinline__ float schur_row_f32(const float *blk, const float *ln, const float *x, const RowOffsets &ro,
+                                               int r, bool has_left, bool has_right)
+{
+    float a0 = 0.f, a1 = 0.f, a2 = 0.f;
+    if (has_left) {
 #pragma unroll
-        for (int cc = 0; cc < NS; ++cc) a += (ACC)ln[PK_LEFT + cc + NS * r] * (ACC)xn[cc];
+        for (int m = 0; m < NS / 2; ++m) {
+            const float2 xv = lds2(x + 2 * m);
+            a0 = fmaf(blk[PK_LEFT + r + NS * (2 * m)], xv.x, a0);
+            a0 = fmaf(blk[PK_LEFT + r + NS * (2 * m + 1)], xv.y, a0);
+        }
+    }
+#pragma unroll
+    for (int m = 0; m < NS / 2; ++m) {
+        const float2 xv = lds2(x + NS + 2 * m);
+        a1 = fmaf(blk[PK_DIAG + ro.o[2 * m]], xv.x, a1);
+        a1 = fmaf(blk[PK_DIAG + ro.o[2 * m + 1]], xv.y, a1);
+    }
+    if (has_right) {
+#pragma unroll
+        for (int m = 0; m < NS / 2; ++m) {
+            const float2 xv = lds2(x + 2 * NS + 2 * m);
+            const float2 lv = lds2(ln + PK_LEFT + NS * r + 2 * m);
+            a2 = fmaf(lv.x, xv.x, a2);
+            a2 = fmaf(lv.y, xv.y, a2);
+        }
+    }
+    return (a0 + a1) + a2;
+}
+
+// Same row with FP64 accumulation (used for the true residual).
+__device__ __forceinline__ double schur_row_f64(const float *blk, const float *ln, const float *x, const RowOffsets &ro,
+                                                int r, bool has_left, bool has_right)
+{
+    double a = 0.0;
+    if (has_left) {
+#pragma unroll
+        for (int cc = 0; cc < NS; ++cc) a = fma((double)blk[PK_LEFT + r + NS * cc], (double)x[cc], a);
+    }
+#pragma unroll
+    for (int cc = 0; cc < NS; ++cc) a = fma((double)blk[PK_DIAG + ro.o[cc]], (double)x[NS + cc], a);
+    if (has_right) {
+#pragma unroll
+        for (int cc = 0; cc < NS; ++cc) a = fma((double)ln[PK_LEFT + NS * r + cc], (double)x[2 * NS + cc], a);
     }
     return a;
 }
 
-__device__ __forceinline__ float pinv_row(const float *Sp, const float *rv, int kl, int r)
+__device__ __forceinline__ float pinv_row(const float *blk, const float *x, const RowOffsets &ro)
 {
-    const float *blk = Sp + (size_t)kl * PK + PK_PINV;
-    const float *x = rv + kl * NS;
-    float a = 0.f;
+    float a0 = 0.f, a1 = 0.f;
 #pragma unroll
-    for (int cc = 0; cc < NS; ++cc) a = fmaf(blk[tri_idx(r, cc)], x[cc], a);
-    return a;
+    for (int m = 0; m < NS / 2; ++m) {
+        const float2 xv = lds2(x + 2 * m);
+        a0 = fmaf(blk[PK_PINV + ro.o[2 * m]], xv.x, a0);
+        a1 = fmaf(blk[PK_PINV + ro.o[2 * m + 1]], xv.y, a1);
+    }
+    return a0 + a1;
 }
 
 // FMT 0: S, Pinv in the reference's 3-block layout (588 floats per knot, Pinv diag at +196)
@@ -153,16 +189,17 @@ __global__ void __launch_bounds__(PCG_THREADS, 1)
 {
     extern __shared__ float4 pcg_dyn_smem[];
     float *base = reinterpret_cast<float *>(pcg_dyn_smem);
-    PcgCtx<CS> c;
+    PcgCtx c;
     c.Sp = base;
     c.left_next = c.Sp + (size_t)kpc_max * PK;
-    c.rv = c.left_next + SS;
-    c.pv = c.rv + NS * kpc_max;
+    c.rv = c.left_next + SS;           // (kpc+2) x 14: residual copy / lambda parts, halo slots at both ends
+    c.pv = c.rv + NS * (kpc_max + 2);  // (kpc+2) x 14: search direction with halos
     c.zh_l = c.pv + NS * (kpc_max + 2);
     c.zh_r = c.zh_l + NS;
-    c.lh_l = c.zh_r + NS;
-    c.lh_r = c.lh_l + NS;
-    c.slots = reinterpret_cast<double *>(c.lh_r + NS + ((size_t)(c.lh_r + NS - base) & 1));
+    {
+        const size_t used = (size_t)(c.zh_r + NS - base);
+        c.slots = reinterpret_cast<double *>(base + used + (used & 1));
+    }
     c.red = c.slots + 2 * SLOT_CS * 4;
 
     const int tid = threadIdx.x;
@@ -171,23 +208,25 @@ __global__ void __launch_bounds__(PCG_THREADS, 1)
     if constexpr (CS > 1) rank = (int)cg::this_cluster().block_rank();
     if (b >= bv.B || !bv.active(b)) return;  // uniform over the cluster
     const int N = bv.N(b), kb = bv.off(b);
-    const int k0 = (rank * N) / CS, k1 = ((rank + 1) * N) / CS, kpc = k1 - k0, nloc = NS * kpc;
+    const int k0 = (rank * N) / CS, k1 = ((rank + 1) * N) / CS, kpc = k1 - k0;
+    // chunk size of the left neighbour (its right halo slot is kpc_left + 1)
+    const int kpc_left = (rank > 0) ? k0 - ((rank - 1) * N) / CS : 0;
 
-    // ---- stage the chunk of S / Pinv (packed) and left block of knot k1
+    // ---- stage the chunk of S / Pinv (packed) and the left block of knot k1
     if (FMT == 1) {
         const float4 *src = reinterpret_cast<const float4 *>(S + (size_t)(kb + k0) * PK);
         float4 *dst = reinterpret_cast<float4 *>(c.Sp);
         for (int i = tid; i < kpc * (PK / 4); i += PCG_THREADS) dst[i] = src[i];
-        for (int i = tid; i < SS; i += PCG_THREADS)
-            c.left_next[i] = (k1 < N) ? S[(size_t)(kb + k1) * PK + i] : 0.f;
+        for (int i = tid; i < SS; i += PCG_THREADS) c.left_next[i] = (k1 < N) ? S[(size_t)(kb + k1) * PK + i] : 0.f;
     } else {
         for (int e = tid; e < kpc * SS; e += PCG_THREADS) {
             const int kl = e / SS, w = e - SS * kl, r = w % NS, cc = w / NS;
             const size_t g = (size_t)S_STRIDE * (kb + k0 + kl);
             c.Sp[kl * PK + PK_LEFT + w] = S[g + w];
             if (r >= cc) {
-                c.Sp[kl * PK + PK_DIAG + tri_idx(r, cc)] = S[g + SS + w];
-                c.Sp[kl * PK + PK_PINV + tri_idx(r, cc)] = Pinv[g + SS + w];
+                const int t = ((r * (r + 1)) >> 1) + cc;
+                c.Sp[kl * PK + PK_DIAG + t] = S[g + SS + w];
+                c.Sp[kl * PK + PK_PINV + t] = Pinv[g + SS + w];
             }
         }
         for (int i = tid; i < SS; i += PCG_THREADS)
@@ -195,224 +234,192 @@ __global__ void __launch_bounds__(PCG_THREADS, 1)
     }
     const float *gb = gamma + (size_t)NS * (kb + k0);
     float *lb = lambda + (size_t)NS * (kb + k0);
-    // lambda (warm start) with halos from global memory
-    for (int i = tid; i < nloc; i += PCG_THREADS) c.pv[NS + i] = lb[i];
+    // warm start (FP32) with halos from global memory into rv
+    for (int i = tid; i < NS * kpc; i += PCG_THREADS) c.rv[NS + i] = lb[i];
     if (tid < NS) {
-        c.pv[tid] = (k0 > 0) ? lambda[(size_t)NS * (kb + k0 - 1) + tid] : 0.f;
-        c.pv[NS * (kpc + 1) + tid] = (k1 < N) ? lambda[(size_t)NS * (kb + k1) + tid] : 0.f;
+        c.rv[tid] = (k0 > 0) ? lambda[(size_t)NS * (kb + k0 - 1) + tid] : 0.f;
+        c.rv[NS * (kpc + 1) + tid] = (k1 < N) ? lambda[(size_t)NS * (kb + k1) + tid] : 0.f;
     }
     __syncthreads();
 
-    // lambda and the residual in FP64 (an FP32 lambda cannot represent a solution whose relative
-    // residual is below ~eps32 ||S|| ||lambda|| / ||gamma||, which exceeds 1e-5 at N = 128); the
-    // matrix, the preconditioned residual z and the search direction p stay FP32.
-    double lam[PCG_RPT], rr_[PCG_RPT];
-    float zz[PCG_RPT], pp[PCG_RPT], gv[PCG_RPT];
-    double acc[3] = {0.0, 0.0, 0.0};
+    // ---- per-thread rows: row r of local knots g0 + PCG_TK * j
+    const bool worker = tid < PCG_WORKERS;
+    const int r = worker ? tid % NS : 0, g0 = worker ? tid / NS : 0;
+    const RowOffsets ro(r);
+    double lam[PCG_KPT], res[PCG_KPT];
+    float pp[PCG_KPT], zz[PCG_KPT], gv[PCG_KPT];
+    bool own[PCG_KPT];
 #pragma unroll
-    for (int q = 0; q < PCG_RPT; ++q) {
-        const int i = tid + q * PCG_THREADS;
-        lam[q] = rr_[q] = 0.0;
-        zz[q] = pp[q] = gv[q] = 0.f;
-        if (i < nloc) {
-            const int kl = i / NS, r = i - NS * kl;
-            gv[q] = gb[i];
-            lam[q] = c.pv[NS + i];
-            rr_[q] = (double)gv[q] - schur_row<double>(c.Sp, c.left_next, c.pv, kl, r, k0 + kl, N, kpc);
-            acc[0] += (double)gv[q] * gv[q];
+    for (int j = 0; j < PCG_KPT; ++j) {
+        const int kl = g0 + PCG_TK * j;
+        own[j] = worker && kl < kpc;
+        lam[j] = res[j] = 0.0;
+        pp[j] = zz[j] = gv[j] = 0.f;
+        if (own[j]) {
+            gv[j] = gb[NS * kl + r];
+            lam[j] = (double)c.rv[NS * (kl + 1) + r];
+        }
+    }
+    auto row_f64 = [&](int j, const float *x) -> double {
+        const int kl = g0 + PCG_TK * j, k = k0 + kl;
+        const float *blk = c.Sp + (size_t)kl * PK;
+        const float *ln = (kl + 1 < kpc) ? blk + PK : c.left_next;
+        return schur_row_f64(blk, ln, x + NS * kl, ro, r, k > 0, k < N - 1);
+    };
+    // initial residual gamma - S lambda (lambda is FP32 here: one FP64 pass is exact to rounding)
+    double acc3[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+    for (int j = 0; j < PCG_KPT; ++j) {
+        if (own[j]) {
+            res[j] = (double)gv[j] - row_f64(j, c.rv);
+            acc3[0] += (double)gv[j] * gv[j];
         }
     }
     int set = 1;
-    double gg = 0.0, eta = 0.0, rr2 = 0.0;
-    int restarts = 0;
 
-    // r -> rv, z = Pinv r, p = z (+ halo exchange of z), eta/rr partials, cluster reduce
-    auto restart_direction = [&](bool with_gg) {
-        __syncthreads();
+    // true residual r = gamma - S lambda with lambda (FP64) split into hi + lo floats
+    auto replace_residual = [&]() {
 #pragma unroll
-        for (int q = 0; q < PCG_RPT; ++q) {
-            const int i = tid + q * PCG_THREADS;
-            if (i < nloc) c.rv[i] = (float)rr_[q];
+        for (int j = 0; j < PCG_KPT; ++j) res[j] = own[j] ? (double)gv[j] : 0.0;
+#pragma unroll
+        for (int part = 0; part < 2; ++part) {
+            __syncthreads();
+#pragma unroll
+            for (int j = 0; j < PCG_KPT; ++j) {
+                if (own[j]) {
+                    const int kl = g0 + PCG_TK * j;
+                    const float hi = (float)lam[j];
+                    const float v = part == 0 ? hi : (float)(lam[j] - (double)hi);
+                    c.rv[NS * (kl + 1) + r] = v;
+                    if constexpr (CS > 1) {
+                        // neighbours keep this CTA's boundary knots in their halo slots
+                        cg::cluster_group cl = cg::this_cluster();
+                        if (kl == 0 && rank > 0) cl.map_shared_rank(c.rv, rank - 1)[NS * (kpc_left + 1) + r] = v;
+                        if (kl == kpc - 1 && rank < CS - 1) cl.map_shared_rank(c.rv, rank + 1)[r] = v;
+                    }
+                }
+            }
+            if constexpr (CS > 1) {
+                cg::this_cluster().sync();
+            } else {
+                __syncthreads();
+            }
+#pragma unroll
+            for (int j = 0; j < PCG_KPT; ++j)
+                if (own[j]) res[j] -= row_f64(j, c.rv);
+            if constexpr (CS > 1) cg::this_cluster().sync();  // halos are rewritten by the next part
         }
+    };
+
+    // z = Pinv r from the FP32 copy of r; halo exchange of z; partial dot products
+    auto precond = [&](double (&d)[3]) {
         __syncthreads();
-        double a3[3] = {with_gg ? acc[0] : 0.0, 0.0, 0.0};
 #pragma unroll
-        for (int q = 0; q < PCG_RPT; ++q) {
-            const int i = tid + q * PCG_THREADS;
-            if (i < nloc) {
-                const int kl = i / NS, r = i - NS * kl;
-                zz[q] = pinv_row(c.Sp, c.rv, kl, r);
-                pp[q] = zz[q];
-                c.pv[NS + i] = pp[q];
-                a3[1] += rr_[q] * (double)zz[q];
-                a3[2] += rr_[q] * rr_[q];
+        for (int j = 0; j < PCG_KPT; ++j)
+            if (own[j]) c.rv[NS * (g0 + PCG_TK * j + 1) + r] = (float)res[j];
+        __syncthreads();
+#pragma unroll
+        for (int j = 0; j < PCG_KPT; ++j) {
+            if (own[j]) {
+                const int kl = g0 + PCG_TK * j;
+                zz[j] = pinv_row(c.Sp + (size_t)kl * PK, c.rv + NS * (kl + 1), ro);
+                d[1] += res[j] * (double)zz[j];
+                d[2] += res[j] * res[j];
                 if constexpr (CS > 1) {
                     cg::cluster_group cl = cg::this_cluster();
-                    if (kl == 0 && rank > 0) cl.map_shared_rank(c.zh_r, rank - 1)[r] = zz[q];
-                    if (kl == kpc - 1 && rank < CS - 1) cl.map_shared_rank(c.zh_l, rank + 1)[r] = zz[q];
+                    if (kl == 0 && rank > 0) cl.map_shared_rank(c.zh_r, rank - 1)[r] = zz[j];
+                    if (kl == kpc - 1 && rank < CS - 1) cl.map_shared_rank(c.zh_l, rank + 1)[r] = zz[j];
                 }
             }
         }
-        cluster_sum<CS, 3>(a3, c, set);
+    };
+
+    // ---- p = z
+    double eta, rr2, gg;
+    {
+        precond(acc3);
+        cluster_sum<CS, 3>(acc3, c, set);
         set ^= 1;
-        if (with_gg) gg = a3[0];
-        eta = a3[1];
-        rr2 = a3[2];
-        // p halos = z halos (zero outside the horizon)
+        gg = acc3[0];
+        eta = acc3[1];
+        rr2 = acc3[2];
+#pragma unroll
+        for (int j = 0; j < PCG_KPT; ++j) {
+            pp[j] = zz[j];
+            if (own[j]) c.pv[NS * (g0 + PCG_TK * j + 1) + r] = pp[j];
+        }
         if (tid < NS) {
             c.pv[tid] = (k0 > 0) ? c.zh_l[tid] : 0.f;
             c.pv[NS * (kpc + 1) + tid] = (k1 < N) ? c.zh_r[tid] : 0.f;
         }
         __syncthreads();
-    };
-    restart_direction(true);
-
+    }
     auto converged = [&](double e, double r2) {
         return exit_mode == 0 ? (r2 <= (double)tol * (double)tol * gg) : (fabs(e) < (double)tol);
     };
+    bool conv = converged(eta, rr2), bad = false;
     int it = 0;
-    bool conv = converged(eta, rr2), bad = false, checked = false;
-    while (true) {
-        if (conv && exit_mode == 0 && !checked) {
-            // true residual gamma - S lambda, FP64 accumulation; lambda (FP64) enters as hi + lo floats
-            double t1[1] = {0.0};
-            double sl[PCG_RPT];
-#pragma unroll
-            for (int q = 0; q < PCG_RPT; ++q) sl[q] = 0.0;
-#pragma unroll
-            for (int part = 0; part < 2; ++part) {
-                __syncthreads();
-#pragma unroll
-                for (int q = 0; q < PCG_RPT; ++q) {
-                    const int i = tid + q * PCG_THREADS;
-                    if (i < nloc) {
-                        const float hi = (float)lam[q];
-                        c.pv[NS + i] = part == 0 ? hi : (float)(lam[q] - (double)hi);
-                    }
-                }
-                if constexpr (CS > 1) {
-                    cg::cluster_group cl = cg::this_cluster();
-#pragma unroll
-                    for (int q = 0; q < PCG_RPT; ++q) {
-                        const int i = tid + q * PCG_THREADS;
-                        if (i < nloc) {
-                            const int kl = i / NS, r = i - NS * kl;
-                            const float hi = (float)lam[q];
-                            const float v = part == 0 ? hi : (float)(lam[q] - (double)hi);
-                            if (kl == 0 && rank > 0) cl.map_shared_rank(c.lh_r, rank - 1)[r] = v;
-                            if (kl == kpc - 1 && rank < CS - 1) cl.map_shared_rank(c.lh_l, rank + 1)[r] = v;
-                        }
-                    }
-                    cl.sync();
-                } else {
-                    __syncthreads();
-                }
-                if (tid < NS) {
-                    c.pv[tid] = (k0 > 0) ? (CS > 1 ? c.lh_l[tid] : 0.f) : 0.f;
-                    c.pv[NS * (kpc + 1) + tid] = (k1 < N) ? (CS > 1 ? c.lh_r[tid] : 0.f) : 0.f;
-                }
-                __syncthreads();
-#pragma unroll
-                for (int q = 0; q < PCG_RPT; ++q) {
-                    const int i = tid + q * PCG_THREADS;
-                    if (i < nloc) {
-                        const int kl = i / NS, r = i - NS * kl;
-                        sl[q] += schur_row<double>(c.Sp, c.left_next, c.pv, kl, r, k0 + kl, N, kpc);
-                    }
-                }
-                if constexpr (CS > 1) cg::this_cluster().sync();  // halos are rewritten by the next part
-            }
-#pragma unroll
-            for (int q = 0; q < PCG_RPT; ++q) {
-                const int i = tid + q * PCG_THREADS;
-                if (i < nloc) {
-                    const double tr = (double)gv[q] - sl[q];
-                    rr_[q] = tr;
-                    t1[0] += tr * tr;
-                }
-            }
-            cluster_sum<CS, 1>(t1, c, set);
-            set ^= 1;
-            if (t1[0] <= (double)tol * (double)tol * gg) break;  // converged on the true residual
-            if (restarts >= PCG_MAX_RESTARTS || it >= max_iter) {
-                conv = false;
-                break;
-            }
-            ++restarts;
-            restart_direction(false);
-            conv = converged(eta, rr2);
-            checked = conv;  // a restart that is already below tol on the true residual stops next round
-            if (conv) break;
-            continue;
-        }
-        if (conv || it >= max_iter) break;
-        // v = S p
+    while (!conv && it < max_iter) {
+        // v = S p (FP32), pAp (FP64)
         double d1[1] = {0.0};
-        double vv[PCG_RPT];
+        float vv[PCG_KPT];
 #pragma unroll
-        for (int q = 0; q < PCG_RPT; ++q) {
-            const int i = tid + q * PCG_THREADS;
-            vv[q] = 0.0;
-            if (i < nloc) {
-                const int kl = i / NS, r = i - NS * kl;
-                vv[q] = schur_row<double>(c.Sp, c.left_next, c.pv, kl, r, k0 + kl, N, kpc);
-                d1[0] += (double)pp[q] * vv[q];
+        for (int j = 0; j < PCG_KPT; ++j) {
+            vv[j] = 0.f;
+            if (own[j]) {
+                const int kl = g0 + PCG_TK * j, k = k0 + kl;
+                const float *blk = c.Sp + (size_t)kl * PK;
+                const float *ln = (kl + 1 < kpc) ? blk + PK : c.left_next;
+                vv[j] = schur_row_f32(blk, ln, c.pv + NS * kl, ro, r, k > 0, k < N - 1);
+                d1[0] += (double)pp[j] * (double)vv[j];
             }
         }
         cluster_sum<CS, 1>(d1, c, set);
         set ^= 1;
-        const double alpha_d = eta / d1[0];
-        if (!isfinite(alpha_d)) {
+        const double alpha = eta / d1[0];
+        if (!isfinite(alpha)) {
             bad = true;
-            conv = false;
             break;
         }
 #pragma unroll
-        for (int q = 0; q < PCG_RPT; ++q) {
-            const int i = tid + q * PCG_THREADS;
-            if (i < nloc) {
-                lam[q] = fma(alpha_d, (double)pp[q], lam[q]);
-                rr_[q] = fma(-alpha_d, vv[q], rr_[q]);
-                c.rv[i] = (float)rr_[q];
-            }
+        for (int j = 0; j < PCG_KPT; ++j) {
+            lam[j] = fma(alpha, (double)pp[j], lam[j]);
+            res[j] = fma(-alpha, (double)vv[j], res[j]);
         }
-        __syncthreads();
-        double d2[2] = {0.0, 0.0};
-#pragma unroll
-        for (int q = 0; q < PCG_RPT; ++q) {
-            const int i = tid + q * PCG_THREADS;
-            if (i < nloc) {
-                const int kl = i / NS, r = i - NS * kl;
-                zz[q] = pinv_row(c.Sp, c.rv, kl, r);
-                d2[0] += rr_[q] * (double)zz[q];
-                d2[1] += rr_[q] * rr_[q];
-                if constexpr (CS > 1) {
-                    cg::cluster_group cl = cg::this_cluster();
-                    if (kl == 0 && rank > 0) cl.map_shared_rank(c.zh_r, rank - 1)[r] = zz[q];
-                    if (kl == kpc - 1 && rank < CS - 1) cl.map_shared_rank(c.zh_l, rank + 1)[r] = zz[q];
-                }
-            }
-        }
-        cluster_sum<CS, 2>(d2, c, set);
-        set ^= 1;
         ++it;
-        if (!isfinite(d2[0])) {
+        bool replaced = false;
+        if (it % RR_PERIOD == 0) {
+            replace_residual();
+            replaced = true;
+        }
+        double d2[3] = {0.0, 0.0, 0.0};
+        precond(d2);
+        cluster_sum<CS, 3>(d2, c, set);
+        set ^= 1;
+        conv = converged(d2[1], d2[2]);
+        if (conv && exit_mode == 0 && !replaced) {
+            // confirm on the true residual
+            replace_residual();
+            double d3[3] = {0.0, 0.0, 0.0};
+            precond(d3);
+            cluster_sum<CS, 3>(d3, c, set);
+            set ^= 1;
+            d2[1] = d3[1];
+            d2[2] = d3[2];
+            conv = converged(d2[1], d2[2]);
+        }
+        if (!isfinite(d2[1])) {
             bad = true;
             conv = false;
             break;
         }
-        conv = converged(d2[0], d2[1]);
-        checked = false;
-        if (conv) continue;  // true-residual check at the top of the loop
-        const float beta = (float)(d2[0] / eta);
-        eta = d2[0];
+        if (conv) break;
+        const float beta = (float)(d2[1] / eta);
+        eta = d2[1];
 #pragma unroll
-        for (int q = 0; q < PCG_RPT; ++q) {
-            const int i = tid + q * PCG_THREADS;
-            if (i < nloc) {
-                pp[q] = fmaf(beta, pp[q], zz[q]);
-                c.pv[NS + i] = pp[q];
-            }
+        for (int j = 0; j < PCG_KPT; ++j) {
+            pp[j] = fmaf(beta, pp[j], zz[j]);
+            if (own[j]) c.pv[NS * (g0 + PCG_TK * j + 1) + r] = pp[j];
         }
         if (tid < NS) {
             // halo p = z_halo + beta p_halo (the neighbour's own update, done locally)
@@ -422,11 +429,11 @@ __global__ void __launch_bounds__(PCG_THREADS, 1)
         __syncthreads();
     }
 #pragma unroll
-    for (int q = 0; q < PCG_RPT; ++q) {
-        const int i = tid + q * PCG_THREADS;
-        if (i < nloc) {
-            lb[i] = (float)lam[q];
-            if (lambda64) lambda64[(size_t)NS * (kb + k0) + i] = lam[q];
+    for (int j = 0; j < PCG_KPT; ++j) {
+        if (own[j]) {
+            const int i = NS * (g0 + PCG_TK * j) + r;
+            lb[i] = (float)lam[j];
+            if (lambda64) lambda64[(size_t)NS * (kb + k0) + i] = lam[j];
         }
     }
     if (tid == 0 && rank == 0) {
