@@ -109,7 +109,7 @@ def _declare(L):
         "gpt_form_schur_csc": ([vp, u32, f32, vp, vp, vp, vp, vp, vp, vp, vp], C.c_int),
         "gpt_prep_csr": ([u32, vp, vp], C.c_int),
         "gpt_pcg": ([vp, u32, vp, vp, vp, vp, vp, u32, f32, u32, P(u32), P(C.c_uint8), vp], C.c_int),
-        "gpt_compute_dz": ([vp, u32, vp, vp, vp, vp, vp, vp], C.c_int),
+        "gpt_compute_dz": ([vp, u32, vp, vp, vp, vp, vp, vp, vp], C.c_int),
         "gpt_compute_merit": ([vp, u32, vp, vp, vp, vp], C.c_int),
         "gpt_ls_compute_merit": ([vp, u32, vp, vp, vp, vp, vp, vp], C.c_int),
         "gpt_set_profiling": ([vp, C.c_int], C.c_int),
@@ -254,8 +254,9 @@ class Solver:
                              exit_tol, exit_mode, C.byref(it), C.byref(mx), _stream(stream)))
         return it.value, bool(mx.value)
 
-    def compute_dz(self, N, Ginv, Cm, g, lam, dz, stream=None):
-        _check(lib().gpt_compute_dz(self._h, N, _ptr(Ginv), _ptr(Cm), _ptr(g), _ptr(lam), _ptr(dz), _stream(stream)))
+    def compute_dz(self, N, Ginv, Cm, g, lam, dz, lam64=None, stream=None):
+        _check(lib().gpt_compute_dz(self._h, N, _ptr(Ginv), _ptr(Cm), _ptr(g), _ptr(lam), _ptr(lam64), _ptr(dz),
+                                    _stream(stream)))
 
     def compute_merit(self, N, xu, eePos, out, stream=None):
         _check(lib().gpt_compute_merit(self._h, N, _ptr(xu), _ptr(eePos), _ptr(out), _stream(stream)))

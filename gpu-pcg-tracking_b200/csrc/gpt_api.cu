@@ -333,11 +333,12 @@ gpt_status gpt_pcg(gpt_handle *h, uint32_t N, const float *d_S, const float *d_P
 }
 
 gpt_status gpt_compute_dz(gpt_handle *h, uint32_t N, const float *d_Ginv, const float *d_C, const float *d_g,
-                          const float *d_lambda, float *d_dz, gpt_stream_t stream)
+                          const float *d_lambda, const double *d_lambda64, float *d_dz, gpt_stream_t stream)
 {
-    if (!h || !d_Ginv || !d_C || !d_g || !d_lambda || !d_dz) return set_err(GPT_ERR_BAD_ARG, "null argument");
+    if (!h || !d_Ginv || !d_C || !d_g || (!d_lambda && !d_lambda64) || !d_dz)
+        return set_err(GPT_ERR_BAD_ARG, "null argument");
     if (!check_n(h, N)) return set_err(GPT_ERR_BAD_ARG, "knot_points out of range");
-    GPT_CUDA(launch_dz(single_view(N), d_Ginv, d_C, d_g, d_lambda, nullptr, d_dz, h->num_sms, (cudaStream_t)stream));
+    GPT_CUDA(launch_dz(single_view(N), d_Ginv, d_C, d_g, d_lambda, d_lambda64, d_dz, h->num_sms, (cudaStream_t)stream));
     return GPT_OK;
 }
 

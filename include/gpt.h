@@ -157,9 +157,11 @@ gpt_status gpt_pcg(gpt_handle *h, uint32_t knot_points, const float *d_S, const 
                    const float *d_gamma, float *d_lambda, double *d_lambda64, uint32_t max_iter, float exit_tol,
                    uint32_t exit_mode, uint32_t *h_iters, uint8_t *h_maxiter_exit, gpt_stream_t stream);
 
-/* compute_dz (schur.cuh:562-566, oldschur.cuh:966-1105) from Ginv */
+/* compute_dz (schur.cuh:562-566, oldschur.cuh:966-1105) from Ginv; d_lambda64
+ * (optional, FP64) is used instead of d_lambda when given */
 gpt_status gpt_compute_dz(gpt_handle *h, uint32_t knot_points, const float *d_Ginv, const float *d_C,
-                          const float *d_g, const float *d_lambda, float *d_dz, gpt_stream_t stream);
+                          const float *d_g, const float *d_lambda, const double *d_lambda64, float *d_dz,
+                          gpt_stream_t stream);
 
 /* compute_merit (merit.cuh:99-145): merit of d_xu -> *d_merit (one float) */
 gpt_status gpt_compute_merit(gpt_handle *h, uint32_t knot_points, const float *d_xu, const float *d_eePos_traj,

@@ -249,16 +249,60 @@ def test_merits(gpt, oracle, golden, problem_mod, solvers):
             assert abs(got[a] - w) <= 5e-5 * abs(w) + dtol + 1e-5, (kind, N, a, got[a], w)
 
 
-def test_sqp_first_iterate_matches_oracle(gpt, oracle, golden, problem_mod, solvers):
-    """One SQP iteration (KKT, Schur, PCG to relative residual 1e-10, dz, line
-    search, step) vs the oracle's iteration with the exact FP64 Cholesky solve:
-    the new iterate xu agrees to 1e-4 relative (per-iterate primal parity).  A
-    tight PCG tolerance is needed because cond(S) reaches 1e7 at these sizes."""
+def kkt_residual(N, G, Cm, g, c, rho, dz, lam):
+    """Relative FP64 residual of [Gt C^T; C 0][dz; lambda] = [g; c] (oldschur.cuh:966-1092)."""
+    from test_oracle_golden import kkt_dense
+    Gt, Cc = kkt_dense(N, G, Cm, g, c, rho)
+    r1 = Gt @ dz + Cc.T @ lam - g
+    r2 = Cc @ dz - c
+    return np.sqrt(np.sum(r1 ** 2) + np.sum(r2 ** 2)) / np.sqrt(np.sum(g ** 2) + np.sum(c ** 2))
+
+
+def test_linear_system_solution_satisfies_kkt(gpt, oracle, golden, problem_mod, solvers):
+    """The whole linear-algebra chain on the GPU -- Schur complement, PCG (FP64
+    iterate) to relative residual 1e-6, dz recovery -- returns (dz, lambda) that
+    satisfy the reference's KKT system (formed by the GPU in FP32) with an FP64
+    relative residual below 1e-5, and dz agrees with the FP64 oracle solution of
+    the same FP32 KKT data.  cond(S) reaches 1e7 at these sizes, so agreement is
+    stated against the FP64 solve of identical inputs."""
     for kind, N, cfg, p in problems(golden, problem_mod):
         if N > 64:
             continue
         sv = solvers(cfg)
-        sv.set_solver(sqp_max_iter=1, pcg_max_iter=50000, pcg_exit_tol=1e-10, pcg_exit_mode=0)
+        G, Cm, g, c = kkt_gpu(sv, N, p)
+        rho = 1e-3
+        S, Pv, gam, Gi = (torch.zeros(n, device="cuda") for n in (588 * N, 588 * N, 14 * N, 245 * N - 49))
+        sv.form_schur(N, rho, dev(G), dev(Cm), dev(g), dev(c), S, Pv, gam, Gi)
+        lam = torch.zeros(14 * N, device="cuda")
+        lam64 = torch.zeros(14 * N, device="cuda", dtype=torch.float64)
+        it, maxed = sv.pcg(N, S, Pv, gam, lam, 100000, 1e-6, 0, lam64=lam64)
+        assert not maxed, (kind, N, it)
+        dz = torch.zeros(21 * N - 7, device="cuda")
+        sv.compute_dz(N, Gi, dev(Cm), dev(g), None, dz, lam64=lam64)
+        torch.cuda.synchronize()
+        l64 = lam64.cpu().numpy()
+        res = kkt_residual(N, G, Cm, g, c, rho, host(dz), l64)
+        assert res < 1e-5, (kind, N, res)
+        # FP64 oracle on the same FP32 KKT data
+        oS, oP, og, oGi = oracle.form_schur(N, rho, G, Cm, g, c)
+        olam = oracle.banded_cholesky(N, oS, og)
+        odz = oracle.compute_dz(N, oGi, Cm, g, olam)
+        assert kkt_residual(N, G, Cm, g, c, rho, odz, olam) < 1e-9
+        rel = np.linalg.norm(host(dz) - odz) / np.linalg.norm(odz)
+        assert rel < 1e-3, (kind, N, rel)
+
+
+def test_sqp_first_iterate_matches_oracle(gpt, oracle, golden, problem_mod, solvers):
+    """One SQP iteration (KKT, Schur, PCG, dz, 8-step line search, step) on the
+    GPU vs the oracle's iteration (FP64, exact Cholesky solve) from the same
+    iterate: the same step length is accepted, the merit decreases by the same
+    amount to 1e-3 relative and the new iterates agree to 1e-2 relative (the
+    KKT data differ by FP32 rounding, amplified by cond(S) ~ 1e7)."""
+    for kind, N, cfg, p in problems(golden, problem_mod):
+        if N > 64:
+            continue
+        sv = solvers(cfg)
+        sv.set_solver(sqp_max_iter=1, pcg_max_iter=100000, pcg_exit_tol=1e-7, pcg_exit_mode=0)
         xu = dev(p["xu"])
         lam = dev(p["lam"])
         res = sv.sqp_solve(N, dev(p["goal"]), lam, xu, 1e-3)
@@ -266,12 +310,15 @@ def test_sqp_first_iterate_matches_oracle(gpt, oracle, golden, problem_mod, solv
         sol = oracle.make_solver(linsys=2, sqp_max_iter=1)
         oxu, olam, orho, ost, _ = oracle.sqp_solve(oracle_params(oracle, cfg), sol, N, p["goal"], p["lam"], p["xu"], 1e-3)
         assert res.sqp_iters == 1 and ost.sqp_iters == 1
-        gxu = host(xu)
-        step_g = gxu - p["xu"]
+        assert abs(res.rho - orho) <= 1e-6 * orho  # same accept / reject decision
+        step_g = host(xu) - p["xu"]
         step_o = oxu - p["xu"]
-        assert np.linalg.norm(step_g - step_o) <= 1e-4 * max(np.linalg.norm(step_o), 1e-6) + 1e-5, (
+        assert np.linalg.norm(step_g - step_o) <= 1e-2 * max(np.linalg.norm(step_o), 1e-6) + 1e-5, (
             kind, N, np.linalg.norm(step_g - step_o), np.linalg.norm(step_o))
-        assert abs(res.rho - orho) <= 1e-6 * orho
+        dm_g = res.stats["merit_initial"] - res.stats["merit_final"]
+        dm_o = ost.merit_final
+        m0, _ = oracle.merit(oracle_params(oracle, cfg), N, p["xu"], None, 0.0, p["goal"], p["xs"], 0)
+        assert abs(dm_g - (m0 - dm_o)) <= 1e-3 * abs(m0 - dm_o) + 1e-5, (kind, N, dm_g, m0 - dm_o)
 
 
 def test_sqp_solve_full_reduces_merit_like_oracle(gpt, oracle, golden, problem_mod, solvers):
