@@ -52,6 +52,8 @@ def parse():
     ap.add_argument("--plain-solves", type=int, default=2)
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="bound of the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--pcg-cluster", type=int, default=0, help="CTAs per instance in the PCG (0 = library choice)")
+    ap.add_argument("--batched-only", action="store_true", help="skip the e2e and plain legs (profiling runs)")
     return ap.parse_args()
 
 
@@ -207,7 +209,7 @@ def main():
     batch = P.make_batch(Ns, seed0=rank * B, dt=SPEC["timestep"])
     sv = gpt.Solver(max_knot_points=N, max_batch=B, **SPEC)
     sv.set_solver(sqp_max_iter=args.sqp_max_iter, pcg_max_iter=args.pcg_max_iter, pcg_exit_tol=args.tol,
-                  pcg_exit_mode=0)
+                  pcg_exit_mode=0, pcg_cluster_size=args.pcg_cluster)
     stream = torch.cuda.current_stream()
     xu0 = torch.as_tensor(batch["xu"], device="cuda")
     goal = torch.as_tensor(batch["goal"], device="cuda")
@@ -256,6 +258,16 @@ def main():
         total_ms = float(t.item())
     ms_per_step = total_ms / args.steps
     value = world * B / (ms_per_step / 1000.0)
+
+    if args.batched_only:
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "value": world * B / (ms_per_step / 1000.0), "unit": "solves/s",
+                              "ms_per_step": ms_per_step, "phase_ms": {k: v[0] for k, v in phases.items()},
+                              "pcg_iters_per_solve": sum(x["pcg_iters_total"] for x in all_stats) / len(all_stats)}),
+                  flush=True)
+        if world > 1:
+            dist.destroy_process_group()
+        return
 
     # e2e through the public API: pinned host in, result out, every step
     h_xu = torch.as_tensor(batch["xu"]).pin_memory()
