@@ -48,7 +48,7 @@ class SolverConfig(C.Structure):
     """gpt_solver_config (include/gpt.h)."""
     _fields_ = [("sqp_max_iter", C.c_uint32), ("pcg_max_iter", C.c_uint32), ("pcg_exit_tol", C.c_float),
                 ("pcg_exit_mode", C.c_uint32), ("rho_factor", C.c_float), ("rho_max", C.c_float),
-                ("rho_min", C.c_float), ("pcg_cluster_size", C.c_uint32)]
+                ("rho_min", C.c_float), ("pcg_cluster_size", C.c_uint32), ("pcg_precond", C.c_uint32)]
 
 
 class SqpStats(C.Structure):

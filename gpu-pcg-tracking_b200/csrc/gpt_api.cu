@@ -92,6 +92,7 @@ SolverParams to_solver(const gpt_solver_config &sc)
     S.rho_max = sc.rho_max;
     S.rho_min = sc.rho_min;
     S.pcg_cluster_size = sc.pcg_cluster_size;
+    S.pcg_precond = sc.pcg_precond;
     return S;
 }
 BatchView single_view(uint32_t N)
@@ -143,6 +144,7 @@ void gpt_default_solver_config(gpt_solver_config *o)
     o->rho_max = 10.0f;
     o->rho_min = 1e-3f;
     o->pcg_cluster_size = 0;
+    o->pcg_precond = 0;
 }
 
 const char *gpt_last_error(void) { return g_last_error.c_str(); }
@@ -155,6 +157,7 @@ gpt_status gpt_set_solver_config(gpt_handle *h, const gpt_solver_config *sc)
     if (!(sc->rho_factor > 1.0f) || !(sc->rho_min > 0.0f)) return set_err(GPT_ERR_BAD_ARG, "rho schedule out of range");
     if (sc->pcg_cluster_size & (sc->pcg_cluster_size - 1) || sc->pcg_cluster_size > 16)
         return set_err(GPT_ERR_BAD_ARG, "pcg_cluster_size must be 0, 1, 2, 4, 8 or 16");
+    if (sc->pcg_precond > 1) return set_err(GPT_ERR_BAD_ARG, "pcg_precond must be 0 or 1");
     if (sc->sqp_max_iter > h->cap_sqp_iter) {
         // pcg log is sized at creation
         return set_err(GPT_ERR_CAPACITY, "sqp_max_iter larger than at creation");
@@ -322,7 +325,7 @@ gpt_status gpt_pcg(gpt_handle *h, uint32_t N, const float *d_S, const float *d_P
     if (!h || !d_S || !d_Pinv || !d_gamma || !d_lambda) return set_err(GPT_ERR_BAD_ARG, "null argument");
     if (!check_n(h, N) || exit_mode > 1) return set_err(GPT_ERR_BAD_ARG, "knot_points/exit_mode out of range");
     cudaStream_t s = (cudaStream_t)stream;
-    GPT_CUDA(launch_pcg(single_view(N), (int)N, (int)N, 0, d_S, d_Pinv, d_gamma, d_lambda, d_lambda64, (int)max_iter, tol,
+    GPT_CUDA(launch_pcg(single_view(N), (int)N, (int)N, 0, (int)h->sc.pcg_precond, d_S, d_Pinv, d_gamma, d_lambda, d_lambda64, (int)max_iter, tol,
                         (int)exit_mode, h->pcg_out, nullptr, 0, (int)h->sc.pcg_cluster_size, h->num_sms, s));
     GPT_CUDA(cudaMemcpyAsync(h->h_pcg_out, h->pcg_out, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
     GPT_CUDA(cudaStreamSynchronize(s));
@@ -475,7 +478,7 @@ static gpt_status sqp_run(gpt_handle *h, uint32_t B, const uint32_t *Ns, const f
         }
         {
             PhaseTimer t(h, s, GPT_PHASE_PCG);
-            GPT_CUDA(launch_pcg(bv, maxN, minN, 1, h->S, nullptr, h->gamma, d_lambda, h->lam64, (int)SP.pcg_max_iter, SP.pcg_tol,
+            GPT_CUDA(launch_pcg(bv, maxN, minN, 1, (int)SP.pcg_precond, h->S, nullptr, h->gamma, d_lambda, h->lam64, (int)SP.pcg_max_iter, SP.pcg_tol,
                                 (int)SP.pcg_exit_mode, nullptr, h->pcg_log, (int)SP.sqp_max_iter,
                                 (int)SP.pcg_cluster_size, ns, s));
         }

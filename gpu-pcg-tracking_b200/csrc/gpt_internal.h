@@ -19,6 +19,7 @@ struct SolverParams {
     uint32_t pcg_exit_mode;
     float rho_factor, rho_max, rho_min;
     uint32_t pcg_cluster_size;  // 0: chosen from N and the batch size
+    uint32_t pcg_precond;       // 0 block-Jacobi (reference), 1 chunk block-tridiagonal LDL^T
 };
 
 cudaError_t launch_kkt(const BatchView &bv, const ProblemParams &P, const float *xu, const float *goal,
@@ -29,7 +30,8 @@ cudaError_t launch_schur(int mode, const BatchView &bv, float rho_scalar, const 
 size_t pcg_cluster_smem_bytes(int kpc);
 int pcg_pick_cluster(int maxN, int B, int num_sms, int requested);
 // fmt 0: S and Pinv in the reference 3-block layout; fmt 1: packed rows (PK floats per knot) in S
-cudaError_t launch_pcg(const BatchView &bv, int max_n_knots, int min_n_knots, int fmt, const float *S,
+// precond 0: block-Jacobi with the given Pinv; 1: exact block-tridiagonal LDL^T of each CTA's chunk
+cudaError_t launch_pcg(const BatchView &bv, int max_n_knots, int min_n_knots, int fmt, int precond, const float *S,
                        const float *Pinv, const float *gamma, float *lambda, double *lambda64, int max_iter,
                        float tol, int exit_mode, uint32_t *out_iters, uint32_t *pcg_log, int log_stride,
                        int cluster_size, int num_sms, cudaStream_t s);

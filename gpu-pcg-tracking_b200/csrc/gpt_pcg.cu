@@ -59,33 +59,33 @@ struct PcgCtx {
 
 // Fixed-order reduction of NV doubles over the cluster; every thread gets the totals.
 template <int CS, int NV>
-__device__ __forceinline__ void cluster_sum(double (&v)[NV], const PcgCtx &c, int set)
+__device__ __forceinline__ void cluster_sum_raw(double (&v)[NV], double *slots, double *red, int set)
 {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
     for (int q = 0; q < NV; ++q) v[q] = warp_sum(v[q]);
     if (lane == 0) {
 #pragma unroll
-        for (int q = 0; q < NV; ++q) c.red[warp * 4 + q] = v[q];
+        for (int q = 0; q < NV; ++q) red[warp * 4 + q] = v[q];
     }
     __syncthreads();
     if (warp == 0) {
         double t[NV];
 #pragma unroll
         for (int q = 0; q < NV; ++q) {
-            t[q] = (lane < PCG_NWARP) ? c.red[lane * 4 + q] : 0.0;
+            t[q] = (lane < PCG_NWARP) ? red[lane * 4 + q] : 0.0;
             t[q] = warp_sum(t[q]);
         }
         if constexpr (CS == 1) {
             if (lane == 0) {
 #pragma unroll
-                for (int q = 0; q < NV; ++q) c.slots[(set * SLOT_CS) * 4 + q] = t[q];
+                for (int q = 0; q < NV; ++q) slots[(set * SLOT_CS) * 4 + q] = t[q];
             }
         } else {
             cg::cluster_group cl = cg::this_cluster();
             const int me = (int)cl.block_rank();
             if (lane < CS) {
-                double *dst = cl.map_shared_rank(c.slots, lane);
+                double *dst = cl.map_shared_rank(slots, lane);
 #pragma unroll
                 for (int q = 0; q < NV; ++q) dst[(set * SLOT_CS + me) * 4 + q] = t[q];
             }
@@ -100,9 +100,15 @@ __device__ __forceinline__ void cluster_sum(double (&v)[NV], const PcgCtx &c, in
     for (int q = 0; q < NV; ++q) {
         double s = 0.0;
 #pragma unroll
-        for (int src = 0; src < CS; ++src) s += c.slots[(set * SLOT_CS + src) * 4 + q];
+        for (int src = 0; src < CS; ++src) s += slots[(set * SLOT_CS + src) * 4 + q];
         v[q] = s;
     }
+}
+
+template <int CS, int NV>
+__device__ __forceinline__ void cluster_sum(double (&v)[NV], const PcgCtx &c, int set)
+{
+    cluster_sum_raw<CS, NV>(v, c.slots, c.red, set);
 }
 
 // Triangle offsets of row r: element (r, c) of a packed lower triangle.
@@ -458,6 +464,461 @@ __global__ void __launch_bounds__(PCG_THREADS, 1)
 }
 
 // ---------------------------------------------------------------------------
+// PCG with the chunk block-tridiagonal LDL^T preconditioner
+// ---------------------------------------------------------------------------
+//
+// M = -S is symmetric positive definite.  On each CTA's chunk of knots,
+// M_chunk = L D L^T with D_0 = M_00 and D_k = M_kk - M_{k,k-1} D_{k-1}^{-1}
+// M_{k,k-1}^T, where M_{k,k-1} = -left_k.  The factorisation runs once per
+// solve in FP64 (products by the whole CTA, each 14x14 inversion by one warp,
+// Gauss-Jordan with the augmented columns on the lanes) and keeps D_k^{-1} in
+// FP64 in shared memory (packed lower triangle).  The preconditioner solves
+// the chunk exactly: z = S_chunk^{-1} r = -x with
+//   forward   y_k = r_k + left_k w_{k-1},   w_k = D_k^{-1} y_k
+//   backward  x_{K-1} = w_{K-1},  x_k = w_k + D_k^{-1} left_{k+1}^T x_{k+1}
+// on one warp (two half-warps split each 14-term product), in FP64.  With one
+// CTA per instance the preconditioner is the inverse of S up to rounding and
+// the PCG stops after one or two iterations; with several CTAs the chunks are
+// coupled through the iterations.  Chunk size 1 reduces to the reference's
+// block-Jacobi preconditioner.  The diagonal blocks of S are read from global
+// memory (L2) by the matvec; the left blocks live in shared memory.
+
+constexpr int CH_SLOTS = 2 * SLOT_CS * 4;
+
+__host__ __device__ constexpr int chain_rv_doubles(int kpc) { return NS * (kpc + 2) > 2 * SS ? NS * (kpc + 2) : 2 * SS; }
+
+size_t pcg_chain_smem_bytes(int kpc)
+{
+    return sizeof(double) * ((size_t)kpc * 105 + (size_t)chain_rv_doubles(kpc) + CH_SLOTS + PCG_NWARP * 4) +
+           sizeof(float) * ((size_t)kpc * SS + SS + (size_t)NS * (kpc + 2) + 2 * NS);
+}
+
+__device__ __forceinline__ int tri_lo(int r, int c)  // packed lower-triangle index of (r, c), any order
+{
+    return r >= c ? ((r * (r + 1)) >> 1) + c : ((c * (c + 1)) >> 1) + r;
+}
+
+// element (r, c) of knot kg's diagonal Schur block (lower triangle used: exactly symmetric)
+template <int FMT>
+__device__ __forceinline__ size_t diag_off(size_t kg, int r, int c)
+{
+    const int hi = r >= c ? r : c, lo = r >= c ? c : r;
+    if (FMT == 1) return kg * PK + PK_DIAG + ((hi * (hi + 1)) >> 1) + lo;
+    return kg * S_STRIDE + SS + hi + NS * lo;
+}
+
+template <int CS, int FMT>
+__global__ void __launch_bounds__(PCG_THREADS, 1)
+    pcg_chain_kernel(BatchView bv, int kpc_max, const float *__restrict__ S, const float *__restrict__ gamma,
+                     float *__restrict__ lambda, double *__restrict__ lambda64, int max_iter, float tol,
+                     int exit_mode, uint32_t *__restrict__ out_iters, uint32_t *__restrict__ pcg_log,
+                     int log_stride)
+{
+    extern __shared__ float4 chain_dyn_smem[];
+    double *Dinv = reinterpret_cast<double *>(chain_dyn_smem);    // kpc_max x 105
+    double *rv = Dinv + (size_t)kpc_max * 105;                    // (kpc_max+2) x 14 (>= 392): vectors, scratch
+    double *slots = rv + chain_rv_doubles(kpc_max);
+    double *red = slots + CH_SLOTS;
+    float *left = reinterpret_cast<float *>(red + PCG_NWARP * 4);  // kpc_max x 196
+    float *left_next = left + (size_t)kpc_max * SS;
+    float *pv = left_next + SS;  // (kpc_max+2) x 14
+    float *zh_l = pv + NS * (kpc_max + 2);
+    float *zh_r = zh_l + NS;
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int b = blockIdx.x / CS;
+    int rank = 0;
+    if constexpr (CS > 1) rank = (int)cg::this_cluster().block_rank();
+    if (b >= bv.B || !bv.active(b)) return;  // uniform over the cluster
+    const int N = bv.N(b), kb = bv.off(b);
+    const int k0 = (rank * N) / CS, k1 = ((rank + 1) * N) / CS, kpc = k1 - k0;
+    const int kpc_left = (rank > 0) ? k0 - ((rank - 1) * N) / CS : 0;
+    const size_t kg0 = (size_t)kb + k0;
+
+    // ---- stage the left blocks of the chunk and of knot k1
+    {
+        const size_t stride = FMT == 1 ? PK : S_STRIDE;
+        for (int i = tid; i < kpc * (SS / 4); i += PCG_THREADS) {
+            const int kl = i / (SS / 4), e4 = i - kl * (SS / 4);
+            reinterpret_cast<float4 *>(left)[i] =
+                reinterpret_cast<const float4 *>(S + (kg0 + kl) * stride)[e4];
+        }
+        for (int i = tid; i < SS; i += PCG_THREADS) left_next[i] = (k1 < N) ? S[((size_t)kb + k1) * stride + i] : 0.f;
+    }
+    __syncthreads();
+
+    // ---- factorisation of the chunk: D_kl^{-1}, FP64
+    {
+        double *Tsc = rv, *Dsc = rv + SS;
+        const int ei = tid % NS, ej = tid / NS;  // column-major element (ei, ej) for tid < 196
+        float dnext = 0.f;
+        if (tid < SS) dnext = S[diag_off<FMT>(kg0, ei, ej)];
+        for (int kl = 0; kl < kpc; ++kl) {
+            double Dv = 0.0;
+            if (tid < SS) {
+                Dv = -(double)dnext;
+                if (kl + 1 < kpc) dnext = S[diag_off<FMT>(kg0 + kl + 1, ei, ej)];  // prefetch
+            }
+            if (kl > 0) {
+                const float *lk = left + (size_t)kl * SS;
+                const double *Dp = Dinv + (size_t)(kl - 1) * 105;
+                if (tid < SS) {
+                    double a = 0.0;
+#pragma unroll
+                    for (int t = 0; t < NS; ++t) a = fma((double)lk[ei + NS * t], Dp[tri_lo(t, ej)], a);
+                    Tsc[tid] = a;  // T = left_k D_{k-1}^{-1}
+                }
+                __syncthreads();
+                if (tid < SS) {
+                    double a = 0.0;
+#pragma unroll
+                    for (int t = 0; t < NS; ++t) a = fma(Tsc[ei + NS * t], (double)lk[ej + NS * t], a);
+                    Dv -= a;  // D_k = M_kk - left_k D_{k-1}^{-1} left_k^T
+                }
+            }
+            if (tid < SS) Dsc[tid] = Dv;
+            __syncthreads();
+            if (warp == 0) {
+                // Gauss-Jordan on [D | I]: lanes 0..13 hold D's columns, 14..27 the identity's
+                double col[NS];
+                const bool lft = lane < NS, rgt = lane >= NS && lane < 2 * NS;
+#pragma unroll
+                for (int r = 0; r < NS; ++r)
+                    col[r] = lft ? Dsc[r + NS * lane] : ((rgt && r == lane - NS) ? 1.0 : 0.0);
+#pragma unroll
+                for (int p = 0; p < NS; ++p) {
+                    double pc[NS];
+#pragma unroll
+                    for (int r = 0; r < NS; ++r) pc[r] = __shfl_sync(0xffffffffu, col[r], p);
+                    const double prow = col[p] / pc[p];
+#pragma unroll
+                    for (int r = 0; r < NS; ++r) col[r] = (r == p) ? prow : fma(-pc[r], prow, col[r]);
+                }
+                if (rgt) {
+                    const int cc = lane - NS;
+                    double *Dk = Dinv + (size_t)kl * 105;
+#pragma unroll
+                    for (int r = 0; r < NS; ++r)
+                        if (r >= cc) Dk[((r * (r + 1)) >> 1) + cc] = col[r];
+                }
+            }
+            __syncthreads();
+        }
+    }
+
+    // ---- per-thread rows
+    const bool worker = tid < PCG_WORKERS;
+    const int r = worker ? tid % NS : 0, g0 = worker ? tid / NS : 0;
+    size_t doff[NS];  // offsets of row r of the diagonal block within a knot block
+#pragma unroll
+    for (int cc = 0; cc < NS; ++cc) doff[cc] = diag_off<FMT>(0, r, cc);
+    const size_t kstride = FMT == 1 ? PK : S_STRIDE;
+    const float *gb = gamma + NS * kg0;
+    float *lb = lambda + NS * kg0;
+    double lam[PCG_KPT], res[PCG_KPT];
+    float pp[PCG_KPT], zz[PCG_KPT], gv[PCG_KPT];
+    bool own[PCG_KPT];
+#pragma unroll
+    for (int j = 0; j < PCG_KPT; ++j) {
+        const int kl = g0 + PCG_TK * j;
+        own[j] = worker && kl < kpc;
+        lam[j] = res[j] = 0.0;
+        pp[j] = zz[j] = gv[j] = 0.f;
+        if (own[j]) {
+            gv[j] = gb[NS * kl + r];
+            lam[j] = (double)lb[NS * kl + r];
+        }
+    }
+    // (S x)_row with FP64 accumulation; x holds 14 (kpc+2) doubles with halo slots
+    auto row_f64 = [&](int j, const double *x) -> double {
+        const int kl = g0 + PCG_TK * j, k = k0 + kl;
+        const float *lk = left + (size_t)kl * SS;
+        const float *dg = S + (kg0 + kl) * kstride;
+        const double *xk = x + NS * kl;
+        double a = 0.0;
+        if (k > 0) {
+#pragma unroll
+            for (int cc = 0; cc < NS; ++cc) a = fma((double)lk[r + NS * cc], xk[cc], a);
+        }
+#pragma unroll
+        for (int cc = 0; cc < NS; ++cc) a = fma((double)__ldg(dg + doff[cc]), xk[NS + cc], a);
+        if (k < N - 1) {
+            const float *ln = (kl + 1 < kpc) ? lk + SS : left_next;
+#pragma unroll
+            for (int cc = 0; cc < NS; ++cc) a = fma((double)ln[cc + NS * r], xk[2 * NS + cc], a);
+        }
+        return a;
+    };
+    // lambda (FP64) with halos into rv; then gamma - S lambda
+    auto true_residual = [&](bool from_global) {
+        __syncthreads();
+#pragma unroll
+        for (int j = 0; j < PCG_KPT; ++j) {
+            if (own[j]) {
+                const int kl = g0 + PCG_TK * j;
+                rv[NS * (kl + 1) + r] = lam[j];
+                if (!from_global) {
+                    if constexpr (CS > 1) {
+                        cg::cluster_group cl = cg::this_cluster();
+                        if (kl == 0 && rank > 0) cl.map_shared_rank(rv, rank - 1)[NS * (kpc_left + 1) + r] = lam[j];
+                        if (kl == kpc - 1 && rank < CS - 1) cl.map_shared_rank(rv, rank + 1)[r] = lam[j];
+                    }
+                }
+            }
+        }
+        if (from_global && tid < NS) {
+            rv[tid] = (k0 > 0) ? (double)lambda[NS * (kg0 - 1) + tid] : 0.0;
+            rv[NS * (kpc + 1) + tid] = (k1 < N) ? (double)lambda[NS * ((size_t)kb + k1) + tid] : 0.0;
+        }
+        if (!from_global && tid < NS) {
+            if (k0 == 0) rv[tid] = 0.0;
+            if (k1 == N) rv[NS * (kpc + 1) + tid] = 0.0;
+        }
+        if constexpr (CS > 1) {
+            if (!from_global) cg::this_cluster().sync();
+            else __syncthreads();
+        } else {
+            __syncthreads();
+        }
+#pragma unroll
+        for (int j = 0; j < PCG_KPT; ++j)
+            if (own[j]) res[j] = (double)gv[j] - row_f64(j, rv);
+        if constexpr (CS > 1) {
+            cg::this_cluster().sync();  // neighbours finished reading this CTA's halo slots
+        } else {
+            __syncthreads();
+        }
+    };
+    // exact chunk solve on warp 0, in place on rv (interior slots): rv <- M_chunk^{-1} rv
+    auto chain_solve = [&]() {
+        if (warp != 0) return;
+        const int rr = lane & 15, h = lane >> 4;
+        const int rc = rr < NS ? rr : NS - 1;
+        double wprev = 0.0;
+        for (int kl = 0; kl < kpc; ++kl) {
+            double y = rv[NS * (kl + 1) + rc];
+            if (kl > 0) {
+                const float *lk = left + (size_t)kl * SS;
+                double t = 0.0;
+#pragma unroll
+                for (int q = 0; q < 7; ++q) {
+                    const int cc = 7 * h + q;
+                    t = fma((double)lk[rc + NS * cc], __shfl_sync(0xffffffffu, wprev, cc), t);
+                }
+                t += __shfl_xor_sync(0xffffffffu, t, 16);
+                y += t;
+            }
+            const double *Dk = Dinv + (size_t)kl * 105;
+            double u = 0.0;
+#pragma unroll
+            for (int q = 0; q < 7; ++q) {
+                const int cc = 7 * h + q;
+                u = fma(Dk[tri_lo(rc, cc)], __shfl_sync(0xffffffffu, y, cc), u);
+            }
+            u += __shfl_xor_sync(0xffffffffu, u, 16);
+            if (rr < NS && h == 0) rv[NS * (kl + 1) + rr] = u;
+            wprev = u;
+        }
+        double xnext = wprev;
+        for (int kl = kpc - 2; kl >= 0; --kl) {
+            const float *ln = left + (size_t)(kl + 1) * SS;
+            double sv = 0.0;
+#pragma unroll
+            for (int q = 0; q < 7; ++q) {
+                const int cc = 7 * h + q;
+                sv = fma((double)ln[cc + NS * rc], __shfl_sync(0xffffffffu, xnext, cc), sv);
+            }
+            sv += __shfl_xor_sync(0xffffffffu, sv, 16);
+            const double *Dk = Dinv + (size_t)kl * 105;
+            double v = 0.0;
+#pragma unroll
+            for (int q = 0; q < 7; ++q) {
+                const int cc = 7 * h + q;
+                v = fma(Dk[tri_lo(rc, cc)], __shfl_sync(0xffffffffu, sv, cc), v);
+            }
+            v += __shfl_xor_sync(0xffffffffu, v, 16);
+            const double x = rv[NS * (kl + 1) + rc] + v;
+            if (rr < NS && h == 0) rv[NS * (kl + 1) + rr] = x;
+            xnext = x;
+        }
+    };
+    // z = S_chunk^{-1} r, halo exchange of z, partial dot products
+    auto precond = [&](double (&d)[3]) {
+        __syncthreads();
+#pragma unroll
+        for (int j = 0; j < PCG_KPT; ++j)
+            if (own[j]) rv[NS * (g0 + PCG_TK * j + 1) + r] = res[j];
+        __syncthreads();
+        chain_solve();
+        __syncthreads();
+#pragma unroll
+        for (int j = 0; j < PCG_KPT; ++j) {
+            if (own[j]) {
+                const int kl = g0 + PCG_TK * j;
+                zz[j] = (float)(-rv[NS * (kl + 1) + r]);
+                d[1] += res[j] * (double)zz[j];
+                d[2] += res[j] * res[j];
+                if constexpr (CS > 1) {
+                    cg::cluster_group cl = cg::this_cluster();
+                    if (kl == 0 && rank > 0) cl.map_shared_rank(zh_r, rank - 1)[r] = zz[j];
+                    if (kl == kpc - 1 && rank < CS - 1) cl.map_shared_rank(zh_l, rank + 1)[r] = zz[j];
+                }
+            }
+        }
+    };
+
+    // ---- initial residual (FP64, lambda FP32 from global with halos)
+    true_residual(true);
+    int set = 1;
+    double eta, rr2, gg;
+    {
+        double acc3[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+        for (int j = 0; j < PCG_KPT; ++j)
+            if (own[j]) acc3[0] += (double)gv[j] * gv[j];
+        precond(acc3);
+        cluster_sum_raw<CS, 3>(acc3, slots, red, set);
+        set ^= 1;
+        gg = acc3[0];
+        eta = acc3[1];
+        rr2 = acc3[2];
+#pragma unroll
+        for (int j = 0; j < PCG_KPT; ++j) {
+            pp[j] = zz[j];
+            if (own[j]) pv[NS * (g0 + PCG_TK * j + 1) + r] = pp[j];
+        }
+        if (tid < NS) {
+            pv[tid] = (k0 > 0) ? zh_l[tid] : 0.f;
+            pv[NS * (kpc + 1) + tid] = (k1 < N) ? zh_r[tid] : 0.f;
+        }
+        __syncthreads();
+    }
+    auto converged = [&](double e, double r2) {
+        return exit_mode == 0 ? (r2 <= (double)tol * (double)tol * gg) : (fabs(e) < (double)tol);
+    };
+    bool conv = converged(eta, rr2), bad = false;
+    int it = 0;
+    while (!conv && it < max_iter) {
+        double d1[1] = {0.0};
+        float vv[PCG_KPT];
+#pragma unroll
+        for (int j = 0; j < PCG_KPT; ++j) {
+            vv[j] = 0.f;
+            if (own[j]) {
+                const int kl = g0 + PCG_TK * j, k = k0 + kl;
+                const float *lk = left + (size_t)kl * SS;
+                const float *dg = S + (kg0 + kl) * kstride;
+                const float *xk = pv + NS * kl;
+                float a0 = 0.f, a1 = 0.f, a2 = 0.f;
+                if (k > 0) {
+#pragma unroll
+                    for (int m = 0; m < NS / 2; ++m) {
+                        const float2 xv = lds2(xk + 2 * m);
+                        a0 = fmaf(lk[r + NS * (2 * m)], xv.x, a0);
+                        a0 = fmaf(lk[r + NS * (2 * m + 1)], xv.y, a0);
+                    }
+                }
+#pragma unroll
+                for (int m = 0; m < NS / 2; ++m) {
+                    const float2 xv = lds2(xk + NS + 2 * m);
+                    a1 = fmaf(__ldg(dg + doff[2 * m]), xv.x, a1);
+                    a1 = fmaf(__ldg(dg + doff[2 * m + 1]), xv.y, a1);
+                }
+                if (k < N - 1) {
+                    const float *ln = (kl + 1 < kpc) ? lk + SS : left_next;
+#pragma unroll
+                    for (int m = 0; m < NS / 2; ++m) {
+                        const float2 xv = lds2(xk + 2 * NS + 2 * m);
+                        const float2 lv = lds2(ln + NS * r + 2 * m);
+                        a2 = fmaf(lv.x, xv.x, a2);
+                        a2 = fmaf(lv.y, xv.y, a2);
+                    }
+                }
+                vv[j] = (a0 + a1) + a2;
+                d1[0] += (double)pp[j] * (double)vv[j];
+            }
+        }
+        cluster_sum_raw<CS, 1>(d1, slots, red, set);
+        set ^= 1;
+        const double alpha = eta / d1[0];
+        if (!isfinite(alpha)) {
+            bad = true;
+            break;
+        }
+#pragma unroll
+        for (int j = 0; j < PCG_KPT; ++j) {
+            lam[j] = fma(alpha, (double)pp[j], lam[j]);
+            res[j] = fma(-alpha, (double)vv[j], res[j]);
+        }
+        ++it;
+        bool replaced = false;
+        if (it % RR_PERIOD == 0) {
+            true_residual(false);
+            replaced = true;
+        }
+        double d2[3] = {0.0, 0.0, 0.0};
+        precond(d2);
+        cluster_sum_raw<CS, 3>(d2, slots, red, set);
+        set ^= 1;
+        conv = converged(d2[1], d2[2]);
+        if (conv && exit_mode == 0 && !replaced) {
+            true_residual(false);
+            double d3[3] = {0.0, 0.0, 0.0};
+            precond(d3);
+            cluster_sum_raw<CS, 3>(d3, slots, red, set);
+            set ^= 1;
+            d2[1] = d3[1];
+            d2[2] = d3[2];
+            conv = converged(d2[1], d2[2]);
+        }
+        if (!isfinite(d2[1])) {
+            bad = true;
+            conv = false;
+            break;
+        }
+        if (conv) break;
+        const float beta = (float)(d2[1] / eta);
+        eta = d2[1];
+#pragma unroll
+        for (int j = 0; j < PCG_KPT; ++j) {
+            pp[j] = fmaf(beta, pp[j], zz[j]);
+            if (own[j]) pv[NS * (g0 + PCG_TK * j + 1) + r] = pp[j];
+        }
+        if (tid < NS) {
+            pv[tid] = (k0 > 0) ? fmaf(beta, pv[tid], zh_l[tid]) : 0.f;
+            pv[NS * (kpc + 1) + tid] = (k1 < N) ? fmaf(beta, pv[NS * (kpc + 1) + tid], zh_r[tid]) : 0.f;
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int j = 0; j < PCG_KPT; ++j) {
+        if (own[j]) {
+            const int i = NS * (g0 + PCG_TK * j) + r;
+            lb[i] = (float)lam[j];
+            if (lambda64) lambda64[NS * kg0 + i] = lam[j];
+        }
+    }
+    if (tid == 0 && rank == 0) {
+        const uint32_t maxit = conv ? 0u : 1u;
+        if (out_iters) {
+            out_iters[2 * b] = (uint32_t)it;
+            out_iters[2 * b + 1] = maxit | (bad ? 2u : 0u);
+        }
+        if (bv.st) {
+            InstState &s = bv.st[b];
+            s.last_pcg_iters = it;
+            s.last_pcg_exit = maxit;
+            s.pcg_iters_total += it;
+            s.pcg_maxiter_count += maxit;
+            if (bad) s.exit_flags |= 4u;
+            if (pcg_log && s.sqp_iters < (uint32_t)log_stride)
+                pcg_log[(size_t)b * log_stride + s.sqp_iters] = (uint32_t)it | (maxit << 31);
+        }
+    }
+    if constexpr (CS > 1) cg::this_cluster().sync();
+}
+
+// ---------------------------------------------------------------------------
 
 int pcg_pick_cluster(int maxN, int B, int num_sms, int requested)
 {
@@ -505,19 +966,58 @@ static cudaError_t launch_pcg_cs(const BatchView &bv, int kpc_max, const float *
                               out_iters, pcg_log, log_stride);
 }
 
-cudaError_t launch_pcg(const BatchView &bv, int max_n_knots, int min_n_knots, int fmt, const float *S,
+template <int CS, int FMT>
+static cudaError_t launch_pcg_chain_cs(const BatchView &bv, int kpc_max, const float *S, const float *gamma,
+                                       float *lambda, double *lambda64, int max_iter, float tol, int exit_mode,
+                                       uint32_t *out_iters, uint32_t *pcg_log, int log_stride, cudaStream_t s)
+{
+    auto kern = pcg_chain_kernel<CS, FMT>;
+    const size_t smem = pcg_chain_smem_bytes(kpc_max);
+    static size_t attr_smem = 0;
+    if (smem > attr_smem) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        if (CS > 8) {
+            e = cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+            if (e != cudaSuccess) return e;
+        }
+        attr_smem = smem;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)(bv.B * CS), 1, 1);
+    cfg.blockDim = dim3(PCG_THREADS, 1, 1);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = CS;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kern, bv, kpc_max, S, gamma, lambda, lambda64, max_iter, tol, exit_mode, out_iters,
+                              pcg_log, log_stride);
+}
+
+cudaError_t launch_pcg(const BatchView &bv, int max_n_knots, int min_n_knots, int fmt, int precond, const float *S,
                        const float *Pinv, const float *gamma, float *lambda, double *lambda64, int max_iter,
                        float tol, int exit_mode, uint32_t *out_iters, uint32_t *pcg_log, int log_stride,
                        int cluster_size, int num_sms, cudaStream_t s)
 {
     if (bv.B <= 0) return cudaSuccess;
     if (max_n_knots > MAX_PCG_KNOTS) return cudaErrorInvalidValue;
-    int cs = pcg_pick_cluster(max_n_knots, bv.B, num_sms, cluster_size);
+    int cs = (precond == 1 && cluster_size == 0) ? 1 : pcg_pick_cluster(max_n_knots, bv.B, num_sms, cluster_size);
+    while ((max_n_knots + cs - 1) / cs > PCG_KPC_MAX) cs *= 2;
     while (cs > 1 && cs > min_n_knots) cs /= 2;  // every CTA owns at least one knot
     const int kpc_max = (max_n_knots + cs - 1) / cs;
-    if (kpc_max > PCG_KPC_MAX) return cudaErrorInvalidValue;
+    if (kpc_max > PCG_KPC_MAX || cs > 16) return cudaErrorInvalidValue;
 #define GPT_PCG_CASE(CSV)                                                                                      \
     case CSV:                                                                                                  \
+        if (precond == 1)                                                                                      \
+            return fmt ? launch_pcg_chain_cs<CSV, 1>(bv, kpc_max, S, gamma, lambda, lambda64, max_iter, tol,   \
+                                                     exit_mode, out_iters, pcg_log, log_stride, s)             \
+                       : launch_pcg_chain_cs<CSV, 0>(bv, kpc_max, S, gamma, lambda, lambda64, max_iter, tol,   \
+                                                     exit_mode, out_iters, pcg_log, log_stride, s);            \
         return fmt ? launch_pcg_cs<CSV, 1>(bv, kpc_max, S, Pinv, gamma, lambda, lambda64, max_iter, tol,       \
                                            exit_mode, out_iters, pcg_log, log_stride, s)                       \
                    : launch_pcg_cs<CSV, 0>(bv, kpc_max, S, Pinv, gamma, lambda, lambda64, max_iter, tol,       \

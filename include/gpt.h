@@ -78,6 +78,8 @@ typedef struct gpt_solver_config {
     float rho_max;             /* RHO_MAX */
     float rho_min;             /* RHO_MIN */
     uint32_t pcg_cluster_size; /* CTAs per instance in the PCG (1,2,4,8,16); 0 = chosen by the library */
+    uint32_t pcg_precond;      /* 0: block-Jacobi Pinv (the reference's, oldschur.cuh:926-933);
+                                  1: exact block-tridiagonal LDL^T of each CTA's chunk of knots */
 } gpt_solver_config;
 
 /* One sqpSolve's outcome (the reference returns a tuple, toplevel.cuh:502) */

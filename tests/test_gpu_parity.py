@@ -135,16 +135,19 @@ def schur_residual(S, lam, gam, N):
     return np.linalg.norm(gam - Sl) / np.linalg.norm(gam)
 
 
+@pytest.mark.parametrize("precond", [0, 1])
 @pytest.mark.parametrize("cluster", [0, 1, 2, 4, 8, 16])
-def test_pcg_reaches_tolerance(gpt, oracle, golden, problem_mod, solvers, cluster):
+def test_pcg_reaches_tolerance(gpt, oracle, golden, problem_mod, solvers, cluster, precond):
     """Exit mode 0 stops on the TRUE relative residual (FP64-evaluated); the
     returned lambda satisfies ||gamma - S lambda|| <= tol ||gamma|| for every
-    cluster size (CTAs per instance); a warm start at the solution exits at once."""
+    cluster size (CTAs per instance) and both preconditioners (0: the
+    reference's block-Jacobi, 1: exact block-tridiagonal LDL^T per chunk); a
+    warm start at the solution needs at most a few iterations."""
     for kind, N, cfg, p in problems(golden, problem_mod):
         if cluster > N:
             continue
         sv = solvers(cfg)
-        sv.set_solver(pcg_cluster_size=cluster)
+        sv.set_solver(pcg_cluster_size=cluster, pcg_precond=precond)
         oG, oC, og, oc = oracle.form_kkt(oracle_params(oracle, cfg), N, p["xu"], p["goal"], p["xs"])
         S, Pv, gam, _ = oracle.form_schur(N, 1e-1, *(x.astype(np.float32) for x in (oG, oC, og, oc)))
         S, Pv, gam = (x.astype(np.float32) for x in (S, Pv, gam))
@@ -164,11 +167,14 @@ def test_pcg_reaches_tolerance(gpt, oracle, golden, problem_mod, solvers, cluste
         lam2 = lam.clone()
         it2, maxed2 = sv.pcg(N, dev(S), dev(Pv), dev(gam), lam2, 20000, tol, 0)
         assert not maxed2 and it2 <= max(5, it // 10), (kind, N, cluster, it2, it)
+        if precond == 1 and cluster in (0, 1):
+            # one chunk = the whole horizon: the preconditioner is the inverse up to rounding
+            assert it <= 4, (kind, N, it)
         # eta-based exit (|r^T Pinv r| < tol) runs and stops
         lam3 = torch.zeros(14 * N, device="cuda")
         it3, maxed3 = sv.pcg(N, dev(S), dev(Pv), dev(gam), lam3, 20000, 1e-12 * float(np.abs(gam).max()) ** 2, 1)
         assert it3 > 0
-        sv.set_solver(pcg_cluster_size=0)
+        sv.set_solver(pcg_cluster_size=0, pcg_precond=0)
 
 
 def test_pcg_cluster_sizes_agree(gpt, oracle, problem_mod, solvers):
@@ -374,3 +380,24 @@ def test_bad_arguments_are_rejected_without_launch(gpt, solvers):
         sv.pcg(600, t, t, t, t, 10, 1e-5)  # N above the handle's capacity
     with pytest.raises(ValueError):
         sv.form_kkt(4, t.cpu(), t, t, t, t, t, t)
+
+
+def test_sqp_solve_chain_preconditioner_matches_block_jacobi(gpt, problem_mod):
+    """Same SQP solve with both preconditioners (relative residual 1e-8): the
+    iterates agree to the PCG tolerance and the chain LDL^T needs far fewer
+    PCG iterations."""
+    N = 64
+    p = problem_mod.make_problem(N, 5, dt=0.01)
+    out = {}
+    for pre in (0, 1):
+        sv = gpt.Solver(max_knot_points=N, **SPEC_CFG)
+        sv.set_solver(sqp_max_iter=3, pcg_max_iter=50000, pcg_exit_tol=1e-8, pcg_precond=pre, pcg_cluster_size=1)
+        xu = dev(p["xu"])
+        r = sv.sqp_solve(N, dev(p["goal"]), dev(p["lam"]), xu, 1e-3)
+        out[pre] = (host(xu), r)
+        sv.close()
+    (x0, r0), (x1, r1) = out[0], out[1]
+    assert r0.sqp_iters == r1.sqp_iters and abs(r0.rho - r1.rho) <= 1e-6 * r0.rho
+    step = np.linalg.norm(x0 - p["xu"])
+    assert np.linalg.norm(x0 - x1) <= 1e-3 * step, (np.linalg.norm(x0 - x1), step)
+    assert sum(r1.pcg_iters) * 20 < sum(r0.pcg_iters), (r1.pcg_iters, r0.pcg_iters)
