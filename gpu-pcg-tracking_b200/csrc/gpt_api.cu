@@ -1,6 +1,7 @@
 // gpt_api.cu -- the C ABI (include/gpt.h): handle, preallocated workspace,
 // the reference's kernels as single-instance entry points, and the SQP loop
 // (toplevel.cuh:24-503) driven from the host with every decision on the device.
+#include <cstdint>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -324,6 +325,7 @@ gpt_status gpt_pcg(gpt_handle *h, uint32_t N, const float *d_S, const float *d_P
 {
     if (!h || !d_S || !d_Pinv || !d_gamma || !d_lambda) return set_err(GPT_ERR_BAD_ARG, "null argument");
     if (!check_n(h, N) || exit_mode > 1) return set_err(GPT_ERR_BAD_ARG, "knot_points/exit_mode out of range");
+    if (((uintptr_t)d_S & 15u) != 0) return set_err(GPT_ERR_BAD_ARG, "d_S must be 16-byte aligned");
     cudaStream_t s = (cudaStream_t)stream;
     GPT_CUDA(launch_pcg(single_view(N), (int)N, (int)N, 0, (int)h->sc.pcg_precond, d_S, d_Pinv, d_gamma, d_lambda, d_lambda64, (int)max_iter, tol,
                         (int)exit_mode, h->pcg_out, nullptr, 0, (int)h->sc.pcg_cluster_size, h->num_sms, s));

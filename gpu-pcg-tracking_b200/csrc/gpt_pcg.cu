@@ -486,11 +486,15 @@ __global__ void __launch_bounds__(PCG_THREADS, 1)
 constexpr int CH_SLOTS = 2 * SLOT_CS * 4;
 
 __host__ __device__ constexpr int chain_rv_doubles(int kpc) { return NS * (kpc + 2) > 2 * SS ? NS * (kpc + 2) : 2 * SS; }
+// doubles ahead of the float region, rounded up so the float region is 16-byte aligned
+__host__ __device__ constexpr int chain_double_words(int kpc)
+{
+    return ((kpc * 105 + chain_rv_doubles(kpc) + 2 * NS + CH_SLOTS + PCG_NWARP * 4) + 1) & ~1;
+}
 
 size_t pcg_chain_smem_bytes(int kpc)
 {
-    return sizeof(double) * ((size_t)kpc * 105 + (size_t)chain_rv_doubles(kpc) + CH_SLOTS + PCG_NWARP * 4) +
-           sizeof(float) * ((size_t)kpc * SS + SS + (size_t)NS * (kpc + 2) + 2 * NS);
+    return sizeof(double) * (size_t)chain_double_words(kpc) + sizeof(float) * ((size_t)kpc * SS + SS);
 }
 
 __device__ __forceinline__ int tri_lo(int r, int c)  // packed lower-triangle index of (r, c), any order
@@ -500,13 +504,17 @@ __device__ __forceinline__ int tri_lo(int r, int c)  // packed lower-triangle in
 
 // element (r, c) of knot kg's diagonal Schur block (lower triangle used: exactly symmetric)
 template <int FMT>
-__device__ __forceinline__ size_t diag_off(size_t kg, int r, int c)
+__device__ __forceinline__ int diag_off(int r, int c)
 {
     const int hi = r >= c ? r : c, lo = r >= c ? c : r;
-    if (FMT == 1) return kg * PK + PK_DIAG + ((hi * (hi + 1)) >> 1) + lo;
-    return kg * S_STRIDE + SS + hi + NS * lo;
+    if (FMT == 1) return PK_DIAG + ((hi * (hi + 1)) >> 1) + lo;
+    return SS + hi + NS * lo;
 }
 
+// Precision: with an exact preconditioner the search direction must not be
+// rounded to FP32 -- the rounding error of p is amplified by cond(S) (up to
+// ~4e7 here) -- so p, z, S p, lambda and r are all FP64; S and the left
+// blocks stay FP32 (their products are exact in FP64).
 template <int CS, int FMT>
 __global__ void __launch_bounds__(PCG_THREADS, 1)
     pcg_chain_kernel(BatchView bv, int kpc_max, const float *__restrict__ S, const float *__restrict__ gamma,
@@ -515,15 +523,14 @@ __global__ void __launch_bounds__(PCG_THREADS, 1)
                      int log_stride)
 {
     extern __shared__ float4 chain_dyn_smem[];
-    double *Dinv = reinterpret_cast<double *>(chain_dyn_smem);    // kpc_max x 105
-    double *rv = Dinv + (size_t)kpc_max * 105;                    // (kpc_max+2) x 14 (>= 392): vectors, scratch
-    double *slots = rv + chain_rv_doubles(kpc_max);
+    double *Dinv = reinterpret_cast<double *>(chain_dyn_smem);  // kpc_max x 105
+    double *rv = Dinv + (size_t)kpc_max * 105;                  // 14 (kpc_max+2) (>= 392): p / r / chain / lambda
+    double *zh_l = rv + chain_rv_doubles(kpc_max);
+    double *zh_r = zh_l + NS;
+    double *slots = zh_r + NS;
     double *red = slots + CH_SLOTS;
-    float *left = reinterpret_cast<float *>(red + PCG_NWARP * 4);  // kpc_max x 196
+    float *left = reinterpret_cast<float *>(reinterpret_cast<double *>(chain_dyn_smem) + chain_double_words(kpc_max));
     float *left_next = left + (size_t)kpc_max * SS;
-    float *pv = left_next + SS;  // (kpc_max+2) x 14
-    float *zh_l = pv + NS * (kpc_max + 2);
-    float *zh_r = zh_l + NS;
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int b = blockIdx.x / CS;
@@ -534,17 +541,14 @@ __global__ void __launch_bounds__(PCG_THREADS, 1)
     const int k0 = (rank * N) / CS, k1 = ((rank + 1) * N) / CS, kpc = k1 - k0;
     const int kpc_left = (rank > 0) ? k0 - ((rank - 1) * N) / CS : 0;
     const size_t kg0 = (size_t)kb + k0;
+    const size_t kstride = FMT == 1 ? PK : S_STRIDE;
 
-    // ---- stage the left blocks of the chunk and of knot k1
-    {
-        const size_t stride = FMT == 1 ? PK : S_STRIDE;
-        for (int i = tid; i < kpc * (SS / 4); i += PCG_THREADS) {
-            const int kl = i / (SS / 4), e4 = i - kl * (SS / 4);
-            reinterpret_cast<float4 *>(left)[i] =
-                reinterpret_cast<const float4 *>(S + (kg0 + kl) * stride)[e4];
-        }
-        for (int i = tid; i < SS; i += PCG_THREADS) left_next[i] = (k1 < N) ? S[((size_t)kb + k1) * stride + i] : 0.f;
+    // ---- stage the left blocks of the chunk and of knot k1 (rows are 16-byte aligned: 196 floats)
+    for (int i = tid; i < kpc * (SS / 4); i += PCG_THREADS) {
+        const int kl = i / (SS / 4), e4 = i - kl * (SS / 4);
+        reinterpret_cast<float4 *>(left)[i] = reinterpret_cast<const float4 *>(S + (kg0 + kl) * kstride)[e4];
     }
+    for (int i = tid; i < SS; i += PCG_THREADS) left_next[i] = (k1 < N) ? S[((size_t)kb + k1) * kstride + i] : 0.f;
     __syncthreads();
 
     // ---- factorisation of the chunk: D_kl^{-1}, FP64
@@ -552,12 +556,12 @@ __global__ void __launch_bounds__(PCG_THREADS, 1)
         double *Tsc = rv, *Dsc = rv + SS;
         const int ei = tid % NS, ej = tid / NS;  // column-major element (ei, ej) for tid < 196
         float dnext = 0.f;
-        if (tid < SS) dnext = S[diag_off<FMT>(kg0, ei, ej)];
+        if (tid < SS) dnext = S[kg0 * kstride + diag_off<FMT>(ei, ej)];
         for (int kl = 0; kl < kpc; ++kl) {
             double Dv = 0.0;
             if (tid < SS) {
                 Dv = -(double)dnext;
-                if (kl + 1 < kpc) dnext = S[diag_off<FMT>(kg0 + kl + 1, ei, ej)];  // prefetch
+                if (kl + 1 < kpc) dnext = S[(kg0 + kl + 1) * kstride + diag_off<FMT>(ei, ej)];  // prefetch
             }
             if (kl > 0) {
                 const float *lk = left + (size_t)kl * SS;
@@ -609,85 +613,91 @@ __global__ void __launch_bounds__(PCG_THREADS, 1)
     // ---- per-thread rows
     const bool worker = tid < PCG_WORKERS;
     const int r = worker ? tid % NS : 0, g0 = worker ? tid / NS : 0;
-    size_t doff[NS];  // offsets of row r of the diagonal block within a knot block
+    int doff[NS];  // offsets of row r of the diagonal block within a knot block
 #pragma unroll
-    for (int cc = 0; cc < NS; ++cc) doff[cc] = diag_off<FMT>(0, r, cc);
-    const size_t kstride = FMT == 1 ? PK : S_STRIDE;
+    for (int cc = 0; cc < NS; ++cc) doff[cc] = diag_off<FMT>(r, cc);
     const float *gb = gamma + NS * kg0;
     float *lb = lambda + NS * kg0;
-    double lam[PCG_KPT], res[PCG_KPT];
-    float pp[PCG_KPT], zz[PCG_KPT], gv[PCG_KPT];
+    double lam[PCG_KPT], res[PCG_KPT], pp[PCG_KPT], zz[PCG_KPT];
+    float gv[PCG_KPT];
     bool own[PCG_KPT];
 #pragma unroll
     for (int j = 0; j < PCG_KPT; ++j) {
         const int kl = g0 + PCG_TK * j;
         own[j] = worker && kl < kpc;
-        lam[j] = res[j] = 0.0;
-        pp[j] = zz[j] = gv[j] = 0.f;
+        lam[j] = res[j] = pp[j] = zz[j] = 0.0;
+        gv[j] = 0.f;
         if (own[j]) {
             gv[j] = gb[NS * kl + r];
             lam[j] = (double)lb[NS * kl + r];
         }
     }
-    // (S x)_row with FP64 accumulation; x holds 14 (kpc+2) doubles with halo slots
-    auto row_f64 = [&](int j, const double *x) -> double {
+    // (S x)_row with FP64 accumulation; x = rv holds 14 (kpc+2) doubles with halo slots
+    auto row_f64 = [&](int j) -> double {
         const int kl = g0 + PCG_TK * j, k = k0 + kl;
         const float *lk = left + (size_t)kl * SS;
         const float *dg = S + (kg0 + kl) * kstride;
-        const double *xk = x + NS * kl;
-        double a = 0.0;
+        const double *xk = rv + NS * kl;
+        double a0 = 0.0, a1 = 0.0, a2 = 0.0;
         if (k > 0) {
 #pragma unroll
-            for (int cc = 0; cc < NS; ++cc) a = fma((double)lk[r + NS * cc], xk[cc], a);
+            for (int cc = 0; cc < NS; ++cc) a0 = fma((double)lk[r + NS * cc], xk[cc], a0);
         }
 #pragma unroll
-        for (int cc = 0; cc < NS; ++cc) a = fma((double)__ldg(dg + doff[cc]), xk[NS + cc], a);
+        for (int cc = 0; cc < NS; ++cc) a1 = fma((double)__ldg(dg + doff[cc]), xk[NS + cc], a1);
         if (k < N - 1) {
             const float *ln = (kl + 1 < kpc) ? lk + SS : left_next;
 #pragma unroll
-            for (int cc = 0; cc < NS; ++cc) a = fma((double)ln[cc + NS * r], xk[2 * NS + cc], a);
+            for (int cc = 0; cc < NS; ++cc) a2 = fma((double)ln[cc + NS * r], xk[2 * NS + cc], a2);
         }
-        return a;
+        return (a0 + a1) + a2;
     };
-    // lambda (FP64) with halos into rv; then gamma - S lambda
-    auto true_residual = [&](bool from_global) {
+    // write a per-row vector (FP64) into rv with its halo knots; barrier makes it visible
+    auto publish = [&](const double (&v)[PCG_KPT], bool halo_from_global) {
         __syncthreads();
 #pragma unroll
         for (int j = 0; j < PCG_KPT; ++j) {
             if (own[j]) {
                 const int kl = g0 + PCG_TK * j;
-                rv[NS * (kl + 1) + r] = lam[j];
-                if (!from_global) {
-                    if constexpr (CS > 1) {
+                rv[NS * (kl + 1) + r] = v[j];
+                if constexpr (CS > 1) {
+                    if (!halo_from_global) {
                         cg::cluster_group cl = cg::this_cluster();
-                        if (kl == 0 && rank > 0) cl.map_shared_rank(rv, rank - 1)[NS * (kpc_left + 1) + r] = lam[j];
-                        if (kl == kpc - 1 && rank < CS - 1) cl.map_shared_rank(rv, rank + 1)[r] = lam[j];
+                        if (kl == 0 && rank > 0) cl.map_shared_rank(rv, rank - 1)[NS * (kpc_left + 1) + r] = v[j];
+                        if (kl == kpc - 1 && rank < CS - 1) cl.map_shared_rank(rv, rank + 1)[r] = v[j];
                     }
                 }
             }
         }
-        if (from_global && tid < NS) {
-            rv[tid] = (k0 > 0) ? (double)lambda[NS * (kg0 - 1) + tid] : 0.0;
-            rv[NS * (kpc + 1) + tid] = (k1 < N) ? (double)lambda[NS * ((size_t)kb + k1) + tid] : 0.0;
-        }
-        if (!from_global && tid < NS) {
-            if (k0 == 0) rv[tid] = 0.0;
-            if (k1 == N) rv[NS * (kpc + 1) + tid] = 0.0;
+        if (tid < NS) {
+            if (halo_from_global) {
+                rv[tid] = (k0 > 0) ? (double)lambda[NS * (kg0 - 1) + tid] : 0.0;
+                rv[NS * (kpc + 1) + tid] = (k1 < N) ? (double)lambda[NS * ((size_t)kb + k1) + tid] : 0.0;
+            } else {
+                if (k0 == 0) rv[tid] = 0.0;
+                if (k1 == N) rv[NS * (kpc + 1) + tid] = 0.0;
+            }
         }
         if constexpr (CS > 1) {
-            if (!from_global) cg::this_cluster().sync();
-            else __syncthreads();
+            cg::this_cluster().sync();
         } else {
             __syncthreads();
         }
+    };
+    // all reads of rv's halo slots by neighbours done before rv is rewritten
+    auto release = [&]() {
+        if constexpr (CS > 1) {
+            cg::this_cluster().sync();
+        } else {
+            __syncthreads();
+        }
+    };
+    auto true_residual = [&](bool from_global) {
+        publish(lam, from_global);
 #pragma unroll
         for (int j = 0; j < PCG_KPT; ++j)
-            if (own[j]) res[j] = (double)gv[j] - row_f64(j, rv);
-        if constexpr (CS > 1) {
-            cg::this_cluster().sync();  // neighbours finished reading this CTA's halo slots
-        } else {
-            __syncthreads();
-        }
+            if (own[j]) res[j] = (double)gv[j] - row_f64(j);
+        release();
     };
     // exact chunk solve on warp 0, in place on rv (interior slots): rv <- M_chunk^{-1} rv
     auto chain_solve = [&]() {
@@ -742,7 +752,7 @@ __global__ void __launch_bounds__(PCG_THREADS, 1)
             xnext = x;
         }
     };
-    // z = S_chunk^{-1} r, halo exchange of z, partial dot products
+    // z = S_chunk^{-1} r, partial dot products
     auto precond = [&](double (&d)[3]) {
         __syncthreads();
 #pragma unroll
@@ -755,19 +765,14 @@ __global__ void __launch_bounds__(PCG_THREADS, 1)
         for (int j = 0; j < PCG_KPT; ++j) {
             if (own[j]) {
                 const int kl = g0 + PCG_TK * j;
-                zz[j] = (float)(-rv[NS * (kl + 1) + r]);
-                d[1] += res[j] * (double)zz[j];
+                zz[j] = -rv[NS * (kl + 1) + r];
+                d[1] += res[j] * zz[j];
                 d[2] += res[j] * res[j];
-                if constexpr (CS > 1) {
-                    cg::cluster_group cl = cg::this_cluster();
-                    if (kl == 0 && rank > 0) cl.map_shared_rank(zh_r, rank - 1)[r] = zz[j];
-                    if (kl == kpc - 1 && rank < CS - 1) cl.map_shared_rank(zh_l, rank + 1)[r] = zz[j];
-                }
             }
         }
     };
 
-    // ---- initial residual (FP64, lambda FP32 from global with halos)
+    // ---- initial residual (FP64, lambda FP32 from global with halos), z, p = z
     true_residual(true);
     int set = 1;
     double eta, rr2, gg;
@@ -783,15 +788,7 @@ __global__ void __launch_bounds__(PCG_THREADS, 1)
         eta = acc3[1];
         rr2 = acc3[2];
 #pragma unroll
-        for (int j = 0; j < PCG_KPT; ++j) {
-            pp[j] = zz[j];
-            if (own[j]) pv[NS * (g0 + PCG_TK * j + 1) + r] = pp[j];
-        }
-        if (tid < NS) {
-            pv[tid] = (k0 > 0) ? zh_l[tid] : 0.f;
-            pv[NS * (kpc + 1) + tid] = (k1 < N) ? zh_r[tid] : 0.f;
-        }
-        __syncthreads();
+        for (int j = 0; j < PCG_KPT; ++j) pp[j] = zz[j];
     }
     auto converged = [&](double e, double r2) {
         return exit_mode == 0 ? (r2 <= (double)tol * (double)tol * gg) : (fabs(e) < (double)tol);
@@ -799,46 +796,18 @@ __global__ void __launch_bounds__(PCG_THREADS, 1)
     bool conv = converged(eta, rr2), bad = false;
     int it = 0;
     while (!conv && it < max_iter) {
+        publish(pp, false);
         double d1[1] = {0.0};
-        float vv[PCG_KPT];
+        double vv[PCG_KPT];
 #pragma unroll
         for (int j = 0; j < PCG_KPT; ++j) {
-            vv[j] = 0.f;
+            vv[j] = 0.0;
             if (own[j]) {
-                const int kl = g0 + PCG_TK * j, k = k0 + kl;
-                const float *lk = left + (size_t)kl * SS;
-                const float *dg = S + (kg0 + kl) * kstride;
-                const float *xk = pv + NS * kl;
-                float a0 = 0.f, a1 = 0.f, a2 = 0.f;
-                if (k > 0) {
-#pragma unroll
-                    for (int m = 0; m < NS / 2; ++m) {
-                        const float2 xv = lds2(xk + 2 * m);
-                        a0 = fmaf(lk[r + NS * (2 * m)], xv.x, a0);
-                        a0 = fmaf(lk[r + NS * (2 * m + 1)], xv.y, a0);
-                    }
-                }
-#pragma unroll
-                for (int m = 0; m < NS / 2; ++m) {
-                    const float2 xv = lds2(xk + NS + 2 * m);
-                    a1 = fmaf(__ldg(dg + doff[2 * m]), xv.x, a1);
-                    a1 = fmaf(__ldg(dg + doff[2 * m + 1]), xv.y, a1);
-                }
-                if (k < N - 1) {
-                    const float *ln = (kl + 1 < kpc) ? lk + SS : left_next;
-#pragma unroll
-                    for (int m = 0; m < NS / 2; ++m) {
-                        const float2 xv = lds2(xk + 2 * NS + 2 * m);
-                        const float2 lv = lds2(ln + NS * r + 2 * m);
-                        a2 = fmaf(lv.x, xv.x, a2);
-                        a2 = fmaf(lv.y, xv.y, a2);
-                    }
-                }
-                vv[j] = (a0 + a1) + a2;
-                d1[0] += (double)pp[j] * (double)vv[j];
+                vv[j] = row_f64(j);
+                d1[0] += pp[j] * vv[j];
             }
         }
-        cluster_sum_raw<CS, 1>(d1, slots, red, set);
+        cluster_sum_raw<CS, 1>(d1, slots, red, set);  // its barrier also releases rv
         set ^= 1;
         const double alpha = eta / d1[0];
         if (!isfinite(alpha)) {
@@ -847,8 +816,8 @@ __global__ void __launch_bounds__(PCG_THREADS, 1)
         }
 #pragma unroll
         for (int j = 0; j < PCG_KPT; ++j) {
-            lam[j] = fma(alpha, (double)pp[j], lam[j]);
-            res[j] = fma(-alpha, (double)vv[j], res[j]);
+            lam[j] = fma(alpha, pp[j], lam[j]);
+            res[j] = fma(-alpha, vv[j], res[j]);
         }
         ++it;
         bool replaced = false;
@@ -877,18 +846,10 @@ __global__ void __launch_bounds__(PCG_THREADS, 1)
             break;
         }
         if (conv) break;
-        const float beta = (float)(d2[1] / eta);
+        const double beta = d2[1] / eta;
         eta = d2[1];
 #pragma unroll
-        for (int j = 0; j < PCG_KPT; ++j) {
-            pp[j] = fmaf(beta, pp[j], zz[j]);
-            if (own[j]) pv[NS * (g0 + PCG_TK * j + 1) + r] = pp[j];
-        }
-        if (tid < NS) {
-            pv[tid] = (k0 > 0) ? fmaf(beta, pv[tid], zh_l[tid]) : 0.f;
-            pv[NS * (kpc + 1) + tid] = (k1 < N) ? fmaf(beta, pv[NS * (kpc + 1) + tid], zh_r[tid]) : 0.f;
-        }
-        __syncthreads();
+        for (int j = 0; j < PCG_KPT; ++j) pp[j] = fma(beta, pp[j], zz[j]);
     }
 #pragma unroll
     for (int j = 0; j < PCG_KPT; ++j) {
