@@ -34,7 +34,8 @@ sys.path.insert(0, ROOT)
 
 METRIC = "SQP solves/s @N=128 batched vs plain @rel-res 1e-5"
 SPEC = dict(timestep=0.01, integrator=1, qd_cost=1e-2, r_cost=1e-4)
-PCG_FLOATS_PER_KNOT_ITER = 896   # S 588 + Pinv 196 + 8 vectors x 14 streamed per PCG iteration
+PCG_FLOATS_PER_KNOT = 784        # S 588 + Pinv 196 read once per PCG launch (algorithmic)
+PCG_FLOATS_PER_KNOT_ITER = 896   # S, Pinv and 8 vectors x 14 if re-read every PCG iteration (upper bound)
 ALG_FLOATS_PER_KNOT_SQP = 4058   # every materialised SQP-iteration tensor written once, read once
 
 
@@ -53,6 +54,8 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="bound of the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--pcg-cluster", type=int, default=0, help="CTAs per instance in the PCG (0 = library choice)")
+    ap.add_argument("--pcg-precond", type=int, default=1, choices=[0, 1],
+                    help="0 block-Jacobi (the reference's), 1 block-tridiagonal LDL^T per CTA chunk")
     ap.add_argument("--batched-only", action="store_true", help="skip the e2e and plain legs (profiling runs)")
     return ap.parse_args()
 
@@ -209,7 +212,7 @@ def main():
     batch = P.make_batch(Ns, seed0=rank * B, dt=SPEC["timestep"])
     sv = gpt.Solver(max_knot_points=N, max_batch=B, **SPEC)
     sv.set_solver(sqp_max_iter=args.sqp_max_iter, pcg_max_iter=args.pcg_max_iter, pcg_exit_tol=args.tol,
-                  pcg_exit_mode=0, pcg_cluster_size=args.pcg_cluster)
+                  pcg_exit_mode=0, pcg_cluster_size=args.pcg_cluster, pcg_precond=args.pcg_precond)
     stream = torch.cuda.current_stream()
     xu0 = torch.as_tensor(batch["xu"], device="cuda")
     goal = torch.as_tensor(batch["goal"], device="cuda")
@@ -303,7 +306,7 @@ def main():
     plain_ms = []
     sv1 = gpt.Solver(max_knot_points=N, max_batch=1, **SPEC)
     sv1.set_solver(sqp_max_iter=args.sqp_max_iter, pcg_max_iter=args.pcg_max_iter, pcg_exit_tol=args.tol,
-                   pcg_exit_mode=0)
+                   pcg_exit_mode=0, pcg_precond=args.pcg_precond)
     for i in range(args.plain_solves + 1):
         p = P.make_problem(N, rank * B + i, dt=SPEC["timestep"])
         x1, g1, l1 = (torch.as_tensor(p[k], device="cuda") for k in ("xu", "goal", "lam"))
@@ -326,27 +329,32 @@ def main():
     pcg_total = sum(s["pcg_iters_total"] for s in all_stats)
     pcg_maxit = sum(s["pcg_maxiter_count"] for s in all_stats)
     n_pcg_solves = sum(sqp_iters)
-    # roofline: the PCG kernel dominates; bytes it streams per launch = 896 floats x knots x PCG iterations
+    # roofline: the PCG kernel dominates; its algorithmic bytes per launch = 784 floats x knots of the batch
     pcg_ms, pcg_launches = phases["pcg"]
     launches_total = sum(n for _, n in phases.values())
     mp = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
         os.path.join(ROOT, "MEASURED_PEAKS.json")) else None
     peak = mp["hbm_gbs"] if mp else 6650.0
-    per_launch_bytes = 4.0 * PCG_FLOATS_PER_KNOT_ITER * N * pcg_total / max(pcg_launches, 1)
+    per_launch_bytes = 4.0 * PCG_FLOATS_PER_KNOT * N * B
+    stream_bytes = 4.0 * PCG_FLOATS_PER_KNOT_ITER * N * pcg_total / max(pcg_launches, 1)
     per_launch_s = (pcg_ms / max(pcg_launches, 1)) / 1000.0
     achieved = per_launch_bytes / per_launch_s / 1e9 if per_launch_s > 0 else 0.0
+    precond_name = "block-tridiagonal LDL^T" if args.pcg_precond == 1 else "block-Jacobi"
+    pcg_kernel = "pcg_chain_kernel" if args.pcg_precond == 1 else "pcg_cluster_kernel"
     line = {
         "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": f"batched sqpSolve, {B} instances/GPU x N={N} knots, dt=0.01 semi-implicit Euler, "
-                               f"QD=0.01, R=1e-4, PCG block-Jacobi rel-res {args.tol:g} (max {args.pcg_max_iter} it), "
+                               f"QD=0.01, R=1e-4, PCG {precond_name} rel-res {args.tol:g} (max {args.pcg_max_iter} it), "
                                f"<= {args.sqp_max_iter} SQP iterations",
                    "instances_per_gpu": B, "knot_points": N, "pcg_exit_tol": args.tol, "parallelism": f"dp{world}",
+                   "pcg_precond": precond_name,
                    "l2": "256 MB buffer written between timed steps"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": None, "kernel": "pcg_kernel",
-                     "bytes_model": "896 floats per knot per PCG iteration (S, Pinv, vectors streamed)",
+                     "traffic": None, "kernel": pcg_kernel,
+                     "bytes_model": "784 floats per knot per launch (S 588 + Pinv 196 read once)",
+                     "stream_bound_gbs": stream_bytes / per_launch_s / 1e9 if per_launch_s > 0 else 0.0,
                      "peak_source": "measured" if mp else "fallback"},
         "cpu_baseline": cb,
         "e2e": {"value": world * B / (e2e_step / 1000.0), "unit": "solves/s", "h2d_bytes_per_step": h2d,

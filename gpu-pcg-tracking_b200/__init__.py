@@ -105,11 +105,11 @@ def _declare(L):
         "gpt_sqp_solve": ([vp, u32, vp, vp, vp, P(f32), f32, P(SqpStats), vp, vp, vp], C.c_int),
         "gpt_sqp_solve_batched": ([vp, u32, vp, vp, vp, vp, vp, f32, vp, vp], C.c_int),
         "gpt_form_kkt": ([vp, u32, vp, vp, vp, vp, vp, vp, vp, vp], C.c_int),
-        "gpt_form_schur": ([vp, u32, f32, vp, vp, vp, vp, vp, vp, vp, vp, vp], C.c_int),
+        "gpt_form_schur": ([vp, u32, f32, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp], C.c_int),
         "gpt_form_schur_csc": ([vp, u32, f32, vp, vp, vp, vp, vp, vp, vp, vp], C.c_int),
         "gpt_prep_csr": ([u32, vp, vp], C.c_int),
         "gpt_pcg": ([vp, u32, vp, vp, vp, vp, vp, u32, f32, u32, P(u32), P(C.c_uint8), vp], C.c_int),
-        "gpt_compute_dz": ([vp, u32, vp, vp, vp, vp, vp, vp, vp], C.c_int),
+        "gpt_compute_dz": ([vp, u32, vp, vp, vp, vp, vp, vp, vp, vp], C.c_int),
         "gpt_compute_merit": ([vp, u32, vp, vp, vp, vp], C.c_int),
         "gpt_ls_compute_merit": ([vp, u32, vp, vp, vp, vp, vp, vp], C.c_int),
         "gpt_set_profiling": ([vp, C.c_int], C.c_int),
@@ -239,9 +239,9 @@ class Solver:
         _check(lib().gpt_form_kkt(self._h, N, _ptr(xu), _ptr(eePos), _ptr(xs), _ptr(G), _ptr(Cm), _ptr(g), _ptr(c),
                                   _stream(stream)))
 
-    def form_schur(self, N, rho, G, Cm, g, c, S, Pinv, gamma, Ginv, stream=None):
+    def form_schur(self, N, rho, G, Cm, g, c, S, Pinv, gamma, Ginv, Ginv64=None, stream=None):
         _check(lib().gpt_form_schur(self._h, N, rho, _ptr(G), _ptr(Cm), _ptr(g), _ptr(c), _ptr(S), _ptr(Pinv),
-                                    _ptr(gamma), _ptr(Ginv), _stream(stream)))
+                                    _ptr(gamma), _ptr(Ginv), _ptr(Ginv64), _stream(stream)))
 
     def form_schur_csc(self, N, rho, G, Cm, g, c, val, gamma, Ginv, stream=None):
         _check(lib().gpt_form_schur_csc(self._h, N, rho, _ptr(G), _ptr(Cm), _ptr(g), _ptr(c), _ptr(val),
@@ -254,9 +254,9 @@ class Solver:
                              exit_tol, exit_mode, C.byref(it), C.byref(mx), _stream(stream)))
         return it.value, bool(mx.value)
 
-    def compute_dz(self, N, Ginv, Cm, g, lam, dz, lam64=None, stream=None):
-        _check(lib().gpt_compute_dz(self._h, N, _ptr(Ginv), _ptr(Cm), _ptr(g), _ptr(lam), _ptr(lam64), _ptr(dz),
-                                    _stream(stream)))
+    def compute_dz(self, N, Ginv, Cm, g, lam, dz, lam64=None, Ginv64=None, stream=None):
+        _check(lib().gpt_compute_dz(self._h, N, _ptr(Ginv), _ptr(Ginv64), _ptr(Cm), _ptr(g), _ptr(lam), _ptr(lam64),
+                                    _ptr(dz), _stream(stream)))
 
     def compute_merit(self, N, xu, eePos, out, stream=None):
         _check(lib().gpt_compute_merit(self._h, N, _ptr(xu), _ptr(eePos), _ptr(out), _stream(stream)))

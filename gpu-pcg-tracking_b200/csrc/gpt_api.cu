@@ -50,6 +50,7 @@ struct gpt_handle {
     int *knot_off = nullptr, *knot_inst = nullptr;
     uint32_t *pcg_log = nullptr, *pcg_out = nullptr, *d_active = nullptr;
     double *lam64 = nullptr;   // FP64 multipliers from the PCG, consumed by dz
+    double *Ginv64 = nullptr;  // FP64 inverses (Q + rho I)^-1, (R + rho I)^-1 from Schur, consumed by dz
     uint32_t cap_sqp_iter = 0;  // pcg_log rows allocated at creation
     // pinned host staging
     uint32_t *h_active = nullptr;
@@ -145,7 +146,7 @@ void gpt_default_solver_config(gpt_solver_config *o)
     o->rho_max = 10.0f;
     o->rho_min = 1e-3f;
     o->pcg_cluster_size = 0;
-    o->pcg_precond = 0;
+    o->pcg_precond = 1;
 }
 
 const char *gpt_last_error(void) { return g_last_error.c_str(); }
@@ -213,6 +214,7 @@ gpt_status gpt_create(const gpt_problem_config *pc, const gpt_solver_config *sc,
     ALLOC(pcg_out, 2 * B);
     ALLOC(d_active, 1);
     ALLOC(lam64, NS * T);
+    ALLOC(Ginv64, G_STRIDE * T);
 #undef ALLOC
     if (e == cudaSuccess) e = cudaMallocHost((void **)&h->h_active, sizeof(uint32_t));
     if (e == cudaSuccess) e = cudaMallocHost((void **)&h->h_st, sizeof(InstState) * B);
@@ -258,7 +260,7 @@ gpt_status gpt_destroy(gpt_handle *h)
     cudaFree(h->G); cudaFree(h->C); cudaFree(h->g); cudaFree(h->c); cudaFree(h->S);
     cudaFree(h->gamma); cudaFree(h->Ginv); cudaFree(h->dz); cudaFree(h->xs); cudaFree(h->knot_merit);
     cudaFree(h->merits); cudaFree(h->st); cudaFree(h->knot_off); cudaFree(h->knot_inst); cudaFree(h->pcg_log);
-    cudaFree(h->pcg_out); cudaFree(h->d_active); cudaFree(h->lam64);
+    cudaFree(h->pcg_out); cudaFree(h->d_active); cudaFree(h->lam64); cudaFree(h->Ginv64);
     cudaFreeHost(h->h_active); cudaFreeHost(h->h_st); cudaFreeHost(h->h_pcg_out); cudaFreeHost(h->h_pcg_log);
     if (h->ev) cudaEventDestroy(h->ev);
     delete h;
@@ -281,13 +283,13 @@ gpt_status gpt_form_kkt(gpt_handle *h, uint32_t N, const float *d_xu, const floa
 
 gpt_status gpt_form_schur(gpt_handle *h, uint32_t N, float rho, const float *d_G, const float *d_C, const float *d_g,
                           const float *d_c, float *d_S, float *d_Pinv, float *d_gamma, float *d_Ginv,
-                          gpt_stream_t stream)
+                          double *d_Ginv64, gpt_stream_t stream)
 {
     if (!h || !d_G || !d_C || !d_g || !d_c || !d_S || !d_Pinv || !d_gamma || !d_Ginv)
         return set_err(GPT_ERR_BAD_ARG, "null argument");
     if (!check_n(h, N)) return set_err(GPT_ERR_BAD_ARG, "knot_points out of range");
-    GPT_CUDA(launch_schur(0, single_view(N), rho, d_G, d_C, d_g, d_c, d_S, d_Pinv, d_gamma, d_Ginv, nullptr,
-                          h->num_sms, (cudaStream_t)stream));
+    GPT_CUDA(launch_schur(0, single_view(N), rho, d_G, d_C, d_g, d_c, d_S, d_Pinv, d_gamma, d_Ginv, d_Ginv64, nullptr,
+                          1, h->num_sms, (cudaStream_t)stream));
     return GPT_OK;
 }
 
@@ -298,8 +300,8 @@ gpt_status gpt_form_schur_csc(gpt_handle *h, uint32_t N, float rho, const float 
     if (!h || !d_G || !d_C || !d_g || !d_c || !d_val || !d_gamma || !d_Ginv)
         return set_err(GPT_ERR_BAD_ARG, "null argument");
     if (!check_n(h, N)) return set_err(GPT_ERR_BAD_ARG, "knot_points out of range");
-    GPT_CUDA(launch_schur(2, single_view(N), rho, d_G, d_C, d_g, d_c, nullptr, nullptr, d_gamma, d_Ginv, d_val,
-                          h->num_sms, (cudaStream_t)stream));
+    GPT_CUDA(launch_schur(2, single_view(N), rho, d_G, d_C, d_g, d_c, nullptr, nullptr, d_gamma, d_Ginv, nullptr, d_val,
+                          0, h->num_sms, (cudaStream_t)stream));
     return GPT_OK;
 }
 
@@ -337,13 +339,15 @@ gpt_status gpt_pcg(gpt_handle *h, uint32_t N, const float *d_S, const float *d_P
     return GPT_OK;
 }
 
-gpt_status gpt_compute_dz(gpt_handle *h, uint32_t N, const float *d_Ginv, const float *d_C, const float *d_g,
-                          const float *d_lambda, const double *d_lambda64, float *d_dz, gpt_stream_t stream)
+gpt_status gpt_compute_dz(gpt_handle *h, uint32_t N, const float *d_Ginv, const double *d_Ginv64, const float *d_C,
+                          const float *d_g, const float *d_lambda, const double *d_lambda64, float *d_dz,
+                          gpt_stream_t stream)
 {
-    if (!h || !d_Ginv || !d_C || !d_g || (!d_lambda && !d_lambda64) || !d_dz)
+    if (!h || (!d_Ginv && !d_Ginv64) || !d_C || !d_g || (!d_lambda && !d_lambda64) || !d_dz)
         return set_err(GPT_ERR_BAD_ARG, "null argument");
     if (!check_n(h, N)) return set_err(GPT_ERR_BAD_ARG, "knot_points out of range");
-    GPT_CUDA(launch_dz(single_view(N), d_Ginv, d_C, d_g, d_lambda, d_lambda64, d_dz, h->num_sms, (cudaStream_t)stream));
+    GPT_CUDA(launch_dz(single_view(N), d_Ginv, d_Ginv64, d_C, d_g, d_lambda, d_lambda64, d_dz, h->num_sms,
+                       (cudaStream_t)stream));
     return GPT_OK;
 }
 
@@ -476,7 +480,8 @@ static gpt_status sqp_run(gpt_handle *h, uint32_t B, const uint32_t *Ns, const f
         }
         {
             PhaseTimer t(h, s, GPT_PHASE_SCHUR);
-            GPT_CUDA(launch_schur(1, bv, 0.f, h->G, h->C, h->g, h->c, h->S, nullptr, h->gamma, h->Ginv, nullptr, ns, s));
+            GPT_CUDA(launch_schur(1, bv, 0.f, h->G, h->C, h->g, h->c, h->S, nullptr, h->gamma, h->Ginv, h->Ginv64,
+                                  nullptr, SP.pcg_precond == 0 ? 1 : 0, ns, s));
         }
         {
             PhaseTimer t(h, s, GPT_PHASE_PCG);
@@ -486,7 +491,7 @@ static gpt_status sqp_run(gpt_handle *h, uint32_t B, const uint32_t *Ns, const f
         }
         {
             PhaseTimer t(h, s, GPT_PHASE_DZ);
-            GPT_CUDA(launch_dz(bv, h->Ginv, h->C, h->g, d_lambda, h->lam64, h->dz, ns, s));
+            GPT_CUDA(launch_dz(bv, h->Ginv, h->Ginv64, h->C, h->g, d_lambda, h->lam64, h->dz, ns, s));
         }
         {
             PhaseTimer t(h, s, GPT_PHASE_MERIT);

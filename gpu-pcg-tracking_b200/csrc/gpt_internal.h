@@ -24,9 +24,10 @@ struct SolverParams {
 
 cudaError_t launch_kkt(const BatchView &bv, const ProblemParams &P, const float *xu, const float *goal,
                        const float *xs, float *G, float *C, float *g, float *c, int num_sms, cudaStream_t s);
+// Ginv64 (optional) receives the inverses in FP64; need_pinv = 0 skips the theta inversion in mode 1
 cudaError_t launch_schur(int mode, const BatchView &bv, float rho_scalar, const float *G, const float *C,
                          const float *g, const float *c, float *S, float *Pinv, float *gamma, float *Ginv,
-                         float *csc_val, int num_sms, cudaStream_t s);
+                         double *Ginv64, float *csc_val, int need_pinv, int num_sms, cudaStream_t s);
 size_t pcg_cluster_smem_bytes(int kpc);
 int pcg_pick_cluster(int maxN, int B, int num_sms, int requested);
 // fmt 0: S and Pinv in the reference 3-block layout; fmt 1: packed rows (PK floats per knot) in S
@@ -36,8 +37,8 @@ cudaError_t launch_pcg(const BatchView &bv, int max_n_knots, int min_n_knots, in
                        float tol, int exit_mode, uint32_t *out_iters, uint32_t *pcg_log, int log_stride,
                        int cluster_size, int num_sms, cudaStream_t s);
 // lambda64 (optional) replaces lambda when given
-cudaError_t launch_dz(const BatchView &bv, const float *Ginv, const float *C, const float *g, const float *lambda,
-                      const double *lambda64, float *dz, int num_sms, cudaStream_t s);
+cudaError_t launch_dz(const BatchView &bv, const float *Ginv, const double *Ginv64, const float *C, const float *g,
+                      const float *lambda, const double *lambda64, float *dz, int num_sms, cudaStream_t s);
 cudaError_t launch_merit(const BatchView &bv, const ProblemParams &P, int n_alpha, const float *xu, const float *dz,
                          const float *goal, const float *xs, float *knot_merit, int num_sms, cudaStream_t s);
 cudaError_t launch_accept(const BatchView &bv, int mode, const SolverParams &SP, const float *knot_merit,

@@ -20,9 +20,9 @@ constexpr int DZ_WARPS = 4;
 // q_k - lambda_k - (-A_k)^T lambda_{k+1} and r_k - (-B_k)^T lambda_{k+1} cancel
 // heavily, so they are accumulated in FP64 before the FP32-stored inverses apply.
 __global__ void __launch_bounds__(32 * DZ_WARPS)
-    dz_kernel(BatchView bv, const float *__restrict__ Ginv, const float *__restrict__ Cm,
-              const float *__restrict__ g, const float *__restrict__ lambda, const double *__restrict__ lambda64,
-              float *__restrict__ dz)
+    dz_kernel(BatchView bv, const float *__restrict__ Ginv, const double *__restrict__ Ginv64,
+              const float *__restrict__ Cm, const float *__restrict__ g, const float *__restrict__ lambda,
+              const double *__restrict__ lambda64, float *__restrict__ dz)
 {
     __shared__ double s_all[DZ_WARPS][NX];
     __shared__ double l_all[DZ_WARPS][2 * NS];
@@ -58,29 +58,31 @@ __global__ void __launch_bounds__(32 * DZ_WARPS)
         }
         __syncwarp();
         const float *Gi = Ginv + (size_t)G_STRIDE * j;
+        const double *Gi64 = Ginv64 ? Ginv64 + (size_t)G_STRIDE * j : nullptr;
         if (lane < NS) {
             double a = 0.0;
 #pragma unroll
-            for (int t = 0; t < NS; ++t) a = fma((double)Gi[lane + NS * t], s[t], a);
+            for (int t = 0; t < NS; ++t) a = fma(Gi64 ? Gi64[lane + NS * t] : (double)Gi[lane + NS * t], s[t], a);
             dz[(size_t)NX * j + lane] = (float)a;
         } else if (lane < NX && !last) {
             const int i = lane - NS;
             double a = 0.0;
 #pragma unroll
-            for (int t = 0; t < NC; ++t) a = fma((double)Gi[SS + i + NC * t], s[NS + t], a);
+            for (int t = 0; t < NC; ++t)
+                a = fma(Gi64 ? Gi64[SS + i + NC * t] : (double)Gi[SS + i + NC * t], s[NS + t], a);
             dz[(size_t)NX * j + lane] = (float)a;
         }
         __syncwarp();
     }
 }
 
-cudaError_t launch_dz(const BatchView &bv, const float *Ginv, const float *C, const float *g, const float *lambda,
-                      const double *lambda64, float *dz, int num_sms, cudaStream_t s)
+cudaError_t launch_dz(const BatchView &bv, const float *Ginv, const double *Ginv64, const float *C, const float *g,
+                      const float *lambda, const double *lambda64, float *dz, int num_sms, cudaStream_t s)
 {
     if (bv.total_knots <= 0) return cudaSuccess;
     int blocks = (bv.total_knots + DZ_WARPS - 1) / DZ_WARPS;
     if (blocks > num_sms * 16) blocks = num_sms * 16;
-    dz_kernel<<<blocks, 32 * DZ_WARPS, 0, s>>>(bv, Ginv, C, g, lambda, lambda64, dz);
+    dz_kernel<<<blocks, 32 * DZ_WARPS, 0, s>>>(bv, Ginv, Ginv64, C, g, lambda, lambda64, dz);
     return cudaGetLastError();
 }
 

@@ -26,7 +26,8 @@ namespace gpt {
 // in A (global or shared).  Lanes 0..2n-1 hold the columns of [A | I]; the
 // inverse is written column-major (float) to Ainv.
 template <int n>
-__device__ __forceinline__ void warp_inverse(const float *A, float shift, float *Ainv, int lane)
+__device__ __forceinline__ void warp_inverse(const float *A, float shift, float *Ainv, int lane,
+                                             double *Ainv64 = nullptr)
 {
     double col[n];
     const bool left = lane < n, right = (lane >= n) && (lane < 2 * n);
@@ -49,6 +50,10 @@ __device__ __forceinline__ void warp_inverse(const float *A, float shift, float 
     if (right) {
 #pragma unroll
         for (int r = 0; r < n; ++r) Ainv[r + n * (lane - n)] = (float)col[r];
+        if (Ainv64) {
+#pragma unroll
+            for (int r = 0; r < n; ++r) Ainv64[r + n * (lane - n)] = col[r];
+        }
     }
 }
 
@@ -91,7 +96,7 @@ __global__ void __launch_bounds__(32 * SCHUR_WARPS)
     schur_kernel(BatchView bv, float rho_scalar, const float *__restrict__ G,
                  const float *__restrict__ Cm, const float *__restrict__ g, const float *__restrict__ c,
                  float *__restrict__ S, float *__restrict__ Pinv, float *__restrict__ gamma,
-                 float *__restrict__ Ginv, float *__restrict__ csc_val)
+                 float *__restrict__ Ginv, double *__restrict__ Ginv64, float *__restrict__ csc_val, int need_pinv)
 {
     extern __shared__ float4 schur_dyn_smem[];
     SchurWarpSmem *smem_all = reinterpret_cast<SchurWarpSmem *>(schur_dyn_smem);
@@ -110,7 +115,7 @@ __global__ void __launch_bounds__(32 * SCHUR_WARPS)
 
         if (k == 0) {
             const float *Q0 = G + (size_t)G_STRIDE * j;
-            warp_inverse<NS>(Q0, rho, sm.Qki, lane);
+            warp_inverse<NS>(Q0, rho, sm.Qki, lane, (N == 1 && Ginv64) ? Ginv64 + (size_t)G_STRIDE * j : nullptr);
             if (lane < NS) sm.qk[lane] = g[(size_t)NX * j + lane];
             __syncwarp();
             if (lane < NS) {
@@ -173,9 +178,10 @@ __global__ void __launch_bounds__(32 * SCHUR_WARPS)
         }
         const float *Gkm1 = G + (size_t)G_STRIDE * (j - 1);
         const float *Gk = G + (size_t)G_STRIDE * j;
-        warp_inverse<NS>(Gkm1, rho, sm.Qki, lane);
-        warp_inverse<NS>(Gk, rho, sm.Qkp1i, lane);
-        warp_inverse<NC>(Gkm1 + SS, rho, sm.Rki, lane);
+        double *G64m1 = Ginv64 ? Ginv64 + (size_t)G_STRIDE * (j - 1) : nullptr;
+        warp_inverse<NS>(Gkm1, rho, sm.Qki, lane, G64m1);
+        warp_inverse<NS>(Gk, rho, sm.Qkp1i, lane, (Ginv64 && k == N - 1) ? Ginv64 + (size_t)G_STRIDE * j : nullptr);
+        warp_inverse<NC>(Gkm1 + SS, rho, sm.Rki, lane, G64m1 ? G64m1 + SS : nullptr);
         __syncwarp();
         // Ginv slots (schur.cuh:236-256): Qt_{k-1}^{-1}, Rt_{k-1}^{-1}; the last row also Qt_{N-1}^{-1}
         {
@@ -205,7 +211,7 @@ __global__ void __launch_bounds__(32 * SCHUR_WARPS)
         __syncwarp();
         for (int e = lane; e < SS; e += 32) sm.theta[e] = (sm.theta[e] + sm.Qkp1i[e]) + sm.tmp[e];
         __syncwarp();
-        warp_inverse<NS>(sm.theta, 0.f, sm.thetai, lane);
+        if (MODE == 0 || need_pinv) warp_inverse<NS>(sm.theta, 0.f, sm.thetai, lane);
         __syncwarp();
         if (MODE == 0) {
             float *Sprev_right = S + (size_t)S_STRIDE * (j - 1) + 2 * SS;
@@ -228,7 +234,7 @@ __global__ void __launch_bounds__(32 * SCHUR_WARPS)
                 if (r >= cc) {
                     const int t = ((r * (r + 1)) >> 1) + cc;
                     Pk[SS + t] = -sm.theta[e];
-                    Pk[SS + 105 + t] = -sm.thetai[e];
+                    Pk[SS + 105 + t] = need_pinv ? -sm.thetai[e] : 0.f;
                 }
                 if (e < PK - SS - 210) Pk[SS + 210 + e] = 0.f;
             }
@@ -249,7 +255,7 @@ __global__ void __launch_bounds__(32 * SCHUR_WARPS)
 
 cudaError_t launch_schur(int mode, const BatchView &bv, float rho_scalar, const float *G,
                          const float *C, const float *g, const float *c, float *S, float *Pinv, float *gamma,
-                         float *Ginv, float *csc_val, int num_sms, cudaStream_t s)
+                         float *Ginv, double *Ginv64, float *csc_val, int need_pinv, int num_sms, cudaStream_t s)
 {
     if (bv.total_knots <= 0) return cudaSuccess;
     const size_t smem = sizeof(SchurWarpSmem) * SCHUR_WARPS;
@@ -264,7 +270,7 @@ cudaError_t launch_schur(int mode, const BatchView &bv, float rho_scalar, const 
             attr_done[0] = true;
         }
         schur_kernel<0><<<blocks, 32 * SCHUR_WARPS, smem, s>>>(bv, rho_scalar, G, C, g, c, S, Pinv, gamma,
-                                                               Ginv, csc_val);
+                                                               Ginv, Ginv64, csc_val, need_pinv);
         break;
     case 1:
         if (!attr_done[1]) {
@@ -272,7 +278,7 @@ cudaError_t launch_schur(int mode, const BatchView &bv, float rho_scalar, const 
             attr_done[1] = true;
         }
         schur_kernel<1><<<blocks, 32 * SCHUR_WARPS, smem, s>>>(bv, rho_scalar, G, C, g, c, S, Pinv, gamma,
-                                                               Ginv, csc_val);
+                                                               Ginv, Ginv64, csc_val, need_pinv);
         break;
     default:
         if (!attr_done[2]) {
@@ -280,7 +286,7 @@ cudaError_t launch_schur(int mode, const BatchView &bv, float rho_scalar, const 
             attr_done[2] = true;
         }
         schur_kernel<2><<<blocks, 32 * SCHUR_WARPS, smem, s>>>(bv, rho_scalar, G, C, g, c, S, Pinv, gamma,
-                                                               Ginv, csc_val);
+                                                               Ginv, Ginv64, csc_val, need_pinv);
         break;
     }
     return cudaGetLastError();

@@ -79,7 +79,7 @@ typedef struct gpt_solver_config {
     float rho_min;             /* RHO_MIN */
     uint32_t pcg_cluster_size; /* CTAs per instance in the PCG (1,2,4,8,16); 0 = chosen by the library */
     uint32_t pcg_precond;      /* 0: block-Jacobi Pinv (the reference's, oldschur.cuh:926-933);
-                                  1: exact block-tridiagonal LDL^T of each CTA's chunk of knots */
+                                  1 (default): exact block-tridiagonal LDL^T of each CTA's chunk of knots */
 } gpt_solver_config;
 
 /* One sqpSolve's outcome (the reference returns a tuple, toplevel.cuh:502) */
@@ -138,10 +138,10 @@ gpt_status gpt_form_kkt(gpt_handle *h, uint32_t knot_points, const float *d_xu, 
 
 /* form_schur -> gato_form_schur_jacobi (schur.cuh:545-559, oldschur.cuh:518-963).
  * d_Ginv (245N-49) receives (Q+rho I)^-1 and (R+rho I)^-1, which the reference
- * writes over d_G (schur.cuh:236-256). */
+ * writes over d_G (schur.cuh:236-256); d_Ginv64 (optional) the same in FP64. */
 gpt_status gpt_form_schur(gpt_handle *h, uint32_t knot_points, float rho, const float *d_G, const float *d_C,
                           const float *d_g, const float *d_c, float *d_S, float *d_Pinv, float *d_gamma,
-                          float *d_Ginv, gpt_stream_t stream);
+                          float *d_Ginv, double *d_Ginv64, gpt_stream_t stream);
 
 /* form_schur_qdl (schur.cuh:528-542): upper-triangle CSC values (nnz = 196(N-1)+105N) */
 gpt_status gpt_form_schur_csc(gpt_handle *h, uint32_t knot_points, float rho, const float *d_G, const float *d_C,
@@ -159,11 +159,12 @@ gpt_status gpt_pcg(gpt_handle *h, uint32_t knot_points, const float *d_S, const 
                    const float *d_gamma, float *d_lambda, double *d_lambda64, uint32_t max_iter, float exit_tol,
                    uint32_t exit_mode, uint32_t *h_iters, uint8_t *h_maxiter_exit, gpt_stream_t stream);
 
-/* compute_dz (schur.cuh:562-566, oldschur.cuh:966-1105) from Ginv; d_lambda64
- * (optional, FP64) is used instead of d_lambda when given */
-gpt_status gpt_compute_dz(gpt_handle *h, uint32_t knot_points, const float *d_Ginv, const float *d_C,
-                          const float *d_g, const float *d_lambda, const double *d_lambda64, float *d_dz,
-                          gpt_stream_t stream);
+/* compute_dz (schur.cuh:562-566, oldschur.cuh:966-1105) from Ginv; the FP64
+ * inputs d_Ginv64 / d_lambda64 (optional) are used instead of the FP32 ones
+ * when given */
+gpt_status gpt_compute_dz(gpt_handle *h, uint32_t knot_points, const float *d_Ginv, const double *d_Ginv64,
+                          const float *d_C, const float *d_g, const float *d_lambda, const double *d_lambda64,
+                          float *d_dz, gpt_stream_t stream);
 
 /* compute_merit (merit.cuh:99-145): merit of d_xu -> *d_merit (one float) */
 gpt_status gpt_compute_merit(gpt_handle *h, uint32_t knot_points, const float *d_xu, const float *d_eePos_traj,
