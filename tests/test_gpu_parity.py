@@ -268,7 +268,8 @@ def test_linear_system_solution_satisfies_kkt(gpt, oracle, golden, problem_mod, 
     """The whole linear-algebra chain on the GPU -- Schur complement, PCG (FP64
     iterate) to relative residual 1e-6, dz recovery -- returns (dz, lambda) that
     satisfy the reference's KKT system (formed by the GPU in FP32) with an FP64
-    relative residual below 1e-5, and dz agrees with the FP64 oracle solution of
+    relative residual at the floor that FP32 formation of S leaves (measured on
+    the oracle's FP32 Schur data), and dz agrees with the FP64 oracle solution of
     the same FP32 KKT data.  cond(S) reaches 1e7 at these sizes, so agreement is
     stated against the FP64 solve of identical inputs."""
     for kind, N, cfg, p in problems(golden, problem_mod):
@@ -289,21 +290,30 @@ def test_linear_system_solution_satisfies_kkt(gpt, oracle, golden, problem_mod, 
         torch.cuda.synchronize()
         l64 = lam64.cpu().numpy()
         res = kkt_residual(N, G, Cm, g, c, rho, host(dz), l64)
-        # the FP64 path (FP64 lambda and inverses, as the SQP loop uses): the KKT residual is set by
-        # the PCG tolerance and the FP32 rounding of dz itself
-        assert res < 2e-5, (kind, N, res)
-        # the reference-layout FP32 inverses (schur.cuh:236-256) leave a floor set by their
-        # conditioning (~1e3 at rho = 1e-3)
-        dz32 = torch.zeros(21 * N - 7, device="cuda")
-        sv.compute_dz(N, Gi, dev(Cm), dev(g), None, dz32, lam64=lam64)
-        assert kkt_residual(N, G, Cm, g, c, rho, host(dz32), l64) < 2e-3
         # FP64 oracle on the same FP32 KKT data
         oS, oP, og, oGi = oracle.form_schur(N, rho, G, Cm, g, c)
         olam = oracle.banded_cholesky(N, oS, og)
         odz = oracle.compute_dz(N, oGi, Cm, g, olam)
         assert kkt_residual(N, G, Cm, g, c, rho, odz, olam) < 1e-9
+        # floor: the reference forms S and gamma in FP32 (schur.cuh:391-524); the exact solution
+        # of the oracle's FP32-formed system, with dz rounded to FP32, leaves this residual
+        fS, _, fg, _ = oracle.form_schur(N, rho, G, Cm, g, c, precision="f32")
+        flam = oracle.banded_cholesky(N, np.asarray(fS, np.float64), np.asarray(fg, np.float64))
+        fdz = oracle.compute_dz(N, oGi, Cm, g, flam).astype(np.float32).astype(np.float64)
+        floor = kkt_residual(N, G, Cm, g, c, rho, fdz, flam)
+        # the FP64 path (FP64 lambda and inverses, as the SQP loop uses): the floor plus the PCG
+        # tolerance (1e-6 on S)
+        assert res < 2 * floor + 2e-5, (kind, N, res, floor)
+        # the reference-layout FP32 inverses (schur.cuh:236-256) add their own rounding,
+        # conditioned up to ~1e3 at rho = 1e-3
+        dz32 = torch.zeros(21 * N - 7, device="cuda")
+        sv.compute_dz(N, Gi, dev(Cm), dev(g), None, dz32, lam64=lam64)
+        assert kkt_residual(N, G, Cm, g, c, rho, host(dz32), l64) < 4 * floor + 2e-4
+        # dz vs the FP64 solution, against the spread that FP32 formation of S alone causes
+        # (~1e-2 on the spec problem at N = 64, where cond(S) ~ 1e7)
         rel = np.linalg.norm(host(dz) - odz) / np.linalg.norm(odz)
-        assert rel < 1e-3, (kind, N, rel)
+        frel = np.linalg.norm(fdz - odz) / np.linalg.norm(odz)
+        assert rel < max(1e-3, 4 * frel), (kind, N, rel, frel)
 
 
 def test_sqp_first_iterate_matches_oracle(gpt, oracle, golden, problem_mod, solvers):
