@@ -32,6 +32,7 @@ EXPORTED = [
     "gpt_set_solver_config", "gpt_last_error", "gpt_version", "gpt_sqp_solve", "gpt_sqp_solve_batched",
     "gpt_form_kkt", "gpt_form_schur", "gpt_form_schur_csc", "gpt_prep_csr", "gpt_pcg", "gpt_compute_dz",
     "gpt_compute_merit", "gpt_ls_compute_merit", "gpt_set_profiling", "gpt_get_phase_stats",
+    "gpt_ls_compute_merit_noalloc",
 ]
 PHASES = ["init", "kkt", "schur", "pcg", "dz", "merit", "accept"]
 
@@ -114,6 +115,7 @@ def _declare(L):
         "gpt_ls_compute_merit": ([vp, u32, vp, vp, vp, vp, vp, vp], C.c_int),
         "gpt_set_profiling": ([vp, C.c_int], C.c_int),
         "gpt_get_phase_stats": ([vp, vp, vp, C.c_int], C.c_int),
+        "gpt_ls_compute_merit_noalloc": ([P(ProblemConfig), u32, vp, vp, vp, vp, vp, vp], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -140,6 +142,17 @@ def default_solver_config(**kw) -> SolverConfig:
     for k, v in kw.items():
         setattr(sc, k, v)
     return sc
+
+
+NOALLOC_MAX_KNOTS = 512  # GPT_NOALLOC_MAX_KNOTS
+
+
+def ls_compute_merit_noalloc(problem: ProblemConfig, N, xs, xu, eePos, dz, out, stream=None):
+    """gpt_ls_compute_merit_noalloc: the 8 line-search merits with no handle and no
+    device allocation (scratch is a fixed 16 KiB array inside the library, shared
+    by every call on a device)."""
+    _check(lib().gpt_ls_compute_merit_noalloc(C.byref(problem), N, _ptr(xs), _ptr(xu), _ptr(eePos), _ptr(dz),
+                                              _ptr(out), _stream(stream)))
 
 
 def _ptr(t):

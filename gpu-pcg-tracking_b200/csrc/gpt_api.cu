@@ -117,6 +117,11 @@ cudaError_t dalloc(T **p, size_t n)
 
 }  // namespace
 
+namespace gpt {
+gpt_status record_error(gpt_status st, const char *msg) { return set_err(st, msg); }
+ProblemParams problem_params(const gpt_problem_config &pc) { return to_params(pc); }
+}  // namespace gpt
+
 extern "C" {
 
 void gpt_default_problem_config(gpt_problem_config *o)

@@ -47,3 +47,12 @@ cudaError_t launch_accept(const BatchView &bv, int mode, const SolverParams &SP,
 cudaError_t launch_init(const BatchView &bv, const float *xu, float *xs, int num_sms, cudaStream_t s);
 
 }  // namespace gpt
+
+#include "../../include/gpt.h"
+
+namespace gpt {
+// for C-ABI entry points defined outside gpt_api.cu: the error text gpt_last_error()
+// returns, and the device-side form of a problem config
+gpt_status record_error(gpt_status st, const char *msg);
+ProblemParams problem_params(const gpt_problem_config &pc);
+}  // namespace gpt

@@ -176,6 +176,23 @@ gpt_status gpt_ls_compute_merit(gpt_handle *h, uint32_t knot_points, const float
                                 const float *d_eePos_traj, const float *d_dz, float *d_merits,
                                 gpt_stream_t stream);
 
+/* The same 8 line-search merits without a handle and without allocating.  No
+ * counterpart in the reference.  For callers that cannot allocate device
+ * memory: a real-time control loop that allocates only at start-up, or a
+ * plug-in whose host framework owns every device allocation (gpt_create
+ * allocates the handle's workspace).  The scratch is a fixed array of
+ * 8 x GPT_NOALLOC_MAX_KNOTS floats (16 KiB) inside the library, held on every
+ * GPU that loads it until the process exits; knot_points above
+ * GPT_NOALLOC_MAX_KNOTS returns GPT_ERR_BAD_ARG.  The first call on each device
+ * looks up the array's device address (cudaGetSymbolAddress) with that device
+ * current; make that first call before any stream capture.  All calls share
+ * the array: calls whose kernels overlap on the GPU (other streams, other host
+ * threads) race.  pc->max_knot_points and max_batch are not used. */
+#define GPT_NOALLOC_MAX_KNOTS 512
+gpt_status gpt_ls_compute_merit_noalloc(const gpt_problem_config *pc, uint32_t knot_points, const float *d_xs,
+                                        const float *d_xu, const float *d_eePos_traj, const float *d_dz,
+                                        float *d_merits, gpt_stream_t stream);
+
 /* ---- instrumentation (no reference counterpart; the reference times with
  * clock_gettime around host syncs, toplevel.cuh:36-38,219-222,286-303) ---- */
 
