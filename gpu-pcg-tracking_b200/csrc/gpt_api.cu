@@ -51,6 +51,7 @@ struct gpt_handle {
     uint32_t *pcg_log = nullptr, *pcg_out = nullptr, *d_active = nullptr;
     double *lam64 = nullptr;   // FP64 multipliers from the PCG, consumed by dz
     double *Ginv64 = nullptr;  // FP64 inverses (Q + rho I)^-1, (R + rho I)^-1 from Schur, consumed by dz
+    double *crw = nullptr;     // FP64 cyclic-reduction couplings of the PCG preconditioner, 196 per knot
     uint32_t cap_sqp_iter = 0;  // pcg_log rows allocated at creation
     // pinned host staging
     uint32_t *h_active = nullptr;
@@ -220,6 +221,7 @@ gpt_status gpt_create(const gpt_problem_config *pc, const gpt_solver_config *sc,
     ALLOC(d_active, 1);
     ALLOC(lam64, NS * T);
     ALLOC(Ginv64, G_STRIDE * T);
+    ALLOC(crw, SS * T);
 #undef ALLOC
     if (e == cudaSuccess) e = cudaMallocHost((void **)&h->h_active, sizeof(uint32_t));
     if (e == cudaSuccess) e = cudaMallocHost((void **)&h->h_st, sizeof(InstState) * B);
@@ -265,7 +267,7 @@ gpt_status gpt_destroy(gpt_handle *h)
     cudaFree(h->G); cudaFree(h->C); cudaFree(h->g); cudaFree(h->c); cudaFree(h->S);
     cudaFree(h->gamma); cudaFree(h->Ginv); cudaFree(h->dz); cudaFree(h->xs); cudaFree(h->knot_merit);
     cudaFree(h->merits); cudaFree(h->st); cudaFree(h->knot_off); cudaFree(h->knot_inst); cudaFree(h->pcg_log);
-    cudaFree(h->pcg_out); cudaFree(h->d_active); cudaFree(h->lam64); cudaFree(h->Ginv64);
+    cudaFree(h->pcg_out); cudaFree(h->d_active); cudaFree(h->lam64); cudaFree(h->Ginv64); cudaFree(h->crw);
     cudaFreeHost(h->h_active); cudaFreeHost(h->h_st); cudaFreeHost(h->h_pcg_out); cudaFreeHost(h->h_pcg_log);
     if (h->ev) cudaEventDestroy(h->ev);
     delete h;
@@ -334,7 +336,7 @@ gpt_status gpt_pcg(gpt_handle *h, uint32_t N, const float *d_S, const float *d_P
     if (!check_n(h, N) || exit_mode > 1) return set_err(GPT_ERR_BAD_ARG, "knot_points/exit_mode out of range");
     if (((uintptr_t)d_S & 15u) != 0) return set_err(GPT_ERR_BAD_ARG, "d_S must be 16-byte aligned");
     cudaStream_t s = (cudaStream_t)stream;
-    GPT_CUDA(launch_pcg(single_view(N), (int)N, (int)N, 0, (int)h->sc.pcg_precond, d_S, d_Pinv, d_gamma, d_lambda, d_lambda64, (int)max_iter, tol,
+    GPT_CUDA(launch_pcg(single_view(N), (int)N, (int)N, 0, (int)h->sc.pcg_precond, d_S, d_Pinv, d_gamma, d_lambda, d_lambda64, h->crw, (int)max_iter, tol,
                         (int)exit_mode, h->pcg_out, nullptr, 0, (int)h->sc.pcg_cluster_size, h->num_sms, s));
     GPT_CUDA(cudaMemcpyAsync(h->h_pcg_out, h->pcg_out, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
     GPT_CUDA(cudaStreamSynchronize(s));
@@ -490,7 +492,7 @@ static gpt_status sqp_run(gpt_handle *h, uint32_t B, const uint32_t *Ns, const f
         }
         {
             PhaseTimer t(h, s, GPT_PHASE_PCG);
-            GPT_CUDA(launch_pcg(bv, maxN, minN, 1, (int)SP.pcg_precond, h->S, nullptr, h->gamma, d_lambda, h->lam64, (int)SP.pcg_max_iter, SP.pcg_tol,
+            GPT_CUDA(launch_pcg(bv, maxN, minN, 1, (int)SP.pcg_precond, h->S, nullptr, h->gamma, d_lambda, h->lam64, h->crw, (int)SP.pcg_max_iter, SP.pcg_tol,
                                 (int)SP.pcg_exit_mode, nullptr, h->pcg_log, (int)SP.sqp_max_iter,
                                 (int)SP.pcg_cluster_size, ns, s));
         }

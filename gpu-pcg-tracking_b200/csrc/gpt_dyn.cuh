@@ -303,7 +303,7 @@ __device__ __forceinline__ bool chol7_factor(const float *M, double *L)
 #pragma unroll
         for (int k = 0; k < j; ++k) d -= L[j + 7 * k] * L[j + 7 * k];
         if (!(d > 0.0)) return false;
-        const double ljj = sqrt(d), inv = 1.0 / ljj;
+        const double ljj = sqrt(d), inv = __drcp_rn(ljj);
         L[j + 7 * j] = ljj;
 #pragma unroll
         for (int i = j + 1; i < 7; ++i) {

@@ -32,9 +32,11 @@ size_t pcg_cluster_smem_bytes(int kpc);
 int pcg_pick_cluster(int maxN, int B, int num_sms, int requested);
 // fmt 0: S and Pinv in the reference 3-block layout; fmt 1: packed rows (PK floats per knot) in S
 // precond 0: block-Jacobi with the given Pinv; 1: exact block-tridiagonal LDL^T of each CTA's chunk
+// cr_ws: FP64 workspace of 196 doubles per knot of the batch (the cyclic-reduction
+// couplings of precond 1; unused by precond 0)
 cudaError_t launch_pcg(const BatchView &bv, int max_n_knots, int min_n_knots, int fmt, int precond, const float *S,
-                       const float *Pinv, const float *gamma, float *lambda, double *lambda64, int max_iter,
-                       float tol, int exit_mode, uint32_t *out_iters, uint32_t *pcg_log, int log_stride,
+                       const float *Pinv, const float *gamma, float *lambda, double *lambda64, double *cr_ws,
+                       int max_iter, float tol, int exit_mode, uint32_t *out_iters, uint32_t *pcg_log, int log_stride,
                        int cluster_size, int num_sms, cudaStream_t s);
 // lambda64 (optional) replaces lambda when given
 cudaError_t launch_dz(const BatchView &bv, const float *Ginv, const double *Ginv64, const float *C, const float *g,

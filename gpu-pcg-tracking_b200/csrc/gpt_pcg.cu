@@ -464,38 +464,47 @@ __global__ void __launch_bounds__(PCG_THREADS, 1)
 }
 
 // ---------------------------------------------------------------------------
-// PCG with the chunk block-tridiagonal LDL^T preconditioner
+// PCG with the chunk block-tridiagonal preconditioner (block cyclic reduction)
 // ---------------------------------------------------------------------------
 //
-// M = -S is symmetric positive definite.  On each CTA's chunk of knots,
-// M_chunk = L D L^T with D_0 = M_00 and D_k = M_kk - M_{k,k-1} D_{k-1}^{-1}
-// M_{k,k-1}^T, where M_{k,k-1} = -left_k.  The factorisation runs once per
-// solve in FP64 (products by the whole CTA, each 14x14 inversion by one warp,
-// Gauss-Jordan with the augmented columns on the lanes) and keeps D_k^{-1} in
-// FP64 in shared memory (packed lower triangle).  The preconditioner solves
-// the chunk exactly: z = S_chunk^{-1} r = -x with
-//   forward   y_k = r_k + left_k w_{k-1},   w_k = D_k^{-1} y_k
-//   backward  x_{K-1} = w_{K-1},  x_k = w_k + D_k^{-1} left_{k+1}^T x_{k+1}
-// on one warp (two half-warps split each 14-term product), in FP64.  With one
-// CTA per instance the preconditioner is the inverse of S up to rounding and
-// the PCG stops after one or two iterations; with several CTAs the chunks are
-// coupled through the iterations.  Chunk size 1 reduces to the reference's
-// block-Jacobi preconditioner.  The diagonal blocks of S are read from global
-// memory (L2) by the matvec; the left blocks live in shared memory.
+// M = -S is symmetric positive definite and block tridiagonal: diagonal
+// blocks A_k = -S_kk, couplings M_{k,k-1} = -L_k with L_k = left_k.  The
+// preconditioner solves each CTA's chunk of K knots exactly, M_chunk x = y,
+// z = S_chunk^{-1} r = -x, by block cyclic reduction (odd-even elimination):
+// at level l (h = 2^l) the knots j = h, 3h, 5h, ... are eliminated from the
+// system on the multiples of h, which leaves a block-tridiagonal system on the
+// multiples of 2h with
+//   A_{j-h} -= L_j^T A_j^{-1} L_j,   A_{j+h} -= L_{j+h} A_j^{-1} L_{j+h}^T,
+//   L'_{j+h} = L_{j+h} A_j^{-1} L_j   (coupling of j+h to j-h at level l+1),
+// until knot 0 is left.  It is Gaussian elimination of an SPD matrix in the
+// odd-even order, so every pivot block is SPD and no pivoting is needed; its
+// depth is log2 K levels instead of the K steps of a sequential LDL^T, and
+// every level's eliminations run in parallel (one warp each).  The factors
+// are FP64: A_j^{-1} in shared memory (packed lower triangle), the level >= 1
+// couplings in a global workspace (L2-resident, K blocks per chunk).  The
+// solve runs the same levels: forward t_j = A_j^{-1} y_j, y_{j-h} += L_j^T t_j,
+// y_{j+h} += L_{j+h} t_j; then x_0 = A_0^{-1} y_0 and backward
+// x_j = t_j + A_j^{-1} (L_j x_{j-h} + L_{j+h}^T x_{j+h}).  With one CTA per
+// instance the preconditioner is the inverse of S up to rounding and the PCG
+// stops after one or two iterations; with several CTAs the chunks are coupled
+// through the iterations.  S (left and diagonal blocks) is read from global
+// memory (L2).
 
 constexpr int CH_SLOTS = 2 * SLOT_CS * 4;
+constexpr int CR_WARP_SCRATCH = 2 * SS;  // two couplings per warp during the factorisation
 
-__host__ __device__ constexpr int chain_rv_doubles(int kpc) { return NS * (kpc + 2) > 2 * SS ? NS * (kpc + 2) : 2 * SS; }
-// doubles ahead of the float region, rounded up so the float region is 16-byte aligned
+// union region: per-warp coupling scratch during the factorisation; then the
+// halo-padded vector rv (14 (K+2)), t (14 K) and s (14 K) of the solve
+__host__ __device__ constexpr int cr_union_doubles(int kpc)
+{
+    return PCG_NWARP * CR_WARP_SCRATCH > NS * (3 * kpc + 2) ? PCG_NWARP * CR_WARP_SCRATCH : NS * (3 * kpc + 2);
+}
 __host__ __device__ constexpr int chain_double_words(int kpc)
 {
-    return ((kpc * 105 + chain_rv_doubles(kpc) + 2 * NS + CH_SLOTS + PCG_NWARP * 4) + 1) & ~1;
+    return kpc * 105 + cr_union_doubles(kpc) + CH_SLOTS + PCG_NWARP * 4;
 }
 
-size_t pcg_chain_smem_bytes(int kpc)
-{
-    return sizeof(double) * (size_t)chain_double_words(kpc) + sizeof(float) * ((size_t)kpc * SS + SS);
-}
+size_t pcg_chain_smem_bytes(int kpc) { return sizeof(double) * (size_t)chain_double_words(kpc); }
 
 __device__ __forceinline__ int tri_lo(int r, int c)  // packed lower-triangle index of (r, c), any order
 {
@@ -511,26 +520,53 @@ __device__ __forceinline__ int diag_off(int r, int c)
     return SS + hi + NS * lo;
 }
 
+// In-place inverse of an SPD 14x14 block held as a packed lower triangle
+// (FP64), by one warp: Gauss-Jordan on [A | I], lanes 0..13 holding A's
+// columns and lanes 14..27 the identity's.
+__device__ __forceinline__ void warp_spd_inverse_packed(double *Ap, int lane)
+{
+    double col[NS];
+    const bool lft = lane < NS, rgt = lane >= NS && lane < 2 * NS;
+#pragma unroll
+    for (int r = 0; r < NS; ++r) col[r] = lft ? Ap[tri_lo(r, lane)] : ((rgt && r == lane - NS) ? 1.0 : 0.0);
+    __syncwarp();
+#pragma unroll
+    for (int p = 0; p < NS; ++p) {
+        double pc[NS];
+#pragma unroll
+        for (int r = 0; r < NS; ++r) pc[r] = __shfl_sync(0xffffffffu, col[r], p);
+        const double prow = col[p] * __drcp_rn(pc[p]);  // correctly rounded reciprocal: ~3x less latency than a divide
+#pragma unroll
+        for (int r = 0; r < NS; ++r) col[r] = (r == p) ? prow : fma(-pc[r], prow, col[r]);
+    }
+    if (rgt) {
+        const int cc = lane - NS;
+#pragma unroll
+        for (int r = 0; r < NS; ++r)
+            if (r >= cc) Ap[((r * (r + 1)) >> 1) + cc] = col[r];
+    }
+    __syncwarp();
+}
+
 // Precision: with an exact preconditioner the search direction must not be
 // rounded to FP32 -- the rounding error of p is amplified by cond(S) (up to
-// ~4e7 here) -- so p, z, S p, lambda and r are all FP64; S and the left
-// blocks stay FP32 (their products are exact in FP64).
+// ~4e7 here) -- so p, z, S p, lambda and r are all FP64; S stays FP32 (its
+// products are exact in FP64).
 template <int CS, int FMT>
 __global__ void __launch_bounds__(PCG_THREADS, 1)
     pcg_chain_kernel(BatchView bv, int kpc_max, const float *__restrict__ S, const float *__restrict__ gamma,
-                     float *__restrict__ lambda, double *__restrict__ lambda64, int max_iter, float tol,
-                     int exit_mode, uint32_t *__restrict__ out_iters, uint32_t *__restrict__ pcg_log,
-                     int log_stride)
+                     float *__restrict__ lambda, double *__restrict__ lambda64, double *__restrict__ cr_ws,
+                     int max_iter, float tol, int exit_mode, uint32_t *__restrict__ out_iters,
+                     uint32_t *__restrict__ pcg_log, int log_stride)
 {
-    extern __shared__ float4 chain_dyn_smem[];
-    double *Dinv = reinterpret_cast<double *>(chain_dyn_smem);  // kpc_max x 105
-    double *rv = Dinv + (size_t)kpc_max * 105;                  // 14 (kpc_max+2) (>= 392): p / r / chain / lambda
-    double *zh_l = rv + chain_rv_doubles(kpc_max);
-    double *zh_r = zh_l + NS;
-    double *slots = zh_r + NS;
+    extern __shared__ double chain_dyn_smem[];
+    double *Aq = chain_dyn_smem;                    // kpc_max x 105: A_k, then A_k^{-1}
+    double *un = Aq + (size_t)kpc_max * 105;         // union region
+    double *rv = un;                                 // 14 (kpc_max+2): p / r / lambda / the solve's y, x
+    double *tv = rv + NS * (kpc_max + 2);            // 14 kpc_max: t_j
+    double *sv = tv + NS * kpc_max;                  // 14 kpc_max: s_j
+    double *slots = un + cr_union_doubles(kpc_max);
     double *red = slots + CH_SLOTS;
-    float *left = reinterpret_cast<float *>(reinterpret_cast<double *>(chain_dyn_smem) + chain_double_words(kpc_max));
-    float *left_next = left + (size_t)kpc_max * SS;
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int b = blockIdx.x / CS;
@@ -542,72 +578,164 @@ __global__ void __launch_bounds__(PCG_THREADS, 1)
     const int kpc_left = (rank > 0) ? k0 - ((rank - 1) * N) / CS : 0;
     const size_t kg0 = (size_t)kb + k0;
     const size_t kstride = FMT == 1 ? PK : S_STRIDE;
+    int nlev = 0;
+    while ((1 << nlev) < kpc) ++nlev;
 
-    // ---- stage the left blocks of the chunk and of knot k1 (rows are 16-byte aligned: 196 floats)
-    for (int i = tid; i < kpc * (SS / 4); i += PCG_THREADS) {
-        const int kl = i / (SS / 4), e4 = i - kl * (SS / 4);
-        reinterpret_cast<float4 *>(left)[i] = reinterpret_cast<const float4 *>(S + (kg0 + kl) * kstride)[e4];
+    // level-l coupling of local knot k (a multiple of 2^l, k >= 2^l) to k - 2^l, column-major:
+    // level 0 is the left block of S, levels >= 1 live in the workspace
+    auto lev_block = [&](int l, int k) -> double * {
+        int o = 0;
+        for (int q = 1; q < l; ++q) o += (kpc - 1) >> q;
+        return cr_ws + (kg0 + (size_t)o + (size_t)((k >> l) - 1)) * SS;
+    };
+    // row rr (col_major = false: elements (rr, cc)) or column rr (true: (cc, rr)) of a level-l
+    // coupling, all 14 loads issued before use
+    auto coupling_line = [&](int l, int k, int rr, bool column, double (&v)[NS]) {
+        if (l == 0) {
+            const float *src = S + (kg0 + k) * kstride;
+            float f[NS];
+#pragma unroll
+            for (int cc = 0; cc < NS; ++cc) f[cc] = __ldg(src + (column ? cc + NS * rr : rr + NS * cc));
+#pragma unroll
+            for (int cc = 0; cc < NS; ++cc) v[cc] = (double)f[cc];
+        } else {
+            const double *src = lev_block(l, k);
+#pragma unroll
+            for (int cc = 0; cc < NS; ++cc) v[cc] = src[column ? cc + NS * rr : rr + NS * cc];
+        }
+    };
+
+    // ---- A_k = -S_kk (FP64, packed lower triangle); loads issued in groups of 8 before the stores
+    {
+        constexpr int G = 8;
+        for (int i0 = tid; i0 < kpc * 105; i0 += G * PCG_THREADS) {
+            float v[G];
+#pragma unroll
+            for (int q = 0; q < G; ++q) {
+                const int i = i0 + q * PCG_THREADS;
+                v[q] = 0.f;
+                if (i < kpc * 105) {
+                    const int kl = i / 105, t = i - kl * 105;
+                    if (FMT == 1) {
+                        v[q] = __ldg(S + (kg0 + kl) * kstride + PK_DIAG + t);  // same packed order
+                    } else {
+                        int rr = 0;
+                        while (((rr + 1) * (rr + 2)) / 2 <= t) ++rr;
+                        const int cc = t - (rr * (rr + 1)) / 2;
+                        v[q] = __ldg(S + (kg0 + kl) * kstride + diag_off<FMT>(rr, cc));
+                    }
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < G; ++q) {
+                const int i = i0 + q * PCG_THREADS;
+                if (i < kpc * 105) Aq[i] = -(double)v[q];
+            }
+        }
     }
-    for (int i = tid; i < SS; i += PCG_THREADS) left_next[i] = (k1 < N) ? S[((size_t)kb + k1) * kstride + i] : 0.f;
     __syncthreads();
 
-    // ---- factorisation of the chunk: D_kl^{-1}, FP64
+    // ---- factorisation by levels; warp w eliminates knots j = h (2m+1), m = w, w+16, ...
     {
-        double *Tsc = rv, *Dsc = rv + SS;
-        const int ei = tid % NS, ej = tid / NS;  // column-major element (ei, ej) for tid < 196
-        float dnext = 0.f;
-        if (tid < SS) dnext = S[kg0 * kstride + diag_off<FMT>(ei, ej)];
-        for (int kl = 0; kl < kpc; ++kl) {
-            double Dv = 0.0;
-            if (tid < SS) {
-                Dv = -(double)dnext;
-                if (kl + 1 < kpc) dnext = S[(kg0 + kl + 1) * kstride + diag_off<FMT>(ei, ej)];  // prefetch
-            }
-            if (kl > 0) {
-                const float *lk = left + (size_t)kl * SS;
-                const double *Dp = Dinv + (size_t)(kl - 1) * 105;
-                if (tid < SS) {
-                    double a = 0.0;
+        double *Lw0 = un + (size_t)warp * CR_WARP_SCRATCH, *Lw1 = Lw0 + SS;
+        const int c = lane >> 1, hh = lane & 1;
+        const bool cval = c < NS;
+        const int cq = cval ? c : NS - 1;
+        // a coupling into the warp's scratch (FP64); all 7 loads per lane issued before the stores
+        auto stage = [&](double *dst, int l, int k) {
+            double v[7];
+            if (l == 0) {
+                const float *src = S + (kg0 + k) * kstride;
 #pragma unroll
-                    for (int t = 0; t < NS; ++t) a = fma((double)lk[ei + NS * t], Dp[tri_lo(t, ej)], a);
-                    Tsc[tid] = a;  // T = left_k D_{k-1}^{-1}
-                }
-                __syncthreads();
-                if (tid < SS) {
-                    double a = 0.0;
+                for (int q = 0; q < 7; ++q) v[q] = (lane + 32 * q < SS) ? (double)__ldg(src + lane + 32 * q) : 0.0;
+            } else {
+                const double *src = lev_block(l, k);
 #pragma unroll
-                    for (int t = 0; t < NS; ++t) a = fma(Tsc[ei + NS * t], (double)lk[ej + NS * t], a);
-                    Dv -= a;  // D_k = M_kk - left_k D_{k-1}^{-1} left_k^T
-                }
+                for (int q = 0; q < 7; ++q) v[q] = (lane + 32 * q < SS) ? src[lane + 32 * q] : 0.0;
             }
-            if (tid < SS) Dsc[tid] = Dv;
+#pragma unroll
+            for (int q = 0; q < 7; ++q)
+                if (lane + 32 * q < SS) dst[lane + 32 * q] = v[q];
+        };
+        // w[q] = (A_j^{-1} X)(7 hh + q, c) for X = Lw (x_cm: X(t, c) = Lw[t + 14 c]) or X = Lw^T
+        auto ainv_times = [&](const double *Ai, const double *Lw, bool transpose, double (&w)[7]) {
+            double xc[NS];
+#pragma unroll
+            for (int t = 0; t < NS; ++t) xc[t] = transpose ? Lw[cq + NS * t] : Lw[t + NS * cq];
+#pragma unroll
+            for (int q = 0; q < 7; ++q) {
+                const int rr = 7 * hh + q;
+                double a = 0.0;
+#pragma unroll
+                for (int t = 0; t < NS; ++t) a = fma(Ai[tri_lo(rr, t)], xc[t], a);
+                w[q] = a;
+            }
+        };
+        // d[a] = (Y W)(a, c) with Y(a, t) = Lw[a + 14 t] (transpose: Lw[t + 14 a]); both lanes of a pair get the sum
+        auto times_w = [&](const double *Lw, bool transpose, const double (&w)[7], double (&d)[NS]) {
+#pragma unroll
+            for (int a = 0; a < NS; ++a) {
+                double acc = 0.0;
+#pragma unroll
+                for (int q = 0; q < 7; ++q) {
+                    const int t = 7 * hh + q;
+                    acc = fma(transpose ? Lw[t + NS * a] : Lw[a + NS * t], w[q], acc);
+                }
+                d[a] = acc + __shfl_xor_sync(0xffffffffu, acc, 1);
+            }
+        };
+        for (int l = 0; l < nlev; ++l) {
+            const int h = 1 << l;
+            const int ne = (kpc - 1 - h) / (2 * h) + 1;
+            // phase A: invert A_j; A_{j-h} -= L_j^T A_j^{-1} L_j
+            for (int m = warp; m < ne; m += PCG_NWARP) {
+                const int j = h * (2 * m + 1);
+                stage(Lw0, l, j);
+                double *Ai = Aq + (size_t)j * 105;
+                warp_spd_inverse_packed(Ai, lane);
+                double w[7], d[NS];
+                ainv_times(Ai, Lw0, false, w);
+                times_w(Lw0, true, w, d);
+                double *Ad = Aq + (size_t)(j - h) * 105;
+                if (cval) {
+#pragma unroll
+                    for (int a = 0; a < NS; ++a)
+                        if (a >= c && (a & 1) == hh) Ad[((a * (a + 1)) >> 1) + c] -= d[a];
+                }
+                __syncwarp();
+            }
             __syncthreads();
-            if (warp == 0) {
-                // Gauss-Jordan on [D | I]: lanes 0..13 hold D's columns, 14..27 the identity's
-                double col[NS];
-                const bool lft = lane < NS, rgt = lane >= NS && lane < 2 * NS;
+            // phase B: L'_{j+h} = L_{j+h} A_j^{-1} L_j; A_{j+h} -= L_{j+h} A_j^{-1} L_{j+h}^T
+            for (int m = warp; m < ne; m += PCG_NWARP) {
+                const int j = h * (2 * m + 1);
+                if (j + h >= kpc) continue;
+                stage(Lw0, l, j);
+                stage(Lw1, l, j + h);
+                __syncwarp();
+                const double *Ai = Aq + (size_t)j * 105;
+                double w[7], d[NS];
+                ainv_times(Ai, Lw0, false, w);
+                times_w(Lw1, false, w, d);
+                double *Ln = lev_block(l + 1, j + h);
+                if (cval) {
 #pragma unroll
-                for (int r = 0; r < NS; ++r)
-                    col[r] = lft ? Dsc[r + NS * lane] : ((rgt && r == lane - NS) ? 1.0 : 0.0);
-#pragma unroll
-                for (int p = 0; p < NS; ++p) {
-                    double pc[NS];
-#pragma unroll
-                    for (int r = 0; r < NS; ++r) pc[r] = __shfl_sync(0xffffffffu, col[r], p);
-                    const double prow = col[p] / pc[p];
-#pragma unroll
-                    for (int r = 0; r < NS; ++r) col[r] = (r == p) ? prow : fma(-pc[r], prow, col[r]);
+                    for (int a = 0; a < NS; ++a)
+                        if ((a & 1) == hh) Ln[a + NS * c] = d[a];
                 }
-                if (rgt) {
-                    const int cc = lane - NS;
-                    double *Dk = Dinv + (size_t)kl * 105;
+                ainv_times(Ai, Lw1, true, w);
+                times_w(Lw1, false, w, d);
+                double *Ad = Aq + (size_t)(j + h) * 105;
+                if (cval) {
 #pragma unroll
-                    for (int r = 0; r < NS; ++r)
-                        if (r >= cc) Dk[((r * (r + 1)) >> 1) + cc] = col[r];
+                    for (int a = 0; a < NS; ++a)
+                        if (a >= c && (a & 1) == hh) Ad[((a * (a + 1)) >> 1) + c] -= d[a];
                 }
+                __syncwarp();
             }
             __syncthreads();
         }
+        if (warp == 0) warp_spd_inverse_packed(Aq, lane);
+        __syncthreads();
     }
 
     // ---- per-thread rows
@@ -635,20 +763,21 @@ __global__ void __launch_bounds__(PCG_THREADS, 1)
     // (S x)_row with FP64 accumulation; x = rv holds 14 (kpc+2) doubles with halo slots
     auto row_f64 = [&](int j) -> double {
         const int kl = g0 + PCG_TK * j, k = k0 + kl;
-        const float *lk = left + (size_t)kl * SS;
-        const float *dg = S + (kg0 + kl) * kstride;
+        const float *lk = S + (kg0 + kl) * kstride;
         const double *xk = rv + NS * kl;
-        double a0 = 0.0, a1 = 0.0, a2 = 0.0;
-        if (k > 0) {
+        float fl[NS], fd[NS], fr[NS];
 #pragma unroll
-            for (int cc = 0; cc < NS; ++cc) a0 = fma((double)lk[r + NS * cc], xk[cc], a0);
+        for (int cc = 0; cc < NS; ++cc) {
+            fl[cc] = (k > 0) ? __ldg(lk + r + NS * cc) : 0.f;
+            fd[cc] = __ldg(lk + doff[cc]);
+            fr[cc] = (k < N - 1) ? __ldg(lk + kstride + cc + NS * r) : 0.f;
         }
+        double a0 = 0.0, a1 = 0.0, a2 = 0.0;
 #pragma unroll
-        for (int cc = 0; cc < NS; ++cc) a1 = fma((double)__ldg(dg + doff[cc]), xk[NS + cc], a1);
-        if (k < N - 1) {
-            const float *ln = (kl + 1 < kpc) ? lk + SS : left_next;
-#pragma unroll
-            for (int cc = 0; cc < NS; ++cc) a2 = fma((double)ln[cc + NS * r], xk[2 * NS + cc], a2);
+        for (int cc = 0; cc < NS; ++cc) {
+            a0 = fma((double)fl[cc], xk[cc], a0);
+            a1 = fma((double)fd[cc], xk[NS + cc], a1);
+            a2 = fma((double)fr[cc], xk[2 * NS + cc], a2);
         }
         return (a0 + a1) + a2;
     };
@@ -699,57 +828,75 @@ __global__ void __launch_bounds__(PCG_THREADS, 1)
             if (own[j]) res[j] = (double)gv[j] - row_f64(j);
         release();
     };
-    // exact chunk solve on warp 0, in place on rv (interior slots): rv <- M_chunk^{-1} rv
+    // exact chunk solve by all threads, in place on rv's interior slots: rv <- M_chunk^{-1} rv
     auto chain_solve = [&]() {
-        if (warp != 0) return;
-        const int rr = lane & 15, h = lane >> 4;
-        const int rc = rr < NS ? rr : NS - 1;
-        double wprev = 0.0;
-        for (int kl = 0; kl < kpc; ++kl) {
-            double y = rv[NS * (kl + 1) + rc];
-            if (kl > 0) {
-                const float *lk = left + (size_t)kl * SS;
-                double t = 0.0;
+        for (int l = 0; l < nlev; ++l) {
+            const int h = 1 << l;
+            const int ne = (kpc - 1 - h) / (2 * h) + 1, ns = (kpc - 1) / (2 * h) + 1;
+            for (int i = tid; i < ne * NS; i += PCG_THREADS) {
+                const int m = i / NS, rr = i - m * NS, j = h * (2 * m + 1);
+                const double *Ai = Aq + (size_t)j * 105, *y = rv + NS * (j + 1);
+                double a = 0.0;
 #pragma unroll
-                for (int q = 0; q < 7; ++q) {
-                    const int cc = 7 * h + q;
-                    t = fma((double)lk[rc + NS * cc], __shfl_sync(0xffffffffu, wprev, cc), t);
+                for (int cc = 0; cc < NS; ++cc) a = fma(Ai[tri_lo(rr, cc)], y[cc], a);
+                tv[NS * j + rr] = a;
+            }
+            __syncthreads();
+            for (int i = tid; i < ns * NS; i += PCG_THREADS) {
+                const int m = i / NS, rr = i - m * NS, k = 2 * h * m;
+                double a = 0.0, cl[NS];
+                if (k > 0) {
+                    coupling_line(l, k, rr, false, cl);
+                    const double *t = tv + NS * (k - h);
+#pragma unroll
+                    for (int cc = 0; cc < NS; ++cc) a = fma(cl[cc], t[cc], a);
                 }
-                t += __shfl_xor_sync(0xffffffffu, t, 16);
-                y += t;
-            }
-            const double *Dk = Dinv + (size_t)kl * 105;
-            double u = 0.0;
+                if (k + h < kpc) {
+                    coupling_line(l, k + h, rr, true, cl);
+                    const double *t = tv + NS * (k + h);
 #pragma unroll
-            for (int q = 0; q < 7; ++q) {
-                const int cc = 7 * h + q;
-                u = fma(Dk[tri_lo(rc, cc)], __shfl_sync(0xffffffffu, y, cc), u);
+                    for (int cc = 0; cc < NS; ++cc) a = fma(cl[cc], t[cc], a);
+                }
+                rv[NS * (k + 1) + rr] += a;
             }
-            u += __shfl_xor_sync(0xffffffffu, u, 16);
-            if (rr < NS && h == 0) rv[NS * (kl + 1) + rr] = u;
-            wprev = u;
+            __syncthreads();
         }
-        double xnext = wprev;
-        for (int kl = kpc - 2; kl >= 0; --kl) {
-            const float *ln = left + (size_t)(kl + 1) * SS;
-            double sv = 0.0;
+        double x0 = 0.0;
+        if (tid < NS) {
 #pragma unroll
-            for (int q = 0; q < 7; ++q) {
-                const int cc = 7 * h + q;
-                sv = fma((double)ln[cc + NS * rc], __shfl_sync(0xffffffffu, xnext, cc), sv);
-            }
-            sv += __shfl_xor_sync(0xffffffffu, sv, 16);
-            const double *Dk = Dinv + (size_t)kl * 105;
-            double v = 0.0;
+            for (int cc = 0; cc < NS; ++cc) x0 = fma(Aq[tri_lo(tid, cc)], rv[NS + cc], x0);
+        }
+        __syncthreads();
+        if (tid < NS) rv[NS + tid] = x0;
+        __syncthreads();
+        for (int l = nlev - 1; l >= 0; --l) {
+            const int h = 1 << l;
+            const int ne = (kpc - 1 - h) / (2 * h) + 1;
+            for (int i = tid; i < ne * NS; i += PCG_THREADS) {
+                const int m = i / NS, rr = i - m * NS, j = h * (2 * m + 1);
+                const double *xl = rv + NS * (j - h + 1);
+                double a = 0.0, cl[NS];
+                coupling_line(l, j, rr, false, cl);
 #pragma unroll
-            for (int q = 0; q < 7; ++q) {
-                const int cc = 7 * h + q;
-                v = fma(Dk[tri_lo(rc, cc)], __shfl_sync(0xffffffffu, sv, cc), v);
+                for (int cc = 0; cc < NS; ++cc) a = fma(cl[cc], xl[cc], a);
+                if (j + h < kpc) {
+                    coupling_line(l, j + h, rr, true, cl);
+                    const double *xr = rv + NS * (j + h + 1);
+#pragma unroll
+                    for (int cc = 0; cc < NS; ++cc) a = fma(cl[cc], xr[cc], a);
+                }
+                sv[NS * j + rr] = a;
             }
-            v += __shfl_xor_sync(0xffffffffu, v, 16);
-            const double x = rv[NS * (kl + 1) + rc] + v;
-            if (rr < NS && h == 0) rv[NS * (kl + 1) + rr] = x;
-            xnext = x;
+            __syncthreads();
+            for (int i = tid; i < ne * NS; i += PCG_THREADS) {
+                const int m = i / NS, rr = i - m * NS, j = h * (2 * m + 1);
+                const double *Ai = Aq + (size_t)j * 105, *sj = sv + NS * j;
+                double a = tv[NS * j + rr];
+#pragma unroll
+                for (int cc = 0; cc < NS; ++cc) a = fma(Ai[tri_lo(rr, cc)], sj[cc], a);
+                rv[NS * (j + 1) + rr] = a;
+            }
+            __syncthreads();
         }
     };
     // z = S_chunk^{-1} r, partial dot products
@@ -825,21 +972,38 @@ __global__ void __launch_bounds__(PCG_THREADS, 1)
             true_residual(false);
             replaced = true;
         }
+        if (exit_mode == 0) {
+            // ||r|| <= tol ||gamma||: tested before preconditioning and confirmed on the true
+            // residual, so the exact chunk solve runs only while the iteration continues
+            double d0[1] = {0.0};
+#pragma unroll
+            for (int j = 0; j < PCG_KPT; ++j)
+                if (own[j]) d0[0] += res[j] * res[j];
+            cluster_sum_raw<CS, 1>(d0, slots, red, set);
+            set ^= 1;
+            if (!isfinite(d0[0])) {
+                bad = true;
+                break;
+            }
+            if (converged(0.0, d0[0]) && !replaced) {
+                true_residual(false);
+                d0[0] = 0.0;
+#pragma unroll
+                for (int j = 0; j < PCG_KPT; ++j)
+                    if (own[j]) d0[0] += res[j] * res[j];
+                cluster_sum_raw<CS, 1>(d0, slots, red, set);
+                set ^= 1;
+            }
+            if (converged(0.0, d0[0])) {
+                conv = true;
+                break;
+            }
+        }
         double d2[3] = {0.0, 0.0, 0.0};
         precond(d2);
         cluster_sum_raw<CS, 3>(d2, slots, red, set);
         set ^= 1;
-        conv = converged(d2[1], d2[2]);
-        if (conv && exit_mode == 0 && !replaced) {
-            true_residual(false);
-            double d3[3] = {0.0, 0.0, 0.0};
-            precond(d3);
-            cluster_sum_raw<CS, 3>(d3, slots, red, set);
-            set ^= 1;
-            d2[1] = d3[1];
-            d2[2] = d3[2];
-            conv = converged(d2[1], d2[2]);
-        }
+        if (exit_mode != 0) conv = converged(d2[1], d2[2]);
         if (!isfinite(d2[1])) {
             bad = true;
             conv = false;
@@ -929,8 +1093,9 @@ static cudaError_t launch_pcg_cs(const BatchView &bv, int kpc_max, const float *
 
 template <int CS, int FMT>
 static cudaError_t launch_pcg_chain_cs(const BatchView &bv, int kpc_max, const float *S, const float *gamma,
-                                       float *lambda, double *lambda64, int max_iter, float tol, int exit_mode,
-                                       uint32_t *out_iters, uint32_t *pcg_log, int log_stride, cudaStream_t s)
+                                       float *lambda, double *lambda64, double *cr_ws, int max_iter, float tol,
+                                       int exit_mode, uint32_t *out_iters, uint32_t *pcg_log, int log_stride,
+                                       cudaStream_t s)
 {
     auto kern = pcg_chain_kernel<CS, FMT>;
     const size_t smem = pcg_chain_smem_bytes(kpc_max);
@@ -956,16 +1121,17 @@ static cudaError_t launch_pcg_chain_cs(const BatchView &bv, int kpc_max, const f
     attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, kern, bv, kpc_max, S, gamma, lambda, lambda64, max_iter, tol, exit_mode, out_iters,
-                              pcg_log, log_stride);
+    return cudaLaunchKernelEx(&cfg, kern, bv, kpc_max, S, gamma, lambda, lambda64, cr_ws, max_iter, tol, exit_mode,
+                              out_iters, pcg_log, log_stride);
 }
 
 cudaError_t launch_pcg(const BatchView &bv, int max_n_knots, int min_n_knots, int fmt, int precond, const float *S,
-                       const float *Pinv, const float *gamma, float *lambda, double *lambda64, int max_iter,
-                       float tol, int exit_mode, uint32_t *out_iters, uint32_t *pcg_log, int log_stride,
+                       const float *Pinv, const float *gamma, float *lambda, double *lambda64, double *cr_ws,
+                       int max_iter, float tol, int exit_mode, uint32_t *out_iters, uint32_t *pcg_log, int log_stride,
                        int cluster_size, int num_sms, cudaStream_t s)
 {
     if (bv.B <= 0) return cudaSuccess;
+    if (precond == 1 && !cr_ws) return cudaErrorInvalidValue;
     if (max_n_knots > MAX_PCG_KNOTS) return cudaErrorInvalidValue;
     int cs = (precond == 1 && cluster_size == 0) ? 1 : pcg_pick_cluster(max_n_knots, bv.B, num_sms, cluster_size);
     while ((max_n_knots + cs - 1) / cs > PCG_KPC_MAX) cs *= 2;
@@ -975,10 +1141,10 @@ cudaError_t launch_pcg(const BatchView &bv, int max_n_knots, int min_n_knots, in
 #define GPT_PCG_CASE(CSV)                                                                                      \
     case CSV:                                                                                                  \
         if (precond == 1)                                                                                      \
-            return fmt ? launch_pcg_chain_cs<CSV, 1>(bv, kpc_max, S, gamma, lambda, lambda64, max_iter, tol,   \
-                                                     exit_mode, out_iters, pcg_log, log_stride, s)             \
-                       : launch_pcg_chain_cs<CSV, 0>(bv, kpc_max, S, gamma, lambda, lambda64, max_iter, tol,   \
-                                                     exit_mode, out_iters, pcg_log, log_stride, s);            \
+            return fmt ? launch_pcg_chain_cs<CSV, 1>(bv, kpc_max, S, gamma, lambda, lambda64, cr_ws, max_iter, \
+                                                     tol, exit_mode, out_iters, pcg_log, log_stride, s)        \
+                       : launch_pcg_chain_cs<CSV, 0>(bv, kpc_max, S, gamma, lambda, lambda64, cr_ws, max_iter, \
+                                                     tol, exit_mode, out_iters, pcg_log, log_stride, s);       \
         return fmt ? launch_pcg_cs<CSV, 1>(bv, kpc_max, S, Pinv, gamma, lambda, lambda64, max_iter, tol,       \
                                            exit_mode, out_iters, pcg_log, log_stride, s)                       \
                    : launch_pcg_cs<CSV, 0>(bv, kpc_max, S, Pinv, gamma, lambda, lambda64, max_iter, tol,       \

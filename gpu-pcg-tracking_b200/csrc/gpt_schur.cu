@@ -43,7 +43,7 @@ __device__ __forceinline__ void warp_inverse(const float *A, float shift, float 
         double pc[n];
 #pragma unroll
         for (int r = 0; r < n; ++r) pc[r] = __shfl_sync(0xffffffffu, col[r], p);
-        const double prow = col[p] / pc[p];
+        const double prow = col[p] * __drcp_rn(pc[p]);  // correctly rounded reciprocal: ~3x less latency than a divide
 #pragma unroll
         for (int r = 0; r < n; ++r) col[r] = (r == p) ? prow : fma(-pc[r], prow, col[r]);
     }
