@@ -522,22 +522,30 @@ __device__ __forceinline__ int diag_off(int r, int c)
 
 // In-place inverse of an SPD 14x14 block held as a packed lower triangle
 // (FP64), by one warp: Gauss-Jordan on [A | I], lanes 0..13 holding A's
-// columns and lanes 14..27 the identity's.
-__device__ __forceinline__ void warp_spd_inverse_packed(double *Ap, int lane)
+// columns and lanes 14..27 the identity's.  Not inlined: its unrolled body is
+// large, and one shared copy stays in the instruction cache across the
+// factorisation's calls (single-warp calls late in the factorisation otherwise
+// run from cold instruction fetches).
+__device__ __noinline__ void warp_spd_inverse_packed(double *Ap, int lane)
 {
     double col[NS];
     const bool lft = lane < NS, rgt = lane >= NS && lane < 2 * NS;
 #pragma unroll
     for (int r = 0; r < NS; ++r) col[r] = lft ? Ap[tri_lo(r, lane)] : ((rgt && r == lane - NS) ? 1.0 : 0.0);
     __syncwarp();
+    // pivot p: the pivot element first, then each row's element of the pivot column is
+    // broadcast just before it is used, so only the 14 column entries stay live
 #pragma unroll
     for (int p = 0; p < NS; ++p) {
-        double pc[NS];
+        const double piv = __shfl_sync(0xffffffffu, col[p], p);
+        const double prow = col[p] * __drcp_rn(piv);  // correctly rounded reciprocal: ~3x less latency than a divide
 #pragma unroll
-        for (int r = 0; r < NS; ++r) pc[r] = __shfl_sync(0xffffffffu, col[r], p);
-        const double prow = col[p] * __drcp_rn(pc[p]);  // correctly rounded reciprocal: ~3x less latency than a divide
-#pragma unroll
-        for (int r = 0; r < NS; ++r) col[r] = (r == p) ? prow : fma(-pc[r], prow, col[r]);
+        for (int r = 0; r < NS; ++r) {
+            if (r == p) continue;
+            const double pr = __shfl_sync(0xffffffffu, col[r], p);
+            col[r] = fma(-pr, prow, col[r]);
+        }
+        col[p] = prow;
     }
     if (rgt) {
         const int cc = lane - NS;

@@ -38,14 +38,19 @@ __device__ __forceinline__ void warp_inverse(const float *A, float shift, float 
         else if (right) v = (r == lane - n) ? 1.0 : 0.0;
         col[r] = v;
     }
+    // pivot p: the pivot element first, then each row's element of the pivot column is
+    // broadcast just before it is used, so only the 14 column entries stay live
 #pragma unroll
     for (int p = 0; p < n; ++p) {
-        double pc[n];
+        const double piv = __shfl_sync(0xffffffffu, col[p], p);
+        const double prow = col[p] * __drcp_rn(piv);  // correctly rounded reciprocal: ~3x less latency than a divide
 #pragma unroll
-        for (int r = 0; r < n; ++r) pc[r] = __shfl_sync(0xffffffffu, col[r], p);
-        const double prow = col[p] * __drcp_rn(pc[p]);  // correctly rounded reciprocal: ~3x less latency than a divide
-#pragma unroll
-        for (int r = 0; r < n; ++r) col[r] = (r == p) ? prow : fma(-pc[r], prow, col[r]);
+        for (int r = 0; r < n; ++r) {
+            if (r == p) continue;
+            const double pr = __shfl_sync(0xffffffffu, col[r], p);
+            col[r] = fma(-pr, prow, col[r]);
+        }
+        col[p] = prow;
     }
     if (right) {
 #pragma unroll
