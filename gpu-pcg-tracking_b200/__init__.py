@@ -212,6 +212,11 @@ class Solver:
             setattr(self.solver, k, v)
         _check(lib().gpt_set_solver_config(self._h, C.byref(self.solver)))
 
+    def reset_solver(self, **kw):
+        """gpt_default_solver_config, then the given fields."""
+        self.solver = default_solver_config(**kw)
+        _check(lib().gpt_set_solver_config(self._h, C.byref(self.solver)))
+
     def set_profiling(self, enable: bool):
         _check(lib().gpt_set_profiling(self._h, int(bool(enable))))
 

@@ -65,7 +65,7 @@ struct ProblemParams {
     float qd_cost;     // QD_COST
     float r_cost;      // R_COST
     float mu;          // merit penalty (toplevel.cuh:54)
-    int ref_terminal;  // 1: terminal Q,q at x_{N-2} like iiwa_eepos_plant.cuh:399
+    int ref_terminal;  // 1: terminal Q,q at x_{N-2}, target Q_{N-2}[0][0..2], as the reference's kernel computes
 };
 
 __device__ __forceinline__ float warp_sum(float v)

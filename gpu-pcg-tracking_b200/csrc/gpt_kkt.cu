@@ -159,15 +159,28 @@ __global__ void __launch_bounds__(32 * KKT_WARPS) kkt_kernel(BatchView bv, Probl
                 v = P.qd_cost * sm.x[lane];
             }
             sm.qv[0][lane] = v;
-        } else if (terminal && lane >= 16 && lane < 16 + NS) {
+        }
+        __syncwarp();
+        if (terminal && lane >= 16 && lane < 16 + NS) {
             const int i = lane - 16;
             const int which = P.ref_terminal ? 0 : 1;
             const float *xt = P.ref_terminal ? sm.x : sm.xn;
+            // terminal target: goal_{N-1}; in the reference's layout (ref_terminal) the kernel
+            // reserves 6 shared floats for the goal but copies 12 (schur.cuh:413-425), so
+            // goal_{N-1} lands on Q_{N-2}'s first row and is overwritten by q_0 q_j before the
+            // terminal cost call reads it (iiwa_eepos_plant.cuh:396-401)
+            float t0 = sm.goal[6], t1 = sm.goal[7], t2 = sm.goal[8];
+            if (P.ref_terminal) {
+                const float q0 = sm.qv[0][0];
+                t0 = q0 * q0;
+                t1 = q0 * sm.qv[0][1];
+                t2 = q0 * sm.qv[0][2];
+            }
             float v;
             if (i < NQ) {
                 const float *J = sm.J[which];
-                v = P.q_ee * (J[3 * i] * (sm.ee[which][0] - sm.goal[6]) + J[3 * i + 1] * (sm.ee[which][1] - sm.goal[7]) +
-                              J[3 * i + 2] * (sm.ee[which][2] - sm.goal[8]));
+                v = P.q_ee * (J[3 * i] * (sm.ee[which][0] - t0) + J[3 * i + 1] * (sm.ee[which][1] - t1) +
+                              J[3 * i + 2] * (sm.ee[which][2] - t2));
             } else {
                 v = P.qd_cost * xt[i];
             }

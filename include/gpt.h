@@ -65,7 +65,10 @@ typedef struct gpt_problem_config {
     float qd_cost;             /* QD_COST */
     float r_cost;              /* R_COST */
     float mu;                  /* merit penalty, 10 in toplevel.cuh:54 */
-    uint32_t ref_terminal;     /* 1: terminal Q,q at x_{N-2} (iiwa_eepos_plant.cuh:399); 0: at x_{N-1} */
+    uint32_t ref_terminal;     /* 1 (reference): terminal Q,q at x_{N-2} with the target the reference's kernel
+                                  actually reads, Q_{N-2}[0][0..2] (goal_{N-1} is overwritten in its shared
+                                  buffer, schur.cuh:413-425, iiwa_eepos_plant.cuh:396-401);
+                                  0: at x_{N-1} with target goal_{N-1} */
 } gpt_problem_config;
 
 /* SQP / PCG controls (settings.cuh:31-50; pcg_config of GPU-PCG, toplevel.cuh:573-576) */

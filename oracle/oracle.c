@@ -532,8 +532,19 @@ void ORC(form_kkt)(const orc_params *P, int N, const R *xu, const R *goal, const
         cost_grad_hess(P, x, u, goal + 6 * k, Qk, qk, Rk, rk);
         if (k == N - 2) {
             const R *xt = P->ref_terminal ? x : xn;
-            cost_grad_hess(P, xt, NULL, goal + 6 * (k + 1), G + GSTRIDE * (k + 1), g + NX * (k + 1), NULL,
-                           NULL);
+            const R *gt = goal + 6 * (k + 1);
+            R alias[3];
+            if (P->ref_terminal) {
+                /* the reference's kernel reserves 6 shared floats for the goal but copies 12
+                 * (schur.cuh:413-425), so goal_{k+1} lands on Q_k's first row, which the first
+                 * cost call overwrites with q_0 q_j before the terminal call reads its target
+                 * (iiwa_eepos_plant.cuh:396-401): the terminal target is Q_k[0][0..2] */
+                alias[0] = Qk[0];
+                alias[1] = Qk[1];
+                alias[2] = Qk[2];
+                gt = alias;
+            }
+            cost_grad_hess(P, xt, NULL, gt, G + GSTRIDE * (k + 1), g + NX * (k + 1), NULL, NULL);
             for (int i = 0; i < NS; ++i) c[i] = xu[i] - xs[i];
         }
         for (int i = 0; i < SS; ++i) C[CSTRIDE * k + i] = -A[i];

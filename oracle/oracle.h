@@ -32,8 +32,10 @@ typedef struct {
     double qd_cost;     /* QD_COST (iiwa_eepos_plant.cuh:58-60) */
     double r_cost;      /* R_COST  (iiwa_eepos_plant.cuh:62-64) */
     double mu;          /* merit penalty, 10 (toplevel.cuh:54) */
-    int ref_terminal;   /* 1: terminal Q,q evaluated at x_{N-2} as the reference does
-                           (iiwa_eepos_plant.cuh:399); 0: at x_{N-1} */
+    int ref_terminal;   /* 1: terminal Q,q evaluated at x_{N-2} with target Q_{N-2}[0][0..2], as
+                           the reference's kernel computes (goal_{N-1} is overwritten in its shared
+                           buffer: schur.cuh:413-425, iiwa_eepos_plant.cuh:396-401);
+                           0: at x_{N-1} with target goal_{N-1} */
 } orc_params;
 
 typedef struct {
