@@ -35,6 +35,9 @@ sys.path.insert(0, ROOT)
 METRIC = "SQP solves/s @N=128 batched vs plain @rel-res 1e-5"
 SPEC = dict(timestep=0.01, integrator=1, qd_cost=1e-2, r_cost=1e-4)
 PCG_FLOATS_PER_KNOT = 784        # S 588 + Pinv 196 read once per PCG launch (algorithmic)
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one pcg_chain_kernel launch measured by
+# ncu on 148 instances x 128 knots (27.07 MB + 0.50 MB), per knot; it scales with the knots of a launch
+PCG_CHAIN_DRAM_BYTES_PER_KNOT = (27.068e6 + 0.504e6) / (148 * 128)
 PCG_FLOATS_PER_KNOT_ITER = 896   # S, Pinv and 8 vectors x 14 if re-read every PCG iteration (upper bound)
 ALG_FLOATS_PER_KNOT_SQP = 4058   # every materialised SQP-iteration tensor written once, read once
 
@@ -352,7 +355,9 @@ def main():
                    "pcg_precond": precond_name,
                    "l2": "256 MB buffer written between timed steps"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": None, "kernel": pcg_kernel,
+                     "traffic": (PCG_CHAIN_DRAM_BYTES_PER_KNOT * N * B if args.pcg_precond == 1 else None),
+                     "traffic_source": "ncu capture of 148 x 128 knots scaled to the launch's knots",
+                     "kernel": pcg_kernel,
                      "bytes_model": "784 floats per knot per launch (S 588 + Pinv 196 read once)",
                      "stream_bound_gbs": stream_bytes / per_launch_s / 1e9 if per_launch_s > 0 else 0.0,
                      "peak_source": "measured" if mp else "fallback"},
