@@ -32,7 +32,7 @@ EXPORTED = [
     "gpt_set_solver_config", "gpt_last_error", "gpt_version", "gpt_sqp_solve", "gpt_sqp_solve_batched",
     "gpt_form_kkt", "gpt_form_schur", "gpt_form_schur_csc", "gpt_prep_csr", "gpt_pcg", "gpt_compute_dz",
     "gpt_compute_merit", "gpt_ls_compute_merit", "gpt_set_profiling", "gpt_get_phase_stats",
-    "gpt_ls_compute_merit_noalloc",
+    "gpt_ls_compute_merit_noalloc", "gpt_sqp_adjoint",
 ]
 PHASES = ["init", "kkt", "schur", "pcg", "dz", "merit", "accept"]
 
@@ -49,7 +49,8 @@ class SolverConfig(C.Structure):
     """gpt_solver_config (include/gpt.h)."""
     _fields_ = [("sqp_max_iter", C.c_uint32), ("pcg_max_iter", C.c_uint32), ("pcg_exit_tol", C.c_float),
                 ("pcg_exit_mode", C.c_uint32), ("rho_factor", C.c_float), ("rho_max", C.c_float),
-                ("rho_min", C.c_float), ("pcg_cluster_size", C.c_uint32), ("pcg_precond", C.c_uint32)]
+                ("rho_min", C.c_float), ("pcg_cluster_size", C.c_uint32), ("pcg_precond", C.c_uint32),
+                ("schur_fp64", C.c_uint32)]
 
 
 class SqpStats(C.Structure):
@@ -116,6 +117,7 @@ def _declare(L):
         "gpt_set_profiling": ([vp, C.c_int], C.c_int),
         "gpt_get_phase_stats": ([vp, vp, vp, C.c_int], C.c_int),
         "gpt_ls_compute_merit_noalloc": ([P(ProblemConfig), u32, vp, vp, vp, vp, vp, vp], C.c_int),
+        "gpt_sqp_adjoint": ([vp, u32, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -251,6 +253,22 @@ class Solver:
                                            _ptr(xu), C.cast(rr, C.c_void_p), rho_reset, C.cast(sts, C.c_void_p),
                                            _stream(stream)))
         return list(rr), [s.as_dict() for s in sts]
+
+    def sqp_adjoint(self, knot_points: Sequence[int], eePos_traj, xs, xu, rho: Sequence[float], grad_xu_next,
+                    xu_next=None, stream=None):
+        """gpt_sqp_adjoint: gradients of l(xu - dz) at the iterate xu given dl/dxu+.
+        Returns {"goal": [6 per knot], "qd": [B, 7], "r": [B, 7], "q_ee": [B]} (CUDA tensors)."""
+        import torch
+        B = len(knot_points)
+        T = sum(knot_points)
+        Ns = (C.c_uint32 * B)(*knot_points)
+        rr = (C.c_float * B)(*rho)
+        out = {"goal": torch.zeros(6 * T, device=xu.device), "qd": torch.zeros(B, 7, device=xu.device),
+               "r": torch.zeros(B, 7, device=xu.device), "q_ee": torch.zeros(B, device=xu.device)}
+        _check(lib().gpt_sqp_adjoint(self._h, B, C.cast(Ns, C.c_void_p), _ptr(eePos_traj), _ptr(xs), _ptr(xu),
+                                     C.cast(rr, C.c_void_p), _ptr(grad_xu_next), _ptr(xu_next), _ptr(out["goal"]),
+                                     _ptr(out["qd"]), _ptr(out["r"]), _ptr(out["q_ee"]), _stream(stream)))
+        return out
 
     # ---- the reference's kernels, one instance ----
     def form_kkt(self, N, xu, eePos, xs, G, Cm, g, c, stream=None):

@@ -52,6 +52,12 @@ struct gpt_handle {
     double *lam64 = nullptr;   // FP64 multipliers from the PCG, consumed by dz
     double *Ginv64 = nullptr;  // FP64 inverses (Q + rho I)^-1, (R + rho I)^-1 from Schur, consumed by dz
     double *crw = nullptr;     // FP64 cyclic-reduction couplings of the PCG preconditioner, 196 per knot
+    // adjoint workspace: right-hand side, its zero constraint part, gamma, multipliers, mu_z, partials
+    float *adj_h = nullptr, *adj_zero = nullptr, *adj_gamma = nullptr, *adj_lam = nullptr, *adj_mu = nullptr,
+          *adj_part = nullptr;
+    double *adj_lam64 = nullptr;
+    // FP64 Schur rows (PK64 doubles per knot) and right-hand sides for the cyclic-reduction PCG
+    double *S64 = nullptr, *gamma64 = nullptr, *adj_gamma64 = nullptr;
     uint32_t cap_sqp_iter = 0;  // pcg_log rows allocated at creation
     // pinned host staging
     uint32_t *h_active = nullptr;
@@ -96,6 +102,7 @@ SolverParams to_solver(const gpt_solver_config &sc)
     S.rho_min = sc.rho_min;
     S.pcg_cluster_size = sc.pcg_cluster_size;
     S.pcg_precond = sc.pcg_precond;
+    S.schur_fp64 = sc.schur_fp64;
     return S;
 }
 BatchView single_view(uint32_t N)
@@ -153,6 +160,7 @@ void gpt_default_solver_config(gpt_solver_config *o)
     o->rho_min = 1e-3f;
     o->pcg_cluster_size = 0;
     o->pcg_precond = 1;
+    o->schur_fp64 = 1;
 }
 
 const char *gpt_last_error(void) { return g_last_error.c_str(); }
@@ -166,6 +174,7 @@ gpt_status gpt_set_solver_config(gpt_handle *h, const gpt_solver_config *sc)
     if (sc->pcg_cluster_size & (sc->pcg_cluster_size - 1) || sc->pcg_cluster_size > 16)
         return set_err(GPT_ERR_BAD_ARG, "pcg_cluster_size must be 0, 1, 2, 4, 8 or 16");
     if (sc->pcg_precond > 1) return set_err(GPT_ERR_BAD_ARG, "pcg_precond must be 0 or 1");
+    if (sc->schur_fp64 > 1) return set_err(GPT_ERR_BAD_ARG, "schur_fp64 must be 0 or 1");
     if (sc->sqp_max_iter > h->cap_sqp_iter) {
         // pcg log is sized at creation
         return set_err(GPT_ERR_CAPACITY, "sqp_max_iter larger than at creation");
@@ -222,6 +231,16 @@ gpt_status gpt_create(const gpt_problem_config *pc, const gpt_solver_config *sc,
     ALLOC(lam64, NS * T);
     ALLOC(Ginv64, G_STRIDE * T);
     ALLOC(crw, SS * T);
+    ALLOC(adj_h, NX * T);
+    ALLOC(adj_zero, NS * T);
+    ALLOC(adj_gamma, NS * T);
+    ALLOC(adj_lam, NS * T);
+    ALLOC(adj_mu, NX * T);
+    ALLOC(adj_part, adjoint_part_floats() * T);
+    ALLOC(adj_lam64, NS * T);
+    ALLOC(S64, PK64 * T);
+    ALLOC(gamma64, NS * T);
+    ALLOC(adj_gamma64, NS * T);
 #undef ALLOC
     if (e == cudaSuccess) e = cudaMallocHost((void **)&h->h_active, sizeof(uint32_t));
     if (e == cudaSuccess) e = cudaMallocHost((void **)&h->h_st, sizeof(InstState) * B);
@@ -268,6 +287,9 @@ gpt_status gpt_destroy(gpt_handle *h)
     cudaFree(h->gamma); cudaFree(h->Ginv); cudaFree(h->dz); cudaFree(h->xs); cudaFree(h->knot_merit);
     cudaFree(h->merits); cudaFree(h->st); cudaFree(h->knot_off); cudaFree(h->knot_inst); cudaFree(h->pcg_log);
     cudaFree(h->pcg_out); cudaFree(h->d_active); cudaFree(h->lam64); cudaFree(h->Ginv64); cudaFree(h->crw);
+    cudaFree(h->adj_h); cudaFree(h->adj_zero); cudaFree(h->adj_gamma); cudaFree(h->adj_lam); cudaFree(h->adj_mu);
+    cudaFree(h->adj_part); cudaFree(h->adj_lam64);
+    cudaFree(h->S64); cudaFree(h->gamma64); cudaFree(h->adj_gamma64);
     cudaFreeHost(h->h_active); cudaFreeHost(h->h_st); cudaFreeHost(h->h_pcg_out); cudaFreeHost(h->h_pcg_log);
     if (h->ev) cudaEventDestroy(h->ev);
     delete h;
@@ -336,7 +358,7 @@ gpt_status gpt_pcg(gpt_handle *h, uint32_t N, const float *d_S, const float *d_P
     if (!check_n(h, N) || exit_mode > 1) return set_err(GPT_ERR_BAD_ARG, "knot_points/exit_mode out of range");
     if (((uintptr_t)d_S & 15u) != 0) return set_err(GPT_ERR_BAD_ARG, "d_S must be 16-byte aligned");
     cudaStream_t s = (cudaStream_t)stream;
-    GPT_CUDA(launch_pcg(single_view(N), (int)N, (int)N, 0, (int)h->sc.pcg_precond, d_S, d_Pinv, d_gamma, d_lambda, d_lambda64, h->crw, (int)max_iter, tol,
+    GPT_CUDA(launch_pcg(single_view(N), (int)N, (int)N, 0, (int)h->sc.pcg_precond, d_S, d_Pinv, d_gamma, nullptr, d_lambda, d_lambda64, h->crw, (int)max_iter, tol,
                         (int)exit_mode, h->pcg_out, nullptr, 0, (int)h->sc.pcg_cluster_size, h->num_sms, s));
     GPT_CUDA(cudaMemcpyAsync(h->h_pcg_out, h->pcg_out, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
     GPT_CUDA(cudaStreamSynchronize(s));
@@ -429,9 +451,10 @@ static void collect_phase_times(gpt_handle *h)
     h->ev_used = 0;
 }
 
-static gpt_status sqp_run(gpt_handle *h, uint32_t B, const uint32_t *Ns, const float *d_goal, float *d_lambda,
-                          float *d_xu, float *h_rho, float rho_reset, gpt_sqp_stats *h_stats, uint32_t *h_pcg_iters,
-                          uint8_t *h_pcg_exit, cudaStream_t s)
+// Batch layout (knot offsets and owner table, cached), per-instance state (rho
+// from h_rho, active) and the view the kernels take.
+static gpt_status setup_batch(gpt_handle *h, uint32_t B, const uint32_t *Ns, const float *h_rho, float rho_reset,
+                              BatchView &bv, int &maxN_out, int &minN_out, cudaStream_t s)
 {
     if (B == 0 || B > h->pc.max_batch) return set_err(GPT_ERR_CAPACITY, "batch exceeds handle capacity");
     // batch layout
@@ -464,15 +487,31 @@ static gpt_status sqp_run(gpt_handle *h, uint32_t B, const uint32_t *Ns, const f
         st.active = 1;
     }
     GPT_CUDA(cudaMemcpyAsync(h->st, h->h_st, sizeof(InstState) * B, cudaMemcpyHostToDevice, s));
-    BatchView bv;
     bv.B = (int)B;
     bv.total_knots = total;
     bv.knot_off = h->knot_off;
     bv.knot_inst = h->knot_inst;
     bv.st = h->st;
+    maxN_out = maxN;
+    minN_out = minN;
+    return GPT_OK;
+}
+
+static gpt_status sqp_run(gpt_handle *h, uint32_t B, const uint32_t *Ns, const float *d_goal, float *d_lambda,
+                          float *d_xu, float *h_rho, float rho_reset, gpt_sqp_stats *h_stats, uint32_t *h_pcg_iters,
+                          uint8_t *h_pcg_exit, cudaStream_t s)
+{
+    BatchView bv;
+    int maxN = 0, minN = 0;
+    {
+        const gpt_status st = setup_batch(h, B, Ns, h_rho, rho_reset, bv, maxN, minN, s);
+        if (st != GPT_OK) return st;
+    }
     const ProblemParams P = to_params(h->pc);
     const SolverParams SP = to_solver(h->sc);
     const int ns = h->num_sms;
+    const bool f64 = SP.pcg_precond == 1 && SP.schur_fp64;
+    const float *S_rows = f64 ? reinterpret_cast<const float *>(h->S64) : h->S;
 
     {
         PhaseTimer t(h, s, GPT_PHASE_INIT);
@@ -487,12 +526,15 @@ static gpt_status sqp_run(gpt_handle *h, uint32_t B, const uint32_t *Ns, const f
         }
         {
             PhaseTimer t(h, s, GPT_PHASE_SCHUR);
-            GPT_CUDA(launch_schur(1, bv, 0.f, h->G, h->C, h->g, h->c, h->S, nullptr, h->gamma, h->Ginv, h->Ginv64,
-                                  nullptr, SP.pcg_precond == 0 ? 1 : 0, ns, s));
+            if (f64)
+                GPT_CUDA(launch_schur64(bv, h->G, h->C, h->g, h->c, h->S64, h->gamma64, h->Ginv, h->Ginv64, ns, s));
+            else
+                GPT_CUDA(launch_schur(1, bv, 0.f, h->G, h->C, h->g, h->c, h->S, nullptr, h->gamma, h->Ginv,
+                                      h->Ginv64, nullptr, SP.pcg_precond == 0 ? 1 : 0, ns, s));
         }
         {
             PhaseTimer t(h, s, GPT_PHASE_PCG);
-            GPT_CUDA(launch_pcg(bv, maxN, minN, 1, (int)SP.pcg_precond, h->S, nullptr, h->gamma, d_lambda, h->lam64, h->crw, (int)SP.pcg_max_iter, SP.pcg_tol,
+            GPT_CUDA(launch_pcg(bv, maxN, minN, f64 ? 2 : 1, (int)SP.pcg_precond, S_rows, nullptr, h->gamma, h->gamma64, d_lambda, h->lam64, h->crw, (int)SP.pcg_max_iter, SP.pcg_tol,
                                 (int)SP.pcg_exit_mode, nullptr, h->pcg_log, (int)SP.sqp_max_iter,
                                 (int)SP.pcg_cluster_size, ns, s));
         }
@@ -564,6 +606,71 @@ gpt_status gpt_sqp_solve_batched(gpt_handle *h, uint32_t B, const uint32_t *h_N,
     if (!h || !h_N || !d_goal || !d_lambda || !d_xu) return set_err(GPT_ERR_BAD_ARG, "null argument");
     return sqp_run(h, B, h_N, d_goal, d_lambda, d_xu, h_rho, rho_reset, h_stats, nullptr, nullptr,
                    (cudaStream_t)stream);
+}
+
+gpt_status gpt_sqp_adjoint(gpt_handle *h, uint32_t B, const uint32_t *h_N, const float *d_goal, const float *d_xs,
+                           const float *d_xu, const float *h_rho, const float *d_grad_xu_next, float *d_xu_next,
+                           float *d_grad_goal, float *d_grad_qd, float *d_grad_r, float *d_grad_q_ee,
+                           gpt_stream_t stream)
+{
+    if (!h || !h_N || !d_goal || !d_xs || !d_xu || !h_rho || !d_grad_xu_next || !d_grad_goal || !d_grad_qd ||
+        !d_grad_r || !d_grad_q_ee)
+        return set_err(GPT_ERR_BAD_ARG, "null argument");
+    cudaStream_t s = (cudaStream_t)stream;
+    BatchView bv;
+    int maxN = 0, minN = 0;
+    {
+        const gpt_status st = setup_batch(h, B, h_N, h_rho, h_rho[0], bv, maxN, minN, s);
+        if (st != GPT_OK) return st;
+    }
+    const ProblemParams P = to_params(h->pc);
+    const SolverParams SP = to_solver(h->sc);
+    const int ns = h->num_sms, T = bv.total_knots, nz = NX * T - NC;
+    const bool f64 = SP.pcg_precond == 1 && SP.schur_fp64;
+    const float *S_rows = f64 ? reinterpret_cast<const float *>(h->S64) : h->S;
+    const int fmt = f64 ? 2 : 1;
+    GPT_CUDA(cudaMemcpyAsync(h->xs, d_xs, sizeof(float) * NS * B, cudaMemcpyDeviceToDevice, s));
+    // ---- the step at xu: K [dz; lambda] = [g; c]
+    GPT_CUDA(launch_kkt(bv, P, d_xu, d_goal, h->xs, h->G, h->C, h->g, h->c, ns, s));
+    if (f64)
+        GPT_CUDA(launch_schur64(bv, h->G, h->C, h->g, h->c, h->S64, h->gamma64, h->Ginv, h->Ginv64, ns, s));
+    else
+        GPT_CUDA(launch_schur(1, bv, 0.f, h->G, h->C, h->g, h->c, h->S, nullptr, h->gamma, h->Ginv, h->Ginv64,
+                              nullptr, SP.pcg_precond == 0 ? 1 : 0, ns, s));
+    GPT_CUDA(cudaMemsetAsync(h->adj_lam, 0, sizeof(float) * NS * T, s));
+    GPT_CUDA(launch_pcg(bv, maxN, minN, fmt, (int)SP.pcg_precond, S_rows, nullptr, h->gamma, h->gamma64, h->adj_lam, h->lam64,
+                        h->crw, (int)SP.pcg_max_iter, SP.pcg_tol, (int)SP.pcg_exit_mode, nullptr, nullptr, 0,
+                        (int)SP.pcg_cluster_size, ns, s));
+    GPT_CUDA(cudaMemsetAsync(h->dz, 0, sizeof(float) * NX * T, s));
+    GPT_CUDA(launch_dz(bv, h->Ginv, h->Ginv64, h->C, h->g, nullptr, h->lam64, h->dz, ns, s));
+    if (d_xu_next) GPT_CUDA(launch_axpy(nz, -1.f, h->dz, d_xu, d_xu_next, ns, s));
+    // ---- adjoint solve K mu = [h; 0], h = dl/d(dz) = -dl/dxu+; same S (recomputed), new gamma
+    GPT_CUDA(cudaMemsetAsync(h->adj_h, 0, sizeof(float) * NX * T, s));
+    GPT_CUDA(launch_axpy(nz, -1.f, d_grad_xu_next, nullptr, h->adj_h, ns, s));
+    GPT_CUDA(cudaMemsetAsync(h->adj_zero, 0, sizeof(float) * NS * T, s));
+    if (f64)
+        GPT_CUDA(launch_schur64(bv, h->G, h->C, h->adj_h, h->adj_zero, h->S64, h->adj_gamma64, h->Ginv, h->Ginv64,
+                                ns, s));
+    else
+        GPT_CUDA(launch_schur(1, bv, 0.f, h->G, h->C, h->adj_h, h->adj_zero, h->S, nullptr, h->adj_gamma, h->Ginv,
+                              h->Ginv64, nullptr, SP.pcg_precond == 0 ? 1 : 0, ns, s));
+    GPT_CUDA(cudaMemsetAsync(h->adj_lam, 0, sizeof(float) * NS * T, s));
+    GPT_CUDA(launch_pcg(bv, maxN, minN, fmt, (int)SP.pcg_precond, S_rows, nullptr, h->adj_gamma, h->adj_gamma64, h->adj_lam,
+                        h->adj_lam64, h->crw, (int)SP.pcg_max_iter, SP.pcg_tol, (int)SP.pcg_exit_mode, nullptr,
+                        nullptr, 0, (int)SP.pcg_cluster_size, ns, s));
+    GPT_CUDA(cudaMemsetAsync(h->adj_mu, 0, sizeof(float) * NX * T, s));
+    GPT_CUDA(launch_dz(bv, h->Ginv, h->Ginv64, h->C, h->adj_h, nullptr, h->adj_lam64, h->adj_mu, ns, s));
+    // ---- dl/dtheta = mu_z^T (dg/dtheta - dG/dtheta dz)
+    GPT_CUDA(launch_adjoint_grad(bv, P, d_xu, d_goal, h->dz, h->adj_mu, d_grad_goal, h->adj_part, d_grad_qd,
+                                 d_grad_r, d_grad_q_ee, ns, s));
+    GPT_CUDA(cudaMemcpyAsync(h->h_st, h->st, sizeof(InstState) * B, cudaMemcpyDeviceToHost, s));
+    GPT_CUDA(cudaStreamSynchronize(s));
+    for (uint32_t b = 0; b < B; ++b) {
+        const InstState &st = h->h_st[b];
+        if (st.exit_flags & 4u) return set_err(GPT_ERR_NONFINITE, "non-finite value in an adjoint solve");
+        if (st.pcg_maxiter_count) return set_err(GPT_ERR_NONFINITE, "PCG reached pcg_max_iter in the adjoint");
+    }
+    return GPT_OK;
 }
 
 }  // extern "C"

@@ -20,6 +20,7 @@ struct SolverParams {
     float rho_factor, rho_max, rho_min;
     uint32_t pcg_cluster_size;  // 0: chosen from N and the batch size
     uint32_t pcg_precond;       // 0 block-Jacobi (reference), 1 chunk block-tridiagonal LDL^T
+    uint32_t schur_fp64;        // with pcg_precond 1: FP64 Schur formation and rows
 };
 
 cudaError_t launch_kkt(const BatchView &bv, const ProblemParams &P, const float *xu, const float *goal,
@@ -34,10 +35,12 @@ int pcg_pick_cluster(int maxN, int B, int num_sms, int requested);
 // precond 0: block-Jacobi with the given Pinv; 1: exact block-tridiagonal LDL^T of each CTA's chunk
 // cr_ws: FP64 workspace of 196 doubles per knot of the batch (the cyclic-reduction
 // couplings of precond 1; unused by precond 0)
+// fmt 0: reference 3-block rows (S, Pinv floats); 1: packed FP32 rows (PK); 2: packed FP64 rows (PK64,
+// S points at doubles) with FP64 gamma64 -- chain preconditioner only
 cudaError_t launch_pcg(const BatchView &bv, int max_n_knots, int min_n_knots, int fmt, int precond, const float *S,
-                       const float *Pinv, const float *gamma, float *lambda, double *lambda64, double *cr_ws,
-                       int max_iter, float tol, int exit_mode, uint32_t *out_iters, uint32_t *pcg_log, int log_stride,
-                       int cluster_size, int num_sms, cudaStream_t s);
+                       const float *Pinv, const float *gamma, const double *gamma64, float *lambda, double *lambda64,
+                       double *cr_ws, int max_iter, float tol, int exit_mode, uint32_t *out_iters, uint32_t *pcg_log,
+                       int log_stride, int cluster_size, int num_sms, cudaStream_t s);
 // lambda64 (optional) replaces lambda when given
 cudaError_t launch_dz(const BatchView &bv, const float *Ginv, const double *Ginv64, const float *C, const float *g,
                       const float *lambda, const double *lambda64, float *dz, int num_sms, cudaStream_t s);
@@ -47,6 +50,17 @@ cudaError_t launch_accept(const BatchView &bv, int mode, const SolverParams &SP,
                           const float *dz, float *xu, float *merits_out, uint32_t *active_count, int num_sms,
                           cudaStream_t s);
 cudaError_t launch_init(const BatchView &bv, const float *xu, float *xs, int num_sms, cudaStream_t s);
+// FP64 Schur complement for the cyclic-reduction PCG: packed rows (PK64 doubles per knot), gamma
+// (FP64), the inverses (Ginv FP32 and Ginv64); rho from bv.st
+cudaError_t launch_schur64(const BatchView &bv, const float *G, const float *C, const float *g, const float *c,
+                           double *S64, double *gamma64, float *Ginv, double *Ginv64, int num_sms, cudaStream_t s);
+// adjoint of the SQP step (gpt_adjoint.cu): per-knot goal gradients, per-instance weight gradients;
+// part holds adjoint_part_floats() floats per knot
+cudaError_t launch_adjoint_grad(const BatchView &bv, const ProblemParams &P, const float *xu, const float *goal,
+                                const float *dz, const float *mu, float *grad_goal, float *part, float *grad_qd,
+                                float *grad_r, float *grad_qee, int num_sms, cudaStream_t s);
+cudaError_t launch_axpy(int n, float alpha, const float *x, const float *a, float *out, int num_sms, cudaStream_t s);
+size_t adjoint_part_floats();
 
 }  // namespace gpt
 

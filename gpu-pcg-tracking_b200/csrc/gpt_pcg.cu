@@ -29,6 +29,7 @@
 // exit test always holds for the true residual.
 // Exit test: mode 0 ||r||_2 <= tol ||gamma||_2; mode 1 |r^T Pinv r| < tol.
 #include <cooperative_groups.h>
+#include <type_traits>
 
 #include "gpt_common.cuh"
 #include "gpt_internal.h"
@@ -516,7 +517,7 @@ template <int FMT>
 __device__ __forceinline__ int diag_off(int r, int c)
 {
     const int hi = r >= c ? r : c, lo = r >= c ? c : r;
-    if (FMT == 1) return PK_DIAG + ((hi * (hi + 1)) >> 1) + lo;
+    if (FMT >= 1) return PK_DIAG + ((hi * (hi + 1)) >> 1) + lo;  // packed rows, FP32 (1) or FP64 (2)
     return SS + hi + NS * lo;
 }
 
@@ -562,11 +563,14 @@ __device__ __noinline__ void warp_spd_inverse_packed(double *Ap, int lane)
 // products are exact in FP64).
 template <int CS, int FMT>
 __global__ void __launch_bounds__(PCG_THREADS, 1)
-    pcg_chain_kernel(BatchView bv, int kpc_max, const float *__restrict__ S, const float *__restrict__ gamma,
-                     float *__restrict__ lambda, double *__restrict__ lambda64, double *__restrict__ cr_ws,
-                     int max_iter, float tol, int exit_mode, uint32_t *__restrict__ out_iters,
-                     uint32_t *__restrict__ pcg_log, int log_stride)
+    pcg_chain_kernel(BatchView bv, int kpc_max, const void *__restrict__ Sv, const float *__restrict__ gamma,
+                     const double *__restrict__ gamma64, float *__restrict__ lambda, double *__restrict__ lambda64,
+                     double *__restrict__ cr_ws, int max_iter, float tol, int exit_mode,
+                     uint32_t *__restrict__ out_iters, uint32_t *__restrict__ pcg_log, int log_stride)
 {
+    // FMT 2: packed FP64 rows (PK64 doubles per knot) and FP64 gamma, from schur64_kernel
+    using ST = typename std::conditional<FMT == 2, double, float>::type;
+    const ST *S = reinterpret_cast<const ST *>(Sv);
     extern __shared__ double chain_dyn_smem[];
     double *Aq = chain_dyn_smem;                    // kpc_max x 105: A_k, then A_k^{-1}
     double *un = Aq + (size_t)kpc_max * 105;         // union region
@@ -585,7 +589,7 @@ __global__ void __launch_bounds__(PCG_THREADS, 1)
     const int k0 = (rank * N) / CS, k1 = ((rank + 1) * N) / CS, kpc = k1 - k0;
     const int kpc_left = (rank > 0) ? k0 - ((rank - 1) * N) / CS : 0;
     const size_t kg0 = (size_t)kb + k0;
-    const size_t kstride = FMT == 1 ? PK : S_STRIDE;
+    const size_t kstride = FMT == 2 ? PK64 : (FMT == 1 ? PK : S_STRIDE);
     int nlev = 0;
     while ((1 << nlev) < kpc) ++nlev;
 
@@ -600,8 +604,8 @@ __global__ void __launch_bounds__(PCG_THREADS, 1)
     // coupling, all 14 loads issued before use
     auto coupling_line = [&](int l, int k, int rr, bool column, double (&v)[NS]) {
         if (l == 0) {
-            const float *src = S + (kg0 + k) * kstride;
-            float f[NS];
+            const ST *src = S + (kg0 + k) * kstride;
+            ST f[NS];
 #pragma unroll
             for (int cc = 0; cc < NS; ++cc) f[cc] = __ldg(src + (column ? cc + NS * rr : rr + NS * cc));
 #pragma unroll
@@ -617,14 +621,14 @@ __global__ void __launch_bounds__(PCG_THREADS, 1)
     {
         constexpr int G = 8;
         for (int i0 = tid; i0 < kpc * 105; i0 += G * PCG_THREADS) {
-            float v[G];
+            ST v[G];
 #pragma unroll
             for (int q = 0; q < G; ++q) {
                 const int i = i0 + q * PCG_THREADS;
                 v[q] = 0.f;
                 if (i < kpc * 105) {
                     const int kl = i / 105, t = i - kl * 105;
-                    if (FMT == 1) {
+                    if (FMT >= 1) {
                         v[q] = __ldg(S + (kg0 + kl) * kstride + PK_DIAG + t);  // same packed order
                     } else {
                         int rr = 0;
@@ -653,7 +657,7 @@ __global__ void __launch_bounds__(PCG_THREADS, 1)
         auto stage = [&](double *dst, int l, int k) {
             double v[7];
             if (l == 0) {
-                const float *src = S + (kg0 + k) * kstride;
+                const ST *src = S + (kg0 + k) * kstride;
 #pragma unroll
                 for (int q = 0; q < 7; ++q) v[q] = (lane + 32 * q < SS) ? (double)__ldg(src + lane + 32 * q) : 0.0;
             } else {
@@ -752,10 +756,11 @@ __global__ void __launch_bounds__(PCG_THREADS, 1)
     int doff[NS];  // offsets of row r of the diagonal block within a knot block
 #pragma unroll
     for (int cc = 0; cc < NS; ++cc) doff[cc] = diag_off<FMT>(r, cc);
-    const float *gb = gamma + NS * kg0;
+    const float *gb = (FMT == 2) ? nullptr : gamma + NS * kg0;
+    const double *gb64 = (FMT == 2) ? gamma64 + NS * kg0 : nullptr;
     float *lb = lambda + NS * kg0;
     double lam[PCG_KPT], res[PCG_KPT], pp[PCG_KPT], zz[PCG_KPT];
-    float gv[PCG_KPT];
+    double gv[PCG_KPT];
     bool own[PCG_KPT];
 #pragma unroll
     for (int j = 0; j < PCG_KPT; ++j) {
@@ -764,16 +769,16 @@ __global__ void __launch_bounds__(PCG_THREADS, 1)
         lam[j] = res[j] = pp[j] = zz[j] = 0.0;
         gv[j] = 0.f;
         if (own[j]) {
-            gv[j] = gb[NS * kl + r];
+            gv[j] = (FMT == 2) ? gb64[NS * kl + r] : (double)gb[NS * kl + r];
             lam[j] = (double)lb[NS * kl + r];
         }
     }
     // (S x)_row with FP64 accumulation; x = rv holds 14 (kpc+2) doubles with halo slots
     auto row_f64 = [&](int j) -> double {
         const int kl = g0 + PCG_TK * j, k = k0 + kl;
-        const float *lk = S + (kg0 + kl) * kstride;
+        const ST *lk = S + (kg0 + kl) * kstride;
         const double *xk = rv + NS * kl;
-        float fl[NS], fd[NS], fr[NS];
+        ST fl[NS], fd[NS], fr[NS];
 #pragma unroll
         for (int cc = 0; cc < NS; ++cc) {
             fl[cc] = (k > 0) ? __ldg(lk + r + NS * cc) : 0.f;
@@ -1100,10 +1105,10 @@ static cudaError_t launch_pcg_cs(const BatchView &bv, int kpc_max, const float *
 }
 
 template <int CS, int FMT>
-static cudaError_t launch_pcg_chain_cs(const BatchView &bv, int kpc_max, const float *S, const float *gamma,
-                                       float *lambda, double *lambda64, double *cr_ws, int max_iter, float tol,
-                                       int exit_mode, uint32_t *out_iters, uint32_t *pcg_log, int log_stride,
-                                       cudaStream_t s)
+static cudaError_t launch_pcg_chain_cs(const BatchView &bv, int kpc_max, const void *S, const float *gamma,
+                                       const double *gamma64, float *lambda, double *lambda64, double *cr_ws,
+                                       int max_iter, float tol, int exit_mode, uint32_t *out_iters, uint32_t *pcg_log,
+                                       int log_stride, cudaStream_t s)
 {
     auto kern = pcg_chain_kernel<CS, FMT>;
     const size_t smem = pcg_chain_smem_bytes(kpc_max);
@@ -1129,17 +1134,18 @@ static cudaError_t launch_pcg_chain_cs(const BatchView &bv, int kpc_max, const f
     attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, kern, bv, kpc_max, S, gamma, lambda, lambda64, cr_ws, max_iter, tol, exit_mode,
-                              out_iters, pcg_log, log_stride);
+    return cudaLaunchKernelEx(&cfg, kern, bv, kpc_max, S, gamma, gamma64, lambda, lambda64, cr_ws, max_iter, tol,
+                              exit_mode, out_iters, pcg_log, log_stride);
 }
 
 cudaError_t launch_pcg(const BatchView &bv, int max_n_knots, int min_n_knots, int fmt, int precond, const float *S,
-                       const float *Pinv, const float *gamma, float *lambda, double *lambda64, double *cr_ws,
-                       int max_iter, float tol, int exit_mode, uint32_t *out_iters, uint32_t *pcg_log, int log_stride,
-                       int cluster_size, int num_sms, cudaStream_t s)
+                       const float *Pinv, const float *gamma, const double *gamma64, float *lambda,
+                       double *lambda64, double *cr_ws, int max_iter, float tol, int exit_mode, uint32_t *out_iters,
+                       uint32_t *pcg_log, int log_stride, int cluster_size, int num_sms, cudaStream_t s)
 {
     if (bv.B <= 0) return cudaSuccess;
     if (precond == 1 && !cr_ws) return cudaErrorInvalidValue;
+    if (fmt == 2 && (precond != 1 || !gamma64)) return cudaErrorInvalidValue;  // FP64 rows: chain preconditioner only
     if (max_n_knots > MAX_PCG_KNOTS) return cudaErrorInvalidValue;
     int cs = (precond == 1 && cluster_size == 0) ? 1 : pcg_pick_cluster(max_n_knots, bv.B, num_sms, cluster_size);
     while ((max_n_knots + cs - 1) / cs > PCG_KPC_MAX) cs *= 2;
@@ -1148,11 +1154,15 @@ cudaError_t launch_pcg(const BatchView &bv, int max_n_knots, int min_n_knots, in
     if (kpc_max > PCG_KPC_MAX || cs > 16) return cudaErrorInvalidValue;
 #define GPT_PCG_CASE(CSV)                                                                                      \
     case CSV:                                                                                                  \
-        if (precond == 1)                                                                                      \
-            return fmt ? launch_pcg_chain_cs<CSV, 1>(bv, kpc_max, S, gamma, lambda, lambda64, cr_ws, max_iter, \
-                                                     tol, exit_mode, out_iters, pcg_log, log_stride, s)        \
-                       : launch_pcg_chain_cs<CSV, 0>(bv, kpc_max, S, gamma, lambda, lambda64, cr_ws, max_iter, \
-                                                     tol, exit_mode, out_iters, pcg_log, log_stride, s);       \
+        if (precond == 1) {                                                                                    \
+            if (fmt == 2)                                                                                      \
+                return launch_pcg_chain_cs<CSV, 2>(bv, kpc_max, S, gamma, gamma64, lambda, lambda64, cr_ws,    \
+                                                   max_iter, tol, exit_mode, out_iters, pcg_log, log_stride, s); \
+            return fmt ? launch_pcg_chain_cs<CSV, 1>(bv, kpc_max, S, gamma, gamma64, lambda, lambda64, cr_ws,  \
+                                                     max_iter, tol, exit_mode, out_iters, pcg_log, log_stride, s) \
+                       : launch_pcg_chain_cs<CSV, 0>(bv, kpc_max, S, gamma, gamma64, lambda, lambda64, cr_ws,  \
+                                                     max_iter, tol, exit_mode, out_iters, pcg_log, log_stride, s); \
+        }                                                                                                      \
         return fmt ? launch_pcg_cs<CSV, 1>(bv, kpc_max, S, Pinv, gamma, lambda, lambda64, max_iter, tol,       \
                                            exit_mode, out_iters, pcg_log, log_stride, s)                       \
                    : launch_pcg_cs<CSV, 0>(bv, kpc_max, S, Pinv, gamma, lambda, lambda64, max_iter, tol,       \

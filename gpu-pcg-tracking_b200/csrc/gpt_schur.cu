@@ -258,6 +258,193 @@ __global__ void __launch_bounds__(32 * SCHUR_WARPS)
     }
 }
 
+// ---------------------------------------------------------------------------
+// FP64 formation for the cyclic-reduction PCG: the same block row as MODE 1,
+// with every product, gamma and the stored row in FP64 (PK64 doubles per knot:
+// left block 196 column-major, lower triangle of the diagonal block 105, pad).
+// FP32 formation perturbs S by ~10 eps32 relative per entry, which cond(S)
+// ~1e7 turns into ~1e-2 relative error of the solution; FP64 formation leaves
+// only the FP32 rounding of the KKT data (G, C, g, c).
+// ---------------------------------------------------------------------------
+
+template <int n>
+__device__ __forceinline__ void warp_inverse64(const float *A, double shift, double *Ainv, int lane,
+                                               float *Ainv32, double *Ainv64g)
+{
+    double col[n];
+    const bool left = lane < n, right = (lane >= n) && (lane < 2 * n);
+#pragma unroll
+    for (int r = 0; r < n; ++r) {
+        double v = 0.0;
+        if (left) v = (double)A[r + n * lane] + ((r == lane) ? shift : 0.0);
+        else if (right) v = (r == lane - n) ? 1.0 : 0.0;
+        col[r] = v;
+    }
+#pragma unroll
+    for (int p = 0; p < n; ++p) {
+        const double piv = __shfl_sync(0xffffffffu, col[p], p);
+        const double prow = col[p] * __drcp_rn(piv);
+#pragma unroll
+        for (int r = 0; r < n; ++r) {
+            if (r == p) continue;
+            const double pr = __shfl_sync(0xffffffffu, col[r], p);
+            col[r] = fma(-pr, prow, col[r]);
+        }
+        col[p] = prow;
+    }
+    if (right) {
+        const int cc = lane - n;
+#pragma unroll
+        for (int r = 0; r < n; ++r) Ainv[r + n * cc] = col[r];
+        if (Ainv32) {
+#pragma unroll
+            for (int r = 0; r < n; ++r) Ainv32[r + n * cc] = (float)col[r];
+        }
+        if (Ainv64g) {
+#pragma unroll
+            for (int r = 0; r < n; ++r) Ainv64g[r + n * cc] = col[r];
+        }
+    }
+}
+
+// out (14 x NCOL, col-major) = A (14 x K, col-major) * op(B), FP64
+template <int K, int NCOL, bool TRANS_B>
+__device__ __forceinline__ void warp_mm64(const double *A, const double *B, int ldb, double *out, int lane)
+{
+    if (lane < 2 * NCOL) {
+        const int col = lane % NCOL, r0 = (lane / NCOL) * 7;
+        double acc[7];
+#pragma unroll
+        for (int i = 0; i < 7; ++i) acc[i] = 0.0;
+#pragma unroll
+        for (int t = 0; t < K; ++t) {
+            const double bv = TRANS_B ? B[col + ldb * t] : B[t + ldb * col];
+#pragma unroll
+            for (int i = 0; i < 7; ++i) acc[i] = fma(A[r0 + i + NS * t], bv, acc[i]);
+        }
+#pragma unroll
+        for (int i = 0; i < 7; ++i) out[r0 + i + NS * col] = acc[i];
+    }
+}
+
+struct Schur64WarpSmem {
+    double A[SS], B[SC];
+    double Qki[SS], Qkp1i[SS], Rki[CC];
+    double phi[SS], BRi[SC], theta[SS], tmp[SS];
+    double qk[NS], qkp1[NS], rk[NC], ck[NS];
+};
+
+__global__ void __launch_bounds__(32 * SCHUR_WARPS)
+    schur64_kernel(BatchView bv, const float *__restrict__ G, const float *__restrict__ Cm,
+                   const float *__restrict__ g, const float *__restrict__ c, double *__restrict__ S64,
+                   double *__restrict__ gamma64, float *__restrict__ Ginv, double *__restrict__ Ginv64)
+{
+    extern __shared__ double4 schur64_dyn_smem[];
+    Schur64WarpSmem *smem_all = reinterpret_cast<Schur64WarpSmem *>(schur64_dyn_smem);
+    const int lane = threadIdx.x & 31;
+    Schur64WarpSmem &sm = smem_all[threadIdx.x >> 5];
+    const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+
+    for (int j = gw; j < bv.total_knots; j += nw) {
+        const int b = bv.inst(j);
+        if (!bv.active(b)) continue;
+        const int N = bv.N(b);
+        const int k = j - bv.off(b);
+        const double rho = (double)bv.st[b].rho;
+        double *Pk = S64 + (size_t)PK64 * j;
+
+        if (k == 0) {
+            const float *Q0 = G + (size_t)G_STRIDE * j;
+            warp_inverse64<NS>(Q0, rho, sm.Qki, lane, N == 1 ? Ginv + (size_t)G_STRIDE * j : nullptr,
+                               N == 1 ? Ginv64 + (size_t)G_STRIDE * j : nullptr);
+            if (lane < NS) sm.qk[lane] = (double)g[(size_t)NX * j + lane];
+            __syncwarp();
+            if (lane < NS) {
+                double acc = 0.0;
+#pragma unroll
+                for (int t = 0; t < NS; ++t) acc = fma(sm.Qki[lane + NS * t], sm.qk[t], acc);
+                gamma64[(size_t)NS * j + lane] = -acc;
+            }
+            for (int e = lane; e < SS; e += 32) {
+                const int r = e % NS, cc = e / NS;
+                Pk[e] = 0.0;  // no left block in row 0
+                if (r >= cc) Pk[SS + ((r * (r + 1)) >> 1) + cc] = -sm.Qki[e];
+            }
+            if (lane == 0) Pk[PK64 - 1] = 0.0;
+            __syncwarp();
+            continue;
+        }
+
+        // ---- rows k >= 1
+        const float *Ck = Cm + (size_t)C_STRIDE * (j - 1);
+        for (int e = lane; e < C_STRIDE; e += 32) {
+            const double v = (double)Ck[e];
+            if (e < SS) sm.A[e] = v;
+            else sm.B[e - SS] = v;
+        }
+        if (lane < NS) {
+            sm.qk[lane] = (double)g[(size_t)NX * (j - 1) + lane];
+            sm.qkp1[lane] = (double)g[(size_t)NX * j + lane];
+            sm.ck[lane] = (double)c[(size_t)NS * j + lane];
+        } else if (lane < NS + NC) {
+            sm.rk[lane - NS] = (double)g[(size_t)NX * (j - 1) + lane];
+        }
+        const float *Gkm1 = G + (size_t)G_STRIDE * (j - 1);
+        const float *Gk = G + (size_t)G_STRIDE * j;
+        float *Gi32 = Ginv + (size_t)G_STRIDE * (j - 1);
+        double *Gi64 = Ginv64 + (size_t)G_STRIDE * (j - 1);
+        warp_inverse64<NS>(Gkm1, rho, sm.Qki, lane, Gi32, Gi64);
+        warp_inverse64<NS>(Gk, rho, sm.Qkp1i, lane, k == N - 1 ? Ginv + (size_t)G_STRIDE * j : nullptr,
+                           k == N - 1 ? Ginv64 + (size_t)G_STRIDE * j : nullptr);
+        warp_inverse64<NC>(Gkm1 + SS, rho, sm.Rki, lane, Gi32 + SS, Gi64 + SS);
+        __syncwarp();
+        warp_mm64<NS, NS, false>(sm.A, sm.Qki, NS, sm.phi, lane);   // phi = (-A) Qt^{-1}
+        warp_mm64<NC, NC, false>(sm.B, sm.Rki, NC, sm.BRi, lane);   // (-B) Rt^{-1}
+        __syncwarp();
+        warp_mm64<NS, NS, true>(sm.phi, sm.A, NS, sm.theta, lane);  // phi (-A)^T
+        warp_mm64<NC, NS, true>(sm.BRi, sm.B, NS, sm.tmp, lane);    // (-B) Rt^{-1} (-B)^T
+        if (lane < NS) {
+            double a1 = 0.0, a2 = 0.0, a3 = 0.0;
+#pragma unroll
+            for (int t = 0; t < NS; ++t) {
+                a1 = fma(sm.Qkp1i[lane + NS * t], sm.qkp1[t], a1);
+                a2 = fma(sm.phi[lane + NS * t], sm.qk[t], a2);
+            }
+#pragma unroll
+            for (int t = 0; t < NC; ++t) a3 = fma(sm.BRi[lane + NS * t], sm.rk[t], a3);
+            gamma64[(size_t)NS * j + lane] = -((a1 - sm.ck[lane]) + (a3 + a2));
+        }
+        __syncwarp();
+        for (int e = lane; e < SS; e += 32) {
+            const int r = e % NS, cc = e / NS;
+            Pk[e] = -sm.phi[e];
+            if (r >= cc) Pk[SS + ((r * (r + 1)) >> 1) + cc] = -((sm.theta[e] + sm.Qkp1i[e]) + sm.tmp[e]);
+        }
+        if (lane == 0) Pk[PK64 - 1] = 0.0;
+        __syncwarp();
+    }
+}
+
+cudaError_t launch_schur64(const BatchView &bv, const float *G, const float *C, const float *g, const float *c,
+                           double *S64, double *gamma64, float *Ginv, double *Ginv64, int num_sms, cudaStream_t s)
+{
+    if (bv.total_knots <= 0) return cudaSuccess;
+    if (!bv.st || !Ginv64) return cudaErrorInvalidValue;
+    const size_t smem = sizeof(Schur64WarpSmem) * SCHUR_WARPS;
+    int blocks = (bv.total_knots + SCHUR_WARPS - 1) / SCHUR_WARPS;
+    const int cap = num_sms * 16;
+    if (blocks > cap) blocks = cap;
+    static bool attr_done = false;
+    if (!attr_done) {
+        cudaError_t e = cudaFuncSetAttribute(schur64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        attr_done = true;
+    }
+    schur64_kernel<<<blocks, 32 * SCHUR_WARPS, smem, s>>>(bv, G, C, g, c, S64, gamma64, Ginv, Ginv64);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_schur(int mode, const BatchView &bv, float rho_scalar, const float *G,
                          const float *C, const float *g, const float *c, float *S, float *Pinv, float *gamma,
                          float *Ginv, double *Ginv64, float *csc_val, int need_pinv, int num_sms, cudaStream_t s)

@@ -83,6 +83,9 @@ typedef struct gpt_solver_config {
     uint32_t pcg_cluster_size; /* CTAs per instance in the PCG (1,2,4,8,16); 0 = chosen by the library */
     uint32_t pcg_precond;      /* 0: block-Jacobi Pinv (the reference's, oldschur.cuh:926-933);
                                   1 (default): exact block-tridiagonal LDL^T of each CTA's chunk of knots */
+    uint32_t schur_fp64;       /* SQP loop and adjoint with pcg_precond 1: 1 (default) forms and stores the
+                                  Schur complement in FP64; 0 in FP32 as the reference does (schur.cuh:391-524).
+                                  FP32 formation moves the solution by ~cond(S) x 1e-7 (~1e-2 at cond 1e7) */
 } gpt_solver_config;
 
 /* One sqpSolve's outcome (the reference returns a tuple, toplevel.cuh:502) */
@@ -132,6 +135,29 @@ gpt_status gpt_sqp_solve(gpt_handle *h, uint32_t knot_points, const float *d_eeP
 gpt_status gpt_sqp_solve_batched(gpt_handle *h, uint32_t batch, const uint32_t *h_knot_points,
                                  const float *d_eePos_traj, float *d_lambda, float *d_xu, float *h_rho,
                                  float rho_reset, gpt_sqp_stats *h_stats, gpt_stream_t stream);
+
+/* Adjoint of the SQP step (no reference counterpart).  At the iterate d_xu
+ * (typically a solve's result) with per-instance rho h_rho and initial states
+ * d_xs (14 per instance, x_0 of the solve's initial guess), the step solves
+ * K [dz; lambda] = [g; c] (the KKT system of gato_form_kkt,
+ * oldschur.cuh:966-1092) and maps xu to xu+ = xu - dz (the first line-search
+ * step, toplevel.cuh:409), written to d_xu_next when non-NULL.  Given
+ * d_grad_xu_next = dl/dxu+ (xu layout), one extra Schur right-hand side and
+ * PCG solve with the same Schur matrix (K is symmetric) give the gradients of
+ * l with respect to
+ *   d_grad_eePos  the goal trajectory (6 per knot: xyz; rpy entries are 0),
+ *   d_grad_qd     the 7 joint-velocity weights (QD_COST per joint), per instance,
+ *   d_grad_r      the 7 control weights (R_COST per joint), per instance,
+ *   d_grad_q_ee   the end-effector position weight, per instance.
+ * Exact derivatives of that map (the SQP's own KKT matrix, with the
+ * reference's terminal target when ref_terminal is set); at a converged
+ * iterate xu+ = xu, so they are the one-step implicit derivatives of the
+ * solution.  Per-knot dynamics and kinematics are recomputed, not stored.
+ * Uses the handle's solver settings for both PCG solves. */
+gpt_status gpt_sqp_adjoint(gpt_handle *h, uint32_t batch, const uint32_t *h_knot_points, const float *d_eePos_traj,
+                           const float *d_xs, const float *d_xu, const float *h_rho, const float *d_grad_xu_next,
+                           float *d_xu_next, float *d_grad_eePos, float *d_grad_qd, float *d_grad_r,
+                           float *d_grad_q_ee, gpt_stream_t stream);
 
 /* ---- the reference's kernels, one instance, device buffers, stream-ordered ---- */
 
