@@ -238,7 +238,10 @@ def main():
         rho, stats = sv.sqp_solve_batched(Ns, goal, lam, xu, [1e-3] * B)
         e1.record(stream)
         e1.synchronize()
+        last_rho[:] = rho
         return e0.elapsed_time(e1), stats
+
+    last_rho = [1e-3] * B
 
     for _ in range(args.warmup):
         one_step()
@@ -265,11 +268,36 @@ def main():
     ms_per_step = total_ms / args.steps
     value = world * B / (ms_per_step / 1000.0)
 
+    # adjoint of the SQP step at the solutions of the last timed step (gpt_sqp_adjoint): gradients of
+    # w . xu+ w.r.t. the goal trajectory and the cost weights, timed like the forward solve
+    offs = [sum(Ns[:b]) for b in range(B)]
+    xs = torch.cat([xu0[21 * o:21 * o + 14] for o in offs])
+    gw = torch.randn(xu.numel(), device="cuda", generator=torch.Generator(device="cuda").manual_seed(7))
+    adj_ms = []
+    for i in range(1 + args.steps):
+        flush.fill_(1.0)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        sv.sqp_adjoint(Ns, goal, xs, xu, last_rho, gw)
+        e1.record(stream)
+        e1.synchronize()
+        if i > 0:
+            adj_ms.append(e0.elapsed_time(e1))
+    adj_step = statistics.mean(adj_ms)
+    if world > 1:
+        t = torch.tensor([adj_step], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        adj_step = float(t.item())
+    adjoint = {"us_per_solve": 1000.0 * adj_step / B, "ms_per_batch": adj_step,
+               "ratio_to_forward_solve": adj_step / ms_per_step,
+               "workload": f"gpt_sqp_adjoint at the {B} solutions of the timed step (goal, QD, R, EE-weight gradients)"}
+
     if args.batched_only:
         if rank == 0:
             print(json.dumps({"metric": METRIC, "value": world * B / (ms_per_step / 1000.0), "unit": "solves/s",
                               "ms_per_step": ms_per_step, "phase_ms": {k: v[0] for k, v in phases.items()},
-                              "pcg_iters_per_solve": sum(x["pcg_iters_total"] for x in all_stats) / len(all_stats)}),
+                              "pcg_iters_per_solve": sum(x["pcg_iters_total"] for x in all_stats) / len(all_stats),
+                              "adjoint": adjoint}),
                   flush=True)
         if world > 1:
             dist.destroy_process_group()
@@ -366,6 +394,7 @@ def main():
                 "d2h_bytes_per_step": d2h},
         "gpu_launches": int(launches_total),
         "clocks": clk,
+        "adjoint": adjoint,
         "plain_solves_per_s": plain_rate,
         "batched_over_plain": (value / world) / plain_rate if plain_rate else None,
         "phase_ms": {k: v[0] for k, v in phases.items()},

@@ -32,7 +32,7 @@ EXPORTED = [
     "gpt_set_solver_config", "gpt_last_error", "gpt_version", "gpt_sqp_solve", "gpt_sqp_solve_batched",
     "gpt_form_kkt", "gpt_form_schur", "gpt_form_schur_csc", "gpt_prep_csr", "gpt_pcg", "gpt_compute_dz",
     "gpt_compute_merit", "gpt_ls_compute_merit", "gpt_set_profiling", "gpt_get_phase_stats",
-    "gpt_ls_compute_merit_noalloc", "gpt_sqp_adjoint",
+    "gpt_ls_compute_merit_noalloc", "gpt_sqp_adjoint", "gpt_set_cost_weights",
 ]
 PHASES = ["init", "kkt", "schur", "pcg", "dz", "merit", "accept"]
 
@@ -118,6 +118,7 @@ def _declare(L):
         "gpt_get_phase_stats": ([vp, vp, vp, C.c_int], C.c_int),
         "gpt_ls_compute_merit_noalloc": ([P(ProblemConfig), u32, vp, vp, vp, vp, vp, vp], C.c_int),
         "gpt_sqp_adjoint": ([vp, u32, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp], C.c_int),
+        "gpt_set_cost_weights": ([vp, f32, f32, f32], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -213,6 +214,11 @@ class Solver:
         for k, v in kw.items():
             setattr(self.solver, k, v)
         _check(lib().gpt_set_solver_config(self._h, C.byref(self.solver)))
+
+    def set_cost_weights(self, q_ee: float, qd_cost: float, r_cost: float):
+        """gpt_set_cost_weights: the end-effector, joint-velocity and control weights of later calls."""
+        _check(lib().gpt_set_cost_weights(self._h, q_ee, qd_cost, r_cost))
+        self.problem.q_ee, self.problem.qd_cost, self.problem.r_cost = q_ee, qd_cost, r_cost
 
     def reset_solver(self, **kw):
         """gpt_default_solver_config, then the given fields."""

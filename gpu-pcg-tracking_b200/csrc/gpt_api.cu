@@ -183,6 +183,17 @@ gpt_status gpt_set_solver_config(gpt_handle *h, const gpt_solver_config *sc)
     return GPT_OK;
 }
 
+gpt_status gpt_set_cost_weights(gpt_handle *h, float q_ee, float qd_cost, float r_cost)
+{
+    if (!h) return set_err(GPT_ERR_BAD_ARG, "null argument");
+    if (!(q_ee >= 0.0f) || !(qd_cost >= 0.0f) || !(r_cost >= 0.0f))
+        return set_err(GPT_ERR_BAD_ARG, "cost weights must be finite and non-negative");
+    h->pc.q_ee = q_ee;
+    h->pc.qd_cost = qd_cost;
+    h->pc.r_cost = r_cost;
+    return GPT_OK;
+}
+
 gpt_status gpt_create(const gpt_problem_config *pc, const gpt_solver_config *sc, gpt_handle **out)
 {
     if (!pc || !sc || !out) return set_err(GPT_ERR_BAD_ARG, "null argument");

@@ -112,6 +112,11 @@ void gpt_default_solver_config(gpt_solver_config *out);
 gpt_status gpt_create(const gpt_problem_config *problem, const gpt_solver_config *solver, gpt_handle **out);
 gpt_status gpt_destroy(gpt_handle *h);
 gpt_status gpt_set_solver_config(gpt_handle *h, const gpt_solver_config *solver);
+
+/* Cost weights of later calls: end-effector position weight, QD_COST and
+ * R_COST (no reference counterpart: the reference compiles them in,
+ * iiwa_eepos_plant.cuh:58-64). */
+gpt_status gpt_set_cost_weights(gpt_handle *h, float q_ee, float qd_cost, float r_cost);
 const char *gpt_last_error(void);
 const char *gpt_version(void);
 

@@ -129,3 +129,35 @@ def test_adjoint_batched_equals_single(gpt, problem_mod):
         np.testing.assert_allclose(host(both["goal"])[6 * off:6 * (off + n)], host(one["goal"]), rtol=1e-5, atol=1e-6)
         off += n
     sv.close()
+
+
+def test_autograd_function_uses_the_adjoint(gpt, problem_mod):
+    """sqp_solve under torch.autograd: the forward pass is gpt_sqp_solve_batched,
+    the backward pass returns gpt_sqp_adjoint's gradients at the returned solution
+    (goal per knot; the three shared weights as sums of the per-joint,
+    per-instance gradients)."""
+    import importlib
+    ag = importlib.import_module("gpu-pcg-tracking_b200.autograd")
+    Ns = [8, 12]
+    ps = [problem_mod.make_problem(n, 20 + i, dt=SPEC["timestep"]) for i, n in enumerate(Ns)]
+    cat = lambda key, pad: np.concatenate([np.concatenate([p[key], np.zeros(pad, np.float32)]) for p in ps])
+    sv = gpt.Solver(max_knot_points=12, max_batch=2, **SPEC)
+    sv.set_solver(sqp_max_iter=5, pcg_exit_tol=1e-8, pcg_max_iter=100000, pcg_cluster_size=1)
+    goal0 = dev(cat("goal", 0))
+    xu0, lam0 = dev(cat("xu", 7)), dev(cat("lam", 0))
+    w = torch.as_tensor(np.random.default_rng(3).normal(0, 1, xu0.numel()).astype(np.float32), device="cuda")
+    # plain calls: solve, then the adjoint at the solution with the final rho
+    xu_r, lam_r = xu0.clone(), lam0.clone()
+    rho_r, _ = sv.sqp_solve_batched(Ns, goal0, lam_r, xu_r, [1e-3, 1e-3])
+    xs = torch.cat([xu0[0:14], xu0[21 * 8:21 * 8 + 14]])
+    ref = sv.sqp_adjoint(Ns, goal0, xs, xu_r, rho_r, w)
+    # the same through autograd
+    goal = goal0.clone().requires_grad_(True)
+    weights = torch.tensor([1.0, SPEC["qd_cost"], SPEC["r_cost"]], device="cuda", requires_grad=True)
+    xu, lam = ag.sqp_solve(sv, Ns, goal, weights, xu0, lam0, [1e-3, 1e-3])
+    assert torch.equal(xu, xu_r)
+    (w * xu).sum().backward()
+    assert torch.equal(goal.grad, ref["goal"])
+    want_w = torch.stack([ref["q_ee"].sum(), ref["qd"].sum(), ref["r"].sum()])
+    assert torch.allclose(weights.grad, want_w, rtol=1e-6, atol=0)
+    sv.close()
