@@ -50,7 +50,7 @@ class SolverConfig(C.Structure):
     _fields_ = [("sqp_max_iter", C.c_uint32), ("pcg_max_iter", C.c_uint32), ("pcg_exit_tol", C.c_float),
                 ("pcg_exit_mode", C.c_uint32), ("rho_factor", C.c_float), ("rho_max", C.c_float),
                 ("rho_min", C.c_float), ("pcg_cluster_size", C.c_uint32), ("pcg_precond", C.c_uint32),
-                ("schur_fp64", C.c_uint32)]
+                ("schur_fp64", C.c_uint32), ("sqp_graph", C.c_uint32)]
 
 
 class SqpStats(C.Structure):

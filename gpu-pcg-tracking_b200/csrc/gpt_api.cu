@@ -36,6 +36,16 @@ gpt_status cuda_err(cudaError_t e, const char *where)
 
 }  // namespace
 
+struct GraphKey {
+    int B, total, maxN, minN;
+    ProblemParams P;
+    SolverParams SP;
+};
+struct GraphEntry {
+    GraphKey key;
+    cudaGraphExec_t exec;
+};
+
 struct gpt_handle {
     gpt_problem_config pc;
     gpt_solver_config sc;
@@ -58,6 +68,12 @@ struct gpt_handle {
     double *adj_lam64 = nullptr;
     // FP64 Schur rows (PK64 doubles per knot) and right-hand sides for the cyclic-reduction PCG
     double *S64 = nullptr, *gamma64 = nullptr, *adj_gamma64 = nullptr;
+    // the SQP loop as a CUDA graph: copies of the caller's buffers, the iteration count of the
+    // device-side while loop, capture streams and the instantiated graphs per batch shape
+    float *gxu = nullptr, *glam = nullptr, *ggoal = nullptr;
+    uint32_t *d_iter = nullptr;
+    cudaStream_t cap_stream = nullptr, body_stream = nullptr;
+    std::vector<GraphEntry> graphs;
     uint32_t cap_sqp_iter = 0;  // pcg_log rows allocated at creation
     // pinned host staging
     uint32_t *h_active = nullptr;
@@ -103,6 +119,7 @@ SolverParams to_solver(const gpt_solver_config &sc)
     S.pcg_cluster_size = sc.pcg_cluster_size;
     S.pcg_precond = sc.pcg_precond;
     S.schur_fp64 = sc.schur_fp64;
+    S.sqp_graph = sc.sqp_graph;
     return S;
 }
 BatchView single_view(uint32_t N)
@@ -161,6 +178,7 @@ void gpt_default_solver_config(gpt_solver_config *o)
     o->pcg_cluster_size = 0;
     o->pcg_precond = 1;
     o->schur_fp64 = 1;
+    o->sqp_graph = 1;
 }
 
 const char *gpt_last_error(void) { return g_last_error.c_str(); }
@@ -175,6 +193,7 @@ gpt_status gpt_set_solver_config(gpt_handle *h, const gpt_solver_config *sc)
         return set_err(GPT_ERR_BAD_ARG, "pcg_cluster_size must be 0, 1, 2, 4, 8 or 16");
     if (sc->pcg_precond > 1) return set_err(GPT_ERR_BAD_ARG, "pcg_precond must be 0 or 1");
     if (sc->schur_fp64 > 1) return set_err(GPT_ERR_BAD_ARG, "schur_fp64 must be 0 or 1");
+    if (sc->sqp_graph > 1) return set_err(GPT_ERR_BAD_ARG, "sqp_graph must be 0 or 1");
     if (sc->sqp_max_iter > h->cap_sqp_iter) {
         // pcg log is sized at creation
         return set_err(GPT_ERR_CAPACITY, "sqp_max_iter larger than at creation");
@@ -252,6 +271,12 @@ gpt_status gpt_create(const gpt_problem_config *pc, const gpt_solver_config *sc,
     ALLOC(S64, PK64 * T);
     ALLOC(gamma64, NS * T);
     ALLOC(adj_gamma64, NS * T);
+    ALLOC(gxu, NX * T);
+    ALLOC(glam, NS * T);
+    ALLOC(ggoal, 6 * T);
+    ALLOC(d_iter, 1);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->cap_stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->body_stream, cudaStreamNonBlocking);
 #undef ALLOC
     if (e == cudaSuccess) e = cudaMallocHost((void **)&h->h_active, sizeof(uint32_t));
     if (e == cudaSuccess) e = cudaMallocHost((void **)&h->h_st, sizeof(InstState) * B);
@@ -301,6 +326,10 @@ gpt_status gpt_destroy(gpt_handle *h)
     cudaFree(h->adj_h); cudaFree(h->adj_zero); cudaFree(h->adj_gamma); cudaFree(h->adj_lam); cudaFree(h->adj_mu);
     cudaFree(h->adj_part); cudaFree(h->adj_lam64);
     cudaFree(h->S64); cudaFree(h->gamma64); cudaFree(h->adj_gamma64);
+    for (auto &ge : h->graphs) cudaGraphExecDestroy(ge.exec);
+    cudaFree(h->gxu); cudaFree(h->glam); cudaFree(h->ggoal); cudaFree(h->d_iter);
+    if (h->cap_stream) cudaStreamDestroy(h->cap_stream);
+    if (h->body_stream) cudaStreamDestroy(h->body_stream);
     cudaFreeHost(h->h_active); cudaFreeHost(h->h_st); cudaFreeHost(h->h_pcg_out); cudaFreeHost(h->h_pcg_log);
     if (h->ev) cudaEventDestroy(h->ev);
     delete h;
@@ -508,6 +537,151 @@ static gpt_status setup_batch(gpt_handle *h, uint32_t B, const uint32_t *Ns, con
     return GPT_OK;
 }
 
+
+// What one batched solve needs beyond the handle: the batch view and the parameters.
+struct SqpPlan {
+    BatchView bv;
+    ProblemParams P;
+    SolverParams SP;
+    int maxN, minN, ns;
+};
+
+// x_s and the merit of the initial iterate (toplevel.cuh:110,235-244)
+static gpt_status enqueue_prologue(gpt_handle *h, const SqpPlan &pl, const float *d_goal, float *d_xu, cudaStream_t s)
+{
+    PhaseTimer t(h, s, GPT_PHASE_INIT);
+    GPT_CUDA(launch_init(pl.bv, d_xu, h->xs, pl.ns, s));
+    GPT_CUDA(launch_merit(pl.bv, pl.P, 1, d_xu, nullptr, d_goal, h->xs, h->knot_merit, pl.ns, s));
+    GPT_CUDA(launch_accept(pl.bv, 0, pl.SP, h->knot_merit, nullptr, nullptr, nullptr, nullptr, pl.ns, s));
+    return GPT_OK;
+}
+
+// One SQP iteration for every active instance (toplevel.cuh:254-446); leaves the number of
+// instances still active in h->d_active.
+static gpt_status enqueue_iteration(gpt_handle *h, const SqpPlan &pl, const float *d_goal, float *d_lambda,
+                                    float *d_xu, cudaStream_t s)
+{
+    const BatchView &bv = pl.bv;
+    const SolverParams &SP = pl.SP;
+    const int ns = pl.ns;
+    const bool f64 = SP.pcg_precond == 1 && SP.schur_fp64;
+    const float *S_rows = f64 ? reinterpret_cast<const float *>(h->S64) : h->S;
+    {
+        PhaseTimer t(h, s, GPT_PHASE_KKT);
+        GPT_CUDA(launch_kkt(bv, pl.P, d_xu, d_goal, h->xs, h->G, h->C, h->g, h->c, ns, s));
+    }
+    {
+        PhaseTimer t(h, s, GPT_PHASE_SCHUR);
+        if (f64)
+            GPT_CUDA(launch_schur64(bv, h->G, h->C, h->g, h->c, h->S64, h->gamma64, h->Ginv, h->Ginv64, ns, s));
+        else
+            GPT_CUDA(launch_schur(1, bv, 0.f, h->G, h->C, h->g, h->c, h->S, nullptr, h->gamma, h->Ginv, h->Ginv64,
+                                  nullptr, SP.pcg_precond == 0 ? 1 : 0, ns, s));
+    }
+    {
+        PhaseTimer t(h, s, GPT_PHASE_PCG);
+        GPT_CUDA(launch_pcg(bv, pl.maxN, pl.minN, f64 ? 2 : 1, (int)SP.pcg_precond, S_rows, nullptr, h->gamma,
+                            h->gamma64, d_lambda, h->lam64, h->crw, (int)SP.pcg_max_iter, SP.pcg_tol,
+                            (int)SP.pcg_exit_mode, nullptr, h->pcg_log, (int)SP.sqp_max_iter,
+                            (int)SP.pcg_cluster_size, ns, s));
+    }
+    {
+        PhaseTimer t(h, s, GPT_PHASE_DZ);
+        GPT_CUDA(launch_dz(bv, h->Ginv, h->Ginv64, h->C, h->g, d_lambda, h->lam64, h->dz, ns, s));
+    }
+    {
+        PhaseTimer t(h, s, GPT_PHASE_MERIT);
+        GPT_CUDA(launch_merit(bv, pl.P, NUM_ALPHAS, d_xu, h->dz, d_goal, h->xs, h->knot_merit, ns, s));
+    }
+    GPT_CUDA(cudaMemsetAsync(h->d_active, 0, sizeof(uint32_t), s));
+    {
+        PhaseTimer t(h, s, GPT_PHASE_ACCEPT);
+        GPT_CUDA(launch_accept(bv, 1, SP, h->knot_merit, h->dz, d_xu, nullptr, h->d_active, ns, s));
+    }
+    return GPT_OK;
+}
+
+// Loop control of the graph's while node: counts the iterations and continues while an
+// instance is active and fewer than sqp_max_iter iterations ran (the count bounds the loop
+// even if the activity flags were never cleared).
+__global__ void sqp_continue_kernel(cudaGraphConditionalHandle cond, const uint32_t *__restrict__ active,
+                                    uint32_t *__restrict__ iter, uint32_t max_iter)
+{
+    const uint32_t it = *iter + 1u;
+    *iter = it;
+    cudaGraphSetConditional(cond, (*active > 0u && it < max_iter) ? 1u : 0u);
+}
+
+// The whole solve as one CUDA graph: prologue, then a while node whose body is one SQP
+// iteration followed by sqp_continue_kernel.  Built by stream capture on the handle's
+// private streams for each (batch shape, parameters) and cached.
+static gpt_status sqp_graph_for(gpt_handle *h, const SqpPlan &pl, cudaGraphExec_t *out)
+{
+    GraphKey key;
+    std::memset(&key, 0, sizeof(key));
+    key.B = pl.bv.B;
+    key.total = pl.bv.total_knots;
+    key.maxN = pl.maxN;
+    key.minN = pl.minN;
+    key.P = pl.P;
+    key.SP = pl.SP;
+    for (auto &e : h->graphs)
+        if (std::memcmp(&e.key, &key, sizeof(key)) == 0) {
+            *out = e.exec;
+            return GPT_OK;
+        }
+    cudaStream_t cs = h->cap_stream, bs = h->body_stream;
+    cudaGraph_t graph = nullptr;
+    GPT_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeRelaxed));
+    gpt_status st = enqueue_prologue(h, pl, h->ggoal, h->gxu, cs);
+    if (st == GPT_OK) {
+        cudaError_t e = cudaMemsetAsync(h->d_iter, 0, sizeof(uint32_t), cs);
+        cudaStreamCaptureStatus cst;
+        const cudaGraphNode_t *deps = nullptr;
+        size_t ndeps = 0;
+        if (e == cudaSuccess) e = cudaStreamGetCaptureInfo(cs, &cst, nullptr, &graph, &deps, &ndeps);
+        cudaGraphConditionalHandle cond;
+        if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&cond, graph, 1u, cudaGraphCondAssignDefault);
+        cudaGraphNodeParams cp = {};
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = cond;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        cudaGraphNode_t node;
+        if (e == cudaSuccess) e = cudaGraphAddNode(&node, graph, deps, ndeps, &cp);
+        if (e == cudaSuccess) e = cudaStreamUpdateCaptureDependencies(cs, &node, 1, cudaStreamSetCaptureDependencies);
+        if (e == cudaSuccess) {
+            cudaGraph_t body = cp.conditional.phGraph_out[0];
+            e = cudaStreamBeginCaptureToGraph(bs, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed);
+            if (e == cudaSuccess) {
+                st = enqueue_iteration(h, pl, h->ggoal, h->glam, h->gxu, bs);
+                if (st == GPT_OK) {
+                    sqp_continue_kernel<<<1, 1, 0, bs>>>(cond, h->d_active, h->d_iter, pl.SP.sqp_max_iter);
+                    e = cudaGetLastError();
+                }
+                cudaGraph_t body_out = nullptr;
+                const cudaError_t e2 = cudaStreamEndCapture(bs, &body_out);
+                if (e == cudaSuccess) e = e2;
+            }
+        }
+        if (e != cudaSuccess && st == GPT_OK) st = cuda_err(e, "SQP graph capture");
+    }
+    cudaGraph_t captured = nullptr;
+    const cudaError_t ee = cudaStreamEndCapture(cs, &captured);
+    if (st != GPT_OK) {
+        if (captured) cudaGraphDestroy(captured);
+        return st;
+    }
+    if (ee != cudaSuccess) return cuda_err(ee, "cudaStreamEndCapture");
+    cudaGraphExec_t exec = nullptr;
+    const cudaError_t ei = cudaGraphInstantiate(&exec, captured, 0);
+    cudaGraphDestroy(captured);
+    if (ei != cudaSuccess) return cuda_err(ei, "cudaGraphInstantiate");
+    h->graphs.push_back({key, exec});
+    *out = exec;
+    return GPT_OK;
+}
+
 static gpt_status sqp_run(gpt_handle *h, uint32_t B, const uint32_t *Ns, const float *d_goal, float *d_lambda,
                           float *d_xu, float *h_rho, float rho_reset, gpt_sqp_stats *h_stats, uint32_t *h_pcg_iters,
                           uint8_t *h_pcg_exit, cudaStream_t s)
@@ -520,52 +694,35 @@ static gpt_status sqp_run(gpt_handle *h, uint32_t B, const uint32_t *Ns, const f
     }
     const ProblemParams P = to_params(h->pc);
     const SolverParams SP = to_solver(h->sc);
-    const int ns = h->num_sms;
-    const bool f64 = SP.pcg_precond == 1 && SP.schur_fp64;
-    const float *S_rows = f64 ? reinterpret_cast<const float *>(h->S64) : h->S;
+    const SqpPlan plan{bv, P, SP, maxN, minN, h->num_sms};
 
-    {
-        PhaseTimer t(h, s, GPT_PHASE_INIT);
-        GPT_CUDA(launch_init(bv, d_xu, h->xs, ns, s));
-        GPT_CUDA(launch_merit(bv, P, 1, d_xu, nullptr, d_goal, h->xs, h->knot_merit, ns, s));
-        GPT_CUDA(launch_accept(bv, 0, SP, h->knot_merit, nullptr, nullptr, nullptr, nullptr, ns, s));
-    }
-    for (uint32_t it = 0; it < SP.sqp_max_iter; ++it) {
+    if (SP.sqp_graph && !h->profile) {
+        // one graph launch for the whole solve on handle-owned copies of the caller's buffers
+        const size_t nxu = (size_t)NX * bv.total_knots - NC, nl = (size_t)NS * bv.total_knots;
+        GPT_CUDA(cudaMemcpyAsync(h->gxu, d_xu, sizeof(float) * nxu, cudaMemcpyDeviceToDevice, s));
+        GPT_CUDA(cudaMemcpyAsync(h->glam, d_lambda, sizeof(float) * nl, cudaMemcpyDeviceToDevice, s));
+        GPT_CUDA(cudaMemcpyAsync(h->ggoal, d_goal, sizeof(float) * 6 * bv.total_knots, cudaMemcpyDeviceToDevice, s));
+        cudaGraphExec_t exec = nullptr;
         {
-            PhaseTimer t(h, s, GPT_PHASE_KKT);
-            GPT_CUDA(launch_kkt(bv, P, d_xu, d_goal, h->xs, h->G, h->C, h->g, h->c, ns, s));
+            const gpt_status st = sqp_graph_for(h, plan, &exec);
+            if (st != GPT_OK) return st;
         }
+        GPT_CUDA(cudaGraphLaunch(exec, s));
+        GPT_CUDA(cudaMemcpyAsync(d_xu, h->gxu, sizeof(float) * nxu, cudaMemcpyDeviceToDevice, s));
+        GPT_CUDA(cudaMemcpyAsync(d_lambda, h->glam, sizeof(float) * nl, cudaMemcpyDeviceToDevice, s));
+    } else {
         {
-            PhaseTimer t(h, s, GPT_PHASE_SCHUR);
-            if (f64)
-                GPT_CUDA(launch_schur64(bv, h->G, h->C, h->g, h->c, h->S64, h->gamma64, h->Ginv, h->Ginv64, ns, s));
-            else
-                GPT_CUDA(launch_schur(1, bv, 0.f, h->G, h->C, h->g, h->c, h->S, nullptr, h->gamma, h->Ginv,
-                                      h->Ginv64, nullptr, SP.pcg_precond == 0 ? 1 : 0, ns, s));
+            const gpt_status st = enqueue_prologue(h, plan, d_goal, d_xu, s);
+            if (st != GPT_OK) return st;
         }
-        {
-            PhaseTimer t(h, s, GPT_PHASE_PCG);
-            GPT_CUDA(launch_pcg(bv, maxN, minN, f64 ? 2 : 1, (int)SP.pcg_precond, S_rows, nullptr, h->gamma, h->gamma64, d_lambda, h->lam64, h->crw, (int)SP.pcg_max_iter, SP.pcg_tol,
-                                (int)SP.pcg_exit_mode, nullptr, h->pcg_log, (int)SP.sqp_max_iter,
-                                (int)SP.pcg_cluster_size, ns, s));
+        for (uint32_t it = 0; it < SP.sqp_max_iter; ++it) {
+            const gpt_status st = enqueue_iteration(h, plan, d_goal, d_lambda, d_xu, s);
+            if (st != GPT_OK) return st;
+            GPT_CUDA(cudaMemcpyAsync(h->h_active, h->d_active, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+            GPT_CUDA(cudaEventRecord(h->ev, s));
+            GPT_CUDA(cudaEventSynchronize(h->ev));
+            if (*h->h_active == 0) break;
         }
-        {
-            PhaseTimer t(h, s, GPT_PHASE_DZ);
-            GPT_CUDA(launch_dz(bv, h->Ginv, h->Ginv64, h->C, h->g, d_lambda, h->lam64, h->dz, ns, s));
-        }
-        {
-            PhaseTimer t(h, s, GPT_PHASE_MERIT);
-            GPT_CUDA(launch_merit(bv, P, NUM_ALPHAS, d_xu, h->dz, d_goal, h->xs, h->knot_merit, ns, s));
-        }
-        GPT_CUDA(cudaMemsetAsync(h->d_active, 0, sizeof(uint32_t), s));
-        {
-            PhaseTimer t(h, s, GPT_PHASE_ACCEPT);
-            GPT_CUDA(launch_accept(bv, 1, SP, h->knot_merit, h->dz, d_xu, nullptr, h->d_active, ns, s));
-        }
-        GPT_CUDA(cudaMemcpyAsync(h->h_active, h->d_active, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
-        GPT_CUDA(cudaEventRecord(h->ev, s));
-        GPT_CUDA(cudaEventSynchronize(h->ev));
-        if (*h->h_active == 0) break;
     }
     GPT_CUDA(cudaMemcpyAsync(h->h_st, h->st, sizeof(InstState) * B, cudaMemcpyDeviceToHost, s));
     if (h_pcg_iters || h_pcg_exit)

@@ -21,6 +21,7 @@ struct SolverParams {
     uint32_t pcg_cluster_size;  // 0: chosen from N and the batch size
     uint32_t pcg_precond;       // 0 block-Jacobi (reference), 1 chunk block-tridiagonal LDL^T
     uint32_t schur_fp64;        // with pcg_precond 1: FP64 Schur formation and rows
+    uint32_t sqp_graph;         // the SQP loop as one CUDA graph with a device-side while loop
 };
 
 cudaError_t launch_kkt(const BatchView &bv, const ProblemParams &P, const float *xu, const float *goal,

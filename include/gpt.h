@@ -86,6 +86,10 @@ typedef struct gpt_solver_config {
     uint32_t schur_fp64;       /* SQP loop and adjoint with pcg_precond 1: 1 (default) forms and stores the
                                   Schur complement in FP64; 0 in FP32 as the reference does (schur.cuh:391-524).
                                   FP32 formation moves the solution by ~cond(S) x 1e-7 (~1e-2 at cond 1e7) */
+    uint32_t sqp_graph;        /* 1 (default): a solve runs as one CUDA graph (built on the first call of each
+                                  batch shape and cached) whose while node repeats the SQP iteration on the
+                                  device; 0: one host synchronisation per SQP iteration, as the reference loop.
+                                  Profiling (gpt_set_profiling) uses the host loop. */
 } gpt_solver_config;
 
 /* One sqpSolve's outcome (the reference returns a tuple, toplevel.cuh:502) */
