@@ -242,6 +242,8 @@ def main():
         return e0.elapsed_time(e1), stats
 
     last_rho = [1e-3] * B
+    # the PCG cluster size for this batch shape, chosen by timing (gpt_autotune) unless given
+    tuned_cs = args.pcg_cluster if args.pcg_cluster else sv.autotune(Ns, goal, lam0, xu0, [1e-3] * B)
 
     for _ in range(args.warmup):
         one_step()
@@ -344,6 +346,9 @@ def main():
     sv1 = gpt.Solver(max_knot_points=N, max_batch=1, **SPEC)
     sv1.set_solver(sqp_max_iter=args.sqp_max_iter, pcg_max_iter=args.pcg_max_iter, pcg_exit_tol=args.tol,
                    pcg_exit_mode=0, pcg_precond=args.pcg_precond)
+    p = P.make_problem(N, rank * B, dt=SPEC["timestep"])
+    plain_cs = args.pcg_cluster if args.pcg_cluster else sv1.autotune(
+        [N], *(torch.as_tensor(p[k], device="cuda") for k in ("goal", "lam", "xu")), [1e-3])
     for i in range(args.plain_solves + 1):
         p = P.make_problem(N, rank * B + i, dt=SPEC["timestep"])
         x1, g1, l1 = (torch.as_tensor(p[k], device="cuda") for k in ("xu", "goal", "lam"))
@@ -387,7 +392,8 @@ def main():
                                f"QD=0.01, R=1e-4, PCG {precond_name} rel-res {args.tol:g} (max {args.pcg_max_iter} it), "
                                f"<= {args.sqp_max_iter} SQP iterations",
                    "instances_per_gpu": B, "knot_points": N, "pcg_exit_tol": args.tol, "parallelism": f"dp{world}",
-                   "pcg_precond": precond_name,
+                   "pcg_precond": precond_name, "pcg_cluster_size": tuned_cs,
+                   "pcg_cluster_source": "given" if args.pcg_cluster else "gpt_autotune",
                    "l2": "256 MB buffer written between timed steps"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": (PCG_CHAIN_DRAM_BYTES_PER_KNOT * N * B if args.pcg_precond == 1 else None),
@@ -402,7 +408,7 @@ def main():
         "gpu_launches": int(launches_total),
         "clocks": clk,
         "adjoint": adjoint,
-        "plain_solves_per_s": plain_rate,
+        "plain_solves_per_s": plain_rate, "plain_pcg_cluster_size": plain_cs,
         "batched_over_plain": (value / world) / plain_rate if plain_rate else None,
         "phase_ms_per_step": {k: v[0] for k, v in phases.items()},
         "phase_launches_per_step": {k: v[1] for k, v in phases.items()},

@@ -32,7 +32,7 @@ EXPORTED = [
     "gpt_set_solver_config", "gpt_last_error", "gpt_version", "gpt_sqp_solve", "gpt_sqp_solve_batched",
     "gpt_form_kkt", "gpt_form_schur", "gpt_form_schur_csc", "gpt_prep_csr", "gpt_pcg", "gpt_compute_dz",
     "gpt_compute_merit", "gpt_ls_compute_merit", "gpt_set_profiling", "gpt_get_phase_stats",
-    "gpt_ls_compute_merit_noalloc", "gpt_sqp_adjoint", "gpt_set_cost_weights",
+    "gpt_ls_compute_merit_noalloc", "gpt_sqp_adjoint", "gpt_set_cost_weights", "gpt_autotune",
 ]
 PHASES = ["init", "kkt", "schur", "pcg", "dz", "merit", "accept"]
 
@@ -119,6 +119,7 @@ def _declare(L):
         "gpt_ls_compute_merit_noalloc": ([P(ProblemConfig), u32, vp, vp, vp, vp, vp, vp], C.c_int),
         "gpt_sqp_adjoint": ([vp, u32, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp], C.c_int),
         "gpt_set_cost_weights": ([vp, f32, f32, f32], C.c_int),
+        "gpt_autotune": ([vp, u32, vp, vp, vp, vp, vp, P(u32), vp], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -259,6 +260,16 @@ class Solver:
                                            _ptr(xu), C.cast(rr, C.c_void_p), rho_reset, C.cast(sts, C.c_void_p),
                                            _stream(stream)))
         return list(rr), [s.as_dict() for s in sts]
+
+    def autotune(self, knot_points: Sequence[int], eePos_traj, lam, xu, rho: Sequence[float], stream=None) -> int:
+        """gpt_autotune: pick and remember the fastest PCG cluster size for this batch shape."""
+        B = len(knot_points)
+        Ns = (C.c_uint32 * B)(*knot_points)
+        rr = (C.c_float * B)(*rho)
+        cs = C.c_uint32(0)
+        _check(lib().gpt_autotune(self._h, B, C.cast(Ns, C.c_void_p), _ptr(eePos_traj), _ptr(lam), _ptr(xu),
+                                  C.cast(rr, C.c_void_p), C.byref(cs), _stream(stream)))
+        return cs.value
 
     def sqp_adjoint(self, knot_points: Sequence[int], eePos_traj, xs, xu, rho: Sequence[float], grad_xu_next,
                     xu_next=None, stream=None):

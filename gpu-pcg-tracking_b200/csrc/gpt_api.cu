@@ -74,6 +74,12 @@ struct gpt_handle {
     uint32_t *d_iter = nullptr;
     cudaStream_t cap_stream = nullptr, body_stream = nullptr;
     std::vector<GraphEntry> graphs;
+    // autotuned PCG cluster size per batch shape (gpt_autotune); used when pcg_cluster_size is 0
+    struct Tuned {
+        int B, total, maxN, minN;
+        uint32_t cluster;
+    };
+    std::vector<Tuned> tuned;
     uint32_t cap_sqp_iter = 0;  // pcg_log rows allocated at creation
     // pinned host staging
     uint32_t *h_active = nullptr;
@@ -693,7 +699,11 @@ static gpt_status sqp_run(gpt_handle *h, uint32_t B, const uint32_t *Ns, const f
         if (st != GPT_OK) return st;
     }
     const ProblemParams P = to_params(h->pc);
-    const SolverParams SP = to_solver(h->sc);
+    SolverParams SP = to_solver(h->sc);
+    if (SP.pcg_cluster_size == 0) {
+        for (const auto &t : h->tuned)
+            if (t.B == bv.B && t.total == bv.total_knots && t.maxN == maxN && t.minN == minN) SP.pcg_cluster_size = t.cluster;
+    }
     const SqpPlan plan{bv, P, SP, maxN, minN, h->num_sms};
 
     if (SP.sqp_graph && !h->profile) {
@@ -774,6 +784,85 @@ gpt_status gpt_sqp_solve_batched(gpt_handle *h, uint32_t B, const uint32_t *h_N,
     if (!h || !h_N || !d_goal || !d_lambda || !d_xu) return set_err(GPT_ERR_BAD_ARG, "null argument");
     return sqp_run(h, B, h_N, d_goal, d_lambda, d_xu, h_rho, rho_reset, h_stats, nullptr, nullptr,
                    (cudaStream_t)stream);
+}
+
+gpt_status gpt_autotune(gpt_handle *h, uint32_t B, const uint32_t *h_N, const float *d_goal, const float *d_lambda,
+                        const float *d_xu, const float *h_rho, uint32_t *h_cluster_out, gpt_stream_t stream)
+{
+    if (!h || !h_N || !d_goal || !d_lambda || !d_xu || !h_rho) return set_err(GPT_ERR_BAD_ARG, "null argument");
+    if (B == 0 || B > h->pc.max_batch) return set_err(GPT_ERR_CAPACITY, "batch exceeds handle capacity");
+    cudaStream_t s = (cudaStream_t)stream;
+    int total = 0, maxN = 0, minN = 1 << 30;
+    for (uint32_t b = 0; b < B; ++b) {
+        if (!check_n(h, h_N[b])) return set_err(GPT_ERR_BAD_ARG, "knot_points out of range");
+        total += (int)h_N[b];
+        maxN = (int)h_N[b] > maxN ? (int)h_N[b] : maxN;
+        minN = (int)h_N[b] < minN ? (int)h_N[b] : minN;
+    }
+    if ((size_t)total > h->cap_knots) return set_err(GPT_ERR_CAPACITY, "total knots exceed workspace");
+    // candidates: the smallest cluster that holds the longest horizon (<= 128 knots per CTA) and 2x, 4x it
+    int cs0 = 1;
+    while ((maxN + cs0 - 1) / cs0 > PCG_KPC_MAX) cs0 *= 2;
+    std::vector<uint32_t> cand;
+    for (int cs = cs0; cs <= 16 && cs <= 4 * cs0 && cs <= minN; cs *= 2) cand.push_back((uint32_t)cs);
+    if (cand.empty()) cand.push_back((uint32_t)cs0);
+    const gpt_solver_config saved = h->sc;
+    const int saved_profile = h->profile;
+    h->profile = 0;
+    const size_t nxu = (size_t)NX * total - NC, nl = (size_t)NS * total;
+    std::vector<float> rho(h_rho, h_rho + B);
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    gpt_status st = GPT_OK;
+    float best_ms = 1e30f;
+    uint32_t best = cand[0];
+    if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) st = set_err(GPT_ERR_CUDA, "event");
+    for (size_t ci = 0; ci < cand.size() && st == GPT_OK; ++ci) {
+        h->sc = saved;
+        h->sc.pcg_cluster_size = cand[ci];
+        h->sc.sqp_max_iter = saved.sqp_max_iter < 2 ? saved.sqp_max_iter : 2;
+        float ms_min = 1e30f;
+        for (int rep = 0; rep < 3 && st == GPT_OK; ++rep) {  // first repetition warms up (attributes, caches)
+            // the solve updates xu and lambda in place: run it on scratch copies
+            cudaError_t e = cudaMemcpyAsync(h->adj_h, d_xu, sizeof(float) * nxu, cudaMemcpyDeviceToDevice, s);
+            if (e == cudaSuccess) e = cudaMemcpyAsync(h->adj_lam, d_lambda, sizeof(float) * nl, cudaMemcpyDeviceToDevice, s);
+            if (e == cudaSuccess) e = cudaEventRecord(e0, s);
+            if (e != cudaSuccess) {
+                st = cuda_err(e, "autotune");
+                break;
+            }
+            std::vector<float> r = rho;
+            st = sqp_run(h, B, h_N, d_goal, h->adj_lam, h->adj_h, r.data(), 1e-3f, nullptr, nullptr, nullptr, s);
+            if (st == GPT_ERR_NONFINITE) st = GPT_OK;  // timing only
+            if (st != GPT_OK) break;
+            float ms = 0.f;
+            e = cudaEventRecord(e1, s);
+            if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+            if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+            if (e != cudaSuccess) {
+                st = cuda_err(e, "autotune timing");
+                break;
+            }
+            if (rep > 0 && ms < ms_min) ms_min = ms;
+        }
+        if (st == GPT_OK && ms_min < best_ms) {
+            best_ms = ms_min;
+            best = cand[ci];
+        }
+    }
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    h->sc = saved;
+    h->profile = saved_profile;
+    if (st != GPT_OK) return st;
+    bool found = false;
+    for (auto &t : h->tuned)
+        if (t.B == (int)B && t.total == total && t.maxN == maxN && t.minN == minN) {
+            t.cluster = best;
+            found = true;
+        }
+    if (!found) h->tuned.push_back({(int)B, total, maxN, minN, best});
+    if (h_cluster_out) *h_cluster_out = best;
+    return GPT_OK;
 }
 
 gpt_status gpt_sqp_adjoint(gpt_handle *h, uint32_t B, const uint32_t *h_N, const float *d_goal, const float *d_xs,

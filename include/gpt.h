@@ -145,6 +145,18 @@ gpt_status gpt_sqp_solve_batched(gpt_handle *h, uint32_t batch, const uint32_t *
                                  const float *d_eePos_traj, float *d_lambda, float *d_xu, float *h_rho,
                                  float rho_reset, gpt_sqp_stats *h_stats, gpt_stream_t stream);
 
+/* Autotuner (no reference counterpart): times two SQP iterations of this batch
+ * (on copies of d_xu, d_lambda; the inputs are not modified) for each candidate
+ * PCG cluster size -- the smallest that holds the longest horizon in
+ * <= 128 knots per CTA, and twice and four times it, up to 16 and to the
+ * shortest horizon -- and remembers the fastest for this batch shape
+ * (instances, total knots, longest and shortest horizon).  Later solves of
+ * that shape use it while pcg_cluster_size is 0.  h_cluster_out (optional)
+ * receives the choice. */
+gpt_status gpt_autotune(gpt_handle *h, uint32_t batch, const uint32_t *h_knot_points, const float *d_eePos_traj,
+                        const float *d_lambda, const float *d_xu, const float *h_rho, uint32_t *h_cluster_out,
+                        gpt_stream_t stream);
+
 /* Adjoint of the SQP step (no reference counterpart).  At the iterate d_xu
  * (typically a solve's result) with per-instance rho h_rho and initial states
  * d_xs (14 per instance, x_0 of the solve's initial guess), the step solves

@@ -468,3 +468,26 @@ def test_sqp_graph_equals_host_loop(gpt, problem_mod):
         assert i0 == i1 and r0 == r1, (i0, i1, r0, r1)
         np.testing.assert_array_equal(x0, x1)
         np.testing.assert_array_equal(l0, l1)
+
+
+def test_autotune_choice_is_used(gpt, problem_mod):
+    """gpt_autotune leaves its inputs unchanged, returns one of its candidate cluster
+    sizes, and a later solve of that batch shape with pcg_cluster_size 0 equals a
+    solve with that size given explicitly, bit for bit."""
+    N = 64
+    p = problem_mod.make_problem(N, 9, dt=0.01)
+    goal, xu0, lam0 = dev(p["goal"]), dev(p["xu"]), dev(p["lam"])
+    sv = gpt.Solver(max_knot_points=N, **SPEC_CFG)
+    sv.set_solver(sqp_max_iter=4)
+    x_in, l_in = xu0.clone(), lam0.clone()
+    cs = sv.autotune([N], goal, l_in, x_in, [1e-3])
+    assert torch.equal(x_in, xu0) and torch.equal(l_in, lam0)
+    assert cs in (1, 2, 4)
+    out = []
+    for given in (0, cs):
+        sv.set_solver(pcg_cluster_size=given)
+        xu, lam = xu0.clone(), lam0.clone()
+        sv.sqp_solve(N, goal, lam, xu, 1e-3)
+        out.append(host(xu))
+    sv.close()
+    np.testing.assert_array_equal(out[0], out[1])
