@@ -209,10 +209,12 @@ def main():
         dist.init_process_group("nccl", timeout=timedelta(seconds=120))
     gpt = importlib.import_module("gpu-pcg-tracking_b200")
     P = importlib.import_module("gpu-pcg-tracking_b200.problem")
+    shard = importlib.import_module("gpu-pcg-tracking_b200.shard")
 
     B, N = args.batch, args.knots
     Ns = [N] * B
-    batch = P.make_batch(Ns, seed0=rank * B, dt=SPEC["timestep"])
+    ids = shard.weak_scaling_ids(rank, world, B)  # this rank's instances (problem seeds)
+    batch = P.make_batch(Ns, seed0=ids[0], dt=SPEC["timestep"])
     sv = gpt.Solver(max_knot_points=N, max_batch=B, **SPEC)
     sv.set_solver(sqp_max_iter=args.sqp_max_iter, pcg_max_iter=args.pcg_max_iter, pcg_exit_tol=args.tol,
                   pcg_exit_mode=0, pcg_cluster_size=args.pcg_cluster, pcg_precond=args.pcg_precond)
@@ -269,10 +271,7 @@ def main():
     # SQP iteration, as many as the KKT launches)
     launches_per_step = sum(n for _, n in phases.values()) + phases["kkt"][1]
     total_ms = sum(step_ms)
-    if world > 1:
-        t = torch.tensor([total_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = shard.max_over_ranks(total_ms, device="cuda")
     ms_per_step = total_ms / args.steps
     value = world * B / (ms_per_step / 1000.0)
 
@@ -292,10 +291,7 @@ def main():
         if i > 0:
             adj_ms.append(e0.elapsed_time(e1))
     adj_step = statistics.mean(adj_ms)
-    if world > 1:
-        t = torch.tensor([adj_step], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        adj_step = float(t.item())
+    adj_step = shard.max_over_ranks(adj_step, device="cuda")
     adjoint = {"us_per_solve": 1000.0 * adj_step / B, "ms_per_batch": adj_step,
                "ratio_to_forward_solve": adj_step / ms_per_step,
                "workload": f"gpt_sqp_adjoint at the {B} solutions of the timed step (goal, QD, R, EE-weight gradients)"}
@@ -334,10 +330,7 @@ def main():
         if i > 0:
             e2e_ms.append(e0.elapsed_time(e1))
     e2e_step = statistics.mean(e2e_ms)
-    if world > 1:
-        t = torch.tensor([e2e_step], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_step = float(t.item())
+    e2e_step = shard.max_over_ranks(e2e_step, device="cuda")
     h2d = 4 * (h_xu.numel() + h_goal.numel() + h_lam.numel())
     d2h = 4 * (o_xu.numel() + o_lam.numel())
 
@@ -346,11 +339,11 @@ def main():
     sv1 = gpt.Solver(max_knot_points=N, max_batch=1, **SPEC)
     sv1.set_solver(sqp_max_iter=args.sqp_max_iter, pcg_max_iter=args.pcg_max_iter, pcg_exit_tol=args.tol,
                    pcg_exit_mode=0, pcg_precond=args.pcg_precond)
-    p = P.make_problem(N, rank * B, dt=SPEC["timestep"])
+    p = P.make_problem(N, ids[0], dt=SPEC["timestep"])
     plain_cs = args.pcg_cluster if args.pcg_cluster else sv1.autotune(
         [N], *(torch.as_tensor(p[k], device="cuda") for k in ("goal", "lam", "xu")), [1e-3])
     for i in range(args.plain_solves + 1):
-        p = P.make_problem(N, rank * B + i, dt=SPEC["timestep"])
+        p = P.make_problem(N, ids[0] + i, dt=SPEC["timestep"])
         x1, g1, l1 = (torch.as_tensor(p[k], device="cuda") for k in ("xu", "goal", "lam"))
         flush.fill_(1.0)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
