@@ -25,6 +25,7 @@ STATUS_NAMES = {0: "OK", 1: "BAD_ARG", 2: "CUDA", 3: "NO_DEVICE", 4: "CAPACITY",
 EXIT_RHO_MAX, EXIT_PCG_MAXITER, EXIT_NONFINITE, EXIT_ITER_LIMIT = 1, 2, 4, 8
 
 STATE_SIZE, CONTROL_SIZE = 14, 7
+PCG_WARP_PAIR = 32  # GPT_PCG_WARP_PAIR: pcg_cluster_size of the one-CTA-per-instance warp-pair PCG
 
 # The C-ABI entry points include/gpt.h declares (checked by the CPU tests).
 EXPORTED = [

@@ -10,6 +10,7 @@ namespace gpt {
 
 constexpr int MAX_PCG_KNOTS = 512;  // horizon limit of this build (16-CTA cluster x 32 knots)
 constexpr int PCG_KPC_MAX = 128;    // knots per CTA held in shared memory by the PCG
+constexpr int PCG_WARP_PAIR = 32;   // pcg_cluster_size value selecting pcg_pair_kernel (one 128-thread CTA per instance)
 
 // SQP control constants (settings.cuh:31-50 and the -D flags of perform_experiment.sh:42-58)
 struct SolverParams {
@@ -37,7 +38,8 @@ int pcg_pick_cluster(int maxN, int B, int num_sms, int requested);
 // cr_ws: FP64 workspace of 196 doubles per knot of the batch (the cyclic-reduction
 // couplings of precond 1; unused by precond 0)
 // fmt 0: reference 3-block rows (S, Pinv floats); 1: packed FP32 rows (PK); 2: packed FP64 rows (PK64,
-// S points at doubles) with FP64 gamma64 -- chain preconditioner only
+// S points at doubles) with FP64 gamma64 -- chain preconditioner only.  cluster_size PCG_WARP_PAIR runs
+// pcg_pair_kernel (precond 1, fmt 1 or 2; cr_ws holds its factors and FP64 vectors)
 cudaError_t launch_pcg(const BatchView &bv, int max_n_knots, int min_n_knots, int fmt, int precond, const float *S,
                        const float *Pinv, const float *gamma, const double *gamma64, float *lambda, double *lambda64,
                        double *cr_ws, int max_iter, float tol, int exit_mode, uint32_t *out_iters, uint32_t *pcg_log,
@@ -62,6 +64,9 @@ cudaError_t launch_adjoint_grad(const BatchView &bv, const ProblemParams &P, con
                                 float *grad_r, float *grad_qee, int num_sms, cudaStream_t s);
 cudaError_t launch_axpy(int n, float alpha, const float *x, const float *a, float *out, int num_sms, cudaStream_t s);
 size_t adjoint_part_floats();
+// reference 3-block FP32 rows -> FP64 packed rows (PK64) and gamma64 (input of the warp-pair PCG)
+cudaError_t launch_pack_rows64(int N, const float *S, const float *gamma, double *S64, double *gamma64, int num_sms,
+                               cudaStream_t s);
 
 }  // namespace gpt
 

@@ -1057,6 +1057,591 @@ __global__ void __launch_bounds__(PCG_THREADS, 1)
 }
 
 // ---------------------------------------------------------------------------
+// Warp-pair PCG: one 128-thread CTA per instance (pcg_cluster_size PCG_WARP_PAIR).
+//
+// The PCG of pcg_chain_kernel with one CTA per instance -- its preconditioner
+// is the exact inverse of the instance's S -- with the factorisation done by a
+// twisted block LDL^T instead of cyclic reduction.  With M = -S (SPD),
+// A_k = -S_kk and E_k = M_{k,k-1} = -L_k (L_k the left block of row k), and
+// m = (n-1)/2:
+//   warp 0, top-down:   D_0 = A_0,         D_k = A_k - E_k D_{k-1}^{-1} E_k^T,          k = 1..m
+//   warp 1, bottom-up:  U_{n-1} = A_{n-1}, U_k = A_k - E_{k+1}^T U_{k+1}^{-1} E_{k+1},  k = n-2..m+1
+//   then                T_m = D_m - E_{m+1}^T U_{m+1}^{-1} E_{m+1}
+// (the two warps run at the same time; the quadratic forms are sign-free, so
+// L is used for E).  M x = y is then solved by
+//   forward   t_k = D_k^{-1} y_k, y_{k+1} += L_{k+1} t_k          (k = 0..m-1)
+//             t_k = U_k^{-1} y_k, y_{k-1} += L_k^T t_k            (k = n-1..m+1)
+//   middle    x_m = T_m^{-1} y_m
+//   backward  x_k = t_k + D_k^{-1} L_{k+1}^T x_{k+1}              (k = m-1..0)
+//             x_k = t_k + U_k^{-1} L_k x_{k-1}                    (k = m+1..n-1)
+// and z = S^{-1} r = -x.  Warps 2-3 form the initial residual gamma - S lambda
+// while warps 0-1 factor.  Each elimination step is sequential, but a CTA
+// holds ~36 KB of shared memory at n = 128 (4 CTAs per SM), so a batch of up to
+// ~600 instances runs in one wave instead of one CTA per SM at a time.
+//
+// Storage: the inverse factors D_k^{-1}, U_k^{-1}, T_m^{-1} (packed lower
+// triangles, FP64) and the PCG vectors lambda, r, p, S p (FP64) live in the
+// FP64 workspace (196 doubles per knot); the solve's x and t in shared memory.
+// S is read from global memory (FP64 rows of schur64_kernel, or FP32 packed
+// rows), the next step's blocks loaded while the current step computes.
+constexpr int PAIR_THREADS = 128;
+constexpr int PAIR_NWARP = PAIR_THREADS / 32;
+constexpr int PW_STRIDE = SS, PW_INV = 0, PW_LAM = 105, PW_RES = 119, PW_P = 133, PW_V = 147;
+constexpr int PAIR_FWARP = 2 * 105 + SS;  // per factoring warp: two factor buffers and one coupling
+
+__host__ __device__ constexpr int pair_smem_doubles(int n)
+{
+    return 2 * NS * n + 2 * PAIR_FWARP + NS + 2 * PAIR_NWARP * 3 + 2;
+}
+size_t pcg_pair_smem_bytes(int n) { return sizeof(double) * (size_t)pair_smem_doubles(n); }
+
+// w[q] = (Ai X)(7 hh + q, c) with X(t, c) = Lw[t + 14 c] (TR: X = Lw^T); Ai packed lower triangle
+template <bool TR>
+__device__ __forceinline__ void pk_times(const double *Ai, const double *Lw, int cq, int hh, double (&w)[7])
+{
+    double xc[NS];
+#pragma unroll
+    for (int t = 0; t < NS; ++t) xc[t] = TR ? Lw[cq + NS * t] : Lw[t + NS * cq];
+#pragma unroll
+    for (int q = 0; q < 7; ++q) {
+        const int rr = 7 * hh + q;
+        double a = 0.0;
+#pragma unroll
+        for (int t = 0; t < NS; ++t) a = fma(Ai[tri_lo(rr, t)], xc[t], a);
+        w[q] = a;
+    }
+}
+// d[a] = (Y W)(a, c) with Y(a, t) = Lw[a + 14 t] (TR: Lw[t + 14 a]); both lanes of a pair get the sum
+template <bool TR>
+__device__ __forceinline__ void lw_times(const double *Lw, int hh, const double (&w)[7], double (&d)[NS])
+{
+#pragma unroll
+    for (int a = 0; a < NS; ++a) {
+        double acc = 0.0;
+#pragma unroll
+        for (int q = 0; q < 7; ++q) {
+            const int t = 7 * hh + q;
+            acc = fma(TR ? Lw[t + NS * a] : Lw[a + NS * t], w[q], acc);
+        }
+        d[a] = acc + __shfl_xor_sync(0xffffffffu, acc, 1);
+    }
+}
+// row r of a 14x14 block times v: lane (r, hh) sums columns 7 hh .. 7 hh + 6, the pair adds up
+__device__ __forceinline__ double pair_dot7(const double (&m)[7], const double *v, int hh)
+{
+    double a = 0.0;
+#pragma unroll
+    for (int q = 0; q < 7; ++q) a = fma(m[q], v[7 * hh + q], a);
+    return a + __shfl_xor_sync(0xffffffffu, a, 1);
+}
+template <typename ST, int CNT>
+__device__ __forceinline__ void warp_fetch(const ST *src, int n, int lane, double (&v)[CNT])
+{
+#pragma unroll
+    for (int i = 0; i < CNT; ++i) {
+        const int e = lane + 32 * i;
+        v[i] = (e < n) ? (double)__ldg(src + e) : 0.0;
+    }
+}
+
+template <int FMT>
+__global__ void __launch_bounds__(PAIR_THREADS, 4)
+    pcg_pair_kernel(BatchView bv, const void *__restrict__ Sv, const float *__restrict__ gamma,
+                    const double *__restrict__ gamma64, float *__restrict__ lambda, double *__restrict__ lambda64,
+                    double *__restrict__ ws, int max_iter, float tol, int exit_mode, uint32_t *__restrict__ out_iters,
+                    uint32_t *__restrict__ pcg_log, int log_stride)
+{
+    static_assert(FMT == 1 || FMT == 2, "packed rows only");
+    using ST = typename std::conditional<FMT == 2, double, float>::type;
+    const ST *S = reinterpret_cast<const ST *>(Sv);
+    const size_t ks = FMT == 2 ? PK64 : PK;
+    const int b = blockIdx.x;
+    if (b >= bv.B || !bv.active(b)) return;
+    const int n = bv.N(b), m = (n - 1) / 2, nv = NS * n;
+    const size_t kg0 = (size_t)bv.off(b);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+
+    extern __shared__ double pair_dyn_smem[];
+    double *xv = pair_dyn_smem;        // 14 n: the solve's vector (y, then x); lambda_0 during set-up
+    double *tv = xv + nv;              // 14 n: t_k of the solve
+    double *fw0 = tv + nv;             // warp 0: D buffers (2 x 105), coupling / scratch (196)
+    double *fw1 = fw0 + PAIR_FWARP;    // warp 1: U buffers, coupling / scratch
+    double *ubot = fw1 + PAIR_FWARP;   // 14: L_{m+1}^T t_{m+1} from the bottom sweep
+    double *red = ubot + NS;           // 2 sets x 4 warps x 3
+    double *ginit = red + 2 * PAIR_NWARP * 3;  // gamma . gamma partials of warps 2, 3
+
+    const ST *Sb = S + kg0 * ks;
+    double *wsb = ws + kg0 * PW_STRIDE;
+    auto wsv = [&](int slot, int e) -> double & { return wsb[(size_t)(e / NS) * PW_STRIDE + slot + e % NS]; };
+    const float *gb = (FMT == 2) ? nullptr : gamma + NS * kg0;
+    const double *gb64 = (FMT == 2) ? gamma64 + NS * kg0 : nullptr;
+    auto gam = [&](int e) -> double { return (FMT == 2) ? gb64[e] : (double)gb[e]; };
+    float *lb = lambda + NS * kg0;
+
+    // (S v)_e with FP64 accumulation (same order as pcg_chain_kernel's rows)
+    auto srow = [&](int e, const double *v) -> double {
+        const int k = e / NS, r = e - NS * k;
+        const ST *row = Sb + (size_t)k * ks;
+        double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+        ST fd[NS];
+#pragma unroll
+        for (int cc = 0; cc < NS; ++cc) fd[cc] = __ldg(row + PK_DIAG + tri_lo(r, cc));
+        if (k > 0) {
+            ST fl[NS];
+#pragma unroll
+            for (int cc = 0; cc < NS; ++cc) fl[cc] = __ldg(row + r + NS * cc);
+#pragma unroll
+            for (int cc = 0; cc < NS; ++cc) a0 = fma((double)fl[cc], v[NS * (k - 1) + cc], a0);
+        }
+#pragma unroll
+        for (int cc = 0; cc < NS; ++cc) a1 = fma((double)fd[cc], v[NS * k + cc], a1);
+        if (k < n - 1) {
+            ST fr[NS];
+#pragma unroll
+            for (int cc = 0; cc < NS; ++cc) fr[cc] = __ldg(row + ks + cc + NS * r);
+#pragma unroll
+            for (int cc = 0; cc < NS; ++cc) a2 = fma((double)fr[cc], v[NS * (k + 1) + cc], a2);
+        }
+        return (a0 + a1) + a2;
+    };
+
+    const int c = lane >> 1, hh = lane & 1;
+    const bool cval = c < NS;
+    const int cq = cval ? c : NS - 1;
+    // D -= d (lower triangle of column c, rows of the lane's parity)
+    auto sub_lower = [&](double *D, const double (&d)[NS]) {
+        if (cval) {
+#pragma unroll
+            for (int a = 0; a < NS; ++a)
+                if (a >= c && (a & 1) == hh) D[((a * (a + 1)) >> 1) + c] -= d[a];
+        }
+    };
+    auto store_inv = [&](const double *Di, int k) {
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const int e = lane + 32 * i;
+            if (e < 105) wsb[(size_t)k * PW_STRIDE + PW_INV + e] = Di[e];
+        }
+    };
+
+    // ---- factorisation (warps 0, 1) and initial residual (warps 2, 3)
+    if (warp == 0) {
+        double *Lw = fw0 + 210;
+        double pre[10];  // row k: left block (196) then diagonal triangle (105)
+        warp_fetch<ST, 10>(Sb, SS + 105, lane, pre);
+        for (int k = 0; k <= m; ++k) {
+            double *Dc = fw0 + 105 * (k & 1), *Dp = fw0 + 105 * ((k + 1) & 1);
+#pragma unroll
+            for (int i = 0; i < 10; ++i) {
+                const int e = lane + 32 * i;
+                if (e < SS) Lw[e] = pre[i];
+                else if (e < SS + 105) Dc[e - SS] = -pre[i];
+            }
+            __syncwarp();
+            if (k < m) warp_fetch<ST, 10>(Sb + (size_t)(k + 1) * ks, SS + 105, lane, pre);
+            if (k > 0) {
+                double w[7], d[NS];
+                pk_times<true>(Dp, Lw, cq, hh, w);
+                lw_times<false>(Lw, hh, w, d);
+                sub_lower(Dc, d);
+                __syncwarp();
+            }
+            if (k < m) {
+                warp_spd_inverse_packed(Dc, lane);
+                store_inv(Dc, k);
+            }
+        }
+    } else if (warp == 1) {
+        double *Lw = fw1 + 210;
+        if (n - 1 > m) {
+            double pd[4], pl[7];
+#pragma unroll
+            for (int i = 0; i < 7; ++i) pl[i] = 0.0;
+            warp_fetch<ST, 4>(Sb + (size_t)(n - 1) * ks + PK_DIAG, 105, lane, pd);
+            for (int k = n - 1; k > m; --k) {
+                double *Uc = fw1 + 105 * (k & 1), *Up = fw1 + 105 * ((k + 1) & 1);
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    const int e = lane + 32 * i;
+                    if (e < 105) Uc[e] = -pd[i];
+                }
+                if (k < n - 1) {
+#pragma unroll
+                    for (int i = 0; i < 7; ++i) {
+                        const int e = lane + 32 * i;
+                        if (e < SS) Lw[e] = pl[i];
+                    }
+                }
+                __syncwarp();
+                if (k - 1 > m) {
+                    warp_fetch<ST, 4>(Sb + (size_t)(k - 1) * ks + PK_DIAG, 105, lane, pd);
+                    warp_fetch<ST, 7>(Sb + (size_t)k * ks, SS, lane, pl);
+                }
+                if (k < n - 1) {
+                    double w[7], d[NS];
+                    pk_times<false>(Up, Lw, cq, hh, w);
+                    lw_times<true>(Lw, hh, w, d);
+                    sub_lower(Uc, d);
+                    __syncwarp();
+                }
+                warp_spd_inverse_packed(Uc, lane);
+                store_inv(Uc, k);
+            }
+        }
+    } else {
+        const int t2 = tid - 64;
+        for (int e = t2; e < nv; e += 64) xv[e] = (double)lb[e];
+        asm volatile("bar.sync 1, 64;" ::: "memory");
+        double g2 = 0.0;
+        for (int e = t2; e < nv; e += 64) {
+            const double gv = gam(e);
+            wsv(PW_RES, e) = gv - srow(e, xv);
+            wsv(PW_LAM, e) = xv[e];
+            g2 += gv * gv;
+        }
+        g2 = warp_sum(g2);
+        if (lane == 0) ginit[warp - 2] = g2;
+    }
+    __syncthreads();
+    // ---- middle knot: T_m = D_m - L_{m+1}^T U_{m+1}^{-1} L_{m+1}, inverted (warp 1)
+    if (warp == 1) {
+        double *Dm = fw0 + 105 * (m & 1);
+        if (m + 1 <= n - 1) {
+            double *Lw = fw1 + 210, *Up = fw1 + 105 * ((m + 1) & 1);
+            double pl[7];
+            warp_fetch<ST, 7>(Sb + (size_t)(m + 1) * ks, SS, lane, pl);
+#pragma unroll
+            for (int i = 0; i < 7; ++i) {
+                const int e = lane + 32 * i;
+                if (e < SS) Lw[e] = pl[i];
+            }
+            __syncwarp();
+            double w[7], d[NS];
+            pk_times<false>(Up, Lw, cq, hh, w);
+            lw_times<true>(Lw, hh, w, d);
+            sub_lower(Dm, d);
+            __syncwarp();
+        }
+        warp_spd_inverse_packed(Dm, lane);
+        store_inv(Dm, m);
+    }
+    const double gg = ginit[0] + ginit[1];
+    __syncthreads();
+
+    // ---- M x = y in place on xv (warps 0, 1; every thread takes the barriers)
+    const int r = c;  // sweep lanes: (row r, half hh)
+    const bool rv = cval;
+    auto ld_inv = [&](int k, double (&v)[7]) {
+#pragma unroll
+        for (int q = 0; q < 7; ++q) v[q] = rv ? wsb[(size_t)k * PW_STRIDE + PW_INV + tri_lo(r, 7 * hh + q)] : 0.0;
+    };
+    // row r (TR: column r) of L_k, columns (rows) 7 hh .. 7 hh + 6
+    auto ld_left = [&](int k, bool tr, double (&v)[7]) {
+        const ST *p = Sb + (size_t)k * ks;
+#pragma unroll
+        for (int q = 0; q < 7; ++q) v[q] = rv ? (double)__ldg(p + (tr ? 7 * hh + q + NS * r : r + NS * (7 * hh + q))) : 0.0;
+    };
+    auto solve = [&]() {
+        if (warp == 0 && m > 0) {
+            double di[7], li[7];
+            ld_inv(0, di);
+            ld_left(1, false, li);
+            for (int k = 0; k < m; ++k) {
+                double dc[7], lc[7];
+#pragma unroll
+                for (int q = 0; q < 7; ++q) {
+                    dc[q] = di[q];
+                    lc[q] = li[q];
+                }
+                if (k + 1 < m) {
+                    ld_inv(k + 1, di);
+                    ld_left(k + 2, false, li);
+                }
+                const double a = pair_dot7(dc, xv + NS * k, hh);
+                if (hh == 0 && rv) tv[NS * k + r] = a;
+                __syncwarp();
+                const double u = pair_dot7(lc, tv + NS * k, hh);
+                if (hh == 0 && rv) xv[NS * (k + 1) + r] += u;
+                __syncwarp();
+            }
+        } else if (warp == 1) {
+            if (n - 1 > m) {
+                double di[7], li[7];
+                ld_inv(n - 1, di);
+                ld_left(n - 1, true, li);
+                for (int k = n - 1; k > m; --k) {
+                    double dc[7], lc[7];
+#pragma unroll
+                    for (int q = 0; q < 7; ++q) {
+                        dc[q] = di[q];
+                        lc[q] = li[q];
+                    }
+                    if (k - 1 > m) {
+                        ld_inv(k - 1, di);
+                        ld_left(k - 1, true, li);
+                    }
+                    const double a = pair_dot7(dc, xv + NS * k, hh);
+                    if (hh == 0 && rv) tv[NS * k + r] = a;
+                    __syncwarp();
+                    const double u = pair_dot7(lc, tv + NS * k, hh);
+                    if (hh == 0 && rv) {
+                        if (k - 1 > m) xv[NS * (k - 1) + r] += u;
+                        else ubot[r] = u;
+                    }
+                    __syncwarp();
+                }
+            } else if (lane < NS) {
+                ubot[lane] = 0.0;
+            }
+        }
+        __syncthreads();
+        if (warp == 0) {
+            double *sc = fw0 + 210;
+            double di[7];
+            ld_inv(m, di);
+            if (lane < NS) sc[lane] = xv[NS * m + lane] + ubot[lane];
+            __syncwarp();
+            const double a = pair_dot7(di, sc, hh);
+            if (hh == 0 && rv) xv[NS * m + r] = a;
+        }
+        __syncthreads();
+        if (warp == 0 && m > 0) {
+            double *sc = fw0 + 210;
+            double di[7], li[7];
+            ld_inv(m - 1, di);
+            ld_left(m, true, li);
+            for (int k = m - 1; k >= 0; --k) {
+                double dc[7], lc[7];
+#pragma unroll
+                for (int q = 0; q < 7; ++q) {
+                    dc[q] = di[q];
+                    lc[q] = li[q];
+                }
+                if (k > 0) {
+                    ld_inv(k - 1, di);
+                    ld_left(k, true, li);
+                }
+                const double s = pair_dot7(lc, xv + NS * (k + 1), hh);
+                if (hh == 0 && rv) sc[r] = s;
+                __syncwarp();
+                const double a = pair_dot7(dc, sc, hh);
+                if (hh == 0 && rv) xv[NS * k + r] = tv[NS * k + r] + a;
+                __syncwarp();
+            }
+        } else if (warp == 1 && n - 1 > m) {
+            double *sc = fw1 + 210;
+            double di[7], li[7];
+            ld_inv(m + 1, di);
+            ld_left(m + 1, false, li);
+            for (int k = m + 1; k < n; ++k) {
+                double dc[7], lc[7];
+#pragma unroll
+                for (int q = 0; q < 7; ++q) {
+                    dc[q] = di[q];
+                    lc[q] = li[q];
+                }
+                if (k + 1 < n) {
+                    ld_inv(k + 1, di);
+                    ld_left(k + 1, false, li);
+                }
+                const double s = pair_dot7(lc, xv + NS * (k - 1), hh);
+                if (hh == 0 && rv) sc[r] = s;
+                __syncwarp();
+                const double a = pair_dot7(dc, sc, hh);
+                if (hh == 0 && rv) xv[NS * k + r] = tv[NS * k + r] + a;
+                __syncwarp();
+            }
+        }
+        __syncthreads();
+    };
+
+    // ---- CG on the instance (the iteration of pcg_chain_kernel with one CTA)
+    int set = 0;
+    auto block_sum = [&](double *v, int cnt) {
+        for (int q = 0; q < cnt; ++q) {
+            const double s = warp_sum(v[q]);
+            if (lane == 0) red[set * PAIR_NWARP * 3 + warp * 3 + q] = s;
+        }
+        __syncthreads();
+        for (int q = 0; q < cnt; ++q) {
+            const double *rs = red + set * PAIR_NWARP * 3 + q;
+            v[q] = ((rs[0] + rs[3]) + rs[6]) + rs[9];
+        }
+        set ^= 1;
+    };
+    auto true_residual = [&]() {
+        __syncthreads();
+        for (int e = tid; e < nv; e += PAIR_THREADS) xv[e] = wsv(PW_LAM, e);
+        __syncthreads();
+        for (int e = tid; e < nv; e += PAIR_THREADS) wsv(PW_RES, e) = gam(e) - srow(e, xv);
+    };
+    // z = S^{-1} r = -x of M x = r (left in xv); d[1] += r.z, d[2] += r.r
+    auto precond = [&](double *d) {
+        __syncthreads();
+        for (int e = tid; e < nv; e += PAIR_THREADS) xv[e] = wsv(PW_RES, e);
+        __syncthreads();
+        solve();
+        for (int e = tid; e < nv; e += PAIR_THREADS) {
+            const double rr = wsv(PW_RES, e), z = -xv[e];
+            d[1] += rr * z;
+            d[2] += rr * rr;
+        }
+    };
+    auto sum_res2 = [&]() {
+        double d0[1] = {0.0};
+        for (int e = tid; e < nv; e += PAIR_THREADS) {
+            const double rr = wsv(PW_RES, e);
+            d0[0] += rr * rr;
+        }
+        block_sum(d0, 1);
+        return d0[0];
+    };
+    auto converged = [&](double e, double r2) {
+        return exit_mode == 0 ? (r2 <= (double)tol * (double)tol * gg) : (fabs(e) < (double)tol);
+    };
+
+    double eta;
+    bool conv, bad = false;
+    {
+        double acc3[3] = {0.0, 0.0, 0.0};
+        precond(acc3);
+        block_sum(acc3, 3);
+        eta = acc3[1];
+        for (int e = tid; e < nv; e += PAIR_THREADS) wsv(PW_P, e) = -xv[e];  // p = z
+        conv = converged(eta, acc3[2]);
+    }
+    int it = 0;
+    while (!conv && it < max_iter) {
+        __syncthreads();
+        for (int e = tid; e < nv; e += PAIR_THREADS) xv[e] = wsv(PW_P, e);
+        __syncthreads();
+        double d1[1] = {0.0};
+        for (int e = tid; e < nv; e += PAIR_THREADS) {
+            const double v = srow(e, xv);
+            wsv(PW_V, e) = v;
+            d1[0] += xv[e] * v;
+        }
+        block_sum(d1, 1);
+        const double alpha = eta / d1[0];
+        if (!isfinite(alpha)) {
+            bad = true;
+            break;
+        }
+        for (int e = tid; e < nv; e += PAIR_THREADS) {
+            wsv(PW_LAM, e) = fma(alpha, xv[e], wsv(PW_LAM, e));
+            wsv(PW_RES, e) = fma(-alpha, wsv(PW_V, e), wsv(PW_RES, e));
+        }
+        ++it;
+        bool replaced = false;
+        if (it % RR_PERIOD == 0) {
+            true_residual();
+            replaced = true;
+        }
+        if (exit_mode == 0) {
+            // ||r|| <= tol ||gamma||: tested before preconditioning and confirmed on the true residual
+            double r2 = sum_res2();
+            if (!isfinite(r2)) {
+                bad = true;
+                break;
+            }
+            if (converged(0.0, r2) && !replaced) {
+                true_residual();
+                r2 = sum_res2();
+            }
+            if (converged(0.0, r2)) {
+                conv = true;
+                break;
+            }
+        }
+        double d2[3] = {0.0, 0.0, 0.0};
+        precond(d2);
+        block_sum(d2, 3);
+        if (exit_mode != 0) conv = converged(d2[1], d2[2]);
+        if (!isfinite(d2[1])) {
+            bad = true;
+            conv = false;
+            break;
+        }
+        if (conv) break;
+        const double beta = d2[1] / eta;
+        eta = d2[1];
+        for (int e = tid; e < nv; e += PAIR_THREADS) wsv(PW_P, e) = fma(beta, wsv(PW_P, e), -xv[e]);
+    }
+    for (int e = tid; e < nv; e += PAIR_THREADS) {
+        const double lam = wsv(PW_LAM, e);
+        lb[e] = (float)lam;
+        if (lambda64) lambda64[NS * kg0 + e] = lam;
+    }
+    if (tid == 0) {
+        const uint32_t maxit = conv ? 0u : 1u;
+        if (out_iters) {
+            out_iters[2 * b] = (uint32_t)it;
+            out_iters[2 * b + 1] = maxit | (bad ? 2u : 0u);
+        }
+        if (bv.st) {
+            InstState &s = bv.st[b];
+            s.last_pcg_iters = it;
+            s.last_pcg_exit = maxit;
+            s.pcg_iters_total += it;
+            s.pcg_maxiter_count += maxit;
+            if (bad) s.exit_flags |= 4u;
+            if (pcg_log && s.sqp_iters < (uint32_t)log_stride)
+                pcg_log[(size_t)b * log_stride + s.sqp_iters] = (uint32_t)it | (maxit << 31);
+        }
+    }
+}
+
+// FP64 packed rows (PK64: left block, diagonal lower triangle, pad) and FP64 gamma from the
+// reference's FP32 3-block rows, for pcg_pair_kernel on a caller's S (gpt_pcg)
+__global__ void pack_rows64_kernel(int N, const float *__restrict__ S, const float *__restrict__ gamma,
+                                   double *__restrict__ S64, double *__restrict__ gamma64)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N * PK64; i += gridDim.x * blockDim.x) {
+        const int k = i / PK64, t = i - k * PK64;
+        double v = 0.0;
+        if (t < SS) {
+            v = (double)S[(size_t)S_STRIDE * k + t];
+        } else if (t < SS + 105) {
+            const int q = t - SS;
+            int rr = 0;
+            while (((rr + 1) * (rr + 2)) / 2 <= q) ++rr;
+            const int cc = q - (rr * (rr + 1)) / 2;
+            v = (double)S[(size_t)S_STRIDE * k + SS + rr + NS * cc];
+        }
+        S64[i] = v;
+        if (t < NS) gamma64[NS * k + t] = (double)gamma[NS * k + t];
+    }
+}
+
+cudaError_t launch_pack_rows64(int N, const float *S, const float *gamma, double *S64, double *gamma64, int num_sms,
+                               cudaStream_t s)
+{
+    int blocks = (N * PK64 + 255) / 256;
+    if (blocks > 4 * num_sms) blocks = 4 * num_sms;
+    pack_rows64_kernel<<<blocks, 256, 0, s>>>(N, S, gamma, S64, gamma64);
+    return cudaGetLastError();
+}
+
+template <int FMT>
+static cudaError_t launch_pcg_pair_t(const BatchView &bv, int max_n, const void *S, const float *gamma,
+                                     const double *gamma64, float *lambda, double *lambda64, double *ws, int max_iter,
+                                     float tol, int exit_mode, uint32_t *out_iters, uint32_t *pcg_log, int log_stride,
+                                     cudaStream_t s)
+{
+    auto kern = pcg_pair_kernel<FMT>;
+    const size_t smem = pcg_pair_smem_bytes(max_n);
+    static size_t attr_smem = 0;
+    if (smem > attr_smem) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        attr_smem = smem;
+    }
+    kern<<<bv.B, PAIR_THREADS, smem, s>>>(bv, S, gamma, gamma64, lambda, lambda64, ws, max_iter, tol, exit_mode,
+                                          out_iters, pcg_log, log_stride);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
 
 int pcg_pick_cluster(int maxN, int B, int num_sms, int requested)
 {
@@ -1147,6 +1732,13 @@ cudaError_t launch_pcg(const BatchView &bv, int max_n_knots, int min_n_knots, in
     if (precond == 1 && !cr_ws) return cudaErrorInvalidValue;
     if (fmt == 2 && (precond != 1 || !gamma64)) return cudaErrorInvalidValue;  // FP64 rows: chain preconditioner only
     if (max_n_knots > MAX_PCG_KNOTS) return cudaErrorInvalidValue;
+    if (cluster_size == PCG_WARP_PAIR) {
+        if (precond != 1 || fmt == 0) return cudaErrorInvalidValue;  // packed rows, exact preconditioner
+        return fmt == 2 ? launch_pcg_pair_t<2>(bv, max_n_knots, S, gamma, gamma64, lambda, lambda64, cr_ws, max_iter,
+                                               tol, exit_mode, out_iters, pcg_log, log_stride, s)
+                        : launch_pcg_pair_t<1>(bv, max_n_knots, S, gamma, gamma64, lambda, lambda64, cr_ws, max_iter,
+                                               tol, exit_mode, out_iters, pcg_log, log_stride, s);
+    }
     int cs = (precond == 1 && cluster_size == 0) ? 1 : pcg_pick_cluster(max_n_knots, bv.B, num_sms, cluster_size);
     while ((max_n_knots + cs - 1) / cs > PCG_KPC_MAX) cs *= 2;
     while (cs > 1 && cs > min_n_knots) cs /= 2;  // every CTA owns at least one knot

@@ -80,7 +80,9 @@ typedef struct gpt_solver_config {
     float rho_factor;          /* RHO_FACTOR */
     float rho_max;             /* RHO_MAX */
     float rho_min;             /* RHO_MIN */
-    uint32_t pcg_cluster_size; /* CTAs per instance in the PCG (1,2,4,8,16); 0 = chosen by the library */
+    uint32_t pcg_cluster_size; /* CTAs per instance in the PCG (1,2,4,8,16); GPT_PCG_WARP_PAIR: one 128-thread
+                                  CTA per instance, factorisation by two warps (pcg_precond 1 only); 0 = chosen
+                                  by the library (gpt_autotune's choice for the batch shape, else 1 ... 16) */
     uint32_t pcg_precond;      /* 0: block-Jacobi Pinv (the reference's, oldschur.cuh:926-933);
                                   1 (default): exact block-tridiagonal LDL^T of each CTA's chunk of knots */
     uint32_t schur_fp64;       /* SQP loop and adjoint with pcg_precond 1: 1 (default) forms and stores the
@@ -103,6 +105,11 @@ typedef struct gpt_sqp_stats {
     float merit_final;
     float rho_final;
 } gpt_sqp_stats;
+
+/* pcg_cluster_size value: the PCG of one instance in one 128-thread CTA whose first two warps factor S
+ * from both ends of the horizon at once (twisted block LDL^T), so that all instances of a large batch run
+ * concurrently; same iteration and preconditioner (exact inverse of S) as pcg_cluster_size 1. */
+#define GPT_PCG_WARP_PAIR 32u
 
 /* Default configs: the reference's logged experiment settings (dt 1/64, Euler,
  * QD = R = 1e-4, RHO_FACTOR 1.2, RHO_MAX 10, RHO_MIN 1e-3, SQP_MAX_ITER 40). */
@@ -149,7 +156,7 @@ gpt_status gpt_sqp_solve_batched(gpt_handle *h, uint32_t batch, const uint32_t *
  * (on copies of d_xu, d_lambda; the inputs are not modified) for each candidate
  * PCG cluster size -- the smallest that holds the longest horizon in
  * <= 128 knots per CTA, and twice and four times it, up to 16 and to the
- * shortest horizon -- and remembers the fastest for this batch shape
+ * shortest horizon, and GPT_PCG_WARP_PAIR with pcg_precond 1 -- and remembers the fastest for this batch shape
  * (instances, total knots, longest and shortest horizon).  Later solves of
  * that shape use it while pcg_cluster_size is 0.  h_cluster_out (optional)
  * receives the choice. */
@@ -204,7 +211,9 @@ gpt_status gpt_prep_csr(uint32_t knot_points, int32_t *h_col_ptr, int32_t *h_row
 /* GPU-PCG pcg<T,STATE_SIZE,KNOT_POINTS> launch (toplevel.cuh:135-157,292-294):
  * solves S lambda = gamma from the warm start in d_lambda (updated in place,
  * FP32).  d_lambda64 (optional, 14N doubles) receives the FP64 iterate; at
- * N >= ~64 only it can carry a relative residual near 1e-5. */
+ * N >= ~64 only it can carry a relative residual near 1e-5.  With
+ * pcg_cluster_size GPT_PCG_WARP_PAIR, S and gamma are first converted (exactly)
+ * to FP64 packed rows in the handle's workspace. */
 gpt_status gpt_pcg(gpt_handle *h, uint32_t knot_points, const float *d_S, const float *d_Pinv,
                    const float *d_gamma, float *d_lambda, double *d_lambda64, uint32_t max_iter, float exit_tol,
                    uint32_t exit_mode, uint32_t *h_iters, uint8_t *h_maxiter_exit, gpt_stream_t stream);

@@ -137,15 +137,19 @@ def schur_residual(S, lam, gam, N):
 
 
 @pytest.mark.parametrize("precond", [0, 1])
-@pytest.mark.parametrize("cluster", [0, 1, 2, 4, 8, 16])
+@pytest.mark.parametrize("cluster", [0, 1, 2, 4, 8, 16, 32])
 def test_pcg_reaches_tolerance(gpt, oracle, golden, problem_mod, solvers, cluster, precond):
     """Exit mode 0 stops on the TRUE relative residual (FP64-evaluated); the
     returned lambda satisfies ||gamma - S lambda|| <= tol ||gamma|| for every
-    cluster size (CTAs per instance) and both preconditioners (0: the
+    cluster size (CTAs per instance; 32 = the warp-pair kernel, one CTA per
+    instance with a twisted factorisation) and both preconditioners (0: the
     reference's block-Jacobi, 1: exact block-tridiagonal LDL^T per chunk); a
     warm start at the solution needs at most a few iterations."""
+    pair = cluster == gpt.PCG_WARP_PAIR
+    if pair and precond == 0:
+        pytest.skip("the warp-pair kernel has the exact preconditioner only")
     for kind, N, cfg, p in problems(golden, problem_mod):
-        if cluster > N:
+        if cluster > N and not pair:
             continue
         sv = solvers(cfg)
         sv.set_solver(pcg_cluster_size=cluster, pcg_precond=precond)
@@ -174,7 +178,7 @@ def test_pcg_reaches_tolerance(gpt, oracle, golden, problem_mod, solvers, cluste
             # the start perturbs the residual by ~eps32 cond(S), so a warm start is no better than
             # a cold one
             assert not maxed2 and it2 <= it, (kind, N, cluster, it2, it)
-        if precond == 1 and cluster in (0, 1):
+        if precond == 1 and (cluster in (0, 1) or pair):
             # one chunk = the whole horizon: the preconditioner is the inverse up to rounding
             assert it <= 4, (kind, N, it)
         # eta-based exit (|r^T Pinv r| < tol) runs and stops
@@ -195,7 +199,7 @@ def test_pcg_cluster_sizes_agree(gpt, oracle, problem_mod, solvers):
     S, Pv, gam = (x.astype(np.float32) for x in (S, Pv, gam))
     lam_star = oracle.banded_cholesky(N, S, gam)
     sols = {}
-    for cs in (1, 2, 4, 8, 16):
+    for cs in (1, 2, 4, 8, 16, gpt.PCG_WARP_PAIR):
         sv.set_solver(pcg_cluster_size=cs)
         lam = torch.zeros(14 * N, device="cuda")
         lam64 = torch.zeros(14 * N, device="cuda", dtype=torch.float64)
@@ -204,6 +208,9 @@ def test_pcg_cluster_sizes_agree(gpt, oracle, problem_mod, solvers):
         sols[cs] = lam64.cpu().numpy()
     sv.set_solver(pcg_cluster_size=0)
     ref = np.linalg.norm(lam_star)
+    # one CTA per instance (cyclic reduction) and the warp pair (twisted factorisation) both apply
+    # the exact inverse: their solutions differ by rounding only
+    assert np.linalg.norm(sols[1] - sols[gpt.PCG_WARP_PAIR]) <= 1e-7 * ref
     errs = {cs: np.linalg.norm(v - lam_star) / ref for cs, v in sols.items()}
     # every split lands within the accuracy the 1e-5 residual allows of the FP64 Cholesky
     # solution (one CTA per instance solves exactly; the chunked splits stop at the tolerance)
@@ -443,6 +450,47 @@ def test_sqp_solve_chain_preconditioner_matches_block_jacobi(gpt, problem_mod):
     assert sum(r1.pcg_iters) * 20 < sum(r0.pcg_iters), (r1.pcg_iters, r0.pcg_iters)
 
 
+@pytest.mark.parametrize("schur_fp64", [1, 0])
+@pytest.mark.parametrize("exit_mode", [0, 1])
+def test_sqp_warp_pair_pcg_matches_chain(gpt, problem_mod, schur_fp64, exit_mode):
+    """The warp-pair PCG (one CTA per instance, twisted factorisation) and the
+    one-CTA chain PCG (cyclic reduction) apply the same exact preconditioner to
+    the same S.  On a batch of uneven horizons (2 and 3 knots included: no top
+    sweep, one knot each side): one SQP iteration from the same iterate gives
+    the same step to 1e-6 (the two factorisation orders differ by FP64
+    rounding only); four iterations take the same SQP decisions with 1-2 PCG
+    iterations per linear system and end within 1e-3 of the step (an FP32
+    rounding difference of an iterate is amplified by cond(S) ~ 1e7 in the
+    next linear system)."""
+    Ns = [2, 3, 17, 64, 128, 5]
+    ps = [problem_mod.make_problem(n, 60 + i, dt=0.01) for i, n in enumerate(Ns)]
+    cat = lambda key, pad: np.concatenate([np.concatenate([p[key], np.zeros(pad, np.float32)]) for p in ps])
+    goal, xu0, lam0 = dev(cat("goal", 0)), dev(cat("xu", 7)), dev(cat("lam", 0))
+    x0 = host(xu0)
+    for iters, tol in ((1, 1e-6), (4, 1e-3)):
+        out = {}
+        for cs in (1, gpt.PCG_WARP_PAIR):
+            sv = gpt.Solver(max_knot_points=128, max_batch=len(Ns), **SPEC_CFG)
+            sv.set_solver(sqp_max_iter=iters, pcg_max_iter=1000, pcg_exit_tol=1e-9 if exit_mode == 0 else 1e-14,
+                          pcg_exit_mode=exit_mode, pcg_cluster_size=cs, schur_fp64=schur_fp64)
+            xu, lam = xu0.clone(), lam0.clone()
+            rho, stats = sv.sqp_solve_batched(Ns, goal, lam, xu, [1e-3] * len(Ns))
+            out[cs] = (host(xu), rho, stats)
+            sv.close()
+        (x1, r1, s1), (x2, r2, s2) = out[1], out[gpt.PCG_WARP_PAIR]
+        assert [s["sqp_iters"] for s in s1] == [s["sqp_iters"] for s in s2]
+        assert r1 == r2
+        off = 0
+        for b, n in enumerate(Ns):
+            sl = slice(21 * off, 21 * off + 21 * n - 7)
+            step = np.linalg.norm(x1[sl] - x0[sl])
+            diff = np.linalg.norm(x2[sl] - x1[sl])
+            assert diff <= tol * step + 1e-6, (iters, n, diff, step)
+            assert s2[b]["pcg_maxiter_count"] == 0
+            assert s2[b]["pcg_iters_total"] <= 2 * s2[b]["sqp_iters"], (n, s2[b])
+            off += n
+
+
 def test_sqp_graph_equals_host_loop(gpt, problem_mod):
     """The solve as one CUDA graph (device-side while loop, the default) and the
     host-driven loop give bit-identical results, on the first call of a batch shape
@@ -482,7 +530,7 @@ def test_autotune_choice_is_used(gpt, problem_mod):
     x_in, l_in = xu0.clone(), lam0.clone()
     cs = sv.autotune([N], goal, l_in, x_in, [1e-3])
     assert torch.equal(x_in, xu0) and torch.equal(l_in, lam0)
-    assert cs in (1, 2, 4)
+    assert cs in (1, 2, 4, gpt.PCG_WARP_PAIR)
     out = []
     for given in (0, cs):
         sv.set_solver(pcg_cluster_size=given)
