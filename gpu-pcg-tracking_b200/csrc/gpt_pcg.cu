@@ -1087,28 +1087,68 @@ __global__ void __launch_bounds__(PCG_THREADS, 1)
 constexpr int PAIR_THREADS = 128;
 constexpr int PAIR_NWARP = PAIR_THREADS / 32;
 constexpr int PW_STRIDE = SS, PW_INV = 0, PW_LAM = 105, PW_RES = 119, PW_P = 133, PW_V = 147;
-constexpr int PAIR_FWARP = 2 * 105 + SS;  // per factoring warp: two factor buffers and one coupling
+// per factoring warp: the previous inverse factor as a full symmetric matrix (196), the coupling
+// block (196) and the diagonal block A_k (packed lower triangle, 105)
+constexpr int PAIR_FWARP = 2 * SS + 105;
+constexpr int PF_INV = 0, PF_L = SS, PF_A = 2 * SS;
 
 __host__ __device__ constexpr int pair_smem_doubles(int n)
 {
-    return 2 * NS * n + 2 * PAIR_FWARP + NS + 2 * PAIR_NWARP * 3 + 2;
+    return 2 * NS * n + 2 * PAIR_FWARP + SS + NS + 2 * PAIR_NWARP * 3 + 2;
 }
 size_t pcg_pair_smem_bytes(int n) { return sizeof(double) * (size_t)pair_smem_doubles(n); }
 
-// w[q] = (Ai X)(7 hh + q, c) with X(t, c) = Lw[t + 14 c] (TR: X = Lw^T); Ai packed lower triangle
+// w[q] = (Ai X)(7 hh + q, c) with X(t, c) = Lw[t + 14 c] (TR: X = Lw^T); Ai a full symmetric
+// 14x14 matrix, column-major, so every shared-memory offset below is a constant from Ai + 7 hh
 template <bool TR>
-__device__ __forceinline__ void pk_times(const double *Ai, const double *Lw, int cq, int hh, double (&w)[7])
+__device__ __forceinline__ void full_times(const double *Ai, const double *Lw, int cq, int hh, double (&w)[7])
 {
     double xc[NS];
 #pragma unroll
     for (int t = 0; t < NS; ++t) xc[t] = TR ? Lw[cq + NS * t] : Lw[t + NS * cq];
+    const double *Ar = Ai + 7 * hh;
 #pragma unroll
     for (int q = 0; q < 7; ++q) {
-        const int rr = 7 * hh + q;
         double a = 0.0;
 #pragma unroll
-        for (int t = 0; t < NS; ++t) a = fma(Ai[tri_lo(rr, t)], xc[t], a);
+        for (int t = 0; t < NS; ++t) a = fma(Ar[q + NS * t], xc[t], a);
         w[q] = a;
+    }
+}
+// Reciprocal by two Newton-Raphson steps r <- r + r (1 - x r) from the PTX approximation
+// rcp.approx.ftz.f64 (quadratic convergence: a seed accurate to ~2^-20 reaches FP64 rounding);
+// x is a positive pivot of an SPD factorisation, far from the FP64 range limits
+__device__ __forceinline__ double rcp_newton(double x)
+{
+    double r;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
+    double e = fma(-x, r, 1.0);
+    r = fma(r, e, r);
+    e = fma(-x, r, 1.0);
+    return fma(r, e, r);
+}
+// In-place Gauss-Jordan inverse of an SPD 14x14 matrix (no pivoting: every pivot is a Schur
+// complement of an SPD matrix) held by lane pairs: lane (c, hh) = (lane >> 1, lane & 1), c < 14,
+// holds rows 7 hh .. 7 hh + 6 of column c in a[]; on return the same entries of the inverse.  At
+// pivot p the lane needs the pivot column's entries of its rows (from lane (p, hh)), the pivot
+// row's entry of its column and the pivot (from lanes (c, p / 7) and (p, p / 7)); column p itself
+// is treated as the identity's column e_p, which the elimination turns into column p of the inverse.
+__device__ __forceinline__ void pair_gj_inverse(double (&a)[7], int c, int hh)
+{
+    const int cs = c < NS ? c : NS - 1;
+#pragma unroll
+    for (int p = 0; p < NS; ++p) {
+        const int hp = p / 7, qp = p - 7 * hp;
+        const double piv = __shfl_sync(0xffffffffu, a[qp], 2 * p + hp);
+        const double apc = __shfl_sync(0xffffffffu, a[qp], 2 * cs + hp);
+        double aip[7];
+#pragma unroll
+        for (int q = 0; q < 7; ++q) aip[q] = __shfl_sync(0xffffffffu, a[q], 2 * p + hh);
+        const double rc = rcp_newton(piv);
+        const bool pc = (c == p);
+        const double f = (pc ? 1.0 : apc) * rc;
+#pragma unroll
+        for (int q = 0; q < 7; ++q) a[q] = (7 * hh + q == p) ? f : fma(-aip[q], f, pc ? 0.0 : a[q]);
     }
 }
 // d[a] = (Y W)(a, c) with Y(a, t) = Lw[a + 14 t] (TR: Lw[t + 14 a]); both lanes of a pair get the sum
@@ -1164,9 +1204,10 @@ __global__ void __launch_bounds__(PAIR_THREADS, 4)
     extern __shared__ double pair_dyn_smem[];
     double *xv = pair_dyn_smem;        // 14 n: the solve's vector (y, then x); lambda_0 during set-up
     double *tv = xv + nv;              // 14 n: t_k of the solve
-    double *fw0 = tv + nv;             // warp 0: D buffers (2 x 105), coupling / scratch (196)
-    double *fw1 = fw0 + PAIR_FWARP;    // warp 1: U buffers, coupling / scratch
-    double *ubot = fw1 + PAIR_FWARP;   // 14: L_{m+1}^T t_{m+1} from the bottom sweep
+    double *fw0 = tv + nv;             // warp 0: D_{k-1}^{-1} (full), coupling / scratch, A_k
+    double *fw1 = fw0 + PAIR_FWARP;    // warp 1: U_{k+1}^{-1} (full), coupling / scratch, A_k
+    double *dmf = fw1 + PAIR_FWARP;    // D_m (full), from warp 0 to the middle step
+    double *ubot = dmf + SS;           // 14: L_{m+1}^T t_{m+1} from the bottom sweep
     double *red = ubot + NS;           // 2 sets x 4 warps x 3
     double *ginit = red + 2 * PAIR_NWARP * 3;  // gamma . gamma partials of warps 2, 3
 
@@ -1208,62 +1249,70 @@ __global__ void __launch_bounds__(PAIR_THREADS, 4)
     const int c = lane >> 1, hh = lane & 1;
     const bool cval = c < NS;
     const int cq = cval ? c : NS - 1;
-    // D -= d (lower triangle of column c, rows of the lane's parity)
-    auto sub_lower = [&](double *D, const double (&d)[NS]) {
+    // lane (c, hh)'s entries of a diagonal block minus the Schur update d (column c, all rows)
+    auto load_block = [&](const double *Apk, const double (&d)[NS], double (&a)[7]) {
+#pragma unroll
+        for (int q = 0; q < 7; ++q) a[q] = Apk[tri_lo(7 * hh + q, cq)] - (hh ? d[7 + q] : d[q]);
+    };
+    // an inverse factor: full matrix into shared memory (next step's products), packed lower
+    // triangle into the workspace (the solve)
+    auto keep_inv = [&](double *F, const double (&a)[7], int k) {
+        __syncwarp();
         if (cval) {
 #pragma unroll
-            for (int a = 0; a < NS; ++a)
-                if (a >= c && (a & 1) == hh) D[((a * (a + 1)) >> 1) + c] -= d[a];
+            for (int q = 0; q < 7; ++q) {
+                const int i = 7 * hh + q;
+                if (F) F[i + NS * c] = a[q];
+                if (i >= c) wsb[(size_t)k * PW_STRIDE + PW_INV + ((i * (i + 1)) >> 1) + c] = a[q];
+            }
         }
-    };
-    auto store_inv = [&](const double *Di, int k) {
-#pragma unroll
-        for (int i = 0; i < 4; ++i) {
-            const int e = lane + 32 * i;
-            if (e < 105) wsb[(size_t)k * PW_STRIDE + PW_INV + e] = Di[e];
-        }
+        __syncwarp();
     };
 
     // ---- factorisation (warps 0, 1) and initial residual (warps 2, 3)
     if (warp == 0) {
-        double *Lw = fw0 + 210;
+        double *Fi = fw0 + PF_INV, *Lw = fw0 + PF_L, *Ap = fw0 + PF_A;
         double pre[10];  // row k: left block (196) then diagonal triangle (105)
         warp_fetch<ST, 10>(Sb, SS + 105, lane, pre);
         for (int k = 0; k <= m; ++k) {
-            double *Dc = fw0 + 105 * (k & 1), *Dp = fw0 + 105 * ((k + 1) & 1);
 #pragma unroll
             for (int i = 0; i < 10; ++i) {
                 const int e = lane + 32 * i;
                 if (e < SS) Lw[e] = pre[i];
-                else if (e < SS + 105) Dc[e - SS] = -pre[i];
+                else if (e < SS + 105) Ap[e - SS] = -pre[i];
             }
             __syncwarp();
             if (k < m) warp_fetch<ST, 10>(Sb + (size_t)(k + 1) * ks, SS + 105, lane, pre);
+            double d[NS];
+#pragma unroll
+            for (int a = 0; a < NS; ++a) d[a] = 0.0;
             if (k > 0) {
-                double w[7], d[NS];
-                pk_times<true>(Dp, Lw, cq, hh, w);
-                lw_times<false>(Lw, hh, w, d);
-                sub_lower(Dc, d);
-                __syncwarp();
+                double w[7];
+                full_times<true>(Fi, Lw, cq, hh, w);  // D_{k-1}^{-1} L_k^T
+                lw_times<false>(Lw, hh, w, d);        // L_k D_{k-1}^{-1} L_k^T
             }
+            double a[7];
+            load_block(Ap, d, a);
             if (k < m) {
-                warp_spd_inverse_packed(Dc, lane);
-                store_inv(Dc, k);
+                pair_gj_inverse(a, c, hh);
+                keep_inv(Fi, a, k);
+            } else if (cval) {
+#pragma unroll
+                for (int q = 0; q < 7; ++q) dmf[7 * hh + q + NS * c] = a[q];
             }
         }
     } else if (warp == 1) {
-        double *Lw = fw1 + 210;
+        double *Fi = fw1 + PF_INV, *Lw = fw1 + PF_L, *Ap = fw1 + PF_A;
         if (n - 1 > m) {
             double pd[4], pl[7];
 #pragma unroll
             for (int i = 0; i < 7; ++i) pl[i] = 0.0;
             warp_fetch<ST, 4>(Sb + (size_t)(n - 1) * ks + PK_DIAG, 105, lane, pd);
             for (int k = n - 1; k > m; --k) {
-                double *Uc = fw1 + 105 * (k & 1), *Up = fw1 + 105 * ((k + 1) & 1);
 #pragma unroll
                 for (int i = 0; i < 4; ++i) {
                     const int e = lane + 32 * i;
-                    if (e < 105) Uc[e] = -pd[i];
+                    if (e < 105) Ap[e] = -pd[i];
                 }
                 if (k < n - 1) {
 #pragma unroll
@@ -1277,15 +1326,18 @@ __global__ void __launch_bounds__(PAIR_THREADS, 4)
                     warp_fetch<ST, 4>(Sb + (size_t)(k - 1) * ks + PK_DIAG, 105, lane, pd);
                     warp_fetch<ST, 7>(Sb + (size_t)k * ks, SS, lane, pl);
                 }
+                double d[NS];
+#pragma unroll
+                for (int a = 0; a < NS; ++a) d[a] = 0.0;
                 if (k < n - 1) {
-                    double w[7], d[NS];
-                    pk_times<false>(Up, Lw, cq, hh, w);
-                    lw_times<true>(Lw, hh, w, d);
-                    sub_lower(Uc, d);
-                    __syncwarp();
+                    double w[7];
+                    full_times<false>(Fi, Lw, cq, hh, w);  // U_{k+1}^{-1} L_{k+1}
+                    lw_times<true>(Lw, hh, w, d);          // L_{k+1}^T U_{k+1}^{-1} L_{k+1}
                 }
-                warp_spd_inverse_packed(Uc, lane);
-                store_inv(Uc, k);
+                double a[7];
+                load_block(Ap, d, a);
+                pair_gj_inverse(a, c, hh);
+                keep_inv(Fi, a, k);
             }
         }
     } else {
@@ -1305,9 +1357,11 @@ __global__ void __launch_bounds__(PAIR_THREADS, 4)
     __syncthreads();
     // ---- middle knot: T_m = D_m - L_{m+1}^T U_{m+1}^{-1} L_{m+1}, inverted (warp 1)
     if (warp == 1) {
-        double *Dm = fw0 + 105 * (m & 1);
+        double d[NS];
+#pragma unroll
+        for (int a = 0; a < NS; ++a) d[a] = 0.0;
         if (m + 1 <= n - 1) {
-            double *Lw = fw1 + 210, *Up = fw1 + 105 * ((m + 1) & 1);
+            double *Fi = fw1 + PF_INV, *Lw = fw1 + PF_L;
             double pl[7];
             warp_fetch<ST, 7>(Sb + (size_t)(m + 1) * ks, SS, lane, pl);
 #pragma unroll
@@ -1316,14 +1370,15 @@ __global__ void __launch_bounds__(PAIR_THREADS, 4)
                 if (e < SS) Lw[e] = pl[i];
             }
             __syncwarp();
-            double w[7], d[NS];
-            pk_times<false>(Up, Lw, cq, hh, w);
+            double w[7];
+            full_times<false>(Fi, Lw, cq, hh, w);
             lw_times<true>(Lw, hh, w, d);
-            sub_lower(Dm, d);
-            __syncwarp();
         }
-        warp_spd_inverse_packed(Dm, lane);
-        store_inv(Dm, m);
+        double a[7];
+#pragma unroll
+        for (int q = 0; q < 7; ++q) a[q] = dmf[7 * hh + q + NS * cq] - (hh ? d[7 + q] : d[q]);
+        pair_gj_inverse(a, c, hh);
+        keep_inv(nullptr, a, m);
     }
     const double gg = ginit[0] + ginit[1];
     __syncthreads();
@@ -1396,7 +1451,7 @@ __global__ void __launch_bounds__(PAIR_THREADS, 4)
         }
         __syncthreads();
         if (warp == 0) {
-            double *sc = fw0 + 210;
+            double *sc = fw0 + PF_L;
             double di[7];
             ld_inv(m, di);
             if (lane < NS) sc[lane] = xv[NS * m + lane] + ubot[lane];
@@ -1406,7 +1461,7 @@ __global__ void __launch_bounds__(PAIR_THREADS, 4)
         }
         __syncthreads();
         if (warp == 0 && m > 0) {
-            double *sc = fw0 + 210;
+            double *sc = fw0 + PF_L;
             double di[7], li[7];
             ld_inv(m - 1, di);
             ld_left(m, true, li);
@@ -1429,7 +1484,7 @@ __global__ void __launch_bounds__(PAIR_THREADS, 4)
                 __syncwarp();
             }
         } else if (warp == 1 && n - 1 > m) {
-            double *sc = fw1 + 210;
+            double *sc = fw1 + PF_L;
             double di[7], li[7];
             ld_inv(m + 1, di);
             ld_left(m + 1, false, li);
