@@ -1127,28 +1127,42 @@ __device__ __forceinline__ double rcp_newton(double x)
     e = fma(-x, r, 1.0);
     return fma(r, e, r);
 }
-// In-place Gauss-Jordan inverse of an SPD 14x14 matrix (no pivoting: every pivot is a Schur
-// complement of an SPD matrix) held by lane pairs: lane (c, hh) = (lane >> 1, lane & 1), c < 14,
-// holds rows 7 hh .. 7 hh + 6 of column c in a[]; on return the same entries of the inverse.  At
-// pivot p the lane needs the pivot column's entries of its rows (from lane (p, hh)), the pivot
-// row's entry of its column and the pivot (from lanes (c, p / 7) and (p, p / 7)); column p itself
-// is treated as the identity's column e_p, which the elimination turns into column p of the inverse.
+// In-place Gauss-Jordan inverse of an SPD 14x14 matrix held by lane pairs: lane (c, hh) =
+// (lane >> 1, lane & 1), c < 14, holds rows 7 hh .. 7 hh + 6 of column c in a[]; on return the
+// same entries of the inverse.  The pivots are the 2x2 diagonal blocks P = {p, p+1} (no pivoting:
+// each is a diagonal block of a Schur complement of an SPD matrix, hence SPD), which halves the
+// chain of dependent reciprocals against scalar pivots.  Per block, with Pi = A_PP^{-1}:
+//   A_Pc <- Pi A_Pc,  A_ic <- A_ic - A_iP (Pi A_Pc)  (i, c outside P),  A_iP <- -A_iP Pi,  A_PP <- Pi,
+// done uniformly by treating the pivot columns as the identity's columns e_p, e_{p+1}.  The lane
+// needs the pivot block, rows p, p+1 of its column and columns p, p+1 of its rows (shuffles).
 __device__ __forceinline__ void pair_gj_inverse(double (&a)[7], int c, int hh)
 {
     const int cs = c < NS ? c : NS - 1;
 #pragma unroll
-    for (int p = 0; p < NS; ++p) {
-        const int hp = p / 7, qp = p - 7 * hp;
-        const double piv = __shfl_sync(0xffffffffu, a[qp], 2 * p + hp);
-        const double apc = __shfl_sync(0xffffffffu, a[qp], 2 * cs + hp);
-        double aip[7];
+    for (int p = 0; p < NS; p += 2) {
+        const int h0 = p / 7, q0 = p - 7 * h0, h1 = (p + 1) / 7, q1 = (p + 1) - 7 * h1;
+        const double x = __shfl_sync(0xffffffffu, a[q0], 2 * p + h0);        // A_pp
+        const double y = __shfl_sync(0xffffffffu, a[q1], 2 * p + h1);        // A_{p+1,p}
+        const double z = __shfl_sync(0xffffffffu, a[q1], 2 * (p + 1) + h1);  // A_{p+1,p+1}
+        const double v0 = __shfl_sync(0xffffffffu, a[q0], 2 * cs + h0);      // A_pc
+        const double v1 = __shfl_sync(0xffffffffu, a[q1], 2 * cs + h1);      // A_{p+1,c}
+        double u0[7], u1[7];                                                 // A_ip, A_i,p+1
 #pragma unroll
-        for (int q = 0; q < 7; ++q) aip[q] = __shfl_sync(0xffffffffu, a[q], 2 * p + hh);
-        const double rc = rcp_newton(piv);
-        const bool pc = (c == p);
-        const double f = (pc ? 1.0 : apc) * rc;
+        for (int q = 0; q < 7; ++q) {
+            u0[q] = __shfl_sync(0xffffffffu, a[q], 2 * p + hh);
+            u1[q] = __shfl_sync(0xffffffffu, a[q], 2 * (p + 1) + hh);
+        }
+        const double rd = rcp_newton(fma(x, z, -y * y));
+        const double i00 = z * rd, i01 = -y * rd, i11 = x * rd;
+        const bool c0 = (c == p), c1 = (c == p + 1), cp = c0 || c1;
+        const double w0 = cp ? (c0 ? 1.0 : 0.0) : v0, w1 = cp ? (c1 ? 1.0 : 0.0) : v1;
+        const double n0 = fma(i00, w0, i01 * w1), n1 = fma(i01, w0, i11 * w1);
 #pragma unroll
-        for (int q = 0; q < 7; ++q) a[q] = (7 * hh + q == p) ? f : fma(-aip[q], f, pc ? 0.0 : a[q]);
+        for (int q = 0; q < 7; ++q) {
+            const int i = 7 * hh + q;
+            const double upd = fma(-u0[q], n0, fma(-u1[q], n1, cp ? 0.0 : a[q]));
+            a[q] = (i == p) ? n0 : ((i == p + 1) ? n1 : upd);
+        }
     }
 }
 // d[a] = (Y W)(a, c) with Y(a, t) = Lw[a + 14 t] (TR: Lw[t + 14 a]); both lanes of a pair get the sum
@@ -1269,73 +1283,56 @@ __global__ void __launch_bounds__(PAIR_THREADS, 4)
         __syncwarp();
     };
 
-    // ---- factorisation (warps 0, 1) and initial residual (warps 2, 3)
-    if (warp == 0) {
-        double *Fi = fw0 + PF_INV, *Lw = fw0 + PF_L, *Ap = fw0 + PF_A;
-        double pre[10];  // row k: left block (196) then diagonal triangle (105)
-        warp_fetch<ST, 10>(Sb, SS + 105, lane, pre);
-        for (int k = 0; k <= m; ++k) {
+    // ---- factorisation (warps 0, 1) and initial residual (warps 2, 3).  Both factoring warps run
+    // one loop body (one copy in the instruction cache): warp 0 walks k = 0 .. m with the coupling
+    // L_k, warp 1 walks k = n-1 .. m+1 with L_{k+1} stored transposed, which turns its update
+    // L_{k+1}^T U_{k+1}^{-1} L_{k+1} into the same products as warp 0's L_k D_{k-1}^{-1} L_k^T.
+    if (warp < 2) {
+        const bool top = warp == 0;
+        double *fw = top ? fw0 : fw1;
+        double *Fi = fw + PF_INV, *Lw = fw + PF_L, *Ap = fw + PF_A;
+        const int steps = top ? m + 1 : n - 1 - m;
+        const int dir = top ? 1 : -1, k0 = top ? 0 : n - 1, lofs = top ? 0 : 1;
+        double pd[4], pl[7];  // diagonal triangle of row k, left block of row k + lofs
+        if (steps > 0) {
+            warp_fetch<ST, 4>(Sb + (size_t)k0 * ks + PK_DIAG, 105, lane, pd);
+            if (top) warp_fetch<ST, 7>(Sb, SS, lane, pl);
+        }
+        for (int st = 0; st < steps; ++st) {
+            const int k = k0 + dir * st;
 #pragma unroll
-            for (int i = 0; i < 10; ++i) {
+            for (int i = 0; i < 4; ++i) {
                 const int e = lane + 32 * i;
-                if (e < SS) Lw[e] = pre[i];
-                else if (e < SS + 105) Ap[e - SS] = -pre[i];
+                if (e < 105) Ap[e] = -pd[i];
+            }
+            if (st > 0) {
+#pragma unroll
+                for (int i = 0; i < 7; ++i) {
+                    const int e = lane + 32 * i;
+                    if (e < SS) Lw[top ? e : (e / NS) + NS * (e % NS)] = pl[i];
+                }
             }
             __syncwarp();
-            if (k < m) warp_fetch<ST, 10>(Sb + (size_t)(k + 1) * ks, SS + 105, lane, pre);
+            if (st + 1 < steps) {
+                warp_fetch<ST, 4>(Sb + (size_t)(k + dir) * ks + PK_DIAG, 105, lane, pd);
+                warp_fetch<ST, 7>(Sb + (size_t)(k + dir + lofs) * ks, SS, lane, pl);
+            }
             double d[NS];
 #pragma unroll
             for (int a = 0; a < NS; ++a) d[a] = 0.0;
-            if (k > 0) {
+            if (st > 0) {
                 double w[7];
-                full_times<true>(Fi, Lw, cq, hh, w);  // D_{k-1}^{-1} L_k^T
-                lw_times<false>(Lw, hh, w, d);        // L_k D_{k-1}^{-1} L_k^T
+                full_times<true>(Fi, Lw, cq, hh, w);
+                lw_times<false>(Lw, hh, w, d);
             }
             double a[7];
             load_block(Ap, d, a);
-            if (k < m) {
-                pair_gj_inverse(a, c, hh);
-                keep_inv(Fi, a, k);
-            } else if (cval) {
+            if (top && k == m) {
+                if (cval) {
 #pragma unroll
-                for (int q = 0; q < 7; ++q) dmf[7 * hh + q + NS * c] = a[q];
-            }
-        }
-    } else if (warp == 1) {
-        double *Fi = fw1 + PF_INV, *Lw = fw1 + PF_L, *Ap = fw1 + PF_A;
-        if (n - 1 > m) {
-            double pd[4], pl[7];
-#pragma unroll
-            for (int i = 0; i < 7; ++i) pl[i] = 0.0;
-            warp_fetch<ST, 4>(Sb + (size_t)(n - 1) * ks + PK_DIAG, 105, lane, pd);
-            for (int k = n - 1; k > m; --k) {
-#pragma unroll
-                for (int i = 0; i < 4; ++i) {
-                    const int e = lane + 32 * i;
-                    if (e < 105) Ap[e] = -pd[i];
+                    for (int q = 0; q < 7; ++q) dmf[7 * hh + q + NS * c] = a[q];
                 }
-                if (k < n - 1) {
-#pragma unroll
-                    for (int i = 0; i < 7; ++i) {
-                        const int e = lane + 32 * i;
-                        if (e < SS) Lw[e] = pl[i];
-                    }
-                }
-                __syncwarp();
-                if (k - 1 > m) {
-                    warp_fetch<ST, 4>(Sb + (size_t)(k - 1) * ks + PK_DIAG, 105, lane, pd);
-                    warp_fetch<ST, 7>(Sb + (size_t)k * ks, SS, lane, pl);
-                }
-                double d[NS];
-#pragma unroll
-                for (int a = 0; a < NS; ++a) d[a] = 0.0;
-                if (k < n - 1) {
-                    double w[7];
-                    full_times<false>(Fi, Lw, cq, hh, w);  // U_{k+1}^{-1} L_{k+1}
-                    lw_times<true>(Lw, hh, w, d);          // L_{k+1}^T U_{k+1}^{-1} L_{k+1}
-                }
-                double a[7];
-                load_block(Ap, d, a);
+            } else {
                 pair_gj_inverse(a, c, hh);
                 keep_inv(Fi, a, k);
             }
@@ -1367,12 +1364,12 @@ __global__ void __launch_bounds__(PAIR_THREADS, 4)
 #pragma unroll
             for (int i = 0; i < 7; ++i) {
                 const int e = lane + 32 * i;
-                if (e < SS) Lw[e] = pl[i];
+                if (e < SS) Lw[(e / NS) + NS * (e % NS)] = pl[i];  // transposed, as in the loop
             }
             __syncwarp();
             double w[7];
-            full_times<false>(Fi, Lw, cq, hh, w);
-            lw_times<true>(Lw, hh, w, d);
+            full_times<true>(Fi, Lw, cq, hh, w);
+            lw_times<false>(Lw, hh, w, d);
         }
         double a[7];
 #pragma unroll

@@ -267,7 +267,10 @@ __global__ void __launch_bounds__(32 * SCHUR_WARPS)
 // only the FP32 rounding of the KKT data (G, C, g, c).
 // ---------------------------------------------------------------------------
 
-template <int n>
+// FP64 Gauss-Jordan inverse of the n x n matrix (A + shift I), A column-major with leading
+// dimension LD; the inverse goes column-major with leading dimension LD to Ainv (and, when given,
+// Ainv32 / Ainv64g)
+template <int n, int LD = n>
 __device__ __forceinline__ void warp_inverse64(const float *A, double shift, double *Ainv, int lane,
                                                float *Ainv32, double *Ainv64g)
 {
@@ -276,7 +279,7 @@ __device__ __forceinline__ void warp_inverse64(const float *A, double shift, dou
 #pragma unroll
     for (int r = 0; r < n; ++r) {
         double v = 0.0;
-        if (left) v = (double)A[r + n * lane] + ((r == lane) ? shift : 0.0);
+        if (left) v = (double)A[r + LD * lane] + ((r == lane) ? shift : 0.0);
         else if (right) v = (r == lane - n) ? 1.0 : 0.0;
         col[r] = v;
     }
@@ -295,15 +298,63 @@ __device__ __forceinline__ void warp_inverse64(const float *A, double shift, dou
     if (right) {
         const int cc = lane - n;
 #pragma unroll
-        for (int r = 0; r < n; ++r) Ainv[r + n * cc] = col[r];
+        for (int r = 0; r < n; ++r) Ainv[r + LD * cc] = col[r];
         if (Ainv32) {
 #pragma unroll
-            for (int r = 0; r < n; ++r) Ainv32[r + n * cc] = (float)col[r];
+            for (int r = 0; r < n; ++r) Ainv32[r + LD * cc] = (float)col[r];
         }
         if (Ainv64g) {
 #pragma unroll
-            for (int r = 0; r < n; ++r) Ainv64g[r + n * cc] = col[r];
+            for (int r = 0; r < n; ++r) Ainv64g[r + LD * cc] = col[r];
         }
+    }
+}
+
+// (Q + shift I)^{-1} of a 14x14 state block.  The blocks kkt_kernel writes are block diagonal --
+// a 7x7 position block (q q^T), a diagonal velocity block (QD) -- and then the inverse is the
+// position block's 7x7 Gauss-Jordan and the reciprocals of the velocity diagonal.  Gauss-Jordan
+// without pivoting never mixes the two blocks of a block-diagonal matrix (every update it would
+// make across them multiplies an exact zero), so this is the same arithmetic as the full 14x14
+// elimination, result for result; any other Q takes the full elimination.
+__device__ __forceinline__ void warp_inverse64_state(const float *Q, double shift, double *Ainv, int lane,
+                                                     float *Ainv32, double *Ainv64g)
+{
+    bool ok = true;
+    for (int e = lane; e < SS; e += 32) {
+        const int r = e % NS, cc = e / NS;
+        if (((r < NC) != (cc < NC)) || (r >= NC && cc >= NC && r != cc)) ok = ok && (Q[e] == 0.f);
+    }
+    if (!__all_sync(0xffffffffu, ok)) {
+        warp_inverse64<NS>(Q, shift, Ainv, lane, Ainv32, Ainv64g);
+        return;
+    }
+    warp_inverse64<NC, NS>(Q, shift, Ainv, lane, Ainv32, Ainv64g);
+    for (int e = lane; e < SS; e += 32) {
+        const int r = e % NS, cc = e / NS;
+        if (r < NC && cc < NC) continue;
+        const double v = (r == cc) ? __drcp_rn((double)Q[e] + shift) : 0.0;
+        Ainv[e] = v;
+        if (Ainv32) Ainv32[e] = (float)v;
+        if (Ainv64g) Ainv64g[e] = v;
+    }
+}
+// (R + shift I)^{-1} of a 7x7 control block: reciprocals when R is diagonal (kkt_kernel's R_COST I;
+// the same arithmetic as the elimination), else Gauss-Jordan
+__device__ __forceinline__ void warp_inverse64_control(const float *R, double shift, double *Ainv, int lane,
+                                                       float *Ainv32, double *Ainv64g)
+{
+    bool ok = true;
+    for (int e = lane; e < CC; e += 32)
+        if (e % NC != e / NC) ok = ok && (R[e] == 0.f);
+    if (!__all_sync(0xffffffffu, ok)) {
+        warp_inverse64<NC>(R, shift, Ainv, lane, Ainv32, Ainv64g);
+        return;
+    }
+    for (int e = lane; e < CC; e += 32) {
+        const double v = (e % NC == e / NC) ? __drcp_rn((double)R[e] + shift) : 0.0;
+        Ainv[e] = v;
+        if (Ainv32) Ainv32[e] = (float)v;
+        if (Ainv64g) Ainv64g[e] = v;
     }
 }
 
@@ -356,8 +407,8 @@ __global__ void __launch_bounds__(32 * SCHUR_WARPS)
 
         if (k == 0) {
             const float *Q0 = G + (size_t)G_STRIDE * j;
-            warp_inverse64<NS>(Q0, rho, sm.Qki, lane, N == 1 ? Ginv + (size_t)G_STRIDE * j : nullptr,
-                               N == 1 ? Ginv64 + (size_t)G_STRIDE * j : nullptr);
+            warp_inverse64_state(Q0, rho, sm.Qki, lane, N == 1 ? Ginv + (size_t)G_STRIDE * j : nullptr,
+                                 N == 1 ? Ginv64 + (size_t)G_STRIDE * j : nullptr);
             if (lane < NS) sm.qk[lane] = (double)g[(size_t)NX * j + lane];
             __syncwarp();
             if (lane < NS) {
@@ -394,10 +445,10 @@ __global__ void __launch_bounds__(32 * SCHUR_WARPS)
         const float *Gk = G + (size_t)G_STRIDE * j;
         float *Gi32 = Ginv + (size_t)G_STRIDE * (j - 1);
         double *Gi64 = Ginv64 + (size_t)G_STRIDE * (j - 1);
-        warp_inverse64<NS>(Gkm1, rho, sm.Qki, lane, Gi32, Gi64);
-        warp_inverse64<NS>(Gk, rho, sm.Qkp1i, lane, k == N - 1 ? Ginv + (size_t)G_STRIDE * j : nullptr,
-                           k == N - 1 ? Ginv64 + (size_t)G_STRIDE * j : nullptr);
-        warp_inverse64<NC>(Gkm1 + SS, rho, sm.Rki, lane, Gi32 + SS, Gi64 + SS);
+        warp_inverse64_state(Gkm1, rho, sm.Qki, lane, Gi32, Gi64);
+        warp_inverse64_state(Gk, rho, sm.Qkp1i, lane, k == N - 1 ? Ginv + (size_t)G_STRIDE * j : nullptr,
+                             k == N - 1 ? Ginv64 + (size_t)G_STRIDE * j : nullptr);
+        warp_inverse64_control(Gkm1 + SS, rho, sm.Rki, lane, Gi32 + SS, Gi64 + SS);
         __syncwarp();
         warp_mm64<NS, NS, false>(sm.A, sm.Qki, NS, sm.phi, lane);   // phi = (-A) Qt^{-1}
         warp_mm64<NC, NC, false>(sm.B, sm.Rki, NC, sm.BRi, lane);   // (-B) Rt^{-1}
