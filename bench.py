@@ -34,11 +34,14 @@ sys.path.insert(0, ROOT)
 
 METRIC = "SQP solves/s @N=128 batched vs plain @rel-res 1e-5"
 SPEC = dict(timestep=0.01, integrator=1, qd_cost=1e-2, r_cost=1e-4)
-PCG_FLOATS_PER_KNOT = 784        # S 588 + Pinv 196 read once per PCG launch (algorithmic)
-# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one pcg_chain_kernel launch measured by
-# ncu on 148 instances x 128 knots (27.07 MB + 0.50 MB), per knot; it scales with the knots of a launch
-PCG_CHAIN_DRAM_BYTES_PER_KNOT = (27.068e6 + 0.504e6) / (148 * 128)
-PCG_FLOATS_PER_KNOT_ITER = 896   # S, Pinv and 8 vectors x 14 if re-read every PCG iteration (upper bound)
+# Algorithmic bytes of one PCG launch per knot with the exact preconditioner: the FP64 Schur row read
+# once (302 doubles: left block 196, diagonal lower triangle 105, pad), gamma (14 doubles), lambda in
+# and out (FP32) and the FP64 lambda written for dz
+PCG_BYTES_PER_KNOT = 8 * 302 + 8 * 14 + 2 * 4 * 14 + 8 * 14
+PCG_BJ_BYTES_PER_KNOT = 4 * 784  # block-Jacobi kernel: FP32 S (588) + Pinv (196) read once
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one launch, per knot, from ncu captures of
+# 148 instances x 128 knots; they scale with the knots of a launch
+PCG_DRAM_BYTES_PER_KNOT = {"pcg_pair_kernel": (52.677e6 + 2.764e6) / (148 * 128)}
 ALG_FLOATS_PER_KNOT_SQP = 4058   # every materialised SQP-iteration tensor written once, read once
 
 
@@ -370,13 +373,13 @@ def main():
     mp = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
         os.path.join(ROOT, "MEASURED_PEAKS.json")) else None
     peak = mp["hbm_gbs"] if mp else 6650.0
-    per_launch_bytes = 4.0 * PCG_FLOATS_PER_KNOT * N * B
-    # PCG iterations per launch over the timed steps (pcg_launches counts one profiled step)
-    stream_bytes = 4.0 * PCG_FLOATS_PER_KNOT_ITER * N * pcg_total / max(pcg_launches * args.steps, 1)
+    pcg_kernel = ("pcg_cluster_kernel" if args.pcg_precond == 0 else
+                  "pcg_pair_kernel" if tuned_cs == gpt.PCG_WARP_PAIR else "pcg_chain_kernel")
+    per_launch_bytes = (PCG_BJ_BYTES_PER_KNOT if args.pcg_precond == 0 else PCG_BYTES_PER_KNOT) * N * B
     per_launch_s = (pcg_ms / max(pcg_launches, 1)) / 1000.0
     achieved = per_launch_bytes / per_launch_s / 1e9 if per_launch_s > 0 else 0.0
     precond_name = "block-tridiagonal LDL^T" if args.pcg_precond == 1 else "block-Jacobi"
-    pcg_kernel = "pcg_chain_kernel" if args.pcg_precond == 1 else "pcg_cluster_kernel"
+    dram_pk = PCG_DRAM_BYTES_PER_KNOT.get(pcg_kernel)
     line = {
         "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
@@ -389,11 +392,12 @@ def main():
                    "pcg_cluster_source": "given" if args.pcg_cluster else "gpt_autotune",
                    "l2": "256 MB buffer written between timed steps"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": (PCG_CHAIN_DRAM_BYTES_PER_KNOT * N * B if args.pcg_precond == 1 else None),
+                     "traffic": dram_pk * N * B if dram_pk else None,
                      "traffic_source": "ncu capture of 148 x 128 knots scaled to the launch's knots",
                      "kernel": pcg_kernel,
-                     "bytes_model": "784 floats per knot per launch (S 588 + Pinv 196 read once)",
-                     "stream_bound_gbs": stream_bytes / per_launch_s / 1e9 if per_launch_s > 0 else 0.0,
+                     "bytes_model": ("2752 B per knot per launch: FP64 Schur row 302 doubles read once, gamma, "
+                                     "lambda in/out FP32, lambda FP64 out" if args.pcg_precond == 1 else
+                                     "784 floats per knot per launch (S 588 + Pinv 196 read once)"),
                      "peak_source": "measured" if mp else "fallback"},
         "cpu_baseline": cb,
         "e2e": {"value": world * B / (e2e_step / 1000.0), "unit": "solves/s", "h2d_bytes_per_step": h2d,

@@ -358,31 +358,34 @@ __device__ __forceinline__ void warp_inverse64_control(const float *R, double sh
     }
 }
 
-// out (14 x NCOL, col-major) = A (14 x K, col-major) * op(B), FP64
-template <int K, int NCOL, bool TRANS_B>
-__device__ __forceinline__ void warp_mm64(const double *A, const double *B, int ldb, double *out, int lane)
+// out (14 x NCOL, col-major) (+)= A (14 x K, col-major) * op(B), FP64 accumulation; A and B may be
+// FP32 or FP64 (FP32 operands are exact in FP64)
+template <int K, int NCOL, bool TRANS_B, bool ACC = false, typename TA, typename TB>
+__device__ __forceinline__ void warp_mm64(const TA *A, const TB *B, int ldb, double *out, int lane)
 {
     if (lane < 2 * NCOL) {
         const int col = lane % NCOL, r0 = (lane / NCOL) * 7;
         double acc[7];
 #pragma unroll
-        for (int i = 0; i < 7; ++i) acc[i] = 0.0;
+        for (int i = 0; i < 7; ++i) acc[i] = ACC ? out[r0 + i + NS * col] : 0.0;
 #pragma unroll
         for (int t = 0; t < K; ++t) {
-            const double bv = TRANS_B ? B[col + ldb * t] : B[t + ldb * col];
+            const double bv = (double)(TRANS_B ? B[col + ldb * t] : B[t + ldb * col]);
 #pragma unroll
-            for (int i = 0; i < 7; ++i) acc[i] = fma(A[r0 + i + NS * t], bv, acc[i]);
+            for (int i = 0; i < 7; ++i) acc[i] = fma((double)A[r0 + i + NS * t], bv, acc[i]);
         }
 #pragma unroll
         for (int i = 0; i < 7; ++i) out[r0 + i + NS * col] = acc[i];
     }
 }
 
+// One warp's shared memory: the knot's KKT blocks staged as FP32 (one batch of loads per knot), the
+// FP64 inverses and products
 struct Schur64WarpSmem {
-    double A[SS], B[SC];
     double Qki[SS], Qkp1i[SS], Rki[CC];
-    double phi[SS], BRi[SC], theta[SS], tmp[SS];
+    double phi[SS], BRi[SC], theta[SS];
     double qk[NS], qkp1[NS], rk[NC], ck[NS];
+    float Gm1[G_STRIDE], Gk[SS], C[C_STRIDE];
 };
 
 __global__ void __launch_bounds__(32 * SCHUR_WARPS)
@@ -407,9 +410,11 @@ __global__ void __launch_bounds__(32 * SCHUR_WARPS)
 
         if (k == 0) {
             const float *Q0 = G + (size_t)G_STRIDE * j;
-            warp_inverse64_state(Q0, rho, sm.Qki, lane, N == 1 ? Ginv + (size_t)G_STRIDE * j : nullptr,
-                                 N == 1 ? Ginv64 + (size_t)G_STRIDE * j : nullptr);
+            for (int e = lane; e < SS; e += 32) sm.Gk[e] = Q0[e];
             if (lane < NS) sm.qk[lane] = (double)g[(size_t)NX * j + lane];
+            __syncwarp();
+            warp_inverse64_state(sm.Gk, rho, sm.Qki, lane, N == 1 ? Ginv + (size_t)G_STRIDE * j : nullptr,
+                                 N == 1 ? Ginv64 + (size_t)G_STRIDE * j : nullptr);
             __syncwarp();
             if (lane < NS) {
                 double acc = 0.0;
@@ -427,34 +432,56 @@ __global__ void __launch_bounds__(32 * SCHUR_WARPS)
             continue;
         }
 
-        // ---- rows k >= 1
-        const float *Ck = Cm + (size_t)C_STRIDE * (j - 1);
-        for (int e = lane; e < C_STRIDE; e += 32) {
-            const double v = (double)Ck[e];
-            if (e < SS) sm.A[e] = v;
-            else sm.B[e - SS] = v;
+        // ---- rows k >= 1: every input of the knot loaded in one batch, then staged
+        {
+            const float *Gkm1 = G + (size_t)G_STRIDE * (j - 1);
+            const float *Gkq = G + (size_t)G_STRIDE * j;
+            const float *Ck = Cm + (size_t)C_STRIDE * (j - 1);
+            constexpr int NL = (G_STRIDE + SS + C_STRIDE + 31) / 32;  // 24 per lane
+            float v[NL];
+#pragma unroll
+            for (int i = 0; i < NL; ++i) {
+                const int e = lane + 32 * i;
+                v[i] = e < G_STRIDE ? Gkm1[e] : (e < G_STRIDE + SS ? Gkq[e - G_STRIDE]
+                                                : (e < G_STRIDE + SS + C_STRIDE ? Ck[e - G_STRIDE - SS] : 0.f));
+            }
+            double gv = 0.0;
+            if (lane < NX) gv = (double)g[(size_t)NX * (j - 1) + lane];
+            double g2 = 0.0, cv = 0.0;
+            if (lane < NS) {
+                g2 = (double)g[(size_t)NX * j + lane];
+                cv = (double)c[(size_t)NS * j + lane];
+            }
+#pragma unroll
+            for (int i = 0; i < NL; ++i) {
+                const int e = lane + 32 * i;
+                if (e < G_STRIDE) sm.Gm1[e] = v[i];
+                else if (e < G_STRIDE + SS) sm.Gk[e - G_STRIDE] = v[i];
+                else if (e < G_STRIDE + SS + C_STRIDE) sm.C[e - G_STRIDE - SS] = v[i];
+            }
+            if (lane < NS) {
+                sm.qk[lane] = gv;
+                sm.qkp1[lane] = g2;
+                sm.ck[lane] = cv;
+            } else if (lane < NX) {
+                sm.rk[lane - NS] = gv;
+            }
         }
-        if (lane < NS) {
-            sm.qk[lane] = (double)g[(size_t)NX * (j - 1) + lane];
-            sm.qkp1[lane] = (double)g[(size_t)NX * j + lane];
-            sm.ck[lane] = (double)c[(size_t)NS * j + lane];
-        } else if (lane < NS + NC) {
-            sm.rk[lane - NS] = (double)g[(size_t)NX * (j - 1) + lane];
-        }
-        const float *Gkm1 = G + (size_t)G_STRIDE * (j - 1);
-        const float *Gk = G + (size_t)G_STRIDE * j;
+        __syncwarp();
         float *Gi32 = Ginv + (size_t)G_STRIDE * (j - 1);
         double *Gi64 = Ginv64 + (size_t)G_STRIDE * (j - 1);
-        warp_inverse64_state(Gkm1, rho, sm.Qki, lane, Gi32, Gi64);
-        warp_inverse64_state(Gk, rho, sm.Qkp1i, lane, k == N - 1 ? Ginv + (size_t)G_STRIDE * j : nullptr,
+        warp_inverse64_state(sm.Gm1, rho, sm.Qki, lane, Gi32, Gi64);
+        warp_inverse64_state(sm.Gk, rho, sm.Qkp1i, lane, k == N - 1 ? Ginv + (size_t)G_STRIDE * j : nullptr,
                              k == N - 1 ? Ginv64 + (size_t)G_STRIDE * j : nullptr);
-        warp_inverse64_control(Gkm1 + SS, rho, sm.Rki, lane, Gi32 + SS, Gi64 + SS);
+        warp_inverse64_control(sm.Gm1 + SS, rho, sm.Rki, lane, Gi32 + SS, Gi64 + SS);
         __syncwarp();
-        warp_mm64<NS, NS, false>(sm.A, sm.Qki, NS, sm.phi, lane);   // phi = (-A) Qt^{-1}
-        warp_mm64<NC, NC, false>(sm.B, sm.Rki, NC, sm.BRi, lane);   // (-B) Rt^{-1}
+        const float *Am = sm.C, *Bm = sm.C + SS;                              // -A, -B
+        warp_mm64<NS, NS, false>(Am, sm.Qki, NS, sm.phi, lane);              // phi = (-A) Qt^{-1}
+        warp_mm64<NC, NC, false>(Bm, sm.Rki, NC, sm.BRi, lane);              // (-B) Rt^{-1}
         __syncwarp();
-        warp_mm64<NS, NS, true>(sm.phi, sm.A, NS, sm.theta, lane);  // phi (-A)^T
-        warp_mm64<NC, NS, true>(sm.BRi, sm.B, NS, sm.tmp, lane);    // (-B) Rt^{-1} (-B)^T
+        warp_mm64<NS, NS, true>(sm.phi, Am, NS, sm.theta, lane);             // phi (-A)^T
+        __syncwarp();
+        warp_mm64<NC, NS, true, true>(sm.BRi, Bm, NS, sm.theta, lane);       // + (-B) Rt^{-1} (-B)^T
         if (lane < NS) {
             double a1 = 0.0, a2 = 0.0, a3 = 0.0;
 #pragma unroll
@@ -470,7 +497,7 @@ __global__ void __launch_bounds__(32 * SCHUR_WARPS)
         for (int e = lane; e < SS; e += 32) {
             const int r = e % NS, cc = e / NS;
             Pk[e] = -sm.phi[e];
-            if (r >= cc) Pk[SS + ((r * (r + 1)) >> 1) + cc] = -((sm.theta[e] + sm.Qkp1i[e]) + sm.tmp[e]);
+            if (r >= cc) Pk[SS + ((r * (r + 1)) >> 1) + cc] = -(sm.theta[e] + sm.Qkp1i[e]);
         }
         if (lane == 0) Pk[PK64 - 1] = 0.0;
         __syncwarp();
