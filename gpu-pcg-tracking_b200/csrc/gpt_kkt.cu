@@ -1,18 +1,18 @@
-// gpt_kkt.cu -- KKT formation: one warp per knot.
+// gpt_kkt.cu -- KKT formation: one half-warp per knot.
 //
 // Replaces gato_form_kkt (schur.cuh:391-524) with the per-knot pieces it
 // calls: integratorAndGradient (integrator.cuh:159-183), the plant's
 // forwardDynamicsAndGradient (rbdfiles/iiwa_eepos_plant.cuh:126-156) and
 // trackingCostGradientAndHessian[_lastblock] (iiwa_eepos_plant.cuh:295-401).
 //
-// Per knot k < N-1 the warp computes, with no block-wide barrier:
+// Per knot k < N-1 the half-warp computes, with no block-wide barrier:
 //   lanes 0..6   M(q) e_j  (inverse dynamics with qd = 0, qdd = e_j)
 //   lane  7      c(q, qd)  (bias force)
 //   lanes 0..7   FP64 Cholesky of M: Minv columns and qdd = Minv (u - c)
 //   lanes 0..13  d ID(q, qd, qdd) / d(q_j | qd_j)  (forward-mode RNEA tangent)
 //   all lanes    df/du = [-Minv dID/dx, Minv], A_k, B_k, defect, cost terms
 // and writes the reference blocks G_k = {Q_k, R_k}, C_k = {-A_k, -B_k},
-// g_k = {q_k, r_k}, c_{k+1}.  The warp of knot N-2 also writes the terminal
+// g_k = {q_k, r_k}, c_{k+1}.  The half-warp of knot N-2 also writes the terminal
 // Q_{N-1}, q_{N-1} and c_0 = x_0 - x_s (schur.cuh:429-479).
 #include "gpt_common.cuh"
 #include "gpt_dyn.cuh"
@@ -36,52 +36,62 @@ struct KktWarpSmem {
 
 constexpr int KKT_WARPS = 4;
 
+// Two knots per warp, one per half-warp (lanes hl = 0..15): the dynamics phases keep at most 14
+// lanes of a knot busy, so a knot per half-warp halves their instructions per knot.  A half-warp
+// without a knot (odd count, last knot of an instance, inactive instance) computes on knot 0's data
+// and writes nothing, so both halves take every __syncwarp.
 __global__ void __launch_bounds__(32 * KKT_WARPS) kkt_kernel(BatchView bv, ProblemParams P, const float *__restrict__ xu,
                                                            const float *__restrict__ goal,
                                                            const float *__restrict__ xs, float *__restrict__ G,
                                                            float *__restrict__ Cm, float *__restrict__ g,
                                                            float *__restrict__ c)
 {
-    __shared__ KktWarpSmem smem_all[KKT_WARPS];
-    const int lane = threadIdx.x & 31;
-    KktWarpSmem &sm = smem_all[threadIdx.x >> 5];
+    __shared__ KktWarpSmem smem_all[2 * KKT_WARPS];
+    const int lane = threadIdx.x & 31, half = lane >> 4, hl = lane & 15;
+    KktWarpSmem &sm = smem_all[2 * (threadIdx.x >> 5) + half];
     const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nw = (gridDim.x * blockDim.x) >> 5;
 
-    for (int j = gw; j < bv.total_knots; j += nw) {
-        const int b = bv.inst(j);
-        const int N = bv.N(b);
-        const int k = j - bv.off(b);
-        if (k >= N - 1 || !bv.active(b)) continue;
-        const bool terminal = (k == N - 2);
+    for (int jp = gw; 2 * jp < bv.total_knots; jp += nw) {
+        const int j = 2 * jp + half;
+        bool valid = j < bv.total_knots;
+        int b = 0, N = 2, k = 0;
+        if (valid) {
+            b = bv.inst(j);
+            N = bv.N(b);
+            k = j - bv.off(b);
+            valid = (k < N - 1) && bv.active(b);
+        }
+        const int jj = valid ? j : 0;  // knot 0 always has a successor (N >= 2)
+        const bool terminal = valid && (k == N - 2);
 
         // ---- stage x_k, u_k, x_{k+1}, goal_k, goal_{k+1}
-        const float *xk = xu + (size_t)NX * j;
-        for (int i = lane; i < NX + NS; i += 32) {
+        const float *xk = xu + (size_t)NX * jj;
+        for (int i = hl; i < NX + NS; i += 16) {
             float v = xk[i];
             if (i < NS) sm.x[i] = v;
             else if (i < NX) sm.u[i - NS] = v;
             else sm.xn[i - NX] = v;
         }
-        if (lane < 12) sm.goal[lane] = goal[(size_t)6 * j + lane];
+        if (hl < 12) sm.goal[hl] = goal[(size_t)6 * jj + hl];
         __syncwarp();
 
         JointTrig trig;
         joint_trig(sm.x, trig);
 
-        // ---- mass-matrix columns and bias force
+        // ---- mass-matrix columns (lanes 0..6) and bias force (lane 7)
         {
             float qd[NQ], qdd[NQ], tau[NQ];
 #pragma unroll
             for (int i = 0; i < NQ; ++i) {
-                qd[i] = (lane == 7) ? sm.x[NQ + i] : 0.f;
-                qdd[i] = (lane == i) ? 1.f : 0.f;
+                qd[i] = (hl == 7) ? sm.x[NQ + i] : 0.f;
+                qdd[i] = (hl == i) ? 1.f : 0.f;
             }
             rnea<false>(trig, qd, qdd, -1, -1, tau, nullptr);
-            if (lane < NQ) {
+            if (hl < NQ) {
 #pragma unroll
-                for (int r = 0; r < NQ; ++r) sm.M[NQ * lane + r] = tau[r];
-            } else if (lane == NQ) {
+                for (int r = 0; r < NQ; ++r) sm.M[NQ * hl + r] = tau[r];
+            } else if (hl == NQ) {
 #pragma unroll
                 for (int r = 0; r < NQ; ++r) sm.cbias[r] = tau[r];
             }
@@ -89,16 +99,16 @@ __global__ void __launch_bounds__(32 * KKT_WARPS) kkt_kernel(BatchView bv, Probl
         __syncwarp();
 
         // ---- Minv columns (lanes 0..6) and qdd (lane 7), FP64 Cholesky
-        if (lane <= NQ) {
+        if (hl <= NQ) {
             double L[CC], rhs[NQ], sol[NQ];
             chol7_factor(sm.M, L);
 #pragma unroll
             for (int i = 0; i < NQ; ++i)
-                rhs[i] = (lane < NQ) ? (double)(lane == i) : (double)sm.u[i] - (double)sm.cbias[i];
+                rhs[i] = (hl < NQ) ? (double)(hl == i) : (double)sm.u[i] - (double)sm.cbias[i];
             chol7_solve(L, rhs, sol);
-            if (lane < NQ) {
+            if (hl < NQ) {
 #pragma unroll
-                for (int i = 0; i < NQ; ++i) sm.Minv[NQ * lane + i] = (float)sol[i];
+                for (int i = 0; i < NQ; ++i) sm.Minv[NQ * hl + i] = (float)sol[i];
             } else {
 #pragma unroll
                 for (int i = 0; i < NQ; ++i) sm.qdd[i] = (float)sol[i];
@@ -114,18 +124,18 @@ __global__ void __launch_bounds__(32 * KKT_WARPS) kkt_kernel(BatchView bv, Probl
                 qd[i] = sm.x[NQ + i];
                 qdd[i] = sm.qdd[i];
             }
-            const int dq_dir = (lane < NQ) ? lane : -1;
-            const int dqd_dir = (lane >= NQ && lane < NS) ? lane - NQ : -1;
+            const int dq_dir = (hl < NQ) ? hl : -1;
+            const int dqd_dir = (hl >= NQ && hl < NS) ? hl - NQ : -1;
             rnea<true>(trig, qd, qdd, dq_dir, dqd_dir, tau, dtau);
-            if (lane < NS) {
+            if (hl < NS) {
 #pragma unroll
-                for (int r = 0; r < NQ; ++r) sm.dc[NQ * lane + r] = dtau[r];
+                for (int r = 0; r < NQ; ++r) sm.dc[NQ * hl + r] = dtau[r];
             }
         }
         // ---- end-effector position and Jacobian (lane 0 at x_k, lane 1 at the terminal state)
-        if (lane == 0) {
+        if (hl == 0) {
             fk_lane<true>(trig, sm.ee[0], sm.J[0]);
-        } else if (lane == 1 && terminal && !P.ref_terminal) {
+        } else if (hl == 1 && terminal && !P.ref_terminal) {
             JointTrig t2;
             joint_trig(sm.xn, t2);
             fk_lane<true>(t2, sm.ee[1], sm.J[1]);
@@ -133,7 +143,7 @@ __global__ void __launch_bounds__(32 * KKT_WARPS) kkt_kernel(BatchView bv, Probl
         __syncwarp();
 
         // ---- df/du (iiwa_eepos_plant.cuh:142-155)
-        for (int e = lane; e < NQ * NX; e += 32) {
+        for (int e = hl; e < NQ * NX; e += 16) {
             float v;
             if (e < NQ * NS) {
                 const int col = e / NQ, r = e - NQ * col;
@@ -147,22 +157,20 @@ __global__ void __launch_bounds__(32 * KKT_WARPS) kkt_kernel(BatchView bv, Probl
             sm.dfdu[e] = v;
         }
         // ---- cost gradient (iiwa_eepos_plant.cuh:329-354)
-        if (lane < NS) {
-            const int which = 0;
+        if (hl < NS) {
             float v;
-            if (lane < NQ) {
-                const float *J = sm.J[which];
-                v = P.q_ee * (J[3 * lane] * (sm.ee[which][0] - sm.goal[0]) +
-                              J[3 * lane + 1] * (sm.ee[which][1] - sm.goal[1]) +
-                              J[3 * lane + 2] * (sm.ee[which][2] - sm.goal[2]));
+            if (hl < NQ) {
+                const float *J = sm.J[0];
+                v = P.q_ee * (J[3 * hl] * (sm.ee[0][0] - sm.goal[0]) + J[3 * hl + 1] * (sm.ee[0][1] - sm.goal[1]) +
+                              J[3 * hl + 2] * (sm.ee[0][2] - sm.goal[2]));
             } else {
-                v = P.qd_cost * sm.x[lane];
+                v = P.qd_cost * sm.x[hl];
             }
-            sm.qv[0][lane] = v;
+            sm.qv[0][hl] = v;
         }
         __syncwarp();
-        if (terminal && lane >= 16 && lane < 16 + NS) {
-            const int i = lane - 16;
+        if (terminal && hl < NS) {
+            const int i = hl;
             const int which = P.ref_terminal ? 0 : 1;
             const float *xt = P.ref_terminal ? sm.x : sm.xn;
             // terminal target: goal_{N-1}; in the reference's layout (ref_terminal) the kernel
@@ -188,72 +196,75 @@ __global__ void __launch_bounds__(32 * KKT_WARPS) kkt_kernel(BatchView bv, Probl
         }
         __syncwarp();
 
-        // ---- C_k = {-A_k, -B_k} (integrator.cuh:85-126, sign from schur.cuh:519-520)
-        float *Ck = Cm + (size_t)C_STRIDE * j;
-        const float dt = P.dt;
-        for (int e = lane; e < C_STRIDE; e += 32) {
-            float val;
-            if (e < SS) {
-                const int col = e / NS, r = e - NS * col;
-                if (P.integrator == 0) {
-                    val = (float)(r == col);
-                    if (r < NQ && r == col - NQ) val += dt;
-                    if (r >= NQ) val += dt * sm.dfdu[col * NQ + r - NQ];
+        if (valid) {
+            // ---- C_k = {-A_k, -B_k} (integrator.cuh:85-126, sign from schur.cuh:519-520)
+            float *Ck = Cm + (size_t)C_STRIDE * j;
+            const float dt = P.dt;
+            for (int e = hl; e < C_STRIDE; e += 16) {
+                float val;
+                if (e < SS) {
+                    const int col = e / NS, r = e - NS * col;
+                    if (P.integrator == 0) {
+                        val = (float)(r == col);
+                        if (r < NQ && r == col - NQ) val += dt;
+                        if (r >= NQ) val += dt * sm.dfdu[col * NQ + r - NQ];
+                    } else {
+                        const int rq = r % NQ;
+                        const float dtv = (r == rq) ? dt : 1.f;
+                        val = (float)(r == col) + dt * (float)(r == col - NQ) + dt * sm.dfdu[col * NQ + rq] * dtv;
+                    }
                 } else {
-                    const int rq = r % NQ;
-                    const float dtv = (r == rq) ? dt : 1.f;
-                    val = (float)(r == col) + dt * (float)(r == col - NQ) + dt * sm.dfdu[col * NQ + rq] * dtv;
+                    const int e2 = e - SS, col = e2 / NS, r = e2 - NS * col;
+                    if (P.integrator == 0) {
+                        val = (r >= NQ) ? dt * sm.dfdu[(NS + col) * NQ + r - NQ] : 0.f;
+                    } else {
+                        const int rq = r % NQ;
+                        const float dtv = (r == rq) ? dt : 1.f;
+                        val = dt * sm.dfdu[SC + col * NQ + rq] * dtv;
+                    }
                 }
-            } else {
-                const int e2 = e - SS, col = e2 / NS, r = e2 - NS * col;
+                Ck[e] = -val;
+            }
+            // ---- defect c_{k+1} = x_{k+1} - f(x_k, u_k)  (integrator.cuh:25-83)
+            if (hl < NQ) {
+                const float q = sm.x[hl], qd = sm.x[NQ + hl], a = sm.qdd[hl];
+                float nq, nqd;
                 if (P.integrator == 0) {
-                    val = (r >= NQ) ? dt * sm.dfdu[(NS + col) * NQ + r - NQ] : 0.f;
+                    nq = q + dt * qd;
+                    nqd = qd + dt * a;
                 } else {
-                    const int rq = r % NQ;
-                    const float dtv = (r == rq) ? dt : 1.f;
-                    val = dt * sm.dfdu[SC + col * NQ + rq] * dtv;
+                    nqd = qd + dt * a;
+                    nq = q + dt * nqd;
                 }
+                float *cn = c + (size_t)NS * (j + 1);
+                cn[hl] = sm.xn[hl] - nq;
+                cn[NQ + hl] = sm.xn[NQ + hl] - nqd;
             }
-            Ck[e] = -val;
-        }
-        // ---- defect c_{k+1} = x_{k+1} - f(x_k, u_k)  (integrator.cuh:25-83)
-        if (lane < NQ) {
-            const float q = sm.x[lane], qd = sm.x[NQ + lane], a = sm.qdd[lane];
-            float nq, nqd;
-            if (P.integrator == 0) {
-                nq = q + dt * qd;
-                nqd = qd + dt * a;
-            } else {
-                nqd = qd + dt * a;
-                nq = q + dt * nqd;
+            // ---- G_k = {Q_k, R_k}, g_k = {q_k, r_k}
+            float *Gk = G + (size_t)G_STRIDE * j;
+            for (int e = hl; e < G_STRIDE; e += 16) {
+                float v;
+                if (e < SS) {
+                    const int i = e / NS, jq = e - NS * i;
+                    v = (i < NQ && jq < NQ) ? sm.qv[0][i] * sm.qv[0][jq] : ((i == jq) ? P.qd_cost : 0.f);
+                } else {
+                    v = ((e - SS) % (NC + 1) == 0) ? P.r_cost : 0.f;
+                }
+                Gk[e] = v;
             }
-            float *cn = c + (size_t)NS * (j + 1);
-            cn[lane] = sm.xn[lane] - nq;
-            cn[NQ + lane] = sm.xn[NQ + lane] - nqd;
-        }
-        // ---- G_k = {Q_k, R_k}, g_k = {q_k, r_k}
-        float *Gk = G + (size_t)G_STRIDE * j;
-        for (int e = lane; e < G_STRIDE; e += 32) {
-            float v;
-            if (e < SS) {
-                const int i = e / NS, jj = e - NS * i;
-                v = (i < NQ && jj < NQ) ? sm.qv[0][i] * sm.qv[0][jj] : ((i == jj) ? P.qd_cost : 0.f);
-            } else {
-                v = ((e - SS) % (NC + 1) == 0) ? P.r_cost : 0.f;
-            }
-            Gk[e] = v;
-        }
-        if (lane < NX) g[(size_t)NX * j + lane] = (lane < NS) ? sm.qv[0][lane] : P.r_cost * sm.u[lane - NS];
-        if (terminal) {
-            float *Gt = G + (size_t)G_STRIDE * (j + 1);
-            for (int e = lane; e < SS; e += 32) {
-                const int i = e / NS, jj = e - NS * i;
-                Gt[e] = (i < NQ && jj < NQ) ? sm.qv[1][i] * sm.qv[1][jj] : ((i == jj) ? P.qd_cost : 0.f);
-            }
-            if (lane < NS) {
-                g[(size_t)NX * (j + 1) + lane] = sm.qv[1][lane];
-                const int j0 = j - k;
-                c[(size_t)NS * j0 + lane] = xu[(size_t)NX * j0 + lane] - xs[(size_t)NS * b + lane];
+            for (int e = hl; e < NX; e += 16)
+                g[(size_t)NX * j + e] = (e < NS) ? sm.qv[0][e] : P.r_cost * sm.u[e - NS];
+            if (terminal) {
+                float *Gt = G + (size_t)G_STRIDE * (j + 1);
+                for (int e = hl; e < SS; e += 16) {
+                    const int i = e / NS, jq = e - NS * i;
+                    Gt[e] = (i < NQ && jq < NQ) ? sm.qv[1][i] * sm.qv[1][jq] : ((i == jq) ? P.qd_cost : 0.f);
+                }
+                if (hl < NS) {
+                    g[(size_t)NX * (j + 1) + hl] = sm.qv[1][hl];
+                    const int j0 = j - k;
+                    c[(size_t)NS * j0 + hl] = xu[(size_t)NX * j0 + hl] - xs[(size_t)NS * b + hl];
+                }
             }
         }
         __syncwarp();
@@ -264,7 +275,7 @@ cudaError_t launch_kkt(const BatchView &bv, const ProblemParams &P, const float 
                        const float *xs, float *G, float *C, float *g, float *c, int num_sms, cudaStream_t s)
 {
     if (bv.total_knots <= 0) return cudaSuccess;
-    int warps = bv.total_knots;
+    int warps = (bv.total_knots + 1) / 2;  // two knots per warp
     int blocks = (warps + KKT_WARPS - 1) / KKT_WARPS;
     const int cap = num_sms * 16;
     if (blocks > cap) blocks = cap;
