@@ -69,6 +69,19 @@ struct ProblemParams {
     int ref_terminal;  // 1: terminal Q,q at x_{N-2}, target Q_{N-2}[0][0..2], as the reference's kernel computes
 };
 
+// Reciprocal by two Newton-Raphson steps r <- r + r (1 - x r) from the PTX approximation
+// rcp.approx.ftz.f64 (quadratic convergence: a seed accurate to ~2^-20 reaches FP64 rounding);
+// x is a positive pivot of an SPD elimination, far from the FP64 range limits
+__device__ __forceinline__ double rcp_newton(double x)
+{
+    double r;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
+    double e = fma(-x, r, 1.0);
+    r = fma(r, e, r);
+    e = fma(-x, r, 1.0);
+    return fma(r, e, r);
+}
+
 __device__ __forceinline__ float warp_sum(float v)
 {
 #pragma unroll

@@ -292,46 +292,23 @@ __device__ __forceinline__ void rnea(const JointTrig &t, const float *qd, const 
     rnea_bwd<0, TANGENT>(t, dq_dir, st, tau, dtau);
 }
 
-// In-register FP64 Cholesky inverse of a 7x7 SPD matrix given column-major in
-// M (shared memory or registers).  Returns false if the matrix is not
-// numerically positive definite.
-__device__ __forceinline__ bool chol7_factor(const float *M, double *L)
+// Gauss-Jordan elimination with a 7x7 SPD matrix M (no pivoting: every pivot is positive) over a
+// group of lanes holding the columns of [M | R]: lane base + i holds column i (7 entries).
+// Afterwards the lanes of R's columns hold M^{-1} R (and M's lanes the identity).  Every lane of
+// the warp calls it; lanes outside a group pass any base of a real group and ignore the result.
+__device__ __forceinline__ void gj7_group(double (&col)[7], int base)
 {
 #pragma unroll
-    for (int j = 0; j < 7; ++j) {
-        double d = (double)M[j + 7 * j];
+    for (int p = 0; p < 7; ++p) {
+        const double piv = __shfl_sync(0xffffffffu, col[p], base + p);
+        const double prow = col[p] * rcp_newton(piv);
 #pragma unroll
-        for (int k = 0; k < j; ++k) d -= L[j + 7 * k] * L[j + 7 * k];
-        if (!(d > 0.0)) return false;
-        const double ljj = sqrt(d), inv = __drcp_rn(ljj);
-        L[j + 7 * j] = ljj;
-#pragma unroll
-        for (int i = j + 1; i < 7; ++i) {
-            double s = 0.5 * ((double)M[i + 7 * j] + (double)M[j + 7 * i]);
-#pragma unroll
-            for (int k = 0; k < j; ++k) s -= L[i + 7 * k] * L[j + 7 * k];
-            L[i + 7 * j] = s * inv;
+        for (int r = 0; r < 7; ++r) {
+            if (r == p) continue;
+            const double pr = __shfl_sync(0xffffffffu, col[r], base + p);
+            col[r] = fma(-pr, prow, col[r]);
         }
-    }
-    return true;
-}
-// x = (L L^T)^{-1} b
-__device__ __forceinline__ void chol7_solve(const double *L, const double *b, double *x)
-{
-    double y[7];
-#pragma unroll
-    for (int i = 0; i < 7; ++i) {
-        double s = b[i];
-#pragma unroll
-        for (int k = 0; k < i; ++k) s -= L[i + 7 * k] * y[k];
-        y[i] = s / L[i + 7 * i];
-    }
-#pragma unroll
-    for (int i = 6; i >= 0; --i) {
-        double s = y[i];
-#pragma unroll
-        for (int k = i + 1; k < 7; ++k) s -= L[k + 7 * i] * x[k];
-        x[i] = s / L[i + 7 * i];
+        col[p] = prow;
     }
 }
 

@@ -8,7 +8,7 @@
 // Per knot k < N-1 the half-warp computes, with no block-wide barrier:
 //   lanes 0..6   M(q) e_j  (inverse dynamics with qd = 0, qdd = e_j)
 //   lane  7      c(q, qd)  (bias force)
-//   lanes 0..7   FP64 Cholesky of M: Minv columns and qdd = Minv (u - c)
+//   lanes 0..14  FP64 Gauss-Jordan on [M | I | u - c]: Minv columns and qdd = Minv (u - c)
 //   lanes 0..13  d ID(q, qd, qdd) / d(q_j | qd_j)  (forward-mode RNEA tangent)
 //   all lanes    df/du = [-Minv dID/dx, Minv], A_k, B_k, defect, cost terms
 // and writes the reference blocks G_k = {Q_k, R_k}, C_k = {-A_k, -B_k},
@@ -98,20 +98,24 @@ __global__ void __launch_bounds__(32 * KKT_WARPS) kkt_kernel(BatchView bv, Probl
         }
         __syncwarp();
 
-        // ---- Minv columns (lanes 0..6) and qdd (lane 7), FP64 Cholesky
-        if (hl <= NQ) {
-            double L[CC], rhs[NQ], sol[NQ];
-            chol7_factor(sm.M, L);
+        // ---- Minv (lanes 7..13) and qdd = Minv (u - c) (lane 14): Gauss-Jordan on [M | I | u - c] in FP64
+        {
+            double col[NQ];
 #pragma unroll
-            for (int i = 0; i < NQ; ++i)
-                rhs[i] = (hl < NQ) ? (double)(hl == i) : (double)sm.u[i] - (double)sm.cbias[i];
-            chol7_solve(L, rhs, sol);
-            if (hl < NQ) {
+            for (int r = 0; r < NQ; ++r) {
+                double v = 0.0;
+                if (hl < NQ) v = 0.5 * ((double)sm.M[NQ * hl + r] + (double)sm.M[NQ * r + hl]);  // symmetric part
+                else if (hl < 2 * NQ) v = (r == hl - NQ) ? 1.0 : 0.0;
+                else if (hl == 2 * NQ) v = (double)sm.u[r] - (double)sm.cbias[r];
+                col[r] = v;
+            }
+            gj7_group(col, 16 * half);
+            if (hl >= NQ && hl < 2 * NQ) {
 #pragma unroll
-                for (int i = 0; i < NQ; ++i) sm.Minv[NQ * hl + i] = (float)sol[i];
-            } else {
+                for (int r = 0; r < NQ; ++r) sm.Minv[NQ * (hl - NQ) + r] = (float)col[r];
+            } else if (hl == 2 * NQ) {
 #pragma unroll
-                for (int i = 0; i < NQ; ++i) sm.qdd[i] = (float)sol[i];
+                for (int r = 0; r < NQ; ++r) sm.qdd[r] = (float)col[r];
             }
         }
         __syncwarp();

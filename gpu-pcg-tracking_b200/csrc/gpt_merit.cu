@@ -96,6 +96,7 @@ struct MeritWarpSmem {
     float goal[3];
     float M[NUM_ALPHAS][CC];
     float cb[NUM_ALPHAS][NQ];
+    double qdd[NUM_ALPHAS][NQ];
     float defect[NUM_ALPHAS];
     float cost[NUM_ALPHAS];
 };
@@ -160,6 +161,24 @@ __global__ void __launch_bounds__(32 * MERIT_WARPS)
                 }
             }
             __syncwarp();
+            // qdd_a = M_a^{-1} (u_a - c_a): Gauss-Jordan on [M_a | u_a - c_a] by lane groups of 8
+            // (lane 8 g + i holds column i), four step sizes per round
+            for (int rd = 0; rd < rounds; ++rd) {
+                const int a = 4 * rd + (lane >> 3), m = lane & 7;
+                const int aa = (a < n_alpha) ? a : 0;
+                const float al = alpha_of(aa, n_alpha);
+                double col[NQ];
+#pragma unroll
+                for (int r = 0; r < NQ; ++r)
+                    col[r] = (m < NQ) ? 0.5 * ((double)sm.M[aa][NQ * m + r] + (double)sm.M[aa][NQ * r + m])
+                                      : (double)fmaf(al, sm.d[NS + r], sm.x[NS + r]) - (double)sm.cb[aa][r];
+                gj7_group(col, lane & ~7);
+                if (m == NQ && a < n_alpha) {
+#pragma unroll
+                    for (int r = 0; r < NQ; ++r) sm.qdd[a][r] = col[r];
+                }
+            }
+            __syncwarp();
         }
         if (lane < n_alpha) {
             // defect ||x_{k+1} - f(x_k, u_k)||_1 at xu + alpha dz (integrator.cuh:187-219)
@@ -167,12 +186,7 @@ __global__ void __launch_bounds__(32 * MERIT_WARPS)
             const float al = alpha_of(a, n_alpha);
             float dsum = 0.f;
             if (!last) {
-                double L[CC], rhs[NQ], qdd[NQ];
-                chol7_factor(sm.M[a], L);
-#pragma unroll
-                for (int i = 0; i < NQ; ++i)
-                    rhs[i] = (double)fmaf(al, sm.d[NS + i], sm.x[NS + i]) - (double)sm.cb[a][i];
-                chol7_solve(L, rhs, qdd);
+                const double *qdd = sm.qdd[a];
 #pragma unroll
                 for (int i = 0; i < NQ; ++i) {
                     const float q = fmaf(al, sm.d[i], sm.x[i]), qd = fmaf(al, sm.d[NQ + i], sm.x[NQ + i]);

@@ -1115,18 +1115,6 @@ __device__ __forceinline__ void full_times(const double *Ai, const double *Lw, i
         w[q] = a;
     }
 }
-// Reciprocal by two Newton-Raphson steps r <- r + r (1 - x r) from the PTX approximation
-// rcp.approx.ftz.f64 (quadratic convergence: a seed accurate to ~2^-20 reaches FP64 rounding);
-// x is a positive pivot of an SPD factorisation, far from the FP64 range limits
-__device__ __forceinline__ double rcp_newton(double x)
-{
-    double r;
-    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
-    double e = fma(-x, r, 1.0);
-    r = fma(r, e, r);
-    e = fma(-x, r, 1.0);
-    return fma(r, e, r);
-}
 // In-place Gauss-Jordan inverse of an SPD 14x14 matrix held by lane pairs: lane (c, hh) =
 // (lane >> 1, lane & 1), c < 14, holds rows 7 hh .. 7 hh + 6 of column c in a[]; on return the
 // same entries of the inverse.  The pivots are the 2x2 diagonal blocks P = {p, p+1} (no pivoting:
