@@ -82,6 +82,48 @@ __device__ __forceinline__ double rcp_newton(double x)
     return fma(r, e, r);
 }
 
+// FP64 tensor-core MMA (mma.sync m8n8k4, the FP64 shape; tcgen05 has no FP64 kind): d += a b for an
+// 8x4 by 4x8 tile pair.  Fragments: a = A(g, t), b = B(t, g), d = D(g, 2t + {0, 1}), with
+// g = lane >> 2, t = lane & 3.
+__device__ __forceinline__ void mma884_f64(double (&d)[2], double a, double b)
+{
+    asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+        : "+d"(d[0]), "+d"(d[1])
+        : "d"(a), "d"(b));
+}
+// c[I][J] += sum over k < 4 KS of A(8I + g, k) B(k, 8J + g'), one warp: TI x TJ output tiles of 8x8,
+// operands read through the element accessors A(i, k), B(k, j) (which return 0 in the padding)
+template <int TI, int TJ, int KS, class FA, class FB>
+__device__ __forceinline__ void warp_dmma(FA A, FB B, double (&c)[TI][TJ][2], int lane)
+{
+    const int g = lane >> 2, t = lane & 3;
+#pragma unroll
+    for (int kk = 0; kk < KS; ++kk) {
+        const int k = 4 * kk + t;
+        double a[TI], b[TJ];
+#pragma unroll
+        for (int I = 0; I < TI; ++I) a[I] = A(8 * I + g, k);
+#pragma unroll
+        for (int J = 0; J < TJ; ++J) b[J] = B(k, 8 * J + g);
+#pragma unroll
+        for (int I = 0; I < TI; ++I)
+#pragma unroll
+            for (int J = 0; J < TJ; ++J) mma884_f64(c[I][J], a[I], b[J]);
+    }
+}
+// hand each element (i, j, value) of the tiles to st
+template <int TI, int TJ, class F>
+__device__ __forceinline__ void warp_dmma_store(const double (&c)[TI][TJ][2], F st, int lane)
+{
+    const int g = lane >> 2, t = lane & 3;
+#pragma unroll
+    for (int I = 0; I < TI; ++I)
+#pragma unroll
+        for (int J = 0; J < TJ; ++J)
+#pragma unroll
+            for (int e = 0; e < 2; ++e) st(8 * I + g, 8 * J + 2 * t + e, c[I][J][e]);
+}
+
 __device__ __forceinline__ float warp_sum(float v)
 {
 #pragma unroll

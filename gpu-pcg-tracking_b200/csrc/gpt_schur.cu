@@ -358,27 +358,6 @@ __device__ __forceinline__ void warp_inverse64_control(const float *R, double sh
     }
 }
 
-// out (14 x NCOL, col-major) (+)= A (14 x K, col-major) * op(B), FP64 accumulation; A and B may be
-// FP32 or FP64 (FP32 operands are exact in FP64)
-template <int K, int NCOL, bool TRANS_B, bool ACC = false, typename TA, typename TB>
-__device__ __forceinline__ void warp_mm64(const TA *A, const TB *B, int ldb, double *out, int lane)
-{
-    if (lane < 2 * NCOL) {
-        const int col = lane % NCOL, r0 = (lane / NCOL) * 7;
-        double acc[7];
-#pragma unroll
-        for (int i = 0; i < 7; ++i) acc[i] = ACC ? out[r0 + i + NS * col] : 0.0;
-#pragma unroll
-        for (int t = 0; t < K; ++t) {
-            const double bv = (double)(TRANS_B ? B[col + ldb * t] : B[t + ldb * col]);
-#pragma unroll
-            for (int i = 0; i < 7; ++i) acc[i] = fma((double)A[r0 + i + NS * t], bv, acc[i]);
-        }
-#pragma unroll
-        for (int i = 0; i < 7; ++i) out[r0 + i + NS * col] = acc[i];
-    }
-}
-
 // One warp's shared memory: the knot's KKT blocks staged as FP32 (one batch of loads per knot), the
 // FP64 inverses and products
 struct Schur64WarpSmem {
@@ -475,13 +454,30 @@ __global__ void __launch_bounds__(32 * SCHUR_WARPS)
                              k == N - 1 ? Ginv64 + (size_t)G_STRIDE * j : nullptr);
         warp_inverse64_control(sm.Gm1 + SS, rho, sm.Rki, lane, Gi32 + SS, Gi64 + SS);
         __syncwarp();
-        const float *Am = sm.C, *Bm = sm.C + SS;                              // -A, -B
-        warp_mm64<NS, NS, false>(Am, sm.Qki, NS, sm.phi, lane);              // phi = (-A) Qt^{-1}
-        warp_mm64<NC, NC, false>(Bm, sm.Rki, NC, sm.BRi, lane);              // (-B) Rt^{-1}
+        // the products on the FP64 tensor cores, 14x14 (14x7) blocks padded to 16x16 (16x8)
+        const float *Am = sm.C, *Bm = sm.C + SS;  // -A, -B
+        {
+            double cp[2][2][2] = {}, cb[2][1][2] = {};
+            warp_dmma<2, 2, 4>([&](int i, int k) { return (i < NS && k < NS) ? (double)Am[i + NS * k] : 0.0; },
+                               [&](int k, int j) { return (k < NS && j < NS) ? sm.Qki[k + NS * j] : 0.0; }, cp,
+                               lane);  // phi = (-A) Qt^{-1}
+            warp_dmma<2, 1, 2>([&](int i, int k) { return (i < NS && k < NC) ? (double)Bm[i + NS * k] : 0.0; },
+                               [&](int k, int j) { return (k < NC && j < NC) ? sm.Rki[k + NC * j] : 0.0; }, cb,
+                               lane);  // (-B) Rt^{-1}
+            warp_dmma_store(cp, [&](int i, int j, double v) { if (i < NS && j < NS) sm.phi[i + NS * j] = v; }, lane);
+            warp_dmma_store(cb, [&](int i, int j, double v) { if (i < NS && j < NC) sm.BRi[i + NS * j] = v; }, lane);
+        }
         __syncwarp();
-        warp_mm64<NS, NS, true>(sm.phi, Am, NS, sm.theta, lane);             // phi (-A)^T
-        __syncwarp();
-        warp_mm64<NC, NS, true, true>(sm.BRi, Bm, NS, sm.theta, lane);       // + (-B) Rt^{-1} (-B)^T
+        {
+            double ct[2][2][2] = {};
+            warp_dmma<2, 2, 4>([&](int i, int k) { return (i < NS && k < NS) ? sm.phi[i + NS * k] : 0.0; },
+                               [&](int k, int j) { return (k < NS && j < NS) ? (double)Am[j + NS * k] : 0.0; }, ct,
+                               lane);  // phi (-A)^T
+            warp_dmma<2, 2, 2>([&](int i, int k) { return (i < NS && k < NC) ? sm.BRi[i + NS * k] : 0.0; },
+                               [&](int k, int j) { return (k < NC && j < NS) ? (double)Bm[j + NS * k] : 0.0; }, ct,
+                               lane);  // + (-B) Rt^{-1} (-B)^T
+            warp_dmma_store(ct, [&](int i, int j, double v) { if (i < NS && j < NS) sm.theta[i + NS * j] = v; }, lane);
+        }
         if (lane < NS) {
             double a1 = 0.0, a2 = 0.0, a3 = 0.0;
 #pragma unroll
