@@ -1088,9 +1088,9 @@ constexpr int PAIR_THREADS = 128;
 constexpr int PAIR_NWARP = PAIR_THREADS / 32;
 constexpr int PW_STRIDE = SS, PW_INV = 0, PW_LAM = 105, PW_RES = 119, PW_P = 133, PW_V = 147;
 // per factoring warp: the previous inverse factor as a full symmetric matrix (196), the coupling
-// block (196) and the diagonal block A_k (packed lower triangle, 105)
-constexpr int PAIR_FWARP = 2 * SS + 105;
-constexpr int PF_INV = 0, PF_L = SS, PF_A = 2 * SS;
+// block (196), the diagonal block A_k (packed lower triangle, 105) and the product buffer (196)
+constexpr int PAIR_FWARP = 3 * SS + 105;
+constexpr int PF_INV = 0, PF_L = SS, PF_A = 2 * SS, PF_W = 2 * SS + 105;
 
 __host__ __device__ constexpr int pair_smem_doubles(int n)
 {
@@ -1098,23 +1098,6 @@ __host__ __device__ constexpr int pair_smem_doubles(int n)
 }
 size_t pcg_pair_smem_bytes(int n) { return sizeof(double) * (size_t)pair_smem_doubles(n); }
 
-// w[q] = (Ai X)(7 hh + q, c) with X(t, c) = Lw[t + 14 c] (TR: X = Lw^T); Ai a full symmetric
-// 14x14 matrix, column-major, so every shared-memory offset below is a constant from Ai + 7 hh
-template <bool TR>
-__device__ __forceinline__ void full_times(const double *Ai, const double *Lw, int cq, int hh, double (&w)[7])
-{
-    double xc[NS];
-#pragma unroll
-    for (int t = 0; t < NS; ++t) xc[t] = TR ? Lw[cq + NS * t] : Lw[t + NS * cq];
-    const double *Ar = Ai + 7 * hh;
-#pragma unroll
-    for (int q = 0; q < 7; ++q) {
-        double a = 0.0;
-#pragma unroll
-        for (int t = 0; t < NS; ++t) a = fma(Ar[q + NS * t], xc[t], a);
-        w[q] = a;
-    }
-}
 // In-place Gauss-Jordan inverse of an SPD 14x14 matrix held by lane pairs: lane (c, hh) =
 // (lane >> 1, lane & 1), c < 14, holds rows 7 hh .. 7 hh + 6 of column c in a[]; on return the
 // same entries of the inverse.  The pivots are the 2x2 diagonal blocks P = {p, p+1} (no pivoting:
@@ -1151,21 +1134,6 @@ __device__ __forceinline__ void pair_gj_inverse(double (&a)[7], int c, int hh)
             const double upd = fma(-u0[q], n0, fma(-u1[q], n1, cp ? 0.0 : a[q]));
             a[q] = (i == p) ? n0 : ((i == p + 1) ? n1 : upd);
         }
-    }
-}
-// d[a] = (Y W)(a, c) with Y(a, t) = Lw[a + 14 t] (TR: Lw[t + 14 a]); both lanes of a pair get the sum
-template <bool TR>
-__device__ __forceinline__ void lw_times(const double *Lw, int hh, const double (&w)[7], double (&d)[NS])
-{
-#pragma unroll
-    for (int a = 0; a < NS; ++a) {
-        double acc = 0.0;
-#pragma unroll
-        for (int q = 0; q < 7; ++q) {
-            const int t = 7 * hh + q;
-            acc = fma(TR ? Lw[t + NS * a] : Lw[a + NS * t], w[q], acc);
-        }
-        d[a] = acc + __shfl_xor_sync(0xffffffffu, acc, 1);
     }
 }
 // row r of a 14x14 block times v: lane (r, hh) sums columns 7 hh .. 7 hh + 6, the pair adds up
@@ -1251,10 +1219,20 @@ __global__ void __launch_bounds__(PAIR_THREADS, 4)
     const int c = lane >> 1, hh = lane & 1;
     const bool cval = c < NS;
     const int cq = cval ? c : NS - 1;
-    // lane (c, hh)'s entries of a diagonal block minus the Schur update d (column c, all rows)
-    auto load_block = [&](const double *Apk, const double (&d)[NS], double (&a)[7]) {
-#pragma unroll
-        for (int q = 0; q < 7; ++q) a[q] = Apk[tri_lo(7 * hh + q, cq)] - (hh ? d[7 + q] : d[q]);
+    // Wb <- L F L^T (F full symmetric, L column-major, both 14x14 in shared memory) on the FP64 tensor
+    // cores: W = F L^T, then L W; every lane of the warp takes part
+    auto schur_update = [&](const double *F, const double *L, double *Wb) {
+        double cw[2][2][2] = {};
+        warp_dmma<2, 2, 4>([&](int i, int k) { return (i < NS && k < NS) ? F[i + NS * k] : 0.0; },
+                           [&](int k, int j) { return (k < NS && j < NS) ? L[j + NS * k] : 0.0; }, cw, lane);
+        warp_dmma_store(cw, [&](int i, int j, double v) { if (i < NS && j < NS) Wb[i + NS * j] = v; }, lane);
+        __syncwarp();
+        double cd[2][2][2] = {};
+        warp_dmma<2, 2, 4>([&](int i, int k) { return (i < NS && k < NS) ? L[i + NS * k] : 0.0; },
+                           [&](int k, int j) { return (k < NS && j < NS) ? Wb[k + NS * j] : 0.0; }, cd, lane);
+        __syncwarp();
+        warp_dmma_store(cd, [&](int i, int j, double v) { if (i < NS && j < NS) Wb[i + NS * j] = v; }, lane);
+        __syncwarp();
     };
     // an inverse factor: full matrix into shared memory (next step's products), packed lower
     // triangle into the workspace (the solve)
@@ -1305,16 +1283,12 @@ __global__ void __launch_bounds__(PAIR_THREADS, 4)
                 warp_fetch<ST, 4>(Sb + (size_t)(k + dir) * ks + PK_DIAG, 105, lane, pd);
                 warp_fetch<ST, 7>(Sb + (size_t)(k + dir + lofs) * ks, SS, lane, pl);
             }
-            double d[NS];
-#pragma unroll
-            for (int a = 0; a < NS; ++a) d[a] = 0.0;
-            if (st > 0) {
-                double w[7];
-                full_times<true>(Fi, Lw, cq, hh, w);
-                lw_times<false>(Lw, hh, w, d);
-            }
+            double *Wb = fw + PF_W;
+            if (st > 0) schur_update(Fi, Lw, Wb);
             double a[7];
-            load_block(Ap, d, a);
+#pragma unroll
+            for (int q = 0; q < 7; ++q)
+                a[q] = Ap[tri_lo(7 * hh + q, cq)] - (st > 0 ? Wb[7 * hh + q + NS * cq] : 0.0);
             if (top && k == m) {
                 if (cval) {
 #pragma unroll
@@ -1342,10 +1316,9 @@ __global__ void __launch_bounds__(PAIR_THREADS, 4)
     __syncthreads();
     // ---- middle knot: T_m = D_m - L_{m+1}^T U_{m+1}^{-1} L_{m+1}, inverted (warp 1)
     if (warp == 1) {
-        double d[NS];
-#pragma unroll
-        for (int a = 0; a < NS; ++a) d[a] = 0.0;
-        if (m + 1 <= n - 1) {
+        double *Wb = fw1 + PF_W;
+        const bool upd = m + 1 <= n - 1;
+        if (upd) {
             double *Fi = fw1 + PF_INV, *Lw = fw1 + PF_L;
             double pl[7];
             warp_fetch<ST, 7>(Sb + (size_t)(m + 1) * ks, SS, lane, pl);
@@ -1355,13 +1328,11 @@ __global__ void __launch_bounds__(PAIR_THREADS, 4)
                 if (e < SS) Lw[(e / NS) + NS * (e % NS)] = pl[i];  // transposed, as in the loop
             }
             __syncwarp();
-            double w[7];
-            full_times<true>(Fi, Lw, cq, hh, w);
-            lw_times<false>(Lw, hh, w, d);
+            schur_update(Fi, Lw, Wb);
         }
         double a[7];
 #pragma unroll
-        for (int q = 0; q < 7; ++q) a[q] = dmf[7 * hh + q + NS * cq] - (hh ? d[7 + q] : d[q]);
+        for (int q = 0; q < 7; ++q) a[q] = dmf[7 * hh + q + NS * cq] - (upd ? Wb[7 * hh + q + NS * cq] : 0.0);
         pair_gj_inverse(a, c, hh);
         keep_inv(nullptr, a, m);
     }
