@@ -18,17 +18,24 @@ constexpr int DZ_WARPS = 4;
 
 // dz from lambda (FP32 or, when lambda64 is given, FP64).  The right-hand sides
 // q_k - lambda_k - (-A_k)^T lambda_{k+1} and r_k - (-B_k)^T lambda_{k+1} cancel
-// heavily, so they are accumulated in FP64 before the FP32-stored inverses apply.
+// heavily, so they are accumulated in FP64 before the inverses apply.  Every input of a
+// knot is loaded in one batch (the kernel is bound by load latency) and staged in shared memory.
+struct DzWarpSmem {
+    double gi[G_STRIDE];  // (Q + rho I)^{-1}, (R + rho I)^{-1}
+    double lv[2 * NS];    // lambda_k, lambda_{k+1}
+    double s[NX];
+    float cm[C_STRIDE];   // -A_k, -B_k
+    float gv[NX];
+};
+
 __global__ void __launch_bounds__(32 * DZ_WARPS)
     dz_kernel(BatchView bv, const float *__restrict__ Ginv, const double *__restrict__ Ginv64,
               const float *__restrict__ Cm, const float *__restrict__ g, const float *__restrict__ lambda,
               const double *__restrict__ lambda64, float *__restrict__ dz)
 {
-    __shared__ double s_all[DZ_WARPS][NX];
-    __shared__ double l_all[DZ_WARPS][2 * NS];
+    __shared__ DzWarpSmem sm_all[DZ_WARPS];
     const int lane = threadIdx.x & 31;
-    double *s = s_all[threadIdx.x >> 5];
-    double *lv = l_all[threadIdx.x >> 5];
+    DzWarpSmem &sm = sm_all[threadIdx.x >> 5];
     const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nw = (gridDim.x * blockDim.x) >> 5;
     for (int j = gw; j < bv.total_knots; j += nw) {
@@ -38,38 +45,66 @@ __global__ void __launch_bounds__(32 * DZ_WARPS)
         const bool last = (k == N - 1);
         const float *Cj = Cm + (size_t)C_STRIDE * j;
         const int nl = last ? NS : 2 * NS;
-        if (lane < nl) lv[lane] = lambda64 ? lambda64[(size_t)NS * j + lane] : (double)lambda[(size_t)NS * j + lane];
+        // ---- all loads of the knot, then the shared-memory stores
+        constexpr int NGI = (G_STRIDE + 31) / 32, NCM = (C_STRIDE + 31) / 32;
+        const int ngi = last ? SS : G_STRIDE;  // the last knot's block has no R part (buffers of 245N - 49)
+        double gi[NGI];
+        float cm[NCM];
+#pragma unroll
+        for (int i = 0; i < NGI; ++i) {
+            const int e = lane + 32 * i;
+            gi[i] = 0.0;
+            if (e < ngi) gi[i] = Ginv64 ? Ginv64[(size_t)G_STRIDE * j + e] : (double)Ginv[(size_t)G_STRIDE * j + e];
+        }
+#pragma unroll
+        for (int i = 0; i < NCM; ++i) {
+            const int e = lane + 32 * i;
+            cm[i] = (!last && e < C_STRIDE) ? Cj[e] : 0.f;
+        }
+        double lvv = 0.0;
+        if (lane < nl) lvv = lambda64 ? lambda64[(size_t)NS * j + lane] : (double)lambda[(size_t)NS * j + lane];
+        float gvv = 0.f;
+        if (lane < NX && (lane < NS || !last)) gvv = g[(size_t)NX * j + lane];
+#pragma unroll
+        for (int i = 0; i < NGI; ++i) {
+            const int e = lane + 32 * i;
+            if (e < G_STRIDE) sm.gi[e] = gi[i];
+        }
+#pragma unroll
+        for (int i = 0; i < NCM; ++i) {
+            const int e = lane + 32 * i;
+            if (e < C_STRIDE) sm.cm[e] = cm[i];
+        }
+        if (lane < 2 * NS) sm.lv[lane] = lvv;
+        if (lane < NX) sm.gv[lane] = gvv;
         __syncwarp();
         if (lane < NS) {
             // q_k - (lambda_k + (-A_k)^T lambda_{k+1})
             double a = 0.0;
             if (!last) {
 #pragma unroll
-                for (int t = 0; t < NS; ++t) a = fma((double)Cj[lane * NS + t], lv[NS + t], a);
+                for (int t = 0; t < NS; ++t) a = fma((double)sm.cm[lane * NS + t], sm.lv[NS + t], a);
             }
-            s[lane] = (double)g[(size_t)NX * j + lane] - (lv[lane] + a);
+            sm.s[lane] = (double)sm.gv[lane] - (sm.lv[lane] + a);
         } else if (lane < NX && !last) {
             // r_k - (-B_k)^T lambda_{k+1}
             const int i = lane - NS;
             double a = 0.0;
 #pragma unroll
-            for (int t = 0; t < NS; ++t) a = fma((double)Cj[SS + i * NS + t], lv[NS + t], a);
-            s[lane] = (double)g[(size_t)NX * j + lane] - a;
+            for (int t = 0; t < NS; ++t) a = fma((double)sm.cm[SS + i * NS + t], sm.lv[NS + t], a);
+            sm.s[lane] = (double)sm.gv[lane] - a;
         }
         __syncwarp();
-        const float *Gi = Ginv + (size_t)G_STRIDE * j;
-        const double *Gi64 = Ginv64 ? Ginv64 + (size_t)G_STRIDE * j : nullptr;
         if (lane < NS) {
             double a = 0.0;
 #pragma unroll
-            for (int t = 0; t < NS; ++t) a = fma(Gi64 ? Gi64[lane + NS * t] : (double)Gi[lane + NS * t], s[t], a);
+            for (int t = 0; t < NS; ++t) a = fma(sm.gi[lane + NS * t], sm.s[t], a);
             dz[(size_t)NX * j + lane] = (float)a;
         } else if (lane < NX && !last) {
             const int i = lane - NS;
             double a = 0.0;
 #pragma unroll
-            for (int t = 0; t < NC; ++t)
-                a = fma(Gi64 ? Gi64[SS + i + NC * t] : (double)Gi[SS + i + NC * t], s[NS + t], a);
+            for (int t = 0; t < NC; ++t) a = fma(sm.gi[SS + i + NC * t], sm.s[NS + t], a);
             dz[(size_t)NX * j + lane] = (float)a;
         }
         __syncwarp();
