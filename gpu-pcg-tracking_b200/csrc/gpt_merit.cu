@@ -132,6 +132,7 @@ struct MeritWarpSmem {
     float M[NUM_ALPHAS][CC];
     float cb[NUM_ALPHAS][NQ];
     double qdd[NUM_ALPHAS][NQ];
+    JointTrig trig[NUM_ALPHAS];  // sin, cos of q + alpha dq per step size
     float defect[NUM_ALPHAS];
     float cost[NUM_ALPHAS];
 };
@@ -167,6 +168,12 @@ __global__ void __launch_bounds__(32 * MERIT_WARPS)
         }
         if (lane < 3) sm.goal[lane] = goal[(size_t)6 * j + lane];
         __syncwarp();
+        // sin, cos of every joint at every step size, once (lane = (step size, joint))
+        for (int t = lane; t < n_alpha * NQ; t += 32) {
+            const int a = t / NQ, i = t - NQ * a;
+            sincosf(fmaf(alpha_of(a, n_alpha), sm.d[i], sm.x[i]), &sm.trig[a].s[i], &sm.trig[a].c[i]);
+        }
+        __syncwarp();
 
         if (!last) {
             // mass-matrix columns (m < 7) and bias force (m == 7) per step size
@@ -175,15 +182,13 @@ __global__ void __launch_bounds__(32 * MERIT_WARPS)
                 const int a = 4 * rd + (lane >> 3), m = lane & 7;
                 const int aa = (a < n_alpha) ? a : 0;
                 const float al = alpha_of(aa, n_alpha);
-                float q[NQ], qd[NQ], qdd[NQ], tau[NQ];
+                float qd[NQ], qdd[NQ], tau[NQ];
 #pragma unroll
                 for (int i = 0; i < NQ; ++i) {
-                    q[i] = fmaf(al, sm.d[i], sm.x[i]);
                     qd[i] = (m == 7) ? fmaf(al, sm.d[NQ + i], sm.x[NQ + i]) : 0.f;
                     qdd[i] = (m == i) ? 1.f : 0.f;
                 }
-                JointTrig t;
-                joint_trig(q, t);
+                const JointTrig t = sm.trig[aa];
                 rnea<false>(t, qd, qdd, -1, -1, tau, nullptr);
                 if (a < n_alpha) {
                     if (m < 7) {
@@ -248,11 +253,10 @@ __global__ void __launch_bounds__(32 * MERIT_WARPS)
             // tracking cost (iiwa_eepos_plant.cuh:240-290)
             const int a = lane - 16;
             const float al = alpha_of(a, n_alpha);
-            float q[NQ], p[3];
+            float p[3];
             float J = 0.f;
 #pragma unroll
             for (int i = 0; i < NQ; ++i) {
-                q[i] = fmaf(al, sm.d[i], sm.x[i]);
                 const float qd = fmaf(al, sm.d[NQ + i], sm.x[NQ + i]);
                 J += 0.5f * (P.qd_cost * qd * qd);
             }
@@ -263,8 +267,7 @@ __global__ void __launch_bounds__(32 * MERIT_WARPS)
                     J += 0.5f * (P.r_cost * u * u);
                 }
             }
-            JointTrig t;
-            joint_trig(q, t);
+            const JointTrig t = sm.trig[a];
             fk_lane<false>(t, p, nullptr);
 #pragma unroll
             for (int d = 0; d < 3; ++d) {
