@@ -32,6 +32,7 @@ struct KktWarpSmem {
     float ee[2][3];
     float J[2][21];
     float qv[2][NS];
+    JointTrig trig;  // sin, cos of q_k, computed once per knot
 };
 
 constexpr int KKT_WARPS = 4;
@@ -75,9 +76,9 @@ __global__ void __launch_bounds__(32 * KKT_WARPS) kkt_kernel(BatchView bv, Probl
         }
         if (hl < 12) sm.goal[hl] = goal[(size_t)6 * jj + hl];
         __syncwarp();
-
-        JointTrig trig;
-        joint_trig(sm.x, trig);
+        if (hl < NQ) sincosf(sm.x[hl], &sm.trig.s[hl], &sm.trig.c[hl]);
+        __syncwarp();
+        const JointTrig trig = sm.trig;
 
         // ---- mass-matrix columns (lanes 0..6) and bias force (lane 7)
         {
