@@ -591,7 +591,7 @@ static gpt_status enqueue_iteration(gpt_handle *h, const SqpPlan &pl, const floa
     {
         PhaseTimer t(h, s, GPT_PHASE_SCHUR);
         if (f64)
-            GPT_CUDA(launch_schur64(bv, h->G, h->C, h->g, h->c, h->S64, h->gamma64, h->Ginv, h->Ginv64, ns, s));
+            GPT_CUDA(launch_schur64(bv, h->G, h->C, h->g, h->c, h->S64, h->gamma64, nullptr, h->Ginv64, ns, s));
         else
             GPT_CUDA(launch_schur(1, bv, 0.f, h->G, h->C, h->g, h->c, h->S, nullptr, h->gamma, h->Ginv, h->Ginv64,
                                   nullptr, SP.pcg_precond == 0 ? 1 : 0, ns, s));
@@ -903,7 +903,7 @@ gpt_status gpt_sqp_adjoint(gpt_handle *h, uint32_t B, const uint32_t *h_N, const
     // ---- the step at xu: K [dz; lambda] = [g; c]
     GPT_CUDA(launch_kkt(bv, P, d_xu, d_goal, h->xs, h->G, h->C, h->g, h->c, ns, s));
     if (f64)
-        GPT_CUDA(launch_schur64(bv, h->G, h->C, h->g, h->c, h->S64, h->gamma64, h->Ginv, h->Ginv64, ns, s));
+        GPT_CUDA(launch_schur64(bv, h->G, h->C, h->g, h->c, h->S64, h->gamma64, nullptr, h->Ginv64, ns, s));
     else
         GPT_CUDA(launch_schur(1, bv, 0.f, h->G, h->C, h->g, h->c, h->S, nullptr, h->gamma, h->Ginv, h->Ginv64,
                               nullptr, SP.pcg_precond == 0 ? 1 : 0, ns, s));
@@ -919,7 +919,7 @@ gpt_status gpt_sqp_adjoint(gpt_handle *h, uint32_t B, const uint32_t *h_N, const
     GPT_CUDA(launch_axpy(nz, -1.f, d_grad_xu_next, nullptr, h->adj_h, ns, s));
     GPT_CUDA(cudaMemsetAsync(h->adj_zero, 0, sizeof(float) * NS * T, s));
     if (f64)
-        GPT_CUDA(launch_schur64(bv, h->G, h->C, h->adj_h, h->adj_zero, h->S64, h->adj_gamma64, h->Ginv, h->Ginv64,
+        GPT_CUDA(launch_schur64(bv, h->G, h->C, h->adj_h, h->adj_zero, h->S64, h->adj_gamma64, nullptr, h->Ginv64,
                                 ns, s));
     else
         GPT_CUDA(launch_schur(1, bv, 0.f, h->G, h->C, h->adj_h, h->adj_zero, h->S, nullptr, h->adj_gamma, h->Ginv,

@@ -53,8 +53,8 @@ cudaError_t launch_accept(const BatchView &bv, int mode, const SolverParams &SP,
                           const float *dz, float *xu, float *merits_out, uint32_t *active_count, int num_sms,
                           cudaStream_t s);
 cudaError_t launch_init(const BatchView &bv, const float *xu, float *xs, int num_sms, cudaStream_t s);
-// FP64 Schur complement for the cyclic-reduction PCG: packed rows (PK64 doubles per knot), gamma
-// (FP64), the inverses (Ginv FP32 and Ginv64); rho from bv.st
+// FP64 Schur complement for the exact-preconditioner PCG: packed rows (PK64 doubles per knot), gamma
+// (FP64), the inverses (Ginv64; Ginv FP32 too when non-null); rho from bv.st
 cudaError_t launch_schur64(const BatchView &bv, const float *G, const float *C, const float *g, const float *c,
                            double *S64, double *gamma64, float *Ginv, double *Ginv64, int num_sms, cudaStream_t s);
 // adjoint of the SQP step (gpt_adjoint.cu): per-knot goal gradients, per-instance weight gradients;

@@ -392,7 +392,7 @@ __global__ void __launch_bounds__(32 * SCHUR_WARPS)
             for (int e = lane; e < SS; e += 32) sm.Gk[e] = Q0[e];
             if (lane < NS) sm.qk[lane] = (double)g[(size_t)NX * j + lane];
             __syncwarp();
-            warp_inverse64_state(sm.Gk, rho, sm.Qki, lane, N == 1 ? Ginv + (size_t)G_STRIDE * j : nullptr,
+            warp_inverse64_state(sm.Gk, rho, sm.Qki, lane, (N == 1 && Ginv) ? Ginv + (size_t)G_STRIDE * j : nullptr,
                                  N == 1 ? Ginv64 + (size_t)G_STRIDE * j : nullptr);
             __syncwarp();
             if (lane < NS) {
@@ -447,12 +447,12 @@ __global__ void __launch_bounds__(32 * SCHUR_WARPS)
             }
         }
         __syncwarp();
-        float *Gi32 = Ginv + (size_t)G_STRIDE * (j - 1);
+        float *Gi32 = Ginv ? Ginv + (size_t)G_STRIDE * (j - 1) : nullptr;
         double *Gi64 = Ginv64 + (size_t)G_STRIDE * (j - 1);
         warp_inverse64_state(sm.Gm1, rho, sm.Qki, lane, Gi32, Gi64);
-        warp_inverse64_state(sm.Gk, rho, sm.Qkp1i, lane, k == N - 1 ? Ginv + (size_t)G_STRIDE * j : nullptr,
+        warp_inverse64_state(sm.Gk, rho, sm.Qkp1i, lane, (k == N - 1 && Ginv) ? Ginv + (size_t)G_STRIDE * j : nullptr,
                              k == N - 1 ? Ginv64 + (size_t)G_STRIDE * j : nullptr);
-        warp_inverse64_control(sm.Gm1 + SS, rho, sm.Rki, lane, Gi32 + SS, Gi64 + SS);
+        warp_inverse64_control(sm.Gm1 + SS, rho, sm.Rki, lane, Gi32 ? Gi32 + SS : nullptr, Gi64 + SS);
         __syncwarp();
         // the products on the FP64 tensor cores, 14x14 (14x7) blocks padded to 16x16 (16x8)
         const float *Am = sm.C, *Bm = sm.C + SS;  // -A, -B
