@@ -986,8 +986,11 @@ __global__ void __launch_bounds__(PCG_THREADS, 1)
             replaced = true;
         }
         if (exit_mode == 0) {
-            // ||r|| <= tol ||gamma||: tested before preconditioning and confirmed on the true
-            // residual, so the exact chunk solve runs only while the iteration continues
+            // ||r|| <= tol ||gamma||: tested before preconditioning, so the exact chunk solve runs
+            // only while the iteration continues, and confirmed on the true residual from the second
+            // iteration on.  After the first, r = r0 - alpha S p with r0 the true residual and S p one
+            // FP64 product: it equals gamma - S lambda up to FP64 rounding, ~eps64 cond(S) relative
+            // (~3e-8 at cond(S) = 2e7), far below any usable tolerance.
             double d0[1] = {0.0};
 #pragma unroll
             for (int j = 0; j < PCG_KPT; ++j)
@@ -998,7 +1001,7 @@ __global__ void __launch_bounds__(PCG_THREADS, 1)
                 bad = true;
                 break;
             }
-            if (converged(0.0, d0[0]) && !replaced) {
+            if (converged(0.0, d0[0]) && !replaced && it > 1) {
                 true_residual(false);
                 d0[0] = 0.0;
 #pragma unroll
@@ -1549,13 +1552,15 @@ __global__ void __launch_bounds__(PAIR_THREADS, 4)
             replaced = true;
         }
         if (exit_mode == 0) {
-            // ||r|| <= tol ||gamma||: tested before preconditioning and confirmed on the true residual
+            // ||r|| <= tol ||gamma||: tested before preconditioning; confirmed on the true residual from
+            // the second iteration on (after the first, r = r0 - alpha S p equals gamma - S lambda up to
+            // FP64 rounding, ~eps64 cond(S) relative, as in pcg_chain_kernel)
             double r2 = sum_res2();
             if (!isfinite(r2)) {
                 bad = true;
                 break;
             }
-            if (converged(0.0, r2) && !replaced) {
+            if (converged(0.0, r2) && !replaced && it > 1) {
                 true_residual();
                 r2 = sum_res2();
             }
