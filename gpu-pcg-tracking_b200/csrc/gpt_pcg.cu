@@ -1355,6 +1355,19 @@ __global__ void __launch_bounds__(PAIR_THREADS, 4)
 #pragma unroll
         for (int q = 0; q < 7; ++q) v[q] = rv ? (double)__ldg(p + (tr ? 7 * hh + q + NS * r : r + NS * (7 * hh + q))) : 0.0;
     };
+    // L2 prefetch of a sweep step's blocks (the packed inverse factor of knot kf, 840 B, and the left
+    // block of row kl) PF_AHEAD steps before they are loaded; every address lies inside its block
+    constexpr int PF_AHEAD = 4;
+    constexpr int LEFT_LINES = (SS * (int)sizeof(ST) + 127) / 128;
+    auto l2_prefetch = [&](int kf, int kl) {
+        if (lane < 7) {
+            if (kf >= 0 && kf < n)
+                asm volatile("prefetch.global.L2 [%0];" ::"l"(reinterpret_cast<const char *>(wsb + (size_t)kf * PW_STRIDE) + 128 * lane));
+        } else if (lane < 7 + LEFT_LINES) {
+            if (kl >= 1 && kl < n)
+                asm volatile("prefetch.global.L2 [%0];" ::"l"(reinterpret_cast<const char *>(Sb + (size_t)kl * ks) + 128 * (lane - 7)));
+        }
+    };
     auto solve = [&]() {
         if (warp == 0 && m > 0) {
             double di[7], li[7];
@@ -1371,6 +1384,7 @@ __global__ void __launch_bounds__(PAIR_THREADS, 4)
                     ld_inv(k + 1, di);
                     ld_left(k + 2, false, li);
                 }
+                l2_prefetch(k + PF_AHEAD < m ? k + PF_AHEAD : -1, k + PF_AHEAD + 1);
                 const double a = pair_dot7(dc, xv + NS * k, hh);
                 if (hh == 0 && rv) tv[NS * k + r] = a;
                 __syncwarp();
@@ -1394,6 +1408,7 @@ __global__ void __launch_bounds__(PAIR_THREADS, 4)
                         ld_inv(k - 1, di);
                         ld_left(k - 1, true, li);
                     }
+                    l2_prefetch(k - PF_AHEAD > m ? k - PF_AHEAD : -1, k - PF_AHEAD > m ? k - PF_AHEAD : -1);
                     const double a = pair_dot7(dc, xv + NS * k, hh);
                     if (hh == 0 && rv) tv[NS * k + r] = a;
                     __syncwarp();
@@ -1435,6 +1450,7 @@ __global__ void __launch_bounds__(PAIR_THREADS, 4)
                     ld_inv(k - 1, di);
                     ld_left(k, true, li);
                 }
+                l2_prefetch(k - PF_AHEAD, k - PF_AHEAD + 1);
                 const double s = pair_dot7(lc, xv + NS * (k + 1), hh);
                 if (hh == 0 && rv) sc[r] = s;
                 __syncwarp();
@@ -1458,6 +1474,7 @@ __global__ void __launch_bounds__(PAIR_THREADS, 4)
                     ld_inv(k + 1, di);
                     ld_left(k + 1, false, li);
                 }
+                l2_prefetch(k + PF_AHEAD, k + PF_AHEAD);
                 const double s = pair_dot7(lc, xv + NS * (k - 1), hh);
                 if (hh == 0 && rv) sc[r] = s;
                 __syncwarp();
