@@ -1558,9 +1558,12 @@ __global__ void __launch_bounds__(PAIR_THREADS, 4)
             bad = true;
             break;
         }
+        double r2acc = 0.0;
         for (int e = tid; e < nv; e += PAIR_THREADS) {
             wsv(PW_LAM, e) = fma(alpha, xv[e], wsv(PW_LAM, e));
-            wsv(PW_RES, e) = fma(-alpha, wsv(PW_V, e), wsv(PW_RES, e));
+            const double rn = fma(-alpha, wsv(PW_V, e), wsv(PW_RES, e));
+            wsv(PW_RES, e) = rn;
+            r2acc += rn * rn;
         }
         ++it;
         bool replaced = false;
@@ -1572,7 +1575,14 @@ __global__ void __launch_bounds__(PAIR_THREADS, 4)
             // ||r|| <= tol ||gamma||: tested before preconditioning; confirmed on the true residual from
             // the second iteration on (after the first, r = r0 - alpha S p equals gamma - S lambda up to
             // FP64 rounding, ~eps64 cond(S) relative, as in pcg_chain_kernel)
-            double r2 = sum_res2();
+            double r2;
+            if (replaced) {
+                r2 = sum_res2();
+            } else {
+                double t1[1] = {r2acc};  // the update pass's sum, in sum_res2's order
+                block_sum(t1, 1);
+                r2 = t1[0];
+            }
             if (!isfinite(r2)) {
                 bad = true;
                 break;
