@@ -34,6 +34,7 @@ EXPORTED = [
     "gpt_form_kkt", "gpt_form_schur", "gpt_form_schur_csc", "gpt_prep_csr", "gpt_pcg", "gpt_compute_dz",
     "gpt_compute_merit", "gpt_ls_compute_merit", "gpt_set_profiling", "gpt_get_phase_stats",
     "gpt_ls_compute_merit_noalloc", "gpt_sqp_adjoint", "gpt_set_cost_weights", "gpt_autotune",
+    "gpt_default_track_config", "gpt_track", "gpt_track_batched", "gpt_simulate",
 ]
 PHASES = ["init", "kkt", "schur", "pcg", "dz", "merit", "accept"]
 
@@ -59,6 +60,23 @@ class SqpStats(C.Structure):
     _fields_ = [("sqp_iters", C.c_uint32), ("exit_flags", C.c_uint32), ("pcg_iters_total", C.c_uint32),
                 ("pcg_maxiter_count", C.c_uint32), ("ls_fail_count", C.c_uint32), ("merit_initial", C.c_float),
                 ("merit_final", C.c_float), ("rho_final", C.c_float)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class TrackConfig(C.Structure):
+    """gpt_track_config (include/gpt.h)."""
+    _fields_ = [("sim_period_us", C.c_float), ("sim_step", C.c_float), ("shift_threshold", C.c_float),
+                ("max_control_updates", C.c_uint32), ("jitter_solves", C.c_uint32), ("rho_reset", C.c_float)]
+
+
+class TrackStats(C.Structure):
+    """gpt_track_stats (include/gpt.h)."""
+    _fields_ = [("control_updates", C.c_uint32), ("shifts", C.c_uint32), ("sqp_iters_total", C.c_uint32),
+                ("pcg_iters_total", C.c_uint32), ("ls_fail_total", C.c_uint32), ("pcg_maxiter_total", C.c_uint32),
+                ("rho_exits", C.c_uint32), ("nonfinite", C.c_uint32), ("tracking_error_mean", C.c_float),
+                ("final_tracking_error", C.c_float), ("rho_final", C.c_float)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -121,6 +139,10 @@ def _declare(L):
         "gpt_sqp_adjoint": ([vp, u32, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp], C.c_int),
         "gpt_set_cost_weights": ([vp, f32, f32, f32], C.c_int),
         "gpt_autotune": ([vp, u32, vp, vp, vp, vp, vp, P(u32), vp], C.c_int),
+        "gpt_default_track_config": ([P(TrackConfig)], None),
+        "gpt_track": ([vp, u32, u32, vp, vp, vp, P(TrackConfig), vp, vp, u32, P(TrackStats), vp], C.c_int),
+        "gpt_track_batched": ([vp, u32, vp, vp, vp, vp, vp, P(TrackConfig), vp, vp, u32, vp, vp], C.c_int),
+        "gpt_simulate": ([vp, u32, vp, vp, C.c_double, C.c_double, f32, vp], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -147,6 +169,14 @@ def default_solver_config(**kw) -> SolverConfig:
     for k, v in kw.items():
         setattr(sc, k, v)
     return sc
+
+
+def default_track_config(**kw) -> TrackConfig:
+    tc = TrackConfig()
+    lib().gpt_default_track_config(C.byref(tc))
+    for k, v in kw.items():
+        setattr(tc, k, v)
+    return tc
 
 
 NOALLOC_MAX_KNOTS = 512  # GPT_NOALLOC_MAX_KNOTS
@@ -287,6 +317,47 @@ class Solver:
                                      C.cast(rr, C.c_void_p), _ptr(grad_xu_next), _ptr(xu_next), _ptr(out["goal"]),
                                      _ptr(out["qd"]), _ptr(out["r"]), _ptr(out["q_ee"]), _stream(stream)))
         return out
+
+    # ---- the MPC tracking loop (toplevel.cuh:507-796) ----
+    def track(self, knot_points: int, eePos_traj, xu_traj, xs, config: Optional[TrackConfig] = None,
+              errors=None, sqp_iters_log=None, stream=None):
+        """gpt_track: receding-horizon tracking of one trajectory (rows of 6 / 21 floats); xs is the
+        plant state, updated in place.  Returns (per-shift tracking errors, stats dict)."""
+        import torch
+        S = eePos_traj.numel() // 6
+        if errors is None:
+            errors = torch.zeros(S, device=xs.device)
+        st = TrackStats()
+        cap = 0 if sqp_iters_log is None else sqp_iters_log.numel()
+        _check(lib().gpt_track(self._h, knot_points, S, _ptr(eePos_traj), _ptr(xu_traj), _ptr(xs),
+                               None if config is None else C.byref(config), _ptr(errors), _ptr(sqp_iters_log), cap,
+                               C.byref(st), _stream(stream)))
+        d = st.as_dict()
+        return errors[:st.shifts], d
+
+    def track_batched(self, knot_points: Sequence[int], traj_steps: Sequence[int], eePos_traj, xu_traj, xs,
+                      config: Optional[TrackConfig] = None, errors=None, sqp_iters_log=None, log_capacity=0,
+                      stream=None):
+        """gpt_track_batched: many tracking runs; instance b owns trajectory rows
+        sum(traj_steps[:b]) .. + traj_steps[b]-1.  Returns (errors tensor, list of stats dicts)."""
+        import torch
+        B = len(knot_points)
+        Ns = (C.c_uint32 * B)(*knot_points)
+        Ss = (C.c_uint32 * B)(*traj_steps)
+        if errors is None:
+            errors = torch.zeros(int(sum(traj_steps)), device=xs.device)
+        sts = (TrackStats * B)()
+        _check(lib().gpt_track_batched(self._h, B, C.cast(Ns, C.c_void_p), C.cast(Ss, C.c_void_p), _ptr(eePos_traj),
+                                       _ptr(xu_traj), _ptr(xs), None if config is None else C.byref(config),
+                                       _ptr(errors), _ptr(sqp_iters_log), log_capacity, C.cast(sts, C.c_void_p),
+                                       _stream(stream)))
+        return errors, [s.as_dict() for s in sts]
+
+    def simulate(self, knot_points: int, xs, xu, time_offset_us: float, sim_time_us: float, sim_step: float = 2e-4,
+                 stream=None):
+        """gpt_simulate (simple_simulate, integrator.cuh:365-398): advances xs in place."""
+        _check(lib().gpt_simulate(self._h, knot_points, _ptr(xs), _ptr(xu), time_offset_us, sim_time_us, sim_step,
+                                  _stream(stream)))
 
     # ---- the reference's kernels, one instance ----
     def form_kkt(self, N, xu, eePos, xs, G, Cm, g, c, stream=None):

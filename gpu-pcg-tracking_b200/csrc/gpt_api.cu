@@ -72,6 +72,14 @@ struct gpt_handle {
     // device-side while loop, capture streams and the instantiated graphs per batch shape
     float *gxu = nullptr, *glam = nullptr, *ggoal = nullptr;
     uint32_t *d_iter = nullptr;
+    // tracking loop: the previous solution (plant controls), trajectory row offsets, the shared
+    // update clock, per-instance totals (the working xu, lambda and goal are gxu, glam, ggoal)
+    float *trk_xu_old = nullptr;
+    int *trk_rows = nullptr;
+    TrackClock *trk_clk = nullptr;
+    TrackInst *trk_inst = nullptr;
+    int *h_trk_rows = nullptr;
+    TrackInst *h_trk_inst = nullptr;
     cudaStream_t cap_stream = nullptr, body_stream = nullptr;
     std::vector<GraphEntry> graphs;
     // autotuned PCG cluster size per batch shape (gpt_autotune); used when pcg_cluster_size is 0
@@ -284,6 +292,10 @@ gpt_status gpt_create(const gpt_problem_config *pc, const gpt_solver_config *sc,
     ALLOC(glam, NS * T);
     ALLOC(ggoal, 6 * T);
     ALLOC(d_iter, 1);
+    ALLOC(trk_xu_old, NX * T);
+    ALLOC(trk_rows, B + 1);
+    ALLOC(trk_clk, 1);
+    ALLOC(trk_inst, B);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->cap_stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->body_stream, cudaStreamNonBlocking);
 #undef ALLOC
@@ -291,6 +303,8 @@ gpt_status gpt_create(const gpt_problem_config *pc, const gpt_solver_config *sc,
     if (e == cudaSuccess) e = cudaMallocHost((void **)&h->h_st, sizeof(InstState) * B);
     if (e == cudaSuccess) e = cudaMallocHost((void **)&h->h_pcg_out, sizeof(uint32_t) * 2 * B);
     if (e == cudaSuccess) e = cudaMallocHost((void **)&h->h_pcg_log, sizeof(uint32_t) * B * sc->sqp_max_iter);
+    if (e == cudaSuccess) e = cudaMallocHost((void **)&h->h_trk_rows, sizeof(int) * (B + 1));
+    if (e == cudaSuccess) e = cudaMallocHost((void **)&h->h_trk_inst, sizeof(TrackInst) * B);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->ev, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaMemset(h->S, 0, sizeof(float) * PK * T);
     if (e == cudaSuccess) e = cudaMemset(h->dz, 0, sizeof(float) * NX * T);
@@ -337,6 +351,8 @@ gpt_status gpt_destroy(gpt_handle *h)
     cudaFree(h->S64); cudaFree(h->gamma64); cudaFree(h->adj_gamma64);
     for (auto &ge : h->graphs) cudaGraphExecDestroy(ge.exec);
     cudaFree(h->gxu); cudaFree(h->glam); cudaFree(h->ggoal); cudaFree(h->d_iter);
+    cudaFree(h->trk_xu_old); cudaFree(h->trk_rows); cudaFree(h->trk_clk); cudaFree(h->trk_inst);
+    cudaFreeHost(h->h_trk_rows); cudaFreeHost(h->h_trk_inst);
     if (h->cap_stream) cudaStreamDestroy(h->cap_stream);
     if (h->body_stream) cudaStreamDestroy(h->body_stream);
     cudaFreeHost(h->h_active); cudaFreeHost(h->h_st); cudaFreeHost(h->h_pcg_out); cudaFreeHost(h->h_pcg_log);
@@ -940,6 +956,203 @@ gpt_status gpt_sqp_adjoint(gpt_handle *h, uint32_t B, const uint32_t *h_N, const
         if (st.exit_flags & 4u) return set_err(GPT_ERR_NONFINITE, "non-finite value in an adjoint solve");
         if (st.pcg_maxiter_count) return set_err(GPT_ERR_NONFINITE, "PCG reached pcg_max_iter in the adjoint");
     }
+    return GPT_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// MPC tracking loop (toplevel.cuh:507-796)
+// ---------------------------------------------------------------------------
+
+namespace {
+
+TrackParams track_params(float timestep, float sim_step, float shift_threshold, double sim_us)
+{
+    TrackParams tp;
+    tp.sim_us = sim_us;
+    tp.shift_threshold = (double)(shift_threshold > 0.f ? shift_threshold : timestep);
+    tp.timestep = (double)timestep;
+    tp.sim_step = sim_step;
+    const double t = sim_us * 1e-6;
+    tp.n_sub = (uint32_t)(t / (double)sim_step);  // integrator.cuh:383
+    tp.sim_last = (float)fmod(t, (double)sim_step);  // integrator.cuh:395
+    return tp;
+}
+
+// Updates the shared clock runs before the longest trajectory is done: the host image of
+// track_clock_kernel's arithmetic (the same doubles in the same order).
+uint32_t track_update_count(const TrackParams &tp, uint32_t max_steps, uint32_t max_updates)
+{
+    double ts = 0.0;
+    bool shifted = false;
+    uint32_t off = 0, u = 0;
+    while (u < max_updates && off < max_steps) {
+        ts += tp.sim_us * 1e-6;
+        if (!shifted && ts > tp.shift_threshold) {
+            off++;
+            shifted = true;
+        }
+        if (ts > tp.timestep) {
+            shifted = false;
+            ts = fmod(ts, tp.timestep);
+        }
+        u++;
+    }
+    return u;
+}
+
+}  // namespace
+
+// One solve of every active instance on the handle's working buffers (gxu, glam, ggoal):
+// the cached graph, or the host loop when graphs are off or profiling is on.
+static gpt_status solve_on_workspace(gpt_handle *h, const SqpPlan &pl, cudaStream_t s)
+{
+    if (pl.SP.sqp_graph && !h->profile) {
+        cudaGraphExec_t exec = nullptr;
+        const gpt_status st = sqp_graph_for(h, pl, &exec);
+        if (st != GPT_OK) return st;
+        GPT_CUDA(cudaGraphLaunch(exec, s));
+        return GPT_OK;
+    }
+    {
+        const gpt_status st = enqueue_prologue(h, pl, h->ggoal, h->gxu, s);
+        if (st != GPT_OK) return st;
+    }
+    for (uint32_t it = 0; it < pl.SP.sqp_max_iter; ++it) {
+        const gpt_status st = enqueue_iteration(h, pl, h->ggoal, h->glam, h->gxu, s);
+        if (st != GPT_OK) return st;
+        GPT_CUDA(cudaMemcpyAsync(h->h_active, h->d_active, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+        GPT_CUDA(cudaEventRecord(h->ev, s));
+        GPT_CUDA(cudaEventSynchronize(h->ev));
+        if (*h->h_active == 0) break;
+    }
+    if (h->profile) collect_phase_times(h);
+    return GPT_OK;
+}
+
+extern "C" {
+
+void gpt_default_track_config(gpt_track_config *o)
+{
+    if (!o) return;
+    o->sim_period_us = 2000.f;      // perform_experiment.sh:29,46
+    o->sim_step = 2e-4f;            // integrator.cuh:378
+    o->shift_threshold = 0.f;       // settings.cuh:29 (1 * timestep)
+    o->max_control_updates = 100000;  // toplevel.cuh:515
+    o->jitter_solves = 0;
+    o->rho_reset = 1e-3f;           // toplevel.cuh:579
+}
+
+gpt_status gpt_track_batched(gpt_handle *h, uint32_t B, const uint32_t *h_N, const uint32_t *h_S,
+                             const float *d_eePos_traj, const float *d_xu_traj, float *d_xs,
+                             const gpt_track_config *tc_in, float *d_err, uint32_t *d_log, uint32_t log_cap,
+                             gpt_track_stats *h_stats, gpt_stream_t stream)
+{
+    if (!h || !h_N || !h_S || !d_eePos_traj || !d_xu_traj || !d_xs || !d_err)
+        return set_err(GPT_ERR_BAD_ARG, "null argument");
+    gpt_track_config tc;
+    gpt_default_track_config(&tc);
+    if (tc_in) tc = *tc_in;
+    if (!(tc.sim_period_us > 0.f) || !(tc.sim_step > 0.f) || !(tc.shift_threshold >= 0.f) || !(tc.rho_reset > 0.f))
+        return set_err(GPT_ERR_BAD_ARG, "sim_period_us, sim_step and rho_reset must be positive");
+    if ((double)tc.sim_period_us * 1e-6 / (double)tc.sim_step > 1e6)
+        return set_err(GPT_ERR_BAD_ARG, "more than 1e6 plant steps per control update");
+    if (B == 0 || B > h->pc.max_batch) return set_err(GPT_ERR_CAPACITY, "batch exceeds handle capacity");
+    uint32_t maxS = 0;
+    h->h_trk_rows[0] = 0;
+    for (uint32_t b = 0; b < B; ++b) {
+        if (h_S[b] < h_N[b])
+            return set_err(GPT_ERR_BAD_ARG, "traj_steps must be >= knot_points (runme.cu:151 skips shorter trajectories)");
+        if ((uint64_t)h->h_trk_rows[b] + h_S[b] > 0x7fffffffu) return set_err(GPT_ERR_BAD_ARG, "trajectories too long");
+        h->h_trk_rows[b + 1] = h->h_trk_rows[b] + (int)h_S[b];
+        maxS = h_S[b] > maxS ? h_S[b] : maxS;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    BatchView bv;
+    int maxN = 0, minN = 0;
+    {
+        const gpt_status st = setup_batch(h, B, h_N, nullptr, tc.rho_reset, bv, maxN, minN, s);
+        if (st != GPT_OK) return st;
+    }
+    const ProblemParams P = to_params(h->pc);
+    SolverParams SP = to_solver(h->sc);
+    if (SP.pcg_cluster_size == 0) {
+        for (const auto &t : h->tuned)
+            if (t.B == bv.B && t.total == bv.total_knots && t.maxN == maxN && t.minN == minN) SP.pcg_cluster_size = t.cluster;
+    }
+    const SqpPlan plan{bv, P, SP, maxN, minN, h->num_sms};
+    const TrackParams tp = track_params(h->pc.timestep, tc.sim_step, tc.shift_threshold, (double)tc.sim_period_us);
+    const uint32_t n_updates = track_update_count(tp, maxS, tc.max_control_updates);
+    const int ns = h->num_sms;
+
+    GPT_CUDA(cudaMemcpyAsync(h->trk_rows, h->h_trk_rows, sizeof(int) * (B + 1), cudaMemcpyHostToDevice, s));
+    GPT_CUDA(cudaMemsetAsync(d_err, 0, sizeof(float) * (size_t)h->h_trk_rows[B], s));
+    GPT_CUDA(launch_track_start(bv, h->trk_rows, d_eePos_traj, d_xu_traj, h->gxu, h->trk_xu_old, h->ggoal, h->glam,
+                                h->trk_clk, h->trk_inst, 1e-3f, 0, ns, s));
+    if (tc.jitter_solves > 0) {  // toplevel.cuh:581-592
+        SolverParams SPj = SP;
+        SPj.pcg_tol = 1e-11f;
+        SPj.pcg_max_iter = 10000;
+        const SqpPlan pj{bv, P, SPj, maxN, minN, ns};
+        for (uint32_t j = 0; j < tc.jitter_solves; ++j) {
+            GPT_CUDA(launch_track_prep(bv, h->trk_rows, h->trk_clk, 1e-3f, 1, s));
+            const gpt_status st = solve_on_workspace(h, pj, s);
+            if (st != GPT_OK) return st;
+            GPT_CUDA(launch_track_start(bv, h->trk_rows, d_eePos_traj, d_xu_traj, h->gxu, h->trk_xu_old, h->ggoal,
+                                        h->glam, h->trk_clk, h->trk_inst, j + 1 == tc.jitter_solves ? 1e-3f : -1.f,
+                                        1, ns, s));
+        }
+    }
+    for (uint32_t u = 0; u < n_updates; ++u) {
+        GPT_CUDA(launch_track_prep(bv, h->trk_rows, h->trk_clk, tc.rho_reset, 0, s));
+        const gpt_status st = solve_on_workspace(h, plan, s);
+        if (st != GPT_OK) return st;
+        GPT_CUDA(launch_track_tail(bv, h->trk_rows, h->trk_clk, tp, d_eePos_traj, d_xu_traj, d_xs, h->gxu,
+                                   h->trk_xu_old, h->ggoal, h->glam, h->adj_h, d_err, h->trk_inst, d_log, log_cap, s));
+    }
+    GPT_CUDA(launch_track_final(bv, d_xs, h->ggoal, h->trk_inst, s));
+    GPT_CUDA(cudaMemcpyAsync(h->h_trk_inst, h->trk_inst, sizeof(TrackInst) * B, cudaMemcpyDeviceToHost, s));
+    GPT_CUDA(cudaStreamSynchronize(s));
+    bool nonfinite = false;
+    for (uint32_t b = 0; b < B; ++b) {
+        const TrackInst &ti = h->h_trk_inst[b];
+        if (ti.nonfinite) nonfinite = true;
+        if (!h_stats) continue;
+        gpt_track_stats &o = h_stats[b];
+        o.control_updates = ti.updates;
+        o.shifts = ti.shifts;
+        o.sqp_iters_total = ti.sqp_iters;
+        o.pcg_iters_total = ti.pcg_iters;
+        o.ls_fail_total = ti.ls_fail;
+        o.pcg_maxiter_total = ti.pcg_maxiter;
+        o.rho_exits = ti.rho_exits;
+        o.nonfinite = ti.nonfinite;
+        o.tracking_error_mean = ti.shifts ? ti.err_sum / (float)ti.shifts : 0.f;
+        o.final_tracking_error = ti.final_err;
+        o.rho_final = ti.rho;
+    }
+    if (nonfinite) return set_err(GPT_ERR_NONFINITE, "non-finite merit or PCG reduction in a tracking solve");
+    return GPT_OK;
+}
+
+gpt_status gpt_track(gpt_handle *h, uint32_t N, uint32_t S, const float *d_eePos_traj, const float *d_xu_traj,
+                     float *d_xs, const gpt_track_config *tc, float *d_err, uint32_t *d_log, uint32_t log_cap,
+                     gpt_track_stats *h_stats, gpt_stream_t stream)
+{
+    return gpt_track_batched(h, 1, &N, &S, d_eePos_traj, d_xu_traj, d_xs, tc, d_err, d_log, log_cap, h_stats, stream);
+}
+
+gpt_status gpt_simulate(gpt_handle *h, uint32_t N, float *d_xs, const float *d_xu, double time_offset_us,
+                        double sim_time_us, float sim_step, gpt_stream_t stream)
+{
+    if (!h || !d_xs || !d_xu) return set_err(GPT_ERR_BAD_ARG, "null argument");
+    if (!check_n(h, N)) return set_err(GPT_ERR_BAD_ARG, "knot_points out of range");
+    if (!(sim_step > 0.f) || !(sim_time_us >= 0.0) || !(time_offset_us >= 0.0) ||
+        sim_time_us * 1e-6 / (double)sim_step > 1e6)
+        return set_err(GPT_ERR_BAD_ARG, "sim_step must be positive, times non-negative, <= 1e6 plant steps");
+    const TrackParams tp = track_params(h->pc.timestep, sim_step, 0.f, sim_time_us);
+    GPT_CUDA(launch_simulate_one((int)N, tp, time_offset_us, d_xs, d_xu, (cudaStream_t)stream));
     return GPT_OK;
 }
 

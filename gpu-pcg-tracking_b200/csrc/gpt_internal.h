@@ -68,6 +68,39 @@ size_t adjoint_part_floats();
 cudaError_t launch_pack_rows64(int N, const float *S, const float *gamma, double *S64, double *gamma64, int num_sms,
                                cudaStream_t s);
 
+// MPC tracking loop (gpt_track.cu).  The loop's clock is shared by the batch: every instance
+// advances on the same schedule; instance b stops once the trajectory offset reaches its length.
+struct TrackClock {
+    double time_since;     // time since the last timestep (toplevel.cuh:524)
+    double prev_sim_us;    // previous update's simulated time (toplevel.cuh:523)
+    double sim_offset_us;  // this update's plant time offset into the previous solution
+    uint32_t shifted, traj_offset, start_offset, do_shift, updates;
+};
+struct TrackInst {  // per-instance totals over the loop
+    uint32_t updates, sqp_iters, pcg_iters, ls_fail, pcg_maxiter, rho_exits, nonfinite, shifts;
+    float err_sum, final_err, rho, pad;
+};
+struct TrackParams {
+    double sim_us;           // SIMULATION_PERIOD
+    double shift_threshold;  // SHIFT_THRESHOLD (s)
+    double timestep;         // the solver's timestep, as double (track's arithmetic)
+    float sim_step;          // plant step, 2e-4 s
+    float sim_last;          // fmod(sim time, sim_step): the final partial step
+    uint32_t n_sub;          // floor(sim time / sim_step)
+};
+cudaError_t launch_track_start(const BatchView &bv, const int *rows, const float *eePos_traj, const float *xu_traj,
+                               float *xu, float *xu_old, float *goal, float *lambda, TrackClock *clk, TrackInst *inst,
+                               float rho0, int reset_xu_only, int num_sms, cudaStream_t s);
+cudaError_t launch_track_prep(const BatchView &bv, const int *rows, const TrackClock *clk, float rho_reset,
+                              int all_live, cudaStream_t s);
+cudaError_t launch_track_tail(const BatchView &bv, const int *rows, TrackClock *clk, const TrackParams &tp,
+                              const float *eePos_traj, const float *xu_traj, float *xs, float *xu, float *xu_old,
+                              float *goal, float *lambda, float *tmp, float *errors, TrackInst *inst,
+                              uint32_t *iters_log, uint32_t log_cap, cudaStream_t s);
+cudaError_t launch_track_final(const BatchView &bv, const float *xs, const float *goal, TrackInst *inst, cudaStream_t s);
+cudaError_t launch_simulate_one(int N, const TrackParams &tp, double t0_us, float *xs, const float *xu,
+                                cudaStream_t s);
+
 }  // namespace gpt
 
 #include "../../include/gpt.h"

@@ -187,6 +187,80 @@ gpt_status gpt_sqp_adjoint(gpt_handle *h, uint32_t batch, const uint32_t *h_knot
                            float *d_xu_next, float *d_grad_eePos, float *d_grad_qd, float *d_grad_r,
                            float *d_grad_q_ee, gpt_stream_t stream);
 
+/* ---- the MPC tracking loop around the solve ---- */
+
+/* Controls of the tracking loop: settings.cuh:26-29,59 and the -DSIMULATION_PERIOD flag of
+ * perform_experiment.sh:46, toplevel.cuh:514-592, integrator.cuh:365-398.  The reference's
+ * CONST_UPDATE_FREQ 1 mode: every control update simulates a fixed plant time. */
+typedef struct gpt_track_config {
+    float sim_period_us;          /* SIMULATION_PERIOD: plant time per control update (2000 in the logged runs) */
+    float sim_step;               /* plant explicit-Euler step, 2e-4 s (integrator.cuh:378) */
+    float shift_threshold;        /* SHIFT_THRESHOLD in seconds (settings.cuh:29: 1 * timestep); 0 = timestep */
+    uint32_t max_control_updates; /* 100000 (toplevel.cuh:515) */
+    uint32_t jitter_solves;       /* REMOVE_JITTERS (settings.cuh:59): solves from the trajectory at PCG
+                                     tolerance 1e-11 / 10000 iterations before tracking, which warm lambda
+                                     (toplevel.cuh:581-592; the reference runs 100); 0 = none */
+    float rho_reset;              /* 1e-3 (toplevel.cuh:579) */
+} gpt_track_config;
+
+/* One instance's tracking run (the reference returns per-update vectors and the final error,
+ * toplevel.cuh:810-815) */
+typedef struct gpt_track_stats {
+    uint32_t control_updates;     /* control updates this instance ran */
+    uint32_t shifts;              /* trajectory offset reached (traj_steps when the run completed) */
+    uint32_t sqp_iters_total;
+    uint32_t pcg_iters_total;
+    uint32_t ls_fail_total;
+    uint32_t pcg_maxiter_total;
+    uint32_t rho_exits;           /* solves that ended with rho > rho_max */
+    uint32_t nonfinite;           /* solves that met a NaN/Inf */
+    float tracking_error_mean;    /* mean of the per-shift errors */
+    float final_tracking_error;   /* after the loop (toplevel.cuh:789-794) */
+    float rho_final;
+} gpt_track_stats;
+
+void gpt_default_track_config(gpt_track_config *out);
+
+/*
+ * Receding-horizon tracking of a precomputed trajectory: replaces
+ *   track<T, R>(state_size, control_size, knot_points, traj_steps, timestep, d_eePos_traj, d_xu_traj,
+ *               d_xs, start_state_ind, goal_state_ind, test_iter, pcg_exit_tol, test_output_prefix)
+ *                                                                      (toplevel.cuh:507-510)
+ * Each control update solves the SQP (the handle's solver settings; sqp_max_iter stands in for the
+ * reference's wall-clock cap SQP_MAX_TIME_US), simulates the plant (explicit Euler at sim_step) for
+ * sim_period_us with the previous solution's controls, and once per timestep records the tracking
+ * error sum_{i<3} |p(x_s)_i - goal_0,i| and shifts xu, the goal window and lambda one knot along
+ * the trajectory (toplevel.cuh:600-726).  The run ends when the offset reaches traj_steps.
+ *   d_eePos_traj  [6 traj_steps]   goal rows (runme.cu:145-150)
+ *   d_xu_traj     [21 traj_steps]  x_k, u_k rows (runme.cu:152-157); traj_steps >= knot_points
+ *   d_xs          [14]             plant state, in/out (the reference's d_xs)
+ *   d_tracking_errors [traj_steps] one error per shift
+ *   d_sqp_iters_log (optional)     SQP iterations of each update, first log_capacity updates
+ *                                  (the returned sqp_iters vector of the reference)
+ * The loop's working xu, lambda and goal window live in the handle (no allocation). */
+gpt_status gpt_track(gpt_handle *h, uint32_t knot_points, uint32_t traj_steps, const float *d_eePos_traj,
+                     const float *d_xu_traj, float *d_xs, const gpt_track_config *tc, float *d_tracking_errors,
+                     uint32_t *d_sqp_iters_log, uint32_t log_capacity, gpt_track_stats *h_stats,
+                     gpt_stream_t stream);
+
+/* Many tracking runs at once (no reference counterpart): instance b has horizon h_knot_points[b]
+ * and owns trajectory rows R_b .. R_b + h_traj_steps[b] - 1 of d_eePos_traj / d_xu_traj and of
+ * d_tracking_errors (R_b = sum of the earlier traj_steps), 14 floats of d_xs, log_capacity
+ * entries of d_sqp_iters_log and one h_stats entry.  Every update is one batched solve plus one
+ * simulation / shift launch for the batch; all instances share the update clock and an instance
+ * stops once the offset reaches its traj_steps. */
+gpt_status gpt_track_batched(gpt_handle *h, uint32_t batch, const uint32_t *h_knot_points,
+                             const uint32_t *h_traj_steps, const float *d_eePos_traj, const float *d_xu_traj,
+                             float *d_xs, const gpt_track_config *tc, float *d_tracking_errors,
+                             uint32_t *d_sqp_iters_log, uint32_t log_capacity, gpt_track_stats *h_stats,
+                             gpt_stream_t stream);
+
+/* simple_simulate (integrator.cuh:365-398): advances the plant state d_xs (14) by sim_time_us of
+ * explicit-Euler steps of sim_step seconds (plus the remainder step), applying the control of
+ * knot floor(t / timestep) of d_xu (21N-7), t starting time_offset_us into the horizon. */
+gpt_status gpt_simulate(gpt_handle *h, uint32_t knot_points, float *d_xs, const float *d_xu, double time_offset_us,
+                        double sim_time_us, float sim_step, gpt_stream_t stream);
+
 /* ---- the reference's kernels, one instance, device buffers, stream-ordered ---- */
 
 /* gato_form_kkt (schur.cuh:391-524); d_xs = x_s (14) */

@@ -1026,3 +1026,130 @@ int ORC(sqp_solve)(const orc_params *P, const orc_solver *SV, int N, const R *go
     free(cp); free(ri); free(val); free(bf); free(xf); free(ld);
     return rc;
 }
+
+/* ------------------------------------------------------------------------ */
+/* plant simulation and the MPC tracking loop                                */
+/* ------------------------------------------------------------------------ */
+
+/* One explicit-Euler plant step x <- x + h [qd; FD(q, qd, u)]: simple_integrator_kernel
+ * (integrator.cuh:306-331), which always integrates with type 0. */
+static void plant_step(R *x, const R *u, R h)
+{
+    R qdd[7], xn[NS];
+    ORC(fd)(x, x + 7, u, qdd);
+    step_state(0, h, x, qdd, xn);
+    memcpy(x, xn, sizeof(xn));
+}
+
+/* Control slot applied at plant time t (s): floor(t / timestep) (integrator.cuh:380-388),
+ * clamped to the last control of the horizon. */
+static int control_slot(double t, double timestep, int N)
+{
+    unsigned co = (unsigned)(t / timestep);
+    return (int)co > N - 2 ? N - 2 : (int)co;
+}
+
+/* simple_simulate (integrator.cuh:365-398): advances x_s by sim_time_us of plant time in
+ * steps of sim_step (a float, as the reference's T), starting time_offset_us into the
+ * horizon xu, then one final step of the remainder fmod(sim_time, sim_step). */
+void ORC(simulate)(int N, R *xs, const R *xu, double timestep, double time_offset_us, double sim_time_us,
+                   double sim_step)
+{
+    const double t0 = time_offset_us * 1e-6, sim_time = sim_time_us * 1e-6;
+    const float h = (float)sim_step;
+    int co = control_slot(t0, timestep, N);
+    const unsigned n = (unsigned)(sim_time / (double)h);
+    for (unsigned step = 0; step < n; ++step) {
+        co = control_slot(t0 + (double)((float)step * h), timestep, N);
+        plant_step(xs, xu + NX * co + NS, (R)h);
+    }
+    const R hl = (R)(float)fmod(sim_time, (double)h);
+    plant_step(xs, xu + NX * co + NS, hl);
+}
+
+/* sum_{i<3} |p(q)_i - goal_i| (toplevel.cuh:674-681) */
+static R tracking_error(const R *xs, const R *goal)
+{
+    R ee[6];
+    ORC(fk)(xs, ee);
+    R e = 0;
+    for (int i = 0; i < 3; ++i) e += (R)fabs((double)(ee[i] - goal[i]));
+    return e;
+}
+
+/* track (toplevel.cuh:507-796) with CONST_UPDATE_FREQ 1, ADD_NOISE 0: each control update
+ * solves the SQP from the shifted previous solution, simulates the plant for sim_period_us
+ * with the previous solution's controls, and once per timestep (SHIFT_THRESHOLD) records the
+ * tracking error and shifts xu, the goal window and lambda one knot along the trajectory.
+ * Trajectory rows: eePos_traj [6 S], xu_traj [21 S] (x_k, u_k per row, runme.cu:145-161).
+ * xs (14) is the plant state, in/out; errors receives one entry per shift (S at most). */
+int ORC(track)(const orc_params *P, const orc_solver *SV, const orc_track_cfg *TC, int N, int S, const R *eePos_traj,
+               const R *xu_traj, R *xs, R *errors, orc_track_stats *ts)
+{
+    const int traj_len = NX * N - NC;
+    const double dt = (double)(float)P->dt;
+    const double thr = (double)(float)TC->shift_threshold;
+    R *xu = malloc(sizeof(R) * NX * N), *xu_old = malloc(sizeof(R) * NX * N), *goal = malloc(sizeof(R) * 6 * N),
+      *lambda = calloc((size_t)NS * N, sizeof(R));
+    memcpy(xu, xu_traj, sizeof(R) * traj_len);      /* toplevel.cuh:550-552 */
+    memcpy(xu_old, xu_traj, sizeof(R) * traj_len);
+    memcpy(goal, eePos_traj, sizeof(R) * 6 * N);
+    memset(ts, 0, sizeof(*ts));
+    R rho = (R)1e-3;
+    orc_stats st;
+    int rc = 0;
+    if (TC->jitter_solves > 0) { /* toplevel.cuh:581-592 */
+        orc_solver jv = *SV;
+        jv.pcg_tol = 1e-11;
+        jv.pcg_max_iter = 10000;
+        for (int j = 0; j < TC->jitter_solves && rc == 0; ++j) {
+            rc = ORC(sqp_solve)(P, &jv, N, goal, lambda, xu, &rho, (R)1e-3, &st, NULL);
+            memcpy(xu, xu_traj, sizeof(R) * traj_len);
+        }
+        rho = (R)1e-3;
+    }
+    double time_since = 0.0, prev_sim = 0.0;
+    int shifted = 0, traj_offset = 0, step;
+    for (step = 0; step < TC->max_control_updates && rc == 0; ++step) {
+        if (traj_offset == S) break;
+        rc = ORC(sqp_solve)(P, SV, N, goal, lambda, xu, &rho, (R)TC->rho_reset, &st, NULL);
+        ts->sqp_iters_total += st.sqp_iters;
+        ts->pcg_iters_total += st.pcg_iters_total;
+        ts->ls_fail_total += st.ls_fail_count;
+        ts->rho_exits += st.rho_exit;
+        const double sim = TC->sim_period_us;
+        ORC(simulate)(N, xs, xu_old, dt, prev_sim, sim, TC->sim_step);
+        memcpy(xu_old, xu, sizeof(R) * traj_len);
+        time_since += sim * 1e-6;
+        if (!shifted && time_since > thr) {
+            errors[traj_offset] = tracking_error(xs, goal);
+            traj_offset++;
+            /* just_shift (integrator.cuh:299-304): knot k <- knot k+1 (x_{N-1} -> x_{N-2}; u_{N-2} kept) */
+            memmove(xu, xu + NX, sizeof(R) * (NX * (N - 2) + NS));
+            if (traj_offset + N < S) {
+                memcpy(xu + traj_len - NX, xu_traj + NX * traj_offset - NC, sizeof(R) * NX);
+            } else {
+                memcpy(xu + traj_len - NS, xu_traj + NX * (S - 1), sizeof(R) * 7);
+                memset(xu + traj_len - 7, 0, sizeof(R) * 7);
+                memset(xu + traj_len - NX, 0, sizeof(R) * NC);
+            }
+            memmove(goal, goal + 6, sizeof(R) * 6 * (N - 1));
+            const int row = (traj_offset + N < S) ? traj_offset + N - 1 : S - 1;
+            memcpy(goal + 6 * (N - 1), eePos_traj + 6 * row, sizeof(R) * 6);
+            memmove(lambda, lambda + NS, sizeof(R) * NS * (N - 1));
+            shifted = 1;
+        }
+        if (time_since > dt) {
+            shifted = 0;
+            time_since = fmod(time_since, dt);
+        }
+        memcpy(xu, xs, sizeof(R) * NS);
+        prev_sim = sim;
+    }
+    ts->control_updates = step;
+    ts->shifts = traj_offset;
+    ts->final_error = tracking_error(xs, goal);
+    ts->rho_final = rho;
+    free(xu); free(xu_old); free(goal); free(lambda);
+    return rc;
+}

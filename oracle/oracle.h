@@ -59,4 +59,25 @@ typedef struct {
     double rho_factor, rho_max, rho_min;   /* RHO_FACTOR, RHO_MAX, RHO_MIN (settings.cuh:50) */
 } orc_solver;
 
+/* MPC tracking loop controls (toplevel.cuh:507-596, settings.cuh:26-29, integrator.cuh:365-398) */
+typedef struct {
+    double sim_period_us;     /* SIMULATION_PERIOD: plant time simulated per control update (CONST_UPDATE_FREQ 1) */
+    double sim_step;          /* plant integration step, 2e-4 s, held as float (integrator.cuh:378) */
+    double shift_threshold;   /* SHIFT_THRESHOLD in s (settings.cuh:29: 1 * timestep) */
+    int max_control_updates;  /* 100000 (toplevel.cuh:515) */
+    int jitter_solves;        /* REMOVE_JITTERS: solves at tol 1e-11 before tracking (toplevel.cuh:581-592) */
+    double rho_reset;         /* 1e-3 (toplevel.cuh:579) */
+} orc_track_cfg;
+
+typedef struct {
+    int control_updates;      /* control_update_step at exit */
+    int shifts;               /* traj_offset at exit */
+    int sqp_iters_total;
+    int pcg_iters_total;
+    int ls_fail_total;
+    int rho_exits;
+    double final_error;       /* cur_tracking_error after the loop (toplevel.cuh:789-794) */
+    double rho_final;
+} orc_track_stats;
+
 #endif

@@ -35,6 +35,19 @@ class Solver(C.Structure):
                 ("rho_max", C.c_double), ("rho_min", C.c_double)]
 
 
+class TrackCfg(C.Structure):
+    """orc_track_cfg (oracle.h)."""
+    _fields_ = [("sim_period_us", C.c_double), ("sim_step", C.c_double), ("shift_threshold", C.c_double),
+                ("max_control_updates", C.c_int), ("jitter_solves", C.c_int), ("rho_reset", C.c_double)]
+
+
+class TrackStats(C.Structure):
+    """orc_track_stats (oracle.h)."""
+    _fields_ = [("control_updates", C.c_int), ("shifts", C.c_int), ("sqp_iters_total", C.c_int),
+                ("pcg_iters_total", C.c_int), ("ls_fail_total", C.c_int), ("rho_exits", C.c_int),
+                ("final_error", C.c_double), ("rho_final", C.c_double)]
+
+
 class Stats(C.Structure):
     """orc_stats (oracle.h)."""
     _fields_ = [("sqp_iters", C.c_int), ("rho_exit", C.c_int), ("ls_fail_count", C.c_int),
@@ -83,6 +96,9 @@ def _declare(L):
         fn("merit", [C.POINTER(Params), C.c_int, rp, C.c_void_p, rt, rp, rp, C.c_int, C.c_void_p], rt)
         fn("sqp_solve", [C.POINTER(Params), C.POINTER(Solver), C.c_int, rp, rp, rp, C.POINTER(rt), rt,
                          C.POINTER(Stats), C.c_void_p], C.c_int)
+        fn("simulate", [C.c_int, rp, rp, C.c_double, C.c_double, C.c_double, C.c_double])
+        fn("track", [C.POINTER(Params), C.POINTER(Solver), C.POINTER(TrackCfg), C.c_int, C.c_int, rp, rp, rp, rp,
+                     C.POINTER(TrackStats)], C.c_int)
     L.orc_ldl_solve.argtypes = [C.c_int, _i32p, _i32p, _f32p, _f32p, _f32p]
     L.orc_ldl_solve.restype = C.c_int
 
@@ -247,3 +263,31 @@ def sqp_solve(params, solver, N, goal, lam, xu, rho, rho_reset=1e-3, precision="
     if rc < 0:
         raise RuntimeError("oracle linear solve failed")
     return xu_a, lam_a, float(rho_c.value), st, pit[:st.linsys_count]
+
+
+def make_track_cfg(sim_period_us=2000.0, sim_step=2e-4, shift_threshold=1.0 / 64, max_control_updates=100000,
+                   jitter_solves=0, rho_reset=1e-3):
+    return TrackCfg(sim_period_us, sim_step, shift_threshold, max_control_updates, jitter_solves, rho_reset)
+
+
+def simulate(N, xs, xu, timestep, time_offset_us, sim_time_us, sim_step=2e-4, precision="f64"):
+    """simple_simulate (integrator.cuh:365-398) on a copy of xs; returns the new state."""
+    x = _a(xs, precision).copy()
+    getattr(lib(), f"orc_{precision}_simulate")(N, x, _a(xu, precision), float(timestep), float(time_offset_us),
+                                               float(sim_time_us), float(sim_step))
+    return x
+
+
+def track(params, solver, cfg, N, eePos_traj, xu_traj, xs, precision="f64"):
+    """track (toplevel.cuh:507-796): returns (final xs, per-shift tracking errors, TrackStats)."""
+    ee = _a(eePos_traj, precision).reshape(-1)
+    tr = _a(xu_traj, precision).reshape(-1)
+    S = ee.size // 6
+    x = _a(xs, precision).copy()
+    err = np.zeros(max(S, 1), _dt(precision))
+    ts = TrackStats()
+    rc = getattr(lib(), f"orc_{precision}_track")(C.byref(params), C.byref(solver), C.byref(cfg), N, S, ee, tr, x,
+                                                 err, C.byref(ts))
+    if rc < 0:
+        raise RuntimeError("oracle linear solve failed")
+    return x, err[:ts.shifts], ts
