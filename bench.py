@@ -63,6 +63,10 @@ def parse():
     ap.add_argument("--pcg-precond", type=int, default=1, choices=[0, 1],
                     help="0 block-Jacobi (the reference's), 1 block-tridiagonal LDL^T per CTA chunk")
     ap.add_argument("--batched-only", action="store_true", help="skip the e2e and plain legs (profiling runs)")
+    ap.add_argument("--no-track", action="store_true", help="skip the MPC tracking leg")
+    ap.add_argument("--track-sqp-iters", type=int, default=4,
+                    help="SQP iterations per solve in the tracking leg (stands in for the wall-clock cap)")
+    ap.add_argument("--track-period-us", type=float, default=2000.0, help="plant time per control update")
     return ap.parse_args()
 
 
@@ -358,6 +362,46 @@ def main():
             plain_ms.append(e0.elapsed_time(e1))
     plain_rate = 1000.0 / statistics.mean(plain_ms) if plain_ms else None
 
+    # MPC tracking leg (gpt_track_batched): every instance tracks its own spline for as many rows as
+    # its horizon (the shortest trajectory the loop accepts); one solve per control update
+    track = None
+    if not args.no_track:
+        sv.set_solver(sqp_max_iter=args.track_sqp_iters, pcg_cluster_size=tuned_cs)
+        tcfg = gpt.default_track_config(sim_period_us=args.track_period_us)
+        xs_t = torch.cat([xu0[21 * o:21 * o + 14] for o in offs]).contiguous()
+        errs = torch.zeros(B * N, device="cuda")
+        sv.sqp_solve_batched(Ns, goal, lam, xu, [1e-3] * B)  # builds this shape's solve graph
+        flush.fill_(1.0)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        _, tstats = sv.track_batched(Ns, [N] * B, goal, xu0, xs_t, tcfg, errors=errs)
+        e1.record(stream)
+        e1.synchronize()
+        t_ms = shard.max_over_ranks(e0.elapsed_time(e1), device="cuda")
+        upd = tstats[0]["control_updates"]
+        # the plain single-instance loop on instance 0's trajectory
+        sv1.set_solver(sqp_max_iter=args.track_sqp_iters)
+        xs1 = xs_t[:14].clone()
+        e0.record(stream)
+        _, pst = sv1.track(N, goal[:6 * N].contiguous(), xu0[:21 * N].contiguous(), xs1, tcfg)
+        e1.record(stream)
+        e1.synchronize()
+        p_ms = e0.elapsed_time(e1)
+        track = {
+            "workload": f"gpt_track_batched: {B} instances x N={N}, trajectory of {N} rows each (the instance's "
+                        f"spline), plant period {args.track_period_us:g} us, {args.track_sqp_iters} SQP iterations "
+                        f"per solve, one solve per control update",
+            "control_updates": upd, "ms": t_ms, "ms_per_update": t_ms / max(upd, 1),
+            "solves_per_s": world * B * upd / (t_ms / 1000.0),
+            "sqp_iters_per_solve": sum(t["sqp_iters_total"] for t in tstats) / max(B * upd, 1),
+            "tracking_error_mean": statistics.mean(t["tracking_error_mean"] for t in tstats),
+            "final_tracking_error_mean": statistics.mean(t["final_tracking_error"] for t in tstats),
+            "rho_exits": sum(t["rho_exits"] for t in tstats),
+            "plain_solves_per_s": pst["control_updates"] / (p_ms / 1000.0),
+            "plain_tracking_error_mean": pst["tracking_error_mean"],
+            "batched_over_plain": (B * upd / t_ms) / (pst["control_updates"] / p_ms),
+        }
+
     if rank != 0:
         if world > 1:
             dist.destroy_process_group()
@@ -413,6 +457,7 @@ def main():
         "sqp_iters_mean": statistics.mean(sqp_iters), "pcg_iters_per_solve": pcg_total / max(len(all_stats), 1),
         "pcg_iters_per_linsys": pcg_total / max(n_pcg_solves, 1), "pcg_maxiter_solves": pcg_maxit,
         "alg_bytes_per_sqp_iter_per_instance": 4 * N * ALG_FLOATS_PER_KNOT_SQP,
+        "track": track,
     }
     print(json.dumps(line), flush=True)
     if world > 1:

@@ -21,8 +21,11 @@
 #include <cstdint>
 #include <cstdio>
 #include <stdexcept>
+#include <string>
 #include <tuple>
 #include <vector>
+
+#include <cuda_runtime.h>
 
 #include "gpt.h"
 
@@ -134,4 +137,67 @@ std::tuple<std::vector<int>, std::vector<double>, double, uint32_t, bool, std::v
     const double us = std::chrono::duration<double, std::micro>(t1 - t0).count();
     const bool sqp_time_exit = (st.exit_flags & GPT_EXIT_RHO_MAX) == 0;
     return std::make_tuple(pcg_iter_vec, std::vector<double>{}, us, st.sqp_iters, sqp_time_exit, pcg_exit_vec);
+}
+
+// Replacement for track<T, return_type> (toplevel.cuh:507-510): the receding-horizon loop
+// runs on the device (gpt_track).  Returns the reference's tuple: per-update SQP iterations
+// (TIME_LINSYS 0), the per-shift tracking errors and the final tracking error.  The
+// experiment bookkeeping arguments (start/goal indices, test_iter, output prefix) only named
+// the reference's CSV dumps and are ignored.  SIMULATION_PERIOD is read when defined.
+template <typename T, typename return_type>
+std::tuple<std::vector<return_type>, std::vector<T>, T> track(
+    uint32_t state_size, uint32_t control_size, uint32_t knot_points, const uint32_t traj_steps, float timestep,
+    T *d_eePos_traj, T *d_xu_traj, T *d_xs, uint32_t /*start_state_ind*/, uint32_t /*goal_state_ind*/,
+    uint32_t /*test_iter*/, T pcg_exit_tol, const std::string & /*test_output_prefix*/ = std::string())
+{
+    static_assert(sizeof(T) == sizeof(float), "the B200 path computes in float32 (pcg_t = float)");
+    if (state_size != 14 || control_size != 7) throw std::runtime_error("iiwa14: state 14, control 7");
+    gpt_handle *h = gpt_dropin::handle_for(knot_points, timestep);
+    gpt_solver_config sc;
+    gpt_default_solver_config(&sc);
+#ifdef SQP_MAX_ITER
+    sc.sqp_max_iter = (uint32_t)(SQP_MAX_ITER);
+#endif
+#ifdef RHO_FACTOR
+    sc.rho_factor = (float)(RHO_FACTOR);
+#endif
+#ifdef RHO_MAX
+    sc.rho_max = (float)(RHO_MAX);
+#endif
+#ifdef PCG_MAX_ITER
+    sc.pcg_max_iter = (uint32_t)(PCG_MAX_ITER);
+#endif
+    sc.pcg_exit_tol = (float)pcg_exit_tol;
+    if (gpt_set_solver_config(h, &sc) != GPT_OK) throw std::runtime_error(gpt_last_error());
+    gpt_track_config tc;
+    gpt_default_track_config(&tc);
+#ifdef SIMULATION_PERIOD
+    tc.sim_period_us = (float)(SIMULATION_PERIOD);
+#endif
+#if defined(REMOVE_JITTERS) && REMOVE_JITTERS
+    tc.jitter_solves = 100;  // toplevel.cuh:584
+#endif
+    float *d_err = nullptr;
+    uint32_t *d_log = nullptr;
+    const uint32_t cap = tc.max_control_updates;
+    // the reference allocates its loop buffers per call too (toplevel.cuh:545-566)
+    if (cudaMalloc((void **)&d_err, sizeof(float) * traj_steps) != cudaSuccess ||
+        cudaMalloc((void **)&d_log, sizeof(uint32_t) * cap) != cudaSuccess) {
+        cudaFree(d_err);
+        throw std::runtime_error("track: cudaMalloc failed");
+    }
+    gpt_track_stats st;
+    const gpt_status s = gpt_track(h, knot_points, traj_steps, (const float *)d_eePos_traj, (const float *)d_xu_traj,
+                                   (float *)d_xs, &tc, d_err, d_log, cap, &st, nullptr);
+    std::vector<float> err(st.shifts);
+    std::vector<uint32_t> log(st.control_updates < cap ? st.control_updates : cap);
+    if (s == GPT_OK || s == GPT_ERR_NONFINITE) {
+        cudaMemcpy(err.data(), d_err, sizeof(float) * err.size(), cudaMemcpyDeviceToHost);
+        cudaMemcpy(log.data(), d_log, sizeof(uint32_t) * log.size(), cudaMemcpyDeviceToHost);
+    }
+    cudaFree(d_err);
+    cudaFree(d_log);
+    if (s != GPT_OK && s != GPT_ERR_NONFINITE) throw std::runtime_error(gpt_last_error());
+    return std::make_tuple(std::vector<return_type>(log.begin(), log.end()), std::vector<T>(err.begin(), err.end()),
+                           (T)st.final_tracking_error);
 }

@@ -76,19 +76,24 @@ def test_problem_generator_is_seeded(problem_mod):
 
 
 def test_cpp_dropin_header_compiles_and_links(tmp_path):
-    """include/gpt_toplevel.hpp (the sqpSolve drop-in) compiles with the reference's
-    macros defined and links against libgpt.so."""
+    """include/gpt_toplevel.hpp (the sqpSolve and track drop-ins) compiles with the
+    reference's macros defined and links against libgpt.so."""
     import subprocess
     src = tmp_path / "dropin.cpp"
     src.write_text(
         '#define QD_COST 1e-4\n#define R_COST 1e-4\n#define RHO_FACTOR 1.2\n#define RHO_MAX 10\n'
+        '#define SIMULATION_PERIOD 2000\n#define REMOVE_JITTERS 1\n'
         '#include "gpt_toplevel.hpp"\n'
         'int main(){ pcg_config cfg; float rho = 1e-3f;\n'
         '  if (0) { auto t = sqpSolve<float>(14, 7, 32, 0.015625f, (float*)0, (float*)0, (float*)0,\n'
-        '              gpt_dynamics_const_mem<float>(), cfg, rho, 1e-3f); (void)t; }\n'
+        '              gpt_dynamics_const_mem<float>(), cfg, rho, 1e-3f); (void)t;\n'
+        '    auto r = track<float, uint32_t>(14, 7, 32, 666, 0.015625f, (float*)0, (float*)0, (float*)0,\n'
+        '              0, 0, 0, 1e-5f, "out"); (void)r; }\n'
         '  gpt_problem_config pc; gpt_default_problem_config(&pc); return pc.state_size == 14 ? 0 : 1; }\n')
     exe = tmp_path / "dropin"
     lib_dir = os.path.join(ROOT, "gpu-pcg-tracking_b200")
-    subprocess.run(["g++", "-std=c++17", "-I", os.path.join(ROOT, "include"), str(src), "-L", lib_dir, "-lgpt",
+    cuda = os.environ.get("CUDA_HOME", "/usr/local/cuda")
+    subprocess.run(["g++", "-std=c++17", "-I", os.path.join(ROOT, "include"), "-I", os.path.join(cuda, "include"),
+                    str(src), "-L", lib_dir, "-lgpt", "-L", os.path.join(cuda, "lib64"), "-lcudart",
                     f"-Wl,-rpath,{lib_dir}", "-o", str(exe)], check=True)
     assert subprocess.run([str(exe)]).returncode == 0
