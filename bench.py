@@ -48,7 +48,7 @@ ALG_FLOATS_PER_KNOT_SQP = 4058   # every materialised SQP-iteration tensor writt
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--batch", type=int, default=512)
@@ -131,6 +131,16 @@ class ClockSampler:
             self.thread.start()
         except Exception:
             self.proc = None
+            return
+        # nvidia-smi's start-up (NVML initialisation) stays out of the timed region: wait for its
+        # first sample, and count only the samples taken after mark()
+        t0 = time.time()
+        while not self.lines and time.time() - t0 < 10.0 and self.proc.poll() is None:
+            time.sleep(0.02)
+        self.first = 0
+
+    def mark(self):
+        self.first = len(self.lines)
 
     def _read(self):
         for line in self.proc.stdout:
@@ -146,7 +156,8 @@ class ClockSampler:
             self.proc.kill()
         sm, mx, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        timed = self.lines[getattr(self, "first", 0):]
+        for ln in (timed if timed else self.lines):
             parts = [x.strip() for x in ln.split(",")]
             if len(parts) < 9:
                 continue
@@ -166,10 +177,8 @@ class ClockSampler:
 def run_reference(args, rank, world):
     if rank != 0:
         return
-    if args.no_cpu_baseline:
-        budget = 5.0
-    else:
-        budget = args.cpu_seconds
+    # each timed step is a bounded sample: about 45 s of host work over all steps, at least 2 s a step
+    budget = 5.0 if args.no_cpu_baseline else max(2.0, min(args.cpu_seconds, 45.0 / max(args.steps, 1)))
     times = []
     rates = []
     cb = None
@@ -254,12 +263,12 @@ def main():
     # the PCG cluster size for this batch shape, chosen by timing (gpt_autotune) unless given
     tuned_cs = args.pcg_cluster if args.pcg_cluster else sv.autotune(Ns, goal, lam0, xu0, [1e-3] * B)
 
+    clocks = ClockSampler(torch.cuda.current_device())
+    clocks.start()
     for _ in range(args.warmup):
         one_step()
     barrier()
-    clocks = ClockSampler(torch.cuda.current_device())
-    clocks.start()
-    barrier()
+    clocks.mark()
     step_ms, all_stats = [], []
     for _ in range(args.steps):
         ms, stats = one_step()
