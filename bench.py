@@ -64,6 +64,8 @@ def parse():
                     help="0 block-Jacobi (the reference's), 1 block-tridiagonal LDL^T per CTA chunk")
     ap.add_argument("--batched-only", action="store_true", help="skip the e2e and plain legs (profiling runs)")
     ap.add_argument("--no-track", action="store_true", help="skip the MPC tracking leg")
+    ap.add_argument("--sqp-graph", type=int, default=1, choices=[0, 1, 2],
+                    help="0 host loop, 1 one graph per solve, 2 graph with two concurrent half-batch branches")
     ap.add_argument("--track-sqp-iters", type=int, default=4,
                     help="SQP iterations per solve in the tracking leg (stands in for the wall-clock cap)")
     ap.add_argument("--track-period-us", type=float, default=2000.0, help="plant time per control update")
@@ -233,7 +235,8 @@ def main():
     batch = P.make_batch(Ns, seed0=ids[0], dt=SPEC["timestep"])
     sv = gpt.Solver(max_knot_points=N, max_batch=B, **SPEC)
     sv.set_solver(sqp_max_iter=args.sqp_max_iter, pcg_max_iter=args.pcg_max_iter, pcg_exit_tol=args.tol,
-                  pcg_exit_mode=0, pcg_cluster_size=args.pcg_cluster, pcg_precond=args.pcg_precond)
+                  pcg_exit_mode=0, pcg_cluster_size=args.pcg_cluster, pcg_precond=args.pcg_precond,
+                  sqp_graph=args.sqp_graph)
     stream = torch.cuda.current_stream()
     xu0 = torch.as_tensor(batch["xu"], device="cuda")
     goal = torch.as_tensor(batch["goal"], device="cuda")

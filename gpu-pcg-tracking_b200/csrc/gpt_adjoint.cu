@@ -72,7 +72,7 @@ __global__ void __launch_bounds__(32 * ADJ_WARPS)
     AdjWarpSmem &sm = smem_all[threadIdx.x >> 5];
     const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nw = (gridDim.x * blockDim.x) >> 5;
-    for (int j = gw; j < bv.total_knots; j += nw) {
+    for (int j = bv.j0 + gw; j < bv.j0 + bv.total_knots; j += nw) {
         const int b = bv.inst(j);
         if (!bv.active(b)) continue;
         const int N = bv.N(b), k = j - bv.off(b);
@@ -196,8 +196,8 @@ __global__ void __launch_bounds__(32 * ADJ_WARPS)
 __global__ void adjoint_reduce_kernel(BatchView bv, const float *__restrict__ part, float *__restrict__ grad_qd,
                                       float *__restrict__ grad_r, float *__restrict__ grad_qee)
 {
-    const int b = blockIdx.x;
-    if (b >= bv.B || !bv.active(b)) return;
+    const int b = bv.b0 + (int)blockIdx.x;
+    if (b >= bv.b0 + bv.B || !bv.active(b)) return;
     const int t = threadIdx.x;  // 0..14
     if (t >= 15) return;
     const int N = bv.N(b), kb = bv.off(b);

@@ -48,6 +48,9 @@ struct BatchView {
     const int *knot_off;     // [B+1] prefix offsets, nullptr => single instance of total_knots
     const int *knot_inst;    // [total_knots] owning instance, nullptr => single instance
     InstState *st;           // [B] or nullptr (always active)
+    // A view of a contiguous sub-range of a batch: instances b0 .. b0+B-1, owning knots
+    // j0 .. j0+total_knots-1.  Instance and knot indices stay those of the whole batch.
+    int j0 = 0, b0 = 0;
 
     __device__ __forceinline__ int inst(int j) const { return knot_inst ? knot_inst[j] : 0; }
     __device__ __forceinline__ int off(int b) const { return knot_off ? knot_off[b] : 0; }

@@ -54,8 +54,8 @@ __global__ void __launch_bounds__(32 * KKT_WARPS) kkt_kernel(BatchView bv, Probl
     const int nw = (gridDim.x * blockDim.x) >> 5;
 
     for (int jp = gw; 2 * jp < bv.total_knots; jp += nw) {
-        const int j = 2 * jp + half;
-        bool valid = j < bv.total_knots;
+        const int j = bv.j0 + 2 * jp + half;
+        bool valid = j < bv.j0 + bv.total_knots;
         int b = 0, N = 2, k = 0;
         if (valid) {
             b = bv.inst(j);
@@ -63,7 +63,7 @@ __global__ void __launch_bounds__(32 * KKT_WARPS) kkt_kernel(BatchView bv, Probl
             k = j - bv.off(b);
             valid = (k < N - 1) && bv.active(b);
         }
-        const int jj = valid ? j : 0;  // knot 0 always has a successor (N >= 2)
+        const int jj = valid ? j : bv.j0;  // the view's first knot always has a successor (N >= 2)
         const bool terminal = valid && (k == N - 2);
 
         // ---- stage x_k, u_k, x_{k+1}, goal_k, goal_{k+1}

@@ -38,7 +38,7 @@ __global__ void __launch_bounds__(32 * DZ_WARPS)
     DzWarpSmem &sm = sm_all[threadIdx.x >> 5];
     const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nw = (gridDim.x * blockDim.x) >> 5;
-    for (int j = gw; j < bv.total_knots; j += nw) {
+    for (int j = bv.j0 + gw; j < bv.j0 + bv.total_knots; j += nw) {
         const int b = bv.inst(j);
         if (!bv.active(b)) continue;
         const int N = bv.N(b), k = j - bv.off(b);
@@ -156,7 +156,7 @@ __global__ void __launch_bounds__(32 * MERIT_WARPS)
     MeritWarpSmem &sm = smem_all[threadIdx.x >> 5];
     const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nw = (gridDim.x * blockDim.x) >> 5;
-    for (int j = gw; j < bv.total_knots; j += nw) {
+    for (int j = bv.j0 + gw; j < bv.j0 + bv.total_knots; j += nw) {
         const int b = bv.inst(j);
         if (!bv.active(b)) continue;
         const int N = bv.N(b), k = j - bv.off(b);
@@ -329,7 +329,7 @@ __global__ void __launch_bounds__(ACC_THREADS)
 {
     __shared__ double scratch[NUM_ALPHAS * (ACC_THREADS / 32) + NUM_ALPHAS];
     __shared__ float s_alpha;
-    for (int b = blockIdx.x; b < bv.B; b += gridDim.x) {
+    for (int b = bv.b0 + blockIdx.x; b < bv.b0 + bv.B; b += gridDim.x) {
         if (!bv.active(b)) continue;
         const int N = bv.N(b), kb = bv.off(b);
         float m[NUM_ALPHAS];
@@ -403,7 +403,7 @@ cudaError_t launch_accept(const BatchView &bv, int mode, const SolverParams &SP,
 // Per-instance start of a solve: x_s = x_0 (toplevel.cuh:110), state from the host image.
 __global__ void init_kernel(BatchView bv, const float *__restrict__ xu, float *__restrict__ xs)
 {
-    for (int b = blockIdx.x; b < bv.B; b += gridDim.x) {
+    for (int b = bv.b0 + blockIdx.x; b < bv.b0 + bv.B; b += gridDim.x) {
         const int kb = bv.off(b);
         if (threadIdx.x < NS) xs[(size_t)NS * b + threadIdx.x] = xu[(size_t)NX * kb + threadIdx.x];
     }

@@ -210,10 +210,10 @@ __global__ void __launch_bounds__(PCG_THREADS, 1)
     c.red = c.slots + 2 * SLOT_CS * 4;
 
     const int tid = threadIdx.x;
-    const int b = blockIdx.x / CS;
+    const int b = bv.b0 + (int)blockIdx.x / CS;
     int rank = 0;
     if constexpr (CS > 1) rank = (int)cg::this_cluster().block_rank();
-    if (b >= bv.B || !bv.active(b)) return;  // uniform over the cluster
+    if (b >= bv.b0 + bv.B || !bv.active(b)) return;  // uniform over the cluster
     const int N = bv.N(b), kb = bv.off(b);
     const int k0 = (rank * N) / CS, k1 = ((rank + 1) * N) / CS, kpc = k1 - k0;
     // chunk size of the left neighbour (its right halo slot is kpc_left + 1)
@@ -581,10 +581,10 @@ __global__ void __launch_bounds__(PCG_THREADS, 1)
     double *red = slots + CH_SLOTS;
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int b = blockIdx.x / CS;
+    const int b = bv.b0 + (int)blockIdx.x / CS;
     int rank = 0;
     if constexpr (CS > 1) rank = (int)cg::this_cluster().block_rank();
-    if (b >= bv.B || !bv.active(b)) return;  // uniform over the cluster
+    if (b >= bv.b0 + bv.B || !bv.active(b)) return;  // uniform over the cluster
     const int N = bv.N(b), kb = bv.off(b);
     const int k0 = (rank * N) / CS, k1 = ((rank + 1) * N) / CS, kpc = k1 - k0;
     const int kpc_left = (rank > 0) ? k0 - ((rank - 1) * N) / CS : 0;
@@ -1168,8 +1168,8 @@ __global__ void __launch_bounds__(PAIR_THREADS, 4)
     using ST = typename std::conditional<FMT == 2, double, float>::type;
     const ST *S = reinterpret_cast<const ST *>(Sv);
     const size_t ks = FMT == 2 ? PK64 : PK;
-    const int b = blockIdx.x;
-    if (b >= bv.B || !bv.active(b)) return;
+    const int b = bv.b0 + (int)blockIdx.x;
+    if (b >= bv.b0 + bv.B || !bv.active(b)) return;
     const int n = bv.N(b), m = (n - 1) / 2, nv = NS * n;
     const size_t kg0 = (size_t)bv.off(b);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;

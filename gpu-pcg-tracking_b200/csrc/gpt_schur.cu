@@ -110,7 +110,7 @@ __global__ void __launch_bounds__(32 * SCHUR_WARPS)
     const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nw = (gridDim.x * blockDim.x) >> 5;
 
-    for (int j = gw; j < bv.total_knots; j += nw) {
+    for (int j = bv.j0 + gw; j < bv.j0 + bv.total_knots; j += nw) {
         const int b = bv.inst(j);
         if (!bv.active(b)) continue;
         const int N = bv.N(b);
@@ -379,7 +379,7 @@ __global__ void __launch_bounds__(32 * SCHUR_WARPS)
     const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nw = (gridDim.x * blockDim.x) >> 5;
 
-    for (int j = gw; j < bv.total_knots; j += nw) {
+    for (int j = bv.j0 + gw; j < bv.j0 + bv.total_knots; j += nw) {
         const int b = bv.inst(j);
         if (!bv.active(b)) continue;
         const int N = bv.N(b);

@@ -491,31 +491,36 @@ def test_sqp_warp_pair_pcg_matches_chain(gpt, problem_mod, schur_fp64, exit_mode
             off += n
 
 
-def test_sqp_graph_equals_host_loop(gpt, problem_mod):
-    """The solve as one CUDA graph (device-side while loop, the default) and the
-    host-driven loop give bit-identical results, on the first call of a batch shape
-    (capture) and on later calls (the cached graph), for a batch whose instances stop
-    at different SQP iterations."""
-    Ns = [16, 24, 32]
+@pytest.mark.parametrize("cluster", [1, 32])
+def test_sqp_graph_equals_host_loop(gpt, problem_mod, cluster):
+    """The solve as one CUDA graph (device-side while loop, the default), the graph with
+    the batch split in two halves on concurrent branches (sqp_graph 2: halves of 2 and
+    3 instances of uneven horizon) and the host-driven loop give bit-identical results,
+    on the first call of a batch shape (capture) and on later calls (the cached graph),
+    for a batch whose instances stop at different SQP iterations; with the chain and
+    the warp-pair PCG kernels."""
+    Ns = [16, 24, 32, 8, 20]
     ps = [problem_mod.make_problem(n, 40 + i, dt=0.01) for i, n in enumerate(Ns)]
     cat = lambda key, pad: np.concatenate([np.concatenate([p[key], np.zeros(pad, np.float32)]) for p in ps])
     goal, xu0, lam0 = dev(cat("goal", 0)), dev(cat("xu", 7)), dev(cat("lam", 0))
     out = {}
-    for graph in (0, 1):
-        sv = gpt.Solver(max_knot_points=32, max_batch=3, **SPEC_CFG)
-        sv.set_solver(sqp_graph=graph, sqp_max_iter=12, pcg_cluster_size=1)
+    B = len(Ns)
+    for graph in (0, 1, 2):
+        sv = gpt.Solver(max_knot_points=32, max_batch=B, **SPEC_CFG)
+        sv.set_solver(sqp_graph=graph, sqp_max_iter=12, pcg_cluster_size=cluster)
         res = []
         for rep in range(2):
             xu, lam = xu0.clone(), lam0.clone()
-            rho, stats = sv.sqp_solve_batched(Ns, goal, lam, xu, [1e-3] * 3)
+            rho, stats = sv.sqp_solve_batched(Ns, goal, lam, xu, [1e-3] * B)
             res.append((host(xu), host(lam), rho, [s["sqp_iters"] for s in stats]))
         sv.close()
         out[graph] = res
-    for rep in range(2):
-        (x0, l0, r0, i0), (x1, l1, r1, i1) = out[0][rep], out[1][rep]
-        assert i0 == i1 and r0 == r1, (i0, i1, r0, r1)
-        np.testing.assert_array_equal(x0, x1)
-        np.testing.assert_array_equal(l0, l1)
+    for graph in (1, 2):
+        for rep in range(2):
+            (x0, l0, r0, i0), (x1, l1, r1, i1) = out[0][rep], out[graph][rep]
+            assert i0 == i1 and r0 == r1, (graph, i0, i1, r0, r1)
+            np.testing.assert_array_equal(x0, x1)
+            np.testing.assert_array_equal(l0, l1)
 
 
 def test_autotune_choice_is_used(gpt, problem_mod):
