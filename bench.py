@@ -64,8 +64,8 @@ def parse():
                     help="0 block-Jacobi (the reference's), 1 block-tridiagonal LDL^T per CTA chunk")
     ap.add_argument("--batched-only", action="store_true", help="skip the e2e and plain legs (profiling runs)")
     ap.add_argument("--no-track", action="store_true", help="skip the MPC tracking leg")
-    ap.add_argument("--sqp-graph", type=int, default=1, choices=[0, 1, 2],
-                    help="0 host loop, 1 one graph per solve, 2 graph with two concurrent half-batch branches")
+    ap.add_argument("--sqp-graph", type=int, default=2, choices=range(0, 9),
+                    help="0 host loop, 1 one graph per solve, K = 2..8 graph with K concurrent part-batch branches")
     ap.add_argument("--track-sqp-iters", type=int, default=4,
                     help="SQP iterations per solve in the tracking leg (stands in for the wall-clock cap)")
     ap.add_argument("--track-period-us", type=float, default=2000.0, help="plant time per control update")

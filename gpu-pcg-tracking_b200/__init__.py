@@ -11,6 +11,7 @@ The directory name contains hyphens, so import it with
 """
 from __future__ import annotations
 
+import collections.abc
 import ctypes as C
 import os
 import subprocess
@@ -80,6 +81,22 @@ class TrackStats(C.Structure):
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class StatsList(collections.abc.Sequence):
+    """Per-instance stats of a batched call, converted to dicts on access (a batch of
+    hundreds of instances costs milliseconds of host time to convert eagerly)."""
+
+    def __init__(self, arr):
+        self._arr = arr
+
+    def __len__(self):
+        return len(self._arr)
+
+    def __getitem__(self, i):
+        if isinstance(i, slice):
+            return [self._arr[j].as_dict() for j in range(*i.indices(len(self._arr)))]
+        return self._arr[i].as_dict()
 
 
 class GptError(RuntimeError):
@@ -290,7 +307,7 @@ class Solver:
         _check(lib().gpt_sqp_solve_batched(self._h, B, C.cast(Ns, C.c_void_p), _ptr(eePos_traj), _ptr(lam),
                                            _ptr(xu), C.cast(rr, C.c_void_p), rho_reset, C.cast(sts, C.c_void_p),
                                            _stream(stream)))
-        return list(rr), [s.as_dict() for s in sts]
+        return list(rr), StatsList(sts)
 
     def autotune(self, knot_points: Sequence[int], eePos_traj, lam, xu, rho: Sequence[float], stream=None) -> int:
         """gpt_autotune: pick and remember the fastest PCG cluster size for this batch shape."""
@@ -351,7 +368,7 @@ class Solver:
                                        _ptr(xu_traj), _ptr(xs), None if config is None else C.byref(config),
                                        _ptr(errors), _ptr(sqp_iters_log), log_capacity, C.cast(sts, C.c_void_p),
                                        _stream(stream)))
-        return errors, [s.as_dict() for s in sts]
+        return errors, StatsList(sts)
 
     def simulate(self, knot_points: int, xs, xu, time_offset_us: float, sim_time_us: float, sim_step: float = 2e-4,
                  stream=None):

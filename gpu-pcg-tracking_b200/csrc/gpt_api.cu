@@ -36,9 +36,11 @@ gpt_status cuda_err(cudaError_t e, const char *where)
 
 }  // namespace
 
+constexpr int MAX_BRANCHES = 8;  // most concurrent part-batch branches of a graph iteration (sqp_graph)
+
 struct GraphKey {
     int B, total, maxN, minN;
-    int split[5];  // sqp_graph 2: first knot of the second half, longest / shortest horizon per half
+    int split[3 * MAX_BRANCHES];  // sqp_graph >= 2: per branch its first knot, longest and shortest horizon
     ProblemParams P;
     SolverParams SP;
 };
@@ -81,8 +83,10 @@ struct gpt_handle {
     TrackInst *trk_inst = nullptr;
     int *h_trk_rows = nullptr;
     TrackInst *h_trk_inst = nullptr;
-    cudaStream_t cap_stream = nullptr, body_stream = nullptr, body_stream2 = nullptr;
-    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;  // the two half-batch branches of a graph iteration
+    cudaStream_t cap_stream = nullptr, body_stream = nullptr;
+    // the part-batch branches of a graph iteration (sqp_graph >= 2): streams 1.. and their events
+    cudaStream_t branch_stream[MAX_BRANCHES] = {};
+    cudaEvent_t ev_fork = nullptr, ev_join[MAX_BRANCHES] = {};
     std::vector<GraphEntry> graphs;
     // autotuned PCG cluster size per batch shape (gpt_autotune); used when pcg_cluster_size is 0
     struct Tuned {
@@ -212,7 +216,7 @@ gpt_status gpt_set_solver_config(gpt_handle *h, const gpt_solver_config *sc)
     }
     if (sc->pcg_precond > 1) return set_err(GPT_ERR_BAD_ARG, "pcg_precond must be 0 or 1");
     if (sc->schur_fp64 > 1) return set_err(GPT_ERR_BAD_ARG, "schur_fp64 must be 0 or 1");
-    if (sc->sqp_graph > 2) return set_err(GPT_ERR_BAD_ARG, "sqp_graph must be 0, 1 or 2");
+    if (sc->sqp_graph > (uint32_t)MAX_BRANCHES) return set_err(GPT_ERR_BAD_ARG, "sqp_graph must be 0 .. 8");
     if (sc->sqp_max_iter > h->cap_sqp_iter) {
         // pcg log is sized at creation
         return set_err(GPT_ERR_CAPACITY, "sqp_max_iter larger than at creation");
@@ -300,9 +304,11 @@ gpt_status gpt_create(const gpt_problem_config *pc, const gpt_solver_config *sc,
     ALLOC(trk_inst, B);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->cap_stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->body_stream, cudaStreamNonBlocking);
-    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->body_stream2, cudaStreamNonBlocking);
+    for (int i = 1; i < MAX_BRANCHES; ++i) {
+        if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->branch_stream[i], cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->ev_join[i], cudaEventDisableTiming);
+    }
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming);
-    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming);
 #undef ALLOC
     if (e == cudaSuccess) e = cudaMallocHost((void **)&h->h_active, sizeof(uint32_t));
     if (e == cudaSuccess) e = cudaMallocHost((void **)&h->h_st, sizeof(InstState) * B);
@@ -360,9 +366,11 @@ gpt_status gpt_destroy(gpt_handle *h)
     cudaFreeHost(h->h_trk_rows); cudaFreeHost(h->h_trk_inst);
     if (h->cap_stream) cudaStreamDestroy(h->cap_stream);
     if (h->body_stream) cudaStreamDestroy(h->body_stream);
-    if (h->body_stream2) cudaStreamDestroy(h->body_stream2);
+    for (int i = 1; i < MAX_BRANCHES; ++i) {
+        if (h->branch_stream[i]) cudaStreamDestroy(h->branch_stream[i]);
+        if (h->ev_join[i]) cudaEventDestroy(h->ev_join[i]);
+    }
     if (h->ev_fork) cudaEventDestroy(h->ev_fork);
-    if (h->ev_join) cudaEventDestroy(h->ev_join);
     cudaFreeHost(h->h_active); cudaFreeHost(h->h_st); cudaFreeHost(h->h_pcg_out); cudaFreeHost(h->h_pcg_log);
     if (h->ev) cudaEventDestroy(h->ev);
     delete h;
@@ -643,25 +651,26 @@ static gpt_status enqueue_iteration(gpt_handle *h, const SqpPlan &pl, const floa
     return GPT_OK;
 }
 
-// sqp_graph 2: the batch as two halves (instances [0, B/2) and [B/2, B)) whose iterations run on two
-// branches of the graph, so that one half's latency-bound PCG overlaps the other half's
-// throughput-bound KKT, Schur and merit kernels.  The halves share no workspace (every buffer is
-// indexed by the batch's knot or instance); the active count is cleared once before both.
-static bool use_split(const gpt_handle *h, const SqpPlan &pl)
+// sqp_graph K >= 2: the batch as K parts (contiguous instance ranges of near-equal size) whose
+// iterations run on K branches of the graph, so that one part's latency-bound PCG overlaps the
+// others' throughput-bound KKT, Schur and merit kernels.  The parts share no workspace (every
+// buffer is indexed by the batch's knot or instance); the active count is cleared once before all.
+static int branch_count(const gpt_handle *h, const SqpPlan &pl)
 {
-    return pl.SP.sqp_graph == 2 && pl.bv.B >= 2 && pl.bv.knot_off != nullptr &&
-           h->off_cache.size() == (size_t)pl.bv.B + 1;
+    if (pl.SP.sqp_graph < 2 || pl.bv.knot_off == nullptr || h->off_cache.size() != (size_t)pl.bv.B + 1) return 1;
+    int k = (int)pl.SP.sqp_graph;
+    k = k < MAX_BRANCHES ? k : MAX_BRANCHES;
+    return k < pl.bv.B ? k : pl.bv.B;
 }
 
-static void split_plan(const gpt_handle *h, const SqpPlan &pl, SqpPlan (&half)[2])
+static void split_plan(const gpt_handle *h, const SqpPlan &pl, int K, SqpPlan *part)
 {
     const std::vector<int> &off = h->off_cache;
-    const int B = pl.bv.B, bh = B / 2;
-    half[0] = pl;
-    half[1] = pl;
-    for (int i = 0; i < 2; ++i) {
-        const int b0 = i == 0 ? 0 : bh, b1 = i == 0 ? bh : B;
-        BatchView &v = half[i].bv;
+    const int B = pl.bv.B;
+    for (int i = 0; i < K; ++i) {
+        const int b0 = (int)((int64_t)B * i / K), b1 = (int)((int64_t)B * (i + 1) / K);
+        part[i] = pl;
+        BatchView &v = part[i].bv;
         v.b0 = b0;
         v.B = b1 - b0;
         v.j0 = off[b0];
@@ -672,24 +681,27 @@ static void split_plan(const gpt_handle *h, const SqpPlan &pl, SqpPlan (&half)[2
             mx = n > mx ? n : mx;
             mn = n < mn ? n : mn;
         }
-        half[i].maxN = mx;
-        half[i].minN = mn;
+        part[i].maxN = mx;
+        part[i].minN = mn;
     }
 }
 
-static gpt_status enqueue_iteration_split(gpt_handle *h, const SqpPlan &pl, cudaStream_t s)
+static gpt_status enqueue_iteration_split(gpt_handle *h, const SqpPlan &pl, int K, cudaStream_t s)
 {
-    SqpPlan half[2];
-    split_plan(h, pl, half);
+    SqpPlan part[MAX_BRANCHES];
+    split_plan(h, pl, K, part);
     GPT_CUDA(cudaMemsetAsync(h->d_active, 0, sizeof(uint32_t), s));
     GPT_CUDA(cudaEventRecord(h->ev_fork, s));
-    GPT_CUDA(cudaStreamWaitEvent(h->body_stream2, h->ev_fork, 0));
-    gpt_status st = enqueue_iteration(h, half[0], h->ggoal, h->glam, h->gxu, s, false);
-    if (st != GPT_OK) return st;
-    st = enqueue_iteration(h, half[1], h->ggoal, h->glam, h->gxu, h->body_stream2, false);
-    if (st != GPT_OK) return st;
-    GPT_CUDA(cudaEventRecord(h->ev_join, h->body_stream2));
-    GPT_CUDA(cudaStreamWaitEvent(s, h->ev_join, 0));
+    for (int i = 1; i < K; ++i) GPT_CUDA(cudaStreamWaitEvent(h->branch_stream[i], h->ev_fork, 0));
+    for (int i = 0; i < K; ++i) {
+        const gpt_status st =
+            enqueue_iteration(h, part[i], h->ggoal, h->glam, h->gxu, i == 0 ? s : h->branch_stream[i], false);
+        if (st != GPT_OK) return st;
+    }
+    for (int i = 1; i < K; ++i) {
+        GPT_CUDA(cudaEventRecord(h->ev_join[i], h->branch_stream[i]));
+        GPT_CUDA(cudaStreamWaitEvent(s, h->ev_join[i], 0));
+    }
     return GPT_OK;
 }
 
@@ -715,14 +727,15 @@ static gpt_status sqp_graph_for(gpt_handle *h, const SqpPlan &pl, cudaGraphExec_
     key.total = pl.bv.total_knots;
     key.maxN = pl.maxN;
     key.minN = pl.minN;
-    if (use_split(h, pl)) {
-        SqpPlan half[2];
-        split_plan(h, pl, half);
-        key.split[0] = half[1].bv.j0;
-        key.split[1] = half[0].maxN;
-        key.split[2] = half[0].minN;
-        key.split[3] = half[1].maxN;
-        key.split[4] = half[1].minN;
+    const int K = branch_count(h, pl);
+    if (K > 1) {
+        SqpPlan part[MAX_BRANCHES];
+        split_plan(h, pl, K, part);
+        for (int i = 0; i < K; ++i) {
+            key.split[3 * i] = part[i].bv.j0;
+            key.split[3 * i + 1] = part[i].maxN;
+            key.split[3 * i + 2] = part[i].minN;
+        }
     }
     key.P = pl.P;
     key.SP = pl.SP;
@@ -755,8 +768,8 @@ static gpt_status sqp_graph_for(gpt_handle *h, const SqpPlan &pl, cudaGraphExec_
             cudaGraph_t body = cp.conditional.phGraph_out[0];
             e = cudaStreamBeginCaptureToGraph(bs, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed);
             if (e == cudaSuccess) {
-                st = use_split(h, pl) ? enqueue_iteration_split(h, pl, bs)
-                                      : enqueue_iteration(h, pl, h->ggoal, h->glam, h->gxu, bs);
+                st = K > 1 ? enqueue_iteration_split(h, pl, K, bs)
+                           : enqueue_iteration(h, pl, h->ggoal, h->glam, h->gxu, bs);
                 if (st == GPT_OK) {
                     sqp_continue_kernel<<<1, 1, 0, bs>>>(cond, h->d_active, h->d_iter, pl.SP.sqp_max_iter);
                     e = cudaGetLastError();

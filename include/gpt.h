@@ -90,11 +90,11 @@ typedef struct gpt_solver_config {
                                   FP32 formation moves the solution by ~cond(S) x 1e-7 (~1e-2 at cond 1e7) */
     uint32_t sqp_graph;        /* 1 (default): a solve runs as one CUDA graph (built on the first call of each
                                   batch shape and cached) whose while node repeats the SQP iteration on the
-                                  device; 2: the same graph with the batch split in two halves whose iterations
-                                  run on concurrent branches (one half's PCG overlaps the other's KKT, Schur and
-                                  merit kernels; identical results); 0: one host synchronisation per SQP
-                                  iteration, as the reference loop.  Profiling (gpt_set_profiling) uses the
-                                  host loop. */
+                                  device; K = 2 .. 8: the same graph with the batch split in K parts whose
+                                  iterations run on concurrent branches (one part's PCG overlaps the others'
+                                  KKT, Schur and merit kernels; identical results); 0: one host
+                                  synchronisation per SQP iteration, as the reference loop.  Profiling
+                                  (gpt_set_profiling) uses the host loop. */
 } gpt_solver_config;
 
 /* One sqpSolve's outcome (the reference returns a tuple, toplevel.cuh:502) */

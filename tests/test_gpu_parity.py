@@ -494,8 +494,8 @@ def test_sqp_warp_pair_pcg_matches_chain(gpt, problem_mod, schur_fp64, exit_mode
 @pytest.mark.parametrize("cluster", [1, 32])
 def test_sqp_graph_equals_host_loop(gpt, problem_mod, cluster):
     """The solve as one CUDA graph (device-side while loop, the default), the graph with
-    the batch split in two halves on concurrent branches (sqp_graph 2: halves of 2 and
-    3 instances of uneven horizon) and the host-driven loop give bit-identical results,
+    the batch split in parts on concurrent branches (sqp_graph 2: 2 + 3 instances of
+    uneven horizon; 4: 1 + 1 + 1 + 2) and the host-driven loop give bit-identical results,
     on the first call of a batch shape (capture) and on later calls (the cached graph),
     for a batch whose instances stop at different SQP iterations; with the chain and
     the warp-pair PCG kernels."""
@@ -505,7 +505,7 @@ def test_sqp_graph_equals_host_loop(gpt, problem_mod, cluster):
     goal, xu0, lam0 = dev(cat("goal", 0)), dev(cat("xu", 7)), dev(cat("lam", 0))
     out = {}
     B = len(Ns)
-    for graph in (0, 1, 2):
+    for graph in (0, 1, 2, 4):
         sv = gpt.Solver(max_knot_points=32, max_batch=B, **SPEC_CFG)
         sv.set_solver(sqp_graph=graph, sqp_max_iter=12, pcg_cluster_size=cluster)
         res = []
@@ -515,7 +515,7 @@ def test_sqp_graph_equals_host_loop(gpt, problem_mod, cluster):
             res.append((host(xu), host(lam), rho, [s["sqp_iters"] for s in stats]))
         sv.close()
         out[graph] = res
-    for graph in (1, 2):
+    for graph in (1, 2, 4):
         for rep in range(2):
             (x0, l0, r0, i0), (x1, l1, r1, i1) = out[0][rep], out[graph][rep]
             assert i0 == i1 and r0 == r1, (graph, i0, i1, r0, r1)

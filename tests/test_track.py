@@ -166,7 +166,7 @@ def test_track_batched_equals_single_runs(gpt, golden):
     tr_all = np.concatenate([golden["traj_0_0"][st:st + S] for _, S, st in specs]).astype(np.float32)
     ee_all = np.concatenate([golden["eepos_0_0"][st:st + S] for _, S, st in specs]).astype(np.float32)
     xs0 = np.concatenate([golden["traj_0_0"][st, :14] for _, _, st in specs]).astype(np.float32)
-    for graph in (1, 2, 0):
+    for graph in (1, 2, 3, 0):
         sv = gpt.Solver(max_knot_points=16, max_batch=3, sqp_max_iter=3, sqp_graph=graph, **REF_CFG, **kw)
         try:
             xs = dev(xs0)
