@@ -41,7 +41,7 @@ PCG_BYTES_PER_KNOT = 8 * 302 + 8 * 14 + 2 * 4 * 14 + 8 * 14
 PCG_BJ_BYTES_PER_KNOT = 4 * 784  # block-Jacobi kernel: FP32 S (588) + Pinv (196) read once
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one launch, per knot, from ncu captures of
 # 148 instances x 128 knots; they scale with the knots of a launch
-PCG_DRAM_BYTES_PER_KNOT = {"pcg_pair_kernel": (52.677e6 + 2.764e6) / (148 * 128)}
+PCG_DRAM_BYTES_PER_KNOT = {"pcg_pair_kernel": (53.330432e6 + 3.051776e6) / (148 * 128)}
 ALG_FLOATS_PER_KNOT_SQP = 4058   # every materialised SQP-iteration tensor written once, read once
 
 
@@ -286,9 +286,11 @@ def main():
     one_step()
     sv.set_profiling(False)
     phases = sv.phase_stats(reset=True)
-    # kernels per timed step: the phases' launches plus the while loop's control kernel (one per
-    # SQP iteration, as many as the KKT launches)
-    launches_per_step = sum(n for _, n in phases.values()) + phases["kkt"][1]
+    # kernels per timed step of the graph: the prologue (init, merit, accept), then per SQP iteration
+    # (as many as the profiled step's KKT launches) the six phase kernels once per part-batch branch
+    # and the while loop's control kernel
+    branches = min(args.sqp_graph, B) if args.sqp_graph >= 2 else 1
+    launches_per_step = 3 + phases["kkt"][1] * (6 * branches + 1)
     total_ms = sum(step_ms)
     total_ms = shard.max_over_ranks(total_ms, device="cuda")
     ms_per_step = total_ms / args.steps
@@ -465,7 +467,8 @@ def main():
         "batched_over_plain": (value / world) / plain_rate if plain_rate else None,
         "phase_ms_per_step": {k: v[0] for k, v in phases.items()},
         "phase_launches_per_step": {k: v[1] for k, v in phases.items()},
-        "sqp_loop": "one CUDA graph per solve (device-side while loop); phase times from a profiled host-loop step",
+        "sqp_loop": (f"one CUDA graph per solve (device-side while loop), {branches} part-batch branch(es) per "
+                     f"iteration; phase times from a profiled host-loop step over the whole batch"),
         "sqp_iters_mean": statistics.mean(sqp_iters), "pcg_iters_per_solve": pcg_total / max(len(all_stats), 1),
         "pcg_iters_per_linsys": pcg_total / max(n_pcg_solves, 1), "pcg_maxiter_solves": pcg_maxit,
         "alg_bytes_per_sqp_iter_per_instance": 4 * N * ALG_FLOATS_PER_KNOT_SQP,
