@@ -40,8 +40,9 @@ constexpr int KKT_WARPS = 4;
 // Two knots per warp, one per half-warp (lanes hl = 0..15): the dynamics phases keep at most 14
 // lanes of a knot busy, so a knot per half-warp halves their instructions per knot.  A half-warp
 // without a knot (odd count, last knot of an instance, inactive instance) computes on knot 0's data
-// and writes nothing, so both halves take every __syncwarp.
-__global__ void __launch_bounds__(32 * KKT_WARPS) kkt_kernel(BatchView bv, ProblemParams P, const float *__restrict__ xu,
+// and writes nothing, so both halves take every __syncwarp.  Four CTAs per SM (16 warps; the
+// kernel fits 128 registers without spilling).
+__global__ void __launch_bounds__(32 * KKT_WARPS, 4) kkt_kernel(BatchView bv, ProblemParams P, const float *__restrict__ xu,
                                                            const float *__restrict__ goal,
                                                            const float *__restrict__ xs, float *__restrict__ G,
                                                            float *__restrict__ Cm, float *__restrict__ g,

@@ -367,7 +367,8 @@ struct Schur64WarpSmem {
     float Gm1[G_STRIDE], Gk[SS], C[C_STRIDE];
 };
 
-__global__ void __launch_bounds__(32 * SCHUR_WARPS)
+// Five CTAs per SM: the shared-memory limit (43 KB per CTA); the registers fit without spilling.
+__global__ void __launch_bounds__(32 * SCHUR_WARPS, 5)
     schur64_kernel(BatchView bv, const float *__restrict__ G, const float *__restrict__ Cm,
                    const float *__restrict__ g, const float *__restrict__ c, double *__restrict__ S64,
                    double *__restrict__ gamma64, float *__restrict__ Ginv, double *__restrict__ Ginv64)
