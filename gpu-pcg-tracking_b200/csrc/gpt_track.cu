@@ -292,7 +292,9 @@ cudaError_t launch_track_tail(const BatchView &bv, const int *rows, TrackClock *
     track_clock_kernel<<<1, 1, 0, s>>>(clk, tp);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    track_sim_kernel<<<(bv.B * 8 + 127) / 128, 128, 0, s>>>(bv, rows, clk, tp, xs, xu_old);
+    // one warp (4 instances) per CTA: the kernel is a dependent chain per instance, so the
+    // instances spread over as many SMs as possible
+    track_sim_kernel<<<(bv.B + 3) / 4, 32, 0, s>>>(bv, rows, clk, tp, xs, xu_old);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     track_post_kernel<<<bv.B, POST_THREADS, 0, s>>>(bv, rows, clk, eePos_traj, xu_traj, xs, xu, xu_old, goal, lambda,
