@@ -36,6 +36,7 @@ EXPORTED = [
     "gpt_compute_merit", "gpt_ls_compute_merit", "gpt_set_profiling", "gpt_get_phase_stats",
     "gpt_ls_compute_merit_noalloc", "gpt_sqp_adjoint", "gpt_set_cost_weights", "gpt_autotune",
     "gpt_default_track_config", "gpt_track", "gpt_track_batched", "gpt_simulate",
+    "gpt_end_effector_positions", "gpt_forward_dynamics", "gpt_read_csv",
 ]
 PHASES = ["init", "kkt", "schur", "pcg", "dz", "merit", "accept"]
 
@@ -160,6 +161,9 @@ def _declare(L):
         "gpt_track": ([vp, u32, u32, vp, vp, vp, P(TrackConfig), vp, vp, u32, P(TrackStats), vp], C.c_int),
         "gpt_track_batched": ([vp, u32, vp, vp, vp, vp, vp, P(TrackConfig), vp, vp, u32, vp, vp], C.c_int),
         "gpt_simulate": ([vp, u32, vp, vp, C.c_double, C.c_double, f32, vp], C.c_int),
+        "gpt_end_effector_positions": ([u32, vp, u32, vp, vp], C.c_int),
+        "gpt_forward_dynamics": ([u32, vp, u32, vp, vp], C.c_int),
+        "gpt_read_csv": ([C.c_char_p, vp, C.c_size_t, P(u32), P(u32)], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -194,6 +198,37 @@ def default_track_config(**kw) -> TrackConfig:
     for k, v in kw.items():
         setattr(tc, k, v)
     return tc
+
+
+def end_effector_positions(x, row_stride: int, out=None, stream=None):
+    """gpt_end_effector_positions: xyz + roll/pitch/yaw of every row of x (CUDA tensor, rows of
+    row_stride floats starting with q) -> tensor [rows, 6]."""
+    import torch
+    n = x.numel() // row_stride
+    if out is None:
+        out = torch.empty(n, 6, device=x.device)
+    _check(lib().gpt_end_effector_positions(n, _ptr(x), row_stride, _ptr(out), _stream(stream)))
+    return out
+
+
+def forward_dynamics(xu, row_stride: int = 21, out=None, stream=None):
+    """gpt_forward_dynamics: qdd of every row [q, qd, u] of xu (CUDA tensor) -> tensor [rows, 7]."""
+    import torch
+    n = xu.numel() // row_stride
+    if out is None:
+        out = torch.empty(n, 7, device=xu.device)
+    _check(lib().gpt_forward_dynamics(n, _ptr(xu), row_stride, _ptr(out), _stream(stream)))
+    return out
+
+
+def read_csv(path: str):
+    """gpt_read_csv (readCSVToVecVec, runme.cu:18-44): a float32 numpy array [rows, cols]."""
+    import numpy as np
+    r, c = C.c_uint32(0), C.c_uint32(0)
+    _check(lib().gpt_read_csv(path.encode(), None, 0, C.byref(r), C.byref(c)))
+    out = np.zeros((r.value, c.value), np.float32)
+    _check(lib().gpt_read_csv(path.encode(), out.ctypes.data_as(C.c_void_p), out.size, C.byref(r), C.byref(c)))
+    return out
 
 
 NOALLOC_MAX_KNOTS = 512  # GPT_NOALLOC_MAX_KNOTS

@@ -1,8 +1,10 @@
 // gpt_api.cu -- the C ABI (include/gpt.h): handle, preallocated workspace,
 // the reference's kernels as single-instance entry points, and the SQP loop
 // (toplevel.cuh:24-503) driven from the host with every decision on the device.
+#include <algorithm>
 #include <cstdint>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -1234,6 +1236,80 @@ gpt_status gpt_simulate(gpt_handle *h, uint32_t N, float *d_xs, const float *d_x
         return set_err(GPT_ERR_BAD_ARG, "sim_step must be positive, times non-negative, <= 1e6 plant steps");
     const TrackParams tp = track_params(h->pc.timestep, sim_step, 0.f, sim_time_us);
     GPT_CUDA(launch_simulate_one((int)N, tp, time_offset_us, d_xs, d_xu, (cudaStream_t)stream));
+    return GPT_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// rigid-body library kernels and trajectory files
+// ---------------------------------------------------------------------------
+
+extern "C" {
+
+gpt_status gpt_end_effector_positions(uint32_t n, const float *d_x, uint32_t stride, float *d_pose,
+                                      gpt_stream_t stream)
+{
+    if (n == 0) return GPT_OK;
+    if (!d_x || !d_pose) return set_err(GPT_ERR_BAD_ARG, "null argument");
+    if (stride < 7 || n > (1u << 28)) return set_err(GPT_ERR_BAD_ARG, "row_stride must be >= 7 and n <= 2^28");
+    GPT_CUDA(launch_ee_pose(n, d_x, stride, d_pose, (cudaStream_t)stream));
+    return GPT_OK;
+}
+
+gpt_status gpt_forward_dynamics(uint32_t n, const float *d_xu, uint32_t stride, float *d_qdd, gpt_stream_t stream)
+{
+    if (n == 0) return GPT_OK;
+    if (!d_xu || !d_qdd) return set_err(GPT_ERR_BAD_ARG, "null argument");
+    if (stride < (uint32_t)NX || n > (1u << 28)) return set_err(GPT_ERR_BAD_ARG, "row_stride must be >= 21 and n <= 2^28");
+    GPT_CUDA(launch_fd(n, d_xu, stride, d_qdd, (cudaStream_t)stream));
+    return GPT_OK;
+}
+
+gpt_status gpt_read_csv(const char *path, float *h_out, size_t capacity, uint32_t *h_rows, uint32_t *h_cols)
+{
+    if (!path || !h_rows || !h_cols) return set_err(GPT_ERR_BAD_ARG, "null argument");
+    *h_rows = 0;
+    *h_cols = 0;
+    FILE *f = std::fopen(path, "r");
+    if (!f) return set_err(GPT_ERR_BAD_ARG, std::string("cannot open ") + path);
+    std::vector<float> vals;
+    std::string line;
+    size_t rows = 0, cols = 0;
+    bool ragged = false;
+    int ch;
+    while (true) {
+        line.clear();
+        while ((ch = std::fgetc(f)) != EOF && ch != '\n') line.push_back((char)ch);
+        if (line.empty() && ch == EOF) break;
+        if (!line.empty() && line.back() == '\r') line.pop_back();
+        if (line.empty()) {
+            if (ch == EOF) break;
+            continue;
+        }
+        // comma-separated fields, each parsed from its leading float (std::stof); like
+        // std::getline(ss, val, ','), a trailing comma ends the row without an empty field
+        size_t n = 0, pos = 0;
+        while (pos < line.size()) {
+            const size_t end = line.find(',', pos);
+            const std::string field = line.substr(pos, end == std::string::npos ? std::string::npos : end - pos);
+            vals.push_back(std::strtof(field.c_str(), nullptr));
+            ++n;
+            if (end == std::string::npos) break;
+            pos = end + 1;
+        }
+        if (rows == 0) cols = n;
+        else if (n != cols) ragged = true;
+        ++rows;
+        if (ch == EOF) break;
+    }
+    std::fclose(f);
+    if (ragged) return set_err(GPT_ERR_BAD_ARG, "rows of unequal length");
+    *h_rows = (uint32_t)rows;
+    *h_cols = (uint32_t)cols;
+    if (!h_out) return GPT_OK;
+    if (capacity < vals.size()) return set_err(GPT_ERR_CAPACITY, "output capacity below rows x cols");
+    std::copy(vals.begin(), vals.end(), h_out);
     return GPT_OK;
 }
 

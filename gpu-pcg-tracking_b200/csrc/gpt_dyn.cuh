@@ -14,6 +14,7 @@
 // inverse_dynamics_gradient_inner :4558, end_effector_positions_inner :2015,
 // end_effector_positions_gradient_inner :2255).
 #pragma once
+#include "gpt_common.cuh"
 #include "gpt_model.cuh"
 
 namespace gpt {
@@ -312,6 +313,35 @@ __device__ __forceinline__ void gj7_group(double (&col)[7], int base)
     }
 }
 
+// Forward dynamics by a group of 8 lanes (lanes base .. base+7): lane m < 7 forms mass-matrix
+// column m by inverse dynamics, lane 7 the bias force c(q, qd); after an FP64 Gauss-Jordan on
+// [M | u - c] (M symmetrised from the lanes' columns) lane base+7's col holds qdd = M^{-1}(u - c).
+// Every lane of the warp calls it with its group's q, qd, u.
+__device__ __forceinline__ void fd_group(const float (&q)[NQ], const float (&qd)[NQ], const float (&u)[NC],
+                                         double (&col)[NQ], int m, int base)
+{
+    JointTrig t;
+    joint_trig(q, t);
+    float v[NQ], a[NQ], tau[NQ];
+#pragma unroll
+    for (int i = 0; i < NQ; ++i) {
+        v[i] = (m == 7) ? qd[i] : 0.f;
+        a[i] = (m == i) ? 1.f : 0.f;
+    }
+    rnea<false>(t, v, a, -1, -1, tau, nullptr);
+#pragma unroll
+    for (int r = 0; r < NQ; ++r) {
+        float mr = 0.f;  // M[m][r] = entry m of column r (lane base + r)
+#pragma unroll
+        for (int e = 0; e < NQ; ++e) {
+            const float ve = __shfl_sync(0xffffffffu, tau[e], base + r);
+            if (e == m) mr = ve;
+        }
+        col[r] = (m < NQ) ? 0.5 * ((double)tau[r] + (double)mr) : (double)u[r] - (double)tau[r];
+    }
+    gj7_group(col, base);
+}
+
 // Forward kinematics: end-effector position p (xyz) and, optionally, the
 // position Jacobian J (3x7, col-major: J[3*j + d]).  Joint j's axis in the
 // base frame is the third column of T_0...T_j; dp/dq_j = z_j x (p - o_j).
@@ -350,6 +380,30 @@ __device__ __forceinline__ void fk_step(const JointTrig &t, FkState &st)
         st.zs[J][0] = st.Rm[2]; st.zs[J][1] = st.Rm[5]; st.zs[J][2] = st.Rm[8];
         st.os[J][0] = st.o[0]; st.os[J][1] = st.o[1]; st.os[J][2] = st.o[2];
     }
+}
+
+// End-effector xyz and roll / pitch / yaw of the last frame (end_effector_positions_inner,
+// rbdfiles/iiwa_eepos_grid.cuh:2015-2090): roll = atan2(R21, R22),
+// pitch = -atan2(R20, sqrt(R21^2 + R22^2)), yaw = atan2(R10, R00)
+__device__ __forceinline__ void fk_pose_lane(const JointTrig &t, float *pose)
+{
+    FkState st;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) st.Rm[k] = (k % 4 == 0) ? 1.f : 0.f;
+    st.o[0] = st.o[1] = st.o[2] = 0.f;
+    fk_step<0, false>(t, st);
+    fk_step<1, false>(t, st);
+    fk_step<2, false>(t, st);
+    fk_step<3, false>(t, st);
+    fk_step<4, false>(t, st);
+    fk_step<5, false>(t, st);
+    fk_step<6, false>(t, st);
+    pose[0] = st.o[0];
+    pose[1] = st.o[1];
+    pose[2] = st.o[2];
+    pose[3] = atan2f(st.Rm[7], st.Rm[8]);
+    pose[4] = -atan2f(st.Rm[6], sqrtf(st.Rm[7] * st.Rm[7] + st.Rm[8] * st.Rm[8]));
+    pose[5] = atan2f(st.Rm[3], st.Rm[0]);
 }
 
 template <bool WITH_JAC>

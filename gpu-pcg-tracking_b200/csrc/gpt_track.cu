@@ -95,34 +95,13 @@ __global__ void track_clock_kernel(TrackClock *clk, TrackParams tp)
     *clk = c;
 }
 
-// One explicit-Euler plant step x <- x + h [qd; M^{-1}(u - c(q, qd))] by a group of 8 lanes:
-// lane m < 7 forms mass-matrix column m, lane 7 the bias force; Gauss-Jordan on [M | u - c].
-// Every lane holds the whole state (q, qd) and the control u.
+// One explicit-Euler plant step x <- x + h [qd; M^{-1}(u - c(q, qd))] by a group of 8 lanes
+// (fd_group).  Every lane holds the whole state (q, qd) and the control u.
 __device__ __forceinline__ void plant_step_group(float (&q)[NQ], float (&qd)[NQ], const float (&u)[NC], float h,
                                                  int m, int base)
 {
-    JointTrig t;
-    joint_trig(q, t);
-    float v[NQ], a[NQ], tau[NQ];
-#pragma unroll
-    for (int i = 0; i < NQ; ++i) {
-        v[i] = (m == 7) ? qd[i] : 0.f;
-        a[i] = (m == i) ? 1.f : 0.f;
-    }
-    rnea<false>(t, v, a, -1, -1, tau, nullptr);
-    // symmetrise M from the lanes' columns (lane base + r holds column r); lane 7 keeps u - c
     double col[NQ];
-#pragma unroll
-    for (int r = 0; r < NQ; ++r) {
-        float mr = 0.f;  // M[m][r] = entry m of column r
-#pragma unroll
-        for (int e = 0; e < NQ; ++e) {
-            const float ve = __shfl_sync(0xffffffffu, tau[e], base + r);
-            if (e == m) mr = ve;
-        }
-        col[r] = (m < NQ) ? 0.5 * ((double)tau[r] + (double)mr) : (double)u[r] - (double)tau[r];
-    }
-    gj7_group(col, base);
+    fd_group(q, qd, u, col, m, base);
 #pragma unroll
     for (int i = 0; i < NQ; ++i) {
         const float qdd = (float)__shfl_sync(0xffffffffu, col[i], base + 7);

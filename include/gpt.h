@@ -264,6 +264,28 @@ gpt_status gpt_track_batched(gpt_handle *h, uint32_t batch, const uint32_t *h_kn
 gpt_status gpt_simulate(gpt_handle *h, uint32_t knot_points, float *d_xs, const float *d_xu, double time_offset_us,
                         double sim_time_us, float sim_step, gpt_stream_t stream);
 
+/* ---- rigid-body library kernels and trajectory files (no handle) ---- */
+
+/* end_effector_positions_kernel (rbdfiles/iiwa_eepos_grid.cuh:2091-2110) for n rows at once (the
+ * reference launches it once per row, generateeepos.cu:101-107): the end-effector xyz and roll,
+ * pitch, yaw of joint vector d_x[i * row_stride + 0..6] -> d_eePos[6 i .. 6 i + 5].  row_stride 21
+ * reads the rows of a trajectory (x, u), 14 plain states. */
+gpt_status gpt_end_effector_positions(uint32_t n, const float *d_x, uint32_t row_stride, float *d_eePos,
+                                      gpt_stream_t stream);
+
+/* forward_dynamics (rbdfiles/iiwa_eepos_grid.cuh:4351-4395, gravity 0) for n rows at once:
+ * qdd = M(q)^{-1} (u - c(q, qd)) of the row [q (7), qd (7), u (7)] at d_xu[i * row_stride]
+ * -> d_qdd[7 i .. 7 i + 6]; row_stride >= 21. */
+gpt_status gpt_forward_dynamics(uint32_t n, const float *d_xu, uint32_t row_stride, float *d_qdd,
+                                gpt_stream_t stream);
+
+/* readCSVToVecVec (runme.cu:18-44, generateeepos.cu:14-40): a text file of comma-separated floats,
+ * one row per line, parsed like std::stof, flattened row by row into h_out (host).  *h_rows and
+ * *h_cols receive the shape; with h_out NULL only the shape is returned.  Rows of unequal length
+ * (GPT_ERR_BAD_ARG) and a capacity (in floats) below rows x cols (GPT_ERR_CAPACITY, shape still
+ * returned) are errors; an unreadable file is GPT_ERR_BAD_ARG. */
+gpt_status gpt_read_csv(const char *path, float *h_out, size_t capacity, uint32_t *h_rows, uint32_t *h_cols);
+
 /* ---- the reference's kernels, one instance, device buffers, stream-ordered ---- */
 
 /* gato_form_kkt (schur.cuh:391-524); d_xs = x_s (14) */
