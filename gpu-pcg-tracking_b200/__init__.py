@@ -36,7 +36,7 @@ EXPORTED = [
     "gpt_compute_merit", "gpt_ls_compute_merit", "gpt_set_profiling", "gpt_get_phase_stats",
     "gpt_ls_compute_merit_noalloc", "gpt_sqp_adjoint", "gpt_set_cost_weights", "gpt_autotune",
     "gpt_default_track_config", "gpt_track", "gpt_track_batched", "gpt_simulate",
-    "gpt_end_effector_positions", "gpt_forward_dynamics", "gpt_read_csv",
+    "gpt_end_effector_positions", "gpt_forward_dynamics", "gpt_read_csv", "gpt_form_ss",
 ]
 PHASES = ["init", "kkt", "schur", "pcg", "dz", "merit", "accept"]
 
@@ -164,6 +164,7 @@ def _declare(L):
         "gpt_end_effector_positions": ([u32, vp, u32, vp, vp], C.c_int),
         "gpt_forward_dynamics": ([u32, vp, u32, vp, vp], C.c_int),
         "gpt_read_csv": ([C.c_char_p, vp, C.c_size_t, P(u32), P(u32)], C.c_int),
+        "gpt_form_ss": ([vp, u32, vp, vp, vp], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -423,6 +424,10 @@ class Solver:
     def form_schur_csc(self, N, rho, G, Cm, g, c, val, gamma, Ginv, stream=None):
         _check(lib().gpt_form_schur_csc(self._h, N, rho, _ptr(G), _ptr(Cm), _ptr(g), _ptr(c), _ptr(val),
                                         _ptr(gamma), _ptr(Ginv), _stream(stream)))
+
+    def form_ss(self, N, S, Pinv, stream=None):
+        """gpt_form_ss: the stair preconditioner's off-diagonal blocks written into Pinv."""
+        _check(lib().gpt_form_ss(self._h, N, _ptr(S), _ptr(Pinv), _stream(stream)))
 
     def pcg(self, N, S, Pinv, gamma, lam, max_iter, exit_tol, exit_mode=0, lam64=None, stream=None):
         it = C.c_uint32(0)

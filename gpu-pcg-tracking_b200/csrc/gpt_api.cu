@@ -417,6 +417,14 @@ gpt_status gpt_form_schur_csc(gpt_handle *h, uint32_t N, float rho, const float 
     return GPT_OK;
 }
 
+gpt_status gpt_form_ss(gpt_handle *h, uint32_t N, const float *d_S, float *d_Pinv, gpt_stream_t stream)
+{
+    if (!h || !d_S || !d_Pinv) return set_err(GPT_ERR_BAD_ARG, "null argument");
+    if (!check_n(h, N)) return set_err(GPT_ERR_BAD_ARG, "knot_points out of range");
+    GPT_CUDA(launch_form_ss((int)N, d_S, d_Pinv, (cudaStream_t)stream));
+    return GPT_OK;
+}
+
 gpt_status gpt_prep_csr(uint32_t N, int32_t *cp, int32_t *ri)
 {
     if (!cp || !ri || N < 1) return set_err(GPT_ERR_BAD_ARG, "bad argument");

@@ -98,6 +98,8 @@ cudaError_t launch_track_tail(const BatchView &bv, const int *rows, TrackClock *
                               float *goal, float *lambda, float *tmp, float *errors, TrackInst *inst,
                               uint32_t *iters_log, uint32_t log_cap, cudaStream_t s);
 cudaError_t launch_track_final(const BatchView &bv, const float *xs, const float *goal, TrackInst *inst, cudaStream_t s);
+// stair preconditioner's off-diagonal Pinv blocks (gato_form_ss_inner), reference 3-block rows
+cudaError_t launch_form_ss(int N, const float *S, float *Pinv, cudaStream_t s);
 // batched rigid-body library kernels (gpt_grid.cu)
 cudaError_t launch_ee_pose(uint32_t n, const float *x, uint32_t stride, float *pose, cudaStream_t s);
 cudaError_t launch_fd(uint32_t n, const float *xu, uint32_t stride, float *qdd, cudaStream_t s);

@@ -560,3 +560,79 @@ cudaError_t launch_schur(int mode, const BatchView &bv, float rho_scalar, const 
 }
 
 }  // namespace gpt
+
+namespace gpt {
+
+// gato_form_ss_inner (oldschur.cuh:334-494): the stair preconditioner's off-diagonal blocks of
+// Pinv (reference 3-block rows) from S and the block-Jacobi diagonal theta_k^{-1} already in Pinv:
+//   Pinv[k].left  = -(theta_k^{-1} S[k].left) theta_{k-1}^{-1}
+//   Pinv[k].right = -(theta_k^{-1} S[k+1].left^T) theta_{k+1}^{-1}
+// One warp per block row; the five input blocks staged in shared memory, products in FP32 with the
+// reference's summation order (column-major, t = 0 .. 13).
+constexpr int SS_WARPS = 4;
+struct SsWarpSmem {
+    float tk[SS], tm[SS], tp[SS], phi[SS], phin[SS], scr[SS];
+};
+
+__device__ __forceinline__ void ss_prod(const float *A, const float *B, float *out, int lane, bool transB)
+{
+    for (int e = lane; e < SS; e += 32) {
+        const int row = e % NS, col = e / NS;
+        float r = 0.f;
+#pragma unroll
+        for (int t = 0; t < NS; ++t) r = fmaf(A[t * NS + row], transB ? B[t * NS + col] : B[col * NS + t], r);
+        out[e] = r;
+    }
+}
+
+__global__ void __launch_bounds__(32 * SS_WARPS) ss_kernel(int N, const float *__restrict__ S, float *__restrict__ Pinv)
+{
+    __shared__ SsWarpSmem sm_all[SS_WARPS];
+    const int lane = threadIdx.x & 31;
+    SsWarpSmem &sm = sm_all[threadIdx.x >> 5];
+    const int k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (k >= N) return;  // warp-uniform
+    for (int e = lane; e < SS; e += 32) {
+        sm.tk[e] = Pinv[(size_t)S_STRIDE * k + SS + e];
+        if (k > 0) {
+            sm.tm[e] = Pinv[(size_t)S_STRIDE * (k - 1) + SS + e];
+            sm.phi[e] = S[(size_t)S_STRIDE * k + e];
+        }
+        if (k < N - 1) {
+            sm.tp[e] = Pinv[(size_t)S_STRIDE * (k + 1) + SS + e];
+            sm.phin[e] = S[(size_t)S_STRIDE * (k + 1) + e];
+        }
+    }
+    __syncwarp();
+    if (k > 0) {
+        ss_prod(sm.tk, sm.phi, sm.scr, lane, false);
+        __syncwarp();
+        for (int e = lane; e < SS; e += 32) {
+            const int row = e % NS, col = e / NS;
+            float r = 0.f;
+#pragma unroll
+            for (int t = 0; t < NS; ++t) r = fmaf(sm.scr[t * NS + row], sm.tm[col * NS + t], r);
+            Pinv[(size_t)S_STRIDE * k + e] = -r;
+        }
+        __syncwarp();
+    }
+    if (k < N - 1) {
+        ss_prod(sm.tk, sm.phin, sm.scr, lane, true);  // theta_k^{-1} phi_{k+1}^T
+        __syncwarp();
+        for (int e = lane; e < SS; e += 32) {
+            const int row = e % NS, col = e / NS;
+            float r = 0.f;
+#pragma unroll
+            for (int t = 0; t < NS; ++t) r = fmaf(sm.scr[t * NS + row], sm.tp[col * NS + t], r);
+            Pinv[(size_t)S_STRIDE * k + 2 * SS + e] = -r;
+        }
+    }
+}
+
+cudaError_t launch_form_ss(int N, const float *S, float *Pinv, cudaStream_t s)
+{
+    ss_kernel<<<(N + SS_WARPS - 1) / SS_WARPS, 32 * SS_WARPS, 0, s>>>(N, S, Pinv);
+    return cudaGetLastError();
+}
+
+}  // namespace gpt

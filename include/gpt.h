@@ -304,6 +304,13 @@ gpt_status gpt_form_schur_csc(gpt_handle *h, uint32_t knot_points, float rho, co
                               const float *d_g, const float *d_c, float *d_val, float *d_gamma, float *d_Ginv,
                               gpt_stream_t stream);
 
+/* gato_form_ss_inner (oldschur.cuh:334-494): the stair ("SS") preconditioner.  Given S and the
+ * block-Jacobi d_Pinv of gpt_form_schur (theta_k^{-1} in the diagonal blocks), fills Pinv's
+ * off-diagonal blocks: left_k = -theta_k^{-1} S[k].left theta_{k-1}^{-1}, right_k =
+ * -theta_k^{-1} S[k+1].left^T theta_{k+1}^{-1}.  The reference ships this kernel without calling
+ * it; the SQP loop here uses the exact block-tridiagonal preconditioner instead. */
+gpt_status gpt_form_ss(gpt_handle *h, uint32_t knot_points, const float *d_S, float *d_Pinv, gpt_stream_t stream);
+
 /* prep_csr (utils.cuh:84-118): CSC column pointers [14N+1] and row indices [nnz] (host arrays) */
 gpt_status gpt_prep_csr(uint32_t knot_points, int32_t *h_col_ptr, int32_t *h_row_ind);
 

@@ -737,13 +737,24 @@ static void s_matvec(int N, const R *S, const R *x, R *y)
         }
     }
 }
+/* y = Pinv x for the block-tridiagonal Pinv (3 blocks per row).  The block-Jacobi Pinv has zero
+ * off-diagonal blocks, whose terms are skipped, so its products are unchanged; the stair
+ * preconditioner (form_ss) fills them. */
 static void p_apply(int N, const R *Pinv, const R *x, R *y)
 {
     for (int k = 0; k < N; ++k) {
         const R *d = Pinv + 3 * SS * k + SS;
+        const R *lft = Pinv + 3 * SS * k, *rgt = Pinv + 3 * SS * k + 2 * SS;
+        int has_l = 0, has_r = 0;
+        for (int i = 0; i < SS && k > 0; ++i) has_l |= lft[i] != 0;
+        for (int i = 0; i < SS && k < N - 1; ++i) has_r |= rgt[i] != 0;
         for (int r = 0; r < NS; ++r) {
             R acc = 0;
             for (int cc = 0; cc < NS; ++cc) acc += d[r + NS * cc] * x[NS * k + cc];
+            if (has_l)
+                for (int cc = 0; cc < NS; ++cc) acc += lft[r + NS * cc] * x[NS * (k - 1) + cc];
+            if (has_r)
+                for (int cc = 0; cc < NS; ++cc) acc += rgt[r + NS * cc] * x[NS * (k + 1) + cc];
             y[NS * k + r] = acc;
         }
     }
@@ -1152,4 +1163,29 @@ int ORC(track)(const orc_params *P, const orc_solver *SV, const orc_track_cfg *T
     ts->rho_final = rho;
     free(xu); free(xu_old); free(goal); free(lambda);
     return rc;
+}
+
+/* gato_form_ss_inner (oldschur.cuh:334-494): the stair ("SS") preconditioner's off-diagonal blocks,
+ * from S and the block-Jacobi diagonal theta_k^{-1} already in Pinv's diagonal blocks:
+ *   Pinv[k].left  = -(theta_k^{-1} S[k].left)  theta_{k-1}^{-1}          (k > 0)
+ *   Pinv[k].right = -(theta_k^{-1} S[k+1].left^T) theta_{k+1}^{-1}       (k < N-1)
+ * with the reference's product order.  The reference ships it without calling it. */
+void ORC(form_ss)(int N, const R *S, R *Pinv)
+{
+    R scratch[SS], out[SS], phiT[SS];
+    for (int k = 0; k < N; ++k) {
+        const R *tk = Pinv + 3 * SS * k + SS;
+        if (k > 0) {
+            mat_mat(scratch, tk, S + 3 * SS * k, NS, NS, NS, NS, 0);
+            mat_mat(out, scratch, Pinv + 3 * SS * (k - 1) + SS, NS, NS, NS, NS, 0);
+            for (int i = 0; i < SS; ++i) Pinv[3 * SS * k + i] = -out[i];
+        }
+        if (k < N - 1) {
+            const R *phi = S + 3 * SS * (k + 1);
+            for (int i = 0; i < SS; ++i) phiT[(i % NS) * NS + i / NS] = phi[i];  /* load_block_bd transpose */
+            mat_mat(scratch, tk, phiT, NS, NS, NS, NS, 0);
+            mat_mat(out, scratch, Pinv + 3 * SS * (k + 1) + SS, NS, NS, NS, NS, 0);
+            for (int i = 0; i < SS; ++i) Pinv[3 * SS * k + 2 * SS + i] = -out[i];
+        }
+    }
 }

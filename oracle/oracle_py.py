@@ -97,6 +97,7 @@ def _declare(L):
         fn("sqp_solve", [C.POINTER(Params), C.POINTER(Solver), C.c_int, rp, rp, rp, C.POINTER(rt), rt,
                          C.POINTER(Stats), C.c_void_p], C.c_int)
         fn("simulate", [C.c_int, rp, rp, C.c_double, C.c_double, C.c_double, C.c_double])
+        fn("form_ss", [C.c_int, rp, rp])
         fn("track", [C.POINTER(Params), C.POINTER(Solver), C.POINTER(TrackCfg), C.c_int, C.c_int, rp, rp, rp, rp,
                      C.POINTER(TrackStats)], C.c_int)
     L.orc_ldl_solve.argtypes = [C.c_int, _i32p, _i32p, _f32p, _f32p, _f32p]
@@ -291,3 +292,11 @@ def track(params, solver, cfg, N, eePos_traj, xu_traj, xs, precision="f64"):
     if rc < 0:
         raise RuntimeError("oracle linear solve failed")
     return x, err[:ts.shifts], ts
+
+
+def form_ss(N, S, Pinv, precision="f64"):
+    """gato_form_ss_inner (oldschur.cuh:334-494): Pinv with the stair preconditioner's
+    off-diagonal blocks filled in (a copy)."""
+    P = _a(Pinv, precision).copy()
+    getattr(lib(), f"orc_{precision}_form_ss")(N, _a(S, precision), P)
+    return P

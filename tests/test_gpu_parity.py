@@ -544,3 +544,30 @@ def test_autotune_choice_is_used(gpt, problem_mod):
         out.append(host(xu))
     sv.close()
     np.testing.assert_array_equal(out[0], out[1])
+
+
+def test_form_ss_matches_oracle(gpt, oracle, golden, problem_mod, solvers):
+    """gpt_form_ss (gato_form_ss_inner) on the GPU's own S and block-Jacobi Pinv against the
+    oracle's stair formation of the same FP32 inputs: off-diagonal blocks within 1e-5 of the
+    largest block entry (FP32 products of 14x14 blocks, FMA vs separate rounding), diagonal
+    blocks untouched, row 0's left and row N-1's right blocks left zero."""
+    for kind, N, cfg, p in problems(golden, problem_mod):
+        if N < 3:
+            continue
+        sv = solvers(cfg)
+        oG, oC, og, oc = oracle.form_kkt(oracle_params(oracle, cfg), N, p["xu"], p["goal"], p["xs"])
+        f = [x.astype(np.float32) for x in (oG, oC, og, oc)]
+        S, Pv, gam, Gi = (torch.zeros(n, device="cuda") for n in (588 * N, 588 * N, 14 * N, 245 * N - 49))
+        sv.form_schur(N, 1e-3, *(dev(x) for x in f), S, Pv, gam, Gi)
+        P0 = host(Pv)
+        sv.form_ss(N, S, Pv)
+        got = host(Pv)
+        want = oracle.form_ss(N, host(S), P0)
+        for k in range(N):
+            np.testing.assert_array_equal(got[588 * k + 196:588 * k + 392], P0[588 * k + 196:588 * k + 392])
+            for b in (0, 2):
+                blk = slice(588 * k + 196 * b, 588 * k + 196 * (b + 1))
+                if (k == 0 and b == 0) or (k == N - 1 and b == 2):
+                    assert np.abs(got[blk]).max() == 0.0
+                    continue
+                close(got[blk], want[blk], 1e-5, f"{kind} N={N} SS[{k}][{b}]", scale=np.abs(want).max())
