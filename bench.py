@@ -69,6 +69,11 @@ def parse():
     ap.add_argument("--track-sqp-iters", type=int, default=4,
                     help="SQP iterations per solve in the tracking leg (stands in for the wall-clock cap)")
     ap.add_argument("--track-period-us", type=float, default=2000.0, help="plant time per control update")
+    ap.add_argument("--mixed-track", action="store_true",
+                    help="only the mixed-horizon tracking workload (2048 instances, N from {64,128,256,512})")
+    ap.add_argument("--mixed-batch", type=int, default=2048)
+    ap.add_argument("--mixed-rows", type=int, default=512, help="trajectory rows per instance")
+    ap.add_argument("--mixed-period-us", type=float, default=10000.0)
     return ap.parse_args()
 
 
@@ -202,6 +207,77 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+# --------------------------------------------------------------------------- mixed tracking workload
+def run_mixed_track(args, rank, world, local_rank):
+    """Receding-horizon tracking of B instances of seeded horizon N ~ U{64, 128, 256, 512}, each
+    tracking its own seeded spline of `mixed_rows` rows (dt 0.01; the goal rows from the batched FK
+    kernel), warm-started through the shift of xu and lambda, 4 SQP iterations per solve, one
+    batched solve and one simulate / shift launch per control update.  Times the whole rollout."""
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    torch.cuda.set_device(local_rank)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    gpt = importlib.import_module("gpu-pcg-tracking_b200")
+    P = importlib.import_module("gpu-pcg-tracking_b200.problem")
+    shard = importlib.import_module("gpu-pcg-tracking_b200.shard")
+    B, S = args.mixed_batch, args.mixed_rows
+    ids = shard.weak_scaling_ids(rank, world, B)
+    rng = np.random.default_rng(4321 + ids[0])
+    Ns = [int(n) for n in rng.choice([64, 128, 256, 512], size=B)]
+    rows, xs = zip(*(P.make_trajectory_rows(S, i, dt=SPEC["timestep"]) for i in ids))
+    xu_traj = torch.as_tensor(np.concatenate(rows).reshape(-1), device="cuda")
+    ee = gpt.end_effector_positions(xu_traj, 21).reshape(-1)
+    xs0 = torch.as_tensor(np.concatenate(xs), device="cuda")
+    sv = gpt.Solver(max_knot_points=max(Ns), max_batch=B, **SPEC)
+    sv.set_solver(sqp_max_iter=args.track_sqp_iters, pcg_max_iter=args.pcg_max_iter, pcg_exit_tol=args.tol,
+                  pcg_exit_mode=0, pcg_cluster_size=gpt.PCG_WARP_PAIR, sqp_graph=args.sqp_graph)
+    tcfg = gpt.default_track_config(sim_period_us=args.mixed_period_us)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+    stream = torch.cuda.current_stream()
+    # warm-up: the first 3 control updates of the same rollout (builds and caches the solve graph)
+    warm = gpt.default_track_config(sim_period_us=args.mixed_period_us, max_control_updates=3)
+    sv.track_batched(Ns, [S] * B, ee, xu_traj, xs0.clone(), warm, errors=torch.zeros(B * S, device="cuda"))
+    xs = xs0.clone()
+    errs = torch.zeros(B * S, device="cuda")
+    clocks = ClockSampler(torch.cuda.current_device())
+    clocks.start()
+    flush.fill_(1.0)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.mark()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    _, st = sv.track_batched(Ns, [S] * B, ee, xu_traj, xs, tcfg, errors=errs)
+    e1.record(stream)
+    e1.synchronize()
+    clk = clocks.stop()
+    t_ms = shard.max_over_ranks(e0.elapsed_time(e1), device="cuda")
+    updates = sum(s["control_updates"] for s in st)
+    line = {
+        "metric": "mixed-horizon tracking solves/s", "value": world * updates / (t_ms / 1000.0), "unit": "solves/s",
+        "n_gpus": world, "higher_is_better": True, "scaling": "weak", "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"gpt_track_batched: {B} instances/GPU, N ~ U{{64,128,256,512}} (seeded), {S} "
+                               f"trajectory rows each, dt 0.01, plant period {args.mixed_period_us:g} us, "
+                               f"{args.track_sqp_iters} SQP iterations per solve",
+                   "instances_per_gpu": B, "knots_total": int(sum(Ns)), "rows": S},
+        "ms": t_ms, "control_updates": st[0]["control_updates"], "ms_per_update": t_ms / max(st[0]["control_updates"], 1),
+        "sqp_iters_per_solve": sum(s["sqp_iters_total"] for s in st) / max(updates, 1),
+        "tracking_error_mean": statistics.mean(s["tracking_error_mean"] for s in st),
+        "final_tracking_error_mean": statistics.mean(s["final_tracking_error"] for s in st),
+        "rho_exits": sum(s["rho_exits"] for s in st), "nonfinite": sum(s["nonfinite"] for s in st),
+        "clocks": clk,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
 # --------------------------------------------------------------------------- our arm
 def main():
     args = parse()
@@ -210,6 +286,10 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         run_reference(args, rank, world)
+        return
+
+    if args.mixed_track:
+        run_mixed_track(args, rank, world, local_rank)
         return
 
     # the CPU baseline's process pool starts before the first GPU call

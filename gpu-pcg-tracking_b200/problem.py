@@ -94,3 +94,22 @@ def make_batch(Ns, seed0: int = 0, dt: float = 0.01, sigma: float = 0.01, t_path
         goal[6 * off:6 * off + 6 * N] = p["goal"]
         off += N
     return {"xu": xu, "goal": goal, "lam": lam, "Ns": Ns}
+
+
+def make_trajectory_rows(S: int, seed: int, dt: float = 0.01, n_waypoints: int = 5, sigma: float = 0.01,
+                         t_path: float = 2.0):
+    """One seeded tracking trajectory as S rows of 21 floats (q, qd, u = 0) -- the row layout of the
+    reference's testfiles/*_traj.csv -- and the initial plant state x_s (waypoint 0 + N(0, sigma),
+    zero velocity), written into row 0.  The goal rows are the end-effector poses of the rows' q
+    (make_problem computes them on the host; a batch can use gpt_end_effector_positions)."""
+    rng = np.random.default_rng(1234 + seed)
+    W = rng.uniform(-0.5, 0.5, size=(n_waypoints, 7)) * JOINT_LIMITS
+    tw = np.linspace(0.0, t_path, n_waypoints)
+    t_raw = np.arange(S) * dt
+    t = np.minimum(t_raw, t_path)
+    rows = np.zeros((S, 21), np.float64)
+    rows[:, :7] = _natural_spline(tw, W, t, 0)
+    rows[:, 7:14] = _natural_spline(tw, W, t, 1) * (t_raw <= t_path)[:, None]
+    xs = np.concatenate([W[0] + rng.normal(0.0, sigma, 7), np.zeros(7)])
+    rows[0, :14] = xs
+    return rows.astype(np.float32), xs.astype(np.float32)
