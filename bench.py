@@ -69,6 +69,8 @@ def parse():
     ap.add_argument("--track-sqp-iters", type=int, default=4,
                     help="SQP iterations per solve in the tracking leg (stands in for the wall-clock cap)")
     ap.add_argument("--track-period-us", type=float, default=2000.0, help="plant time per control update")
+    ap.add_argument("--sweep-plain", action="store_true",
+                    help="only the plain single-instance sweep over N in {64,128,256,512} x tol in {1e-4,1e-5,1e-6}")
     ap.add_argument("--mixed-track", action="store_true",
                     help="only the mixed-horizon tracking workload (2048 instances, N from {64,128,256,512})")
     ap.add_argument("--mixed-batch", type=int, default=2048)
@@ -207,6 +209,59 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+# --------------------------------------------------------------------------- plain sweep
+def run_sweep_plain(args, rank, local_rank):
+    """The plain method as the drop-in (gpt_sqp_solve, one instance) over N in {64, 128, 256, 512}
+    and PCG exit tolerance in {1e-4, 1e-5, 1e-6}: solves/s (graph path, mean of 3 solves after one
+    warm-up), device microseconds per linear solve (PCG phase of a profiled solve / its launches),
+    PCG iterations per linear solve, and the PCG launch's algorithmic bytes / duration."""
+    import torch
+    if rank != 0:
+        return
+    torch.cuda.set_device(local_rank)
+    gpt = importlib.import_module("gpu-pcg-tracking_b200")
+    P = importlib.import_module("gpu-pcg-tracking_b200.problem")
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+    rows = []
+    for N in (64, 128, 256, 512):
+        p = P.make_problem(N, 0, dt=SPEC["timestep"])
+        x0, g0, l0 = (torch.as_tensor(p[k], device="cuda") for k in ("xu", "goal", "lam"))
+        sv = gpt.Solver(max_knot_points=N, max_batch=1, **SPEC)
+        sv.set_solver(sqp_max_iter=args.sqp_max_iter, pcg_max_iter=args.pcg_max_iter, pcg_exit_mode=0)
+        cs = sv.autotune([N], g0, l0, x0, [1e-3])
+        for tol in (1e-4, 1e-5, 1e-6):
+            sv.set_solver(pcg_exit_tol=tol)
+            ms, its = [], []
+            for i in range(4):
+                xu, lam = x0.clone(), l0.clone()
+                flush.fill_(1.0)
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                res = sv.sqp_solve(N, g0, lam, xu, 1e-3)
+                e1.record(stream)
+                e1.synchronize()
+                if i > 0:
+                    ms.append(e0.elapsed_time(e1))
+                    its.append(res.stats["pcg_iters_total"] / max(res.sqp_iters, 1))
+            sv.phase_stats(reset=True)
+            sv.set_profiling(True)
+            sv.sqp_solve(N, g0, l0.clone(), x0.clone(), 1e-3)
+            sv.set_profiling(False)
+            pcg_ms, pcg_n = sv.phase_stats(reset=True)["pcg"]
+            us = 1000.0 * pcg_ms / max(pcg_n, 1)
+            rows.append({"N": N, "tol": tol, "pcg_cluster_size": cs, "solves_per_s": 1000.0 / statistics.mean(ms),
+                         "ms_per_solve": statistics.mean(ms), "linsys_us": us,
+                         "pcg_iters_per_linsys": statistics.mean(its),
+                         "pcg_gbs": PCG_BYTES_PER_KNOT * N / (us * 1e-6) / 1e9 if us > 0 else None})
+        sv.close()
+    print(json.dumps({"metric": "plain sqpSolve sweep", "unit": "solves/s", "dtype": "f32", "data": "synthetic",
+                      "config": {"workload": f"gpt_sqp_solve, one instance, dt 0.01 semi-implicit Euler, QD 0.01, "
+                                             f"R 1e-4, <= {args.sqp_max_iter} SQP iterations, exact preconditioner",
+                                 "l2": "256 MB buffer written between timed solves"},
+                      "rows": rows}), flush=True)
+
+
 # --------------------------------------------------------------------------- mixed tracking workload
 def run_mixed_track(args, rank, world, local_rank):
     """Receding-horizon tracking of B instances of seeded horizon N ~ U{64, 128, 256, 512}, each
@@ -290,6 +345,9 @@ def main():
 
     if args.mixed_track:
         run_mixed_track(args, rank, world, local_rank)
+        return
+    if args.sweep_plain:
+        run_sweep_plain(args, rank, local_rank)
         return
 
     # the CPU baseline's process pool starts before the first GPU call

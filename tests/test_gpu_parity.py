@@ -571,3 +571,34 @@ def test_form_ss_matches_oracle(gpt, oracle, golden, problem_mod, solvers):
                     assert np.abs(got[blk]).max() == 0.0
                     continue
                 close(got[blk], want[blk], 1e-5, f"{kind} N={N} SS[{k}][{b}]", scale=np.abs(want).max())
+
+
+@pytest.mark.parametrize("N", [64, 128, 256, 512])
+def test_plain_sweep_linear_solve_accuracy(gpt, oracle, problem_mod, solvers, N):
+    """The plain method's linear solve over the horizon / tolerance sweep (N in {64, 128, 256,
+    512} x PCG tolerance in {1e-4, 1e-5, 1e-6}) on the first SQP iterate's Schur system of a
+    seeded problem: for the plain path's default PCG (cluster 0, exact preconditioner) and the
+    warp-pair kernel, the FP64 true relative residual meets the tolerance, and the multipliers lie
+    at least as close to the FP64 banded-Cholesky solution as the FP32 LDL^T of the reference's
+    qdldl path does."""
+    p = problem_mod.make_problem(N, 11, dt=0.01)
+    sv = solvers(SPEC_CFG)
+    oG, oC, og, oc = oracle.form_kkt(oracle_params(oracle, SPEC_CFG), N, p["xu"], p["goal"], p["xs"])
+    S, Pv, gam, _ = oracle.form_schur(N, 1e-3, *(x.astype(np.float32) for x in (oG, oC, og, oc)))
+    S, Pv, gam = (x.astype(np.float32) for x in (S, Pv, gam))
+    ref = oracle.banded_cholesky(N, S.astype(np.float64), gam.astype(np.float64))
+    ldl = oracle.ldl_solve(N, S.astype(np.float64), gam.astype(np.float64)).astype(np.float64)
+    err_ldl = np.abs(ldl - ref).max() / np.abs(ref).max()
+    for cluster in (0, gpt.PCG_WARP_PAIR):
+        sv.set_solver(pcg_cluster_size=cluster, pcg_precond=1)
+        for tol in (1e-4, 1e-5, 1e-6):
+            lam = torch.zeros(14 * N, device="cuda")
+            lam64 = torch.zeros(14 * N, device="cuda", dtype=torch.float64)
+            it, maxed = sv.pcg(N, dev(S), dev(Pv), dev(gam), lam, 2000, tol, 0, lam64=lam64)
+            torch.cuda.synchronize()
+            l64 = lam64.cpu().numpy()
+            relres = schur_residual(S, l64, gam.astype(np.float64), N)
+            assert not maxed and relres <= 1.02 * tol, (N, cluster, tol, it, relres)
+            err = np.abs(l64 - ref).max() / np.abs(ref).max()
+            assert err <= max(err_ldl, 1e-6), (N, cluster, tol, err, err_ldl)
+    sv.set_solver(pcg_cluster_size=0, pcg_precond=0)
