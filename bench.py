@@ -439,21 +439,27 @@ def main():
     offs = [sum(Ns[:b]) for b in range(B)]
     xs = torch.cat([xu0[21 * o:21 * o + 14] for o in offs])
     gw = torch.randn(xu.numel(), device="cuda", generator=torch.Generator(device="cuda").manual_seed(7))
-    adj_ms = []
+    adj_ms, ar_ms = [], []
     for i in range(1 + args.steps):
         flush.fill_(1.0)
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
         e0.record(stream)
-        sv.sqp_adjoint(Ns, goal, xs, xu, last_rho, gw)
+        grads = sv.sqp_adjoint(Ns, goal, xs, xu, last_rho, gw)
         e1.record(stream)
-        e1.synchronize()
+        # the exchange step of data-parallel weight tuning: batch-summed weight gradients, all-reduced
+        shard.allreduce_weight_grads(grads["qd"], grads["r"], grads["q_ee"])
+        e2.record(stream)
+        e2.synchronize()
         if i > 0:
             adj_ms.append(e0.elapsed_time(e1))
+            ar_ms.append(e1.elapsed_time(e2))
     adj_step = statistics.mean(adj_ms)
     adj_step = shard.max_over_ranks(adj_step, device="cuda")
     adjoint = {"us_per_solve": 1000.0 * adj_step / B, "ms_per_batch": adj_step,
                "ratio_to_forward_solve": adj_step / ms_per_step,
-               "workload": f"gpt_sqp_adjoint at the {B} solutions of the timed step (goal, QD, R, EE-weight gradients)"}
+               "weight_grad_allreduce_us": 1000.0 * shard.max_over_ranks(statistics.mean(ar_ms), device="cuda"),
+               "workload": f"gpt_sqp_adjoint at the {B} solutions of the timed step (goal, QD, R, EE-weight "
+                           f"gradients), then the 15 batch-summed weight gradients all-reduced over {world} rank(s)"}
 
     if args.batched_only:
         if rank == 0:

@@ -1,8 +1,9 @@
 """Instance sharding across ranks (one process per GPU, torch.distributed).
 
 Batched instances are independent, so a batch shards by instance with no
-collective on the data path; the only collective is the max over ranks of the
-measured times.  Two layouts:
+collective on the forward data path.  The one exchange step is the adjoint's
+weight gradient, summed over every rank's instances (allreduce_weight_grads);
+the bench also takes the max over ranks of its measured times.  Two layouts:
 
 * weak scaling (the bench): every rank solves `per_rank` instances of its own,
   global instance ids rank * per_rank + i (the problem generator's seeds);
@@ -37,3 +38,18 @@ def max_over_ranks(value: float, device=None) -> float:
     t = torch.tensor([float(value)], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def allreduce_weight_grads(grad_qd, grad_r, grad_q_ee):
+    """The adjoint's exchange step for data-parallel tuning of the cost weights: each rank sums
+    gpt_sqp_adjoint's per-instance gradients over its instances (grad_qd [B, 7], grad_r [B, 7],
+    grad_q_ee [B]), and one all-reduce (sum) over the ranks of the packed 15 numbers gives every
+    rank the gradient of the whole batch.  Returns the packed float64 vector [qd (7), r (7), q_ee]
+    on the inputs' device (the rank's own sums without a process group)."""
+    import torch
+    import torch.distributed as dist
+    packed = torch.cat([grad_qd.reshape(-1, 7).sum(0), grad_r.reshape(-1, 7).sum(0),
+                        grad_q_ee.reshape(-1).sum().reshape(1)]).to(torch.float64)
+    if dist.is_available() and dist.is_initialized() and dist.get_world_size() > 1:
+        dist.all_reduce(packed, op=dist.ReduceOp.SUM)
+    return packed

@@ -1,7 +1,8 @@
 """The multi-GPU path's host logic on CPU: two gloo ranks shard a batch of
 uneven horizons, solve their instances (with the CPU oracle standing in for the
 GPU solve), and the gathered results equal one process solving the whole batch;
-the timing reduction takes the max over ranks."""
+the adjoint's weight-gradient all-reduce equals one process summing the whole
+batch; the timing reduction takes the max over ranks."""
 import os
 import socket
 import sys
@@ -32,6 +33,15 @@ def solve_instances(ids):
     return out
 
 
+def weight_grads(ids):
+    """Deterministic stand-ins for gpt_sqp_adjoint's per-instance weight gradients of instances ids."""
+    ids = list(ids)
+    gq = torch.tensor([[np.sin(i + 0.1 * j) for j in range(7)] for i in ids], dtype=torch.float32)
+    gr = torch.tensor([[np.cos(i - 0.2 * j) for j in range(7)] for i in ids], dtype=torch.float32)
+    ge = torch.tensor([0.5 + i for i in ids], dtype=torch.float32)
+    return gq, gr, ge
+
+
 def worker(rank, world, port, q):
     import torch.distributed as dist
     sys.path.insert(0, ROOT)
@@ -46,8 +56,11 @@ def worker(rank, world, port, q):
     gathered = [None] * world
     dist.all_gather_object(gathered, {"ids": ids, "res": res})
     tmax = shard.max_over_ranks(float(rank + 1), device="cpu")
+    # the adjoint's weight-gradient exchange: every rank contributes its instances' gradients
+    gq, gr, ge = weight_grads(ids)
+    packed = shard.allreduce_weight_grads(gq, gr, ge)
     if rank == 0:
-        q.put({"gathered": gathered, "tmax": tmax})
+        q.put({"gathered": gathered, "tmax": tmax, "grads": packed.numpy()})
     dist.barrier()
     dist.destroy_process_group()
 
@@ -89,6 +102,10 @@ def test_two_gloo_ranks_equal_one_process(gpt, oracle):
         p.join(timeout=120)
         assert p.exitcode == 0
     assert out["tmax"] == 2.0
+    # the all-reduced weight gradient equals one process summing the whole batch
+    gq, gr, ge = weight_grads(range(len(NS)))
+    want = torch.cat([gq.sum(0), gr.sum(0), ge.sum().reshape(1)]).to(torch.float64).numpy()
+    np.testing.assert_allclose(out["grads"], want, rtol=1e-6, atol=1e-6)
     ids = sorted(i for g in out["gathered"] for i in g["ids"])
     assert ids == list(range(len(NS)))
     merged = {}
