@@ -618,14 +618,14 @@ static gpt_status enqueue_prologue(gpt_handle *h, const SqpPlan &pl, const float
 
 // One SQP iteration for every active instance (toplevel.cuh:254-446); leaves the number of
 // instances still active in h->d_active (cleared first unless reset_active is false).
-// The iteration's front half: KKT formation and the Schur complement at the current iterate.
-static gpt_status enqueue_front(gpt_handle *h, const SqpPlan &pl, const float *d_goal, const float *d_xu,
-                                cudaStream_t s)
+static gpt_status enqueue_iteration(gpt_handle *h, const SqpPlan &pl, const float *d_goal, float *d_lambda,
+                                    float *d_xu, cudaStream_t s, bool reset_active = true)
 {
     const BatchView &bv = pl.bv;
     const SolverParams &SP = pl.SP;
     const int ns = pl.ns;
     const bool f64 = SP.pcg_precond == 1 && SP.schur_fp64;
+    const float *S_rows = f64 ? reinterpret_cast<const float *>(h->S64) : h->S;
     {
         PhaseTimer t(h, s, GPT_PHASE_KKT);
         GPT_CUDA(launch_kkt(bv, pl.P, d_xu, d_goal, h->xs, h->G, h->C, h->g, h->c, ns, s));
@@ -638,19 +638,6 @@ static gpt_status enqueue_front(gpt_handle *h, const SqpPlan &pl, const float *d
             GPT_CUDA(launch_schur(1, bv, 0.f, h->G, h->C, h->g, h->c, h->S, nullptr, h->gamma, h->Ginv, h->Ginv64,
                                   nullptr, SP.pcg_precond == 0 ? 1 : 0, ns, s));
     }
-    return GPT_OK;
-}
-
-// The back half: PCG, dz, line-search merits and the accept step; adds the instances still active
-// to h->d_active (cleared first when reset_active).
-static gpt_status enqueue_back(gpt_handle *h, const SqpPlan &pl, const float *d_goal, float *d_lambda, float *d_xu,
-                               cudaStream_t s, bool reset_active)
-{
-    const BatchView &bv = pl.bv;
-    const SolverParams &SP = pl.SP;
-    const int ns = pl.ns;
-    const bool f64 = SP.pcg_precond == 1 && SP.schur_fp64;
-    const float *S_rows = f64 ? reinterpret_cast<const float *>(h->S64) : h->S;
     {
         PhaseTimer t(h, s, GPT_PHASE_PCG);
         GPT_CUDA(launch_pcg(bv, pl.maxN, pl.minN, f64 ? 2 : 1, (int)SP.pcg_precond, S_rows, nullptr, h->gamma,
@@ -674,21 +661,10 @@ static gpt_status enqueue_back(gpt_handle *h, const SqpPlan &pl, const float *d_
     return GPT_OK;
 }
 
-static gpt_status enqueue_iteration(gpt_handle *h, const SqpPlan &pl, const float *d_goal, float *d_lambda,
-                                    float *d_xu, cudaStream_t s, bool reset_active = true)
-{
-    const gpt_status st = enqueue_front(h, pl, d_goal, d_xu, s);
-    return st != GPT_OK ? st : enqueue_back(h, pl, d_goal, d_lambda, d_xu, s, reset_active);
-}
-
 // sqp_graph K >= 2: the batch as K parts (contiguous instance ranges of near-equal size) whose
-// iterations run on K branches of the graph.  The even-numbered parts run their iteration rotated
-// by half: their first front half (KKT, Schur) runs before the loop, and each loop body runs their
-// back half (PCG, dz, merit, accept) and then the next iteration's front half, while the odd parts
-// run front then back.  So one part's latency-bound PCG overlaps another part's throughput-bound
-// KKT and Schur kernels; every instance still sees the same operations in the same order.  The
-// parts share no workspace (every buffer is indexed by the batch's knot or instance); the active
-// count is cleared once before all.
+// iterations run on K branches of the graph, so that one part's latency-bound PCG overlaps the
+// others' throughput-bound KKT, Schur and merit kernels.  The parts share no workspace (every
+// buffer is indexed by the batch's knot or instance); the active count is cleared once before all.
 static int branch_count(const gpt_handle *h, const SqpPlan &pl)
 {
     if (pl.SP.sqp_graph < 2 || pl.bv.knot_off == nullptr || h->off_cache.size() != (size_t)pl.bv.B + 1) return 1;
@@ -728,14 +704,8 @@ static gpt_status enqueue_iteration_split(gpt_handle *h, const SqpPlan &pl, int 
     GPT_CUDA(cudaEventRecord(h->ev_fork, s));
     for (int i = 1; i < K; ++i) GPT_CUDA(cudaStreamWaitEvent(h->branch_stream[i], h->ev_fork, 0));
     for (int i = 0; i < K; ++i) {
-        cudaStream_t bs = i == 0 ? s : h->branch_stream[i];
-        gpt_status st;
-        if (i % 2 == 0) {
-            st = enqueue_back(h, part[i], h->ggoal, h->glam, h->gxu, bs, false);
-            if (st == GPT_OK) st = enqueue_front(h, part[i], h->ggoal, h->gxu, bs);
-        } else {
-            st = enqueue_iteration(h, part[i], h->ggoal, h->glam, h->gxu, bs, false);
-        }
+        const gpt_status st =
+            enqueue_iteration(h, part[i], h->ggoal, h->glam, h->gxu, i == 0 ? s : h->branch_stream[i], false);
         if (st != GPT_OK) return st;
     }
     for (int i = 1; i < K; ++i) {
@@ -788,11 +758,6 @@ static gpt_status sqp_graph_for(gpt_handle *h, const SqpPlan &pl, cudaGraphExec_
     cudaGraph_t graph = nullptr;
     GPT_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeRelaxed));
     gpt_status st = enqueue_prologue(h, pl, h->ggoal, h->gxu, cs);
-    if (st == GPT_OK && K > 1) {  // the rotated parts' first front half
-        SqpPlan part[MAX_BRANCHES];
-        split_plan(h, pl, K, part);
-        for (int i = 0; i < K && st == GPT_OK; i += 2) st = enqueue_front(h, part[i], h->ggoal, h->gxu, cs);
-    }
     if (st == GPT_OK) {
         cudaError_t e = cudaMemsetAsync(h->d_iter, 0, sizeof(uint32_t), cs);
         cudaStreamCaptureStatus cst;
