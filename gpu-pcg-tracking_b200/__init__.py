@@ -37,6 +37,7 @@ EXPORTED = [
     "gpt_ls_compute_merit_noalloc", "gpt_sqp_adjoint", "gpt_set_cost_weights", "gpt_autotune",
     "gpt_default_track_config", "gpt_track", "gpt_track_batched", "gpt_simulate",
     "gpt_end_effector_positions", "gpt_forward_dynamics", "gpt_read_csv", "gpt_form_ss",
+    "gpt_forward_dynamics_gradient",
 ]
 PHASES = ["init", "kkt", "schur", "pcg", "dz", "merit", "accept"]
 
@@ -165,6 +166,7 @@ def _declare(L):
         "gpt_forward_dynamics": ([u32, vp, u32, vp, vp], C.c_int),
         "gpt_read_csv": ([C.c_char_p, vp, C.c_size_t, P(u32), P(u32)], C.c_int),
         "gpt_form_ss": ([vp, u32, vp, vp, vp], C.c_int),
+        "gpt_forward_dynamics_gradient": ([u32, vp, u32, vp, vp, vp], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -220,6 +222,16 @@ def forward_dynamics(xu, row_stride: int = 21, out=None, stream=None):
         out = torch.empty(n, 7, device=xu.device)
     _check(lib().gpt_forward_dynamics(n, _ptr(xu), row_stride, _ptr(out), _stream(stream)))
     return out
+
+
+def forward_dynamics_gradient(xu, row_stride: int = 21, stream=None):
+    """gpt_forward_dynamics_gradient: (qdd [rows, 7], df/du [rows, 147] = 7 x 21 column-major)."""
+    import torch
+    n = xu.numel() // row_stride
+    qdd = torch.empty(n, 7, device=xu.device)
+    df = torch.empty(n, 147, device=xu.device)
+    _check(lib().gpt_forward_dynamics_gradient(n, _ptr(xu), row_stride, _ptr(qdd), _ptr(df), _stream(stream)))
+    return qdd, df
 
 
 def read_csv(path: str):

@@ -1274,6 +1274,16 @@ gpt_status gpt_forward_dynamics(uint32_t n, const float *d_xu, uint32_t stride, 
     return GPT_OK;
 }
 
+gpt_status gpt_forward_dynamics_gradient(uint32_t n, const float *d_xu, uint32_t stride, float *d_qdd, float *d_df,
+                                         gpt_stream_t stream)
+{
+    if (n == 0) return GPT_OK;
+    if (!d_xu || !d_qdd || !d_df) return set_err(GPT_ERR_BAD_ARG, "null argument");
+    if (stride < (uint32_t)NX || n > (1u << 26)) return set_err(GPT_ERR_BAD_ARG, "row_stride must be >= 21 and n <= 2^26");
+    GPT_CUDA(launch_fd_grad(n, d_xu, stride, d_qdd, d_df, (cudaStream_t)stream));
+    return GPT_OK;
+}
+
 gpt_status gpt_read_csv(const char *path, float *h_out, size_t capacity, uint32_t *h_rows, uint32_t *h_cols)
 {
     if (!path || !h_rows || !h_cols) return set_err(GPT_ERR_BAD_ARG, "null argument");

@@ -103,6 +103,7 @@ cudaError_t launch_form_ss(int N, const float *S, float *Pinv, cudaStream_t s);
 // batched rigid-body library kernels (gpt_grid.cu)
 cudaError_t launch_ee_pose(uint32_t n, const float *x, uint32_t stride, float *pose, cudaStream_t s);
 cudaError_t launch_fd(uint32_t n, const float *xu, uint32_t stride, float *qdd, cudaStream_t s);
+cudaError_t launch_fd_grad(uint32_t n, const float *xu, uint32_t stride, float *qdd, float *df, cudaStream_t s);
 cudaError_t launch_simulate_one(int N, const TrackParams &tp, double t0_us, float *xs, const float *xu,
                                 cudaStream_t s);
 

@@ -279,6 +279,12 @@ gpt_status gpt_end_effector_positions(uint32_t n, const float *d_x, uint32_t row
 gpt_status gpt_forward_dynamics(uint32_t n, const float *d_xu, uint32_t row_stride, float *d_qdd,
                                 gpt_stream_t stream);
 
+/* forwardDynamicsAndGradient (rbdfiles/iiwa_eepos_plant.cuh:130-160) for n rows at once: qdd
+ * (7 per row) and df/du = [-M^{-1} dID/dq, -M^{-1} dID/dqd, M^{-1}] (7 x 21 column-major, 147 per
+ * row) of the row [q, qd, u] at d_xu[i * row_stride]; row_stride >= 21. */
+gpt_status gpt_forward_dynamics_gradient(uint32_t n, const float *d_xu, uint32_t row_stride, float *d_qdd,
+                                         float *d_dfdu, gpt_stream_t stream);
+
 /* readCSVToVecVec (runme.cu:18-44, generateeepos.cu:14-40): a text file of comma-separated floats,
  * one row per line, parsed like std::stof, flattened row by row into h_out (host).  *h_rows and
  * *h_cols receive the shape; with h_out NULL only the shape is returned.  Rows of unequal length

@@ -80,3 +80,21 @@ def test_library_kernels_reject_bad_strides(gpt):
         gpt.forward_dynamics(x, 14)
     with pytest.raises(gpt.GptError):
         gpt.end_effector_positions(x, 3)
+
+
+@pytest.mark.gpu
+def test_forward_dynamics_gradient_matches_oracle(gpt, oracle, golden):
+    """gpt_forward_dynamics_gradient (forwardDynamicsAndGradient) on rows of the reference's
+    trajectories against the FP64 oracle's fd_grad: qdd within 1e-5 and each 7 x 7 block of df/du
+    within 1e-4 of its largest entry (FP32 tangent inverse dynamics); qdd also agrees with
+    gpt_forward_dynamics."""
+    tr = np.concatenate([golden["traj_0_1"][::5], golden["traj_3_4"][::5]])
+    qdd, df = (t.cpu().numpy().astype(np.float64) for t in gpt.forward_dynamics_gradient(dev(tr), 21))
+    qdd_fd = gpt.forward_dynamics(dev(tr), 21).cpu().numpy().astype(np.float64)
+    assert np.abs(qdd - qdd_fd).max() <= 1e-5 * max(1.0, np.abs(qdd_fd).max())
+    for k, row in enumerate(tr.astype(np.float64)):
+        wq, wdf = oracle.fd_grad(row[:7], row[7:14], row[14:21])
+        assert np.abs(qdd[k] - wq).max() <= 1e-5 * max(1.0, np.abs(wq).max()), k
+        for b in range(3):
+            blk = slice(49 * b, 49 * (b + 1))
+            assert np.abs(df[k, blk] - wdf[blk]).max() <= 1e-4 * max(1e-3, np.abs(wdf[blk]).max()), (k, b)
