@@ -196,3 +196,59 @@ def test_track_rejects_short_trajectories(gpt, golden):
             sv.track(N, dev(ee), dev(tr), dev(tr[0, :14]))
     finally:
         sv.close()
+
+
+def test_oracle_track_loop_matches_restated_host_logic(oracle, golden):
+    """The oracle's track loop against a line-by-line restatement of the reference's host logic
+    (toplevel.cuh:600-726: the clock, just_shift's knot-by-knot copies, the fills -- inside the
+    trajectory from row traj_offset, past it the last q with zero velocity and zero control -- the
+    goal-window shift and x_0 <- x_s), with the SQP solve switched off (sqp_max_iter 0) so that
+    only the loop's bookkeeping and the plant act: identical errors and final state in FP64."""
+    N, S, dt, sim = 6, 14, 1.0 / 64, 6000.0
+    tr = golden["traj_0_0"][:S].astype(np.float64)
+    ee = golden["eepos_0_0"][:S].astype(np.float64)
+    P = oracle.make_params()
+    SV = oracle.make_solver(linsys=2, sqp_max_iter=0)
+    cfg = oracle.make_track_cfg(sim_period_us=sim)
+    xs_o, err_o, ts = oracle.track(P, SV, cfg, N, ee, tr, tr[0, :14].copy())
+
+    L = 21 * N - 7
+    trf, eef = tr.reshape(-1), ee.reshape(-1)
+    xu = trf[:L].copy()
+    xu_old = xu.copy()
+    goal = eef[:6 * N].copy()
+    xs = tr[0, :14].copy()
+    errs = []
+    time_since, prev, shifted, off = 0.0, 0.0, False, 0
+    for _ in range(100000):
+        if off == S:
+            break
+        xs = oracle.simulate(N, xs, xu_old, dt, prev, sim)
+        xu_old = xu.copy()
+        time_since += sim * 1e-6
+        if not shifted and time_since > dt:
+            p = oracle.fk(xs[:7])
+            errs.append(abs(p[0] - goal[0]) + abs(p[1] - goal[1]) + abs(p[2] - goal[2]))
+            off += 1
+            for k in range(N - 1):  # just_shift: knot k <- knot k+1, the last step copies the state only
+                n = 14 + (7 if k < N - 2 else 0)
+                xu[21 * k:21 * k + n] = xu[21 * (k + 1):21 * (k + 1) + n]
+            if off + N < S:
+                xu[L - 21:L] = trf[21 * off - 7:21 * off + 14]
+            else:
+                xu[L - 14:L - 7] = trf[21 * (S - 1):21 * (S - 1) + 7]
+                xu[L - 7:L] = 0.0
+                xu[L - 21:L - 14] = 0.0
+            for k in range(N - 1):
+                goal[6 * k:6 * k + 6] = goal[6 * (k + 1):6 * (k + 1) + 6]
+            row = off + N - 1 if off + N < S else S - 1
+            goal[6 * (N - 1):] = eef[6 * row:6 * row + 6]
+            shifted = True
+        if time_since > dt:
+            shifted = False
+            time_since = np.fmod(time_since, dt)
+        xu[:14] = xs
+        prev = sim
+    assert ts.shifts == S == len(errs)
+    np.testing.assert_array_equal(err_o, np.array(errs))
+    np.testing.assert_array_equal(xs_o, xs)
