@@ -25,7 +25,7 @@ constexpr int S_STRIDE = 3 * SS;         // 588 (toplevel.cuh:103)
 constexpr int NUM_ALPHAS = 8;            // toplevel.cuh:55
 constexpr int PK = 408;                  // packed Schur row for the PCG: left 196 + tri 105 + Pinv tri 105 + 2
 constexpr int PK64 = 302;                // FP64 packed Schur row: left 196 + diagonal lower triangle 105 + 1 pad (doubles)
-constexpr int MAX_KNOTS = 1024;          // per-instance horizon limit of this build
+constexpr int MAX_KNOTS = 1024;          // per-instance horizon limit of the library
 
 // Per-instance SQP state kept on the device across the phases of one solve.
 struct InstState {

@@ -8,7 +8,7 @@
 
 namespace gpt {
 
-constexpr int MAX_PCG_KNOTS = 512;  // horizon limit of this build (16-CTA cluster x 32 knots)
+constexpr int MAX_PCG_KNOTS = 512;  // horizon limit of the library (16-CTA cluster x 32 knots)
 constexpr int PCG_KPC_MAX = 128;    // knots per CTA held in shared memory by the PCG
 constexpr int PCG_WARP_PAIR = 32;   // pcg_cluster_size value selecting pcg_pair_kernel (one 128-thread CTA per instance)
 

@@ -959,7 +959,7 @@ R ORC(merit)(const orc_params *P, int N, const R *xu, const R *dz, R alpha, cons
 int orc_ldl_solve(int n, const int32_t *Ap, const int32_t *Ai, const float *Ax, const float *b, float *x);
 
 /* ------------------------------------------------------------------------ */
-/* SQP driver: toplevel.cuh:24-503 (wall-clock cap removed)                   */
+/* SQP loop: toplevel.cuh:24-503 (wall-clock cap removed)                     */
 /* ------------------------------------------------------------------------ */
 
 int ORC(sqp_solve)(const orc_params *P, const orc_solver *SV, int N, const R *goal, R *lambda, R *xu,
