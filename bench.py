@@ -56,7 +56,11 @@ def parse():
     ap.add_argument("--tol", type=float, default=1e-5)
     ap.add_argument("--pcg-max-iter", type=int, default=10000)
     ap.add_argument("--sqp-max-iter", type=int, default=40)
-    ap.add_argument("--plain-solves", type=int, default=2)
+    ap.add_argument("--plain-solves", type=int, default=20)
+    ap.add_argument("--accuracy-instances", type=int, default=8,
+                    help="instances of the batch whose every SQP iterate is re-solved in FP64 on the host")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the mixed-horizon batch, the K_sqp = 4 line and the FP64 accuracy block")
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="bound of the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--pcg-cluster", type=int, default=0, help="CTAs per instance in the PCG (0 = library choice)")
@@ -82,7 +86,9 @@ def parse():
 # --------------------------------------------------------------------------- CPU (oracle) legs
 def _cpu_worker(task):
     """Solve seeded instances with the oracle's restatement of the reference's qdldl path (FP32,
-    KKT + Schur + LDL^T + dz + merit on one host core) until the time budget is used."""
+    KKT + Schur + LDL^T + dz + merit on one host core) until the time budget is used.  Only the
+    solves are timed (the problems are generated before each solve's clock starts); returns
+    (completed solves, seconds spent in them)."""
     N, seeds, budget, sqp_max_iter = task
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle_py as O
@@ -90,34 +96,60 @@ def _cpu_worker(task):
     par = O.make_params(dt=SPEC["timestep"], integrator=SPEC["integrator"], qd_cost=SPEC["qd_cost"],
                         r_cost=SPEC["r_cost"])
     sv = O.make_solver(linsys=1, sqp_max_iter=sqp_max_iter)
-    t0 = time.perf_counter()
+    busy = 0.0
     done = 0
     for s in seeds:
         p = P.make_problem(N, s, dt=SPEC["timestep"])
+        t0 = time.perf_counter()
         O.sqp_solve(par, sv, N, p["goal"], p["lam"], p["xu"], 1e-3, precision="f32")
+        busy += time.perf_counter() - t0
         done += 1
-        if time.perf_counter() - t0 > budget:
+        if busy > budget:
             break
-    return done, time.perf_counter() - t0
+    return done, busy
+
+
+class CpuPool:
+    """Host processes (spawn, started before the first GPU call) that time the oracle's qdldl path.
+    A sample's rate is the sum over processes of completed solves / the time those solves took, so
+    no process is charged for another's unfinished solve and no start-up is timed."""
+
+    def __init__(self, cores=None):
+        import multiprocessing as mp
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle_py
+        oracle_py.build()
+        self.cores = cores or (os.cpu_count() or 1)
+        self.pool = mp.get_context("spawn").Pool(self.cores)
+        self.calls = 0
+
+    def sample(self, N, budget, sqp_max_iter):
+        base = 100000 * self.calls
+        self.calls += 1
+        tasks = [(N, list(range(base + 1000 * i, base + 1000 * i + 1000)), budget, sqp_max_iter)
+                 for i in range(self.cores)]
+        t0 = time.perf_counter()
+        res = self.pool.map(_cpu_worker, tasks)
+        wall = time.perf_counter() - t0
+        solves = sum(r[0] for r in res)
+        rate = sum(r[0] / r[1] for r in res if r[1] > 0)
+        return {"value": rate, "unit": "solves/s", "cores": self.cores, "kind": "port",
+                "sample": f"{solves} seeded N={N} instances, sqpSolve qdldl path (FP32 KKT/Schur/LDL^T/dz/merit "
+                          f"restated in C), {self.cores} processes x ~{budget:.0f}s of solves (sum of per-process "
+                          f"solves per busy second), wall {wall:.1f}s"}
+
+    def close(self):
+        self.pool.close()
+        self.pool.join()
 
 
 def cpu_baseline(N, budget, sqp_max_iter, cores=None):
-    import multiprocessing as mp
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle_py
-    oracle_py.build()
-    cores = cores or (os.cpu_count() or 1)
-    ctx = mp.get_context("spawn")
-    tasks = [(N, list(range(1000 * i, 1000 * i + 64)), budget, sqp_max_iter) for i in range(cores)]
-    t0 = time.perf_counter()
-    with ctx.Pool(cores) as pool:
-        res = pool.map(_cpu_worker, tasks)
-    wall = time.perf_counter() - t0
-    solves = sum(r[0] for r in res)
-    busy = max(r[1] for r in res)
-    return {"value": solves / busy, "unit": "solves/s", "cores": cores, "kind": "port",
-            "sample": f"{solves} seeded N={N} instances, sqpSolve qdldl path (FP32 KKT/Schur/LDL^T/dz/merit "
-                      f"restated in C), {cores} processes x ~{budget:.0f}s, wall {wall:.1f}s"}
+    pool = CpuPool(cores)
+    try:
+        pool.sample(N, min(budget, 3.0), sqp_max_iter)  # warm-up: first solves of fresh processes
+        return pool.sample(N, budget, sqp_max_iter)
+    finally:
+        pool.close()
 
 
 # --------------------------------------------------------------------------- clocks
@@ -186,16 +218,20 @@ class ClockSampler:
 def run_reference(args, rank, world):
     if rank != 0:
         return
-    # each timed step is a bounded sample: about 45 s of host work over all steps, at least 2 s a step
-    budget = 5.0 if args.no_cpu_baseline else max(2.0, min(args.cpu_seconds, 45.0 / max(args.steps, 1)))
-    times = []
+    # every step is a bounded sample of the same per-process rate as the cpu_baseline leg: about 60 s of
+    # host work over the timed steps, at least 4 s of solves per process a step
+    budget = max(4.0, min(args.cpu_seconds, 60.0 / max(args.steps, 1)))
+    pool = CpuPool()
     rates = []
     cb = None
-    for i in range(args.warmup + args.steps):
-        r = cpu_baseline(args.knots, budget if i >= args.warmup else 2.0, args.sqp_max_iter)
-        if i >= args.warmup:
-            rates.append(r["value"])
-            cb = r
+    try:
+        for i in range(args.warmup + args.steps):
+            r = pool.sample(args.knots, budget if i >= args.warmup else 2.0, args.sqp_max_iter)
+            if i >= args.warmup:
+                rates.append(r["value"])
+                cb = r
+    finally:
+        pool.close()
     val = statistics.mean(rates)
     line = {"impl": "reference", "metric": METRIC, "value": val, "unit": "solves/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * budget,
@@ -331,6 +367,104 @@ def run_mixed_track(args, rank, world, local_rank):
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
+
+
+# --------------------------------------------------------------------------- extras of the default line
+def fp64_accuracy(gpt, sv, Ns, batch, n_inst, iters):
+    """Relative error of the solve's lambda and dz against an FP64 host re-solve of the same KKT
+    system, for every SQP iterate of n_inst sampled instances of the batch (a traced solve of the same
+    batch, outside the timed region; the KKT blocks at each recorded iterate come from the CUDA KKT
+    kernel, the FP64 Schur complement, block Cholesky and dz from fp64check)."""
+    import numpy as np
+    import torch
+    F = importlib.import_module("gpu-pcg-tracking_b200.fp64check")
+    B = len(Ns)
+    offs = np.concatenate([[0], np.cumsum(Ns)])
+    xu = torch.as_tensor(batch["xu"], device="cuda")
+    goal = torch.as_tensor(batch["goal"], device="cuda")
+    lam = torch.as_tensor(batch["lam"], device="cuda")
+    _, stats, tr = sv.sqp_solve_batched_trace(Ns, goal, lam, xu, [1e-3] * B, iters)
+    rec = gpt.trace_record_fields(tr["rec"])
+    sample = [0] + sorted(np.random.default_rng(5).choice(np.arange(1, B), min(n_inst, B) - 1, replace=False).tolist())
+    e_lam, e_dz, n = 0.0, 0.0, 0
+    for b in sample:
+        N, o = Ns[b], int(offs[b])
+        g_b = goal[6 * o:6 * o + 6 * N]
+        xs_b = xu.new_tensor(batch["xu"][21 * o:21 * o + 14])
+        for i in range(min(iters, int(stats[b]["sqp_iters"]))):
+            Gd, Cd, gd, cd = (torch.zeros(m, device="cuda") for m in (245 * N - 49, 294 * (N - 1), 21 * N - 7, 14 * N))
+            sv.form_kkt(N, tr["xu"][i, 21 * o:21 * o + 21 * N - 7].contiguous(), g_b, xs_b, Gd, Cd, gd, cd)
+            l64, d64 = F.solve_step(N, float(rec["rho"][i, b]), *(t.cpu().numpy() for t in (Gd, Cd, gd, cd)))
+            e_lam = max(e_lam, F.rel_err(tr["lam"][i, 14 * o:14 * o + 14 * N].cpu().numpy(), l64))
+            e_dz = max(e_dz, F.rel_err(tr["dz"][i, 21 * o:21 * o + 21 * N - 7].cpu().numpy(), d64))
+            n += 1
+    del tr
+    return {"lambda_max_rel_err": e_lam, "dz_max_rel_err": e_dz, "iterates": n, "instances": sample,
+            "reference": "FP64 host Schur complement + block Cholesky + dz of the GPU's own KKT blocks at each "
+                         "recorded iterate (max |err| / max |FP64|)"}
+
+
+def mixed_horizon_batch(gpt, P, args, seed0, flush, stream):
+    """Batched form with uneven horizons: 512 seeded instances of N ~ U{32, 64, 128, 256}, one batched
+    solve (graph, autotuned PCG) per step, against the same 512 instances solved one after another by
+    the plain single-instance path (gpt_sqp_solve)."""
+    import numpy as np
+    import torch
+    B = 512
+    rng = np.random.default_rng(2024 + seed0)
+    Ns = [int(n) for n in rng.choice([32, 64, 128, 256], size=B)]
+    batch = P.make_batch(Ns, seed0=seed0, dt=SPEC["timestep"])
+    sv = gpt.Solver(max_knot_points=max(Ns), max_batch=B, **SPEC)
+    sv.set_solver(sqp_max_iter=args.sqp_max_iter, pcg_max_iter=args.pcg_max_iter, pcg_exit_tol=args.tol,
+                  pcg_exit_mode=0, sqp_graph=args.sqp_graph)
+    xu0, goal, lam0 = (torch.as_tensor(batch[k], device="cuda") for k in ("xu", "goal", "lam"))
+    cs = sv.autotune(Ns, goal, lam0, xu0, [1e-3] * B)
+    ms = []
+    for i in range(3 + 5):
+        xu, lam = xu0.clone(), lam0.clone()
+        flush.fill_(1.0)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        sv.sqp_solve_batched(Ns, goal, lam, xu, [1e-3] * B)
+        e1.record(stream)
+        e1.synchronize()
+        if i >= 3:
+            ms.append(e0.elapsed_time(e1))
+    sv.close()
+    batched_ms = statistics.mean(ms)
+    # the same instances, one plain solve each, in sequence (one solver per horizon, autotuned)
+    offs = np.concatenate([[0], np.cumsum(Ns)])
+    plains = {}
+    for n in sorted(set(Ns)):
+        s1 = gpt.Solver(max_knot_points=n, max_batch=1, **SPEC)
+        s1.set_solver(sqp_max_iter=args.sqp_max_iter, pcg_max_iter=args.pcg_max_iter, pcg_exit_tol=args.tol,
+                      pcg_exit_mode=0)
+        b0 = Ns.index(n)
+        o = int(offs[b0])
+        s1.autotune([n], goal[6 * o:6 * o + 6 * n], lam0[14 * o:14 * o + 14 * n],
+                    xu0[21 * o:21 * o + 21 * n - 7].contiguous(), [1e-3])
+        s1.sqp_solve(n, goal[6 * o:6 * o + 6 * n], lam0[14 * o:14 * o + 14 * n].clone(),
+                     xu0[21 * o:21 * o + 21 * n - 7].clone(), 1e-3)  # builds the graph
+        plains[n] = s1
+    xs_all = [xu0[21 * int(offs[b]):21 * int(offs[b]) + 21 * Ns[b] - 7].clone() for b in range(B)]
+    ls_all = [lam0[14 * int(offs[b]):14 * int(offs[b]) + 14 * Ns[b]].clone() for b in range(B)]
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for b in range(B):
+        o = int(offs[b])
+        plains[Ns[b]].sqp_solve(Ns[b], goal[6 * o:6 * o + 6 * Ns[b]], ls_all[b], xs_all[b], 1e-3)
+    e1.record(stream)
+    e1.synchronize()
+    seq_ms = e0.elapsed_time(e1)
+    for s1 in plains.values():
+        s1.close()
+    return {"workload": f"{B} instances, N ~ U{{32,64,128,256}} (seeded, {int(sum(Ns))} knots), one batched "
+                        f"solve per step (graph, PCG cluster {cs}) vs the same {B} instances solved one after "
+                        f"another by gpt_sqp_solve",
+            "solves_per_s": B / (batched_ms / 1000.0), "ms_per_batch": batched_ms,
+            "sequential_plain_solves_per_s": B / (seq_ms / 1000.0), "sequential_plain_ms": seq_ms,
+            "batched_over_sequential_plain": seq_ms / batched_ms}
 
 
 # --------------------------------------------------------------------------- our arm
@@ -520,6 +654,25 @@ def main():
             plain_ms.append(e0.elapsed_time(e1))
     plain_rate = 1000.0 / statistics.mean(plain_ms) if plain_ms else None
 
+    # extras of the default line (rank 0, outside the timed region, no collective): the headline batch at
+    # a fixed K_sqp = 4 iterations per solve, the FP64 accuracy of every iterate of sampled instances, and
+    # the batched form with uneven horizons against sequential plain solves
+    extras = {}
+    if rank == 0 and not args.no_extras:
+        sv.set_solver(sqp_max_iter=4)
+        k4 = []
+        for i in range(args.warmup + args.steps):
+            ms4, st4 = one_step()
+            if i >= args.warmup:
+                k4.append(ms4)
+        sv.set_solver(sqp_max_iter=args.sqp_max_iter)
+        extras["k_sqp4"] = {"solves_per_s": B / (statistics.mean(k4) / 1000.0), "ms_per_step": statistics.mean(k4),
+                            "sqp_iters_mean": statistics.mean(x["sqp_iters"] for x in st4),
+                            "workload": f"the headline batch with sqp_max_iter = 4 (the reference's logged mean of "
+                                        f"3.96 SQP iterations per control step at N = 128)"}
+        extras["fp64_rel_err"] = fp64_accuracy(gpt, sv, Ns, batch, args.accuracy_instances, args.sqp_max_iter)
+        extras["mixed_horizon"] = mixed_horizon_batch(gpt, P, args, ids[0], flush, stream)
+
     # MPC tracking leg (gpt_track_batched): every instance tracks its own spline for as many rows as
     # its horizon (the shortest trajectory the loop accepts); one solve per control update
     track = None
@@ -618,6 +771,7 @@ def main():
         "alg_bytes_per_sqp_iter_per_instance": 4 * N * ALG_FLOATS_PER_KNOT_SQP,
         "track": track,
     }
+    line.update(extras)
     print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()

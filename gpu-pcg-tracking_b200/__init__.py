@@ -23,7 +23,7 @@ LIB_PATH = os.path.join(HERE, "libgpt.so")
 
 GPT_OK = 0
 STATUS_NAMES = {0: "OK", 1: "BAD_ARG", 2: "CUDA", 3: "NO_DEVICE", 4: "CAPACITY", 5: "NONFINITE", 6: "FACTOR"}
-EXIT_RHO_MAX, EXIT_PCG_MAXITER, EXIT_NONFINITE, EXIT_ITER_LIMIT = 1, 2, 4, 8
+EXIT_RHO_MAX, EXIT_PCG_MAXITER, EXIT_NONFINITE, EXIT_ITER_LIMIT, EXIT_FACTOR = 1, 2, 4, 8, 16
 
 STATE_SIZE, CONTROL_SIZE = 14, 7
 PCG_WARP_PAIR = 32  # GPT_PCG_WARP_PAIR: pcg_cluster_size of the one-CTA-per-instance warp-pair PCG
@@ -37,9 +37,22 @@ EXPORTED = [
     "gpt_ls_compute_merit_noalloc", "gpt_sqp_adjoint", "gpt_set_cost_weights", "gpt_autotune",
     "gpt_default_track_config", "gpt_track", "gpt_track_batched", "gpt_simulate",
     "gpt_end_effector_positions", "gpt_forward_dynamics", "gpt_read_csv", "gpt_form_ss",
-    "gpt_forward_dynamics_gradient",
+    "gpt_forward_dynamics_gradient", "gpt_sqp_solve_batched_trace",
 ]
 PHASES = ["init", "kkt", "schur", "pcg", "dz", "merit", "accept"]
+# gpt_iterate_record as 14 floats: rho, rho_next, merit_prev, merits[8], alpha, active (uint32), pcg_iters (uint32)
+TRACE_REC_FLOATS = 14
+TRACE_REC = {"rho": 0, "rho_next": 1, "merit_prev": 2, "merits": slice(3, 11), "alpha": 11, "active": 12,
+             "pcg_iters": 13}
+
+
+def trace_record_fields(rec):
+    """Decode rows of gpt_iterate_record (a float32 tensor/array [..., 14]) into a dict of numpy arrays."""
+    import numpy as np
+    a = rec.cpu().numpy() if hasattr(rec, "cpu") else np.asarray(rec, dtype=np.float32)
+    u = a.view(np.uint32)
+    return {"rho": a[..., 0], "rho_next": a[..., 1], "merit_prev": a[..., 2], "merits": a[..., 3:11],
+            "alpha": a[..., 11], "active": u[..., 12], "pcg_iters": u[..., 13]}
 
 
 class ProblemConfig(C.Structure):
@@ -167,6 +180,7 @@ def _declare(L):
         "gpt_read_csv": ([C.c_char_p, vp, C.c_size_t, P(u32), P(u32)], C.c_int),
         "gpt_form_ss": ([vp, u32, vp, vp, vp], C.c_int),
         "gpt_forward_dynamics_gradient": ([u32, vp, u32, vp, vp, vp], C.c_int),
+        "gpt_sqp_solve_batched_trace": ([vp, u32, vp, vp, vp, vp, vp, f32, vp, u32, vp, vp, vp, vp, vp], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -356,6 +370,28 @@ class Solver:
                                            _ptr(xu), C.cast(rr, C.c_void_p), rho_reset, C.cast(sts, C.c_void_p),
                                            _stream(stream)))
         return list(rr), StatsList(sts)
+
+    def sqp_solve_batched_trace(self, knot_points: Sequence[int], eePos_traj, lam, xu, rho: Sequence[float],
+                                trace_iters: int, rho_reset: float = 1e-3, stream=None):
+        """gpt_sqp_solve_batched_trace: the batched solve with its first trace_iters iterates recorded.
+        Returns (rho list, stats, trace) with trace = {"xu": [I, 21T], "lam": [I, 14T] (FP64),
+        "dz": [I, 21T], "rec": [I, B, 14] float32 rows of gpt_iterate_record (TRACE_REC fields)}."""
+        import torch
+        B = len(knot_points)
+        T = int(sum(knot_points))
+        dev = xu.device
+        tr = {"xu": torch.zeros(trace_iters, 21 * T, device=dev),
+              "lam": torch.zeros(trace_iters, 14 * T, dtype=torch.float64, device=dev),
+              "dz": torch.zeros(trace_iters, 21 * T, device=dev),
+              "rec": torch.zeros(trace_iters, B, TRACE_REC_FLOATS, device=dev)}
+        Ns = (C.c_uint32 * B)(*knot_points)
+        rr = (C.c_float * B)(*rho)
+        sts = (SqpStats * B)()
+        _check(lib().gpt_sqp_solve_batched_trace(self._h, B, C.cast(Ns, C.c_void_p), _ptr(eePos_traj), _ptr(lam),
+                                                 _ptr(xu), C.cast(rr, C.c_void_p), rho_reset,
+                                                 C.cast(sts, C.c_void_p), trace_iters, _ptr(tr["xu"]),
+                                                 _ptr(tr["lam"]), _ptr(tr["dz"]), _ptr(tr["rec"]), _stream(stream)))
+        return list(rr), StatsList(sts), tr
 
     def autotune(self, knot_points: Sequence[int], eePos_traj, lam, xu, rho: Sequence[float], stream=None) -> int:
         """gpt_autotune: pick and remember the fastest PCG cluster size for this batch shape."""

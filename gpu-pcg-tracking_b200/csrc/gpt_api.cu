@@ -36,7 +36,64 @@ gpt_status cuda_err(cudaError_t e, const char *where)
         if (e_ != cudaSuccess) return cuda_err(e_, #call);    \
     } while (0)
 
+// Makes a handle's device current for the duration of one entry point and restores the
+// caller's current device on return, so a handle may be used from a thread whose current
+// device is another GPU.
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev)
+    {
+        int cur = -1;
+        if (cudaGetDevice(&cur) != cudaSuccess) {
+            cudaGetLastError();
+            return;
+        }
+        if (cur != dev && cudaSetDevice(dev) == cudaSuccess) prev = cur;
+    }
+    ~DeviceGuard()
+    {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+    DeviceGuard(const DeviceGuard &) = delete;
+    DeviceGuard &operator=(const DeviceGuard &) = delete;
+};
+
 }  // namespace
+
+namespace gpt {
+cudaError_t ensure_func_attrs(const void *func, size_t smem_bytes, bool cluster16)
+{
+    static std::mutex mu;
+    struct Entry {
+        const void *func;
+        int device;
+        size_t smem;
+        bool cluster16;
+    };
+    static std::vector<Entry> done;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lk(mu);
+    Entry *hit = nullptr;
+    for (Entry &t : done)
+        if (t.func == func && t.device == dev) hit = &t;
+    if (hit && hit->smem >= smem_bytes && (hit->cluster16 || !cluster16)) return cudaSuccess;
+    e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes);
+    if (e != cudaSuccess) return e;
+    if (cluster16) {
+        e = cudaFuncSetAttribute(func, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+        if (e != cudaSuccess) return e;
+    }
+    if (hit) {
+        hit->smem = smem_bytes;
+        hit->cluster16 = hit->cluster16 || cluster16;
+    } else {
+        done.push_back({func, dev, smem_bytes, cluster16});
+    }
+    return cudaSuccess;
+}
+}  // namespace gpt
 
 constexpr int MAX_BRANCHES = 8;  // most concurrent part-batch branches of a graph iteration (sqp_graph)
 
@@ -102,6 +159,7 @@ struct gpt_handle {
     InstState *h_st = nullptr;
     uint32_t *h_pcg_out = nullptr;
     uint32_t *h_pcg_log = nullptr;
+    int *h_knot_off = nullptr, *h_knot_inst = nullptr;  // staging of the batch layout's upload
     // cached batch layout
     std::vector<int> off_cache;
     cudaEvent_t ev = nullptr;
@@ -316,6 +374,8 @@ gpt_status gpt_create(const gpt_problem_config *pc, const gpt_solver_config *sc,
     if (e == cudaSuccess) e = cudaMallocHost((void **)&h->h_st, sizeof(InstState) * B);
     if (e == cudaSuccess) e = cudaMallocHost((void **)&h->h_pcg_out, sizeof(uint32_t) * 2 * B);
     if (e == cudaSuccess) e = cudaMallocHost((void **)&h->h_pcg_log, sizeof(uint32_t) * B * sc->sqp_max_iter);
+    if (e == cudaSuccess) e = cudaMallocHost((void **)&h->h_knot_off, sizeof(int) * (B + 1));
+    if (e == cudaSuccess) e = cudaMallocHost((void **)&h->h_knot_inst, sizeof(int) * T);
     if (e == cudaSuccess) e = cudaMallocHost((void **)&h->h_trk_rows, sizeof(int) * (B + 1));
     if (e == cudaSuccess) e = cudaMallocHost((void **)&h->h_trk_inst, sizeof(TrackInst) * B);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->ev, cudaEventDisableTiming);
@@ -354,6 +414,7 @@ gpt_status gpt_get_phase_stats(gpt_handle *h, double *h_ms, uint64_t *h_launches
 gpt_status gpt_destroy(gpt_handle *h)
 {
     if (!h) return GPT_OK;
+    DeviceGuard dg(h->device);
     for (cudaEvent_t e : h->ev_pool) cudaEventDestroy(e);
     cudaFree(h->G); cudaFree(h->C); cudaFree(h->g); cudaFree(h->c); cudaFree(h->S);
     cudaFree(h->gamma); cudaFree(h->Ginv); cudaFree(h->dz); cudaFree(h->xs); cudaFree(h->knot_merit);
@@ -366,6 +427,7 @@ gpt_status gpt_destroy(gpt_handle *h)
     cudaFree(h->gxu); cudaFree(h->glam); cudaFree(h->ggoal); cudaFree(h->d_iter);
     cudaFree(h->trk_xu_old); cudaFree(h->trk_rows); cudaFree(h->trk_clk); cudaFree(h->trk_inst);
     cudaFreeHost(h->h_trk_rows); cudaFreeHost(h->h_trk_inst);
+    cudaFreeHost(h->h_knot_off); cudaFreeHost(h->h_knot_inst);
     if (h->cap_stream) cudaStreamDestroy(h->cap_stream);
     if (h->body_stream) cudaStreamDestroy(h->body_stream);
     for (int i = 1; i < MAX_BRANCHES; ++i) {
@@ -387,6 +449,7 @@ gpt_status gpt_form_kkt(gpt_handle *h, uint32_t N, const float *d_xu, const floa
                         float *d_G, float *d_C, float *d_g, float *d_c, gpt_stream_t stream)
 {
     if (!h || !d_xu || !d_goal || !d_xs || !d_G || !d_C || !d_g || !d_c) return set_err(GPT_ERR_BAD_ARG, "null argument");
+    DeviceGuard dg(h->device);
     if (!check_n(h, N)) return set_err(GPT_ERR_BAD_ARG, "knot_points out of range");
     GPT_CUDA(launch_kkt(single_view(N), to_params(h->pc), d_xu, d_goal, d_xs, d_G, d_C, d_g, d_c, h->num_sms,
                         (cudaStream_t)stream));
@@ -399,6 +462,7 @@ gpt_status gpt_form_schur(gpt_handle *h, uint32_t N, float rho, const float *d_G
 {
     if (!h || !d_G || !d_C || !d_g || !d_c || !d_S || !d_Pinv || !d_gamma || !d_Ginv)
         return set_err(GPT_ERR_BAD_ARG, "null argument");
+    DeviceGuard dg(h->device);
     if (!check_n(h, N)) return set_err(GPT_ERR_BAD_ARG, "knot_points out of range");
     GPT_CUDA(launch_schur(0, single_view(N), rho, d_G, d_C, d_g, d_c, d_S, d_Pinv, d_gamma, d_Ginv, d_Ginv64, nullptr,
                           1, h->num_sms, (cudaStream_t)stream));
@@ -411,6 +475,7 @@ gpt_status gpt_form_schur_csc(gpt_handle *h, uint32_t N, float rho, const float 
 {
     if (!h || !d_G || !d_C || !d_g || !d_c || !d_val || !d_gamma || !d_Ginv)
         return set_err(GPT_ERR_BAD_ARG, "null argument");
+    DeviceGuard dg(h->device);
     if (!check_n(h, N)) return set_err(GPT_ERR_BAD_ARG, "knot_points out of range");
     GPT_CUDA(launch_schur(2, single_view(N), rho, d_G, d_C, d_g, d_c, nullptr, nullptr, d_gamma, d_Ginv, nullptr, d_val,
                           0, h->num_sms, (cudaStream_t)stream));
@@ -420,6 +485,7 @@ gpt_status gpt_form_schur_csc(gpt_handle *h, uint32_t N, float rho, const float 
 gpt_status gpt_form_ss(gpt_handle *h, uint32_t N, const float *d_S, float *d_Pinv, gpt_stream_t stream)
 {
     if (!h || !d_S || !d_Pinv) return set_err(GPT_ERR_BAD_ARG, "null argument");
+    DeviceGuard dg(h->device);
     if (!check_n(h, N)) return set_err(GPT_ERR_BAD_ARG, "knot_points out of range");
     GPT_CUDA(launch_form_ss((int)N, d_S, d_Pinv, (cudaStream_t)stream));
     return GPT_OK;
@@ -446,6 +512,7 @@ gpt_status gpt_pcg(gpt_handle *h, uint32_t N, const float *d_S, const float *d_P
                    uint32_t *h_iters, uint8_t *h_maxit, gpt_stream_t stream)
 {
     if (!h || !d_S || !d_Pinv || !d_gamma || !d_lambda) return set_err(GPT_ERR_BAD_ARG, "null argument");
+    DeviceGuard dg(h->device);
     if (!check_n(h, N) || exit_mode > 1) return set_err(GPT_ERR_BAD_ARG, "knot_points/exit_mode out of range");
     if (((uintptr_t)d_S & 15u) != 0) return set_err(GPT_ERR_BAD_ARG, "d_S must be 16-byte aligned");
     cudaStream_t s = (cudaStream_t)stream;
@@ -474,6 +541,7 @@ gpt_status gpt_compute_dz(gpt_handle *h, uint32_t N, const float *d_Ginv, const 
 {
     if (!h || (!d_Ginv && !d_Ginv64) || !d_C || !d_g || (!d_lambda && !d_lambda64) || !d_dz)
         return set_err(GPT_ERR_BAD_ARG, "null argument");
+    DeviceGuard dg(h->device);
     if (!check_n(h, N)) return set_err(GPT_ERR_BAD_ARG, "knot_points out of range");
     GPT_CUDA(launch_dz(single_view(N), d_Ginv, d_Ginv64, d_C, d_g, d_lambda, d_lambda64, d_dz, h->num_sms,
                        (cudaStream_t)stream));
@@ -484,6 +552,7 @@ gpt_status gpt_compute_merit(gpt_handle *h, uint32_t N, const float *d_xu, const
                              gpt_stream_t stream)
 {
     if (!h || !d_xu || !d_goal || !d_merit) return set_err(GPT_ERR_BAD_ARG, "null argument");
+    DeviceGuard dg(h->device);
     if (!check_n(h, N)) return set_err(GPT_ERR_BAD_ARG, "knot_points out of range");
     cudaStream_t s = (cudaStream_t)stream;
     BatchView bv = single_view(N);
@@ -497,6 +566,7 @@ gpt_status gpt_ls_compute_merit(gpt_handle *h, uint32_t N, const float *d_xs, co
                                 const float *d_dz, float *d_merits, gpt_stream_t stream)
 {
     if (!h || !d_xs || !d_xu || !d_goal || !d_dz || !d_merits) return set_err(GPT_ERR_BAD_ARG, "null argument");
+    DeviceGuard dg(h->device);
     if (!check_n(h, N)) return set_err(GPT_ERR_BAD_ARG, "knot_points out of range");
     cudaStream_t s = (cudaStream_t)stream;
     BatchView bv = single_view(N);
@@ -571,11 +641,13 @@ static gpt_status setup_batch(gpt_handle *h, uint32_t B, const uint32_t *Ns, con
         minN = Ns[b] < (uint32_t)minN ? (int)Ns[b] : minN;
     }
     if (off != h->off_cache) {
-        std::vector<int> inst(total);
+        // stream-ordered upload from pinned staging: every entry point that reaches here synchronises
+        // its stream before returning, so the staging is free again at the next call
+        for (uint32_t b = 0; b <= B; ++b) h->h_knot_off[b] = off[b];
         for (uint32_t b = 0; b < B; ++b)
-            for (int k = off[b]; k < off[b + 1]; ++k) inst[k] = (int)b;
-        GPT_CUDA(cudaMemcpy(h->knot_off, off.data(), sizeof(int) * (B + 1), cudaMemcpyHostToDevice));
-        GPT_CUDA(cudaMemcpy(h->knot_inst, inst.data(), sizeof(int) * total, cudaMemcpyHostToDevice));
+            for (int k = off[b]; k < off[b + 1]; ++k) h->h_knot_inst[k] = (int)b;
+        GPT_CUDA(cudaMemcpyAsync(h->knot_off, h->h_knot_off, sizeof(int) * (B + 1), cudaMemcpyHostToDevice, s));
+        GPT_CUDA(cudaMemcpyAsync(h->knot_inst, h->h_knot_inst, sizeof(int) * total, cudaMemcpyHostToDevice, s));
         h->off_cache = off;
     }
     for (uint32_t b = 0; b < B; ++b) {
@@ -619,7 +691,8 @@ static gpt_status enqueue_prologue(gpt_handle *h, const SqpPlan &pl, const float
 // One SQP iteration for every active instance (toplevel.cuh:254-446); leaves the number of
 // instances still active in h->d_active (cleared first unless reset_active is false).
 static gpt_status enqueue_iteration(gpt_handle *h, const SqpPlan &pl, const float *d_goal, float *d_lambda,
-                                    float *d_xu, cudaStream_t s, bool reset_active = true)
+                                    float *d_xu, cudaStream_t s, bool reset_active = true,
+                                    float *merits_out = nullptr)
 {
     const BatchView &bv = pl.bv;
     const SolverParams &SP = pl.SP;
@@ -656,7 +729,7 @@ static gpt_status enqueue_iteration(gpt_handle *h, const SqpPlan &pl, const floa
     if (reset_active) GPT_CUDA(cudaMemsetAsync(h->d_active, 0, sizeof(uint32_t), s));
     {
         PhaseTimer t(h, s, GPT_PHASE_ACCEPT);
-        GPT_CUDA(launch_accept(bv, 1, SP, h->knot_merit, h->dz, d_xu, nullptr, h->d_active, ns, s));
+        GPT_CUDA(launch_accept(bv, 1, SP, h->knot_merit, h->dz, d_xu, merits_out, h->d_active, ns, s));
     }
     return GPT_OK;
 }
@@ -807,9 +880,18 @@ static gpt_status sqp_graph_for(gpt_handle *h, const SqpPlan &pl, cudaGraphExec_
     return GPT_OK;
 }
 
+// Buffers of gpt_sqp_solve_batched_trace
+struct SqpTrace {
+    uint32_t iters;
+    float *xu;
+    double *lam;
+    float *dz;
+    gpt_iterate_record *rec;
+};
+
 static gpt_status sqp_run(gpt_handle *h, uint32_t B, const uint32_t *Ns, const float *d_goal, float *d_lambda,
                           float *d_xu, float *h_rho, float rho_reset, gpt_sqp_stats *h_stats, uint32_t *h_pcg_iters,
-                          uint8_t *h_pcg_exit, cudaStream_t s)
+                          uint8_t *h_pcg_exit, cudaStream_t s, const SqpTrace *tr = nullptr)
 {
     BatchView bv;
     int maxN = 0, minN = 0;
@@ -825,7 +907,7 @@ static gpt_status sqp_run(gpt_handle *h, uint32_t B, const uint32_t *Ns, const f
     }
     const SqpPlan plan{bv, P, SP, maxN, minN, h->num_sms};
 
-    if (SP.sqp_graph && !h->profile) {
+    if (SP.sqp_graph && !h->profile && !tr) {
         // one graph launch for the whole solve on handle-owned copies of the caller's buffers
         const size_t nxu = (size_t)NX * bv.total_knots - NC, nl = (size_t)NS * bv.total_knots;
         GPT_CUDA(cudaMemcpyAsync(h->gxu, d_xu, sizeof(float) * nxu, cudaMemcpyDeviceToDevice, s));
@@ -844,9 +926,22 @@ static gpt_status sqp_run(gpt_handle *h, uint32_t B, const uint32_t *Ns, const f
             const gpt_status st = enqueue_prologue(h, plan, d_goal, d_xu, s);
             if (st != GPT_OK) return st;
         }
+        const size_t T = (size_t)bv.total_knots;
         for (uint32_t it = 0; it < SP.sqp_max_iter; ++it) {
-            const gpt_status st = enqueue_iteration(h, plan, d_goal, d_lambda, d_xu, s);
+            const bool rec = tr && it < tr->iters;
+            if (rec && tr->xu)
+                GPT_CUDA(cudaMemcpyAsync(tr->xu + NX * T * it, d_xu, sizeof(float) * (NX * T - NC),
+                                         cudaMemcpyDeviceToDevice, s));
+            if (rec && tr->rec) GPT_CUDA(launch_trace_record(bv, 0, nullptr, tr->rec + (size_t)B * it, plan.ns, s));
+            const gpt_status st = enqueue_iteration(h, plan, d_goal, d_lambda, d_xu, s, true, rec ? h->merits : nullptr);
             if (st != GPT_OK) return st;
+            if (rec && tr->lam)
+                GPT_CUDA(cudaMemcpyAsync(tr->lam + NS * T * it, h->lam64, sizeof(double) * NS * T,
+                                         cudaMemcpyDeviceToDevice, s));
+            if (rec && tr->dz)
+                GPT_CUDA(cudaMemcpyAsync(tr->dz + NX * T * it, h->dz, sizeof(float) * (NX * T - NC),
+                                         cudaMemcpyDeviceToDevice, s));
+            if (rec && tr->rec) GPT_CUDA(launch_trace_record(bv, 1, h->merits, tr->rec + (size_t)B * it, plan.ns, s));
             GPT_CUDA(cudaMemcpyAsync(h->h_active, h->d_active, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
             GPT_CUDA(cudaEventRecord(h->ev, s));
             GPT_CUDA(cudaEventSynchronize(h->ev));
@@ -858,11 +953,12 @@ static gpt_status sqp_run(gpt_handle *h, uint32_t B, const uint32_t *Ns, const f
         GPT_CUDA(cudaMemcpyAsync(h->h_pcg_log, h->pcg_log, sizeof(uint32_t) * SP.sqp_max_iter, cudaMemcpyDeviceToHost, s));
     GPT_CUDA(cudaStreamSynchronize(s));
     if (h->profile) collect_phase_times(h);
-    bool nonfinite = false;
+    bool nonfinite = false, factor = false;
     for (uint32_t b = 0; b < B; ++b) {
         const InstState &st = h->h_st[b];
         if (h_rho) h_rho[b] = st.rho;
-        if (st.exit_flags & 4u) nonfinite = true;
+        if (st.exit_flags & GPT_EXIT_NONFINITE) nonfinite = true;
+        if (st.exit_flags & GPT_EXIT_FACTOR) factor = true;
         if (h_stats) {
             gpt_sqp_stats &o = h_stats[b];
             o.sqp_iters = st.sqp_iters;
@@ -883,6 +979,8 @@ static gpt_status sqp_run(gpt_handle *h, uint32_t B, const uint32_t *Ns, const f
             if (h_pcg_exit) h_pcg_exit[i] = (uint8_t)(v >> 31);
         }
     }
+    if (factor)
+        return set_err(GPT_ERR_FACTOR, "(Q + rho I) or (R + rho I) not positive definite in at least one instance");
     if (nonfinite) return set_err(GPT_ERR_NONFINITE, "non-finite merit or PCG reduction in at least one instance");
     return GPT_OK;
 }
@@ -892,6 +990,7 @@ gpt_status gpt_sqp_solve(gpt_handle *h, uint32_t N, const float *d_goal, float *
                          gpt_stream_t stream)
 {
     if (!h || !d_goal || !d_lambda || !d_xu || !h_rho) return set_err(GPT_ERR_BAD_ARG, "null argument");
+    DeviceGuard dg(h->device);
     return sqp_run(h, 1, &N, d_goal, d_lambda, d_xu, h_rho, rho_reset, h_stats, h_pcg_iters, h_pcg_exit,
                    (cudaStream_t)stream);
 }
@@ -901,14 +1000,29 @@ gpt_status gpt_sqp_solve_batched(gpt_handle *h, uint32_t B, const uint32_t *h_N,
                                  gpt_stream_t stream)
 {
     if (!h || !h_N || !d_goal || !d_lambda || !d_xu) return set_err(GPT_ERR_BAD_ARG, "null argument");
+    DeviceGuard dg(h->device);
     return sqp_run(h, B, h_N, d_goal, d_lambda, d_xu, h_rho, rho_reset, h_stats, nullptr, nullptr,
                    (cudaStream_t)stream);
+}
+
+gpt_status gpt_sqp_solve_batched_trace(gpt_handle *h, uint32_t B, const uint32_t *h_N, const float *d_goal,
+                                       float *d_lambda, float *d_xu, float *h_rho, float rho_reset,
+                                       gpt_sqp_stats *h_stats, uint32_t trace_iters, float *d_trace_xu,
+                                       double *d_trace_lambda, float *d_trace_dz, gpt_iterate_record *d_trace_rec,
+                                       gpt_stream_t stream)
+{
+    if (!h || !h_N || !d_goal || !d_lambda || !d_xu) return set_err(GPT_ERR_BAD_ARG, "null argument");
+    DeviceGuard dg(h->device);
+    const SqpTrace tr{trace_iters, d_trace_xu, d_trace_lambda, d_trace_dz, d_trace_rec};
+    return sqp_run(h, B, h_N, d_goal, d_lambda, d_xu, h_rho, rho_reset, h_stats, nullptr, nullptr,
+                   (cudaStream_t)stream, &tr);
 }
 
 gpt_status gpt_autotune(gpt_handle *h, uint32_t B, const uint32_t *h_N, const float *d_goal, const float *d_lambda,
                         const float *d_xu, const float *h_rho, uint32_t *h_cluster_out, gpt_stream_t stream)
 {
     if (!h || !h_N || !d_goal || !d_lambda || !d_xu || !h_rho) return set_err(GPT_ERR_BAD_ARG, "null argument");
+    DeviceGuard dg(h->device);
     if (B == 0 || B > h->pc.max_batch) return set_err(GPT_ERR_CAPACITY, "batch exceeds handle capacity");
     cudaStream_t s = (cudaStream_t)stream;
     int total = 0, maxN = 0, minN = 1 << 30;
@@ -993,6 +1107,7 @@ gpt_status gpt_sqp_adjoint(gpt_handle *h, uint32_t B, const uint32_t *h_N, const
     if (!h || !h_N || !d_goal || !d_xs || !d_xu || !h_rho || !d_grad_xu_next || !d_grad_goal || !d_grad_qd ||
         !d_grad_r || !d_grad_q_ee)
         return set_err(GPT_ERR_BAD_ARG, "null argument");
+    DeviceGuard dg(h->device);
     cudaStream_t s = (cudaStream_t)stream;
     BatchView bv;
     int maxN = 0, minN = 0;
@@ -1044,6 +1159,8 @@ gpt_status gpt_sqp_adjoint(gpt_handle *h, uint32_t B, const uint32_t *h_N, const
     GPT_CUDA(cudaStreamSynchronize(s));
     for (uint32_t b = 0; b < B; ++b) {
         const InstState &st = h->h_st[b];
+        if (st.exit_flags & GPT_EXIT_FACTOR)
+            return set_err(GPT_ERR_FACTOR, "(Q + rho I) or (R + rho I) not positive definite in the adjoint");
         if (st.exit_flags & 4u) return set_err(GPT_ERR_NONFINITE, "non-finite value in an adjoint solve");
         if (st.pcg_maxiter_count) return set_err(GPT_ERR_NONFINITE, "PCG reached pcg_max_iter in the adjoint");
     }
@@ -1142,6 +1259,7 @@ gpt_status gpt_track_batched(gpt_handle *h, uint32_t B, const uint32_t *h_N, con
 {
     if (!h || !h_N || !h_S || !d_eePos_traj || !d_xu_traj || !d_xs || !d_err)
         return set_err(GPT_ERR_BAD_ARG, "null argument");
+    DeviceGuard dg(h->device);
     gpt_track_config tc;
     gpt_default_track_config(&tc);
     if (tc_in) tc = *tc_in;
@@ -1238,6 +1356,7 @@ gpt_status gpt_simulate(gpt_handle *h, uint32_t N, float *d_xs, const float *d_x
                         double sim_time_us, float sim_step, gpt_stream_t stream)
 {
     if (!h || !d_xs || !d_xu) return set_err(GPT_ERR_BAD_ARG, "null argument");
+    DeviceGuard dg(h->device);
     if (!check_n(h, N)) return set_err(GPT_ERR_BAD_ARG, "knot_points out of range");
     if (!(sim_step > 0.f) || !(sim_time_us >= 0.0) || !(time_offset_us >= 0.0) ||
         sim_time_us * 1e-6 / (double)sim_step > 1e6)

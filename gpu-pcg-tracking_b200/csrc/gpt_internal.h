@@ -25,6 +25,12 @@ struct SolverParams {
     uint32_t sqp_graph;         // the SQP loop as one CUDA graph with a device-side while loop
 };
 
+// cudaFuncSetAttribute(MaxDynamicSharedMemorySize >= smem_bytes, and NonPortableClusterSizeAllowed when
+// cluster16) for func on the CURRENT device, once per (kernel, device); thread-safe.  Function
+// attributes apply to the device that is current when they are set, so a per-process flag is not enough
+// when handles live on several devices.
+cudaError_t ensure_func_attrs(const void *func, size_t smem_bytes, bool cluster16 = false);
+
 cudaError_t launch_kkt(const BatchView &bv, const ProblemParams &P, const float *xu, const float *goal,
                        const float *xs, float *G, float *C, float *g, float *c, int num_sms, cudaStream_t s);
 // Ginv64 (optional) receives the inverses in FP64; need_pinv = 0 skips the theta inversion in mode 1
@@ -115,5 +121,10 @@ namespace gpt {
 // for C-ABI entry points defined outside gpt_api.cu: the error text gpt_last_error()
 // returns, and the device-side form of a problem config
 gpt_status record_error(gpt_status st, const char *msg);
+// per-iteration scalars of gpt_sqp_solve_batched_trace: phase 0 (before an iteration) records rho,
+// the iterate's merit and the activity; phase 1 (after it) the line-search merits (merits, 8 per
+// instance), the accepted step (the accept kernel's argmin), the next rho and the PCG count
+cudaError_t launch_trace_record(const BatchView &bv, int phase, const float *merits, gpt_iterate_record *rec,
+                                int num_sms, cudaStream_t s);
 ProblemParams problem_params(const gpt_problem_config &pc);
 }  // namespace gpt

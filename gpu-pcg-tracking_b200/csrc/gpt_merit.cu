@@ -372,6 +372,8 @@ __global__ void __launch_bounds__(ACC_THREADS)
                         s.active = 0;
                         s.exit_flags |= 8u;
                     }
+                    // a failed factorisation or a non-finite reduction leaves no usable iterate
+                    if (s.exit_flags & (GPT_EXIT_NONFINITE | GPT_EXIT_FACTOR)) s.active = 0;
                 }
                 if (active_count && s.active) atomicAdd(active_count, 1u);
             }
@@ -401,6 +403,51 @@ cudaError_t launch_accept(const BatchView &bv, int mode, const SolverParams &SP,
 }
 
 // Per-instance start of a solve: x_s = x_0 (toplevel.cuh:110), state from the host image.
+__global__ void trace_record_kernel(BatchView bv, int phase, const float *__restrict__ merits,
+                                    gpt_iterate_record *__restrict__ rec)
+{
+    for (int b = bv.b0 + blockIdx.x * blockDim.x + threadIdx.x; b < bv.b0 + bv.B; b += gridDim.x * blockDim.x) {
+        const InstState &s = bv.st[b];
+        gpt_iterate_record &r = rec[b];
+        if (phase == 0) {
+            r.rho = s.rho;
+            r.merit_prev = s.merit0;
+            r.active = s.active;
+            r.rho_next = s.rho;
+            r.alpha = 0.f;
+            r.pcg_iters = 0;
+            for (int a = 0; a < NUM_ALPHAS; ++a) r.merits[a] = 0.f;
+            continue;
+        }
+        if (!r.active) continue;
+        // the accept kernel's decision, same comparisons in the same order
+        float minm = r.merit_prev;
+        int best = 0;
+        for (int a = 0; a < NUM_ALPHAS; ++a) {
+            const float m = merits[NUM_ALPHAS * b + a];
+            r.merits[a] = m;
+            if (m < minm) {
+                minm = m;
+                best = a;
+            }
+        }
+        r.alpha = (minm == r.merit_prev) ? 0.f : -1.f / (float)(1 << best);
+        r.rho_next = s.rho;
+        r.pcg_iters = s.last_pcg_iters;
+    }
+}
+
+cudaError_t launch_trace_record(const BatchView &bv, int phase, const float *merits, gpt_iterate_record *rec,
+                                int num_sms, cudaStream_t s)
+{
+    if (bv.B <= 0) return cudaSuccess;
+    if (!bv.st || !rec || (phase == 1 && !merits)) return cudaErrorInvalidValue;
+    int blocks = (bv.B + 127) / 128;
+    if (blocks > num_sms) blocks = num_sms;
+    trace_record_kernel<<<blocks, 128, 0, s>>>(bv, phase, merits, rec);
+    return cudaGetLastError();
+}
+
 __global__ void init_kernel(BatchView bv, const float *__restrict__ xu, float *__restrict__ xs)
 {
     for (int b = bv.b0 + blockIdx.x; b < bv.b0 + bv.B; b += gridDim.x) {

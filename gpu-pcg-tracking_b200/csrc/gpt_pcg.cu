@@ -1673,11 +1673,9 @@ static cudaError_t launch_pcg_pair_t(const BatchView &bv, int max_n, const void 
 {
     auto kern = pcg_pair_kernel<FMT>;
     const size_t smem = pcg_pair_smem_bytes(max_n);
-    static size_t attr_smem = 0;
-    if (smem > attr_smem) {
-        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    {
+        const cudaError_t e = ensure_func_attrs((const void *)kern, smem);
         if (e != cudaSuccess) return e;
-        attr_smem = smem;
     }
     kern<<<bv.B, PAIR_THREADS, smem, s>>>(bv, S, gamma, gamma64, lambda, lambda64, ws, max_iter, tol, exit_mode,
                                           out_iters, pcg_log, log_stride);
@@ -1706,15 +1704,9 @@ static cudaError_t launch_pcg_cs(const BatchView &bv, int kpc_max, const float *
 {
     auto kern = pcg_cluster_kernel<CS, FMT>;
     const size_t smem = pcg_cluster_smem_bytes(kpc_max);
-    static size_t attr_smem = 0;
-    if (smem > attr_smem) {
-        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    {
+        const cudaError_t e = ensure_func_attrs((const void *)kern, smem, CS > 8);
         if (e != cudaSuccess) return e;
-        if (CS > 8) {
-            e = cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
-            if (e != cudaSuccess) return e;
-        }
-        attr_smem = smem;
     }
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)(bv.B * CS), 1, 1);
@@ -1740,15 +1732,9 @@ static cudaError_t launch_pcg_chain_cs(const BatchView &bv, int kpc_max, const v
 {
     auto kern = pcg_chain_kernel<CS, FMT>;
     const size_t smem = pcg_chain_smem_bytes(kpc_max);
-    static size_t attr_smem = 0;
-    if (smem > attr_smem) {
-        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    {
+        const cudaError_t e = ensure_func_attrs((const void *)kern, smem, CS > 8);
         if (e != cudaSuccess) return e;
-        if (CS > 8) {
-            e = cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
-            if (e != cudaSuccess) return e;
-        }
-        attr_smem = smem;
     }
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)(bv.B * CS), 1, 1);

@@ -267,14 +267,21 @@ __global__ void __launch_bounds__(32 * SCHUR_WARPS)
 // only the FP32 rounding of the KKT data (G, C, g, c).
 // ---------------------------------------------------------------------------
 
+// Pivot test of the Schur complement's inverses: (Q + rho I) and (R + rho I) must be positive
+// definite, so every Gauss-Jordan pivot must be positive and not vanish against the diagonal entry it
+// came from (a relative 1e-13 catches a singular matrix whose exact zero pivot rounding turned into a
+// tiny number of either sign; NaN fails too)
+constexpr double PIVOT_REL_MIN = 1e-13;
+
 // FP64 Gauss-Jordan inverse of the n x n matrix (A + shift I), A column-major with leading
 // dimension LD; the inverse goes column-major with leading dimension LD to Ainv (and, when given,
-// Ainv32 / Ainv64g)
+// Ainv32 / Ainv64g).  Returns false (on every lane) if a pivot failed the test above.
 template <int n, int LD = n>
-__device__ __forceinline__ void warp_inverse64(const float *A, double shift, double *Ainv, int lane,
+__device__ __forceinline__ bool warp_inverse64(const float *A, double shift, double *Ainv, int lane,
                                                float *Ainv32, double *Ainv64g)
 {
     double col[n];
+    double diag_own = 0.0;  // lane p < n: the diagonal entry (p, p) of A + shift I
     const bool left = lane < n, right = (lane >= n) && (lane < 2 * n);
 #pragma unroll
     for (int r = 0; r < n; ++r) {
@@ -282,10 +289,14 @@ __device__ __forceinline__ void warp_inverse64(const float *A, double shift, dou
         if (left) v = (double)A[r + LD * lane] + ((r == lane) ? shift : 0.0);
         else if (right) v = (r == lane - n) ? 1.0 : 0.0;
         col[r] = v;
+        if (left && r == lane) diag_own = v;
     }
+    bool ok = true;
 #pragma unroll
     for (int p = 0; p < n; ++p) {
         const double piv = __shfl_sync(0xffffffffu, col[p], p);
+        const double d0 = __shfl_sync(0xffffffffu, diag_own, p);
+        ok = ok && (piv > PIVOT_REL_MIN * d0) && (d0 > 0.0);
         const double prow = col[p] * __drcp_rn(piv);
 #pragma unroll
         for (int r = 0; r < n; ++r) {
@@ -308,6 +319,7 @@ __device__ __forceinline__ void warp_inverse64(const float *A, double shift, dou
             for (int r = 0; r < n; ++r) Ainv64g[r + LD * cc] = col[r];
         }
     }
+    return ok;
 }
 
 // (Q + shift I)^{-1} of a 14x14 state block.  The blocks kkt_kernel writes are block diagonal --
@@ -316,7 +328,7 @@ __device__ __forceinline__ void warp_inverse64(const float *A, double shift, dou
 // without pivoting never mixes the two blocks of a block-diagonal matrix (every update it would
 // make across them multiplies an exact zero), so this is the same arithmetic as the full 14x14
 // elimination, result for result; any other Q takes the full elimination.
-__device__ __forceinline__ void warp_inverse64_state(const float *Q, double shift, double *Ainv, int lane,
+__device__ __forceinline__ bool warp_inverse64_state(const float *Q, double shift, double *Ainv, int lane,
                                                      float *Ainv32, double *Ainv64g)
 {
     bool ok = true;
@@ -324,38 +336,45 @@ __device__ __forceinline__ void warp_inverse64_state(const float *Q, double shif
         const int r = e % NS, cc = e / NS;
         if (((r < NC) != (cc < NC)) || (r >= NC && cc >= NC && r != cc)) ok = ok && (Q[e] == 0.f);
     }
-    if (!__all_sync(0xffffffffu, ok)) {
-        warp_inverse64<NS>(Q, shift, Ainv, lane, Ainv32, Ainv64g);
-        return;
-    }
-    warp_inverse64<NC, NS>(Q, shift, Ainv, lane, Ainv32, Ainv64g);
+    if (!__all_sync(0xffffffffu, ok)) return warp_inverse64<NS>(Q, shift, Ainv, lane, Ainv32, Ainv64g);
+    bool piv_ok = warp_inverse64<NC, NS>(Q, shift, Ainv, lane, Ainv32, Ainv64g);
     for (int e = lane; e < SS; e += 32) {
         const int r = e % NS, cc = e / NS;
         if (r < NC && cc < NC) continue;
-        const double v = (r == cc) ? __drcp_rn((double)Q[e] + shift) : 0.0;
+        double v = 0.0;
+        if (r == cc) {
+            const double d = (double)Q[e] + shift;
+            piv_ok = piv_ok && (d > 0.0);
+            v = __drcp_rn(d);
+        }
         Ainv[e] = v;
         if (Ainv32) Ainv32[e] = (float)v;
         if (Ainv64g) Ainv64g[e] = v;
     }
+    return __all_sync(0xffffffffu, piv_ok);
 }
 // (R + shift I)^{-1} of a 7x7 control block: reciprocals when R is diagonal (kkt_kernel's R_COST I;
 // the same arithmetic as the elimination), else Gauss-Jordan
-__device__ __forceinline__ void warp_inverse64_control(const float *R, double shift, double *Ainv, int lane,
+__device__ __forceinline__ bool warp_inverse64_control(const float *R, double shift, double *Ainv, int lane,
                                                        float *Ainv32, double *Ainv64g)
 {
     bool ok = true;
     for (int e = lane; e < CC; e += 32)
         if (e % NC != e / NC) ok = ok && (R[e] == 0.f);
-    if (!__all_sync(0xffffffffu, ok)) {
-        warp_inverse64<NC>(R, shift, Ainv, lane, Ainv32, Ainv64g);
-        return;
-    }
+    if (!__all_sync(0xffffffffu, ok)) return warp_inverse64<NC>(R, shift, Ainv, lane, Ainv32, Ainv64g);
+    bool piv_ok = true;
     for (int e = lane; e < CC; e += 32) {
-        const double v = (e % NC == e / NC) ? __drcp_rn((double)R[e] + shift) : 0.0;
+        double v = 0.0;
+        if (e % NC == e / NC) {
+            const double d = (double)R[e] + shift;
+            piv_ok = piv_ok && (d > 0.0);
+            v = __drcp_rn(d);
+        }
         Ainv[e] = v;
         if (Ainv32) Ainv32[e] = (float)v;
         if (Ainv64g) Ainv64g[e] = v;
     }
+    return __all_sync(0xffffffffu, piv_ok);
 }
 
 // One warp's shared memory: the knot's KKT blocks staged as FP32 (one batch of loads per knot), the
@@ -393,8 +412,10 @@ __global__ void __launch_bounds__(32 * SCHUR_WARPS, 5)
             for (int e = lane; e < SS; e += 32) sm.Gk[e] = Q0[e];
             if (lane < NS) sm.qk[lane] = (double)g[(size_t)NX * j + lane];
             __syncwarp();
-            warp_inverse64_state(sm.Gk, rho, sm.Qki, lane, (N == 1 && Ginv) ? Ginv + (size_t)G_STRIDE * j : nullptr,
-                                 N == 1 ? Ginv64 + (size_t)G_STRIDE * j : nullptr);
+            const bool ok0 = warp_inverse64_state(sm.Gk, rho, sm.Qki, lane,
+                                                  (N == 1 && Ginv) ? Ginv + (size_t)G_STRIDE * j : nullptr,
+                                                  N == 1 ? Ginv64 + (size_t)G_STRIDE * j : nullptr);
+            if (!ok0 && lane == 0) atomicOr(&bv.st[b].exit_flags, GPT_EXIT_FACTOR);
             __syncwarp();
             if (lane < NS) {
                 double acc = 0.0;
@@ -450,10 +471,11 @@ __global__ void __launch_bounds__(32 * SCHUR_WARPS, 5)
         __syncwarp();
         float *Gi32 = Ginv ? Ginv + (size_t)G_STRIDE * (j - 1) : nullptr;
         double *Gi64 = Ginv64 + (size_t)G_STRIDE * (j - 1);
-        warp_inverse64_state(sm.Gm1, rho, sm.Qki, lane, Gi32, Gi64);
-        warp_inverse64_state(sm.Gk, rho, sm.Qkp1i, lane, (k == N - 1 && Ginv) ? Ginv + (size_t)G_STRIDE * j : nullptr,
-                             k == N - 1 ? Ginv64 + (size_t)G_STRIDE * j : nullptr);
-        warp_inverse64_control(sm.Gm1 + SS, rho, sm.Rki, lane, Gi32 ? Gi32 + SS : nullptr, Gi64 + SS);
+        bool ok = warp_inverse64_state(sm.Gm1, rho, sm.Qki, lane, Gi32, Gi64);
+        ok = warp_inverse64_state(sm.Gk, rho, sm.Qkp1i, lane, (k == N - 1 && Ginv) ? Ginv + (size_t)G_STRIDE * j : nullptr,
+                                  k == N - 1 ? Ginv64 + (size_t)G_STRIDE * j : nullptr) && ok;
+        ok = warp_inverse64_control(sm.Gm1 + SS, rho, sm.Rki, lane, Gi32 ? Gi32 + SS : nullptr, Gi64 + SS) && ok;
+        if (!ok && lane == 0) atomicOr(&bv.st[b].exit_flags, GPT_EXIT_FACTOR);
         __syncwarp();
         // the products on the FP64 tensor cores, 14x14 (14x7) blocks padded to 16x16 (16x8)
         const float *Am = sm.C, *Bm = sm.C + SS;  // -A, -B
@@ -510,11 +532,9 @@ cudaError_t launch_schur64(const BatchView &bv, const float *G, const float *C, 
     int blocks = (bv.total_knots + SCHUR_WARPS - 1) / SCHUR_WARPS;
     const int cap = num_sms * 16;
     if (blocks > cap) blocks = cap;
-    static bool attr_done = false;
-    if (!attr_done) {
-        cudaError_t e = cudaFuncSetAttribute(schur64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    {
+        const cudaError_t e = ensure_func_attrs((const void *)schur64_kernel, smem);
         if (e != cudaSuccess) return e;
-        attr_done = true;
     }
     schur64_kernel<<<blocks, 32 * SCHUR_WARPS, smem, s>>>(bv, G, C, g, c, S64, gamma64, Ginv, Ginv64);
     return cudaGetLastError();
@@ -529,29 +549,22 @@ cudaError_t launch_schur(int mode, const BatchView &bv, float rho_scalar, const 
     int blocks = (bv.total_knots + SCHUR_WARPS - 1) / SCHUR_WARPS;
     const int cap = num_sms * 16;
     if (blocks > cap) blocks = cap;
-    static bool attr_done[3] = {false, false, false};
+    {
+        const void *fn = mode == 0 ? (const void *)schur_kernel<0>
+                                   : (mode == 1 ? (const void *)schur_kernel<1> : (const void *)schur_kernel<2>);
+        const cudaError_t e = ensure_func_attrs(fn, smem);
+        if (e != cudaSuccess) return e;
+    }
     switch (mode) {
     case 0:
-        if (!attr_done[0]) {
-            cudaFuncSetAttribute(schur_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            attr_done[0] = true;
-        }
         schur_kernel<0><<<blocks, 32 * SCHUR_WARPS, smem, s>>>(bv, rho_scalar, G, C, g, c, S, Pinv, gamma,
                                                                Ginv, Ginv64, csc_val, need_pinv);
         break;
     case 1:
-        if (!attr_done[1]) {
-            cudaFuncSetAttribute(schur_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            attr_done[1] = true;
-        }
         schur_kernel<1><<<blocks, 32 * SCHUR_WARPS, smem, s>>>(bv, rho_scalar, G, C, g, c, S, Pinv, gamma,
                                                                Ginv, Ginv64, csc_val, need_pinv);
         break;
     default:
-        if (!attr_done[2]) {
-            cudaFuncSetAttribute(schur_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            attr_done[2] = true;
-        }
         schur_kernel<2><<<blocks, 32 * SCHUR_WARPS, smem, s>>>(bv, rho_scalar, G, C, g, c, S, Pinv, gamma,
                                                                Ginv, Ginv64, csc_val, need_pinv);
         break;

@@ -51,6 +51,9 @@ typedef enum gpt_status {
 #define GPT_EXIT_PCG_MAXITER 2u  /* at least one PCG solve hit its iteration limit */
 #define GPT_EXIT_NONFINITE 4u    /* NaN/Inf in a merit or a PCG reduction */
 #define GPT_EXIT_ITER_LIMIT 8u   /* SQP_MAX_ITER iterations done (toplevel.cuh:254) */
+#define GPT_EXIT_FACTOR 16u      /* (Q + rho I) or (R + rho I) was not positive definite (a non-positive or vanishing
+                                    pivot in the Schur complement's inverses, e.g. rho = 0 with a rank-deficient
+                                    cost block); the instance stops and the call returns GPT_ERR_FACTOR */
 
 /* Problem description; the reference's compile-time macros become fields.
  * Replaces settings.cuh and the -D flags of perform_experiment.sh:42-58. */
@@ -154,6 +157,33 @@ gpt_status gpt_sqp_solve(gpt_handle *h, uint32_t knot_points, const float *d_eeP
 gpt_status gpt_sqp_solve_batched(gpt_handle *h, uint32_t batch, const uint32_t *h_knot_points,
                                  const float *d_eePos_traj, float *d_lambda, float *d_xu, float *h_rho,
                                  float rho_reset, gpt_sqp_stats *h_stats, gpt_stream_t stream);
+
+/* Scalars of one SQP iteration of one instance, recorded by gpt_sqp_solve_batched_trace */
+typedef struct gpt_iterate_record {
+    float rho;          /* rho of this iteration's Schur complement ((Q + rho I), (R + rho I)) */
+    float rho_next;     /* rho after the schedule of toplevel.cuh:396-412 (the next iteration's) */
+    float merit_prev;   /* merit of the iterate: the line search must go below it (toplevel.cuh:384-392) */
+    float merits[8];    /* line-search merits of xu + alpha_p dz, alpha_p = -2^-p (toplevel.cuh:357-374) */
+    float alpha;        /* accepted step; 0 when the line search failed (xu unchanged) */
+    uint32_t active;    /* 1 when the instance ran this iteration; the other fields are then defined */
+    uint32_t pcg_iters; /* PCG iterations of this iteration's linear solve */
+} gpt_iterate_record;
+
+/* gpt_sqp_solve_batched with every SQP iterate recorded (no reference counterpart: the reference
+ * returns only per-iteration PCG counts, toplevel.cuh:502).  Same kernels and results; the loop is
+ * driven from the host (one synchronisation per iteration).  For the first trace_iters iterations
+ * it writes, per iteration i (T = total knots of the batch, batch layout of gpt_sqp_solve_batched):
+ *   d_trace_xu     [trace_iters][21 T]     xu at the start of iteration i
+ *   d_trace_lambda [trace_iters][14 T]     the FP64 multipliers of iteration i's linear solve (dz's input)
+ *   d_trace_dz     [trace_iters][21 T]     the step dz of iteration i
+ *   d_trace_rec    [trace_iters][batch]    the iteration's scalars
+ * Any of the four may be NULL.  Vectors of an instance with rec.active == 0 in iteration i are not
+ * written. */
+gpt_status gpt_sqp_solve_batched_trace(gpt_handle *h, uint32_t batch, const uint32_t *h_knot_points,
+                                       const float *d_eePos_traj, float *d_lambda, float *d_xu, float *h_rho,
+                                       float rho_reset, gpt_sqp_stats *h_stats, uint32_t trace_iters,
+                                       float *d_trace_xu, double *d_trace_lambda, float *d_trace_dz,
+                                       gpt_iterate_record *d_trace_rec, gpt_stream_t stream);
 
 /* Autotuner (no reference counterpart): times two SQP iterations of this batch
  * (on copies of d_xu, d_lambda; the inputs are not modified) for each candidate
@@ -356,7 +386,9 @@ gpt_status gpt_ls_compute_merit(gpt_handle *h, uint32_t knot_points, const float
  * GPU that loads it until the process exits; knot_points above
  * GPT_NOALLOC_MAX_KNOTS returns GPT_ERR_BAD_ARG.  The first call on each device
  * looks up the array's device address (cudaGetSymbolAddress) with that device
- * current; make that first call before any stream capture.  All calls share
+ * current; make that first call before any stream capture.  That address is
+ * cached for the life of the process: after cudaDeviceReset on a device, this
+ * entry point must not be called on that device again.  All calls share
  * the array: calls whose kernels overlap on the GPU (other streams, other host
  * threads) race.  pc->max_knot_points and max_batch are not used. */
 #define GPT_NOALLOC_MAX_KNOTS 512

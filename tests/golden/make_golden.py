@@ -1,7 +1,8 @@
 """Regenerates the golden fixtures in this folder from the reference's own test data.
 
-Run from the repository root in a container that has the reference mounted:
-    python tests/golden/make_golden.py /root/reference
+Run from the repository root in a container that has the reference tree, given as the argument or
+in the environment variable GPT_REFERENCE_DIR:
+    GPT_REFERENCE_DIR=<reference tree> python tests/golden/make_golden.py
 
 It reads the reference's known-answer files (testfiles/0_0_eepos.traj, the
 forward kinematics of every row of testfiles/0_0_traj.csv written by
@@ -32,4 +33,7 @@ def main(ref_root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("GPT_REFERENCE_DIR")
+    if not root or not os.path.isdir(root):
+        sys.exit("make_golden.py: give the reference tree as the argument or in GPT_REFERENCE_DIR")
+    main(root)

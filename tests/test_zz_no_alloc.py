@@ -30,13 +30,15 @@ def case(N, p, seed):
 
 
 def test_noalloc_merit_matches_handle_entry_point(gpt, golden, problem_mod):
-    """Two calls in a row (N = 64 spec problem, then N = 32 reference problem, so the
-    second call leaves the first call's tail of the shared scratch untouched): each
-    call's 8 merits equal the handle-based entry point's within the line-search merit
-    tolerance of the parity tests (relative 5e-5 + 1e-5)."""
+    """Calls in a row (N = 64 spec problem, then N = 32 reference problem, so the second
+    call leaves the first call's tail of the shared scratch untouched, then the largest
+    accepted size, GPT_NOALLOC_MAX_KNOTS = 512, which fills the whole array): each call's
+    8 merits equal the handle-based entry point's within the line-search merit tolerance
+    of the parity tests (relative 5e-5 + 1e-5)."""
     L = gpt.lib()
     cases = [(64, SPEC_CFG, problem_mod.make_problem(64, 3, dt=0.01), 11),
-             (32, REF_CFG, ref_problem(golden, 32), 12)]
+             (32, REF_CFG, ref_problem(golden, 32), 12),
+             (gpt.NOALLOC_MAX_KNOTS, SPEC_CFG, problem_mod.make_problem(gpt.NOALLOC_MAX_KNOTS, 4, dt=0.01), 13)]
     for N, cfg, p, seed in cases:
         xs, xu, goal, dz = case(N, p, seed)
         pc = gpt.default_problem_config(**cfg)
