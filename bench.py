@@ -246,6 +246,41 @@ def run_reference(args, rank, world):
 
 
 # --------------------------------------------------------------------------- plain sweep
+def sweep_diffs(gpt, sv, N, p, x0, g0, l0, iters):
+    """Per-iterate linear-solve differences of one traced solve: at every SQP iterate the KKT blocks
+    the CUDA kernel formed are solved (a) in FP64 on the host (fp64check: Schur complement, block
+    Cholesky, dz) and (b) by the reference's qdldl path -- the CPU baseline's linear solve: FP32 Schur
+    complement in CSC form, FP32 LDL^T, FP32 dz (qdldl_helper.cuh:62-180, restated in oracle/); the
+    max over iterates of max |err| / max |FP64| for the B200 solve and for the qdldl path."""
+    import numpy as np
+    import torch
+    F = importlib.import_module("gpu-pcg-tracking_b200.fp64check")
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle_py as O
+    _, st, tr = sv.sqp_solve_batched_trace([N], g0, l0.clone(), x0.clone(), [1e-3], iters)
+    rec = gpt.trace_record_fields(tr["rec"])
+    out = {"gpu_vs_fp64": {"lambda": 0.0, "dz": 0.0}, "qdldl_vs_fp64": {"lambda": 0.0, "dz": 0.0},
+           "gpu_vs_qdldl": {"lambda": 0.0, "dz": 0.0}}
+    xs = torch.as_tensor(p["xu"][:14], device="cuda")
+    n_it = min(iters, int(st[0]["sqp_iters"]))
+    for i in range(n_it):
+        Gd, Cd, gd, cd = (torch.zeros(m, device="cuda") for m in (245 * N - 49, 294 * (N - 1), 21 * N - 7, 14 * N))
+        sv.form_kkt(N, tr["xu"][i, :21 * N - 7].contiguous(), g0, xs, Gd, Cd, gd, cd)
+        G, Cm, g, c = (t.cpu().numpy() for t in (Gd, Cd, gd, cd))
+        rho = float(rec["rho"][i, 0])
+        l64, d64 = F.solve_step(N, rho, G, Cm, g, c)
+        S32, _, gam32, Gi32 = O.form_schur(N, rho, G, Cm, g, c, "f32")
+        lq = O.ldl_solve(N, S32, gam32, "f32")
+        dq = O.compute_dz(N, Gi32, Cm, g, lq, "f32")
+        lg, dg = tr["lam"][i, :14 * N].cpu().numpy(), tr["dz"][i, :21 * N - 7].cpu().numpy()
+        for key, (la, da, lb, db) in {"gpu_vs_fp64": (lg, dg, l64, d64), "qdldl_vs_fp64": (lq, dq, l64, d64),
+                                      "gpu_vs_qdldl": (lg, dg, lq, dq)}.items():
+            out[key]["lambda"] = max(out[key]["lambda"], F.rel_err(la, lb))
+            out[key]["dz"] = max(out[key]["dz"], F.rel_err(da, db))
+    out["iterates"] = n_it
+    return out
+
+
 def run_sweep_plain(args, rank, local_rank):
     """The plain method as the drop-in (gpt_sqp_solve, one instance) over N in {64, 128, 256, 512}
     and PCG exit tolerance in {1e-4, 1e-5, 1e-6}: solves/s (graph path, mean of 3 solves after one
@@ -289,7 +324,8 @@ def run_sweep_plain(args, rank, local_rank):
             rows.append({"N": N, "tol": tol, "pcg_cluster_size": cs, "solves_per_s": 1000.0 / statistics.mean(ms),
                          "ms_per_solve": statistics.mean(ms), "linsys_us": us,
                          "pcg_iters_per_linsys": statistics.mean(its),
-                         "pcg_gbs": PCG_BYTES_PER_KNOT * N / (us * 1e-6) / 1e9 if us > 0 else None})
+                         "pcg_gbs": PCG_BYTES_PER_KNOT * N / (us * 1e-6) / 1e9 if us > 0 else None,
+                         "per_iterate_diffs": sweep_diffs(gpt, sv, N, p, x0, g0, l0, args.sqp_max_iter)})
         sv.close()
     print(json.dumps({"metric": "plain sqpSolve sweep", "unit": "solves/s", "dtype": "f32", "data": "synthetic",
                       "config": {"workload": f"gpt_sqp_solve, one instance, dt 0.01 semi-implicit Euler, QD 0.01, "

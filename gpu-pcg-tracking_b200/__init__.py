@@ -27,6 +27,7 @@ EXIT_RHO_MAX, EXIT_PCG_MAXITER, EXIT_NONFINITE, EXIT_ITER_LIMIT, EXIT_FACTOR = 1
 
 STATE_SIZE, CONTROL_SIZE = 14, 7
 PCG_WARP_PAIR = 32  # GPT_PCG_WARP_PAIR: pcg_cluster_size of the one-CTA-per-instance warp-pair PCG
+PCG_WARP_QUAD = 64  # GPT_PCG_WARP_QUAD: pcg_cluster_size of the one-CTA-per-instance partitioned PCG (4 warps)
 
 # The C-ABI entry points include/gpt.h declares (checked by the CPU tests).
 EXPORTED = [

@@ -269,10 +269,12 @@ gpt_status gpt_set_solver_config(gpt_handle *h, const gpt_solver_config *sc)
     if (!h || !sc) return set_err(GPT_ERR_BAD_ARG, "null argument");
     if (sc->sqp_max_iter == 0 || sc->sqp_max_iter > 4096) return set_err(GPT_ERR_BAD_ARG, "sqp_max_iter out of range");
     if (!(sc->rho_factor > 1.0f) || !(sc->rho_min > 0.0f)) return set_err(GPT_ERR_BAD_ARG, "rho schedule out of range");
-    if (sc->pcg_cluster_size == GPT_PCG_WARP_PAIR) {
-        if (sc->pcg_precond != 1) return set_err(GPT_ERR_BAD_ARG, "pcg_cluster_size GPT_PCG_WARP_PAIR needs pcg_precond 1");
+    if (sc->pcg_cluster_size == GPT_PCG_WARP_PAIR || sc->pcg_cluster_size == GPT_PCG_WARP_QUAD) {
+        if (sc->pcg_precond != 1)
+            return set_err(GPT_ERR_BAD_ARG, "pcg_cluster_size GPT_PCG_WARP_PAIR / GPT_PCG_WARP_QUAD needs pcg_precond 1");
     } else if (sc->pcg_cluster_size & (sc->pcg_cluster_size - 1) || sc->pcg_cluster_size > 16) {
-        return set_err(GPT_ERR_BAD_ARG, "pcg_cluster_size must be 0, 1, 2, 4, 8, 16 or GPT_PCG_WARP_PAIR");
+        return set_err(GPT_ERR_BAD_ARG,
+                       "pcg_cluster_size must be 0, 1, 2, 4, 8, 16, GPT_PCG_WARP_PAIR or GPT_PCG_WARP_QUAD");
     }
     if (sc->pcg_precond > 1) return set_err(GPT_ERR_BAD_ARG, "pcg_precond must be 0 or 1");
     if (sc->schur_fp64 > 1) return set_err(GPT_ERR_BAD_ARG, "schur_fp64 must be 0 or 1");
@@ -343,7 +345,7 @@ gpt_status gpt_create(const gpt_problem_config *pc, const gpt_solver_config *sc,
     ALLOC(d_active, 1);
     ALLOC(lam64, NS * T);
     ALLOC(Ginv64, G_STRIDE * T);
-    ALLOC(crw, SS * T);
+    ALLOC(crw, 2 * SS * T);
     ALLOC(adj_h, NX * T);
     ALLOC(adj_zero, NS * T);
     ALLOC(adj_gamma, NS * T);
@@ -516,12 +518,12 @@ gpt_status gpt_pcg(gpt_handle *h, uint32_t N, const float *d_S, const float *d_P
     if (!check_n(h, N) || exit_mode > 1) return set_err(GPT_ERR_BAD_ARG, "knot_points/exit_mode out of range");
     if (((uintptr_t)d_S & 15u) != 0) return set_err(GPT_ERR_BAD_ARG, "d_S must be 16-byte aligned");
     cudaStream_t s = (cudaStream_t)stream;
-    if (h->sc.pcg_cluster_size == GPT_PCG_WARP_PAIR) {
-        // the warp-pair kernel reads packed FP64 rows: the caller's S and gamma, converted exactly
+    if (h->sc.pcg_cluster_size == GPT_PCG_WARP_PAIR || h->sc.pcg_cluster_size == GPT_PCG_WARP_QUAD) {
+        // the one-CTA kernels read packed FP64 rows: the caller's S and gamma, converted exactly
         GPT_CUDA(launch_pack_rows64((int)N, d_S, d_gamma, h->S64, h->gamma64, h->num_sms, s));
         GPT_CUDA(launch_pcg(single_view(N), (int)N, (int)N, 2, 1, reinterpret_cast<const float *>(h->S64), d_Pinv,
                             d_gamma, h->gamma64, d_lambda, d_lambda64, h->crw, (int)max_iter, tol, (int)exit_mode,
-                            h->pcg_out, nullptr, 0, PCG_WARP_PAIR, h->num_sms, s));
+                            h->pcg_out, nullptr, 0, (int)h->sc.pcg_cluster_size, h->num_sms, s));
     } else {
         GPT_CUDA(launch_pcg(single_view(N), (int)N, (int)N, 0, (int)h->sc.pcg_precond, d_S, d_Pinv, d_gamma, nullptr,
                             d_lambda, d_lambda64, h->crw, (int)max_iter, tol, (int)exit_mode, h->pcg_out, nullptr, 0,
@@ -1039,7 +1041,10 @@ gpt_status gpt_autotune(gpt_handle *h, uint32_t B, const uint32_t *h_N, const fl
     std::vector<uint32_t> cand;
     for (int cs = cs0; cs <= 16 && cs <= 4 * cs0 && cs <= minN; cs *= 2) cand.push_back((uint32_t)cs);
     if (cand.empty()) cand.push_back((uint32_t)cs0);
-    if (h->sc.pcg_precond == 1) cand.push_back(GPT_PCG_WARP_PAIR);  // one 128-thread CTA per instance
+    if (h->sc.pcg_precond == 1) {  // one 128-thread CTA per instance: two or four factoring warps
+        cand.push_back(GPT_PCG_WARP_PAIR);
+        cand.push_back(GPT_PCG_WARP_QUAD);
+    }
     const gpt_solver_config saved = h->sc;
     const int saved_profile = h->profile;
     h->profile = 0;

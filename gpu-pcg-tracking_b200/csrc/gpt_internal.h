@@ -11,6 +11,7 @@ namespace gpt {
 constexpr int MAX_PCG_KNOTS = 512;  // horizon limit of the library (16-CTA cluster x 32 knots)
 constexpr int PCG_KPC_MAX = 128;    // knots per CTA held in shared memory by the PCG
 constexpr int PCG_WARP_PAIR = 32;   // pcg_cluster_size value selecting pcg_pair_kernel (one 128-thread CTA per instance)
+constexpr int PCG_WARP_QUAD = 64;   // pcg_cluster_size value selecting pcg_quad_kernel (four warps factor four parts)
 
 // SQP control constants (settings.cuh:31-50 and the -D flags of perform_experiment.sh:42-58)
 struct SolverParams {
@@ -41,8 +42,9 @@ size_t pcg_cluster_smem_bytes(int kpc);
 int pcg_pick_cluster(int maxN, int B, int num_sms, int requested);
 // fmt 0: S and Pinv in the reference 3-block layout; fmt 1: packed rows (PK floats per knot) in S
 // precond 0: block-Jacobi with the given Pinv; 1: exact block-tridiagonal LDL^T of each CTA's chunk
-// cr_ws: FP64 workspace of 196 doubles per knot of the batch (the cyclic-reduction
-// couplings of precond 1; unused by precond 0)
+// cr_ws: FP64 workspace of 2 x 196 doubles per knot of the batch (the cyclic-reduction couplings of
+// precond 1, the warp-pair kernel's factors and vectors, the partitioned kernel's factors, vectors and
+// coupling blocks; unused by precond 0)
 // fmt 0: reference 3-block rows (S, Pinv floats); 1: packed FP32 rows (PK); 2: packed FP64 rows (PK64,
 // S points at doubles) with FP64 gamma64 -- chain preconditioner only.  cluster_size PCG_WARP_PAIR runs
 // pcg_pair_kernel (precond 1, fmt 1 or 2; cr_ws holds its factors and FP64 vectors)

@@ -1634,6 +1634,660 @@ __global__ void __launch_bounds__(PAIR_THREADS, 4)
     }
 }
 
+// ---------------------------------------------------------------------------
+// Partitioned PCG: one 128-thread CTA per instance whose four warps factor four parts of the
+// horizon (pcg_cluster_size PCG_WARP_QUAD).
+//
+// The exact preconditioner of pcg_pair_kernel (S^{-1} up to rounding), with the factorisation
+// split four ways so that each warp walks about a quarter of the horizon instead of half of it,
+// and every warp of the CTA (hence every SM sub-partition) factors.  With M = -S (SPD), A_k = M_kk,
+// E_k = M_{k,k-1} = -L_k, the horizon is cut by P - 1 separator knots s_1 < ... < s_{P-1}
+// (P = 4 from n = 7 on) into P parts.  Part 0 is factored top-down toward s_1 and part P-1
+// bottom-up toward s_{P-1} (the two ends of the twisted factorisation); a middle part a .. b
+// between s_p and s_{p+1} top-down, which couples its two separators: with F_k = M_{k, s_p}
+// (F_a = E_a = -L_a) it carries
+//   F_{k+1} = L_{k+1} D_k^{-1} F_k   and accumulates   Acc = sum_k F_k^T D_k^{-1} F_k,
+// and ends with E^ = L_{s_{p+1}} D_b^{-1} F_b = M_{s_{p+1}, s_p} after its elimination.  The
+// separators' reduced system (block tridiagonal, P - 1 blocks) has the diagonal blocks
+//   A_{s_j} - (update of the part on its left) - (Acc of the middle part on its right, or the
+//   update of the last part)
+// and is factored by one warp after the parts.  The solve runs the same order: each part forward
+// (t_k = D_k^{-1} y_k, pushing L_{k+1} t_k to the next knot and, in a middle part, -F_k^T t_k to
+// its left separator), the reduced system forward and back, each part backward
+// (x_k = t_k + D_k^{-1} (L_{k+1}^T x_{k+1} - F_k x_{s_p})).  This is the block LDL^T of M with the
+// parts' knots ordered before the separators, so the preconditioner stays exact (z = S^{-1} r =
+// -x) and the CG of pcg_pair_kernel stops after one iteration.  Edge parts have two block products
+// per step, middle parts five, so edge parts are made 1.3 times as long.
+//
+// Storage: per knot 2 x 196 doubles of the FP64 workspace: the pair kernel's slots (packed inverse
+// factor, lambda, r, p, S p) and the middle parts' F_k (full); the solve's t_k overwrites y_k in
+// the shared vector and x_k overwrites t_k.  Shared memory: the vector (14 n), per warp the
+// factorisation scratch of the pair kernel, per middle part F, D^{-1} F and Acc, the separators'
+// right-hand-side contributions.
+constexpr int QUAD_THREADS = 128;
+constexpr int QUAD_NWARP = 4;
+constexpr int QW_STRIDE = 2 * SS;  // workspace doubles per knot
+constexpr int QW_SPIKE = SS;       // F_k (full 14 x 14) at this offset of a middle part's knot
+constexpr int QSP = 3 * SS;        // per middle part: F, X = D^{-1} F, Acc
+
+struct QuadLayout {
+    int P;
+    int a[QUAD_NWARP], b[QUAD_NWARP];  // part p: knots a[p] .. b[p] (b[p] < a[p]: empty)
+    int s[QUAD_NWARP - 1];             // separator knots
+};
+__host__ __device__ inline QuadLayout quad_layout(int n)
+{
+    QuadLayout L;
+    int P = QUAD_NWARP;
+    if (n < 2 * P) {
+        P = (n + 1) / 2;
+        P = P < 1 ? 1 : (P > QUAD_NWARP ? QUAD_NWARP : P);
+    }
+    L.P = P;
+    const int nint = n - (P - 1);
+    int len[QUAD_NWARP] = {0, 0, 0, 0};
+    if (P == 1) {
+        len[0] = n;
+    } else if (P == 2) {
+        len[0] = nint / 2;
+        len[1] = nint - len[0];
+    } else {
+        const int y = (10 * nint) / (26 + 10 * (P - 2));  // edge parts weighted 1.3
+        const int rest = nint - (P - 2) * y;
+        len[0] = rest / 2;
+        for (int p = 1; p < P - 1; ++p) len[p] = y;
+        len[P - 1] = rest - len[0];
+    }
+    int pos = 0;
+    for (int p = 0; p < QUAD_NWARP; ++p) {
+        L.a[p] = pos;
+        L.b[p] = pos + (p < P ? len[p] : 0) - 1;
+        pos += p < P ? len[p] : 0;
+        if (p < QUAD_NWARP - 1) {
+            L.s[p] = pos;
+            if (p < P - 1) ++pos;
+        }
+    }
+    return L;
+}
+
+__host__ __device__ constexpr int quad_smem_doubles(int n)
+{
+    return NS * n + QUAD_NWARP * PAIR_FWARP + (QUAD_NWARP - 2) * QSP + (QUAD_NWARP - 1) * 2 * NS +
+           2 * QUAD_NWARP * 3 + QUAD_NWARP + 2;
+}
+size_t pcg_quad_smem_bytes(int n) { return sizeof(double) * (size_t)quad_smem_doubles(n); }
+
+// C (<-|+=) op(A) op(B) for 14 x 14 blocks (column-major, shared memory), FP64 tensor cores; one warp.
+// C must not alias A or B.
+template <bool TA, bool TB, bool ACC>
+__device__ __forceinline__ void blk_mm(const double *A, const double *B, double *C, int lane)
+{
+    const int g = lane >> 2, t = lane & 3;
+    double c[2][2][2];
+#pragma unroll
+    for (int I = 0; I < 2; ++I)
+#pragma unroll
+        for (int J = 0; J < 2; ++J)
+#pragma unroll
+            for (int e = 0; e < 2; ++e) {
+                const int i = 8 * I + g, j = 8 * J + 2 * t + e;
+                c[I][J][e] = (ACC && i < NS && j < NS) ? C[i + NS * j] : 0.0;
+            }
+    warp_dmma<2, 2, 4>([&](int i, int k) { return (i < NS && k < NS) ? (TA ? A[k + NS * i] : A[i + NS * k]) : 0.0; },
+                       [&](int k, int j) { return (k < NS && j < NS) ? (TB ? B[j + NS * k] : B[k + NS * j]) : 0.0; },
+                       c, lane);
+    __syncwarp();
+    warp_dmma_store(c, [&](int i, int j, double v) { if (i < NS && j < NS) C[i + NS * j] = v; }, lane);
+    __syncwarp();
+}
+
+template <int FMT>
+__global__ void __launch_bounds__(QUAD_THREADS, 4)
+    pcg_quad_kernel(BatchView bv, const void *__restrict__ Sv, const float *__restrict__ gamma,
+                    const double *__restrict__ gamma64, float *__restrict__ lambda, double *__restrict__ lambda64,
+                    double *__restrict__ ws, int max_iter, float tol, int exit_mode, uint32_t *__restrict__ out_iters,
+                    uint32_t *__restrict__ pcg_log, int log_stride)
+{
+    static_assert(FMT == 1 || FMT == 2, "packed rows only");
+    using ST = typename std::conditional<FMT == 2, double, float>::type;
+    const ST *S = reinterpret_cast<const ST *>(Sv);
+    const size_t ks = FMT == 2 ? PK64 : PK;
+    const int b = bv.b0 + (int)blockIdx.x;
+    if (b >= bv.b0 + bv.B || !bv.active(b)) return;
+    const int n = bv.N(b), nv = NS * n;
+    const QuadLayout lay = quad_layout(n);
+    const int P = lay.P;
+    const size_t kg0 = (size_t)bv.off(b);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+
+    extern __shared__ double quad_dyn_smem[];
+    double *xv = quad_dyn_smem;                       // 14 n: y, then t (forward), then x (backward)
+    double *fwall = xv + nv;                          // per warp: inverse factor (full), coupling, A_k, product
+    double *spall = fwall + QUAD_NWARP * PAIR_FWARP;  // middle parts 1, 2: F, X = D^{-1} F, Acc
+    double *sacc = spall + (QUAD_NWARP - 2) * QSP;    // per separator: right-hand-side pushes from left, right
+    double *red = sacc + (QUAD_NWARP - 1) * 2 * NS;   // 2 sets x 4 warps x 3
+    double *ginit = red + 2 * QUAD_NWARP * 3;         // gamma . gamma per warp
+
+    const ST *Sb = S + kg0 * ks;
+    double *wsb = ws + kg0 * QW_STRIDE;
+    auto wsv = [&](int slot, int e) -> double & { return wsb[(size_t)(e / NS) * QW_STRIDE + slot + e % NS]; };
+    const float *gb = (FMT == 2) ? nullptr : gamma + NS * kg0;
+    const double *gb64 = (FMT == 2) ? gamma64 + NS * kg0 : nullptr;
+    auto gam = [&](int e) -> double { return (FMT == 2) ? gb64[e] : (double)gb[e]; };
+    float *lb = lambda + NS * kg0;
+
+    // (S v)_e with FP64 accumulation (the order of pcg_pair_kernel)
+    auto srow = [&](int e, const double *v) -> double {
+        const int k = e / NS, r = e - NS * k;
+        const ST *row = Sb + (size_t)k * ks;
+        double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+        ST fd[NS];
+#pragma unroll
+        for (int cc = 0; cc < NS; ++cc) fd[cc] = __ldg(row + PK_DIAG + tri_lo(r, cc));
+        if (k > 0) {
+            ST fl[NS];
+#pragma unroll
+            for (int cc = 0; cc < NS; ++cc) fl[cc] = __ldg(row + r + NS * cc);
+#pragma unroll
+            for (int cc = 0; cc < NS; ++cc) a0 = fma((double)fl[cc], v[NS * (k - 1) + cc], a0);
+        }
+#pragma unroll
+        for (int cc = 0; cc < NS; ++cc) a1 = fma((double)fd[cc], v[NS * k + cc], a1);
+        if (k < n - 1) {
+            ST fr[NS];
+#pragma unroll
+            for (int cc = 0; cc < NS; ++cc) fr[cc] = __ldg(row + ks + cc + NS * r);
+#pragma unroll
+            for (int cc = 0; cc < NS; ++cc) a2 = fma((double)fr[cc], v[NS * (k + 1) + cc], a2);
+        }
+        return (a0 + a1) + a2;
+    };
+
+    const int c = lane >> 1, hh = lane & 1;
+    const bool cval = c < NS;
+    const int cq = cval ? c : NS - 1;
+    auto keep_inv = [&](double *F, const double (&a)[7], int k) {
+        __syncwarp();
+        if (cval) {
+#pragma unroll
+            for (int q = 0; q < 7; ++q) {
+                const int i = 7 * hh + q;
+                if (F) F[i + NS * c] = a[q];
+                if (i >= c) wsb[(size_t)k * QW_STRIDE + PW_INV + ((i * (i + 1)) >> 1) + c] = a[q];
+            }
+        }
+        __syncwarp();
+    };
+
+    // ---- initial residual r = gamma - S lambda (all threads)
+    for (int e = tid; e < nv; e += QUAD_THREADS) xv[e] = (double)lb[e];
+    __syncthreads();
+    {
+        double g2 = 0.0;
+        for (int e = tid; e < nv; e += QUAD_THREADS) {
+            const double gv = gam(e);
+            wsv(PW_RES, e) = gv - srow(e, xv);
+            wsv(PW_LAM, e) = xv[e];
+            g2 += gv * gv;
+        }
+        g2 = warp_sum(g2);
+        if (lane == 0) ginit[warp] = g2;
+    }
+
+    // ---- factorisation of the parts: warp w walks part w (top-down, or bottom-up for the last part)
+    if (warp < P) {
+        const int w = warp;
+        const bool top = (w < P - 1) || (P == 1);
+        const bool spk = top && w > 0;                 // middle part: carries F toward separator s_{w-1}
+        const bool has_sep = top ? (w < P - 1) : true;  // a separator after the walk
+        const int pa = lay.a[w], pb = lay.b[w];
+        const int len = pb >= pa ? pb - pa + 1 : 0;
+        double *fw = fwall + w * PAIR_FWARP;
+        double *Fi = fw + PF_INV, *Lw = fw + PF_L, *Ap = fw + PF_A, *Wb = fw + PF_W;
+        double *Fsp = spk ? spall + (w - 1) * QSP : nullptr;
+        double *Xb = spk ? Fsp + SS : nullptr, *Acc = spk ? Fsp + 2 * SS : nullptr;
+        const int k0 = top ? pa : pb, dir = top ? 1 : -1, lofs = top ? 0 : 1;
+        double pd[4] = {0.0, 0.0, 0.0, 0.0}, pl[7] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+        if (len > 0) warp_fetch<ST, 4>(Sb + (size_t)k0 * ks + PK_DIAG, 105, lane, pd);
+        if (spk) {
+            // F_a = E_a = -L_a (row a's left block couples a to s_{w-1}); for an empty part a is s_w and
+            // -L_{s_w} is the separators' own coupling
+            double fl[7];
+            warp_fetch<ST, 7>(Sb + (size_t)pa * ks, SS, lane, fl);
+#pragma unroll
+            for (int i = 0; i < 7; ++i) {
+                const int e = lane + 32 * i;
+                if (e < SS) {
+                    Fsp[e] = -fl[i];
+                    Acc[e] = 0.0;
+                }
+            }
+        }
+        if (len == 0) {
+            for (int e = lane; e < SS; e += 32) Wb[e] = 0.0;  // no update of the separator
+        } else if (len > 1 || has_sep) {
+            warp_fetch<ST, 7>(Sb + (size_t)(k0 + dir + lofs) * ks, SS, lane, pl);
+        }
+        __syncwarp();
+        for (int st = 0; st < len || (st == len && has_sep && len > 0); ++st) {
+            const bool sep_step = st == len;
+            const int k = k0 + dir * st;
+            if (!sep_step) {
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    const int e = lane + 32 * i;
+                    if (e < 105) Ap[e] = -pd[i];
+                }
+            }
+            if (st > 0) {
+#pragma unroll
+                for (int i = 0; i < 7; ++i) {
+                    const int e = lane + 32 * i;
+                    if (e < SS) Lw[top ? e : (e / NS) + NS * (e % NS)] = pl[i];
+                }
+            }
+            __syncwarp();
+            if (!sep_step) {
+                if (st + 1 < len) {
+                    warp_fetch<ST, 4>(Sb + (size_t)(k + dir) * ks + PK_DIAG, 105, lane, pd);
+                    warp_fetch<ST, 7>(Sb + (size_t)(k + dir + lofs) * ks, SS, lane, pl);
+                } else if (has_sep) {
+                    warp_fetch<ST, 7>(Sb + (size_t)(k + dir + lofs) * ks, SS, lane, pl);
+                }
+            }
+            if (spk && st > 0) blk_mm<false, false, false>(Lw, Xb, Fsp, lane);  // F_k = L_k D_{k-1}^{-1} F_{k-1}
+            if (st > 0) {
+                // Wb <- L D_prev^{-1} L^T = L (D_prev^{-1} L^T): W = D^{-1} L^T, then L W
+                blk_mm<false, true, false>(Fi, Lw, Wb, lane);
+                double cd[2][2][2] = {};
+                warp_dmma<2, 2, 4>([&](int i, int kk) { return (i < NS && kk < NS) ? Lw[i + NS * kk] : 0.0; },
+                                   [&](int kk, int j) { return (kk < NS && j < NS) ? Wb[kk + NS * j] : 0.0; }, cd,
+                                   lane);
+                __syncwarp();
+                warp_dmma_store(cd, [&](int i, int j, double v) { if (i < NS && j < NS) Wb[i + NS * j] = v; }, lane);
+                __syncwarp();
+            }
+            if (sep_step) break;  // Wb: the separator's update; Fsp (middle part): E^ = M_{s_w, s_{w-1}}
+            double a[7];
+#pragma unroll
+            for (int q = 0; q < 7; ++q)
+                a[q] = Ap[tri_lo(7 * hh + q, cq)] - (st > 0 ? Wb[7 * hh + q + NS * cq] : 0.0);
+            pair_gj_inverse(a, c, hh);
+            keep_inv(Fi, a, k);
+            if (spk) {
+                double *fg = wsb + (size_t)k * QW_STRIDE + QW_SPIKE;
+                for (int e = lane; e < SS; e += 32) fg[e] = Fsp[e];
+                blk_mm<false, false, false>(Fi, Fsp, Xb, lane);  // X_k = D_k^{-1} F_k
+                blk_mm<true, false, true>(Fsp, Xb, Acc, lane);   // Acc += F_k^T X_k
+            }
+        }
+    }
+    __syncthreads();
+    const double gg = ((ginit[0] + ginit[1]) + ginit[2]) + ginit[3];
+
+    // ---- the separators' reduced system, factored top-down by warp 0:
+    //   D^_j = A_{s_j} - (left part's update) - (right part's Acc or update) - E^_j D^_{j-1}^{-1} E^_j^T
+    if (warp == 0 && P >= 2) {
+        double *Fi0 = fwall + PF_INV, *T0 = fwall + PF_L, *Ap0 = fwall + PF_A, *W0 = fwall + PF_W;
+        for (int j = 0; j < P - 1; ++j) {
+            const int s = lay.s[j];
+            double pd[4];
+            warp_fetch<ST, 4>(Sb + (size_t)s * ks + PK_DIAG, 105, lane, pd);
+            const double *cl = fwall + j * PAIR_FWARP + PF_W;  // j = 0: W0, read before W0 is reused
+            const double *cr = (j + 1 == P - 1) ? fwall + (P - 1) * PAIR_FWARP + PF_W : spall + j * QSP + 2 * SS;
+            double a[7];
+            if (j > 0) {
+                const double *Eh = spall + (j - 1) * QSP;  // E^_j: the middle part between s_{j-1} and s_j
+                blk_mm<false, false, false>(Eh, Fi0, T0, lane);  // E^_j D^_{j-1}^{-1}
+                blk_mm<false, true, false>(T0, Eh, W0, lane);    // ... E^_j^T
+            }
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                const int e = lane + 32 * i;
+                if (e < 105) Ap0[e] = -pd[i];
+            }
+            __syncwarp();
+#pragma unroll
+            for (int q = 0; q < 7; ++q) {
+                const int i = 7 * hh + q;
+                a[q] = ((Ap0[tri_lo(i, cq)] - cl[i + NS * cq]) - cr[i + NS * cq]) - (j > 0 ? W0[i + NS * cq] : 0.0);
+            }
+            pair_gj_inverse(a, c, hh);
+            keep_inv(Fi0, a, s);
+        }
+    }
+    __syncthreads();
+
+    // ---- M x = y in place on xv (every thread takes the barriers)
+    const int r = c;
+    const bool rv = cval;
+    auto ld_inv = [&](int k, double (&v)[7]) {
+#pragma unroll
+        for (int q = 0; q < 7; ++q) v[q] = rv ? wsb[(size_t)k * QW_STRIDE + PW_INV + tri_lo(r, 7 * hh + q)] : 0.0;
+    };
+    // row r of L_k (TR: of L_k^T), columns 7 hh .. 7 hh + 6
+    auto ld_left = [&](int k, bool tr, double (&v)[7]) {
+        const ST *p = Sb + (size_t)k * ks;
+#pragma unroll
+        for (int q = 0; q < 7; ++q)
+            v[q] = rv ? (double)__ldg(p + (tr ? 7 * hh + q + NS * r : r + NS * (7 * hh + q))) : 0.0;
+    };
+    // row r of F_k (TR: of F_k^T)
+    auto ld_spike = [&](int k, bool tr, double (&v)[7]) {
+        const double *p = wsb + (size_t)k * QW_STRIDE + QW_SPIKE;
+#pragma unroll
+        for (int q = 0; q < 7; ++q) v[q] = rv ? p[tr ? 7 * hh + q + NS * r : r + NS * (7 * hh + q)] : 0.0;
+    };
+    auto solve = [&]() {
+        // forward through every part: t_k = D_k^{-1} y_k overwrites y_k
+        if (warp < P) {
+            const int w = warp;
+            const bool top = (w < P - 1) || (P == 1);
+            const bool spk = top && w > 0;
+            const bool has_sep = top ? (w < P - 1) : true;
+            const int pa = lay.a[w], pb = lay.b[w];
+            if (top) {
+                double accv = 0.0;
+                for (int k = pa; k <= pb; ++k) {
+                    double di[7], li[7], fi[7];
+                    ld_inv(k, di);
+                    const int kn = k < pb ? k + 1 : (has_sep ? lay.s[w] : -1);  // the knot y_k pushes to
+                    if (kn >= 0) ld_left(kn, false, li);
+                    if (spk) ld_spike(k, true, fi);
+                    const double t = pair_dot7(di, xv + NS * k, hh);
+                    __syncwarp();
+                    if (hh == 0 && rv) xv[NS * k + r] = t;
+                    __syncwarp();
+                    if (spk) {
+                        double p = 0.0;
+#pragma unroll
+                        for (int q = 0; q < 7; ++q) p = fma(fi[q], xv[NS * k + 7 * hh + q], p);
+                        accv -= p;  // -F_k^T t_k, this lane's half
+                    }
+                    if (kn >= 0) {
+                        const double u = pair_dot7(li, xv + NS * k, hh);
+                        if (hh == 0 && rv) {
+                            if (k < pb) xv[NS * kn + r] += u;
+                            else sacc[(2 * w) * NS + r] = u;
+                        }
+                    }
+                    __syncwarp();
+                }
+                if (pb < pa && has_sep && lane < NS) sacc[(2 * w) * NS + lane] = 0.0;
+                if (spk) {
+                    accv += __shfl_xor_sync(0xffffffffu, accv, 1);
+                    if (hh == 0 && rv) sacc[(2 * (w - 1) + 1) * NS + r] = accv;
+                }
+            } else {
+                for (int k = pb; k >= pa; --k) {
+                    double di[7], li[7];
+                    ld_inv(k, di);
+                    ld_left(k, true, li);  // L_k^T: pushes to k - 1 (the separator s_{P-1} at k = a)
+                    const double t = pair_dot7(di, xv + NS * k, hh);
+                    __syncwarp();
+                    if (hh == 0 && rv) xv[NS * k + r] = t;
+                    __syncwarp();
+                    const double u = pair_dot7(li, xv + NS * k, hh);
+                    if (hh == 0 && rv) {
+                        if (k > pa) xv[NS * (k - 1) + r] += u;
+                        else sacc[(2 * (P - 2) + 1) * NS + r] = u;
+                    }
+                    __syncwarp();
+                }
+                if (pb < pa && lane < NS) sacc[(2 * (P - 2) + 1) * NS + lane] = 0.0;
+            }
+        }
+        __syncthreads();
+        // the reduced system (warp 0): forward t^_j, then x_{s_j} = t^_j - D^_j^{-1} E^_{j+1}^T x_{s_{j+1}}
+        if (warp == 0 && P >= 2) {
+            double *sc = fwall + PF_L;
+            for (int j = 0; j < P - 1; ++j) {
+                const int s = lay.s[j];
+                double di[7];
+                ld_inv(s, di);
+                if (lane < NS) {
+                    double z = (xv[NS * s + lane] + sacc[(2 * j) * NS + lane]) + sacc[(2 * j + 1) * NS + lane];
+                    if (j > 0) {
+                        const double *Eh = spall + (j - 1) * QSP;
+                        const int sp = lay.s[j - 1];
+#pragma unroll
+                        for (int t = 0; t < NS; ++t) z = fma(-Eh[lane + NS * t], xv[NS * sp + t], z);
+                    }
+                    sc[lane] = z;
+                }
+                __syncwarp();
+                const double t = pair_dot7(di, sc, hh);
+                __syncwarp();
+                if (hh == 0 && rv) xv[NS * s + r] = t;
+                __syncwarp();
+            }
+            for (int j = P - 3; j >= 0; --j) {
+                const int s = lay.s[j], sn = lay.s[j + 1];
+                const double *Eh = spall + j * QSP;  // E^_{j+1}
+                double di[7];
+                ld_inv(s, di);
+                if (lane < NS) {
+                    double z = 0.0;
+#pragma unroll
+                    for (int t = 0; t < NS; ++t) z = fma(Eh[t + NS * lane], xv[NS * sn + t], z);
+                    sc[lane] = z;
+                }
+                __syncwarp();
+                const double u = pair_dot7(di, sc, hh);
+                __syncwarp();
+                if (hh == 0 && rv) xv[NS * s + r] -= u;
+                __syncwarp();
+            }
+        }
+        __syncthreads();
+        // backward through every part: x_k = t_k + D_k^{-1} (coupling to the knots after it)
+        if (warp < P) {
+            const int w = warp;
+            const bool top = (w < P - 1) || (P == 1);
+            const bool spk = top && w > 0;
+            const bool has_sep = top ? (w < P - 1) : true;
+            const int pa = lay.a[w], pb = lay.b[w];
+            double *sc = fwall + w * PAIR_FWARP + PF_L;
+            if (top) {
+                for (int k = pb; k >= pa; --k) {
+                    double di[7], li[7], fi[7];
+                    ld_inv(k, di);
+                    const int kn = k < pb ? k + 1 : (has_sep ? lay.s[w] : -1);
+                    if (kn >= 0) ld_left(kn, true, li);
+                    if (spk) ld_spike(k, false, fi);
+                    double v = kn >= 0 ? pair_dot7(li, xv + NS * kn, hh) : 0.0;  // L_{k+1}^T x_{k+1}
+                    if (spk) {
+                        double p = 0.0;
+#pragma unroll
+                        for (int q = 0; q < 7; ++q) p = fma(fi[q], xv[NS * (pa - 1) + 7 * hh + q], p);
+                        v -= p + __shfl_xor_sync(0xffffffffu, p, 1);  // - F_k x_{s_{w-1}}
+                    }
+                    if (hh == 0 && rv) sc[r] = v;
+                    __syncwarp();
+                    const double a = pair_dot7(di, sc, hh);
+                    if (hh == 0 && rv) xv[NS * k + r] += a;
+                    __syncwarp();
+                }
+            } else {
+                for (int k = pa; k <= pb; ++k) {
+                    double di[7], li[7];
+                    ld_inv(k, di);
+                    ld_left(k, false, li);  // L_k x_{k-1}
+                    const double v = pair_dot7(li, xv + NS * (k - 1), hh);
+                    if (hh == 0 && rv) sc[r] = v;
+                    __syncwarp();
+                    const double a = pair_dot7(di, sc, hh);
+                    if (hh == 0 && rv) xv[NS * k + r] += a;
+                    __syncwarp();
+                }
+            }
+        }
+        __syncthreads();
+    };
+
+    // ---- CG on the instance (the iteration of pcg_pair_kernel)
+    int set = 0;
+    auto block_sum = [&](double *v, int cnt) {
+        for (int q = 0; q < cnt; ++q) {
+            const double s = warp_sum(v[q]);
+            if (lane == 0) red[set * QUAD_NWARP * 3 + warp * 3 + q] = s;
+        }
+        __syncthreads();
+        for (int q = 0; q < cnt; ++q) {
+            const double *rs = red + set * QUAD_NWARP * 3 + q;
+            v[q] = ((rs[0] + rs[3]) + rs[6]) + rs[9];
+        }
+        set ^= 1;
+    };
+    auto true_residual = [&]() {
+        __syncthreads();
+        for (int e = tid; e < nv; e += QUAD_THREADS) xv[e] = wsv(PW_LAM, e);
+        __syncthreads();
+        for (int e = tid; e < nv; e += QUAD_THREADS) wsv(PW_RES, e) = gam(e) - srow(e, xv);
+    };
+    // z = S^{-1} r = -x of M x = r (left in xv); d[1] += r.z, d[2] += r.r
+    auto precond = [&](double *d) {
+        __syncthreads();
+        for (int e = tid; e < nv; e += QUAD_THREADS) xv[e] = wsv(PW_RES, e);
+        __syncthreads();
+        solve();
+        for (int e = tid; e < nv; e += QUAD_THREADS) {
+            const double rr = wsv(PW_RES, e), z = -xv[e];
+            d[1] += rr * z;
+            d[2] += rr * rr;
+        }
+    };
+    auto sum_res2 = [&]() {
+        double d0[1] = {0.0};
+        for (int e = tid; e < nv; e += QUAD_THREADS) {
+            const double rr = wsv(PW_RES, e);
+            d0[0] += rr * rr;
+        }
+        block_sum(d0, 1);
+        return d0[0];
+    };
+    auto converged = [&](double e, double r2) {
+        return exit_mode == 0 ? (r2 <= (double)tol * (double)tol * gg) : (fabs(e) < (double)tol);
+    };
+
+    double eta;
+    bool conv, bad = false;
+    {
+        double acc3[3] = {0.0, 0.0, 0.0};
+        precond(acc3);
+        block_sum(acc3, 3);
+        eta = acc3[1];
+        for (int e = tid; e < nv; e += QUAD_THREADS) wsv(PW_P, e) = -xv[e];  // p = z
+        conv = converged(eta, acc3[2]);
+    }
+    int it = 0;
+    while (!conv && it < max_iter) {
+        __syncthreads();
+        for (int e = tid; e < nv; e += QUAD_THREADS) xv[e] = wsv(PW_P, e);
+        __syncthreads();
+        double d1[1] = {0.0};
+        for (int e = tid; e < nv; e += QUAD_THREADS) {
+            const double v = srow(e, xv);
+            wsv(PW_V, e) = v;
+            d1[0] += xv[e] * v;
+        }
+        block_sum(d1, 1);
+        const double alpha = eta / d1[0];
+        if (!isfinite(alpha)) {
+            bad = true;
+            break;
+        }
+        double r2acc = 0.0;
+        for (int e = tid; e < nv; e += QUAD_THREADS) {
+            wsv(PW_LAM, e) = fma(alpha, xv[e], wsv(PW_LAM, e));
+            const double rn = fma(-alpha, wsv(PW_V, e), wsv(PW_RES, e));
+            wsv(PW_RES, e) = rn;
+            r2acc += rn * rn;
+        }
+        ++it;
+        bool replaced = false;
+        if (it % RR_PERIOD == 0) {
+            true_residual();
+            replaced = true;
+        }
+        if (exit_mode == 0) {
+            double r2;
+            if (replaced) {
+                r2 = sum_res2();
+            } else {
+                double t1[1] = {r2acc};
+                block_sum(t1, 1);
+                r2 = t1[0];
+            }
+            if (!isfinite(r2)) {
+                bad = true;
+                break;
+            }
+            if (converged(0.0, r2) && !replaced && it > 1) {
+                true_residual();
+                r2 = sum_res2();
+            }
+            if (converged(0.0, r2)) {
+                conv = true;
+                break;
+            }
+        }
+        double d2[3] = {0.0, 0.0, 0.0};
+        precond(d2);
+        block_sum(d2, 3);
+        if (exit_mode != 0) conv = converged(d2[1], d2[2]);
+        if (!isfinite(d2[1])) {
+            bad = true;
+            conv = false;
+            break;
+        }
+        if (conv) break;
+        const double beta = d2[1] / eta;
+        eta = d2[1];
+        for (int e = tid; e < nv; e += QUAD_THREADS) wsv(PW_P, e) = fma(beta, wsv(PW_P, e), -xv[e]);
+    }
+    for (int e = tid; e < nv; e += QUAD_THREADS) {
+        const double lam = wsv(PW_LAM, e);
+        lb[e] = (float)lam;
+        if (lambda64) lambda64[NS * kg0 + e] = lam;
+    }
+    if (tid == 0) {
+        const uint32_t maxit = conv ? 0u : 1u;
+        if (out_iters) {
+            out_iters[2 * b] = (uint32_t)it;
+            out_iters[2 * b + 1] = maxit | (bad ? 2u : 0u);
+        }
+        if (bv.st) {
+            InstState &s = bv.st[b];
+            s.last_pcg_iters = it;
+            s.last_pcg_exit = maxit;
+            s.pcg_iters_total += it;
+            s.pcg_maxiter_count += maxit;
+            if (bad) s.exit_flags |= 4u;
+            if (pcg_log && s.sqp_iters < (uint32_t)log_stride)
+                pcg_log[(size_t)b * log_stride + s.sqp_iters] = (uint32_t)it | (maxit << 31);
+        }
+    }
+}
+
+template <int FMT>
+static cudaError_t launch_pcg_quad_t(const BatchView &bv, int max_n, const void *S, const float *gamma,
+                                     const double *gamma64, float *lambda, double *lambda64, double *ws, int max_iter,
+                                     float tol, int exit_mode, uint32_t *out_iters, uint32_t *pcg_log, int log_stride,
+                                     cudaStream_t s)
+{
+    auto kern = pcg_quad_kernel<FMT>;
+    const size_t smem = pcg_quad_smem_bytes(max_n);
+    {
+        const cudaError_t e = ensure_func_attrs((const void *)kern, smem);
+        if (e != cudaSuccess) return e;
+    }
+    kern<<<bv.B, QUAD_THREADS, smem, s>>>(bv, S, gamma, gamma64, lambda, lambda64, ws, max_iter, tol, exit_mode,
+                                          out_iters, pcg_log, log_stride);
+    return cudaGetLastError();
+}
+
 // FP64 packed rows (PK64: left block, diagonal lower triangle, pad) and FP64 gamma from the
 // reference's FP32 3-block rows, for pcg_pair_kernel on a caller's S (gpt_pcg)
 __global__ void pack_rows64_kernel(int N, const float *__restrict__ S, const float *__restrict__ gamma,
@@ -1761,6 +2415,13 @@ cudaError_t launch_pcg(const BatchView &bv, int max_n_knots, int min_n_knots, in
     if (precond == 1 && !cr_ws) return cudaErrorInvalidValue;
     if (fmt == 2 && (precond != 1 || !gamma64)) return cudaErrorInvalidValue;  // FP64 rows: chain preconditioner only
     if (max_n_knots > MAX_PCG_KNOTS) return cudaErrorInvalidValue;
+    if (cluster_size == PCG_WARP_QUAD) {
+        if (precond != 1 || fmt == 0) return cudaErrorInvalidValue;  // packed rows, exact preconditioner
+        return fmt == 2 ? launch_pcg_quad_t<2>(bv, max_n_knots, S, gamma, gamma64, lambda, lambda64, cr_ws, max_iter,
+                                               tol, exit_mode, out_iters, pcg_log, log_stride, s)
+                        : launch_pcg_quad_t<1>(bv, max_n_knots, S, gamma, gamma64, lambda, lambda64, cr_ws, max_iter,
+                                               tol, exit_mode, out_iters, pcg_log, log_stride, s);
+    }
     if (cluster_size == PCG_WARP_PAIR) {
         if (precond != 1 || fmt == 0) return cudaErrorInvalidValue;  // packed rows, exact preconditioner
         return fmt == 2 ? launch_pcg_pair_t<2>(bv, max_n_knots, S, gamma, gamma64, lambda, lambda64, cr_ws, max_iter,

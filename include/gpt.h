@@ -83,9 +83,10 @@ typedef struct gpt_solver_config {
     float rho_factor;          /* RHO_FACTOR */
     float rho_max;             /* RHO_MAX */
     float rho_min;             /* RHO_MIN */
-    uint32_t pcg_cluster_size; /* CTAs per instance in the PCG (1,2,4,8,16); GPT_PCG_WARP_PAIR: one 128-thread
-                                  CTA per instance, factorisation by two warps (pcg_precond 1 only); 0 = chosen
-                                  by the library (gpt_autotune's choice for the batch shape, else 1 ... 16) */
+    uint32_t pcg_cluster_size; /* CTAs per instance in the PCG (1,2,4,8,16); GPT_PCG_WARP_PAIR / GPT_PCG_WARP_QUAD:
+                                  one 128-thread CTA per instance, factorisation by two / four warps (pcg_precond 1
+                                  only); 0 = chosen by the library (gpt_autotune's choice for the batch shape, else
+                                  1 ... 16) */
     uint32_t pcg_precond;      /* 0: block-Jacobi Pinv (the reference's, oldschur.cuh:926-933);
                                   1 (default): exact block-tridiagonal LDL^T of each CTA's chunk of knots */
     uint32_t schur_fp64;       /* SQP loop and adjoint with pcg_precond 1: 1 (default) forms and stores the
@@ -116,6 +117,12 @@ typedef struct gpt_sqp_stats {
  * from both ends of the horizon at once (twisted block LDL^T), so that all instances of a large batch run
  * concurrently; same iteration and preconditioner (exact inverse of S) as pcg_cluster_size 1. */
 #define GPT_PCG_WARP_PAIR 32u
+
+/* pcg_cluster_size value: the PCG of one instance in one 128-thread CTA whose four warps each factor about a
+ * quarter of the horizon (partitioned block LDL^T: three separator knots, a 3-block reduced system), so every
+ * SM sub-partition factors and each warp's chain is half the warp-pair kernel's; same iteration and
+ * preconditioner (exact inverse of S) as pcg_cluster_size 1. */
+#define GPT_PCG_WARP_QUAD 64u
 
 /* Default configs: the reference's logged experiment settings (dt 1/64, Euler,
  * QD = R = 1e-4, RHO_FACTOR 1.2, RHO_MAX 10, RHO_MIN 1e-3, SQP_MAX_ITER 40). */

@@ -137,17 +137,18 @@ def schur_residual(S, lam, gam, N):
 
 
 @pytest.mark.parametrize("precond", [0, 1])
-@pytest.mark.parametrize("cluster", [0, 1, 2, 4, 8, 16, 32])
+@pytest.mark.parametrize("cluster", [0, 1, 2, 4, 8, 16, 32, 64])
 def test_pcg_reaches_tolerance(gpt, oracle, golden, problem_mod, solvers, cluster, precond):
     """Exit mode 0 stops on the TRUE relative residual (FP64-evaluated); the
     returned lambda satisfies ||gamma - S lambda|| <= tol ||gamma|| for every
     cluster size (CTAs per instance; 32 = the warp-pair kernel, one CTA per
-    instance with a twisted factorisation) and both preconditioners (0: the
+    instance with a twisted factorisation; 64 = the partitioned kernel, one CTA
+    per instance, four factoring warps) and both preconditioners (0: the
     reference's block-Jacobi, 1: exact block-tridiagonal LDL^T per chunk); a
     warm start at the solution needs at most a few iterations."""
-    pair = cluster == gpt.PCG_WARP_PAIR
+    pair = cluster in (gpt.PCG_WARP_PAIR, gpt.PCG_WARP_QUAD)
     if pair and precond == 0:
-        pytest.skip("the warp-pair kernel has the exact preconditioner only")
+        pytest.skip("the one-CTA kernels have the exact preconditioner only")
     for kind, N, cfg, p in problems(golden, problem_mod):
         if cluster > N and not pair:
             continue
@@ -199,7 +200,7 @@ def test_pcg_cluster_sizes_agree(gpt, oracle, problem_mod, solvers):
     S, Pv, gam = (x.astype(np.float32) for x in (S, Pv, gam))
     lam_star = oracle.banded_cholesky(N, S, gam)
     sols = {}
-    for cs in (1, 2, 4, 8, 16, gpt.PCG_WARP_PAIR):
+    for cs in (1, 2, 4, 8, 16, gpt.PCG_WARP_PAIR, gpt.PCG_WARP_QUAD):
         sv.set_solver(pcg_cluster_size=cs)
         lam = torch.zeros(14 * N, device="cuda")
         lam64 = torch.zeros(14 * N, device="cuda", dtype=torch.float64)
@@ -211,6 +212,7 @@ def test_pcg_cluster_sizes_agree(gpt, oracle, problem_mod, solvers):
     # one CTA per instance (cyclic reduction) and the warp pair (twisted factorisation) both apply
     # the exact inverse: their solutions differ by rounding only
     assert np.linalg.norm(sols[1] - sols[gpt.PCG_WARP_PAIR]) <= 1e-7 * ref
+    assert np.linalg.norm(sols[1] - sols[gpt.PCG_WARP_QUAD]) <= 1e-7 * ref
     errs = {cs: np.linalg.norm(v - lam_star) / ref for cs, v in sols.items()}
     # every split lands within the accuracy the 1e-5 residual allows of the FP64 Cholesky
     # solution (one CTA per instance solves exactly; the chunked splits stop at the tolerance)
@@ -469,7 +471,7 @@ def test_sqp_warp_pair_pcg_matches_chain(gpt, problem_mod, schur_fp64, exit_mode
     x0 = host(xu0)
     for iters, tol in ((1, 1e-6), (4, 1e-3)):
         out = {}
-        for cs in (1, gpt.PCG_WARP_PAIR):
+        for cs in (1, gpt.PCG_WARP_PAIR, gpt.PCG_WARP_QUAD):
             sv = gpt.Solver(max_knot_points=128, max_batch=len(Ns), **SPEC_CFG)
             sv.set_solver(sqp_max_iter=iters, pcg_max_iter=1000, pcg_exit_tol=1e-9 if exit_mode == 0 else 1e-14,
                           pcg_exit_mode=exit_mode, pcg_cluster_size=cs, schur_fp64=schur_fp64)
@@ -477,21 +479,23 @@ def test_sqp_warp_pair_pcg_matches_chain(gpt, problem_mod, schur_fp64, exit_mode
             rho, stats = sv.sqp_solve_batched(Ns, goal, lam, xu, [1e-3] * len(Ns))
             out[cs] = (host(xu), rho, stats)
             sv.close()
-        (x1, r1, s1), (x2, r2, s2) = out[1], out[gpt.PCG_WARP_PAIR]
-        assert [s["sqp_iters"] for s in s1] == [s["sqp_iters"] for s in s2]
-        assert r1 == r2
-        off = 0
-        for b, n in enumerate(Ns):
-            sl = slice(21 * off, 21 * off + 21 * n - 7)
-            step = np.linalg.norm(x1[sl] - x0[sl])
-            diff = np.linalg.norm(x2[sl] - x1[sl])
-            assert diff <= tol * step + 1e-6, (iters, n, diff, step)
-            assert s2[b]["pcg_maxiter_count"] == 0
-            assert s2[b]["pcg_iters_total"] <= 2 * s2[b]["sqp_iters"], (n, s2[b])
-            off += n
+        x1, r1, s1 = out[1]
+        for other in (gpt.PCG_WARP_PAIR, gpt.PCG_WARP_QUAD):
+            x2, r2, s2 = out[other]
+            assert [s["sqp_iters"] for s in s1] == [s["sqp_iters"] for s in s2]
+            assert r1 == r2
+            off = 0
+            for b, n in enumerate(Ns):
+                sl = slice(21 * off, 21 * off + 21 * n - 7)
+                step = np.linalg.norm(x1[sl] - x0[sl])
+                diff = np.linalg.norm(x2[sl] - x1[sl])
+                assert diff <= tol * step + 1e-6, (other, iters, n, diff, step)
+                assert s2[b]["pcg_maxiter_count"] == 0
+                assert s2[b]["pcg_iters_total"] <= 2 * s2[b]["sqp_iters"], (other, n, s2[b])
+                off += n
 
 
-@pytest.mark.parametrize("cluster", [1, 32])
+@pytest.mark.parametrize("cluster", [1, 32, 64])
 def test_sqp_graph_equals_host_loop(gpt, problem_mod, cluster):
     """The solve as one CUDA graph (device-side while loop, the default), the graph with
     the batch split in parts on concurrent branches (sqp_graph 2: 2 + 3 instances of
@@ -535,7 +539,7 @@ def test_autotune_choice_is_used(gpt, problem_mod):
     x_in, l_in = xu0.clone(), lam0.clone()
     cs = sv.autotune([N], goal, l_in, x_in, [1e-3])
     assert torch.equal(x_in, xu0) and torch.equal(l_in, lam0)
-    assert cs in (1, 2, 4, gpt.PCG_WARP_PAIR)
+    assert cs in (1, 2, 4, gpt.PCG_WARP_PAIR, gpt.PCG_WARP_QUAD)
     out = []
     for given in (0, cs):
         sv.set_solver(pcg_cluster_size=given)
@@ -589,7 +593,7 @@ def test_plain_sweep_linear_solve_accuracy(gpt, oracle, problem_mod, solvers, N)
     ref = oracle.banded_cholesky(N, S.astype(np.float64), gam.astype(np.float64))
     ldl = oracle.ldl_solve(N, S.astype(np.float64), gam.astype(np.float64)).astype(np.float64)
     err_ldl = np.abs(ldl - ref).max() / np.abs(ref).max()
-    for cluster in (0, gpt.PCG_WARP_PAIR):
+    for cluster in (0, gpt.PCG_WARP_PAIR, gpt.PCG_WARP_QUAD):
         sv.set_solver(pcg_cluster_size=cluster, pcg_precond=1)
         for tol in (1e-4, 1e-5, 1e-6):
             lam = torch.zeros(14 * N, device="cuda")
@@ -601,4 +605,30 @@ def test_plain_sweep_linear_solve_accuracy(gpt, oracle, problem_mod, solvers, N)
             assert not maxed and relres <= 1.02 * tol, (N, cluster, tol, it, relres)
             err = np.abs(l64 - ref).max() / np.abs(ref).max()
             assert err <= max(err_ldl, 1e-6), (N, cluster, tol, err, err_ldl)
+    sv.set_solver(pcg_cluster_size=0, pcg_precond=0)
+
+
+def test_partitioned_pcg_every_part_layout(gpt, oracle, problem_mod, solvers):
+    """The partitioned kernel (GPT_PCG_WARP_QUAD) over horizons whose part layouts differ: one part
+    (N = 2), two and three parts with empty parts (N = 3 .. 7), four parts with empty middle parts
+    (N = 7 .. 10) and the long horizons.  It applies the exact inverse of S: the true relative residual
+    meets a 1e-9 tolerance within two iterations and the solution is the FP64 Cholesky solution to
+    the rounding cond(S) allows."""
+    sv = solvers(SPEC_CFG)
+    sv.set_solver(pcg_cluster_size=gpt.PCG_WARP_QUAD, pcg_precond=1)
+    for N in list(range(2, 21)) + [31, 33, 64, 100, 128, 129, 255, 256, 511, 512]:
+        p = problem_mod.make_problem(N, 70 + N, dt=0.01)
+        oG, oC, og, oc = oracle.form_kkt(oracle_params(oracle, SPEC_CFG), N, p["xu"], p["goal"], p["xs"])
+        S, Pv, gam, _ = oracle.form_schur(N, 1e-2, *(x.astype(np.float32) for x in (oG, oC, og, oc)))
+        S, Pv, gam = (x.astype(np.float32) for x in (S, Pv, gam))
+        ref = oracle.banded_cholesky(N, S.astype(np.float64), gam.astype(np.float64))
+        lam = torch.zeros(14 * N, device="cuda")
+        lam64 = torch.zeros(14 * N, device="cuda", dtype=torch.float64)
+        it, maxed = sv.pcg(N, dev(S), dev(Pv), dev(gam), lam, 50, 1e-9, 0, lam64=lam64)
+        torch.cuda.synchronize()
+        l64 = lam64.cpu().numpy()
+        relres = schur_residual(S, l64, gam.astype(np.float64), N)
+        assert not maxed and it <= 2 and relres <= 1.02e-9, (N, it, relres)
+        err = np.abs(l64 - ref).max() / np.abs(ref).max()
+        assert err <= 1e-6, (N, err)
     sv.set_solver(pcg_cluster_size=0, pcg_precond=0)

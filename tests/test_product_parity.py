@@ -8,9 +8,9 @@ instances and every iteration the oracle is fed the GPU's own KKT blocks at the 
 complement, banded Cholesky, dz: the reference's sqpSolve linear algebra, toplevel.cuh:254-335 with
 the qdldl solve of qdldl_helper.cuh:62-180 replaced by its exact FP64 counterpart).  Bars:
   * lambda and dz within 1e-4 relative (max |err| / max |oracle|) of the FP64 solution;
-  * the line-search merits within 5e-5 relative of the oracle's FP64 merits of the same candidates
-    (the merit is FP32 arithmetic, as the reference's: its defect terms x_{k+1} - f(x_k, u_k) cancel,
-    ~1e-6 per component over 14 N components with weight mu = 10 on merits of ~1e3);
+  * the line-search merits within 5e-5 relative plus the FP32 rounding of their defect sums of the
+    oracle's FP64 merits of the same candidates (the merit is FP32 arithmetic, as the reference's: each
+    defect component x_{k+1} - f(x_k, u_k) cancels, leaving ~eps32 |x| per component, weighted by mu);
   * the accept decision the argmin of the GPU's own merits exactly, and the oracle's argmin up to a
     tie within the merits' FP32 error; rho after the schedule identical bit for bit
     (toplevel.cuh:384-412, float arithmetic); the next iterate equal to fl32(xu + alpha dz) bit for bit.
@@ -87,9 +87,13 @@ def check_trace(gpt, oracle, sv, par, Ns, batch, sample, iters):
             # line-search merits of the GPU's candidates xu + alpha_p dz, in FP64 by the oracle
             mo = np.array([oracle.merit(par, N, xu_b[i], dz_b[i], -2.0 ** -a, gb, xs, 1)[0] for a in range(8)])
             mg = rec["merits"][i, b].astype(np.float64)
-            em = np.abs(mg - mo).max() / np.abs(mo).max()
-            assert em <= MERIT_RTOL, f"instance {b} iteration {i}: merit rel err {em:.3e}"
-            worst["merit"] = max(worst["merit"], em)
+            # FP32 rounding of the defect sums: mu x 4 eps32 per unit of |x| at the candidates
+            xs_abs = np.array([np.abs(xu_b[i].astype(np.float64) - 2.0 ** -a * dz_b[i]).sum() for a in range(8)])
+            tolm = MERIT_RTOL * np.abs(mo) + par.mu * 4 * 2.0 ** -23 * xs_abs
+            em = (np.abs(mg - mo) / tolm).max()
+            assert em <= 1.0, f"instance {b} iteration {i}: merit error {em:.3f} x its bound"
+            worst_m = (np.abs(mg - mo) / np.abs(mo)).max()
+            worst["merit"] = max(worst["merit"], worst_m)
             # the accept decision: exactly the argmin of the GPU's merits against the iterate's merit
             # (strict <, first minimum, toplevel.cuh:384-392) ...
             m_prev = np.float32(rec["merit_prev"][i, b])
@@ -106,7 +110,7 @@ def check_trace(gpt, oracle, sv, par, Ns, batch, sample, iters):
             acc_o = mo[a_o] < m_prev
             if acc_g != acc_o or (acc_g and a_g != a_o):
                 alt = mo[a_g] if acc_g else float(m_prev)
-                assert abs(alt - mo[a_o]) <= 2 * MERIT_RTOL * abs(mo[a_o]), (b, i, alpha, mo, m_prev)
+                assert abs(alt - mo[a_o]) <= 2 * tolm.max(), (b, i, alpha, mo, m_prev)
             rho_n, drho = rho_law(rho, drho, acc_g)
             assert np.float32(rec["rho_next"][i, b]) == rho_n, (b, i, rec["rho_next"][i, b], rho_n)
             if i + 1 < min(iters, n_active):
@@ -129,7 +133,7 @@ def test_default_batched_path_matches_oracle_per_iterate(gpt, oracle, problem_mo
         sv.set_solver(sqp_max_iter=40, pcg_max_iter=10000, pcg_exit_tol=1e-5, pcg_exit_mode=0)
         assert sv.solver.schur_fp64 == 1 and sv.solver.pcg_precond == 1
         cs = sv.autotune(Ns, *(torch.as_tensor(batch[k], device="cuda") for k in ("goal", "lam", "xu")), [1e-3] * B)
-        assert cs == gpt.PCG_WARP_PAIR, f"the autotuner chose {cs} for the bench shape"
+        assert cs in (gpt.PCG_WARP_PAIR, gpt.PCG_WARP_QUAD), f"the autotuner chose {cs} for the bench shape"
         sample = [0] + sorted(np.random.default_rng(11).choice(np.arange(1, B), 8, replace=False).tolist())
         par = oracle.make_params(dt=0.01, integrator=1, qd_cost=1e-2, r_cost=1e-4)
         worst, n = check_trace(gpt, oracle, sv, par, Ns, batch, sample, 40)
@@ -138,8 +142,9 @@ def test_default_batched_path_matches_oracle_per_iterate(gpt, oracle, problem_mo
         sv.close()
 
 
+@pytest.mark.parametrize("cluster", [32, 64])
 @pytest.mark.parametrize("N", [32, 128])
-def test_reference_trajectory_batch_matches_oracle_per_iterate(gpt, oracle, golden, N):
+def test_reference_trajectory_batch_matches_oracle_per_iterate(gpt, oracle, golden, N, cluster):
     """The reference's own trajectory testfiles/0_0_traj.csv (dt 1/64, explicit Euler, QD = R = 1e-4,
     the settings of its logged runs): 16 windows of N rows as a batch, every iterate of 4 of them."""
     B = 16
@@ -153,7 +158,7 @@ def test_reference_trajectory_batch_matches_oracle_per_iterate(gpt, oracle, gold
     sv = gpt.Solver(max_knot_points=N, max_batch=B, **REF_CFG)
     try:
         sv.set_solver(sqp_max_iter=40, pcg_max_iter=10000, pcg_exit_tol=1e-5, pcg_exit_mode=0,
-                      pcg_cluster_size=gpt.PCG_WARP_PAIR)
+                      pcg_cluster_size=cluster)
         par = oracle.make_params()
         worst, n = check_trace(gpt, oracle, sv, par, Ns, batch, [0, 5, 10, 15], 40)
         print(f"reference trajectory N={N}:", n, "iterates checked, worst", worst)
