@@ -33,6 +33,7 @@
 
 #include "gpt_common.cuh"
 #include "gpt_internal.h"
+#include "gpt_layout.h"
 
 namespace cg = cooperative_groups;
 
@@ -1656,8 +1657,10 @@ __global__ void __launch_bounds__(PAIR_THREADS, 4)
 // its left separator), the reduced system forward and back, each part backward
 // (x_k = t_k + D_k^{-1} (L_{k+1}^T x_{k+1} - F_k x_{s_p})).  This is the block LDL^T of M with the
 // parts' knots ordered before the separators, so the preconditioner stays exact (z = S^{-1} r =
-// -x) and the CG of pcg_pair_kernel stops after one iteration.  Edge parts have two block products
-// per step, middle parts five, so edge parts are made 1.3 times as long.
+// -x) and the CG of pcg_pair_kernel stops after one iteration.  For that reason the iteration starts
+// from lambda = 0 (r_0 = gamma, no product with S before the factorisation; the caller's warm start
+// cannot save the one iteration), unlike pcg_pair_kernel.  Edge parts have two block products per
+// step, middle parts five, so edge parts are made 1.3 times as long.
 //
 // Storage: per knot 2 x 196 doubles of the FP64 workspace: the pair kernel's slots (packed inverse
 // factor, lambda, r, p, S p) and the middle parts' F_k (full); the solve's t_k overwrites y_k in
@@ -1665,51 +1668,9 @@ __global__ void __launch_bounds__(PAIR_THREADS, 4)
 // factorisation scratch of the pair kernel, per middle part F, D^{-1} F and Acc, the separators'
 // right-hand-side contributions.
 constexpr int QUAD_THREADS = 128;
-constexpr int QUAD_NWARP = 4;
 constexpr int QW_STRIDE = 2 * SS;  // workspace doubles per knot
 constexpr int QW_SPIKE = SS;       // F_k (full 14 x 14) at this offset of a middle part's knot
 constexpr int QSP = 3 * SS;        // per middle part: F, X = D^{-1} F, Acc
-
-struct QuadLayout {
-    int P;
-    int a[QUAD_NWARP], b[QUAD_NWARP];  // part p: knots a[p] .. b[p] (b[p] < a[p]: empty)
-    int s[QUAD_NWARP - 1];             // separator knots
-};
-__host__ __device__ inline QuadLayout quad_layout(int n)
-{
-    QuadLayout L;
-    int P = QUAD_NWARP;
-    if (n < 2 * P) {
-        P = (n + 1) / 2;
-        P = P < 1 ? 1 : (P > QUAD_NWARP ? QUAD_NWARP : P);
-    }
-    L.P = P;
-    const int nint = n - (P - 1);
-    int len[QUAD_NWARP] = {0, 0, 0, 0};
-    if (P == 1) {
-        len[0] = n;
-    } else if (P == 2) {
-        len[0] = nint / 2;
-        len[1] = nint - len[0];
-    } else {
-        const int y = (10 * nint) / (26 + 10 * (P - 2));  // edge parts weighted 1.3
-        const int rest = nint - (P - 2) * y;
-        len[0] = rest / 2;
-        for (int p = 1; p < P - 1; ++p) len[p] = y;
-        len[P - 1] = rest - len[0];
-    }
-    int pos = 0;
-    for (int p = 0; p < QUAD_NWARP; ++p) {
-        L.a[p] = pos;
-        L.b[p] = pos + (p < P ? len[p] : 0) - 1;
-        pos += p < P ? len[p] : 0;
-        if (p < QUAD_NWARP - 1) {
-            L.s[p] = pos;
-            if (p < P - 1) ++pos;
-        }
-    }
-    return L;
-}
 
 __host__ __device__ constexpr int quad_smem_doubles(int n)
 {
@@ -1820,21 +1781,42 @@ __global__ void __launch_bounds__(QUAD_THREADS, 4)
         __syncwarp();
     };
 
-    // ---- initial residual r = gamma - S lambda (all threads)
-    for (int e = tid; e < nv; e += QUAD_THREADS) xv[e] = (double)lb[e];
-    __syncthreads();
-    {
-        double g2 = 0.0;
-        for (int e = tid; e < nv; e += QUAD_THREADS) {
-            const double gv = gam(e);
-            wsv(PW_RES, e) = gv - srow(e, xv);
-            wsv(PW_LAM, e) = xv[e];
-            g2 += gv * gv;
-        }
-        g2 = warp_sum(g2);
-        if (lane == 0) ginit[warp] = g2;
+    // ---- the iteration starts from lambda = 0: with the exact preconditioner one iteration reaches
+    // the solution from any start, and r_0 = gamma needs no product with S
+    double g2acc = 0.0;  // gamma . gamma, this thread's entries
+    for (int e = tid; e < nv; e += QUAD_THREADS) {
+        const double gv = gam(e);
+        wsv(PW_RES, e) = gv;
+        wsv(PW_LAM, e) = 0.0;
+        g2acc = fma(gv, gv, g2acc);
     }
-
+    const int r = c;
+    const bool rv = cval;
+    // (S v)_k row r on the lane pair (r, hh): left, diagonal and right blocks, columns 7 hh .. 7 hh + 6
+    // (FP64 accumulation; the pair's halves summed by a shuffle)
+    auto row_block = [&](int k, const double *v) -> double {
+        const ST *row = Sb + (size_t)k * ks;
+        const bool hl = k > 0, hr = k < n - 1;
+        double acc = 0.0;
+        if (rv) {
+            ST fl[7], fd[7], fr[7];
+#pragma unroll
+            for (int q = 0; q < 7; ++q) {
+                const int cc = 7 * hh + q;
+                fl[q] = hl ? __ldg(row + r + NS * cc) : (ST)0;
+                fd[q] = __ldg(row + PK_DIAG + tri_lo(r, cc));
+                fr[q] = hr ? __ldg(row + ks + cc + NS * r) : (ST)0;
+            }
+#pragma unroll
+            for (int q = 0; q < 7; ++q) {
+                const int cc = 7 * hh + q;
+                if (hl) acc = fma((double)fl[q], v[NS * (k - 1) + cc], acc);
+                acc = fma((double)fd[q], v[NS * k + cc], acc);
+                if (hr) acc = fma((double)fr[q], v[NS * (k + 1) + cc], acc);
+            }
+        }
+        return acc + __shfl_xor_sync(0xffffffffu, acc, 1);
+    };
     // ---- factorisation of the parts: warp w walks part w (top-down, or bottom-up for the last part)
     if (warp < P) {
         const int w = warp;
@@ -1923,6 +1905,10 @@ __global__ void __launch_bounds__(QUAD_THREADS, 4)
             }
         }
     }
+    {
+        const double g2 = warp_sum(g2acc);
+        if (lane == 0) ginit[warp] = g2;
+    }
     __syncthreads();
     const double gg = ((ginit[0] + ginit[1]) + ginit[2]) + ginit[3];
 
@@ -1960,8 +1946,6 @@ __global__ void __launch_bounds__(QUAD_THREADS, 4)
     __syncthreads();
 
     // ---- M x = y in place on xv (every thread takes the barriers)
-    const int r = c;
-    const bool rv = cval;
     auto ld_inv = [&](int k, double (&v)[7]) {
 #pragma unroll
         for (int q = 0; q < 7; ++q) v[q] = rv ? wsb[(size_t)k * QW_STRIDE + PW_INV + tri_lo(r, 7 * hh + q)] : 0.0;
@@ -1979,6 +1963,22 @@ __global__ void __launch_bounds__(QUAD_THREADS, 4)
 #pragma unroll
         for (int q = 0; q < 7; ++q) v[q] = rv ? p[tr ? 7 * hh + q + NS * r : r + NS * (7 * hh + q)] : 0.0;
     };
+    // L2 prefetch of the blocks a sweep step loads QPF steps later: the packed inverse factor (840 B), the
+    // coupling block of S and, for a middle part, F_k; every address lies inside its block
+    constexpr int QPF = 4;
+    constexpr int INV_LINES = (105 * 8 + 127) / 128, L_LINES = (SS * (int)sizeof(ST) + 127) / 128,
+                  F_LINES = (SS * 8 + 127) / 128;
+    auto l2_pf = [&](int ki, int kl, int kf) {
+        const char *pi = reinterpret_cast<const char *>(wsb + (size_t)ki * QW_STRIDE);
+        const char *pl = reinterpret_cast<const char *>(Sb + (size_t)kl * ks);
+        const char *pf = reinterpret_cast<const char *>(wsb + (size_t)kf * QW_STRIDE + QW_SPIKE);
+        if (lane < INV_LINES) {
+            if (ki >= 0 && ki < n) asm volatile("prefetch.global.L2 [%0];" ::"l"(pi + 128 * lane));
+        } else if (lane < INV_LINES + L_LINES) {
+            if (kl >= 0 && kl < n) asm volatile("prefetch.global.L2 [%0];" ::"l"(pl + 128 * (lane - INV_LINES)));
+        }
+        if (lane < F_LINES && kf >= 0 && kf < n) asm volatile("prefetch.global.L2 [%0];" ::"l"(pf + 128 * lane));
+    };
     auto solve = [&]() {
         // forward through every part: t_k = D_k^{-1} y_k overwrites y_k
         if (warp < P) {
@@ -1990,23 +1990,26 @@ __global__ void __launch_bounds__(QUAD_THREADS, 4)
             if (top) {
                 double accv = 0.0;
                 for (int k = pa; k <= pb; ++k) {
-                    double di[7], li[7], fi[7];
-                    ld_inv(k, di);
-                    const int kn = k < pb ? k + 1 : (has_sep ? lay.s[w] : -1);  // the knot y_k pushes to
-                    if (kn >= 0) ld_left(kn, false, li);
-                    if (spk) ld_spike(k, true, fi);
-                    const double t = pair_dot7(di, xv + NS * k, hh);
+                    double dc[7], lc[7], fc[7];
+                    const int kn0 = k < pb ? k + 1 : (has_sep ? lay.s[w] : -1);
+                    ld_inv(k, dc);
+                    if (kn0 >= 0) ld_left(kn0, false, lc);
+                    if (spk) ld_spike(k, true, fc);
+                    l2_pf(k + QPF <= pb ? k + QPF : -1, k + QPF + 1 <= pb ? k + QPF + 1 : -1,
+                          spk && k + QPF <= pb ? k + QPF : -1);
+                    const int kn = k < pb ? k + 1 : (has_sep ? lay.s[w] : -1);
+                    const double t = pair_dot7(dc, xv + NS * k, hh);
                     __syncwarp();
                     if (hh == 0 && rv) xv[NS * k + r] = t;
                     __syncwarp();
                     if (spk) {
                         double p = 0.0;
 #pragma unroll
-                        for (int q = 0; q < 7; ++q) p = fma(fi[q], xv[NS * k + 7 * hh + q], p);
+                        for (int q2 = 0; q2 < 7; ++q2) p = fma(fc[q2], xv[NS * k + 7 * hh + q2], p);
                         accv -= p;  // -F_k^T t_k, this lane's half
                     }
                     if (kn >= 0) {
-                        const double u = pair_dot7(li, xv + NS * k, hh);
+                        const double u = pair_dot7(lc, xv + NS * k, hh);
                         if (hh == 0 && rv) {
                             if (k < pb) xv[NS * kn + r] += u;
                             else sacc[(2 * w) * NS + r] = u;
@@ -2021,14 +2024,15 @@ __global__ void __launch_bounds__(QUAD_THREADS, 4)
                 }
             } else {
                 for (int k = pb; k >= pa; --k) {
-                    double di[7], li[7];
-                    ld_inv(k, di);
-                    ld_left(k, true, li);  // L_k^T: pushes to k - 1 (the separator s_{P-1} at k = a)
-                    const double t = pair_dot7(di, xv + NS * k, hh);
+                    double dc[7], lc[7];
+                    ld_inv(k, dc);
+                    ld_left(k, true, lc);
+                    l2_pf(k - QPF >= pa ? k - QPF : -1, k - QPF >= pa ? k - QPF : -1, -1);
+                    const double t = pair_dot7(dc, xv + NS * k, hh);
                     __syncwarp();
                     if (hh == 0 && rv) xv[NS * k + r] = t;
                     __syncwarp();
-                    const double u = pair_dot7(li, xv + NS * k, hh);
+                    const double u = pair_dot7(lc, xv + NS * k, hh);
                     if (hh == 0 && rv) {
                         if (k > pa) xv[NS * (k - 1) + r] += u;
                         else sacc[(2 * (P - 2) + 1) * NS + r] = u;
@@ -2091,33 +2095,37 @@ __global__ void __launch_bounds__(QUAD_THREADS, 4)
             double *sc = fwall + w * PAIR_FWARP + PF_L;
             if (top) {
                 for (int k = pb; k >= pa; --k) {
-                    double di[7], li[7], fi[7];
-                    ld_inv(k, di);
+                    double dc[7], lc[7], fc[7];
+                    const int kn0 = k < pb ? k + 1 : (has_sep ? lay.s[w] : -1);
+                    ld_inv(k, dc);
+                    if (kn0 >= 0) ld_left(kn0, true, lc);
+                    if (spk) ld_spike(k, false, fc);
+                    l2_pf(k - QPF >= pa ? k - QPF : -1, k - QPF + 1 >= pa ? k - QPF + 1 : -1,
+                          spk && k - QPF >= pa ? k - QPF : -1);
                     const int kn = k < pb ? k + 1 : (has_sep ? lay.s[w] : -1);
-                    if (kn >= 0) ld_left(kn, true, li);
-                    if (spk) ld_spike(k, false, fi);
-                    double v = kn >= 0 ? pair_dot7(li, xv + NS * kn, hh) : 0.0;  // L_{k+1}^T x_{k+1}
+                    double v = kn >= 0 ? pair_dot7(lc, xv + NS * kn, hh) : 0.0;  // L_{k+1}^T x_{k+1}
                     if (spk) {
                         double p = 0.0;
 #pragma unroll
-                        for (int q = 0; q < 7; ++q) p = fma(fi[q], xv[NS * (pa - 1) + 7 * hh + q], p);
+                        for (int q2 = 0; q2 < 7; ++q2) p = fma(fc[q2], xv[NS * (pa - 1) + 7 * hh + q2], p);
                         v -= p + __shfl_xor_sync(0xffffffffu, p, 1);  // - F_k x_{s_{w-1}}
                     }
                     if (hh == 0 && rv) sc[r] = v;
                     __syncwarp();
-                    const double a = pair_dot7(di, sc, hh);
+                    const double a = pair_dot7(dc, sc, hh);
                     if (hh == 0 && rv) xv[NS * k + r] += a;
                     __syncwarp();
                 }
             } else {
                 for (int k = pa; k <= pb; ++k) {
-                    double di[7], li[7];
-                    ld_inv(k, di);
-                    ld_left(k, false, li);  // L_k x_{k-1}
-                    const double v = pair_dot7(li, xv + NS * (k - 1), hh);
+                    double dc[7], lc[7];
+                    ld_inv(k, dc);
+                    ld_left(k, false, lc);
+                    l2_pf(k + QPF <= pb ? k + QPF : -1, k + QPF <= pb ? k + QPF : -1, -1);
+                    const double v = pair_dot7(lc, xv + NS * (k - 1), hh);
                     if (hh == 0 && rv) sc[r] = v;
                     __syncwarp();
-                    const double a = pair_dot7(di, sc, hh);
+                    const double a = pair_dot7(dc, sc, hh);
                     if (hh == 0 && rv) xv[NS * k + r] += a;
                     __syncwarp();
                 }
@@ -2187,10 +2195,13 @@ __global__ void __launch_bounds__(QUAD_THREADS, 4)
         for (int e = tid; e < nv; e += QUAD_THREADS) xv[e] = wsv(PW_P, e);
         __syncthreads();
         double d1[1] = {0.0};
-        for (int e = tid; e < nv; e += QUAD_THREADS) {
-            const double v = srow(e, xv);
-            wsv(PW_V, e) = v;
-            d1[0] += xv[e] * v;
+        // S p: a knot per warp and step
+        for (int k = warp; k < n; k += QUAD_NWARP) {
+            const double v1 = row_block(k, xv);
+            if (hh == 0 && rv) {
+                wsb[(size_t)k * QW_STRIDE + PW_V + r] = v1;
+                d1[0] = fma(xv[NS * k + r], v1, d1[0]);
+            }
         }
         block_sum(d1, 1);
         const double alpha = eta / d1[0];
