@@ -130,6 +130,9 @@ struct gpt_handle {
     double *adj_lam64 = nullptr;
     // FP64 Schur rows (PK64 doubles per knot) and right-hand sides for the cyclic-reduction PCG
     double *S64 = nullptr, *gamma64 = nullptr, *adj_gamma64 = nullptr;
+    // the stair preconditioner (pcg_precond 2): S and Pinv in the reference's 3-block layout (allocated when
+    // that preconditioner is first configured)
+    float *Sref = nullptr, *Pref = nullptr;
     // the SQP loop as a CUDA graph: copies of the caller's buffers, the iteration count of the
     // device-side while loop, capture streams and the instantiated graphs per batch shape
     float *gxu = nullptr, *glam = nullptr, *ggoal = nullptr;
@@ -276,7 +279,21 @@ gpt_status gpt_set_solver_config(gpt_handle *h, const gpt_solver_config *sc)
         return set_err(GPT_ERR_BAD_ARG,
                        "pcg_cluster_size must be 0, 1, 2, 4, 8, 16, GPT_PCG_WARP_PAIR or GPT_PCG_WARP_QUAD");
     }
-    if (sc->pcg_precond > 1) return set_err(GPT_ERR_BAD_ARG, "pcg_precond must be 0 or 1");
+    if (sc->pcg_precond > 2) return set_err(GPT_ERR_BAD_ARG, "pcg_precond must be 0, 1 or 2");
+    if (sc->pcg_precond == 2 && !h->Sref) {
+        // the stair preconditioner's SQP loop forms S and Pinv in the reference's 3-block layout: its
+        // buffers are allocated here, outside any solve
+        const size_t T = h->cap_knots;
+        if (cudaMalloc((void **)&h->Sref, sizeof(float) * S_STRIDE * T) != cudaSuccess ||
+            cudaMalloc((void **)&h->Pref, sizeof(float) * S_STRIDE * T) != cudaSuccess) {
+            cudaGetLastError();
+            cudaFree(h->Sref);
+            h->Sref = nullptr;
+            return set_err(GPT_ERR_CUDA, "cannot allocate the stair preconditioner's Schur buffers");
+        }
+        cudaMemset(h->Sref, 0, sizeof(float) * S_STRIDE * T);
+        cudaMemset(h->Pref, 0, sizeof(float) * S_STRIDE * T);
+    }
     if (sc->schur_fp64 > 1) return set_err(GPT_ERR_BAD_ARG, "schur_fp64 must be 0 or 1");
     if (sc->sqp_graph > (uint32_t)MAX_BRANCHES) return set_err(GPT_ERR_BAD_ARG, "sqp_graph must be 0 .. 8");
     if (sc->sqp_max_iter > h->cap_sqp_iter) {
@@ -388,6 +405,13 @@ gpt_status gpt_create(const gpt_problem_config *pc, const gpt_solver_config *sc,
         gpt_destroy(h);
         return cuda_err(e, "gpt_create workspace");
     }
+    if (sc->pcg_precond == 2) {
+        const gpt_status st2 = gpt_set_solver_config(h, sc);
+        if (st2 != GPT_OK) {
+            gpt_destroy(h);
+            return st2;
+        }
+    }
     *out = h;
     return GPT_OK;
 }
@@ -425,6 +449,7 @@ gpt_status gpt_destroy(gpt_handle *h)
     cudaFree(h->adj_h); cudaFree(h->adj_zero); cudaFree(h->adj_gamma); cudaFree(h->adj_lam); cudaFree(h->adj_mu);
     cudaFree(h->adj_part); cudaFree(h->adj_lam64);
     cudaFree(h->S64); cudaFree(h->gamma64); cudaFree(h->adj_gamma64);
+    cudaFree(h->Sref); cudaFree(h->Pref);
     for (auto &ge : h->graphs) cudaGraphExecDestroy(ge.exec);
     cudaFree(h->gxu); cudaFree(h->glam); cudaFree(h->ggoal); cudaFree(h->d_iter);
     cudaFree(h->trk_xu_old); cudaFree(h->trk_rows); cudaFree(h->trk_clk); cudaFree(h->trk_inst);
@@ -489,7 +514,7 @@ gpt_status gpt_form_ss(gpt_handle *h, uint32_t N, const float *d_S, float *d_Pin
     if (!h || !d_S || !d_Pinv) return set_err(GPT_ERR_BAD_ARG, "null argument");
     DeviceGuard dg(h->device);
     if (!check_n(h, N)) return set_err(GPT_ERR_BAD_ARG, "knot_points out of range");
-    GPT_CUDA(launch_form_ss((int)N, d_S, d_Pinv, (cudaStream_t)stream));
+    GPT_CUDA(launch_form_ss(single_view(N), d_S, d_Pinv, h->num_sms, (cudaStream_t)stream));
     return GPT_OK;
 }
 
@@ -700,22 +725,31 @@ static gpt_status enqueue_iteration(gpt_handle *h, const SqpPlan &pl, const floa
     const SolverParams &SP = pl.SP;
     const int ns = pl.ns;
     const bool f64 = SP.pcg_precond == 1 && SP.schur_fp64;
-    const float *S_rows = f64 ? reinterpret_cast<const float *>(h->S64) : h->S;
+    const bool stair = SP.pcg_precond == 2;
+    const float *S_rows = f64 ? reinterpret_cast<const float *>(h->S64) : (stair ? h->Sref : h->S);
     {
         PhaseTimer t(h, s, GPT_PHASE_KKT);
         GPT_CUDA(launch_kkt(bv, pl.P, d_xu, d_goal, h->xs, h->G, h->C, h->g, h->c, ns, s));
     }
     {
         PhaseTimer t(h, s, GPT_PHASE_SCHUR);
-        if (f64)
+        if (f64) {
             GPT_CUDA(launch_schur64(bv, h->G, h->C, h->g, h->c, h->S64, h->gamma64, nullptr, h->Ginv64, ns, s));
-        else
+        } else if (stair) {
+            // the reference's rows and block-Jacobi Pinv (gato_form_schur_jacobi), then the stair blocks
+            if (!h->Sref) return set_err(GPT_ERR_BAD_ARG, "pcg_precond 2 was not configured on this handle");
+            GPT_CUDA(launch_schur(0, bv, 0.f, h->G, h->C, h->g, h->c, h->Sref, h->Pref, h->gamma, h->Ginv, h->Ginv64,
+                                  nullptr, 1, ns, s));
+            GPT_CUDA(launch_form_ss(bv, h->Sref, h->Pref, ns, s));
+        } else {
             GPT_CUDA(launch_schur(1, bv, 0.f, h->G, h->C, h->g, h->c, h->S, nullptr, h->gamma, h->Ginv, h->Ginv64,
                                   nullptr, SP.pcg_precond == 0 ? 1 : 0, ns, s));
+        }
     }
     {
         PhaseTimer t(h, s, GPT_PHASE_PCG);
-        GPT_CUDA(launch_pcg(bv, pl.maxN, pl.minN, f64 ? 2 : 1, (int)SP.pcg_precond, S_rows, nullptr, h->gamma,
+        GPT_CUDA(launch_pcg(bv, pl.maxN, pl.minN, f64 ? 2 : (stair ? 0 : 1), (int)SP.pcg_precond, S_rows,
+                            stair ? h->Pref : nullptr, h->gamma,
                             h->gamma64, d_lambda, h->lam64, h->crw, (int)SP.pcg_max_iter, SP.pcg_tol,
                             (int)SP.pcg_exit_mode, nullptr, h->pcg_log, (int)SP.sqp_max_iter,
                             (int)SP.pcg_cluster_size, ns, s));
@@ -1037,7 +1071,8 @@ gpt_status gpt_autotune(gpt_handle *h, uint32_t B, const uint32_t *h_N, const fl
     if ((size_t)total > h->cap_knots) return set_err(GPT_ERR_CAPACITY, "total knots exceed workspace");
     // candidates: the smallest cluster that holds the longest horizon (<= 128 knots per CTA) and 2x, 4x it
     int cs0 = 1;
-    while ((maxN + cs0 - 1) / cs0 > PCG_KPC_MAX) cs0 *= 2;
+    const int kpc_cap = h->sc.pcg_precond == 2 ? PCG_KPC_STAIR : PCG_KPC_MAX;
+    while ((maxN + cs0 - 1) / cs0 > kpc_cap) cs0 *= 2;
     std::vector<uint32_t> cand;
     for (int cs = cs0; cs <= 16 && cs <= 4 * cs0 && cs <= minN; cs *= 2) cand.push_back((uint32_t)cs);
     if (cand.empty()) cand.push_back((uint32_t)cs0);
@@ -1114,6 +1149,7 @@ gpt_status gpt_sqp_adjoint(gpt_handle *h, uint32_t B, const uint32_t *h_N, const
         return set_err(GPT_ERR_BAD_ARG, "null argument");
     DeviceGuard dg(h->device);
     cudaStream_t s = (cudaStream_t)stream;
+    if (h->sc.pcg_precond == 2) return set_err(GPT_ERR_BAD_ARG, "the adjoint runs with pcg_precond 0 or 1");
     BatchView bv;
     int maxN = 0, minN = 0;
     {

@@ -10,6 +10,7 @@ namespace gpt {
 
 constexpr int MAX_PCG_KNOTS = 512;  // horizon limit of the library (16-CTA cluster x 32 knots)
 constexpr int PCG_KPC_MAX = 128;    // knots per CTA held in shared memory by the PCG
+constexpr int PCG_KPC_STAIR = 64;   // with the stair preconditioner (its Pinv blocks staged too)
 constexpr int PCG_WARP_PAIR = 32;   // pcg_cluster_size value selecting pcg_pair_kernel (one 128-thread CTA per instance)
 constexpr int PCG_WARP_QUAD = 64;   // pcg_cluster_size value selecting pcg_quad_kernel (four warps factor four parts)
 
@@ -41,7 +42,8 @@ cudaError_t launch_schur(int mode, const BatchView &bv, float rho_scalar, const 
 size_t pcg_cluster_smem_bytes(int kpc);
 int pcg_pick_cluster(int maxN, int B, int num_sms, int requested);
 // fmt 0: S and Pinv in the reference 3-block layout; fmt 1: packed rows (PK floats per knot) in S
-// precond 0: block-Jacobi with the given Pinv; 1: exact block-tridiagonal LDL^T of each CTA's chunk
+// precond 0: block-Jacobi with the given Pinv; 1: exact block-tridiagonal LDL^T of each CTA's chunk;
+// 2: the stair preconditioner (Pinv's diagonal and off-diagonal blocks of gpt_form_ss, fmt 0 only)
 // cr_ws: FP64 workspace of 2 x 196 doubles per knot of the batch (the cyclic-reduction couplings of
 // precond 1, the warp-pair kernel's factors and vectors, the partitioned kernel's factors, vectors and
 // coupling blocks; unused by precond 0)
@@ -107,7 +109,7 @@ cudaError_t launch_track_tail(const BatchView &bv, const int *rows, TrackClock *
                               uint32_t *iters_log, uint32_t log_cap, cudaStream_t s);
 cudaError_t launch_track_final(const BatchView &bv, const float *xs, const float *goal, TrackInst *inst, cudaStream_t s);
 // stair preconditioner's off-diagonal Pinv blocks (gato_form_ss_inner), reference 3-block rows
-cudaError_t launch_form_ss(int N, const float *S, float *Pinv, cudaStream_t s);
+cudaError_t launch_form_ss(const BatchView &bv, const float *S, float *Pinv, int num_sms, cudaStream_t s);
 // batched rigid-body library kernels (gpt_grid.cu)
 cudaError_t launch_ee_pose(uint32_t n, const float *x, uint32_t stride, float *pose, cudaStream_t s);
 cudaError_t launch_fd(uint32_t n, const float *xu, uint32_t stride, float *qdd, cudaStream_t s);

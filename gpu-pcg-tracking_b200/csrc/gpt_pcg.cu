@@ -48,15 +48,20 @@ constexpr int PCG_KPT = (PCG_KPC_MAX + PCG_TK - 1) / PCG_TK;  // knots per threa
 constexpr int RR_PERIOD = 32;
 constexpr int SLOT_CS = 16;
 
-size_t pcg_cluster_smem_bytes(int kpc)
+// stair: the stair preconditioner's left blocks of Pinv, per knot of the chunk and for the next
+// chunk's first knot ((kpc + 1) x 196 floats)
+size_t pcg_cluster_smem_bytes(int kpc, bool stair)
 {
     return sizeof(float) * ((size_t)kpc * PK + SS + 2 * (size_t)NS * (kpc + 2) + 2 * NS) +
-           sizeof(double) * (2 * SLOT_CS * 4 + PCG_NWARP * 4) + 16;
+           sizeof(double) * (2 * SLOT_CS * 4 + PCG_NWARP * 4) + 16 +
+           (stair ? sizeof(float) * (size_t)(kpc + 1) * SS : 0);
 }
+size_t pcg_cluster_smem_bytes(int kpc) { return pcg_cluster_smem_bytes(kpc, false); }
 
 struct PcgCtx {
     float *Sp, *left_next, *rv, *pv, *zh_l, *zh_r;
     double *slots, *red;
+    float *Pl;  // stair preconditioner: Pinv left blocks (kpc_max + 1 blocks; the last one is the next chunk's)
 };
 
 // Fixed-order reduction of NV doubles over the cluster; every thread gets the totals.
@@ -188,7 +193,12 @@ __device__ __forceinline__ float pinv_row(const float *blk, const float *x, cons
 
 // FMT 0: S, Pinv in the reference's 3-block layout (588 floats per knot, Pinv diag at +196)
 // FMT 1: packed 408 floats per knot (written by the Schur kernel of the SQP loop)
-template <int CS, int FMT>
+// PRE 0: block-Jacobi (Pinv's diagonal blocks); PRE 2: the stair preconditioner of gato_form_ss
+// (oldschur.cuh:334-494; FMT 0 only), z_k = Pinv[k].left r_{k-1} + Pinv[k].diag r_k + Pinv[k].right r_{k+1}
+// with Pinv[k].right = Pinv[k+1].left^T (both are -theta^{-1} L theta^{-1} products of the symmetric
+// theta^{-1}), so only the left blocks are staged; the residual's neighbouring knots come through
+// the halo slots of the residual copy, exchanged through distributed shared memory like p's.
+template <int CS, int FMT, int PRE>
 __global__ void __launch_bounds__(PCG_THREADS, 1)
     pcg_cluster_kernel(BatchView bv, int kpc_max, const float *__restrict__ S, const float *__restrict__ Pinv,
                        const float *__restrict__ gamma, float *__restrict__ lambda, double *__restrict__ lambda64,
@@ -209,6 +219,8 @@ __global__ void __launch_bounds__(PCG_THREADS, 1)
         c.slots = reinterpret_cast<double *>(base + used + (used & 1));
     }
     c.red = c.slots + 2 * SLOT_CS * 4;
+    c.Pl = reinterpret_cast<float *>(c.red + PCG_NWARP * 4);
+    static_assert(PRE == 0 || FMT == 0, "the stair preconditioner reads the reference's 3-block Pinv");
 
     const int tid = threadIdx.x;
     const int b = bv.b0 + (int)blockIdx.x / CS;
@@ -236,9 +248,12 @@ __global__ void __launch_bounds__(PCG_THREADS, 1)
                 c.Sp[kl * PK + PK_DIAG + t] = S[g + SS + w];
                 c.Sp[kl * PK + PK_PINV + t] = Pinv[g + SS + w];
             }
+            if (PRE == 2) c.Pl[kl * SS + w] = Pinv[g + w];
         }
-        for (int i = tid; i < SS; i += PCG_THREADS)
+        for (int i = tid; i < SS; i += PCG_THREADS) {
             c.left_next[i] = (k1 < N) ? S[(size_t)S_STRIDE * (kb + k1) + i] : 0.f;
+            if (PRE == 2) c.Pl[kpc_max * SS + i] = (k1 < N) ? Pinv[(size_t)S_STRIDE * (kb + k1) + i] : 0.f;
+        }
     }
     const float *gb = gamma + (size_t)NS * (kb + k0);
     float *lb = lambda + (size_t)NS * (kb + k0);
@@ -325,12 +340,46 @@ __global__ void __launch_bounds__(PCG_THREADS, 1)
 #pragma unroll
         for (int j = 0; j < PCG_KPT; ++j)
             if (own[j]) c.rv[NS * (g0 + PCG_TK * j + 1) + r] = (float)res[j];
-        __syncthreads();
+        if constexpr (PRE == 2) {
+            // the neighbouring chunks' boundary residuals into the halo slots (zero at the horizon's ends)
+            if (tid < NS) {
+                if (k0 == 0) c.rv[tid] = 0.f;
+                if (k1 == N) c.rv[NS * (kpc + 1) + tid] = 0.f;
+            }
+            if constexpr (CS > 1) {
+                cg::cluster_group cl = cg::this_cluster();
+#pragma unroll
+                for (int j = 0; j < PCG_KPT; ++j) {
+                    if (own[j]) {
+                        const int kl = g0 + PCG_TK * j;
+                        if (kl == 0 && rank > 0) cl.map_shared_rank(c.rv, rank - 1)[NS * (kpc_left + 1) + r] = (float)res[j];
+                        if (kl == kpc - 1 && rank < CS - 1) cl.map_shared_rank(c.rv, rank + 1)[r] = (float)res[j];
+                    }
+                }
+                cl.sync();
+            } else {
+                __syncthreads();
+            }
+        } else {
+            __syncthreads();
+        }
 #pragma unroll
         for (int j = 0; j < PCG_KPT; ++j) {
             if (own[j]) {
                 const int kl = g0 + PCG_TK * j;
                 zz[j] = pinv_row(c.Sp + (size_t)kl * PK, c.rv + NS * (kl + 1), ro);
+                if constexpr (PRE == 2) {
+                    const int k = k0 + kl;
+                    const float *pl = c.Pl + (size_t)kl * SS;                                  // Pinv[k].left
+                    const float *pn = c.Pl + (size_t)(kl + 1 < kpc ? kl + 1 : kpc_max) * SS;  // Pinv[k+1].left
+                    float a0 = 0.f, a1 = 0.f;
+#pragma unroll
+                    for (int t = 0; t < NS; ++t) {
+                        if (k > 0) a0 = fmaf(pl[r + NS * t], c.rv[NS * kl + t], a0);
+                        if (k < N - 1) a1 = fmaf(pn[t + NS * r], c.rv[NS * (kl + 2) + t], a1);
+                    }
+                    zz[j] += a0 + a1;
+                }
                 d[1] += res[j] * (double)zz[j];
                 d[2] += res[j] * res[j];
                 if constexpr (CS > 1) {
@@ -2362,13 +2411,13 @@ int pcg_pick_cluster(int maxN, int B, int num_sms, int requested)
     return cs;
 }
 
-template <int CS, int FMT>
+template <int CS, int FMT, int PRE = 0>
 static cudaError_t launch_pcg_cs(const BatchView &bv, int kpc_max, const float *S, const float *Pinv,
                                  const float *gamma, float *lambda, double *lambda64, int max_iter, float tol,
                                  int exit_mode, uint32_t *out_iters, uint32_t *pcg_log, int log_stride, cudaStream_t s)
 {
-    auto kern = pcg_cluster_kernel<CS, FMT>;
-    const size_t smem = pcg_cluster_smem_bytes(kpc_max);
+    auto kern = pcg_cluster_kernel<CS, FMT, PRE>;
+    const size_t smem = pcg_cluster_smem_bytes(kpc_max, PRE == 2);
     {
         const cudaError_t e = ensure_func_attrs((const void *)kern, smem, CS > 8);
         if (e != cudaSuccess) return e;
@@ -2440,11 +2489,13 @@ cudaError_t launch_pcg(const BatchView &bv, int max_n_knots, int min_n_knots, in
                         : launch_pcg_pair_t<1>(bv, max_n_knots, S, gamma, gamma64, lambda, lambda64, cr_ws, max_iter,
                                                tol, exit_mode, out_iters, pcg_log, log_stride, s);
     }
+    if (precond == 2 && fmt != 0) return cudaErrorInvalidValue;  // the stair Pinv comes in the reference layout
+    const int kpc_cap = precond == 2 ? PCG_KPC_STAIR : PCG_KPC_MAX;
     int cs = (precond == 1 && cluster_size == 0) ? 1 : pcg_pick_cluster(max_n_knots, bv.B, num_sms, cluster_size);
-    while ((max_n_knots + cs - 1) / cs > PCG_KPC_MAX) cs *= 2;
+    while ((max_n_knots + cs - 1) / cs > kpc_cap) cs *= 2;
     while (cs > 1 && cs > min_n_knots) cs /= 2;  // every CTA owns at least one knot
     const int kpc_max = (max_n_knots + cs - 1) / cs;
-    if (kpc_max > PCG_KPC_MAX || cs > 16) return cudaErrorInvalidValue;
+    if (kpc_max > kpc_cap || cs > 16) return cudaErrorInvalidValue;
 #define GPT_PCG_CASE(CSV)                                                                                      \
     case CSV:                                                                                                  \
         if (precond == 1) {                                                                                    \
@@ -2456,6 +2507,9 @@ cudaError_t launch_pcg(const BatchView &bv, int max_n_knots, int min_n_knots, in
                        : launch_pcg_chain_cs<CSV, 0>(bv, kpc_max, S, gamma, gamma64, lambda, lambda64, cr_ws,  \
                                                      max_iter, tol, exit_mode, out_iters, pcg_log, log_stride, s); \
         }                                                                                                      \
+        if (precond == 2)                                                                                      \
+            return launch_pcg_cs<CSV, 0, 2>(bv, kpc_max, S, Pinv, gamma, lambda, lambda64, max_iter, tol,      \
+                                            exit_mode, out_iters, pcg_log, log_stride, s);                     \
         return fmt ? launch_pcg_cs<CSV, 1>(bv, kpc_max, S, Pinv, gamma, lambda, lambda64, max_iter, tol,       \
                                            exit_mode, out_iters, pcg_log, log_stride, s)                       \
                    : launch_pcg_cs<CSV, 0>(bv, kpc_max, S, Pinv, gamma, lambda, lambda64, max_iter, tol,       \

@@ -624,22 +624,27 @@ __device__ __forceinline__ void ss_prod(const float *A, const float *B, float *o
     }
 }
 
-__global__ void __launch_bounds__(32 * SS_WARPS) ss_kernel(int N, const float *__restrict__ S, float *__restrict__ Pinv)
+__global__ void __launch_bounds__(32 * SS_WARPS) ss_kernel(BatchView bv, const float *__restrict__ S,
+                                                           float *__restrict__ Pinv)
 {
     __shared__ SsWarpSmem sm_all[SS_WARPS];
     const int lane = threadIdx.x & 31;
     SsWarpSmem &sm = sm_all[threadIdx.x >> 5];
-    const int k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    if (k >= N) return;  // warp-uniform
+    const int j = bv.j0 + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    if (j >= bv.j0 + bv.total_knots) return;  // warp-uniform
+    const int b = bv.inst(j);
+    if (!bv.active(b)) return;
+    const int N = bv.N(b), k = j - bv.off(b);
+    // knot j of the batch; its neighbours j - 1, j + 1 belong to the same instance when k > 0, k < N - 1
     for (int e = lane; e < SS; e += 32) {
-        sm.tk[e] = Pinv[(size_t)S_STRIDE * k + SS + e];
+        sm.tk[e] = Pinv[(size_t)S_STRIDE * j + SS + e];
         if (k > 0) {
-            sm.tm[e] = Pinv[(size_t)S_STRIDE * (k - 1) + SS + e];
-            sm.phi[e] = S[(size_t)S_STRIDE * k + e];
+            sm.tm[e] = Pinv[(size_t)S_STRIDE * (j - 1) + SS + e];
+            sm.phi[e] = S[(size_t)S_STRIDE * j + e];
         }
         if (k < N - 1) {
-            sm.tp[e] = Pinv[(size_t)S_STRIDE * (k + 1) + SS + e];
-            sm.phin[e] = S[(size_t)S_STRIDE * (k + 1) + e];
+            sm.tp[e] = Pinv[(size_t)S_STRIDE * (j + 1) + SS + e];
+            sm.phin[e] = S[(size_t)S_STRIDE * (j + 1) + e];
         }
     }
     __syncwarp();
@@ -651,7 +656,7 @@ __global__ void __launch_bounds__(32 * SS_WARPS) ss_kernel(int N, const float *_
             float r = 0.f;
 #pragma unroll
             for (int t = 0; t < NS; ++t) r = fmaf(sm.scr[t * NS + row], sm.tm[col * NS + t], r);
-            Pinv[(size_t)S_STRIDE * k + e] = -r;
+            Pinv[(size_t)S_STRIDE * j + e] = -r;
         }
         __syncwarp();
     }
@@ -663,14 +668,16 @@ __global__ void __launch_bounds__(32 * SS_WARPS) ss_kernel(int N, const float *_
             float r = 0.f;
 #pragma unroll
             for (int t = 0; t < NS; ++t) r = fmaf(sm.scr[t * NS + row], sm.tp[col * NS + t], r);
-            Pinv[(size_t)S_STRIDE * k + 2 * SS + e] = -r;
+            Pinv[(size_t)S_STRIDE * j + 2 * SS + e] = -r;
         }
     }
 }
 
-cudaError_t launch_form_ss(int N, const float *S, float *Pinv, cudaStream_t s)
+cudaError_t launch_form_ss(const BatchView &bv, const float *S, float *Pinv, int num_sms, cudaStream_t s)
 {
-    ss_kernel<<<(N + SS_WARPS - 1) / SS_WARPS, 32 * SS_WARPS, 0, s>>>(N, S, Pinv);
+    (void)num_sms;
+    if (bv.total_knots <= 0) return cudaSuccess;
+    ss_kernel<<<(bv.total_knots + SS_WARPS - 1) / SS_WARPS, 32 * SS_WARPS, 0, s>>>(bv, S, Pinv);
     return cudaGetLastError();
 }
 
