@@ -572,7 +572,9 @@ def main():
 
     last_rho = [1e-3] * B
     # the PCG cluster size for this batch shape, chosen by timing (gpt_autotune) unless given
-    tuned_cs = args.pcg_cluster if args.pcg_cluster else sv.autotune(Ns, goal, lam0, xu0, [1e-3] * B)
+    schedule = {}
+    tuned_cs = args.pcg_cluster if args.pcg_cluster else sv.autotune(Ns, goal, lam0, xu0, [1e-3] * B,
+                                                                     schedule=schedule)
 
     clocks = ClockSampler(torch.cuda.current_device())
     clocks.start()
@@ -780,6 +782,7 @@ def main():
                                f"<= {args.sqp_max_iter} SQP iterations",
                    "instances_per_gpu": B, "knot_points": N, "pcg_exit_tol": args.tol, "parallelism": f"dp{world}",
                    "pcg_precond": precond_name, "pcg_cluster_size": tuned_cs,
+                   "launch_schedule_ctas_per_sm": schedule or None,
                    "pcg_cluster_source": "given" if args.pcg_cluster else "gpt_autotune",
                    "l2": "256 MB buffer written between timed steps"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,

@@ -171,7 +171,7 @@ def _declare(L):
         "gpt_ls_compute_merit_noalloc": ([P(ProblemConfig), u32, vp, vp, vp, vp, vp, vp], C.c_int),
         "gpt_sqp_adjoint": ([vp, u32, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp], C.c_int),
         "gpt_set_cost_weights": ([vp, f32, f32, f32], C.c_int),
-        "gpt_autotune": ([vp, u32, vp, vp, vp, vp, vp, P(u32), vp], C.c_int),
+        "gpt_autotune": ([vp, u32, vp, vp, vp, vp, vp, P(u32), vp, vp], C.c_int),
         "gpt_default_track_config": ([P(TrackConfig)], None),
         "gpt_track": ([vp, u32, u32, vp, vp, vp, P(TrackConfig), vp, vp, u32, P(TrackStats), vp], C.c_int),
         "gpt_track_batched": ([vp, u32, vp, vp, vp, vp, vp, P(TrackConfig), vp, vp, u32, vp, vp], C.c_int),
@@ -394,14 +394,20 @@ class Solver:
                                                  _ptr(tr["lam"]), _ptr(tr["dz"]), _ptr(tr["rec"]), _stream(stream)))
         return list(rr), StatsList(sts), tr
 
-    def autotune(self, knot_points: Sequence[int], eePos_traj, lam, xu, rho: Sequence[float], stream=None) -> int:
-        """gpt_autotune: pick and remember the fastest PCG cluster size for this batch shape."""
+    def autotune(self, knot_points: Sequence[int], eePos_traj, lam, xu, rho: Sequence[float], stream=None,
+                 schedule: Optional[dict] = None) -> int:
+        """gpt_autotune: pick and remember the fastest PCG kernel and per-knot launch schedule for this batch
+        shape.  Returns the PCG cluster size; `schedule` (a dict, optional) receives the CTAs per SM chosen
+        for the KKT, Schur, merit and dz launches."""
         B = len(knot_points)
         Ns = (C.c_uint32 * B)(*knot_points)
         rr = (C.c_float * B)(*rho)
         cs = C.c_uint32(0)
+        sched = (C.c_uint32 * 4)()
         _check(lib().gpt_autotune(self._h, B, C.cast(Ns, C.c_void_p), _ptr(eePos_traj), _ptr(lam), _ptr(xu),
-                                  C.cast(rr, C.c_void_p), C.byref(cs), _stream(stream)))
+                                  C.cast(rr, C.c_void_p), C.byref(cs), C.cast(sched, C.c_void_p), _stream(stream)))
+        if schedule is not None:
+            schedule.update(dict(zip(("kkt", "schur", "merit", "dz"), list(sched))))
         return cs.value
 
     def sqp_adjoint(self, knot_points: Sequence[int], eePos_traj, xs, xu, rho: Sequence[float], grad_xu_next,

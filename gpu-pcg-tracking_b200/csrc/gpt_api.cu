@@ -154,7 +154,11 @@ struct gpt_handle {
     struct Tuned {
         int B, total, maxN, minN;
         uint32_t cluster;
+        uint8_t cta[4];  // CTAs per SM of the KKT, FP64 Schur, merit and dz launches
     };
+    // a schedule under trial inside gpt_autotune (overrides the tuned entry)
+    bool trial = false;
+    uint8_t trial_cta[4] = {0, 0, 0, 0};
     std::vector<Tuned> tuned;
     uint32_t cap_sqp_iter = 0;  // pcg_log rows allocated at creation
     // pinned host staging
@@ -191,7 +195,7 @@ ProblemParams to_params(const gpt_problem_config &pc)
 }
 SolverParams to_solver(const gpt_solver_config &sc)
 {
-    SolverParams S;
+    SolverParams S{};
     S.sqp_max_iter = sc.sqp_max_iter;
     S.pcg_max_iter = sc.pcg_max_iter;
     S.pcg_tol = sc.pcg_exit_tol;
@@ -710,7 +714,8 @@ static gpt_status enqueue_prologue(gpt_handle *h, const SqpPlan &pl, const float
 {
     PhaseTimer t(h, s, GPT_PHASE_INIT);
     GPT_CUDA(launch_init(pl.bv, d_xu, h->xs, pl.ns, s));
-    GPT_CUDA(launch_merit(pl.bv, pl.P, 1, d_xu, nullptr, d_goal, h->xs, h->knot_merit, pl.ns, s));
+    GPT_CUDA(launch_merit(pl.bv, pl.P, 1, d_xu, nullptr, d_goal, h->xs, h->knot_merit, pl.ns, s,
+                          ctas_or_default(pl.SP.cta_merit)));
     GPT_CUDA(launch_accept(pl.bv, 0, pl.SP, h->knot_merit, nullptr, nullptr, nullptr, nullptr, pl.ns, s));
     return GPT_OK;
 }
@@ -729,12 +734,13 @@ static gpt_status enqueue_iteration(gpt_handle *h, const SqpPlan &pl, const floa
     const float *S_rows = f64 ? reinterpret_cast<const float *>(h->S64) : (stair ? h->Sref : h->S);
     {
         PhaseTimer t(h, s, GPT_PHASE_KKT);
-        GPT_CUDA(launch_kkt(bv, pl.P, d_xu, d_goal, h->xs, h->G, h->C, h->g, h->c, ns, s));
+        GPT_CUDA(launch_kkt(bv, pl.P, d_xu, d_goal, h->xs, h->G, h->C, h->g, h->c, ns, s, ctas_or_default(SP.cta_kkt)));
     }
     {
         PhaseTimer t(h, s, GPT_PHASE_SCHUR);
         if (f64) {
-            GPT_CUDA(launch_schur64(bv, h->G, h->C, h->g, h->c, h->S64, h->gamma64, nullptr, h->Ginv64, ns, s));
+            GPT_CUDA(launch_schur64(bv, h->G, h->C, h->g, h->c, h->S64, h->gamma64, nullptr, h->Ginv64, ns, s,
+                                    ctas_or_default(SP.cta_schur)));
         } else if (stair) {
             // the reference's rows and block-Jacobi Pinv (gato_form_schur_jacobi), then the stair blocks
             if (!h->Sref) return set_err(GPT_ERR_BAD_ARG, "pcg_precond 2 was not configured on this handle");
@@ -756,11 +762,13 @@ static gpt_status enqueue_iteration(gpt_handle *h, const SqpPlan &pl, const floa
     }
     {
         PhaseTimer t(h, s, GPT_PHASE_DZ);
-        GPT_CUDA(launch_dz(bv, h->Ginv, h->Ginv64, h->C, h->g, d_lambda, h->lam64, h->dz, ns, s));
+        GPT_CUDA(launch_dz(bv, h->Ginv, h->Ginv64, h->C, h->g, d_lambda, h->lam64, h->dz, ns, s,
+                           ctas_or_default(SP.cta_dz)));
     }
     {
         PhaseTimer t(h, s, GPT_PHASE_MERIT);
-        GPT_CUDA(launch_merit(bv, pl.P, NUM_ALPHAS, d_xu, h->dz, d_goal, h->xs, h->knot_merit, ns, s));
+        GPT_CUDA(launch_merit(bv, pl.P, NUM_ALPHAS, d_xu, h->dz, d_goal, h->xs, h->knot_merit, ns, s,
+                              ctas_or_default(SP.cta_merit)));
     }
     if (reset_active) GPT_CUDA(cudaMemsetAsync(h->d_active, 0, sizeof(uint32_t), s));
     {
@@ -916,6 +924,28 @@ static gpt_status sqp_graph_for(gpt_handle *h, const SqpPlan &pl, cudaGraphExec_
     return GPT_OK;
 }
 
+// The autotuned PCG kernel and launch schedule of this batch shape (gpt_autotune), where the solver
+// config leaves the PCG cluster size to the library; a schedule under trial takes precedence.
+static void apply_tuned(const gpt_handle *h, const BatchView &bv, int maxN, int minN, SolverParams &SP)
+{
+    if (SP.pcg_cluster_size == 0) {
+        for (const auto &t : h->tuned)
+            if (t.B == bv.B && t.total == bv.total_knots && t.maxN == maxN && t.minN == minN) {
+                SP.pcg_cluster_size = t.cluster;
+                SP.cta_kkt = t.cta[0];
+                SP.cta_schur = t.cta[1];
+                SP.cta_merit = t.cta[2];
+                SP.cta_dz = t.cta[3];
+            }
+    }
+    if (h->trial) {
+        SP.cta_kkt = h->trial_cta[0];
+        SP.cta_schur = h->trial_cta[1];
+        SP.cta_merit = h->trial_cta[2];
+        SP.cta_dz = h->trial_cta[3];
+    }
+}
+
 // Buffers of gpt_sqp_solve_batched_trace
 struct SqpTrace {
     uint32_t iters;
@@ -937,10 +967,7 @@ static gpt_status sqp_run(gpt_handle *h, uint32_t B, const uint32_t *Ns, const f
     }
     const ProblemParams P = to_params(h->pc);
     SolverParams SP = to_solver(h->sc);
-    if (SP.pcg_cluster_size == 0) {
-        for (const auto &t : h->tuned)
-            if (t.B == bv.B && t.total == bv.total_knots && t.maxN == maxN && t.minN == minN) SP.pcg_cluster_size = t.cluster;
-    }
+    apply_tuned(h, bv, maxN, minN, SP);
     const SqpPlan plan{bv, P, SP, maxN, minN, h->num_sms};
 
     if (SP.sqp_graph && !h->profile && !tr) {
@@ -1055,7 +1082,8 @@ gpt_status gpt_sqp_solve_batched_trace(gpt_handle *h, uint32_t B, const uint32_t
 }
 
 gpt_status gpt_autotune(gpt_handle *h, uint32_t B, const uint32_t *h_N, const float *d_goal, const float *d_lambda,
-                        const float *d_xu, const float *h_rho, uint32_t *h_cluster_out, gpt_stream_t stream)
+                        const float *d_xu, const float *h_rho, uint32_t *h_cluster_out, uint32_t *h_schedule_out,
+                        gpt_stream_t stream)
 {
     if (!h || !h_N || !d_goal || !d_lambda || !d_xu || !h_rho) return set_err(GPT_ERR_BAD_ARG, "null argument");
     DeviceGuard dg(h->device);
@@ -1069,7 +1097,7 @@ gpt_status gpt_autotune(gpt_handle *h, uint32_t B, const uint32_t *h_N, const fl
         minN = (int)h_N[b] < minN ? (int)h_N[b] : minN;
     }
     if ((size_t)total > h->cap_knots) return set_err(GPT_ERR_CAPACITY, "total knots exceed workspace");
-    // candidates: the smallest cluster that holds the longest horizon (<= 128 knots per CTA) and 2x, 4x it
+    // PCG candidates: the smallest cluster that holds the longest horizon (<= 128 knots per CTA) and 2x, 4x it
     int cs0 = 1;
     const int kpc_cap = h->sc.pcg_precond == 2 ? PCG_KPC_STAIR : PCG_KPC_MAX;
     while ((maxN + cs0 - 1) / cs0 > kpc_cap) cs0 *= 2;
@@ -1087,15 +1115,17 @@ gpt_status gpt_autotune(gpt_handle *h, uint32_t B, const uint32_t *h_N, const fl
     std::vector<float> rho(h_rho, h_rho + B);
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     gpt_status st = GPT_OK;
-    float best_ms = 1e30f;
-    uint32_t best = cand[0];
     if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) st = set_err(GPT_ERR_CUDA, "event");
-    for (size_t ci = 0; ci < cand.size() && st == GPT_OK; ++ci) {
+    // two SQP iterations of the batch with a given PCG kernel and launch schedule: the best of two timed
+    // repetitions after one warm-up (attributes, graph capture, caches)
+    auto time_schedule = [&](uint32_t cluster, const uint8_t *cta) -> float {
         h->sc = saved;
-        h->sc.pcg_cluster_size = cand[ci];
+        h->sc.pcg_cluster_size = cluster;
         h->sc.sqp_max_iter = saved.sqp_max_iter < 2 ? saved.sqp_max_iter : 2;
+        h->trial = true;
+        for (int i = 0; i < 4; ++i) h->trial_cta[i] = cta[i];
         float ms_min = 1e30f;
-        for (int rep = 0; rep < 3 && st == GPT_OK; ++rep) {  // first repetition warms up (attributes, caches)
+        for (int rep = 0; rep < 3 && st == GPT_OK; ++rep) {
             // the solve updates xu and lambda in place: run it on scratch copies
             cudaError_t e = cudaMemcpyAsync(h->adj_h, d_xu, sizeof(float) * nxu, cudaMemcpyDeviceToDevice, s);
             if (e == cudaSuccess) e = cudaMemcpyAsync(h->adj_lam, d_lambda, sizeof(float) * nl, cudaMemcpyDeviceToDevice, s);
@@ -1106,7 +1136,7 @@ gpt_status gpt_autotune(gpt_handle *h, uint32_t B, const uint32_t *h_N, const fl
             }
             std::vector<float> r = rho;
             st = sqp_run(h, B, h_N, d_goal, h->adj_lam, h->adj_h, r.data(), 1e-3f, nullptr, nullptr, nullptr, s);
-            if (st == GPT_ERR_NONFINITE) st = GPT_OK;  // timing only
+            if (st == GPT_ERR_NONFINITE || st == GPT_ERR_FACTOR) st = GPT_OK;  // timing only
             if (st != GPT_OK) break;
             float ms = 0.f;
             e = cudaEventRecord(e1, s);
@@ -1118,24 +1148,54 @@ gpt_status gpt_autotune(gpt_handle *h, uint32_t B, const uint32_t *h_N, const fl
             }
             if (rep > 0 && ms < ms_min) ms_min = ms;
         }
-        if (st == GPT_OK && ms_min < best_ms) {
-            best_ms = ms_min;
+        h->trial = false;
+        return ms_min;
+    };
+    // 1. the PCG kernel / cluster size with the default schedule
+    uint8_t cta[4] = {0, 0, 0, 0};
+    float best_ms = 1e30f;
+    uint32_t best = cand[0];
+    for (size_t ci = 0; ci < cand.size() && st == GPT_OK; ++ci) {
+        const float ms = time_schedule(cand[ci], cta);
+        if (st == GPT_OK && ms < best_ms) {
+            best_ms = ms;
             best = cand[ci];
         }
+    }
+    // 2. the per-knot kernels' grids, one kernel at a time (coordinate descent): CTAs per SM from one
+    // resident wave to the default 16 (a smaller grid gives each Schur warp a longer run of knots whose
+    // inverses it reuses, and leaves no partial last wave); a change must gain 1 %
+    static const uint8_t cta_cand[] = {4, 5, 6, 8};
+    for (int which = 0; which < 4 && st == GPT_OK; ++which) {
+        uint8_t keep = cta[which];
+        for (uint8_t cv : cta_cand) {
+            cta[which] = cv;
+            const float ms = time_schedule(best, cta);
+            if (st != GPT_OK) break;
+            if (ms < 0.99f * best_ms) {
+                best_ms = ms;
+                keep = cv;
+            }
+        }
+        cta[which] = keep;
     }
     if (e0) cudaEventDestroy(e0);
     if (e1) cudaEventDestroy(e1);
     h->sc = saved;
     h->profile = saved_profile;
+    h->trial = false;
     if (st != GPT_OK) return st;
     bool found = false;
     for (auto &t : h->tuned)
         if (t.B == (int)B && t.total == total && t.maxN == maxN && t.minN == minN) {
             t.cluster = best;
+            std::memcpy(t.cta, cta, sizeof(cta));
             found = true;
         }
-    if (!found) h->tuned.push_back({(int)B, total, maxN, minN, best});
+    if (!found) h->tuned.push_back({(int)B, total, maxN, minN, best, {cta[0], cta[1], cta[2], cta[3]}});
     if (h_cluster_out) *h_cluster_out = best;
+    if (h_schedule_out)
+        for (int i = 0; i < 4; ++i) h_schedule_out[i] = (uint32_t)ctas_or_default(cta[i]);
     return GPT_OK;
 }
 
@@ -1327,10 +1387,7 @@ gpt_status gpt_track_batched(gpt_handle *h, uint32_t B, const uint32_t *h_N, con
     }
     const ProblemParams P = to_params(h->pc);
     SolverParams SP = to_solver(h->sc);
-    if (SP.pcg_cluster_size == 0) {
-        for (const auto &t : h->tuned)
-            if (t.B == bv.B && t.total == bv.total_knots && t.maxN == maxN && t.minN == minN) SP.pcg_cluster_size = t.cluster;
-    }
+    apply_tuned(h, bv, maxN, minN, SP);
     const SqpPlan plan{bv, P, SP, maxN, minN, h->num_sms};
     const TrackParams tp = track_params(h->pc.timestep, tc.sim_step, tc.shift_threshold, (double)tc.sim_period_us);
     const uint32_t n_updates = track_update_count(tp, maxS, tc.max_control_updates);

@@ -25,7 +25,13 @@ struct SolverParams {
     uint32_t pcg_precond;       // 0 block-Jacobi (reference), 1 chunk block-tridiagonal LDL^T
     uint32_t schur_fp64;        // with pcg_precond 1: FP64 Schur formation and rows
     uint32_t sqp_graph;         // the SQP loop as one CUDA graph with a device-side while loop
+    // launch schedule of the per-knot kernels: CTAs per SM of the grid-stride launches (KKT, FP64 Schur,
+    // merit, dz); the grid is ctas_per_sm x SMs CTAs, each warp taking knots strided by the grid (KKT,
+    // merit, dz) or a contiguous run of total / grid-warps knots (Schur, whose inverses a run shares).
+    // 0 = 16.  Chosen by gpt_autotune.
+    uint8_t cta_kkt, cta_schur, cta_merit, cta_dz;
 };
+inline int ctas_or_default(uint8_t v) { return v ? (int)v : 16; }
 
 // cudaFuncSetAttribute(MaxDynamicSharedMemorySize >= smem_bytes, and NonPortableClusterSizeAllowed when
 // cluster16) for func on the CURRENT device, once per (kernel, device); thread-safe.  Function
@@ -34,7 +40,8 @@ struct SolverParams {
 cudaError_t ensure_func_attrs(const void *func, size_t smem_bytes, bool cluster16 = false);
 
 cudaError_t launch_kkt(const BatchView &bv, const ProblemParams &P, const float *xu, const float *goal,
-                       const float *xs, float *G, float *C, float *g, float *c, int num_sms, cudaStream_t s);
+                       const float *xs, float *G, float *C, float *g, float *c, int num_sms, cudaStream_t s,
+                       int ctas_per_sm = 16);
 // Ginv64 (optional) receives the inverses in FP64; need_pinv = 0 skips the theta inversion in mode 1
 cudaError_t launch_schur(int mode, const BatchView &bv, float rho_scalar, const float *G, const float *C,
                          const float *g, const float *c, float *S, float *Pinv, float *gamma, float *Ginv,
@@ -56,9 +63,11 @@ cudaError_t launch_pcg(const BatchView &bv, int max_n_knots, int min_n_knots, in
                        int log_stride, int cluster_size, int num_sms, cudaStream_t s);
 // lambda64 (optional) replaces lambda when given
 cudaError_t launch_dz(const BatchView &bv, const float *Ginv, const double *Ginv64, const float *C, const float *g,
-                      const float *lambda, const double *lambda64, float *dz, int num_sms, cudaStream_t s);
+                      const float *lambda, const double *lambda64, float *dz, int num_sms, cudaStream_t s,
+                      int ctas_per_sm = 16);
 cudaError_t launch_merit(const BatchView &bv, const ProblemParams &P, int n_alpha, const float *xu, const float *dz,
-                         const float *goal, const float *xs, float *knot_merit, int num_sms, cudaStream_t s);
+                         const float *goal, const float *xs, float *knot_merit, int num_sms, cudaStream_t s,
+                         int ctas_per_sm = 16);
 cudaError_t launch_accept(const BatchView &bv, int mode, const SolverParams &SP, const float *knot_merit,
                           const float *dz, float *xu, float *merits_out, uint32_t *active_count, int num_sms,
                           cudaStream_t s);
@@ -66,7 +75,8 @@ cudaError_t launch_init(const BatchView &bv, const float *xu, float *xs, int num
 // FP64 Schur complement for the exact-preconditioner PCG: packed rows (PK64 doubles per knot), gamma
 // (FP64), the inverses (Ginv64; Ginv FP32 too when non-null); rho from bv.st
 cudaError_t launch_schur64(const BatchView &bv, const float *G, const float *C, const float *g, const float *c,
-                           double *S64, double *gamma64, float *Ginv, double *Ginv64, int num_sms, cudaStream_t s);
+                           double *S64, double *gamma64, float *Ginv, double *Ginv64, int num_sms, cudaStream_t s,
+                           int ctas_per_sm = 16);
 // adjoint of the SQP step (gpt_adjoint.cu): per-knot goal gradients, per-instance weight gradients;
 // part holds adjoint_part_floats() floats per knot
 cudaError_t launch_adjoint_grad(const BatchView &bv, const ProblemParams &P, const float *xu, const float *goal,

@@ -278,12 +278,13 @@ __global__ void __launch_bounds__(32 * KKT_WARPS, 4) kkt_kernel(BatchView bv, Pr
 }
 
 cudaError_t launch_kkt(const BatchView &bv, const ProblemParams &P, const float *xu, const float *goal,
-                       const float *xs, float *G, float *C, float *g, float *c, int num_sms, cudaStream_t s)
+                       const float *xs, float *G, float *C, float *g, float *c, int num_sms, cudaStream_t s,
+                       int ctas_per_sm)
 {
     if (bv.total_knots <= 0) return cudaSuccess;
     int warps = (bv.total_knots + 1) / 2;  // two knots per warp
     int blocks = (warps + KKT_WARPS - 1) / KKT_WARPS;
-    const int cap = num_sms * 16;
+    const int cap = num_sms * ctas_per_sm;
     if (blocks > cap) blocks = cap;
     kkt_kernel<<<blocks, 32 * KKT_WARPS, 0, s>>>(bv, P, xu, goal, xs, G, C, g, c);
     return cudaGetLastError();

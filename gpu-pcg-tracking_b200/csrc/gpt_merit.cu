@@ -112,11 +112,12 @@ __global__ void __launch_bounds__(32 * DZ_WARPS)
 }
 
 cudaError_t launch_dz(const BatchView &bv, const float *Ginv, const double *Ginv64, const float *C, const float *g,
-                      const float *lambda, const double *lambda64, float *dz, int num_sms, cudaStream_t s)
+                      const float *lambda, const double *lambda64, float *dz, int num_sms, cudaStream_t s,
+                      int ctas_per_sm)
 {
     if (bv.total_knots <= 0) return cudaSuccess;
     int blocks = (bv.total_knots + DZ_WARPS - 1) / DZ_WARPS;
-    if (blocks > num_sms * 16) blocks = num_sms * 16;
+    if (blocks > num_sms * ctas_per_sm) blocks = num_sms * ctas_per_sm;
     dz_kernel<<<blocks, 32 * DZ_WARPS, 0, s>>>(bv, Ginv, Ginv64, C, g, lambda, lambda64, dz);
     return cudaGetLastError();
 }
@@ -283,11 +284,12 @@ __global__ void __launch_bounds__(32 * MERIT_WARPS)
 }
 
 cudaError_t launch_merit(const BatchView &bv, const ProblemParams &P, int n_alpha, const float *xu, const float *dz,
-                         const float *goal, const float *xs, float *knot_merit, int num_sms, cudaStream_t s)
+                         const float *goal, const float *xs, float *knot_merit, int num_sms, cudaStream_t s,
+                         int ctas_per_sm)
 {
     if (bv.total_knots <= 0) return cudaSuccess;
     int blocks = (bv.total_knots + MERIT_WARPS - 1) / MERIT_WARPS;
-    if (blocks > num_sms * 16) blocks = num_sms * 16;
+    if (blocks > num_sms * ctas_per_sm) blocks = num_sms * ctas_per_sm;
     merit_kernel<<<blocks, 32 * MERIT_WARPS, 0, s>>>(bv, P, n_alpha, xu, dz, goal, xs, knot_merit);
     return cudaGetLastError();
 }

@@ -550,13 +550,14 @@ __global__ void __launch_bounds__(32 * SCHUR_WARPS, 5)
 }
 
 cudaError_t launch_schur64(const BatchView &bv, const float *G, const float *C, const float *g, const float *c,
-                           double *S64, double *gamma64, float *Ginv, double *Ginv64, int num_sms, cudaStream_t s)
+                           double *S64, double *gamma64, float *Ginv, double *Ginv64, int num_sms, cudaStream_t s,
+                           int ctas_per_sm)
 {
     if (bv.total_knots <= 0) return cudaSuccess;
     if (!bv.st || !Ginv64) return cudaErrorInvalidValue;
     const size_t smem = sizeof(Schur64WarpSmem) * SCHUR_WARPS;
     int blocks = (bv.total_knots + SCHUR_WARPS - 1) / SCHUR_WARPS;
-    const int cap = num_sms * 16;
+    const int cap = num_sms * ctas_per_sm;
     if (blocks > cap) blocks = cap;
     {
         const cudaError_t e = ensure_func_attrs((const void *)schur64_kernel, smem);

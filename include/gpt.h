@@ -192,17 +192,20 @@ gpt_status gpt_sqp_solve_batched_trace(gpt_handle *h, uint32_t batch, const uint
                                        float *d_trace_xu, double *d_trace_lambda, float *d_trace_dz,
                                        gpt_iterate_record *d_trace_rec, gpt_stream_t stream);
 
-/* Autotuner (no reference counterpart): times two SQP iterations of this batch
- * (on copies of d_xu, d_lambda; the inputs are not modified) for each candidate
- * PCG cluster size -- the smallest that holds the longest horizon in
- * <= 128 knots per CTA, and twice and four times it, up to 16 and to the
- * shortest horizon, and GPT_PCG_WARP_PAIR with pcg_precond 1 -- and remembers the fastest for this batch shape
- * (instances, total knots, longest and shortest horizon).  Later solves of
- * that shape use it while pcg_cluster_size is 0.  h_cluster_out (optional)
- * receives the choice. */
+/* Autotuner (no reference counterpart).  Picks, by timing two SQP iterations of this batch (on copies of
+ * d_xu and d_lambda; the inputs are not modified), the schedule of the batch shape (instances, total knots,
+ * longest and shortest horizon), which later solves of that shape use while pcg_cluster_size is 0:
+ *   1. the PCG kernel: cluster sizes from the smallest that holds the longest horizon in <= 128 knots per
+ *      CTA (64 with the stair preconditioner) to four times it, up to 16 and the shortest horizon, and,
+ *      with pcg_precond 1, GPT_PCG_WARP_PAIR and GPT_PCG_WARP_QUAD;
+ *   2. then, one kernel at a time, the grid of the per-knot kernels -- KKT formation, FP64 Schur complement,
+ *      line-search merit, dz recovery -- as CTAs per SM in {4, 5, 6, 8, 16} (16 is the default; a change
+ *      must gain 1 %).
+ * h_cluster_out (optional) receives the PCG choice, h_schedule_out (optional, 4 entries) the CTAs per SM of
+ * the KKT, Schur, merit and dz launches. */
 gpt_status gpt_autotune(gpt_handle *h, uint32_t batch, const uint32_t *h_knot_points, const float *d_eePos_traj,
                         const float *d_lambda, const float *d_xu, const float *h_rho, uint32_t *h_cluster_out,
-                        gpt_stream_t stream);
+                        uint32_t *h_schedule_out, gpt_stream_t stream);
 
 /* Adjoint of the SQP step (no reference counterpart).  At the iterate d_xu
  * (typically a solve's result) with per-instance rho h_rho and initial states

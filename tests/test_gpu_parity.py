@@ -537,9 +537,11 @@ def test_autotune_choice_is_used(gpt, problem_mod):
     sv = gpt.Solver(max_knot_points=N, **SPEC_CFG)
     sv.set_solver(sqp_max_iter=4)
     x_in, l_in = xu0.clone(), lam0.clone()
-    cs = sv.autotune([N], goal, l_in, x_in, [1e-3])
+    sched = {}
+    cs = sv.autotune([N], goal, l_in, x_in, [1e-3], schedule=sched)
     assert torch.equal(x_in, xu0) and torch.equal(l_in, lam0)
     assert cs in (1, 2, 4, gpt.PCG_WARP_PAIR, gpt.PCG_WARP_QUAD)
+    assert sorted(sched) == ["dz", "kkt", "merit", "schur"] and set(sched.values()) <= {4, 5, 6, 8, 16}, sched
     out = []
     for given in (0, cs):
         sv.set_solver(pcg_cluster_size=given)
