@@ -40,8 +40,10 @@ SPEC = dict(timestep=0.01, integrator=1, qd_cost=1e-2, r_cost=1e-4)
 PCG_BYTES_PER_KNOT = 8 * 302 + 8 * 14 + 2 * 4 * 14 + 8 * 14
 PCG_BJ_BYTES_PER_KNOT = 4 * 784  # block-Jacobi kernel: FP32 S (588) + Pinv (196) read once
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one launch, per knot, from ncu captures of
-# 148 instances x 128 knots; they scale with the knots of a launch
-PCG_DRAM_BYTES_PER_KNOT = {"pcg_pair_kernel": (53.330432e6 + 3.051776e6) / (148 * 128)}
+# the bench's batch, 512 instances x 128 knots (the working set of a launch, ~0.26 GB, exceeds the L2, so
+# the traffic per knot depends on the batch and is not scaled to other batches)
+PCG_DRAM_BYTES_PER_KNOT = {"pcg_pair_kernel": (779.677440e6 + 92.534528e6) / (512 * 128)}
+PCG_DRAM_SOURCE = "ncu capture of the 512 x 128 bench batch, one launch
 ALG_FLOATS_PER_KNOT_SQP = 4058   # every materialised SQP-iteration tensor written once, read once
 
 
@@ -767,7 +769,8 @@ def main():
         os.path.join(ROOT, "MEASURED_PEAKS.json")) else None
     peak = mp["hbm_gbs"] if mp else 6650.0
     pcg_kernel = ("pcg_cluster_kernel" if args.pcg_precond == 0 else
-                  "pcg_pair_kernel" if tuned_cs == gpt.PCG_WARP_PAIR else "pcg_chain_kernel")
+                  "pcg_pair_kernel" if tuned_cs == gpt.PCG_WARP_PAIR else
+                  "pcg_quad_kernel" if tuned_cs == gpt.PCG_WARP_QUAD else "pcg_chain_kernel")
     per_launch_bytes = (PCG_BJ_BYTES_PER_KNOT if args.pcg_precond == 0 else PCG_BYTES_PER_KNOT) * N * B
     per_launch_s = (pcg_ms / max(pcg_launches, 1)) / 1000.0
     achieved = per_launch_bytes / per_launch_s / 1e9 if per_launch_s > 0 else 0.0
@@ -786,8 +789,8 @@ def main():
                    "pcg_cluster_source": "given" if args.pcg_cluster else "gpt_autotune",
                    "l2": "256 MB buffer written between timed steps"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": dram_pk * N * B if dram_pk else None,
-                     "traffic_source": "ncu capture of 148 x 128 knots scaled to the launch's knots",
+                     "traffic": dram_pk * N * B if (dram_pk and N * B == 512 * 128) else None,
+                     "traffic_source": PCG_DRAM_SOURCE,
                      "kernel": pcg_kernel,
                      "bytes_model": ("2752 B per knot per launch: FP64 Schur row 302 doubles read once, gamma, "
                                      "lambda in/out FP32, lambda FP64 out" if args.pcg_precond == 1 else
