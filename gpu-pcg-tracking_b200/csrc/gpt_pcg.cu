@@ -336,7 +336,13 @@ __global__ void __launch_bounds__(PCG_THREADS, 1)
 
     // z = Pinv r from the FP32 copy of r; halo exchange of z; partial dot products
     auto precond = [&](double (&d)[3]) {
-        __syncthreads();
+        // with the stair preconditioner the neighbours' halo slots of rv are written below: every CTA
+        // of the cluster must be done reading its rv (the initial residual reads the warm start's halos)
+        if constexpr (PRE == 2 && CS > 1) {
+            cg::this_cluster().sync();
+        } else {
+            __syncthreads();
+        }
 #pragma unroll
         for (int j = 0; j < PCG_KPT; ++j)
             if (own[j]) c.rv[NS * (g0 + PCG_TK * j + 1) + r] = (float)res[j];

@@ -675,6 +675,7 @@ def test_stair_preconditioner_on_the_gpu(gpt, oracle, problem_mod, solvers, clus
             its[pre] = it
         assert its[2] <= 0.75 * its[0], (N, cluster, its)
         _, o_it, o_max = oracle.pcg(N, host(S), host(Pv), host(gam), np.zeros(14 * N), 50000, tol, 0, "f32")
+        print(f"stair N={N} cluster={cluster}: block-Jacobi {its[0]}, stair {its[2]}, oracle stair {o_it}")
         assert not o_max and abs(its[2] - o_it) <= 0.25 * o_it + 5, (N, cluster, its[2], o_it)
     sv.set_solver(pcg_cluster_size=0, pcg_precond=0)
 
