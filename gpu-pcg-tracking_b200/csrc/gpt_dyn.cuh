@@ -293,6 +293,112 @@ __device__ __forceinline__ void rnea(const JointTrig &t, const float *qd, const 
     rnea_bwd<0, TANGENT>(t, dq_dir, st, tau, dtau);
 }
 
+// Joint-space mass matrix M(q) on one lane.  Column j is inverse dynamics at zero velocity with a unit
+// acceleration of joint j (gravity plays no part): only links j .. 6 accelerate (a_K = X_K a_{K-1},
+// f_K = I_K a_K, no velocity products), and the rows k >= j -- M's lower triangle -- are the joint
+// components of the forces after the backward pass has reached link j.  About a third of the work of
+// seven full inverse-dynamics passes.  M is stored packed: entry (k, j), k >= j, at k (k + 1) / 2 + j.
+template <int J, int K>
+__device__ __forceinline__ void mcol_fwd(const JointTrig &t, const float *ap, float (&f)[model::NJ][6])
+{
+    float a[6];
+    xmot<K>(t.c[K], t.s[K], ap, a);
+    inertia_apply<K>(a, f[K]);
+    if constexpr (K + 1 < model::NJ) mcol_fwd<J, K + 1>(t, a, f);
+}
+template <int J, int K>
+__device__ __forceinline__ void mcol_bwd(const JointTrig &t, float (&f)[model::NJ][6])
+{
+    if constexpr (K > J) {
+        float tf[6];
+        xforce_T<K>(t.c[K], t.s[K], f[K], tf);
+#pragma unroll
+        for (int i = 0; i < 6; ++i) f[K - 1][i] += tf[i];
+        mcol_bwd<J, K - 1>(t, f);
+    }
+}
+template <int J>
+__device__ __forceinline__ void mass_column(const JointTrig &t, float (&M)[28])
+{
+    float f[model::NJ][6];
+    const float sz[6] = {0.f, 0.f, 1.f, 0.f, 0.f, 0.f};  // S_J: rotation about the joint's z axis
+    inertia_apply<J>(sz, f[J]);
+    if constexpr (J + 1 < model::NJ) mcol_fwd<J, J + 1>(t, sz, f);
+    mcol_bwd<J, model::NJ - 1>(t, f);
+#pragma unroll
+    for (int k = J; k < model::NJ; ++k) M[(k * (k + 1)) / 2 + J] = f[k][2];
+}
+__device__ __forceinline__ void mass_matrix_lane(const JointTrig &t, float (&M)[28])
+{
+    mass_column<0>(t, M);
+    mass_column<1>(t, M);
+    mass_column<2>(t, M);
+    mass_column<3>(t, M);
+    mass_column<4>(t, M);
+    mass_column<5>(t, M);
+    mass_column<6>(t, M);
+}
+
+// x = M^{-1} b for the SPD 7x7 M (packed lower triangle, FP32) on one lane: an FP32 Cholesky
+// factorisation, the two triangular solves, then one step of iterative refinement with the residual
+// b - M x accumulated in FP64 (M's FP32 entries are exact in FP64), which brings x to the accuracy
+// of an FP64 solve of the same M while cond(M) eps32 << 1 (the iiwa's M: cond ~ 1e2 .. 1e3).
+__device__ __forceinline__ void spd7_solve_lane(const float (&M)[28], const double (&b)[NQ], double (&x)[NQ])
+{
+    float L[28];
+#pragma unroll
+    for (int j = 0; j < NQ; ++j) {
+        float d = M[(j * (j + 1)) / 2 + j];
+#pragma unroll
+        for (int k = 0; k < j; ++k) d = fmaf(-L[(j * (j + 1)) / 2 + k], L[(j * (j + 1)) / 2 + k], d);
+        const float ljj = sqrtf(d), inv = 1.f / ljj;
+        L[(j * (j + 1)) / 2 + j] = ljj;
+#pragma unroll
+        for (int i = j + 1; i < NQ; ++i) {
+            float v = M[(i * (i + 1)) / 2 + j];
+#pragma unroll
+            for (int k = 0; k < j; ++k) v = fmaf(-L[(i * (i + 1)) / 2 + k], L[(j * (j + 1)) / 2 + k], v);
+            L[(i * (i + 1)) / 2 + j] = v * inv;
+        }
+    }
+    auto solve = [&](const float (&r)[NQ], float (&y)[NQ]) {
+#pragma unroll
+        for (int i = 0; i < NQ; ++i) {
+            float v = r[i];
+#pragma unroll
+            for (int k = 0; k < i; ++k) v = fmaf(-L[(i * (i + 1)) / 2 + k], y[k], v);
+            y[i] = v / L[(i * (i + 1)) / 2 + i];
+        }
+#pragma unroll
+        for (int i = NQ - 1; i >= 0; --i) {
+            float v = y[i];
+#pragma unroll
+            for (int k = i + 1; k < NQ; ++k) v = fmaf(-L[(k * (k + 1)) / 2 + i], y[k], v);
+            y[i] = v / L[(i * (i + 1)) / 2 + i];
+        }
+    };
+    float r[NQ], y[NQ];
+#pragma unroll
+    for (int i = 0; i < NQ; ++i) r[i] = (float)b[i];
+    solve(r, y);
+#pragma unroll
+    for (int i = 0; i < NQ; ++i) x[i] = (double)y[i];
+    // refinement: r = b - M x in FP64
+#pragma unroll
+    for (int i = 0; i < NQ; ++i) {
+        double v = b[i];
+#pragma unroll
+        for (int k = 0; k < NQ; ++k) {
+            const float mik = i >= k ? M[(i * (i + 1)) / 2 + k] : M[(k * (k + 1)) / 2 + i];
+            v = fma(-(double)mik, x[k], v);
+        }
+        r[i] = (float)v;
+    }
+    solve(r, y);
+#pragma unroll
+    for (int i = 0; i < NQ; ++i) x[i] += (double)y[i];
+}
+
 // Gauss-Jordan elimination with a 7x7 SPD matrix M (no pivoting: every pivot is positive) over a
 // group of lanes holding the columns of [M | R]: lane base + i holds column i (7 entries).
 // Afterwards the lanes of R's columns hold M^{-1} R (and M's lanes the identity).  Every lane of

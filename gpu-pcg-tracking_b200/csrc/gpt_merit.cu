@@ -126,18 +126,6 @@ cudaError_t launch_dz(const BatchView &bv, const float *Ginv, const double *Ginv
 // merit
 // ------------------------------------------------------------------------
 
-struct MeritWarpSmem {
-    float x[NX + NS];    // x_k, u_k, x_{k+1}
-    float d[NX + NS];    // dz_k, dz_{k+1}
-    float goal[3];
-    float M[NUM_ALPHAS][CC];
-    float cb[NUM_ALPHAS][NQ];
-    double qdd[NUM_ALPHAS][NQ];
-    JointTrig trig[NUM_ALPHAS];  // sin, cos of q + alpha dq per step size
-    float defect[NUM_ALPHAS];
-    float cost[NUM_ALPHAS];
-};
-
 constexpr int MERIT_WARPS = 4;
 
 __device__ __forceinline__ float alpha_of(int a, int n_alpha)
@@ -145,141 +133,96 @@ __device__ __forceinline__ float alpha_of(int a, int n_alpha)
     return n_alpha == 1 ? 0.f : -1.f / (float)(1 << a);  // toplevel.cuh:409, merit.cuh:47
 }
 
-// n_alpha = 8: line search (last knot adds ||x_0 + alpha dz_0 - x_s||_1);
-// n_alpha = 1: merit at the current iterate (last knot defect 0).
+// One lane per (knot, step size): with the 8 line-search step sizes a warp takes 4 knots, for the
+// merit of the iterate (n_alpha = 1) 32.  The lane evaluates its candidate xu + alpha dz at its knot:
+// the tracking cost (iiwa_eepos_plant.cuh:240-290; forward kinematics for the end-effector term) and
+// the defect ||x_{k+1} - f(x_k, u_k)||_1 (integrator.cuh:187-219) with q'' = M^{-1} (u - c(q, q')):
+// M by its lower-triangle columns at zero velocity, c by one inverse-dynamics pass, the 7x7 solve by
+// an FP32 Cholesky refined in FP64.  The last knot: the line search adds ||x_0 + alpha dz_0 - x_s||_1,
+// the iterate's merit no defect (merit.cuh:68-77,135-137).  No shared memory and no warp synchronisation:
+// the lanes of a knot read the same addresses (one transaction per warp load).
 __global__ void __launch_bounds__(32 * MERIT_WARPS)
     merit_kernel(BatchView bv, ProblemParams P, int n_alpha, const float *__restrict__ xu,
                  const float *__restrict__ dz, const float *__restrict__ goal, const float *__restrict__ xs,
                  float *__restrict__ knot_merit)
 {
-    __shared__ MeritWarpSmem smem_all[MERIT_WARPS];
     const int lane = threadIdx.x & 31;
-    MeritWarpSmem &sm = smem_all[threadIdx.x >> 5];
+    const int per = n_alpha > 1 ? NUM_ALPHAS : 1;  // lanes per knot
+    const int kpw = 32 / per;                      // knots per warp
+    const int slot = lane / per, a = lane - per * slot;
     const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nw = (gridDim.x * blockDim.x) >> 5;
-    for (int j = bv.j0 + gw; j < bv.j0 + bv.total_knots; j += nw) {
+    const int jend = bv.j0 + bv.total_knots;
+    for (int j0 = bv.j0 + gw * kpw; j0 < jend; j0 += nw * kpw) {
+        const int j = j0 + slot;
+        if (j >= jend) continue;
         const int b = bv.inst(j);
         if (!bv.active(b)) continue;
         const int N = bv.N(b), k = j - bv.off(b);
         const bool last = (k == N - 1);
-        const int len = last ? NS : NX + NS;
-        for (int i = lane; i < len; i += 32) {
-            sm.x[i] = xu[(size_t)NX * j + i];
-            sm.d[i] = (n_alpha > 1) ? dz[(size_t)NX * j + i] : 0.f;
+        const float al = alpha_of(a, n_alpha);
+        const bool step = n_alpha > 1;
+        const float *xj = xu + (size_t)NX * j;
+        const float *dj = step ? dz + (size_t)NX * j : nullptr;
+        float q[NQ], qd[NQ];
+#pragma unroll
+        for (int i = 0; i < NQ; ++i) {
+            q[i] = step ? fmaf(al, dj[i], xj[i]) : xj[i];
+            qd[i] = step ? fmaf(al, dj[NQ + i], xj[NQ + i]) : xj[NQ + i];
         }
-        if (lane < 3) sm.goal[lane] = goal[(size_t)6 * j + lane];
-        __syncwarp();
-        // sin, cos of every joint at every step size, once (lane = (step size, joint))
-        for (int t = lane; t < n_alpha * NQ; t += 32) {
-            const int a = t / NQ, i = t - NQ * a;
-            sincosf(fmaf(alpha_of(a, n_alpha), sm.d[i], sm.x[i]), &sm.trig[a].s[i], &sm.trig[a].c[i]);
-        }
-        __syncwarp();
-
+        JointTrig t;
+        joint_trig(q, t);
+        // tracking cost
+        float J = 0.f;
+#pragma unroll
+        for (int i = 0; i < NQ; ++i) J += 0.5f * (P.qd_cost * qd[i] * qd[i]);
+        float dsum = 0.f;
         if (!last) {
-            // mass-matrix columns (m < 7) and bias force (m == 7) per step size
-            const int rounds = (n_alpha * 8 + 31) / 32;
-            for (int rd = 0; rd < rounds; ++rd) {
-                const int a = 4 * rd + (lane >> 3), m = lane & 7;
-                const int aa = (a < n_alpha) ? a : 0;
-                const float al = alpha_of(aa, n_alpha);
-                float qd[NQ], qdd[NQ], tau[NQ];
+            float u[NC];
 #pragma unroll
-                for (int i = 0; i < NQ; ++i) {
-                    qd[i] = (m == 7) ? fmaf(al, sm.d[NQ + i], sm.x[NQ + i]) : 0.f;
-                    qdd[i] = (m == i) ? 1.f : 0.f;
-                }
-                const JointTrig t = sm.trig[aa];
-                rnea<false>(t, qd, qdd, -1, -1, tau, nullptr);
-                if (a < n_alpha) {
-                    if (m < 7) {
-#pragma unroll
-                        for (int r = 0; r < NQ; ++r) sm.M[a][NQ * m + r] = tau[r];
-                    } else {
-#pragma unroll
-                        for (int r = 0; r < NQ; ++r) sm.cb[a][r] = tau[r];
-                    }
-                }
+            for (int i = 0; i < NC; ++i) {
+                u[i] = step ? fmaf(al, dj[NS + i], xj[NS + i]) : xj[NS + i];
+                J += 0.5f * (P.r_cost * u[i] * u[i]);
             }
-            __syncwarp();
-            // qdd_a = M_a^{-1} (u_a - c_a): Gauss-Jordan on [M_a | u_a - c_a] by lane groups of 8
-            // (lane 8 g + i holds column i), four step sizes per round
-            for (int rd = 0; rd < rounds; ++rd) {
-                const int a = 4 * rd + (lane >> 3), m = lane & 7;
-                const int aa = (a < n_alpha) ? a : 0;
-                const float al = alpha_of(aa, n_alpha);
-                double col[NQ];
+            // defect: q'' = M^{-1} (u - c) of the candidate, one integrator step, against x_{k+1}
+            float M[28];
+            mass_matrix_lane(t, M);
+            float zero[NQ], c[NQ];
 #pragma unroll
-                for (int r = 0; r < NQ; ++r)
-                    col[r] = (m < NQ) ? 0.5 * ((double)sm.M[aa][NQ * m + r] + (double)sm.M[aa][NQ * r + m])
-                                      : (double)fmaf(al, sm.d[NS + r], sm.x[NS + r]) - (double)sm.cb[aa][r];
-                gj7_group(col, lane & ~7);
-                if (m == NQ && a < n_alpha) {
+            for (int i = 0; i < NQ; ++i) zero[i] = 0.f;
+            rnea<false>(t, qd, zero, -1, -1, c, nullptr);
+            double rhs[NQ], qdd[NQ];
 #pragma unroll
-                    for (int r = 0; r < NQ; ++r) sm.qdd[a][r] = col[r];
-                }
-            }
-            __syncwarp();
-        }
-        if (lane < n_alpha) {
-            // defect ||x_{k+1} - f(x_k, u_k)||_1 at xu + alpha dz (integrator.cuh:187-219)
-            const int a = lane;
-            const float al = alpha_of(a, n_alpha);
-            float dsum = 0.f;
-            if (!last) {
-                const double *qdd = sm.qdd[a];
-#pragma unroll
-                for (int i = 0; i < NQ; ++i) {
-                    const float q = fmaf(al, sm.d[i], sm.x[i]), qd = fmaf(al, sm.d[NQ + i], sm.x[NQ + i]);
-                    const float qn = fmaf(al, sm.d[NX + i], sm.x[NX + i]);
-                    const float qdn = fmaf(al, sm.d[NX + NQ + i], sm.x[NX + NQ + i]);
-                    float nq, nqd;
-                    if (P.integrator == 0) {
-                        nq = q + P.dt * qd;
-                        nqd = qd + P.dt * (float)qdd[i];
-                    } else {
-                        nqd = qd + P.dt * (float)qdd[i];
-                        nq = q + P.dt * nqd;
-                    }
-                    dsum += fabsf(qn - nq) + fabsf(qdn - nqd);
-                }
-            } else if (n_alpha > 1) {
-                const int j0 = j - k;
-#pragma unroll
-                for (int i = 0; i < NS; ++i)
-                    dsum += fabsf(fmaf(al, dz[(size_t)NX * j0 + i], xu[(size_t)NX * j0 + i]) - xs[(size_t)NS * b + i]);
-            }
-            sm.defect[a] = dsum;
-        } else if (lane >= 16 && lane < 16 + n_alpha) {
-            // tracking cost (iiwa_eepos_plant.cuh:240-290)
-            const int a = lane - 16;
-            const float al = alpha_of(a, n_alpha);
-            float p[3];
-            float J = 0.f;
+            for (int i = 0; i < NQ; ++i) rhs[i] = (double)u[i] - (double)c[i];
+            spd7_solve_lane(M, rhs, qdd);
 #pragma unroll
             for (int i = 0; i < NQ; ++i) {
-                const float qd = fmaf(al, sm.d[NQ + i], sm.x[NQ + i]);
-                J += 0.5f * (P.qd_cost * qd * qd);
-            }
-            if (!last) {
-#pragma unroll
-                for (int i = 0; i < NC; ++i) {
-                    const float u = fmaf(al, sm.d[NS + i], sm.x[NS + i]);
-                    J += 0.5f * (P.r_cost * u * u);
+                const float qn = step ? fmaf(al, dj[NX + i], xj[NX + i]) : xj[NX + i];
+                const float qdn = step ? fmaf(al, dj[NX + NQ + i], xj[NX + NQ + i]) : xj[NX + NQ + i];
+                float nq, nqd;
+                if (P.integrator == 0) {
+                    nq = q[i] + P.dt * qd[i];
+                    nqd = qd[i] + P.dt * (float)qdd[i];
+                } else {
+                    nqd = qd[i] + P.dt * (float)qdd[i];
+                    nq = q[i] + P.dt * nqd;
                 }
+                dsum += fabsf(qn - nq) + fabsf(qdn - nqd);
             }
-            const JointTrig t = sm.trig[a];
-            fk_lane<false>(t, p, nullptr);
+        } else if (step) {
+            const int jf = j - k;
 #pragma unroll
-            for (int d = 0; d < 3; ++d) {
-                const float e = p[d] - sm.goal[d];
-                J += 0.5f * P.q_ee * e * e;
-            }
-            sm.cost[a] = J;
+            for (int i = 0; i < NS; ++i)
+                dsum += fabsf(fmaf(al, dz[(size_t)NX * jf + i], xu[(size_t)NX * jf + i]) - xs[(size_t)NS * b + i]);
         }
-        __syncwarp();
-        if (lane < n_alpha) knot_merit[(size_t)NUM_ALPHAS * j + lane] = sm.cost[lane] + P.mu * sm.defect[lane];
-        __syncwarp();
+        float p[3];
+        fk_lane<false>(t, p, nullptr);
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            const float e = p[d] - goal[(size_t)6 * j + d];
+            J += 0.5f * P.q_ee * e * e;
+        }
+        knot_merit[(size_t)NUM_ALPHAS * j + a] = J + P.mu * dsum;
     }
 }
 
@@ -288,7 +231,9 @@ cudaError_t launch_merit(const BatchView &bv, const ProblemParams &P, int n_alph
                          int ctas_per_sm)
 {
     if (bv.total_knots <= 0) return cudaSuccess;
-    int blocks = (bv.total_knots + MERIT_WARPS - 1) / MERIT_WARPS;
+    const int kpw = n_alpha > 1 ? 32 / NUM_ALPHAS : 32;
+    const int warps = (bv.total_knots + kpw - 1) / kpw;
+    int blocks = (warps + MERIT_WARPS - 1) / MERIT_WARPS;
     if (blocks > num_sms * ctas_per_sm) blocks = num_sms * ctas_per_sm;
     merit_kernel<<<blocks, 32 * MERIT_WARPS, 0, s>>>(bv, P, n_alpha, xu, dz, goal, xs, knot_merit);
     return cudaGetLastError();
