@@ -1727,10 +1727,35 @@ constexpr int QW_STRIDE = 2 * SS;  // workspace doubles per knot
 constexpr int QW_SPIKE = SS;       // F_k (full 14 x 14) at this offset of a middle part's knot
 constexpr int QSP = 3 * SS;        // per middle part: F, X = D^{-1} F, Acc
 
+// The backward solve sweep stages each step's packed inverse factor (106 doubles, read as 53 16-byte
+// chunks; the last double is the knot's first lambda entry) and coupling block (196 entries of S) into
+// shared memory by cp.async, QSTAGE slots per warp (two steps ahead), in the factorisation's scratch.
+constexpr int QSTAGE = 3, QINV_D = 106, QSLOT = QINV_D + SS;
+constexpr int QREGION = QUAD_NWARP * PAIR_FWARP > QUAD_NWARP * QSTAGE * QSLOT ? QUAD_NWARP * PAIR_FWARP
+                                                                               : QUAD_NWARP * QSTAGE * QSLOT;
 __host__ __device__ constexpr int quad_smem_doubles(int n)
 {
-    return NS * n + QUAD_NWARP * PAIR_FWARP + (QUAD_NWARP - 2) * QSP + (QUAD_NWARP - 1) * 2 * NS +
-           2 * QUAD_NWARP * 3 + QUAD_NWARP + 2;
+    return NS * n + QREGION + (QUAD_NWARP - 2) * QSP + (QUAD_NWARP - 1) * 2 * NS + 2 * QUAD_NWARP * 3 +
+           QUAD_NWARP + QUAD_NWARP * NS + 2;
+}
+
+__device__ __forceinline__ void cp_async16(void *sdst, const void *gsrc)
+{
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((uint32_t)__cvta_generic_to_shared(sdst)),
+                 "l"(gsrc)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait()
+{
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+// the lanes of a warp copy `chunks` 16-byte chunks (both addresses 16-byte aligned)
+__device__ __forceinline__ void warp_cp_async(void *sdst, const void *gsrc, int chunks, int lane)
+{
+    for (int i = lane; i < chunks; i += 32)
+        cp_async16(reinterpret_cast<char *>(sdst) + 16 * i, reinterpret_cast<const char *>(gsrc) + 16 * i);
 }
 size_t pcg_quad_smem_bytes(int n) { return sizeof(double) * (size_t)quad_smem_doubles(n); }
 
@@ -1779,11 +1804,13 @@ __global__ void __launch_bounds__(QUAD_THREADS, 4)
 
     extern __shared__ double quad_dyn_smem[];
     double *xv = quad_dyn_smem;                       // 14 n: y, then t (forward), then x (backward)
-    double *fwall = xv + nv;                          // per warp: inverse factor (full), coupling, A_k, product
-    double *spall = fwall + QUAD_NWARP * PAIR_FWARP;  // middle parts 1, 2: F, X = D^{-1} F, Acc
+    double *fwall = xv + nv;                          // per warp: inverse factor (full), coupling, A_k, product;
+                                                      // the backward sweep's staging slots
+    double *spall = fwall + QREGION;                  // middle parts 1, 2: F, X = D^{-1} F, Acc
     double *sacc = spall + (QUAD_NWARP - 2) * QSP;    // per separator: right-hand-side pushes from left, right
     double *red = sacc + (QUAD_NWARP - 1) * 2 * NS;   // 2 sets x 4 warps x 3
     double *ginit = red + 2 * QUAD_NWARP * 3;         // gamma . gamma per warp
+    double *scw = ginit + QUAD_NWARP;                 // per warp: 14 doubles of the backward sweep
 
     const ST *Sb = S + kg0 * ks;
     double *wsb = ws + kg0 * QW_STRIDE;
@@ -1843,36 +1870,24 @@ __global__ void __launch_bounds__(QUAD_THREADS, 4)
         const double gv = gam(e);
         wsv(PW_RES, e) = gv;
         wsv(PW_LAM, e) = 0.0;
+        xv[e] = gv;  // y of the first preconditioner solve, M x = r_0
         g2acc = fma(gv, gv, g2acc);
     }
     const int r = c;
     const bool rv = cval;
-    // (S v)_k row r on the lane pair (r, hh): left, diagonal and right blocks, columns 7 hh .. 7 hh + 6
-    // (FP64 accumulation; the pair's halves summed by a shuffle)
-    auto row_block = [&](int k, const double *v) -> double {
-        const ST *row = Sb + (size_t)k * ks;
-        const bool hl = k > 0, hr = k < n - 1;
+    // row r of a 14 x 14 block in shared memory (column-major) times v, on the lane pair (r, hh)
+    auto blk_row_dot = [&](const double *Mb, const double *v) -> double {
         double acc = 0.0;
-        if (rv) {
-            ST fl[7], fd[7], fr[7];
 #pragma unroll
-            for (int q = 0; q < 7; ++q) {
-                const int cc = 7 * hh + q;
-                fl[q] = hl ? __ldg(row + r + NS * cc) : (ST)0;
-                fd[q] = __ldg(row + PK_DIAG + tri_lo(r, cc));
-                fr[q] = hr ? __ldg(row + ks + cc + NS * r) : (ST)0;
-            }
-#pragma unroll
-            for (int q = 0; q < 7; ++q) {
-                const int cc = 7 * hh + q;
-                if (hl) acc = fma((double)fl[q], v[NS * (k - 1) + cc], acc);
-                acc = fma((double)fd[q], v[NS * k + cc], acc);
-                if (hr) acc = fma((double)fr[q], v[NS * (k + 1) + cc], acc);
-            }
-        }
+        for (int q = 0; q < 7; ++q) acc = fma(Mb[r + NS * (7 * hh + q)], v[7 * hh + q], acc);
         return acc + __shfl_xor_sync(0xffffffffu, acc, 1);
     };
-    // ---- factorisation of the parts: warp w walks part w (top-down, or bottom-up for the last part)
+    __syncthreads();
+    // ---- factorisation of the parts: warp w walks part w (top-down, or bottom-up for the last part).
+    // The forward half of the first preconditioner solve runs in the same walk: after knot k's inverse
+    // factor, t_k = D_k^{-1} y_k, and the next step pushes its coupling times t_k onto y (or, after the
+    // part's last knot, onto the separator's right-hand side); a middle part accumulates -F_k^T t_k for
+    // its left separator.  r_0 = gamma is known before the factorisation (the iteration starts from 0).
     if (warp < P) {
         const int w = warp;
         const bool top = (w < P - 1) || (P == 1);
@@ -1885,6 +1900,8 @@ __global__ void __launch_bounds__(QUAD_THREADS, 4)
         double *Fsp = spk ? spall + (w - 1) * QSP : nullptr;
         double *Xb = spk ? Fsp + SS : nullptr, *Acc = spk ? Fsp + 2 * SS : nullptr;
         const int k0 = top ? pa : pb, dir = top ? 1 : -1, lofs = top ? 0 : 1;
+        const int sep_slot = top ? 2 * w : 2 * (P - 2) + 1;  // this part's push onto its separator
+        double accv = 0.0;                                   // -F_k^T t_k summed (middle part), this lane's half
         double pd[4] = {0.0, 0.0, 0.0, 0.0}, pl[7] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
         if (len > 0) warp_fetch<ST, 4>(Sb + (size_t)k0 * ks + PK_DIAG, 105, lane, pd);
         if (spk) {
@@ -1944,6 +1961,13 @@ __global__ void __launch_bounds__(QUAD_THREADS, 4)
                 __syncwarp();
                 warp_dmma_store(cd, [&](int i, int j, double v) { if (i < NS && j < NS) Wb[i + NS * j] = v; }, lane);
                 __syncwarp();
+                // forward solve: the previous knot's t through the coupling block Lw
+                const double u = blk_row_dot(Lw, xv + NS * (k - dir));
+                if (hh == 0 && rv) {
+                    if (sep_step) sacc[sep_slot * NS + r] = u;
+                    else xv[NS * k + r] += u;
+                }
+                __syncwarp();
             }
             if (sep_step) break;  // Wb: the separator's update; Fsp (middle part): E^ = M_{s_w, s_{w-1}}
             double a[7];
@@ -1952,6 +1976,18 @@ __global__ void __launch_bounds__(QUAD_THREADS, 4)
                 a[q] = Ap[tri_lo(7 * hh + q, cq)] - (st > 0 ? Wb[7 * hh + q + NS * cq] : 0.0);
             pair_gj_inverse(a, c, hh);
             keep_inv(Fi, a, k);
+            {
+                const double t = pair_dot7(a, xv + NS * k, hh);  // t_k = D_k^{-1} y_k (D_k^{-1} symmetric)
+                __syncwarp();
+                if (hh == 0 && rv) xv[NS * k + r] = t;
+                __syncwarp();
+                if (spk) {
+                    double pf = 0.0;
+#pragma unroll
+                    for (int q = 0; q < 7; ++q) pf = fma(Fsp[7 * hh + q + NS * r], xv[NS * k + 7 * hh + q], pf);
+                    accv -= pf;
+                }
+            }
             if (spk) {
                 double *fg = wsb + (size_t)k * QW_STRIDE + QW_SPIKE;
                 for (int e = lane; e < SS; e += 32) fg[e] = Fsp[e];
@@ -1959,6 +1995,11 @@ __global__ void __launch_bounds__(QUAD_THREADS, 4)
                 blk_mm<true, false, true>(Fsp, Xb, Acc, lane);   // Acc += F_k^T X_k
             }
         }
+        if (spk) {
+            accv += __shfl_xor_sync(0xffffffffu, accv, 1);
+            if (hh == 0 && rv) sacc[(2 * (w - 1) + 1) * NS + r] = accv;
+        }
+        if (len == 0 && has_sep && lane < NS) sacc[sep_slot * NS + lane] = 0.0;
     }
     {
         const double g2 = warp_sum(g2acc);
@@ -2034,9 +2075,10 @@ __global__ void __launch_bounds__(QUAD_THREADS, 4)
         }
         if (lane < F_LINES && kf >= 0 && kf < n) asm volatile("prefetch.global.L2 [%0];" ::"l"(pf + 128 * lane));
     };
-    auto solve = [&]() {
+    // fwd: run the forward half (false when the factorisation's walk already ran it)
+    auto solve = [&](bool fwd) {
         // forward through every part: t_k = D_k^{-1} y_k overwrites y_k
-        if (warp < P) {
+        if (fwd && warp < P) {
             const int w = warp;
             const bool top = (w < P - 1) || (P == 1);
             const bool spk = top && w > 0;
@@ -2140,51 +2182,75 @@ __global__ void __launch_bounds__(QUAD_THREADS, 4)
             }
         }
         __syncthreads();
-        // backward through every part: x_k = t_k + D_k^{-1} (coupling to the knots after it)
+        // backward through every part: x_k = t_k + D_k^{-1} (coupling to the knots after it).  Step i of a
+        // part (knot pb - i top-down, pa + i bottom-up) reads its inverse factor and coupling block from
+        // a shared-memory slot filled by cp.async two steps earlier
         if (warp < P) {
             const int w = warp;
             const bool top = (w < P - 1) || (P == 1);
             const bool spk = top && w > 0;
             const bool has_sep = top ? (w < P - 1) : true;
             const int pa = lay.a[w], pb = lay.b[w];
-            double *sc = fwall + w * PAIR_FWARP + PF_L;
-            if (top) {
-                for (int k = pb; k >= pa; --k) {
-                    double dc[7], lc[7], fc[7];
-                    const int kn0 = k < pb ? k + 1 : (has_sep ? lay.s[w] : -1);
-                    ld_inv(k, dc);
-                    if (kn0 >= 0) ld_left(kn0, true, lc);
-                    if (spk) ld_spike(k, false, fc);
-                    l2_pf(k - QPF >= pa ? k - QPF : -1, k - QPF + 1 >= pa ? k - QPF + 1 : -1,
-                          spk && k - QPF >= pa ? k - QPF : -1);
-                    const int kn = k < pb ? k + 1 : (has_sep ? lay.s[w] : -1);
-                    double v = kn >= 0 ? pair_dot7(lc, xv + NS * kn, hh) : 0.0;  // L_{k+1}^T x_{k+1}
+            const int len = pb >= pa ? pb - pa + 1 : 0;
+            double *sc = scw + w * NS;
+            double *stg = fwall + w * QSTAGE * QSLOT;
+            constexpr int LEFT_CHUNKS = SS * (int)sizeof(ST) / 16;
+            auto knot_of = [&](int i) { return top ? pb - i : pa + i; };
+            // the row whose left block step i needs (top-down: L_{k+1}, or the separator's; bottom-up: L_k)
+            auto cpl_of = [&](int i) {
+                const int k = knot_of(i);
+                return top ? (k < pb ? k + 1 : (has_sep ? lay.s[w] : -1)) : k;
+            };
+            auto stage = [&](int i) {
+                if (i < len) {
+                    double *sl = stg + (i % QSTAGE) * QSLOT;
+                    const int kl = cpl_of(i);
+                    warp_cp_async(sl, wsb + (size_t)knot_of(i) * QW_STRIDE + PW_INV, QINV_D / 2, lane);
+                    if (kl >= 0) warp_cp_async(sl + QINV_D, Sb + (size_t)kl * ks, LEFT_CHUNKS, lane);
+                }
+                cp_async_commit();
+            };
+            stage(0);
+            stage(1);
+            double fcn[7];  // middle part: row r of F_k of the next step (the term -F_k x_{s_{w-1}})
+            if (spk && len > 0) ld_spike(knot_of(0), false, fcn);
+            for (int i = 0; i < len; ++i) {
+                stage(i + 2);
+                {
+                    const int ip = i + QPF < len ? i + QPF : -1, kp = ip >= 0 ? knot_of(ip) : -1;
+                    l2_pf(kp, ip >= 0 ? cpl_of(ip) : -1, spk ? kp : -1);
+                }
+                cp_async_wait<QSTAGE - 1>();
+                __syncwarp();
+                const int k = knot_of(i), kl = cpl_of(i);
+                const double *sl = stg + (i % QSTAGE) * QSLOT;
+                const ST *sleft = reinterpret_cast<const ST *>(sl + QINV_D);
+                double dc[7], lc[7];
+#pragma unroll
+                for (int q = 0; q < 7; ++q) {
+                    dc[q] = rv ? sl[tri_lo(r, 7 * hh + q)] : 0.0;
+                    lc[q] = (rv && kl >= 0) ? (double)sleft[top ? 7 * hh + q + NS * r : r + NS * (7 * hh + q)] : 0.0;
+                }
+                double v = 0.0;
+                if (top) {
+                    if (kl >= 0) v = pair_dot7(lc, xv + NS * kl, hh);  // L_{k+1}^T x_{k+1}
                     if (spk) {
                         double p = 0.0;
 #pragma unroll
-                        for (int q2 = 0; q2 < 7; ++q2) p = fma(fc[q2], xv[NS * (pa - 1) + 7 * hh + q2], p);
+                        for (int q2 = 0; q2 < 7; ++q2) p = fma(fcn[q2], xv[NS * (pa - 1) + 7 * hh + q2], p);
                         v -= p + __shfl_xor_sync(0xffffffffu, p, 1);  // - F_k x_{s_{w-1}}
+                        if (i + 1 < len) ld_spike(knot_of(i + 1), false, fcn);
                     }
-                    if (hh == 0 && rv) sc[r] = v;
-                    __syncwarp();
-                    const double a = pair_dot7(dc, sc, hh);
-                    if (hh == 0 && rv) xv[NS * k + r] += a;
-                    __syncwarp();
+                } else {
+                    v = pair_dot7(lc, xv + NS * (k - 1), hh);  // L_k x_{k-1}
                 }
-            } else {
-                for (int k = pa; k <= pb; ++k) {
-                    double dc[7], lc[7];
-                    ld_inv(k, dc);
-                    ld_left(k, false, lc);
-                    l2_pf(k + QPF <= pb ? k + QPF : -1, k + QPF <= pb ? k + QPF : -1, -1);
-                    const double v = pair_dot7(lc, xv + NS * (k - 1), hh);
-                    if (hh == 0 && rv) sc[r] = v;
-                    __syncwarp();
-                    const double a = pair_dot7(dc, sc, hh);
-                    if (hh == 0 && rv) xv[NS * k + r] += a;
-                    __syncwarp();
-                }
+                if (hh == 0 && rv) sc[r] = v;
+                __syncwarp();
+                const double a = pair_dot7(dc, sc, hh);
+                if (hh == 0 && rv) xv[NS * k + r] += a;
+                __syncwarp();
             }
+            cp_async_wait<0>();
         }
         __syncthreads();
     };
@@ -2209,12 +2275,15 @@ __global__ void __launch_bounds__(QUAD_THREADS, 4)
         __syncthreads();
         for (int e = tid; e < nv; e += QUAD_THREADS) wsv(PW_RES, e) = gam(e) - srow(e, xv);
     };
-    // z = S^{-1} r = -x of M x = r (left in xv); d[1] += r.z, d[2] += r.r
-    auto precond = [&](double *d) {
-        __syncthreads();
-        for (int e = tid; e < nv; e += QUAD_THREADS) xv[e] = wsv(PW_RES, e);
-        __syncthreads();
-        solve();
+    // z = S^{-1} r = -x of M x = r (left in xv); d[1] += r.z, d[2] += r.r.  The first call finds the
+    // forward half done by the factorisation (y = r_0 = gamma)
+    auto precond = [&](double *d, bool first) {
+        if (!first) {
+            __syncthreads();
+            for (int e = tid; e < nv; e += QUAD_THREADS) xv[e] = wsv(PW_RES, e);
+            __syncthreads();
+        }
+        solve(!first);
         for (int e = tid; e < nv; e += QUAD_THREADS) {
             const double rr = wsv(PW_RES, e), z = -xv[e];
             d[1] += rr * z;
@@ -2238,7 +2307,7 @@ __global__ void __launch_bounds__(QUAD_THREADS, 4)
     bool conv, bad = false;
     {
         double acc3[3] = {0.0, 0.0, 0.0};
-        precond(acc3);
+        precond(acc3, true);
         block_sum(acc3, 3);
         eta = acc3[1];
         for (int e = tid; e < nv; e += QUAD_THREADS) wsv(PW_P, e) = -xv[e];  // p = z
@@ -2250,13 +2319,47 @@ __global__ void __launch_bounds__(QUAD_THREADS, 4)
         for (int e = tid; e < nv; e += QUAD_THREADS) xv[e] = wsv(PW_P, e);
         __syncthreads();
         double d1[1] = {0.0};
-        // S p: a knot per warp and step
-        for (int k = warp; k < n; k += QUAD_NWARP) {
-            const double v1 = row_block(k, xv);
-            if (hh == 0 && rv) {
-                wsb[(size_t)k * QW_STRIDE + PW_V + r] = v1;
-                d1[0] = fma(xv[NS * k + r], v1, d1[0]);
+        // S p: warp w takes the knots w n / 4 .. (w + 1) n / 4 - 1 in order; each row of S (the left block
+        // and the diagonal triangle) is staged in shared memory by cp.async, the next two rows in flight
+        {
+            const int kb = (warp * n) / QUAD_NWARP, ke = ((warp + 1) * n) / QUAD_NWARP;
+            double *stg = fwall + warp * QSTAGE * QSLOT;
+            constexpr int ROW_CHUNKS = (PK_DIAG + 105) * (int)sizeof(ST) / 16 + 1;  // left + triangle, rounded up
+            static_assert(ROW_CHUNKS * 16 <= QSLOT * 8 && ROW_CHUNKS * 16 <= (FMT == 2 ? PK64 * 8 : PK * 4),
+                          "a staged row fits its slot and its row of S");
+            auto stage = [&](int i) {
+                if (kb + i < n && i <= ke - kb) warp_cp_async(stg + (i % QSTAGE) * QSLOT, Sb + (size_t)(kb + i) * ks,
+                                                             ROW_CHUNKS, lane);
+                cp_async_commit();
+            };
+            stage(0);
+            stage(1);
+            for (int i = 0; i < ke - kb; ++i) {
+                stage(i + 2);
+                cp_async_wait<QSTAGE - 2>();  // the rows of knots k and k + 1 have landed
+                __syncwarp();
+                const int k = kb + i;
+                const ST *row = reinterpret_cast<const ST *>(stg + (i % QSTAGE) * QSLOT);
+                const ST *nxt = reinterpret_cast<const ST *>(stg + ((i + 1) % QSTAGE) * QSLOT);
+                const bool hl = k > 0, hr = k < n - 1;
+                double acc = 0.0;
+                if (rv) {
+#pragma unroll
+                    for (int q = 0; q < 7; ++q) {
+                        const int cc = 7 * hh + q;
+                        if (hl) acc = fma((double)row[r + NS * cc], xv[NS * (k - 1) + cc], acc);
+                        acc = fma((double)row[PK_DIAG + tri_lo(r, cc)], xv[NS * k + cc], acc);
+                        if (hr) acc = fma((double)nxt[cc + NS * r], xv[NS * (k + 1) + cc], acc);
+                    }
+                }
+                const double v1 = acc + __shfl_xor_sync(0xffffffffu, acc, 1);
+                if (hh == 0 && rv) {
+                    wsb[(size_t)k * QW_STRIDE + PW_V + r] = v1;
+                    d1[0] = fma(xv[NS * k + r], v1, d1[0]);
+                }
+                __syncwarp();
             }
+            cp_async_wait<0>();
         }
         block_sum(d1, 1);
         const double alpha = eta / d1[0];
@@ -2300,7 +2403,7 @@ __global__ void __launch_bounds__(QUAD_THREADS, 4)
             }
         }
         double d2[3] = {0.0, 0.0, 0.0};
-        precond(d2);
+        precond(d2, false);
         block_sum(d2, 3);
         if (exit_mode != 0) conv = converged(d2[1], d2[2]);
         if (!isfinite(d2[1])) {
