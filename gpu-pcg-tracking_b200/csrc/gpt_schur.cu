@@ -328,15 +328,18 @@ __device__ __forceinline__ bool warp_inverse64(const float *A, double shift, dou
 // without pivoting never mixes the two blocks of a block-diagonal matrix (every update it would
 // make across them multiplies an exact zero), so this is the same arithmetic as the full 14x14
 // elimination, result for result; any other Q takes the full elimination.
+// *blockdiag (optional) tells which path ran: true when the inverse has that block-diagonal zero pattern.
 __device__ __forceinline__ bool warp_inverse64_state(const float *Q, double shift, double *Ainv, int lane,
-                                                     float *Ainv32, double *Ainv64g)
+                                                     float *Ainv32, double *Ainv64g, bool *blockdiag = nullptr)
 {
     bool ok = true;
     for (int e = lane; e < SS; e += 32) {
         const int r = e % NS, cc = e / NS;
         if (((r < NC) != (cc < NC)) || (r >= NC && cc >= NC && r != cc)) ok = ok && (Q[e] == 0.f);
     }
-    if (!__all_sync(0xffffffffu, ok)) return warp_inverse64<NS>(Q, shift, Ainv, lane, Ainv32, Ainv64g);
+    const bool bd = __all_sync(0xffffffffu, ok);
+    if (blockdiag) *blockdiag = bd;
+    if (!bd) return warp_inverse64<NS>(Q, shift, Ainv, lane, Ainv32, Ainv64g);
     bool piv_ok = warp_inverse64<NC, NS>(Q, shift, Ainv, lane, Ainv32, Ainv64g);
     for (int e = lane; e < SS; e += 32) {
         const int r = e % NS, cc = e / NS;
@@ -355,13 +358,16 @@ __device__ __forceinline__ bool warp_inverse64_state(const float *Q, double shif
 }
 // (R + shift I)^{-1} of a 7x7 control block: reciprocals when R is diagonal (kkt_kernel's R_COST I;
 // the same arithmetic as the elimination), else Gauss-Jordan
+// *diagonal (optional): true when R was diagonal (and so is the inverse).
 __device__ __forceinline__ bool warp_inverse64_control(const float *R, double shift, double *Ainv, int lane,
-                                                       float *Ainv32, double *Ainv64g)
+                                                       float *Ainv32, double *Ainv64g, bool *diagonal = nullptr)
 {
     bool ok = true;
     for (int e = lane; e < CC; e += 32)
         if (e % NC != e / NC) ok = ok && (R[e] == 0.f);
-    if (!__all_sync(0xffffffffu, ok)) return warp_inverse64<NC>(R, shift, Ainv, lane, Ainv32, Ainv64g);
+    const bool dg = __all_sync(0xffffffffu, ok);
+    if (diagonal) *diagonal = dg;
+    if (!dg) return warp_inverse64<NC>(R, shift, Ainv, lane, Ainv32, Ainv64g);
     bool piv_ok = true;
     for (int e = lane; e < CC; e += 32) {
         double v = 0.0;
@@ -405,8 +411,9 @@ __global__ void __launch_bounds__(32 * SCHUR_WARPS, 5)
     const int chunk = (bv.total_knots + nw - 1) / nw;
     const int jbeg = bv.j0 + gw * chunk;
     const int jend = min(jbeg + chunk, bv.j0 + bv.total_knots);
-    int have = -1;  // knot whose inverse sm.Qinv[cur] holds
+    int have = -1;         // knot whose inverse sm.Qinv[cur] holds
     int cur = 0;
+    bool have_bd = false;  // that inverse is block diagonal (position block, diagonal velocity block)
     for (int j = jbeg; j < jend; ++j) {
         const int b = bv.inst(j);
         if (!bv.active(b)) {
@@ -426,7 +433,7 @@ __global__ void __launch_bounds__(32 * SCHUR_WARPS, 5)
             __syncwarp();
             const bool ok0 = warp_inverse64_state(sm.Gk, rho, Q0i, lane,
                                                   (N == 1 && Ginv) ? Ginv + (size_t)G_STRIDE * j : nullptr,
-                                                  N == 1 ? Ginv64 + (size_t)G_STRIDE * j : nullptr);
+                                                  N == 1 ? Ginv64 + (size_t)G_STRIDE * j : nullptr, &have_bd);
             if (!ok0 && lane == 0) atomicOr(&bv.st[b].exit_flags, GPT_EXIT_FACTOR);
             __syncwarp();
             if (lane < NS) {
@@ -485,7 +492,7 @@ __global__ void __launch_bounds__(32 * SCHUR_WARPS, 5)
         float *Gi32 = Ginv ? Ginv + (size_t)G_STRIDE * (j - 1) : nullptr;
         double *Gi64 = Ginv64 + (size_t)G_STRIDE * (j - 1);
         double *const Qki = sm.Qinv[cur], *const Qkp1i = sm.Qinv[cur ^ 1];
-        bool ok = true;
+        bool ok = true, bd_ki = have_bd, bd_kp1 = false, r_diag = false;
         if (have == j - 1) {
             // formed by this warp's previous row; its outputs for knot j - 1 are written here, as the
             // elimination below would
@@ -494,25 +501,46 @@ __global__ void __launch_bounds__(32 * SCHUR_WARPS, 5)
                 if (Gi32) Gi32[e] = (float)Qki[e];
             }
         } else {
-            ok = warp_inverse64_state(sm.Gm1, rho, Qki, lane, Gi32, Gi64);
+            ok = warp_inverse64_state(sm.Gm1, rho, Qki, lane, Gi32, Gi64, &bd_ki);
         }
         ok = warp_inverse64_state(sm.Gk, rho, Qkp1i, lane, (k == N - 1 && Ginv) ? Ginv + (size_t)G_STRIDE * j : nullptr,
-                                  k == N - 1 ? Ginv64 + (size_t)G_STRIDE * j : nullptr) && ok;
-        ok = warp_inverse64_control(sm.Gm1 + SS, rho, sm.Rki, lane, Gi32 ? Gi32 + SS : nullptr, Gi64 + SS) && ok;
+                                  k == N - 1 ? Ginv64 + (size_t)G_STRIDE * j : nullptr, &bd_kp1) && ok;
+        ok = warp_inverse64_control(sm.Gm1 + SS, rho, sm.Rki, lane, Gi32 ? Gi32 + SS : nullptr, Gi64 + SS, &r_diag) &&
+             ok;
         if (!ok && lane == 0) atomicOr(&bv.st[b].exit_flags, GPT_EXIT_FACTOR);
         __syncwarp();
         // the products on the FP64 tensor cores, 14x14 (14x7) blocks padded to 16x16 (16x8)
         const float *Am = sm.C, *Bm = sm.C + SS;  // -A, -B
         {
-            double cp[2][2][2] = {}, cb[2][1][2] = {};
-            warp_dmma<2, 2, 4>([&](int i, int k) { return (i < NS && k < NS) ? (double)Am[i + NS * k] : 0.0; },
-                               [&](int k, int j) { return (k < NS && j < NS) ? Qki[k + NS * j] : 0.0; }, cp,
-                               lane);  // phi = (-A) Qt^{-1}
-            warp_dmma<2, 1, 2>([&](int i, int k) { return (i < NS && k < NC) ? (double)Bm[i + NS * k] : 0.0; },
-                               [&](int k, int j) { return (k < NC && j < NC) ? sm.Rki[k + NC * j] : 0.0; }, cb,
-                               lane);  // (-B) Rt^{-1}
+            double cp[2][2][2] = {};
+            auto a_el = [&](int i, int k) { return (i < NS && k < NS) ? (double)Am[i + NS * k] : 0.0; };
+            auto q_el = [&](int k, int j) { return (k < NS && j < NS) ? Qki[k + NS * j] : 0.0; };
+            if (bd_ki) {
+                // block-diagonal Qt^{-1}: columns 0-7 draw only on k < 8, columns 8-15 only on k >= 8
+                // (every skipped product is an exact zero, so the sums are those of the full product)
+                const int g = lane >> 2, t = lane & 3;
+#pragma unroll
+                for (int kk = 0; kk < 4; ++kk) {
+                    const int kx = 4 * kk + t, J = kk < 2 ? 0 : 1;
+                    const double b = q_el(kx, 8 * J + g);
+#pragma unroll
+                    for (int I = 0; I < 2; ++I) mma884_f64(cp[I][J], a_el(8 * I + g, kx), b);
+                }
+            } else {
+                warp_dmma<2, 2, 4>(a_el, q_el, cp, lane);  // phi = (-A) Qt^{-1}
+            }
             warp_dmma_store(cp, [&](int i, int j, double v) { if (i < NS && j < NS) sm.phi[i + NS * j] = v; }, lane);
-            warp_dmma_store(cb, [&](int i, int j, double v) { if (i < NS && j < NC) sm.BRi[i + NS * j] = v; }, lane);
+            if (r_diag) {
+                // (-B) Rt^{-1} with a diagonal Rt^{-1}: a column scaling
+                for (int e = lane; e < SC; e += 32) sm.BRi[e] = (double)Bm[e] * sm.Rki[(e / NS) * (NC + 1)];
+            } else {
+                double cb[2][1][2] = {};
+                warp_dmma<2, 1, 2>([&](int i, int k) { return (i < NS && k < NC) ? (double)Bm[i + NS * k] : 0.0; },
+                                   [&](int k, int j) { return (k < NC && j < NC) ? sm.Rki[k + NC * j] : 0.0; }, cb,
+                                   lane);  // (-B) Rt^{-1}
+                warp_dmma_store(cb, [&](int i, int j, double v) { if (i < NS && j < NC) sm.BRi[i + NS * j] = v; },
+                                lane);
+            }
         }
         __syncwarp();
         {
@@ -545,6 +573,7 @@ __global__ void __launch_bounds__(32 * SCHUR_WARPS, 5)
         if (lane == 0) Pk[PK64 - 1] = 0.0;
         __syncwarp();
         have = j;  // (Q_k + rho I)^{-1} stays for row k + 1
+        have_bd = bd_kp1;
         cur ^= 1;
     }
 }
