@@ -43,7 +43,7 @@ PCG_BJ_BYTES_PER_KNOT = 4 * 784  # block-Jacobi kernel: FP32 S (588) + Pinv (196
 # the bench's batch, 512 instances x 128 knots (the working set of a launch, ~0.26 GB, exceeds the L2, so
 # the traffic per knot depends on the batch and is not scaled to other batches)
 PCG_DRAM_BYTES_PER_KNOT = {"pcg_pair_kernel": (779.677440e6 + 92.534528e6) / (512 * 128),
-                           "pcg_quad_kernel": (775.0e6 + 144.2e6) / (512 * 128)}
+                           "pcg_quad_kernel": (536.024320e6 + 146.112256e6) / (512 * 128)}
 PCG_DRAM_SOURCE = "ncu capture of the 512 x 128 bench batch, one launch"
 ALG_FLOATS_PER_KNOT_SQP = 4058   # every materialised SQP-iteration tensor written once, read once
 
