@@ -36,7 +36,7 @@ EXPORTED = [
     "gpt_form_kkt", "gpt_form_schur", "gpt_form_schur_csc", "gpt_prep_csr", "gpt_pcg", "gpt_compute_dz",
     "gpt_compute_merit", "gpt_ls_compute_merit", "gpt_set_profiling", "gpt_get_phase_stats",
     "gpt_ls_compute_merit_noalloc", "gpt_sqp_adjoint", "gpt_set_cost_weights", "gpt_autotune",
-    "gpt_default_track_config", "gpt_track", "gpt_track_batched", "gpt_simulate",
+    "gpt_default_track_config", "gpt_track", "gpt_track_batched", "gpt_track_batched_adjoint", "gpt_simulate",
     "gpt_end_effector_positions", "gpt_forward_dynamics", "gpt_read_csv", "gpt_form_ss",
     "gpt_forward_dynamics_gradient", "gpt_sqp_solve_batched_trace",
 ]
@@ -175,6 +175,8 @@ def _declare(L):
         "gpt_default_track_config": ([P(TrackConfig)], None),
         "gpt_track": ([vp, u32, u32, vp, vp, vp, P(TrackConfig), vp, vp, u32, P(TrackStats), vp], C.c_int),
         "gpt_track_batched": ([vp, u32, vp, vp, vp, vp, vp, P(TrackConfig), vp, vp, u32, vp, vp], C.c_int),
+        "gpt_track_batched_adjoint": ([vp, u32, vp, vp, vp, vp, vp, P(TrackConfig), vp, vp, u32, vp, vp, vp, vp, vp],
+                                      C.c_int),
         "gpt_simulate": ([vp, u32, vp, vp, C.c_double, C.c_double, f32, vp], C.c_int),
         "gpt_end_effector_positions": ([u32, vp, u32, vp, vp], C.c_int),
         "gpt_forward_dynamics": ([u32, vp, u32, vp, vp], C.c_int),
@@ -460,6 +462,29 @@ class Solver:
                                        _ptr(errors), _ptr(sqp_iters_log), log_capacity, C.cast(sts, C.c_void_p),
                                        _stream(stream)))
         return errors, StatsList(sts)
+
+    def track_batched_adjoint(self, knot_points: Sequence[int], traj_steps: Sequence[int], eePos_traj, xu_traj, xs,
+                              config: Optional[TrackConfig] = None, errors=None, sqp_iters_log=None, log_capacity=0,
+                              stream=None):
+        """gpt_track_batched_adjoint: gpt_track_batched plus, after every control update's solve, the
+        one-step adjoint of that update's horizon tracking loss; returns (errors, stats, weight_grad
+        [B, 15] = (dl/dqd, dl/dr, dl/dq_ee) summed over each instance's updates, loss [B], adjoint
+        failures per instance)."""
+        import torch
+        B = len(knot_points)
+        Ns = (C.c_uint32 * B)(*knot_points)
+        Ss = (C.c_uint32 * B)(*traj_steps)
+        if errors is None:
+            errors = torch.zeros(int(sum(traj_steps)), device=xs.device)
+        wgrad = torch.zeros(B, 15, device=xs.device)
+        loss = torch.zeros(B, device=xs.device)
+        fails = (C.c_uint32 * B)()
+        sts = (TrackStats * B)()
+        _check(lib().gpt_track_batched_adjoint(
+            self._h, B, C.cast(Ns, C.c_void_p), C.cast(Ss, C.c_void_p), _ptr(eePos_traj), _ptr(xu_traj), _ptr(xs),
+            None if config is None else C.byref(config), _ptr(errors), _ptr(sqp_iters_log), log_capacity,
+            _ptr(wgrad), _ptr(loss), C.cast(fails, C.c_void_p), C.cast(sts, C.c_void_p), _stream(stream)))
+        return errors, StatsList(sts), wgrad, loss, list(fails)
 
     def simulate(self, knot_points: int, xs, xu, time_offset_us: float, sim_time_us: float, sim_step: float = 2e-4,
                  stream=None):

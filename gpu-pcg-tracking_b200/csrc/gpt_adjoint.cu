@@ -193,8 +193,9 @@ __global__ void __launch_bounds__(32 * ADJ_WARPS)
 }
 
 // per instance: fixed-order FP64 sums of the per-knot partials (knots 0..N-2)
+// (wacc: added to wacc[15 b + t] instead)
 __global__ void adjoint_reduce_kernel(BatchView bv, const float *__restrict__ part, float *__restrict__ grad_qd,
-                                      float *__restrict__ grad_r, float *__restrict__ grad_qee)
+                                      float *__restrict__ grad_r, float *__restrict__ grad_qee, float *__restrict__ wacc)
 {
     const int b = bv.b0 + (int)blockIdx.x;
     if (b >= bv.b0 + bv.B || !bv.active(b)) return;
@@ -203,7 +204,8 @@ __global__ void adjoint_reduce_kernel(BatchView bv, const float *__restrict__ pa
     const int N = bv.N(b), kb = bv.off(b);
     double a = 0.0;
     for (int k = 0; k < N - 1; ++k) a += (double)part[(size_t)ADJ_PART * (kb + k) + t];
-    if (t < NQ) grad_qd[(size_t)NQ * b + t] = (float)a;
+    if (wacc) wacc[(size_t)15 * b + t] += (float)a;
+    else if (t < NQ) grad_qd[(size_t)NQ * b + t] = (float)a;
     else if (t < NQ + NC) grad_r[(size_t)NC * b + t - NQ] = (float)a;
     else grad_qee[b] = (float)a;
 }
@@ -218,7 +220,7 @@ __global__ void axpy_kernel(int n, float alpha, const float *__restrict__ x, con
 
 cudaError_t launch_adjoint_grad(const BatchView &bv, const ProblemParams &P, const float *xu, const float *goal,
                                 const float *dz, const float *mu, float *grad_goal, float *part, float *grad_qd,
-                                float *grad_r, float *grad_qee, int num_sms, cudaStream_t s)
+                                float *grad_r, float *grad_qee, int num_sms, cudaStream_t s, float *wacc)
 {
     if (bv.total_knots <= 0) return cudaSuccess;
     int blocks = (bv.total_knots + ADJ_WARPS - 1) / ADJ_WARPS;
@@ -226,7 +228,7 @@ cudaError_t launch_adjoint_grad(const BatchView &bv, const ProblemParams &P, con
     adjoint_grad_kernel<<<blocks, 32 * ADJ_WARPS, 0, s>>>(bv, P, xu, goal, dz, mu, grad_goal, part);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    adjoint_reduce_kernel<<<bv.B, 32, 0, s>>>(bv, part, grad_qd, grad_r, grad_qee);
+    adjoint_reduce_kernel<<<bv.B, 32, 0, s>>>(bv, part, grad_qd, grad_r, grad_qee, wacc);
     return cudaGetLastError();
 }
 

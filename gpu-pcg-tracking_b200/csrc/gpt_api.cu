@@ -143,6 +143,9 @@ struct gpt_handle {
     int *trk_rows = nullptr;
     TrackClock *trk_clk = nullptr;
     TrackInst *trk_inst = nullptr;
+    InstState *trk_stbak = nullptr;  // per-solve state saved around an update's adjoint
+    float *trk_ggrad = nullptr;      // the adjoint's per-knot goal gradients (6 per knot)
+    float *trk_kloss = nullptr;      // the update's per-knot loss terms
     int *h_trk_rows = nullptr;
     TrackInst *h_trk_inst = nullptr;
     cudaStream_t cap_stream = nullptr, body_stream = nullptr;
@@ -385,6 +388,9 @@ gpt_status gpt_create(const gpt_problem_config *pc, const gpt_solver_config *sc,
     ALLOC(trk_rows, B + 1);
     ALLOC(trk_clk, 1);
     ALLOC(trk_inst, B);
+    ALLOC(trk_stbak, B);
+    ALLOC(trk_ggrad, 6 * T);
+    ALLOC(trk_kloss, T);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->cap_stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->body_stream, cudaStreamNonBlocking);
     for (int i = 1; i < MAX_BRANCHES; ++i) {
@@ -457,6 +463,7 @@ gpt_status gpt_destroy(gpt_handle *h)
     for (auto &ge : h->graphs) cudaGraphExecDestroy(ge.exec);
     cudaFree(h->gxu); cudaFree(h->glam); cudaFree(h->ggoal); cudaFree(h->d_iter);
     cudaFree(h->trk_xu_old); cudaFree(h->trk_rows); cudaFree(h->trk_clk); cudaFree(h->trk_inst);
+    cudaFree(h->trk_stbak); cudaFree(h->trk_ggrad); cudaFree(h->trk_kloss);
     cudaFreeHost(h->h_trk_rows); cudaFreeHost(h->h_trk_inst);
     cudaFreeHost(h->h_knot_off); cudaFreeHost(h->h_knot_inst);
     if (h->cap_stream) cudaStreamDestroy(h->cap_stream);
@@ -1353,14 +1360,65 @@ void gpt_default_track_config(gpt_track_config *o)
     o->rho_reset = 1e-3f;           // toplevel.cuh:579
 }
 
-gpt_status gpt_track_batched(gpt_handle *h, uint32_t B, const uint32_t *h_N, const uint32_t *h_S,
+}  // extern "C"
+
+// The adjoint of one update's solve at its solution xu (the handle's gxu), on the loss of the update's
+// horizon l = 1/2 sum_k |p(q_k+) - p*_k|^2 at xu+ = xu - dz: the steps of gpt_sqp_adjoint with the
+// loss gradient formed on the device, the weight gradients added to d_wgrad and l to d_loss.  The
+// solve's per-instance state is saved and restored around it.
+static gpt_status enqueue_track_adjoint(gpt_handle *h, const SqpPlan &pl, float *d_wgrad, float *d_loss,
+                                        cudaStream_t s)
+{
+    const BatchView &bv = pl.bv;
+    const SolverParams &SP = pl.SP;
+    const int ns = h->num_sms, T = bv.total_knots;
+    const bool f64 = SP.pcg_precond == 1 && SP.schur_fp64;
+    const float *S_rows = f64 ? reinterpret_cast<const float *>(h->S64) : h->S;
+    const int fmt = f64 ? 2 : 1;
+    GPT_CUDA(launch_track_adj_begin(bv, h->trk_rows, h->trk_clk, h->trk_stbak, s));
+    // the step at the solution: K [dz; lambda] = [g; c]
+    GPT_CUDA(launch_kkt(bv, pl.P, h->gxu, h->ggoal, h->xs, h->G, h->C, h->g, h->c, ns, s));
+    if (f64)
+        GPT_CUDA(launch_schur64(bv, h->G, h->C, h->g, h->c, h->S64, h->gamma64, nullptr, h->Ginv64, ns, s));
+    else
+        GPT_CUDA(launch_schur(1, bv, 0.f, h->G, h->C, h->g, h->c, h->S, nullptr, h->gamma, h->Ginv, h->Ginv64,
+                              nullptr, SP.pcg_precond == 0 ? 1 : 0, ns, s));
+    GPT_CUDA(cudaMemsetAsync(h->adj_lam, 0, sizeof(float) * NS * T, s));
+    GPT_CUDA(launch_pcg(bv, pl.maxN, pl.minN, fmt, (int)SP.pcg_precond, S_rows, nullptr, h->gamma, h->gamma64,
+                        h->adj_lam, h->lam64, h->crw, (int)SP.pcg_max_iter, SP.pcg_tol, (int)SP.pcg_exit_mode, nullptr,
+                        nullptr, 0, (int)SP.pcg_cluster_size, ns, s));
+    GPT_CUDA(cudaMemsetAsync(h->dz, 0, sizeof(float) * NX * T, s));
+    GPT_CUDA(launch_dz(bv, h->Ginv, h->Ginv64, h->C, h->g, nullptr, h->lam64, h->dz, ns, s));
+    // the adjoint solve K mu = [h; 0], h = dl/d(dz)
+    GPT_CUDA(cudaMemsetAsync(h->adj_h, 0, sizeof(float) * NX * T, s));
+    GPT_CUDA(launch_track_loss_grad(bv, h->gxu, h->dz, h->ggoal, h->adj_h, h->trk_kloss, ns, s));
+    GPT_CUDA(cudaMemsetAsync(h->adj_zero, 0, sizeof(float) * NS * T, s));
+    if (f64)
+        GPT_CUDA(launch_schur64(bv, h->G, h->C, h->adj_h, h->adj_zero, h->S64, h->adj_gamma64, nullptr, h->Ginv64,
+                                ns, s));
+    else
+        GPT_CUDA(launch_schur(1, bv, 0.f, h->G, h->C, h->adj_h, h->adj_zero, h->S, nullptr, h->adj_gamma, h->Ginv,
+                              h->Ginv64, nullptr, SP.pcg_precond == 0 ? 1 : 0, ns, s));
+    GPT_CUDA(cudaMemsetAsync(h->adj_lam, 0, sizeof(float) * NS * T, s));
+    GPT_CUDA(launch_pcg(bv, pl.maxN, pl.minN, fmt, (int)SP.pcg_precond, S_rows, nullptr, h->adj_gamma,
+                        h->adj_gamma64, h->adj_lam, h->adj_lam64, h->crw, (int)SP.pcg_max_iter, SP.pcg_tol,
+                        (int)SP.pcg_exit_mode, nullptr, nullptr, 0, (int)SP.pcg_cluster_size, ns, s));
+    GPT_CUDA(cudaMemsetAsync(h->adj_mu, 0, sizeof(float) * NX * T, s));
+    GPT_CUDA(launch_dz(bv, h->Ginv, h->Ginv64, h->C, h->adj_h, nullptr, h->adj_lam64, h->adj_mu, ns, s));
+    // dl/dtheta = mu_z^T (dg/dtheta - dG/dtheta dz), added to d_wgrad
+    GPT_CUDA(launch_adjoint_grad(bv, pl.P, h->gxu, h->ggoal, h->dz, h->adj_mu, h->trk_ggrad, h->adj_part, nullptr,
+                                 nullptr, nullptr, ns, s, d_wgrad));
+    GPT_CUDA(launch_track_adj_end(bv, h->trk_stbak, h->trk_kloss, d_loss, h->trk_inst, s));
+    return GPT_OK;
+}
+
+// gpt_track_batched, and with d_wgrad non-null gpt_track_batched_adjoint
+static gpt_status track_impl(gpt_handle *h, uint32_t B, const uint32_t *h_N, const uint32_t *h_S,
                              const float *d_eePos_traj, const float *d_xu_traj, float *d_xs,
                              const gpt_track_config *tc_in, float *d_err, uint32_t *d_log, uint32_t log_cap,
-                             gpt_track_stats *h_stats, gpt_stream_t stream)
+                             float *d_wgrad, float *d_loss, uint32_t *h_adj_fail, gpt_track_stats *h_stats,
+                             cudaStream_t s)
 {
-    if (!h || !h_N || !h_S || !d_eePos_traj || !d_xu_traj || !d_xs || !d_err)
-        return set_err(GPT_ERR_BAD_ARG, "null argument");
-    DeviceGuard dg(h->device);
     gpt_track_config tc;
     gpt_default_track_config(&tc);
     if (tc_in) tc = *tc_in;
@@ -1378,7 +1436,6 @@ gpt_status gpt_track_batched(gpt_handle *h, uint32_t B, const uint32_t *h_N, con
         h->h_trk_rows[b + 1] = h->h_trk_rows[b] + (int)h_S[b];
         maxS = h_S[b] > maxS ? h_S[b] : maxS;
     }
-    cudaStream_t s = (cudaStream_t)stream;
     BatchView bv;
     int maxN = 0, minN = 0;
     {
@@ -1389,12 +1446,15 @@ gpt_status gpt_track_batched(gpt_handle *h, uint32_t B, const uint32_t *h_N, con
     SolverParams SP = to_solver(h->sc);
     apply_tuned(h, bv, maxN, minN, SP);
     const SqpPlan plan{bv, P, SP, maxN, minN, h->num_sms};
+    if (d_wgrad && SP.pcg_precond == 2) return set_err(GPT_ERR_BAD_ARG, "the adjoint runs with pcg_precond 0 or 1");
     const TrackParams tp = track_params(h->pc.timestep, tc.sim_step, tc.shift_threshold, (double)tc.sim_period_us);
     const uint32_t n_updates = track_update_count(tp, maxS, tc.max_control_updates);
     const int ns = h->num_sms;
 
     GPT_CUDA(cudaMemcpyAsync(h->trk_rows, h->h_trk_rows, sizeof(int) * (B + 1), cudaMemcpyHostToDevice, s));
     GPT_CUDA(cudaMemsetAsync(d_err, 0, sizeof(float) * (size_t)h->h_trk_rows[B], s));
+    if (d_wgrad) GPT_CUDA(cudaMemsetAsync(d_wgrad, 0, sizeof(float) * 15 * B, s));
+    if (d_loss) GPT_CUDA(cudaMemsetAsync(d_loss, 0, sizeof(float) * B, s));
     GPT_CUDA(launch_track_start(bv, h->trk_rows, d_eePos_traj, d_xu_traj, h->gxu, h->trk_xu_old, h->ggoal, h->glam,
                                 h->trk_clk, h->trk_inst, 1e-3f, 0, ns, s));
     if (tc.jitter_solves > 0) {  // toplevel.cuh:581-592
@@ -1415,6 +1475,10 @@ gpt_status gpt_track_batched(gpt_handle *h, uint32_t B, const uint32_t *h_N, con
         GPT_CUDA(launch_track_prep(bv, h->trk_rows, h->trk_clk, tc.rho_reset, 0, s));
         const gpt_status st = solve_on_workspace(h, plan, s);
         if (st != GPT_OK) return st;
+        if (d_wgrad) {
+            const gpt_status sa = enqueue_track_adjoint(h, plan, d_wgrad, d_loss, s);
+            if (sa != GPT_OK) return sa;
+        }
         GPT_CUDA(launch_track_tail(bv, h->trk_rows, h->trk_clk, tp, d_eePos_traj, d_xu_traj, d_xs, h->gxu,
                                    h->trk_xu_old, h->ggoal, h->glam, h->adj_h, d_err, h->trk_inst, d_log, log_cap, s));
     }
@@ -1425,6 +1489,7 @@ gpt_status gpt_track_batched(gpt_handle *h, uint32_t B, const uint32_t *h_N, con
     for (uint32_t b = 0; b < B; ++b) {
         const TrackInst &ti = h->h_trk_inst[b];
         if (ti.nonfinite) nonfinite = true;
+        if (h_adj_fail) h_adj_fail[b] = ti.adj_fail;
         if (!h_stats) continue;
         gpt_track_stats &o = h_stats[b];
         o.control_updates = ti.updates;
@@ -1441,6 +1506,33 @@ gpt_status gpt_track_batched(gpt_handle *h, uint32_t B, const uint32_t *h_N, con
     }
     if (nonfinite) return set_err(GPT_ERR_NONFINITE, "non-finite merit or PCG reduction in a tracking solve");
     return GPT_OK;
+}
+
+extern "C" {
+
+gpt_status gpt_track_batched(gpt_handle *h, uint32_t B, const uint32_t *h_N, const uint32_t *h_S,
+                             const float *d_eePos_traj, const float *d_xu_traj, float *d_xs,
+                             const gpt_track_config *tc, float *d_err, uint32_t *d_log, uint32_t log_cap,
+                             gpt_track_stats *h_stats, gpt_stream_t stream)
+{
+    if (!h || !h_N || !h_S || !d_eePos_traj || !d_xu_traj || !d_xs || !d_err)
+        return set_err(GPT_ERR_BAD_ARG, "null argument");
+    DeviceGuard dg(h->device);
+    return track_impl(h, B, h_N, h_S, d_eePos_traj, d_xu_traj, d_xs, tc, d_err, d_log, log_cap, nullptr, nullptr,
+                      nullptr, h_stats, (cudaStream_t)stream);
+}
+
+gpt_status gpt_track_batched_adjoint(gpt_handle *h, uint32_t B, const uint32_t *h_N, const uint32_t *h_S,
+                                     const float *d_eePos_traj, const float *d_xu_traj, float *d_xs,
+                                     const gpt_track_config *tc, float *d_err, uint32_t *d_log, uint32_t log_cap,
+                                     float *d_weight_grad, float *d_loss, uint32_t *h_adjoint_fail,
+                                     gpt_track_stats *h_stats, gpt_stream_t stream)
+{
+    if (!h || !h_N || !h_S || !d_eePos_traj || !d_xu_traj || !d_xs || !d_err || !d_weight_grad)
+        return set_err(GPT_ERR_BAD_ARG, "null argument");
+    DeviceGuard dg(h->device);
+    return track_impl(h, B, h_N, h_S, d_eePos_traj, d_xu_traj, d_xs, tc, d_err, d_log, log_cap, d_weight_grad,
+                      d_loss, h_adjoint_fail, h_stats, (cudaStream_t)stream);
 }
 
 gpt_status gpt_track(gpt_handle *h, uint32_t N, uint32_t S, const float *d_eePos_traj, const float *d_xu_traj,

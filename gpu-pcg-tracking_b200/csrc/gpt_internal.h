@@ -79,9 +79,11 @@ cudaError_t launch_schur64(const BatchView &bv, const float *G, const float *C, 
                            int ctas_per_sm = 16);
 // adjoint of the SQP step (gpt_adjoint.cu): per-knot goal gradients, per-instance weight gradients;
 // part holds adjoint_part_floats() floats per knot
+// (wacc non-null: the 15 weight gradients of each active instance are added to wacc[15 b ..] instead of
+// written to grad_qd / grad_r / grad_qee)
 cudaError_t launch_adjoint_grad(const BatchView &bv, const ProblemParams &P, const float *xu, const float *goal,
                                 const float *dz, const float *mu, float *grad_goal, float *part, float *grad_qd,
-                                float *grad_r, float *grad_qee, int num_sms, cudaStream_t s);
+                                float *grad_r, float *grad_qee, int num_sms, cudaStream_t s, float *wacc = nullptr);
 cudaError_t launch_axpy(int n, float alpha, const float *x, const float *a, float *out, int num_sms, cudaStream_t s);
 size_t adjoint_part_floats();
 // reference 3-block FP32 rows -> FP64 packed rows (PK64) and gamma64 (input of the warp-pair PCG)
@@ -98,7 +100,8 @@ struct TrackClock {
 };
 struct TrackInst {  // per-instance totals over the loop
     uint32_t updates, sqp_iters, pcg_iters, ls_fail, pcg_maxiter, rho_exits, nonfinite, shifts;
-    float err_sum, final_err, rho, pad;
+    float err_sum, final_err, rho;
+    uint32_t adj_fail;  // updates whose adjoint solve failed (gpt_track_batched_adjoint)
 };
 struct TrackParams {
     double sim_us;           // SIMULATION_PERIOD
@@ -118,6 +121,16 @@ cudaError_t launch_track_tail(const BatchView &bv, const int *rows, TrackClock *
                               float *goal, float *lambda, float *tmp, float *errors, TrackInst *inst,
                               uint32_t *iters_log, uint32_t log_cap, cudaStream_t s);
 cudaError_t launch_track_final(const BatchView &bv, const float *xs, const float *goal, TrackInst *inst, cudaStream_t s);
+// the adjoint of each update's solve (gpt_track_batched_adjoint): begin saves the per-solve state and
+// marks the instances that track this update active; loss_grad writes h = dl/d(dz) = -dl/dxu+ of the
+// update's horizon loss l = 1/2 sum_k |p(q_k - dz_q,k) - p*_k|^2 (q entries only) and each knot's
+// term of l; end adds each live instance's l to loss, counts failed adjoint solves and restores the state
+cudaError_t launch_track_adj_begin(const BatchView &bv, const int *rows, const TrackClock *clk, InstState *bak,
+                                   cudaStream_t s);
+cudaError_t launch_track_loss_grad(const BatchView &bv, const float *xu, const float *dz, const float *goal, float *h,
+                                   float *kloss, int num_sms, cudaStream_t s);
+cudaError_t launch_track_adj_end(const BatchView &bv, const InstState *bak, const float *kloss, float *loss,
+                                 TrackInst *inst, cudaStream_t s);
 // stair preconditioner's off-diagonal Pinv blocks (gato_form_ss_inner), reference 3-block rows
 cudaError_t launch_form_ss(const BatchView &bv, const float *S, float *Pinv, int num_sms, cudaStream_t s);
 // batched rigid-body library kernels (gpt_grid.cu)

@@ -287,6 +287,89 @@ cudaError_t launch_track_final(const BatchView &bv, const float *xs, const float
     return cudaGetLastError();
 }
 
+// ---- the adjoint of each update's solve (gpt_track_batched_adjoint; no reference counterpart)
+
+// Saves every instance's per-solve state (the adjoint's KKT, Schur and PCG launches reuse the
+// solve's kernels, which count into it) and marks the instances that track this update active.
+__global__ void track_adj_begin_kernel(BatchView bv, const int *__restrict__ rows, const TrackClock *__restrict__ clk,
+                                       InstState *__restrict__ bak)
+{
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= bv.B) return;
+    InstState &s = bv.st[b];
+    bak[b] = s;
+    s.active = clk->traj_offset < (uint32_t)(rows[b + 1] - rows[b]) ? 1u : 0u;
+    s.exit_flags = 0u;
+    s.pcg_maxiter_count = 0u;
+}
+
+// One thread per knot of an active instance: q+ = q - dz_q, p = p(q+), e = p - p*_k;
+// kloss_k = |e|^2 / 2 and h_q = -J(q+)^T e (the adjoint right-hand side dl/d(dz) = -dl/dxu+).
+__global__ void track_loss_grad_kernel(BatchView bv, const float *__restrict__ xu, const float *__restrict__ dz,
+                                       const float *__restrict__ goal, float *__restrict__ h,
+                                       float *__restrict__ kloss)
+{
+    for (int j = bv.j0 + blockIdx.x * blockDim.x + threadIdx.x; j < bv.j0 + bv.total_knots;
+         j += gridDim.x * blockDim.x) {
+        if (!bv.active(bv.inst(j))) continue;
+        float q[NQ];
+#pragma unroll
+        for (int i = 0; i < NQ; ++i) q[i] = xu[(size_t)NX * j + i] - dz[(size_t)NX * j + i];
+        JointTrig t;
+        joint_trig(q, t);
+        float p[3], J[3 * NQ];
+        fk_lane<true>(t, p, J);
+        const float e0 = p[0] - goal[(size_t)6 * j], e1 = p[1] - goal[(size_t)6 * j + 1],
+                    e2 = p[2] - goal[(size_t)6 * j + 2];
+        kloss[j] = 0.5f * (e0 * e0 + e1 * e1 + e2 * e2);
+#pragma unroll
+        for (int i = 0; i < NQ; ++i) h[(size_t)NX * j + i] = -(J[3 * i] * e0 + J[3 * i + 1] * e1 + J[3 * i + 2] * e2);
+    }
+}
+
+// Per instance: loss[b] += the update's loss (a fixed-order FP64 sum of the knots' terms) and one
+// more failed update when an adjoint solve stopped (factorisation, non-finite value, PCG cap); then
+// the saved per-solve state comes back.
+__global__ void track_adj_end_kernel(BatchView bv, const InstState *__restrict__ bak, const float *__restrict__ kloss,
+                                     float *__restrict__ loss, TrackInst *__restrict__ inst)
+{
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= bv.B) return;
+    InstState &s = bv.st[b];
+    if (s.active) {
+        const int kb = bv.off(b), N = bv.N(b);
+        double a = 0.0;
+        for (int k = 0; k < N; ++k) a += (double)kloss[kb + k];
+        if (loss) loss[b] += (float)a;
+        if ((s.exit_flags & (GPT_EXIT_NONFINITE | GPT_EXIT_FACTOR)) || s.pcg_maxiter_count) inst[b].adj_fail++;
+    }
+    s = bak[b];
+}
+
+cudaError_t launch_track_adj_begin(const BatchView &bv, const int *rows, const TrackClock *clk, InstState *bak,
+                                   cudaStream_t s)
+{
+    track_adj_begin_kernel<<<(bv.B + 127) / 128, 128, 0, s>>>(bv, rows, clk, bak);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_track_loss_grad(const BatchView &bv, const float *xu, const float *dz, const float *goal, float *h,
+                                   float *kloss, int num_sms, cudaStream_t s)
+{
+    if (bv.total_knots <= 0) return cudaSuccess;
+    int blocks = (bv.total_knots + 127) / 128;
+    if (blocks > num_sms * 8) blocks = num_sms * 8;
+    track_loss_grad_kernel<<<blocks, 128, 0, s>>>(bv, xu, dz, goal, h, kloss);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_track_adj_end(const BatchView &bv, const InstState *bak, const float *kloss, float *loss,
+                                 TrackInst *inst, cudaStream_t s)
+{
+    track_adj_end_kernel<<<(bv.B + 127) / 128, 128, 0, s>>>(bv, bak, kloss, loss, inst);
+    return cudaGetLastError();
+}
+
 // simple_simulate of one state over one horizon (the gpt_simulate entry point): the clock
 // holds the time offset; one group of 8 lanes.
 __global__ void simulate_one_kernel(int N, TrackParams tp, double t0_us, float *__restrict__ xs,

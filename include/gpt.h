@@ -298,6 +298,24 @@ gpt_status gpt_track_batched(gpt_handle *h, uint32_t batch, const uint32_t *h_kn
                              uint32_t *d_sqp_iters_log, uint32_t log_capacity, gpt_track_stats *h_stats,
                              gpt_stream_t stream);
 
+/* gpt_track_batched with the adjoint of every control update's solve (no reference counterpart):
+ * after an update's solve, the one-step adjoint of gpt_sqp_adjoint at the update's solution xu, on
+ * that update's predicted tracking loss l = 1/2 sum_k |p(q_k+) - p*_k|^2 over the horizon at
+ * xu+ = xu - dz (the solution's next SQP step) against the update's goal window, accumulated over
+ * the updates each instance tracks:
+ *   d_weight_grad [15 batch]  per instance dl/dqd (7), dl/dr (7), dl/dq_ee, summed over its updates
+ *   d_loss        [batch]     sum of l over its updates (may be NULL)
+ *   h_adjoint_fail [batch]    updates whose adjoint solve failed: factorisation, non-finite value or
+ *                             PCG iteration cap (may be NULL)
+ * Both device arrays are overwritten.  The forward run (tracking errors, logs, statistics, plant
+ * state) equals gpt_track_batched's bit for bit.  Needs pcg_precond 0 or 1. */
+gpt_status gpt_track_batched_adjoint(gpt_handle *h, uint32_t batch, const uint32_t *h_knot_points,
+                                     const uint32_t *h_traj_steps, const float *d_eePos_traj,
+                                     const float *d_xu_traj, float *d_xs, const gpt_track_config *tc,
+                                     float *d_tracking_errors, uint32_t *d_sqp_iters_log, uint32_t log_capacity,
+                                     float *d_weight_grad, float *d_loss, uint32_t *h_adjoint_fail,
+                                     gpt_track_stats *h_stats, gpt_stream_t stream);
+
 /* simple_simulate (integrator.cuh:365-398): advances the plant state d_xs (14) by sim_time_us of
  * explicit-Euler steps of sim_step seconds (plus the remainder step), applying the control of
  * knot floor(t / timestep) of d_xu (21N-7), t starting time_offset_us into the horizon. */
