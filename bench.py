@@ -341,8 +341,12 @@ def run_sweep_plain(args, rank, local_rank):
 def run_mixed_track(args, rank, world, local_rank):
     """Receding-horizon tracking of B instances of seeded horizon N ~ U{64, 128, 256, 512}, each
     tracking its own seeded spline of `mixed_rows` rows (dt 0.01; the goal rows from the batched FK
-    kernel), warm-started through the shift of xu and lambda, 4 SQP iterations per solve, one
-    batched solve and one simulate / shift launch per control update.  Times the whole rollout."""
+    kernel), warm-started through the shift of xu and lambda, 4 SQP iterations per solve, 500 control
+    updates, one batched solve (the replayed solve graph) and one simulate / shift launch per update.
+    Times the rollout twice: forward only (gpt_track_batched), then with the adjoint of every update's
+    solve and the weight gradients accumulated per instance (gpt_track_batched_adjoint); then, outside
+    the timed regions, the tracking error of sampled instances against the plain single-instance
+    loop (gpt_track) and the FP64 error of the solver's steps on a mixed-horizon batch."""
     import numpy as np
     import torch
     import torch.distributed as dist
@@ -362,45 +366,102 @@ def run_mixed_track(args, rank, world, local_rank):
     xu_traj = torch.as_tensor(np.concatenate(rows).reshape(-1), device="cuda")
     ee = gpt.end_effector_positions(xu_traj, 21).reshape(-1)
     xs0 = torch.as_tensor(np.concatenate(xs), device="cuda")
+    solver_kw = dict(sqp_max_iter=args.track_sqp_iters, pcg_max_iter=args.pcg_max_iter, pcg_exit_tol=args.tol,
+                     pcg_exit_mode=0, pcg_cluster_size=gpt.PCG_WARP_QUAD, sqp_graph=args.sqp_graph)
     sv = gpt.Solver(max_knot_points=max(Ns), max_batch=B, **SPEC)
-    sv.set_solver(sqp_max_iter=args.track_sqp_iters, pcg_max_iter=args.pcg_max_iter, pcg_exit_tol=args.tol,
-                  pcg_exit_mode=0, pcg_cluster_size=gpt.PCG_WARP_PAIR, sqp_graph=args.sqp_graph)
-    tcfg = gpt.default_track_config(sim_period_us=args.mixed_period_us)
+    sv.set_solver(**solver_kw)
+    n_updates = 500
+    tcfg = gpt.default_track_config(sim_period_us=args.mixed_period_us, max_control_updates=n_updates)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
     stream = torch.cuda.current_stream()
-    # warm-up: the first 3 control updates of the same rollout (builds and caches the solve graph)
+    # warm-up: the first 3 control updates of the same rollout, both forms (builds the solve graph)
     warm = gpt.default_track_config(sim_period_us=args.mixed_period_us, max_control_updates=3)
     sv.track_batched(Ns, [S] * B, ee, xu_traj, xs0.clone(), warm, errors=torch.zeros(B * S, device="cuda"))
-    xs = xs0.clone()
-    errs = torch.zeros(B * S, device="cuda")
-    clocks = ClockSampler(torch.cuda.current_device())
-    clocks.start()
-    flush.fill_(1.0)
-    if world > 1:
-        dist.barrier()
-    torch.cuda.synchronize()
-    clocks.mark()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    _, st = sv.track_batched(Ns, [S] * B, ee, xu_traj, xs, tcfg, errors=errs)
-    e1.record(stream)
-    e1.synchronize()
-    clk = clocks.stop()
-    t_ms = shard.max_over_ranks(e0.elapsed_time(e1), device="cuda")
+    sv.track_batched_adjoint(Ns, [S] * B, ee, xu_traj, xs0.clone(), warm, errors=torch.zeros(B * S, device="cuda"))
+
+    def timed(adjoint):
+        xs = xs0.clone()
+        errs = torch.zeros(B * S, device="cuda")
+        clocks = ClockSampler(torch.cuda.current_device())
+        clocks.start()
+        flush.fill_(1.0)
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        clocks.mark()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        if adjoint:
+            _, st, wgrad, loss, fails = sv.track_batched_adjoint(Ns, [S] * B, ee, xu_traj, xs, tcfg, errors=errs)
+        else:
+            _, st = sv.track_batched(Ns, [S] * B, ee, xu_traj, xs, tcfg, errors=errs)
+            wgrad = loss = fails = None
+        e1.record(stream)
+        e1.synchronize()
+        clk = clocks.stop()
+        return shard.max_over_ranks(e0.elapsed_time(e1), device="cuda"), st, wgrad, loss, fails, clk
+
+    t_ms, st, _, _, _, clk = timed(False)
+    t_adj, st_a, wgrad, loss, fails, clk_a = timed(True)
     updates = sum(s["control_updates"] for s in st)
+    # the weight gradient summed over the batch (the data-parallel reduction of shard.allreduce_weight_grads)
+    wsum = wgrad.sum(0)
+    if world > 1:
+        dist.all_reduce(wsum)
+    wsum = wsum.cpu().numpy()
+    adjoint = {
+        "ms": t_adj, "solves_per_s": world * updates / (t_adj / 1000.0),
+        "overhead_ratio": (t_adj - t_ms) / t_ms,
+        "us_per_solve": 1000.0 * (t_adj - t_ms) / max(updates / world, 1),
+        "forward_equal": all(st[b] == st_a[b] for b in range(B)),
+        "loss_total": float(loss.double().sum()), "adjoint_failures": int(sum(fails)),
+        "weight_grad_batch_sum": {"qd": [float(v) for v in wsum[:7]], "r": [float(v) for v in wsum[7:14]],
+                                  "q_ee": float(wsum[14])},
+        "workload": "gpt_track_batched_adjoint: the same rollout with, after every update's solve, the one-step "
+                    "adjoint of that update's horizon tracking loss (KKT, Schur, PCG and dz at the solution, the "
+                    "loss gradient, the transposed solve, the weight gradients accumulated per instance)",
+        "clocks": clk_a,
+    }
+    # the plain single-instance loop on sampled instances (one of each horizon), outside the timed region
+    sample = [next(b for b in range(B) if Ns[b] == n) for n in (64, 128, 256, 512) if n in Ns]
+    plain = []
+    for b in sample:
+        s1 = gpt.Solver(max_knot_points=Ns[b], **SPEC)
+        s1.set_solver(**solver_kw)
+        xs1 = xs0[14 * b:14 * b + 14].clone()
+        tr_b = xu_traj[21 * S * b:21 * S * (b + 1)]
+        ee_b = ee[6 * S * b:6 * S * (b + 1)]
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        _, st1 = s1.track(Ns[b], ee_b, tr_b, xs1, tcfg)
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        s1.close()
+        plain.append({"instance": b, "N": Ns[b], "batched_tracking_error": st[b]["tracking_error_mean"],
+                      "plain_tracking_error": st1["tracking_error_mean"],
+                      "plain_solves_per_s": st1["control_updates"] / dt})
+    # the FP64 error of the solver's steps on a mixed-horizon batch (one problem of each horizon)
+    mb_Ns = [64, 128, 256, 512]
+    mb = P.make_batch(mb_Ns, seed0=ids[0], dt=SPEC["timestep"])
+    fp64 = fp64_accuracy(gpt, sv, mb_Ns, mb, len(mb_Ns), args.track_sqp_iters)
     line = {
         "metric": "mixed-horizon tracking solves/s", "value": world * updates / (t_ms / 1000.0), "unit": "solves/s",
         "n_gpus": world, "higher_is_better": True, "scaling": "weak", "dtype": "f32", "data": "synthetic",
         "config": {"workload": f"gpt_track_batched: {B} instances/GPU, N ~ U{{64,128,256,512}} (seeded), {S} "
-                               f"trajectory rows each, dt 0.01, plant period {args.mixed_period_us:g} us, "
-                               f"{args.track_sqp_iters} SQP iterations per solve",
+                               f"trajectory rows each, {n_updates} control updates, dt 0.01, plant period "
+                               f"{args.mixed_period_us:g} us, {args.track_sqp_iters} SQP iterations per solve, "
+                               f"partitioned PCG",
                    "instances_per_gpu": B, "knots_total": int(sum(Ns)), "rows": S},
         "ms": t_ms, "control_updates": st[0]["control_updates"], "ms_per_update": t_ms / max(st[0]["control_updates"], 1),
         "sqp_iters_per_solve": sum(s["sqp_iters_total"] for s in st) / max(updates, 1),
         "tracking_error_mean": statistics.mean(s["tracking_error_mean"] for s in st),
         "final_tracking_error_mean": statistics.mean(s["final_tracking_error"] for s in st),
         "rho_exits": sum(s["rho_exits"] for s in st), "nonfinite": sum(s["nonfinite"] for s in st),
-        "clocks": clk,
+        "clocks": clk, "adjoint": adjoint,
+        "plain_vs_batched": {"instances": plain,
+                             "max_abs_tracking_error_diff": max(abs(p["batched_tracking_error"] -
+                                                                    p["plain_tracking_error"]) for p in plain)},
+        "fp64_rel_err": fp64,
     }
     if rank == 0:
         print(json.dumps(line), flush=True)
