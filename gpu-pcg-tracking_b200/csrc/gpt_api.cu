@@ -721,6 +721,7 @@ static gpt_status enqueue_prologue(gpt_handle *h, const SqpPlan &pl, const float
 {
     PhaseTimer t(h, s, GPT_PHASE_INIT);
     GPT_CUDA(launch_init(pl.bv, d_xu, h->xs, pl.ns, s));
+    GPT_CUDA(launch_kkt_gconst(pl.bv, pl.P, h->G, pl.ns, s));  // G's weight-only entries, once per solve
     GPT_CUDA(launch_merit(pl.bv, pl.P, 1, d_xu, nullptr, d_goal, h->xs, h->knot_merit, pl.ns, s,
                           ctas_or_default(pl.SP.cta_merit)));
     GPT_CUDA(launch_accept(pl.bv, 0, pl.SP, h->knot_merit, nullptr, nullptr, nullptr, nullptr, pl.ns, s));
@@ -741,7 +742,8 @@ static gpt_status enqueue_iteration(gpt_handle *h, const SqpPlan &pl, const floa
     const float *S_rows = f64 ? reinterpret_cast<const float *>(h->S64) : (stair ? h->Sref : h->S);
     {
         PhaseTimer t(h, s, GPT_PHASE_KKT);
-        GPT_CUDA(launch_kkt(bv, pl.P, d_xu, d_goal, h->xs, h->G, h->C, h->g, h->c, ns, s, ctas_or_default(SP.cta_kkt)));
+        GPT_CUDA(launch_kkt(bv, pl.P, d_xu, d_goal, h->xs, h->G, h->C, h->g, h->c, ns, s, ctas_or_default(SP.cta_kkt),
+                            false));
     }
     {
         PhaseTimer t(h, s, GPT_PHASE_SCHUR);

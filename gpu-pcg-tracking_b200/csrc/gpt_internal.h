@@ -39,9 +39,12 @@ inline int ctas_or_default(uint8_t v) { return v ? (int)v : 16; }
 // when handles live on several devices.
 cudaError_t ensure_func_attrs(const void *func, size_t smem_bytes, bool cluster16 = false);
 
+// full_g false: only the position block of each Q_k is written (the SQP loop, after launch_kkt_gconst
+// wrote the rest of G for the same view and weights)
 cudaError_t launch_kkt(const BatchView &bv, const ProblemParams &P, const float *xu, const float *goal,
                        const float *xs, float *G, float *C, float *g, float *c, int num_sms, cudaStream_t s,
-                       int ctas_per_sm = 16);
+                       int ctas_per_sm = 16, bool full_g = true);
+cudaError_t launch_kkt_gconst(const BatchView &bv, const ProblemParams &P, float *G, int num_sms, cudaStream_t s);
 // Ginv64 (optional) receives the inverses in FP64; need_pinv = 0 skips the theta inversion in mode 1
 cudaError_t launch_schur(int mode, const BatchView &bv, float rho_scalar, const float *G, const float *C,
                          const float *g, const float *c, float *S, float *Pinv, float *gamma, float *Ginv,

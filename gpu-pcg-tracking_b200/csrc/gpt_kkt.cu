@@ -13,7 +13,10 @@
 //   all lanes    df/du = [-Minv dID/dx, Minv], A_k, B_k, defect, cost terms
 // and writes the reference blocks G_k = {Q_k, R_k}, C_k = {-A_k, -B_k},
 // g_k = {q_k, r_k}, c_{k+1}.  The half-warp of knot N-2 also writes the terminal
-// Q_{N-1}, q_{N-1} and c_0 = x_0 - x_s (schur.cuh:429-479).
+// Q_{N-1}, q_{N-1} and c_0 = x_0 - x_s (schur.cuh:429-479).  Inside the SQP loop
+// (FULL_G false) only the knot-dependent 7x7 position block of Q_k is written: the
+// rest of G (the velocity diagonal, R, the zeros) depends on the cost weights only and
+// is written once per solve by gconst_kernel.
 #include "gpt_common.cuh"
 #include "gpt_dyn.cuh"
 #include "gpt_internal.h"
@@ -42,6 +45,39 @@ constexpr int KKT_WARPS = 4;
 // without a knot (odd count, last knot of an instance, inactive instance) computes on knot 0's data
 // and writes nothing, so both halves take every __syncwarp.  Four CTAs per SM (16 warps; the
 // kernel fits 128 registers without spilling).
+// The knot a half-warp takes in pair step jp, and the inputs it stages: lane hl loads entries hl,
+// hl + 16 and hl + 32 of x_k, u_k, x_{k+1} and entry hl of goal_k, goal_{k+1} (the next step's are
+// loaded while the current step computes).
+struct KktKnot {
+    int j, b, N, k, jj;
+    bool valid;
+};
+__device__ __forceinline__ KktKnot kkt_knot(const BatchView &bv, int jp, int half)
+{
+    KktKnot kn;
+    kn.j = bv.j0 + 2 * jp + half;
+    kn.valid = kn.j < bv.j0 + bv.total_knots;
+    kn.b = 0;
+    kn.N = 2;
+    kn.k = 0;
+    if (kn.valid) {
+        kn.b = bv.inst(kn.j);
+        kn.N = bv.N(kn.b);
+        kn.k = kn.j - bv.off(kn.b);
+        kn.valid = (kn.k < kn.N - 1) && bv.active(kn.b);
+    }
+    kn.jj = kn.valid ? kn.j : bv.j0;  // the view's first knot always has a successor (N >= 2)
+    return kn;
+}
+__device__ __forceinline__ void kkt_fetch(const float *xu, const float *goal, int jj, int hl, float (&v)[4])
+{
+    const float *xk = xu + (size_t)NX * jj;
+#pragma unroll
+    for (int q = 0; q < 3; ++q) v[q] = (hl + 16 * q < NX + NS) ? __ldg(xk + hl + 16 * q) : 0.f;
+    v[3] = hl < 12 ? __ldg(goal + (size_t)6 * jj + hl) : 0.f;
+}
+
+template <bool FULL_G>
 __global__ void __launch_bounds__(32 * KKT_WARPS, 4) kkt_kernel(BatchView bv, ProblemParams P, const float *__restrict__ xu,
                                                            const float *__restrict__ goal,
                                                            const float *__restrict__ xs, float *__restrict__ G,
@@ -54,28 +90,24 @@ __global__ void __launch_bounds__(32 * KKT_WARPS, 4) kkt_kernel(BatchView bv, Pr
     const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nw = (gridDim.x * blockDim.x) >> 5;
 
+    float pv[4];
+    kkt_fetch(xu, goal, kkt_knot(bv, gw, half).jj, hl, pv);
     for (int jp = gw; 2 * jp < bv.total_knots; jp += nw) {
-        const int j = bv.j0 + 2 * jp + half;
-        bool valid = j < bv.j0 + bv.total_knots;
-        int b = 0, N = 2, k = 0;
-        if (valid) {
-            b = bv.inst(j);
-            N = bv.N(b);
-            k = j - bv.off(b);
-            valid = (k < N - 1) && bv.active(b);
-        }
-        const int jj = valid ? j : bv.j0;  // the view's first knot always has a successor (N >= 2)
+        const KktKnot kn = kkt_knot(bv, jp, half);
+        const int j = kn.j, b = kn.b, N = kn.N, k = kn.k;
+        const bool valid = kn.valid;
         const bool terminal = valid && (k == N - 2);
 
-        // ---- stage x_k, u_k, x_{k+1}, goal_k, goal_{k+1}
-        const float *xk = xu + (size_t)NX * jj;
-        for (int i = hl; i < NX + NS; i += 16) {
-            float v = xk[i];
-            if (i < NS) sm.x[i] = v;
-            else if (i < NX) sm.u[i - NS] = v;
-            else sm.xn[i - NX] = v;
+        // ---- stage x_k, u_k, x_{k+1}, goal_k, goal_{k+1} (fetched during the previous step)
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+            const int i = hl + 16 * q;
+            if (i < NS) sm.x[i] = pv[q];
+            else if (i < NX) sm.u[i - NS] = pv[q];
+            else if (i < NX + NS) sm.xn[i - NX] = pv[q];
         }
-        if (hl < 12) sm.goal[hl] = goal[(size_t)6 * jj + hl];
+        if (hl < 12) sm.goal[hl] = pv[3];
+        if (2 * (jp + nw) < bv.total_knots) kkt_fetch(xu, goal, kkt_knot(bv, jp + nw, half).jj, hl, pv);
         __syncwarp();
         if (hl < NQ) sincosf(sm.x[hl], &sm.trig.s[hl], &sm.trig.c[hl]);
         __syncwarp();
@@ -203,33 +235,32 @@ __global__ void __launch_bounds__(32 * KKT_WARPS, 4) kkt_kernel(BatchView bv, Pr
         __syncwarp();
 
         if (valid) {
-            // ---- C_k = {-A_k, -B_k} (integrator.cuh:85-126, sign from schur.cuh:519-520)
+            // ---- C_k = {-A_k, -B_k} (integrator.cuh:85-126, sign from schur.cuh:519-520): lane r writes row r
+            // of the 21 columns (each store a contiguous column of 14 floats per half-warp)
             float *Ck = Cm + (size_t)C_STRIDE * j;
             const float dt = P.dt;
-            for (int e = hl; e < C_STRIDE; e += 16) {
-                float val;
-                if (e < SS) {
-                    const int col = e / NS, r = e - NS * col;
-                    if (P.integrator == 0) {
-                        val = (float)(r == col);
+            if (hl < NS) {
+                const int r = hl, rq = r < NQ ? r : r - NQ;
+                if (P.integrator == 0) {
+#pragma unroll
+                    for (int col = 0; col < NS; ++col) {
+                        float val = (float)(r == col);
                         if (r < NQ && r == col - NQ) val += dt;
                         if (r >= NQ) val += dt * sm.dfdu[col * NQ + r - NQ];
-                    } else {
-                        const int rq = r % NQ;
-                        const float dtv = (r == rq) ? dt : 1.f;
-                        val = (float)(r == col) + dt * (float)(r == col - NQ) + dt * sm.dfdu[col * NQ + rq] * dtv;
+                        Ck[r + NS * col] = -val;
                     }
+#pragma unroll
+                    for (int col = 0; col < NC; ++col)
+                        Ck[SS + r + NS * col] = -((r >= NQ) ? dt * sm.dfdu[(NS + col) * NQ + r - NQ] : 0.f);
                 } else {
-                    const int e2 = e - SS, col = e2 / NS, r = e2 - NS * col;
-                    if (P.integrator == 0) {
-                        val = (r >= NQ) ? dt * sm.dfdu[(NS + col) * NQ + r - NQ] : 0.f;
-                    } else {
-                        const int rq = r % NQ;
-                        const float dtv = (r == rq) ? dt : 1.f;
-                        val = dt * sm.dfdu[SC + col * NQ + rq] * dtv;
-                    }
+                    const float dtv = (r == rq) ? dt : 1.f;
+#pragma unroll
+                    for (int col = 0; col < NS; ++col)
+                        Ck[r + NS * col] = -((float)(r == col) + dt * (float)(r == col - NQ) +
+                                             dt * sm.dfdu[col * NQ + rq] * dtv);
+#pragma unroll
+                    for (int col = 0; col < NC; ++col) Ck[SS + r + NS * col] = -(dt * sm.dfdu[SC + col * NQ + rq] * dtv);
                 }
-                Ck[e] = -val;
             }
             // ---- defect c_{k+1} = x_{k+1} - f(x_k, u_k)  (integrator.cuh:25-83)
             if (hl < NQ) {
@@ -248,23 +279,33 @@ __global__ void __launch_bounds__(32 * KKT_WARPS, 4) kkt_kernel(BatchView bv, Pr
             }
             // ---- G_k = {Q_k, R_k}, g_k = {q_k, r_k}
             float *Gk = G + (size_t)G_STRIDE * j;
-            for (int e = hl; e < G_STRIDE; e += 16) {
-                float v;
-                if (e < SS) {
-                    const int i = e / NS, jq = e - NS * i;
-                    v = (i < NQ && jq < NQ) ? sm.qv[0][i] * sm.qv[0][jq] : ((i == jq) ? P.qd_cost : 0.f);
-                } else {
-                    v = ((e - SS) % (NC + 1) == 0) ? P.r_cost : 0.f;
+            if constexpr (FULL_G) {
+                for (int e = hl; e < G_STRIDE; e += 16) {
+                    float v;
+                    if (e < SS) {
+                        const int i = e / NS, jq = e - NS * i;
+                        v = (i < NQ && jq < NQ) ? sm.qv[0][i] * sm.qv[0][jq] : ((i == jq) ? P.qd_cost : 0.f);
+                    } else {
+                        v = ((e - SS) % (NC + 1) == 0) ? P.r_cost : 0.f;
+                    }
+                    Gk[e] = v;
                 }
-                Gk[e] = v;
+            } else if (hl < NQ) {
+#pragma unroll
+                for (int i = 0; i < NQ; ++i) Gk[NS * i + hl] = sm.qv[0][i] * sm.qv[0][hl];
             }
             for (int e = hl; e < NX; e += 16)
                 g[(size_t)NX * j + e] = (e < NS) ? sm.qv[0][e] : P.r_cost * sm.u[e - NS];
             if (terminal) {
                 float *Gt = G + (size_t)G_STRIDE * (j + 1);
-                for (int e = hl; e < SS; e += 16) {
-                    const int i = e / NS, jq = e - NS * i;
-                    Gt[e] = (i < NQ && jq < NQ) ? sm.qv[1][i] * sm.qv[1][jq] : ((i == jq) ? P.qd_cost : 0.f);
+                if constexpr (FULL_G) {
+                    for (int e = hl; e < SS; e += 16) {
+                        const int i = e / NS, jq = e - NS * i;
+                        Gt[e] = (i < NQ && jq < NQ) ? sm.qv[1][i] * sm.qv[1][jq] : ((i == jq) ? P.qd_cost : 0.f);
+                    }
+                } else if (hl < NQ) {
+#pragma unroll
+                    for (int i = 0; i < NQ; ++i) Gt[NS * i + hl] = sm.qv[1][i] * sm.qv[1][hl];
                 }
                 if (hl < NS) {
                     g[(size_t)NX * (j + 1) + hl] = sm.qv[1][hl];
@@ -277,16 +318,51 @@ __global__ void __launch_bounds__(32 * KKT_WARPS, 4) kkt_kernel(BatchView bv, Pr
     }
 }
 
+// The cost-weight-only entries of G for every knot of the view: Q's velocity diagonal and zeros outside
+// the position block, R = r_cost I (the terminal knot has no R).  One thread per entry.
+__global__ void gconst_kernel(BatchView bv, float qd_cost, float r_cost, float *__restrict__ G)
+{
+    const size_t n = (size_t)G_STRIDE * bv.total_knots;
+    for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (size_t)gridDim.x * blockDim.x) {
+        const int e = (int)(t % G_STRIDE);
+        const int j = bv.j0 + (int)(t / G_STRIDE);
+        const int b = bv.inst(j);
+        if (!bv.active(b)) continue;
+        const bool last = j - bv.off(b) == bv.N(b) - 1;
+        float *Gk = G + (size_t)G_STRIDE * j;
+        if (e < SS) {
+            const int i = e / NS, jq = e - NS * i;
+            if (i < NQ && jq < NQ) continue;  // the position block: kkt_kernel's
+            Gk[e] = (i == jq) ? qd_cost : 0.f;
+        } else if (!last) {
+            Gk[e] = ((e - SS) % (NC + 1) == 0) ? r_cost : 0.f;
+        }
+    }
+}
+
 cudaError_t launch_kkt(const BatchView &bv, const ProblemParams &P, const float *xu, const float *goal,
                        const float *xs, float *G, float *C, float *g, float *c, int num_sms, cudaStream_t s,
-                       int ctas_per_sm)
+                       int ctas_per_sm, bool full_g)
 {
     if (bv.total_knots <= 0) return cudaSuccess;
     int warps = (bv.total_knots + 1) / 2;  // two knots per warp
     int blocks = (warps + KKT_WARPS - 1) / KKT_WARPS;
     const int cap = num_sms * ctas_per_sm;
     if (blocks > cap) blocks = cap;
-    kkt_kernel<<<blocks, 32 * KKT_WARPS, 0, s>>>(bv, P, xu, goal, xs, G, C, g, c);
+    if (full_g)
+        kkt_kernel<true><<<blocks, 32 * KKT_WARPS, 0, s>>>(bv, P, xu, goal, xs, G, C, g, c);
+    else
+        kkt_kernel<false><<<blocks, 32 * KKT_WARPS, 0, s>>>(bv, P, xu, goal, xs, G, C, g, c);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_kkt_gconst(const BatchView &bv, const ProblemParams &P, float *G, int num_sms, cudaStream_t s)
+{
+    if (bv.total_knots <= 0) return cudaSuccess;
+    const size_t n = (size_t)G_STRIDE * bv.total_knots;
+    size_t blocks = (n + 255) / 256;
+    if (blocks > (size_t)num_sms * 8) blocks = (size_t)num_sms * 8;
+    gconst_kernel<<<(unsigned)blocks, 256, 0, s>>>(bv, P.qd_cost, P.r_cost, G);
     return cudaGetLastError();
 }
 
