@@ -30,7 +30,6 @@ struct KktWarpSmem {
     float cbias[NQ];
     float Minv[CC];
     float qdd[NQ];
-    float dc[NQ * NS];     // dID/dx, col-major 7x14
     float dfdu[NQ * NX];   // [dqdd/dq dqdd/dqd dqdd/du], col-major 7x21
     float ee[2][3];
     float J[2][21];
@@ -145,8 +144,12 @@ __global__ void __launch_bounds__(32 * KKT_WARPS, 4) kkt_kernel(BatchView bv, Pr
             }
             gj7_group(col, 16 * half);
             if (hl >= NQ && hl < 2 * NQ) {
+                // Minv column hl - 7: kept for the products below, and dqdd/du's column of df/du
 #pragma unroll
-                for (int r = 0; r < NQ; ++r) sm.Minv[NQ * (hl - NQ) + r] = (float)col[r];
+                for (int r = 0; r < NQ; ++r) {
+                    sm.Minv[NQ * (hl - NQ) + r] = (float)col[r];
+                    sm.dfdu[SC + NQ * (hl - NQ) + r] = (float)col[r];
+                }
             } else if (hl == 2 * NQ) {
 #pragma unroll
                 for (int r = 0; r < NQ; ++r) sm.qdd[r] = (float)col[r];
@@ -154,9 +157,10 @@ __global__ void __launch_bounds__(32 * KKT_WARPS, 4) kkt_kernel(BatchView bv, Pr
         }
         __syncwarp();
 
-        // ---- dID/dq_j, dID/dqd_j at (q, qd, qdd), lanes 0..13
+        // ---- dID/dq_j, dID/dqd_j at (q, qd, qdd), lanes 0..13 (lane hl: direction hl of x)
+        float dtau[NQ];
         {
-            float qd[NQ], qdd[NQ], tau[NQ], dtau[NQ];
+            float qd[NQ], qdd[NQ], tau[NQ];
 #pragma unroll
             for (int i = 0; i < NQ; ++i) {
                 qd[i] = sm.x[NQ + i];
@@ -165,9 +169,16 @@ __global__ void __launch_bounds__(32 * KKT_WARPS, 4) kkt_kernel(BatchView bv, Pr
             const int dq_dir = (hl < NQ) ? hl : -1;
             const int dqd_dir = (hl >= NQ && hl < NS) ? hl - NQ : -1;
             rnea<true>(trig, qd, qdd, dq_dir, dqd_dir, tau, dtau);
-            if (hl < NS) {
+        }
+        // ---- df/du (iiwa_eepos_plant.cuh:142-155): lane hl < 14 forms column hl of -Minv dID/dx from its
+        // own tangent; the Minv columns came from the elimination
+        if (hl < NS) {
+#pragma unroll 1
+            for (int r = 0; r < NQ; ++r) {
+                float acc = 0.f;
 #pragma unroll
-                for (int r = 0; r < NQ; ++r) sm.dc[NQ * hl + r] = dtau[r];
+                for (int t = 0; t < NQ; ++t) acc += sm.Minv[r + NQ * t] * dtau[t];
+                sm.dfdu[NQ * hl + r] = -acc;
             }
         }
         // ---- end-effector position and Jacobian (lane 0 at x_k, lane 1 at the terminal state)
@@ -180,20 +191,6 @@ __global__ void __launch_bounds__(32 * KKT_WARPS, 4) kkt_kernel(BatchView bv, Pr
         }
         __syncwarp();
 
-        // ---- df/du (iiwa_eepos_plant.cuh:142-155)
-        for (int e = hl; e < NQ * NX; e += 16) {
-            float v;
-            if (e < NQ * NS) {
-                const int col = e / NQ, r = e - NQ * col;
-                float acc = 0.f;
-#pragma unroll
-                for (int t = 0; t < NQ; ++t) acc += sm.Minv[r + NQ * t] * sm.dc[NQ * col + t];
-                v = -acc;
-            } else {
-                v = sm.Minv[e - NQ * NS];
-            }
-            sm.dfdu[e] = v;
-        }
         // ---- cost gradient (iiwa_eepos_plant.cuh:329-354)
         if (hl < NS) {
             float v;
