@@ -322,37 +322,122 @@ __device__ __forceinline__ bool warp_inverse64(const float *A, double shift, dou
     return ok;
 }
 
+// FP64 inverse of the 7x7 position block (A + shift I) of a state block (A column-major with leading
+// dimension LD), by Gauss-Jordan with 2x2 block pivots {0,1}, {2,3}, {4,5} and the scalar pivot 6
+// (no pivoting: the blocks are diagonal blocks of Schur complements of an SPD matrix).  Lanes 0..6 hold
+// A's columns, lanes 7..13 the identity's; a 2x2 step needs the block's three entries and the two pivot
+// columns' rows (shuffles), and one reciprocal of its determinant, so the chain of dependent steps is
+// four long instead of seven.  The pivot test is the scalar elimination's, pivot by pivot: x > 1e-13 d_p
+// and det / x > 1e-13 d_{p+1} (d the entries of A + shift I's diagonal).  Lanes 7..13 write the inverse.
+template <int LD>
+__device__ __forceinline__ bool warp_inverse64_pos7(const float *A, double shift, double *Ainv, int lane,
+                                                    float *Ainv32, double *Ainv64g)
+{
+    constexpr int n = NC;
+    double col[n];
+    double diag_own = 0.0;
+    const bool left = lane < n, right = (lane >= n) && (lane < 2 * n);
+#pragma unroll
+    for (int r = 0; r < n; ++r) {
+        double v = 0.0;
+        if (left) v = (double)A[r + LD * lane] + ((r == lane) ? shift : 0.0);
+        else if (right) v = (r == lane - n) ? 1.0 : 0.0;
+        col[r] = v;
+        if (left && r == lane) diag_own = v;
+    }
+    bool ok = true;
+#pragma unroll
+    for (int p = 0; p + 1 < n; p += 2) {
+        const double x = __shfl_sync(0xffffffffu, col[p], p);
+        const double y = __shfl_sync(0xffffffffu, col[p + 1], p);
+        const double z = __shfl_sync(0xffffffffu, col[p + 1], p + 1);
+        const double d0 = __shfl_sync(0xffffffffu, diag_own, p), d1 = __shfl_sync(0xffffffffu, diag_own, p + 1);
+        double pr0[n], pr1[n];  // rows r of the pivot columns p, p + 1
+#pragma unroll
+        for (int r = 0; r < n; ++r) {
+            if (r == p || r == p + 1) continue;
+            pr0[r] = __shfl_sync(0xffffffffu, col[r], p);
+            pr1[r] = __shfl_sync(0xffffffffu, col[r], p + 1);
+        }
+        const double det = fma(x, z, -y * y);
+        ok = ok && (d0 > 0.0) && (d1 > 0.0) && (x > PIVOT_REL_MIN * d0) && (det > PIVOT_REL_MIN * d1 * x);
+        const double rd = __drcp_rn(det);
+        const double i00 = z * rd, i01 = -y * rd, i11 = x * rd;
+        const double w0 = col[p], w1 = col[p + 1];
+        const double n0 = fma(i00, w0, i01 * w1), n1 = fma(i01, w0, i11 * w1);
+#pragma unroll
+        for (int r = 0; r < n; ++r) {
+            if (r == p || r == p + 1) continue;
+            col[r] = fma(-pr0[r], n0, fma(-pr1[r], n1, col[r]));
+        }
+        col[p] = n0;
+        col[p + 1] = n1;
+    }
+    {
+        constexpr int p = n - 1;
+        const double piv = __shfl_sync(0xffffffffu, col[p], p);
+        const double d0 = __shfl_sync(0xffffffffu, diag_own, p);
+        ok = ok && (d0 > 0.0) && (piv > PIVOT_REL_MIN * d0);
+        double pr[n];
+#pragma unroll
+        for (int r = 0; r < p; ++r) pr[r] = __shfl_sync(0xffffffffu, col[r], p);
+        const double prow = col[p] * __drcp_rn(piv);
+#pragma unroll
+        for (int r = 0; r < p; ++r) col[r] = fma(-pr[r], prow, col[r]);
+        col[p] = prow;
+    }
+    if (right) {
+        const int cc = lane - n;
+#pragma unroll
+        for (int r = 0; r < n; ++r) Ainv[r + LD * cc] = col[r];
+        if (Ainv32) {
+#pragma unroll
+            for (int r = 0; r < n; ++r) Ainv32[r + LD * cc] = (float)col[r];
+        }
+        if (Ainv64g) {
+#pragma unroll
+            for (int r = 0; r < n; ++r) Ainv64g[r + LD * cc] = col[r];
+        }
+    }
+    return ok;
+}
+
 // (Q + shift I)^{-1} of a 14x14 state block.  The blocks kkt_kernel writes are block diagonal --
 // a 7x7 position block (q q^T), a diagonal velocity block (QD) -- and then the inverse is the
-// position block's 7x7 Gauss-Jordan and the reciprocals of the velocity diagonal.  Gauss-Jordan
-// without pivoting never mixes the two blocks of a block-diagonal matrix (every update it would
-// make across them multiplies an exact zero), so this is the same arithmetic as the full 14x14
-// elimination, result for result; any other Q takes the full elimination.
+// position block's inverse (warp_inverse64_pos7) and the reciprocals of the velocity diagonal (lanes
+// 0..6, one each); any other Q takes the full 14x14 elimination.  The structure test reads every
+// entry outside the blocks without branching on the running result (the loads issue together).
 // *blockdiag (optional) tells which path ran: true when the inverse has that block-diagonal zero pattern.
 __device__ __forceinline__ bool warp_inverse64_state(const float *Q, double shift, double *Ainv, int lane,
                                                      float *Ainv32, double *Ainv64g, bool *blockdiag = nullptr)
 {
     bool ok = true;
-    for (int e = lane; e < SS; e += 32) {
+#pragma unroll
+    for (int i = 0; i < (SS + 31) / 32; ++i) {
+        const int e = lane + 32 * i;
         const int r = e % NS, cc = e / NS;
-        if (((r < NC) != (cc < NC)) || (r >= NC && cc >= NC && r != cc)) ok = ok && (Q[e] == 0.f);
+        const bool outside = (e < SS) && (((r < NC) != (cc < NC)) || (r >= NC && cc >= NC && r != cc));
+        ok &= !outside || (Q[e < SS ? e : 0] == 0.f);
     }
     const bool bd = __all_sync(0xffffffffu, ok);
     if (blockdiag) *blockdiag = bd;
     if (!bd) return warp_inverse64<NS>(Q, shift, Ainv, lane, Ainv32, Ainv64g);
-    bool piv_ok = warp_inverse64<NC, NS>(Q, shift, Ainv, lane, Ainv32, Ainv64g);
-    for (int e = lane; e < SS; e += 32) {
-        const int r = e % NS, cc = e / NS;
-        if (r < NC && cc < NC) continue;
-        double v = 0.0;
-        if (r == cc) {
-            const double d = (double)Q[e] + shift;
-            piv_ok = piv_ok && (d > 0.0);
-            v = __drcp_rn(d);
-        }
+    bool piv_ok = warp_inverse64_pos7<NS>(Q, shift, Ainv, lane, Ainv32, Ainv64g);
+    if (lane < NC) {
+        const int e = (NC + lane) * (NS + 1);
+        const double d = (double)Q[e] + shift;
+        piv_ok = piv_ok && (d > 0.0);
+        const double v = __drcp_rn(d);
         Ainv[e] = v;
         if (Ainv32) Ainv32[e] = (float)v;
         if (Ainv64g) Ainv64g[e] = v;
+    }
+    for (int e = lane; e < SS; e += 32) {
+        const int r = e % NS, cc = e / NS;
+        if ((r < NC && cc < NC) || r == cc) continue;
+        Ainv[e] = 0.0;
+        if (Ainv32) Ainv32[e] = 0.f;
+        if (Ainv64g) Ainv64g[e] = 0.0;
     }
     return __all_sync(0xffffffffu, piv_ok);
 }
@@ -363,22 +448,30 @@ __device__ __forceinline__ bool warp_inverse64_control(const float *R, double sh
                                                        float *Ainv32, double *Ainv64g, bool *diagonal = nullptr)
 {
     bool ok = true;
-    for (int e = lane; e < CC; e += 32)
-        if (e % NC != e / NC) ok = ok && (R[e] == 0.f);
+#pragma unroll
+    for (int i = 0; i < (CC + 31) / 32; ++i) {
+        const int e = lane + 32 * i;
+        const bool off = (e < CC) && (e % NC != e / NC);
+        ok &= !off || (R[e < CC ? e : 0] == 0.f);
+    }
     const bool dg = __all_sync(0xffffffffu, ok);
     if (diagonal) *diagonal = dg;
     if (!dg) return warp_inverse64<NC>(R, shift, Ainv, lane, Ainv32, Ainv64g);
     bool piv_ok = true;
-    for (int e = lane; e < CC; e += 32) {
-        double v = 0.0;
-        if (e % NC == e / NC) {
-            const double d = (double)R[e] + shift;
-            piv_ok = piv_ok && (d > 0.0);
-            v = __drcp_rn(d);
-        }
+    if (lane < NC) {
+        const int e = lane * (NC + 1);
+        const double d = (double)R[e] + shift;
+        piv_ok = d > 0.0;
+        const double v = __drcp_rn(d);
         Ainv[e] = v;
         if (Ainv32) Ainv32[e] = (float)v;
         if (Ainv64g) Ainv64g[e] = v;
+    }
+    for (int e = lane; e < CC; e += 32) {
+        if (e % NC == e / NC) continue;
+        Ainv[e] = 0.0;
+        if (Ainv32) Ainv32[e] = 0.f;
+        if (Ainv64g) Ainv64g[e] = 0.0;
     }
     return __all_sync(0xffffffffu, piv_ok);
 }
