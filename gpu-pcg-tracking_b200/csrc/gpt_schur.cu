@@ -546,7 +546,10 @@ __global__ void __launch_bounds__(32 * SCHUR_WARPS, 5)
             continue;
         }
 
-        // ---- rows k >= 1: every input of the knot loaded in one batch, then staged
+        // ---- rows k >= 1: every input of the knot loaded in one batch, then staged.  Q_{k-1} is needed
+        // only to invert it, which the previous row of a run did already (have == j - 1): then its 196
+        // entries are not loaded
+        const bool reuse = have == j - 1;
         {
             const float *Gkm1 = G + (size_t)G_STRIDE * (j - 1);
             const float *Gkq = G + (size_t)G_STRIDE * j;
@@ -556,8 +559,9 @@ __global__ void __launch_bounds__(32 * SCHUR_WARPS, 5)
 #pragma unroll
             for (int i = 0; i < NL; ++i) {
                 const int e = lane + 32 * i;
-                v[i] = e < G_STRIDE ? Gkm1[e] : (e < G_STRIDE + SS ? Gkq[e - G_STRIDE]
-                                                : (e < G_STRIDE + SS + C_STRIDE ? Ck[e - G_STRIDE - SS] : 0.f));
+                v[i] = e < G_STRIDE ? ((reuse && e < SS) ? 0.f : Gkm1[e])
+                                    : (e < G_STRIDE + SS ? Gkq[e - G_STRIDE]
+                                                         : (e < G_STRIDE + SS + C_STRIDE ? Ck[e - G_STRIDE - SS] : 0.f));
             }
             double gv = 0.0;
             if (lane < NX) gv = (double)g[(size_t)NX * (j - 1) + lane];
@@ -569,7 +573,9 @@ __global__ void __launch_bounds__(32 * SCHUR_WARPS, 5)
 #pragma unroll
             for (int i = 0; i < NL; ++i) {
                 const int e = lane + 32 * i;
-                if (e < G_STRIDE) sm.Gm1[e] = v[i];
+                if (e < G_STRIDE) {
+                    if (!reuse || e >= SS) sm.Gm1[e] = v[i];
+                }
                 else if (e < G_STRIDE + SS) sm.Gk[e - G_STRIDE] = v[i];
                 else if (e < G_STRIDE + SS + C_STRIDE) sm.C[e - G_STRIDE - SS] = v[i];
             }
@@ -586,7 +592,7 @@ __global__ void __launch_bounds__(32 * SCHUR_WARPS, 5)
         double *Gi64 = Ginv64 + (size_t)G_STRIDE * (j - 1);
         double *const Qki = sm.Qinv[cur], *const Qkp1i = sm.Qinv[cur ^ 1];
         bool ok = true, bd_ki = have_bd, bd_kp1 = false, r_diag = false;
-        if (have == j - 1) {
+        if (reuse) {
             // formed by this warp's previous row; its outputs for knot j - 1 are written here, as the
             // elimination below would
             for (int e = lane; e < SS; e += 32) {
