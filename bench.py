@@ -71,7 +71,7 @@ def parse():
                     help="0 block-Jacobi (the reference's), 1 block-tridiagonal LDL^T per CTA chunk")
     ap.add_argument("--batched-only", action="store_true", help="skip the e2e and plain legs (profiling runs)")
     ap.add_argument("--no-track", action="store_true", help="skip the MPC tracking leg")
-    ap.add_argument("--sqp-graph", type=int, default=2, choices=range(0, 9),
+    ap.add_argument("--sqp-graph", type=int, default=4, choices=range(0, 9),
                     help="0 host loop, 1 one graph per solve, K = 2..8 graph with K concurrent part-batch branches")
     ap.add_argument("--track-sqp-iters", type=int, default=4,
                     help="SQP iterations per solve in the tracking leg (stands in for the wall-clock cap)")
