@@ -660,11 +660,11 @@ def main():
     one_step()
     sv.set_profiling(False)
     phases = sv.phase_stats(reset=True)
-    # kernels per timed step of the graph: the prologue (init, merit, accept), then per SQP iteration
-    # (as many as the profiled step's KKT launches) the six phase kernels once per part-batch branch
-    # and the while loop's control kernel
+    # kernels per timed step of the graph: the prologue (init, G's weight-only entries, merit, accept),
+    # then per SQP iteration (as many as the profiled step's KKT launches) the six phase kernels once
+    # per part-batch branch and the while loop's control kernel
     branches = min(args.sqp_graph, B) if args.sqp_graph >= 2 else 1
-    launches_per_step = 3 + phases["kkt"][1] * (6 * branches + 1)
+    launches_per_step = 4 + phases["kkt"][1] * (6 * branches + 1)
     total_ms = sum(step_ms)
     total_ms = shard.max_over_ranks(total_ms, device="cuda")
     ms_per_step = total_ms / args.steps
