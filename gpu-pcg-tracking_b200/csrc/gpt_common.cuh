@@ -127,6 +127,27 @@ __device__ __forceinline__ void warp_dmma_store(const double (&c)[TI][TJ][2], F 
             for (int e = 0; e < 2; ++e) st(8 * I + g, 8 * J + 2 * t + e, c[I][J][e]);
 }
 
+// Asynchronous global -> shared copies (cp.async): 16 bytes (both addresses 16-byte aligned, L1
+// bypassed) or 4 bytes; a thread's copies form groups (commit) it can wait for (all but the newest N).
+__device__ __forceinline__ void cp_async16(void *sdst, const void *gsrc)
+{
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((uint32_t)__cvta_generic_to_shared(sdst)),
+                 "l"(gsrc)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async4(void *sdst, const void *gsrc)
+{
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"((uint32_t)__cvta_generic_to_shared(sdst)),
+                 "l"(gsrc)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait()
+{
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
 __device__ __forceinline__ float warp_sum(float v)
 {
 #pragma unroll

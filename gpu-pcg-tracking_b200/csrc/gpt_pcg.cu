@@ -1739,18 +1739,6 @@ __host__ __device__ constexpr int quad_smem_doubles(int n)
            QUAD_NWARP + QUAD_NWARP * NS + 2;
 }
 
-__device__ __forceinline__ void cp_async16(void *sdst, const void *gsrc)
-{
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((uint32_t)__cvta_generic_to_shared(sdst)),
-                 "l"(gsrc)
-                 : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait()
-{
-    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
-}
 // the lanes of a warp copy `chunks` 16-byte chunks (both addresses 16-byte aligned)
 __device__ __forceinline__ void warp_cp_async(void *sdst, const void *gsrc, int chunks, int lane)
 {

@@ -504,6 +504,7 @@ __global__ void __launch_bounds__(32 * SCHUR_WARPS, 5)
     const int chunk = (bv.total_knots + nw - 1) / nw;
     const int jbeg = bv.j0 + gw * chunk;
     const int jend = min(jbeg + chunk, bv.j0 + bv.total_knots);
+    bool pref = false;     // this row's R_{k-1}, Q_k and C_{k-1} arrived by cp.async during the previous row
     int have = -1;         // knot whose inverse sm.Qinv[cur] holds
     int cur = 0;
     bool have_bd = false;  // that inverse is block diagonal (position block, diagonal velocity block)
@@ -556,12 +557,14 @@ __global__ void __launch_bounds__(32 * SCHUR_WARPS, 5)
             const float *Ck = Cm + (size_t)C_STRIDE * (j - 1);
             constexpr int NL = (G_STRIDE + SS + C_STRIDE + 31) / 32;  // 24 per lane
             float v[NL];
+            if (!pref) {
 #pragma unroll
-            for (int i = 0; i < NL; ++i) {
-                const int e = lane + 32 * i;
-                v[i] = e < G_STRIDE ? ((reuse && e < SS) ? 0.f : Gkm1[e])
-                                    : (e < G_STRIDE + SS ? Gkq[e - G_STRIDE]
-                                                         : (e < G_STRIDE + SS + C_STRIDE ? Ck[e - G_STRIDE - SS] : 0.f));
+                for (int i = 0; i < NL; ++i) {
+                    const int e = lane + 32 * i;
+                    v[i] = e < G_STRIDE ? ((reuse && e < SS) ? 0.f : Gkm1[e])
+                                        : (e < G_STRIDE + SS ? Gkq[e - G_STRIDE]
+                                                             : (e < G_STRIDE + SS + C_STRIDE ? Ck[e - G_STRIDE - SS] : 0.f));
+                }
             }
             double gv = 0.0;
             if (lane < NX) gv = (double)g[(size_t)NX * (j - 1) + lane];
@@ -570,14 +573,18 @@ __global__ void __launch_bounds__(32 * SCHUR_WARPS, 5)
                 g2 = (double)g[(size_t)NX * j + lane];
                 cv = (double)c[(size_t)NS * j + lane];
             }
+            if (!pref) {
 #pragma unroll
-            for (int i = 0; i < NL; ++i) {
-                const int e = lane + 32 * i;
-                if (e < G_STRIDE) {
-                    if (!reuse || e >= SS) sm.Gm1[e] = v[i];
+                for (int i = 0; i < NL; ++i) {
+                    const int e = lane + 32 * i;
+                    if (e < G_STRIDE) {
+                        if (!reuse || e >= SS) sm.Gm1[e] = v[i];
+                    }
+                    else if (e < G_STRIDE + SS) sm.Gk[e - G_STRIDE] = v[i];
+                    else if (e < G_STRIDE + SS + C_STRIDE) sm.C[e - G_STRIDE - SS] = v[i];
                 }
-                else if (e < G_STRIDE + SS) sm.Gk[e - G_STRIDE] = v[i];
-                else if (e < G_STRIDE + SS + C_STRIDE) sm.C[e - G_STRIDE - SS] = v[i];
+            } else {
+                cp_async_wait<0>();  // this row's blocks, copied during the previous row
             }
             if (lane < NS) {
                 sm.qk[lane] = gv;
@@ -608,6 +615,15 @@ __global__ void __launch_bounds__(32 * SCHUR_WARPS, 5)
              ok;
         if (!ok && lane == 0) atomicOr(&bv.st[b].exit_flags, GPT_EXIT_FACTOR);
         __syncwarp();
+        // the next row of the same instance (k + 1 < N) needs R_k, Q_{k+1} and C_k: R_k and Q_{k+1} are
+        // copied now into the blocks the inverses above have finished with, C_k once the products below
+        // are done with C_{k-1}; its Q_k is not needed (its inverse is this row's (Q_k + rho I)^{-1})
+        const bool next = (j + 1 < jend) && (k + 1 < N);
+        if (next) {
+            const float *Rk = G + (size_t)G_STRIDE * j + SS, *Qn = G + (size_t)G_STRIDE * (j + 1);
+            for (int e = lane; e < CC; e += 32) cp_async4(sm.Gm1 + SS + e, Rk + e);
+            for (int e = lane; e < SS; e += 32) cp_async4(sm.Gk + e, Qn + e);
+        }
         // the products on the FP64 tensor cores, 14x14 (14x7) blocks padded to 16x16 (16x8)
         const float *Am = sm.C, *Bm = sm.C + SS;  // -A, -B
         {
@@ -652,6 +668,13 @@ __global__ void __launch_bounds__(32 * SCHUR_WARPS, 5)
                                lane);  // + (-B) Rt^{-1} (-B)^T
             warp_dmma_store(ct, [&](int i, int j, double v) { if (i < NS && j < NS) sm.theta[i + NS * j] = v; }, lane);
         }
+        if (next) {
+            __syncwarp();  // every lane has read C_{k-1}
+            const float *Cn = Cm + (size_t)C_STRIDE * j;
+            for (int e = lane; e < C_STRIDE; e += 32) cp_async4(sm.C + e, Cn + e);
+        }
+        cp_async_commit();
+        pref = next;
         if (lane < NS) {
             double a1 = 0.0, a2 = 0.0, a3 = 0.0;
 #pragma unroll
