@@ -552,19 +552,16 @@ __global__ void __launch_bounds__(32 * SCHUR_WARPS, 5)
         // entries are not loaded
         const bool reuse = have == j - 1;
         {
-            const float *Gkm1 = G + (size_t)G_STRIDE * (j - 1);
-            const float *Gkq = G + (size_t)G_STRIDE * j;
-            const float *Ck = Cm + (size_t)C_STRIDE * (j - 1);
-            constexpr int NL = (G_STRIDE + SS + C_STRIDE + 31) / 32;  // 24 per lane
-            float v[NL];
             if (!pref) {
-#pragma unroll
-                for (int i = 0; i < NL; ++i) {
-                    const int e = lane + 32 * i;
-                    v[i] = e < G_STRIDE ? ((reuse && e < SS) ? 0.f : Gkm1[e])
-                                        : (e < G_STRIDE + SS ? Gkq[e - G_STRIDE]
-                                                             : (e < G_STRIDE + SS + C_STRIDE ? Ck[e - G_STRIDE - SS] : 0.f));
-                }
+                // this row's blocks were not copied ahead (the first row of a run, or of an instance
+                // inside it): copy them now; Q_{k-1} only when the run's previous row did not invert it
+                const float *Gkm1 = G + (size_t)G_STRIDE * (j - 1);
+                const float *Gkq = G + (size_t)G_STRIDE * j;
+                const float *Ck = Cm + (size_t)C_STRIDE * (j - 1);
+                for (int e = reuse ? SS + lane : lane; e < G_STRIDE; e += 32) cp_async4(sm.Gm1 + e, Gkm1 + e);
+                for (int e = lane; e < SS; e += 32) cp_async4(sm.Gk + e, Gkq + e);
+                for (int e = lane; e < C_STRIDE; e += 32) cp_async4(sm.C + e, Ck + e);
+                cp_async_commit();
             }
             double gv = 0.0;
             if (lane < NX) gv = (double)g[(size_t)NX * (j - 1) + lane];
@@ -573,19 +570,7 @@ __global__ void __launch_bounds__(32 * SCHUR_WARPS, 5)
                 g2 = (double)g[(size_t)NX * j + lane];
                 cv = (double)c[(size_t)NS * j + lane];
             }
-            if (!pref) {
-#pragma unroll
-                for (int i = 0; i < NL; ++i) {
-                    const int e = lane + 32 * i;
-                    if (e < G_STRIDE) {
-                        if (!reuse || e >= SS) sm.Gm1[e] = v[i];
-                    }
-                    else if (e < G_STRIDE + SS) sm.Gk[e - G_STRIDE] = v[i];
-                    else if (e < G_STRIDE + SS + C_STRIDE) sm.C[e - G_STRIDE - SS] = v[i];
-                }
-            } else {
-                cp_async_wait<0>();  // this row's blocks, copied during the previous row
-            }
+            cp_async_wait<0>();  // this row's blocks (copied now, or during the previous row)
             if (lane < NS) {
                 sm.qk[lane] = gv;
                 sm.qkp1[lane] = g2;
