@@ -59,11 +59,12 @@ def fd(f, theta, rel=1e-4, floor=1e-6):
     return out
 
 
-@pytest.mark.parametrize("ref_terminal", [1, 0])
-def test_adjoint_matches_fd(gpt, oracle, problem_mod, ref_terminal):
+@pytest.mark.parametrize("ref_terminal,N,rho", [(1, 12, 1e-2), (0, 12, 1e-2), (1, 32, 1e-2), (1, 12, 1e-3), (1, 128, 1e-3)])
+def test_adjoint_matches_fd(gpt, oracle, problem_mod, ref_terminal, N, rho):
     """Gradients of w . xu+ w.r.t. qd (7), r (7), q_ee and the goal (xyz per
-    knot) match FP64 central differences to 1e-3 relative (per group)."""
-    N, rho = 12, 1e-2
+    knot) match FP64 central differences to 1e-3 relative (per group), also at
+    longer horizons and a smaller regularisation, up to the bench's horizon
+    N = 128 at rho = 1e-3."""
     p = problem_mod.make_problem(N, 3, dt=SPEC["timestep"])
     xu, goal, xs = (p[k].astype(np.float64) for k in ("xu", "goal", "xs"))
     # an iterate off the goal (the initial guess tracks it to rounding), rounded to FP32 as the GPU sees it
