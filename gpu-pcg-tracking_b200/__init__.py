@@ -400,16 +400,17 @@ class Solver:
                  schedule: Optional[dict] = None) -> int:
         """gpt_autotune: pick and remember the fastest PCG kernel and per-knot launch schedule for this batch
         shape.  Returns the PCG cluster size; `schedule` (a dict, optional) receives the CTAs per SM chosen
-        for the KKT, Schur, merit and dz launches."""
+        for the KKT, Schur, merit and dz launches and the part-batch branches per graph iteration
+        ("branches": tuned when sqp_graph is 1, else the configured value)."""
         B = len(knot_points)
         Ns = (C.c_uint32 * B)(*knot_points)
         rr = (C.c_float * B)(*rho)
         cs = C.c_uint32(0)
-        sched = (C.c_uint32 * 4)()
+        sched = (C.c_uint32 * 5)()
         _check(lib().gpt_autotune(self._h, B, C.cast(Ns, C.c_void_p), _ptr(eePos_traj), _ptr(lam), _ptr(xu),
                                   C.cast(rr, C.c_void_p), C.byref(cs), C.cast(sched, C.c_void_p), _stream(stream)))
         if schedule is not None:
-            schedule.update(dict(zip(("kkt", "schur", "merit", "dz"), list(sched))))
+            schedule.update(dict(zip(("kkt", "schur", "merit", "dz", "branches"), list(sched))))
         return cs.value
 
     def sqp_adjoint(self, knot_points: Sequence[int], eePos_traj, xs, xu, rho: Sequence[float], grad_xu_next,

@@ -157,7 +157,8 @@ struct gpt_handle {
     struct Tuned {
         int B, total, maxN, minN;
         uint32_t cluster;
-        uint8_t cta[4];  // CTAs per SM of the KKT, FP64 Schur, merit and dz launches
+        uint8_t cta[4];    // CTAs per SM of the KKT, FP64 Schur, merit and dz launches
+        uint8_t branches;  // part-batch branches per graph iteration (sqp_graph 1 only; 0 = not tuned)
     };
     // a schedule under trial inside gpt_autotune (overrides the tuned entry)
     bool trial = false;
@@ -937,16 +938,18 @@ static gpt_status sqp_graph_for(gpt_handle *h, const SqpPlan &pl, cudaGraphExec_
 // config leaves the PCG cluster size to the library; a schedule under trial takes precedence.
 static void apply_tuned(const gpt_handle *h, const BatchView &bv, int maxN, int minN, SolverParams &SP)
 {
-    if (SP.pcg_cluster_size == 0) {
-        for (const auto &t : h->tuned)
-            if (t.B == bv.B && t.total == bv.total_knots && t.maxN == maxN && t.minN == minN) {
+    const bool tune_graph = SP.sqp_graph == 1 && !h->trial;  // a graph solve whose branch count is not given
+    for (const auto &t : h->tuned)
+        if (t.B == bv.B && t.total == bv.total_knots && t.maxN == maxN && t.minN == minN) {
+            if (SP.pcg_cluster_size == 0) {
                 SP.pcg_cluster_size = t.cluster;
                 SP.cta_kkt = t.cta[0];
                 SP.cta_schur = t.cta[1];
                 SP.cta_merit = t.cta[2];
                 SP.cta_dz = t.cta[3];
             }
-    }
+            if (tune_graph && t.branches > 1) SP.sqp_graph = t.branches;
+        }
     if (h->trial) {
         SP.cta_kkt = h->trial_cta[0];
         SP.cta_schur = h->trial_cta[1];
@@ -1127,9 +1130,11 @@ gpt_status gpt_autotune(gpt_handle *h, uint32_t B, const uint32_t *h_N, const fl
     if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) st = set_err(GPT_ERR_CUDA, "event");
     // two SQP iterations of the batch with a given PCG kernel and launch schedule: the best of two timed
     // repetitions after one warm-up (attributes, graph capture, caches)
+    uint32_t branches = 1;  // part-batch branches of the trials (a graph solve: the caller's sqp_graph 1)
     auto time_schedule = [&](uint32_t cluster, const uint8_t *cta) -> float {
         h->sc = saved;
         h->sc.pcg_cluster_size = cluster;
+        if (saved.sqp_graph == 1) h->sc.sqp_graph = branches;
         h->sc.sqp_max_iter = saved.sqp_max_iter < 2 ? saved.sqp_max_iter : 2;
         h->trial = true;
         for (int i = 0; i < 4; ++i) h->trial_cta[i] = cta[i];
@@ -1188,6 +1193,23 @@ gpt_status gpt_autotune(gpt_handle *h, uint32_t B, const uint32_t *h_N, const fl
         }
         cta[which] = keep;
     }
+    // 3. for a graph solve whose branch count the caller left to the library (sqp_graph 1), the number of
+    // concurrent part-batch branches per SQP iteration, 1, 2 or 4 (no more than the instances); a change
+    // must gain 1 %
+    uint32_t best_branches = 1;
+    if (saved.sqp_graph == 1 && st == GPT_OK) {
+        for (uint32_t kb : {2u, 4u}) {
+            if (kb > B) break;
+            branches = kb;
+            const float ms = time_schedule(best, cta);
+            if (st != GPT_OK) break;
+            if (ms < 0.99f * best_ms) {
+                best_ms = ms;
+                best_branches = kb;
+            }
+        }
+        branches = 1;
+    }
     if (e0) cudaEventDestroy(e0);
     if (e1) cudaEventDestroy(e1);
     h->sc = saved;
@@ -1199,12 +1221,16 @@ gpt_status gpt_autotune(gpt_handle *h, uint32_t B, const uint32_t *h_N, const fl
         if (t.B == (int)B && t.total == total && t.maxN == maxN && t.minN == minN) {
             t.cluster = best;
             std::memcpy(t.cta, cta, sizeof(cta));
+            t.branches = (uint8_t)best_branches;
             found = true;
         }
-    if (!found) h->tuned.push_back({(int)B, total, maxN, minN, best, {cta[0], cta[1], cta[2], cta[3]}});
+    if (!found)
+        h->tuned.push_back({(int)B, total, maxN, minN, best, {cta[0], cta[1], cta[2], cta[3]}, (uint8_t)best_branches});
     if (h_cluster_out) *h_cluster_out = best;
-    if (h_schedule_out)
+    if (h_schedule_out) {
         for (int i = 0; i < 4; ++i) h_schedule_out[i] = (uint32_t)ctas_or_default(cta[i]);
+        h_schedule_out[4] = saved.sqp_graph == 1 ? best_branches : saved.sqp_graph;
+    }
     return GPT_OK;
 }
 

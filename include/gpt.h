@@ -94,9 +94,11 @@ typedef struct gpt_solver_config {
                                   FP32 formation moves the solution by ~cond(S) x 1e-7 (~1e-2 at cond 1e7) */
     uint32_t sqp_graph;        /* 1 (default): a solve runs as one CUDA graph (built on the first call of each
                                   batch shape and cached) whose while node repeats the SQP iteration on the
-                                  device; K = 2 .. 8: the same graph with the batch split in K parts whose
-                                  iterations run on concurrent branches (one part's PCG overlaps the others'
-                                  KKT, Schur and merit kernels; identical results); 0: one host
+                                  device, split in the part-batch branches gpt_autotune chose for the shape
+                                  (one when it was not tuned); K = 2 .. 8: the same graph with the batch split
+                                  in K parts whose iterations run on concurrent branches (one part's PCG
+                                  overlaps the others' KKT, Schur and merit kernels; identical results); 0:
+                                  one host
                                   synchronisation per SQP iteration, as the reference loop.  Profiling
                                   (gpt_set_profiling) uses the host loop. */
 } gpt_solver_config;
@@ -200,9 +202,13 @@ gpt_status gpt_sqp_solve_batched_trace(gpt_handle *h, uint32_t batch, const uint
  *      with pcg_precond 1, GPT_PCG_WARP_PAIR and GPT_PCG_WARP_QUAD;
  *   2. then, one kernel at a time, the grid of the per-knot kernels -- KKT formation, FP64 Schur complement,
  *      line-search merit, dz recovery -- as CTAs per SM in {4, 5, 6, 8, 16} (16 is the default; a change
- *      must gain 1 %).
- * h_cluster_out (optional) receives the PCG choice, h_schedule_out (optional, 4 entries) the CTAs per SM of
- * the KKT, Schur, merit and dz launches. */
+ *      must gain 1 %);
+ *   3. then, when the handle's sqp_graph is 1 (a graph solve whose branch count is left to the library),
+ *      the part-batch branches per graph iteration in {1, 2, 4} (at most the batch; a change must gain
+ *      1 %), which later graph solves of the shape use while sqp_graph stays 1.
+ * h_cluster_out (optional) receives the PCG choice, h_schedule_out (optional, 5 entries) the CTAs per SM of
+ * the KKT, Schur, merit and dz launches and the branches per graph iteration (the tuned count with
+ * sqp_graph 1, else sqp_graph itself). */
 gpt_status gpt_autotune(gpt_handle *h, uint32_t batch, const uint32_t *h_knot_points, const float *d_eePos_traj,
                         const float *d_lambda, const float *d_xu, const float *h_rho, uint32_t *h_cluster_out,
                         uint32_t *h_schedule_out, gpt_stream_t stream);

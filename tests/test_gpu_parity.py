@@ -541,7 +541,9 @@ def test_autotune_choice_is_used(gpt, problem_mod):
     cs = sv.autotune([N], goal, l_in, x_in, [1e-3], schedule=sched)
     assert torch.equal(x_in, xu0) and torch.equal(l_in, lam0)
     assert cs in (1, 2, 4, gpt.PCG_WARP_PAIR, gpt.PCG_WARP_QUAD)
-    assert sorted(sched) == ["dz", "kkt", "merit", "schur"] and set(sched.values()) <= {4, 5, 6, 8, 16}, sched
+    assert sorted(sched) == ["branches", "dz", "kkt", "merit", "schur"], sched
+    assert sched["branches"] == 1, sched  # one instance: no part-batch branches to try
+    assert {sched[k] for k in ("kkt", "schur", "merit", "dz")} <= {4, 5, 6, 8, 16}, sched
     out = []
     for given in (0, cs):
         sv.set_solver(pcg_cluster_size=given)
@@ -551,6 +553,32 @@ def test_autotune_choice_is_used(gpt, problem_mod):
     sv.close()
     np.testing.assert_array_equal(out[0], out[1])
 
+
+
+@pytest.mark.gpu
+def test_autotune_picks_graph_branches(gpt, problem_mod):
+    """With sqp_graph 1 the autotuner also times 2 and 4 part-batch branches per graph iteration for a
+    batch (8 instances of N = 32); the solve that uses its choice gives the bits of the host-driven loop
+    with the same tuned PCG kernel and grids."""
+    Ns = [32] * 8
+    batch = problem_mod.make_batch(Ns, seed0=21, dt=0.01)
+    goal, xu0, lam0 = (dev(batch[k]) for k in ("goal", "xu", "lam"))
+    sv = gpt.Solver(max_knot_points=32, max_batch=8, sqp_graph=1, **SPEC_CFG)
+    try:
+        sv.set_solver(sqp_max_iter=4)
+        sched = {}
+        sv.autotune(Ns, goal, lam0, xu0, [1e-3] * 8, schedule=sched)
+        assert sched["branches"] in (1, 2, 4), sched
+        out = []
+        for graph in (1, 0):
+            sv.set_solver(sqp_graph=graph)
+            xu, lam = xu0.clone(), lam0.clone()
+            sv.sqp_solve_batched(Ns, goal, lam, xu, [1e-3] * 8)
+            out.append((host(xu), host(lam)))
+    finally:
+        sv.close()
+    np.testing.assert_array_equal(out[0][0], out[1][0])
+    np.testing.assert_array_equal(out[0][1], out[1][1])
 
 def test_form_ss_matches_oracle(gpt, oracle, golden, problem_mod, solvers):
     """gpt_form_ss (gato_form_ss_inner) on the GPU's own S and block-Jacobi Pinv against the
