@@ -123,6 +123,7 @@ struct gpt_handle {
     uint32_t *pcg_log = nullptr, *pcg_out = nullptr, *d_active = nullptr;
     double *lam64 = nullptr;   // FP64 multipliers from the PCG, consumed by dz
     double *Ginv64 = nullptr;  // FP64 inverses (Q + rho I)^-1, (R + rho I)^-1 from Schur, consumed by dz
+    double *Ginv64c = nullptr; // the same in compact form (GC64 doubles per knot) from the FP64 Schur kernel
     double *crw = nullptr;     // FP64 cyclic-reduction couplings of the PCG preconditioner, 196 per knot
     // adjoint workspace: right-hand side, its zero constraint part, gamma, multipliers, mu_z, partials
     float *adj_h = nullptr, *adj_zero = nullptr, *adj_gamma = nullptr, *adj_lam = nullptr, *adj_mu = nullptr,
@@ -370,6 +371,7 @@ gpt_status gpt_create(const gpt_problem_config *pc, const gpt_solver_config *sc,
     ALLOC(d_active, 1);
     ALLOC(lam64, NS * T);
     ALLOC(Ginv64, G_STRIDE * T);
+    ALLOC(Ginv64c, GC64 * T);
     ALLOC(crw, 2 * SS * T);
     ALLOC(adj_h, NX * T);
     ALLOC(adj_zero, NS * T);
@@ -456,7 +458,8 @@ gpt_status gpt_destroy(gpt_handle *h)
     cudaFree(h->G); cudaFree(h->C); cudaFree(h->g); cudaFree(h->c); cudaFree(h->S);
     cudaFree(h->gamma); cudaFree(h->Ginv); cudaFree(h->dz); cudaFree(h->xs); cudaFree(h->knot_merit);
     cudaFree(h->merits); cudaFree(h->st); cudaFree(h->knot_off); cudaFree(h->knot_inst); cudaFree(h->pcg_log);
-    cudaFree(h->pcg_out); cudaFree(h->d_active); cudaFree(h->lam64); cudaFree(h->Ginv64); cudaFree(h->crw);
+    cudaFree(h->pcg_out); cudaFree(h->d_active); cudaFree(h->lam64); cudaFree(h->Ginv64); cudaFree(h->Ginv64c);
+    cudaFree(h->crw);
     cudaFree(h->adj_h); cudaFree(h->adj_zero); cudaFree(h->adj_gamma); cudaFree(h->adj_lam); cudaFree(h->adj_mu);
     cudaFree(h->adj_part); cudaFree(h->adj_lam64);
     cudaFree(h->S64); cudaFree(h->gamma64); cudaFree(h->adj_gamma64);
@@ -582,7 +585,7 @@ gpt_status gpt_compute_dz(gpt_handle *h, uint32_t N, const float *d_Ginv, const 
         return set_err(GPT_ERR_BAD_ARG, "null argument");
     DeviceGuard dg(h->device);
     if (!check_n(h, N)) return set_err(GPT_ERR_BAD_ARG, "knot_points out of range");
-    GPT_CUDA(launch_dz(single_view(N), d_Ginv, d_Ginv64, d_C, d_g, d_lambda, d_lambda64, d_dz, h->num_sms,
+    GPT_CUDA(launch_dz(single_view(N), d_Ginv, d_Ginv64, nullptr, d_C, d_g, d_lambda, d_lambda64, d_dz, h->num_sms,
                        (cudaStream_t)stream));
     return GPT_OK;
 }
@@ -749,8 +752,8 @@ static gpt_status enqueue_iteration(gpt_handle *h, const SqpPlan &pl, const floa
     {
         PhaseTimer t(h, s, GPT_PHASE_SCHUR);
         if (f64) {
-            GPT_CUDA(launch_schur64(bv, h->G, h->C, h->g, h->c, h->S64, h->gamma64, nullptr, h->Ginv64, ns, s,
-                                    ctas_or_default(SP.cta_schur)));
+            GPT_CUDA(launch_schur64(bv, h->G, h->C, h->g, h->c, h->S64, h->gamma64, nullptr, h->Ginv64, h->Ginv64c,
+                                    ns, s, ctas_or_default(SP.cta_schur)));
         } else if (stair) {
             // the reference's rows and block-Jacobi Pinv (gato_form_schur_jacobi), then the stair blocks
             if (!h->Sref) return set_err(GPT_ERR_BAD_ARG, "pcg_precond 2 was not configured on this handle");
@@ -772,8 +775,8 @@ static gpt_status enqueue_iteration(gpt_handle *h, const SqpPlan &pl, const floa
     }
     {
         PhaseTimer t(h, s, GPT_PHASE_DZ);
-        GPT_CUDA(launch_dz(bv, h->Ginv, h->Ginv64, h->C, h->g, d_lambda, h->lam64, h->dz, ns, s,
-                           ctas_or_default(SP.cta_dz)));
+        GPT_CUDA(launch_dz(bv, h->Ginv, h->Ginv64, f64 ? h->Ginv64c : nullptr, h->C, h->g, d_lambda, h->lam64, h->dz,
+                           ns, s, ctas_or_default(SP.cta_dz)));
     }
     {
         PhaseTimer t(h, s, GPT_PHASE_MERIT);
@@ -1261,7 +1264,8 @@ gpt_status gpt_sqp_adjoint(gpt_handle *h, uint32_t B, const uint32_t *h_N, const
     // ---- the step at xu: K [dz; lambda] = [g; c]
     GPT_CUDA(launch_kkt(bv, P, d_xu, d_goal, h->xs, h->G, h->C, h->g, h->c, ns, s));
     if (f64)
-        GPT_CUDA(launch_schur64(bv, h->G, h->C, h->g, h->c, h->S64, h->gamma64, nullptr, h->Ginv64, ns, s));
+        GPT_CUDA(launch_schur64(bv, h->G, h->C, h->g, h->c, h->S64, h->gamma64, nullptr, h->Ginv64, h->Ginv64c, ns,
+                                s));
     else
         GPT_CUDA(launch_schur(1, bv, 0.f, h->G, h->C, h->g, h->c, h->S, nullptr, h->gamma, h->Ginv, h->Ginv64,
                               nullptr, SP.pcg_precond == 0 ? 1 : 0, ns, s));
@@ -1270,7 +1274,8 @@ gpt_status gpt_sqp_adjoint(gpt_handle *h, uint32_t B, const uint32_t *h_N, const
                         h->crw, (int)SP.pcg_max_iter, SP.pcg_tol, (int)SP.pcg_exit_mode, nullptr, nullptr, 0,
                         (int)SP.pcg_cluster_size, ns, s));
     GPT_CUDA(cudaMemsetAsync(h->dz, 0, sizeof(float) * NX * T, s));
-    GPT_CUDA(launch_dz(bv, h->Ginv, h->Ginv64, h->C, h->g, nullptr, h->lam64, h->dz, ns, s));
+    GPT_CUDA(launch_dz(bv, h->Ginv, h->Ginv64, f64 ? h->Ginv64c : nullptr, h->C, h->g, nullptr, h->lam64, h->dz, ns,
+                       s));
     if (d_xu_next) GPT_CUDA(launch_axpy(nz, -1.f, h->dz, d_xu, d_xu_next, ns, s));
     // ---- adjoint solve K mu = [h; 0], h = dl/d(dz) = -dl/dxu+; same S (recomputed), new gamma
     GPT_CUDA(cudaMemsetAsync(h->adj_h, 0, sizeof(float) * NX * T, s));
@@ -1278,7 +1283,7 @@ gpt_status gpt_sqp_adjoint(gpt_handle *h, uint32_t B, const uint32_t *h_N, const
     GPT_CUDA(cudaMemsetAsync(h->adj_zero, 0, sizeof(float) * NS * T, s));
     if (f64)
         GPT_CUDA(launch_schur64(bv, h->G, h->C, h->adj_h, h->adj_zero, h->S64, h->adj_gamma64, nullptr, h->Ginv64,
-                                ns, s));
+                                h->Ginv64c, ns, s));
     else
         GPT_CUDA(launch_schur(1, bv, 0.f, h->G, h->C, h->adj_h, h->adj_zero, h->S, nullptr, h->adj_gamma, h->Ginv,
                               h->Ginv64, nullptr, SP.pcg_precond == 0 ? 1 : 0, ns, s));
@@ -1287,7 +1292,8 @@ gpt_status gpt_sqp_adjoint(gpt_handle *h, uint32_t B, const uint32_t *h_N, const
                         h->adj_lam64, h->crw, (int)SP.pcg_max_iter, SP.pcg_tol, (int)SP.pcg_exit_mode, nullptr,
                         nullptr, 0, (int)SP.pcg_cluster_size, ns, s));
     GPT_CUDA(cudaMemsetAsync(h->adj_mu, 0, sizeof(float) * NX * T, s));
-    GPT_CUDA(launch_dz(bv, h->Ginv, h->Ginv64, h->C, h->adj_h, nullptr, h->adj_lam64, h->adj_mu, ns, s));
+    GPT_CUDA(launch_dz(bv, h->Ginv, h->Ginv64, f64 ? h->Ginv64c : nullptr, h->C, h->adj_h, nullptr, h->adj_lam64,
+                       h->adj_mu, ns, s));
     // ---- dl/dtheta = mu_z^T (dg/dtheta - dG/dtheta dz)
     GPT_CUDA(launch_adjoint_grad(bv, P, d_xu, d_goal, h->dz, h->adj_mu, d_grad_goal, h->adj_part, d_grad_qd,
                                  d_grad_r, d_grad_q_ee, ns, s));
@@ -1407,7 +1413,8 @@ static gpt_status enqueue_track_adjoint(gpt_handle *h, const SqpPlan &pl, float 
     // the step at the solution: K [dz; lambda] = [g; c]
     GPT_CUDA(launch_kkt(bv, pl.P, h->gxu, h->ggoal, h->xs, h->G, h->C, h->g, h->c, ns, s));
     if (f64)
-        GPT_CUDA(launch_schur64(bv, h->G, h->C, h->g, h->c, h->S64, h->gamma64, nullptr, h->Ginv64, ns, s));
+        GPT_CUDA(launch_schur64(bv, h->G, h->C, h->g, h->c, h->S64, h->gamma64, nullptr, h->Ginv64, h->Ginv64c, ns,
+                                s));
     else
         GPT_CUDA(launch_schur(1, bv, 0.f, h->G, h->C, h->g, h->c, h->S, nullptr, h->gamma, h->Ginv, h->Ginv64,
                               nullptr, SP.pcg_precond == 0 ? 1 : 0, ns, s));
@@ -1416,14 +1423,15 @@ static gpt_status enqueue_track_adjoint(gpt_handle *h, const SqpPlan &pl, float 
                         h->adj_lam, h->lam64, h->crw, (int)SP.pcg_max_iter, SP.pcg_tol, (int)SP.pcg_exit_mode, nullptr,
                         nullptr, 0, (int)SP.pcg_cluster_size, ns, s));
     GPT_CUDA(cudaMemsetAsync(h->dz, 0, sizeof(float) * NX * T, s));
-    GPT_CUDA(launch_dz(bv, h->Ginv, h->Ginv64, h->C, h->g, nullptr, h->lam64, h->dz, ns, s));
+    GPT_CUDA(launch_dz(bv, h->Ginv, h->Ginv64, f64 ? h->Ginv64c : nullptr, h->C, h->g, nullptr, h->lam64, h->dz, ns,
+                       s));
     // the adjoint solve K mu = [h; 0], h = dl/d(dz)
     GPT_CUDA(cudaMemsetAsync(h->adj_h, 0, sizeof(float) * NX * T, s));
     GPT_CUDA(launch_track_loss_grad(bv, h->gxu, h->dz, h->ggoal, h->adj_h, h->trk_kloss, ns, s));
     GPT_CUDA(cudaMemsetAsync(h->adj_zero, 0, sizeof(float) * NS * T, s));
     if (f64)
         GPT_CUDA(launch_schur64(bv, h->G, h->C, h->adj_h, h->adj_zero, h->S64, h->adj_gamma64, nullptr, h->Ginv64,
-                                ns, s));
+                                h->Ginv64c, ns, s));
     else
         GPT_CUDA(launch_schur(1, bv, 0.f, h->G, h->C, h->adj_h, h->adj_zero, h->S, nullptr, h->adj_gamma, h->Ginv,
                               h->Ginv64, nullptr, SP.pcg_precond == 0 ? 1 : 0, ns, s));
@@ -1432,7 +1440,8 @@ static gpt_status enqueue_track_adjoint(gpt_handle *h, const SqpPlan &pl, float 
                         h->adj_gamma64, h->adj_lam, h->adj_lam64, h->crw, (int)SP.pcg_max_iter, SP.pcg_tol,
                         (int)SP.pcg_exit_mode, nullptr, nullptr, 0, (int)SP.pcg_cluster_size, ns, s));
     GPT_CUDA(cudaMemsetAsync(h->adj_mu, 0, sizeof(float) * NX * T, s));
-    GPT_CUDA(launch_dz(bv, h->Ginv, h->Ginv64, h->C, h->adj_h, nullptr, h->adj_lam64, h->adj_mu, ns, s));
+    GPT_CUDA(launch_dz(bv, h->Ginv, h->Ginv64, f64 ? h->Ginv64c : nullptr, h->C, h->adj_h, nullptr, h->adj_lam64,
+                       h->adj_mu, ns, s));
     // dl/dtheta = mu_z^T (dg/dtheta - dG/dtheta dz), added to d_wgrad
     GPT_CUDA(launch_adjoint_grad(bv, pl.P, h->gxu, h->ggoal, h->dz, h->adj_mu, h->trk_ggrad, h->adj_part, nullptr,
                                  nullptr, nullptr, ns, s, d_wgrad));

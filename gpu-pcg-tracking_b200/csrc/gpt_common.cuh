@@ -25,6 +25,12 @@ constexpr int S_STRIDE = 3 * SS;         // 588 (toplevel.cuh:103)
 constexpr int NUM_ALPHAS = 8;            // toplevel.cuh:55
 constexpr int PK = 408;                  // packed Schur row for the PCG: left 196 + tri 105 + Pinv tri 105 + 2
 constexpr int PK64 = 302;                // FP64 packed Schur row: left 196 + diagonal lower triangle 105 + 1 pad (doubles)
+// Compact FP64 inverses of a knot's cost blocks (doubles; the FP64 Schur kernel's output for dz):
+// [0] flags (1: (Q + rho I)^{-1} is not block diagonal, 2: (R + rho I)^{-1} is not diagonal -- that
+// block is then in the full-layout buffer of G_STRIDE doubles per knot instead), [1, 50) the
+// position block's inverse (7 x 7, column-major), [50, 57) the velocity diagonal, [57, 64) the
+// control diagonal (zero for an instance's last knot).
+constexpr int GC64 = 64, GC_POS = 1, GC_VEL = 50, GC_CTL = 57;
 constexpr int MAX_KNOTS = 1024;          // per-instance horizon limit of the library
 
 // Per-instance SQP state kept on the device across the phases of one solve.

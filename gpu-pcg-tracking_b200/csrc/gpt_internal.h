@@ -64,10 +64,11 @@ cudaError_t launch_pcg(const BatchView &bv, int max_n_knots, int min_n_knots, in
                        const float *Pinv, const float *gamma, const double *gamma64, float *lambda, double *lambda64,
                        double *cr_ws, int max_iter, float tol, int exit_mode, uint32_t *out_iters, uint32_t *pcg_log,
                        int log_stride, int cluster_size, int num_sms, cudaStream_t s);
-// lambda64 (optional) replaces lambda when given
-cudaError_t launch_dz(const BatchView &bv, const float *Ginv, const double *Ginv64, const float *C, const float *g,
-                      const float *lambda, const double *lambda64, float *dz, int num_sms, cudaStream_t s,
-                      int ctas_per_sm = 16);
+// lambda64 (optional) replaces lambda when given; Ginv64c (optional): the compact inverses of
+// launch_schur64 (GC64 doubles per knot), with Ginv64 holding only the blocks its flags name
+cudaError_t launch_dz(const BatchView &bv, const float *Ginv, const double *Ginv64, const double *Ginv64c,
+                      const float *C, const float *g, const float *lambda, const double *lambda64, float *dz,
+                      int num_sms, cudaStream_t s, int ctas_per_sm = 16);
 cudaError_t launch_merit(const BatchView &bv, const ProblemParams &P, int n_alpha, const float *xu, const float *dz,
                          const float *goal, const float *xs, float *knot_merit, int num_sms, cudaStream_t s,
                          int ctas_per_sm = 16);
@@ -76,10 +77,12 @@ cudaError_t launch_accept(const BatchView &bv, int mode, const SolverParams &SP,
                           cudaStream_t s);
 cudaError_t launch_init(const BatchView &bv, const float *xu, float *xs, int num_sms, cudaStream_t s);
 // FP64 Schur complement for the exact-preconditioner PCG: packed rows (PK64 doubles per knot), gamma
-// (FP64), the inverses (Ginv64; Ginv FP32 too when non-null); rho from bv.st
+// (FP64), the inverses in compact form (Ginv64c, GC64 doubles per knot; a block that is not
+// (block) diagonal in the full layout of Ginv64 instead; Ginv FP32 in the full layout too when
+// non-null); rho from bv.st
 cudaError_t launch_schur64(const BatchView &bv, const float *G, const float *C, const float *g, const float *c,
-                           double *S64, double *gamma64, float *Ginv, double *Ginv64, int num_sms, cudaStream_t s,
-                           int ctas_per_sm = 16);
+                           double *S64, double *gamma64, float *Ginv, double *Ginv64, double *Ginv64c, int num_sms,
+                           cudaStream_t s, int ctas_per_sm = 16);
 // adjoint of the SQP step (gpt_adjoint.cu): per-knot goal gradients, per-instance weight gradients;
 // part holds adjoint_part_floats() floats per knot
 // (wacc non-null: the 15 weight gradients of each active instance are added to wacc[15 b ..] instead of

@@ -20,24 +20,31 @@ constexpr int DZ_WARPS = 4;
 // q_k - lambda_k - (-A_k)^T lambda_{k+1} and r_k - (-B_k)^T lambda_{k+1} cancel
 // heavily, so they are accumulated in FP64 before the inverses apply.  Every input of a
 // knot is loaded in one batch (the kernel is bound by load latency) and staged in shared memory.
+// COMPACT: the inverses come as launch_schur64's compact blocks (GC64 doubles per knot: the position
+// block, the velocity and control diagonals -- a quarter of the full layout's bytes); a block its
+// flags mark as not (block) diagonal is read from the full layout instead.  The sums are those of
+// the full layout term by term (the skipped terms are exact zeros).
+template <bool COMPACT>
 struct DzWarpSmem {
-    double gi[G_STRIDE];  // (Q + rho I)^{-1}, (R + rho I)^{-1}
-    double lv[2 * NS];    // lambda_k, lambda_{k+1}
+    double gi[COMPACT ? GC64 : G_STRIDE];  // (Q + rho I)^{-1}, (R + rho I)^{-1}
+    double lv[2 * NS];                     // lambda_k, lambda_{k+1}
     double s[NX];
-    float cm[C_STRIDE];   // -A_k, -B_k
+    float cm[C_STRIDE];  // -A_k, -B_k
     float gv[NX];
 };
 
+template <bool COMPACT>
 __global__ void __launch_bounds__(32 * DZ_WARPS)
     dz_kernel(BatchView bv, const float *__restrict__ Ginv, const double *__restrict__ Ginv64,
-              const float *__restrict__ Cm, const float *__restrict__ g, const float *__restrict__ lambda,
-              const double *__restrict__ lambda64, float *__restrict__ dz)
+              const double *__restrict__ Ginv64c, const float *__restrict__ Cm, const float *__restrict__ g,
+              const float *__restrict__ lambda, const double *__restrict__ lambda64, float *__restrict__ dz)
 {
-    __shared__ DzWarpSmem sm_all[DZ_WARPS];
+    __shared__ DzWarpSmem<COMPACT> sm_all[DZ_WARPS];
     const int lane = threadIdx.x & 31;
-    DzWarpSmem &sm = sm_all[threadIdx.x >> 5];
+    DzWarpSmem<COMPACT> &sm = sm_all[threadIdx.x >> 5];
     const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nw = (gridDim.x * blockDim.x) >> 5;
+    constexpr int GIN = COMPACT ? GC64 : G_STRIDE;
     for (int j = bv.j0 + gw; j < bv.j0 + bv.total_knots; j += nw) {
         const int b = bv.inst(j);
         if (!bv.active(b)) continue;
@@ -46,15 +53,19 @@ __global__ void __launch_bounds__(32 * DZ_WARPS)
         const float *Cj = Cm + (size_t)C_STRIDE * j;
         const int nl = last ? NS : 2 * NS;
         // ---- all loads of the knot, then the shared-memory stores
-        constexpr int NGI = (G_STRIDE + 31) / 32, NCM = (C_STRIDE + 31) / 32;
-        const int ngi = last ? SS : G_STRIDE;  // the last knot's block has no R part (buffers of 245N - 49)
+        constexpr int NGI = (GIN + 31) / 32, NCM = (C_STRIDE + 31) / 32;
+        // the last knot's block has no R part (buffers of 245N - 49)
+        const int ngi = COMPACT ? GC64 : (last ? SS : G_STRIDE);
         double gi[NGI];
         float cm[NCM];
 #pragma unroll
         for (int i = 0; i < NGI; ++i) {
             const int e = lane + 32 * i;
             gi[i] = 0.0;
-            if (e < ngi) gi[i] = Ginv64 ? Ginv64[(size_t)G_STRIDE * j + e] : (double)Ginv[(size_t)G_STRIDE * j + e];
+            if (COMPACT)
+                gi[i] = Ginv64c[(size_t)GC64 * j + e];
+            else if (e < ngi)
+                gi[i] = Ginv64 ? Ginv64[(size_t)G_STRIDE * j + e] : (double)Ginv[(size_t)G_STRIDE * j + e];
         }
 #pragma unroll
         for (int i = 0; i < NCM; ++i) {
@@ -68,7 +79,7 @@ __global__ void __launch_bounds__(32 * DZ_WARPS)
 #pragma unroll
         for (int i = 0; i < NGI; ++i) {
             const int e = lane + 32 * i;
-            if (e < G_STRIDE) sm.gi[e] = gi[i];
+            if (e < GIN) sm.gi[e] = gi[i];
         }
 #pragma unroll
         for (int i = 0; i < NCM; ++i) {
@@ -95,30 +106,51 @@ __global__ void __launch_bounds__(32 * DZ_WARPS)
             sm.s[lane] = (double)sm.gv[lane] - a;
         }
         __syncwarp();
+        const int flags = COMPACT ? (int)sm.gi[0] : 0;
+        const double *full = COMPACT ? Ginv64 + (size_t)G_STRIDE * j : nullptr;  // the flagged blocks
         if (lane < NS) {
             double a = 0.0;
+            if (!COMPACT) {
 #pragma unroll
-            for (int t = 0; t < NS; ++t) a = fma(sm.gi[lane + NS * t], sm.s[t], a);
+                for (int t = 0; t < NS; ++t) a = fma(sm.gi[lane + NS * t], sm.s[t], a);
+            } else if (flags & 1) {
+                for (int t = 0; t < NS; ++t) a = fma(full[lane + NS * t], sm.s[t], a);
+            } else if (lane < NC) {
+#pragma unroll
+                for (int t = 0; t < NC; ++t) a = fma(sm.gi[GC_POS + lane + NC * t], sm.s[t], a);
+            } else {
+                a = sm.gi[GC_VEL + lane - NC] * sm.s[lane];
+            }
             dz[(size_t)NX * j + lane] = (float)a;
         } else if (lane < NX && !last) {
             const int i = lane - NS;
             double a = 0.0;
+            if (!COMPACT) {
 #pragma unroll
-            for (int t = 0; t < NC; ++t) a = fma(sm.gi[SS + i + NC * t], sm.s[NS + t], a);
+                for (int t = 0; t < NC; ++t) a = fma(sm.gi[SS + i + NC * t], sm.s[NS + t], a);
+            } else if (flags & 2) {
+                for (int t = 0; t < NC; ++t) a = fma(full[SS + i + NC * t], sm.s[NS + t], a);
+            } else {
+                a = sm.gi[GC_CTL + i] * sm.s[lane];
+            }
             dz[(size_t)NX * j + lane] = (float)a;
         }
         __syncwarp();
     }
 }
 
-cudaError_t launch_dz(const BatchView &bv, const float *Ginv, const double *Ginv64, const float *C, const float *g,
-                      const float *lambda, const double *lambda64, float *dz, int num_sms, cudaStream_t s,
-                      int ctas_per_sm)
+cudaError_t launch_dz(const BatchView &bv, const float *Ginv, const double *Ginv64, const double *Ginv64c,
+                      const float *C, const float *g, const float *lambda, const double *lambda64, float *dz,
+                      int num_sms, cudaStream_t s, int ctas_per_sm)
 {
     if (bv.total_knots <= 0) return cudaSuccess;
+    if (Ginv64c && !Ginv64) return cudaErrorInvalidValue;
     int blocks = (bv.total_knots + DZ_WARPS - 1) / DZ_WARPS;
     if (blocks > num_sms * ctas_per_sm) blocks = num_sms * ctas_per_sm;
-    dz_kernel<<<blocks, 32 * DZ_WARPS, 0, s>>>(bv, Ginv, Ginv64, C, g, lambda, lambda64, dz);
+    if (Ginv64c)
+        dz_kernel<true><<<blocks, 32 * DZ_WARPS, 0, s>>>(bv, Ginv, Ginv64, Ginv64c, C, g, lambda, lambda64, dz);
+    else
+        dz_kernel<false><<<blocks, 32 * DZ_WARPS, 0, s>>>(bv, Ginv, Ginv64, nullptr, C, g, lambda, lambda64, dz);
     return cudaGetLastError();
 }
 

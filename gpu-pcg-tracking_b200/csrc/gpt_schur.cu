@@ -476,6 +476,34 @@ __device__ __forceinline__ bool warp_inverse64_control(const float *R, double sh
     return __all_sync(0xffffffffu, piv_ok);
 }
 
+// A knot's FP64 inverses for dz, from shared memory (Qi: 14 x 14, Ri: 7 x 7 or null for an
+// instance's last knot), as GC64 contiguous doubles (two stores per lane) plus, only for a block
+// that is not (block) diagonal, that block in the full layout (G_STRIDE doubles per knot).
+__device__ __forceinline__ void write_ginv_compact(double *dc, double *dfull, const double *Qi, const double *Ri,
+                                                   bool q_bd, bool r_dg, int lane)
+{
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        const int e = lane + 32 * h;
+        double v;
+        if (e == 0) {
+            v = (q_bd ? 0.0 : 1.0) + (r_dg ? 0.0 : 2.0);
+        } else if (e < GC_VEL) {
+            const int i = e - GC_POS;
+            v = Qi[i % NC + NS * (i / NC)];
+        } else if (e < GC_CTL) {
+            v = Qi[(NC + e - GC_VEL) * (NS + 1)];
+        } else {
+            v = Ri ? Ri[(e - GC_CTL) * (NC + 1)] : 0.0;
+        }
+        dc[e] = v;
+    }
+    if (!q_bd)
+        for (int e = lane; e < SS; e += 32) dfull[e] = Qi[e];
+    if (Ri && !r_dg)
+        for (int e = lane; e < CC; e += 32) dfull[SS + e] = Ri[e];
+}
+
 // One warp's shared memory: the knot's KKT blocks staged as FP32 (one batch of loads per knot), the
 // FP64 inverses and products
 struct Schur64WarpSmem {
@@ -489,7 +517,8 @@ struct Schur64WarpSmem {
 __global__ void __launch_bounds__(32 * SCHUR_WARPS, 5)
     schur64_kernel(BatchView bv, const float *__restrict__ G, const float *__restrict__ Cm,
                    const float *__restrict__ g, const float *__restrict__ c, double *__restrict__ S64,
-                   double *__restrict__ gamma64, float *__restrict__ Ginv, double *__restrict__ Ginv64)
+                   double *__restrict__ gamma64, float *__restrict__ Ginv, double *__restrict__ Ginv64,
+                   double *__restrict__ Ginv64c)
 {
     extern __shared__ double4 schur64_dyn_smem[];
     Schur64WarpSmem *smem_all = reinterpret_cast<Schur64WarpSmem *>(schur64_dyn_smem);
@@ -527,9 +556,12 @@ __global__ void __launch_bounds__(32 * SCHUR_WARPS, 5)
             __syncwarp();
             const bool ok0 = warp_inverse64_state(sm.Gk, rho, Q0i, lane,
                                                   (N == 1 && Ginv) ? Ginv + (size_t)G_STRIDE * j : nullptr,
-                                                  N == 1 ? Ginv64 + (size_t)G_STRIDE * j : nullptr, &have_bd);
+                                                  nullptr, &have_bd);
             if (!ok0 && lane == 0) atomicOr(&bv.st[b].exit_flags, GPT_EXIT_FACTOR);
             __syncwarp();
+            if (N == 1)
+                write_ginv_compact(Ginv64c + (size_t)GC64 * j, Ginv64 + (size_t)G_STRIDE * j, Q0i, nullptr, have_bd,
+                                   true, lane);
             if (lane < NS) {
                 double acc = 0.0;
 #pragma unroll
@@ -581,25 +613,27 @@ __global__ void __launch_bounds__(32 * SCHUR_WARPS, 5)
         }
         __syncwarp();
         float *Gi32 = Ginv ? Ginv + (size_t)G_STRIDE * (j - 1) : nullptr;
-        double *Gi64 = Ginv64 + (size_t)G_STRIDE * (j - 1);
         double *const Qki = sm.Qinv[cur], *const Qkp1i = sm.Qinv[cur ^ 1];
         bool ok = true, bd_ki = have_bd, bd_kp1 = false, r_diag = false;
         if (reuse) {
-            // formed by this warp's previous row; its outputs for knot j - 1 are written here, as the
+            // formed by this warp's previous row; its FP32 copy for knot j - 1 is written here, as the
             // elimination below would
-            for (int e = lane; e < SS; e += 32) {
-                Gi64[e] = Qki[e];
-                if (Gi32) Gi32[e] = (float)Qki[e];
-            }
+            if (Gi32)
+                for (int e = lane; e < SS; e += 32) Gi32[e] = (float)Qki[e];
         } else {
-            ok = warp_inverse64_state(sm.Gm1, rho, Qki, lane, Gi32, Gi64, &bd_ki);
+            ok = warp_inverse64_state(sm.Gm1, rho, Qki, lane, Gi32, nullptr, &bd_ki);
         }
         ok = warp_inverse64_state(sm.Gk, rho, Qkp1i, lane, (k == N - 1 && Ginv) ? Ginv + (size_t)G_STRIDE * j : nullptr,
-                                  k == N - 1 ? Ginv64 + (size_t)G_STRIDE * j : nullptr, &bd_kp1) && ok;
-        ok = warp_inverse64_control(sm.Gm1 + SS, rho, sm.Rki, lane, Gi32 ? Gi32 + SS : nullptr, Gi64 + SS, &r_diag) &&
+                                  nullptr, &bd_kp1) && ok;
+        ok = warp_inverse64_control(sm.Gm1 + SS, rho, sm.Rki, lane, Gi32 ? Gi32 + SS : nullptr, nullptr, &r_diag) &&
              ok;
         if (!ok && lane == 0) atomicOr(&bv.st[b].exit_flags, GPT_EXIT_FACTOR);
         __syncwarp();
+        write_ginv_compact(Ginv64c + (size_t)GC64 * (j - 1), Ginv64 + (size_t)G_STRIDE * (j - 1), Qki, sm.Rki, bd_ki,
+                           r_diag, lane);
+        if (k == N - 1)
+            write_ginv_compact(Ginv64c + (size_t)GC64 * j, Ginv64 + (size_t)G_STRIDE * j, Qkp1i, nullptr, bd_kp1, true,
+                               lane);
         // the next row of the same instance (k + 1 < N) needs R_k, Q_{k+1} and C_k: R_k and Q_{k+1} are
         // copied now into the blocks the inverses above have finished with, C_k once the products below
         // are done with C_{k-1}; its Q_k is not needed (its inverse is this row's (Q_k + rho I)^{-1})
@@ -686,11 +720,11 @@ __global__ void __launch_bounds__(32 * SCHUR_WARPS, 5)
 }
 
 cudaError_t launch_schur64(const BatchView &bv, const float *G, const float *C, const float *g, const float *c,
-                           double *S64, double *gamma64, float *Ginv, double *Ginv64, int num_sms, cudaStream_t s,
-                           int ctas_per_sm)
+                           double *S64, double *gamma64, float *Ginv, double *Ginv64, double *Ginv64c, int num_sms,
+                           cudaStream_t s, int ctas_per_sm)
 {
     if (bv.total_knots <= 0) return cudaSuccess;
-    if (!bv.st || !Ginv64) return cudaErrorInvalidValue;
+    if (!bv.st || !Ginv64 || !Ginv64c) return cudaErrorInvalidValue;
     const size_t smem = sizeof(Schur64WarpSmem) * SCHUR_WARPS;
     int blocks = (bv.total_knots + SCHUR_WARPS - 1) / SCHUR_WARPS;
     const int cap = num_sms * ctas_per_sm;
@@ -699,7 +733,7 @@ cudaError_t launch_schur64(const BatchView &bv, const float *G, const float *C, 
         const cudaError_t e = ensure_func_attrs((const void *)schur64_kernel, smem);
         if (e != cudaSuccess) return e;
     }
-    schur64_kernel<<<blocks, 32 * SCHUR_WARPS, smem, s>>>(bv, G, C, g, c, S64, gamma64, Ginv, Ginv64);
+    schur64_kernel<<<blocks, 32 * SCHUR_WARPS, smem, s>>>(bv, G, C, g, c, S64, gamma64, Ginv, Ginv64, Ginv64c);
     return cudaGetLastError();
 }
 
