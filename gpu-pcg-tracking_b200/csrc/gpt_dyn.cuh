@@ -345,20 +345,28 @@ __device__ __forceinline__ void mass_matrix_lane(const JointTrig &t, float (&M)[
 // of an FP64 solve of the same M while cond(M) eps32 << 1 (the iiwa's M: cond ~ 1e2 .. 1e3).
 __device__ __forceinline__ void spd7_solve_lane(const float (&M)[28], const double (&b)[NQ], double (&x)[NQ])
 {
+    // Every loop runs over the full constant range with the triangle as a guard, so that all of them
+    // unroll and M, L stay in registers (loops bounded by an outer index left both in local memory);
+    // the operations and their order are those of the triangular loops.
+    auto tri = [](int i, int j) { return (i * (i + 1)) / 2 + j; };
     float L[28];
 #pragma unroll
     for (int j = 0; j < NQ; ++j) {
-        float d = M[(j * (j + 1)) / 2 + j];
+        float d = M[tri(j, j)];
 #pragma unroll
-        for (int k = 0; k < j; ++k) d = fmaf(-L[(j * (j + 1)) / 2 + k], L[(j * (j + 1)) / 2 + k], d);
+        for (int k = 0; k < NQ; ++k)
+            if (k < j) d = fmaf(-L[tri(j, k)], L[tri(j, k)], d);
         const float ljj = sqrtf(d), inv = 1.f / ljj;
-        L[(j * (j + 1)) / 2 + j] = ljj;
+        L[tri(j, j)] = ljj;
 #pragma unroll
-        for (int i = j + 1; i < NQ; ++i) {
-            float v = M[(i * (i + 1)) / 2 + j];
+        for (int i = 0; i < NQ; ++i) {
+            if (i > j) {
+                float v = M[tri(i, j)];
 #pragma unroll
-            for (int k = 0; k < j; ++k) v = fmaf(-L[(i * (i + 1)) / 2 + k], L[(j * (j + 1)) / 2 + k], v);
-            L[(i * (i + 1)) / 2 + j] = v * inv;
+                for (int k = 0; k < NQ; ++k)
+                    if (k < j) v = fmaf(-L[tri(i, k)], L[tri(j, k)], v);
+                L[tri(i, j)] = v * inv;
+            }
         }
     }
     auto solve = [&](const float (&r)[NQ], float (&y)[NQ]) {
@@ -366,15 +374,18 @@ __device__ __forceinline__ void spd7_solve_lane(const float (&M)[28], const doub
         for (int i = 0; i < NQ; ++i) {
             float v = r[i];
 #pragma unroll
-            for (int k = 0; k < i; ++k) v = fmaf(-L[(i * (i + 1)) / 2 + k], y[k], v);
-            y[i] = v / L[(i * (i + 1)) / 2 + i];
+            for (int k = 0; k < NQ; ++k)
+                if (k < i) v = fmaf(-L[tri(i, k)], y[k], v);
+            y[i] = v / L[tri(i, i)];
         }
 #pragma unroll
-        for (int i = NQ - 1; i >= 0; --i) {
+        for (int ii = 0; ii < NQ; ++ii) {
+            const int i = NQ - 1 - ii;
             float v = y[i];
 #pragma unroll
-            for (int k = i + 1; k < NQ; ++k) v = fmaf(-L[(k * (k + 1)) / 2 + i], y[k], v);
-            y[i] = v / L[(i * (i + 1)) / 2 + i];
+            for (int k = 0; k < NQ; ++k)
+                if (k > i) v = fmaf(-L[tri(k, i)], y[k], v);
+            y[i] = v / L[tri(i, i)];
         }
     };
     float r[NQ], y[NQ];
@@ -389,7 +400,7 @@ __device__ __forceinline__ void spd7_solve_lane(const float (&M)[28], const doub
         double v = b[i];
 #pragma unroll
         for (int k = 0; k < NQ; ++k) {
-            const float mik = i >= k ? M[(i * (i + 1)) / 2 + k] : M[(k * (k + 1)) / 2 + i];
+            const float mik = i >= k ? M[tri(i, k)] : M[tri(k, i)];
             v = fma(-(double)mik, x[k], v);
         }
         r[i] = (float)v;
