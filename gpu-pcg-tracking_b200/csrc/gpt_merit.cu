@@ -172,8 +172,9 @@ __device__ __forceinline__ float alpha_of(int a, int n_alpha)
 // M by its lower-triangle columns at zero velocity, c by one inverse-dynamics pass, the 7x7 solve by
 // an FP32 Cholesky refined in FP64.  The last knot: the line search adds ||x_0 + alpha dz_0 - x_s||_1,
 // the iterate's merit no defect (merit.cuh:68-77,135-137).  No shared memory and no warp synchronisation:
-// the lanes of a knot read the same addresses (one transaction per warp load).
-__global__ void __launch_bounds__(32 * MERIT_WARPS)
+// the lanes of a knot read the same addresses (one transaction per warp load).  Four CTAs per SM:
+// 128 registers without spilling (the unbounded build took 136, which let three fit).
+__global__ void __launch_bounds__(32 * MERIT_WARPS, 4)
     merit_kernel(BatchView bv, ProblemParams P, int n_alpha, const float *__restrict__ xu,
                  const float *__restrict__ dz, const float *__restrict__ goal, const float *__restrict__ xs,
                  float *__restrict__ knot_merit)
