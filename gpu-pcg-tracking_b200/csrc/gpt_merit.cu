@@ -278,25 +278,43 @@ cudaError_t launch_merit(const BatchView &bv, const ProblemParams &P, int n_alph
 
 constexpr int ACC_THREADS = 256;
 
-// Fixed-order sum of knot_merit[8 (kb + k) + a] over k for all a; result in out[a] (all threads).
-__device__ void merit_sums(const float *km, int kb, int N, int n_alpha, float *out, double *scratch)
+// Fixed-order sum of knot_merit[8 (kb + k) + a] over k for a < NA; result in out[a] (all threads).  A
+// thread loads its knots' NA merits together (two 16-byte loads for the 8 step sizes) and keeps NA
+// running sums; each sum adds the knots in the same order as a pass per step size would.
+template <int NA>
+__device__ __forceinline__ void merit_sums(const float *km, int kb, int N, float (&out)[NA], double *scratch)
 {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     constexpr int NW = ACC_THREADS / 32;
-    for (int a = 0; a < n_alpha; ++a) {
-        double v = 0.0;
-        for (int k = tid; k < N; k += ACC_THREADS) v += (double)km[(size_t)NUM_ALPHAS * (kb + k) + a];
-        v = warp_sum(v);
-        if (lane == 0) scratch[a * NW + warp] = v;
+    double v[NA];
+#pragma unroll
+    for (int a = 0; a < NA; ++a) v[a] = 0.0;
+    for (int k = tid; k < N; k += ACC_THREADS) {
+        const float *row = km + (size_t)NUM_ALPHAS * (kb + k);
+        if constexpr (NA == NUM_ALPHAS) {
+            const float4 lo = *reinterpret_cast<const float4 *>(row), hi = *reinterpret_cast<const float4 *>(row + 4);
+            const float e[8] = {lo.x, lo.y, lo.z, lo.w, hi.x, hi.y, hi.z, hi.w};
+#pragma unroll
+            for (int a = 0; a < NA; ++a) v[a] += (double)e[a];
+        } else {
+#pragma unroll
+            for (int a = 0; a < NA; ++a) v[a] += (double)row[a];
+        }
+    }
+#pragma unroll
+    for (int a = 0; a < NA; ++a) {
+        const double w = warp_sum(v[a]);
+        if (lane == 0) scratch[a * NW + warp] = w;
     }
     __syncthreads();
-    if (tid < n_alpha) {
+    if (tid < NA) {
         double t = 0.0;
         for (int w = 0; w < NW; ++w) t += scratch[tid * NW + w];
         scratch[NUM_ALPHAS * NW + tid] = t;
     }
     __syncthreads();
-    for (int a = 0; a < n_alpha; ++a) out[a] = (float)scratch[NUM_ALPHAS * NW + a];
+#pragma unroll
+    for (int a = 0; a < NA; ++a) out[a] = (float)scratch[NUM_ALPHAS * NW + a];
     __syncthreads();
 }
 
@@ -313,11 +331,20 @@ __global__ void __launch_bounds__(ACC_THREADS)
         if (!bv.active(b)) continue;
         const int N = bv.N(b), kb = bv.off(b);
         float m[NUM_ALPHAS];
-        merit_sums(knot_merit, kb, N, mode == 0 ? 1 : NUM_ALPHAS, m, scratch);
+        if (mode == 0) {
+            float m0[1];
+            merit_sums<1>(knot_merit, kb, N, m0, scratch);
+#pragma unroll
+            for (int a = 0; a < NUM_ALPHAS; ++a) m[a] = m0[0];
+        } else {
+            merit_sums<NUM_ALPHAS>(knot_merit, kb, N, m, scratch);
+        }
         if (threadIdx.x == 0) {
             float alpha = 0.f;
             if (merits_out) {
-                for (int a = 0; a < (mode == 0 ? 1 : NUM_ALPHAS); ++a) merits_out[NUM_ALPHAS * b + a] = m[a];
+#pragma unroll
+                for (int a = 0; a < NUM_ALPHAS; ++a)
+                    if (mode != 0 || a == 0) merits_out[NUM_ALPHAS * b + a] = m[a];
             }
             if (bv.st) {
                 InstState &s = bv.st[b];
