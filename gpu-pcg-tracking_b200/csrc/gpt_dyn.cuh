@@ -346,10 +346,11 @@ __device__ __forceinline__ void mass_matrix_lane(const JointTrig &t, float (&M)[
 __device__ __forceinline__ void spd7_solve_lane(const float (&M)[28], const double (&b)[NQ], double (&x)[NQ])
 {
     // Every loop runs over the full constant range with the triangle as a guard, so that all of them
-    // unroll and M, L stay in registers (loops bounded by an outer index left both in local memory);
-    // the operations and their order are those of the triangular loops.
+    // unroll and M, L stay in registers (loops bounded by an outer index left both in local memory).
+    // The triangular solves multiply by the diagonal's reciprocals instead of dividing: the FP64
+    // refinement step below removes the FP32 solve's rounding either way.
     auto tri = [](int i, int j) { return (i * (i + 1)) / 2 + j; };
-    float L[28];
+    float L[28], Li[NQ];  // the factor and the reciprocals of its diagonal
 #pragma unroll
     for (int j = 0; j < NQ; ++j) {
         float d = M[tri(j, j)];
@@ -358,6 +359,7 @@ __device__ __forceinline__ void spd7_solve_lane(const float (&M)[28], const doub
             if (k < j) d = fmaf(-L[tri(j, k)], L[tri(j, k)], d);
         const float ljj = sqrtf(d), inv = 1.f / ljj;
         L[tri(j, j)] = ljj;
+        Li[j] = inv;
 #pragma unroll
         for (int i = 0; i < NQ; ++i) {
             if (i > j) {
@@ -376,7 +378,7 @@ __device__ __forceinline__ void spd7_solve_lane(const float (&M)[28], const doub
 #pragma unroll
             for (int k = 0; k < NQ; ++k)
                 if (k < i) v = fmaf(-L[tri(i, k)], y[k], v);
-            y[i] = v / L[tri(i, i)];
+            y[i] = v * Li[i];
         }
 #pragma unroll
         for (int ii = 0; ii < NQ; ++ii) {
@@ -385,7 +387,7 @@ __device__ __forceinline__ void spd7_solve_lane(const float (&M)[28], const doub
 #pragma unroll
             for (int k = 0; k < NQ; ++k)
                 if (k > i) v = fmaf(-L[tri(k, i)], y[k], v);
-            y[i] = v / L[tri(i, i)];
+            y[i] = v * Li[i];
         }
     };
     float r[NQ], y[NQ];
