@@ -347,18 +347,17 @@ __device__ __forceinline__ void spd7_solve_lane(const float (&M)[28], const doub
 {
     // Every loop runs over the full constant range with the triangle as a guard, so that all of them
     // unroll and M, L stay in registers (loops bounded by an outer index left both in local memory).
-    // The triangular solves multiply by the diagonal's reciprocals instead of dividing: the FP64
-    // refinement step below removes the FP32 solve's rounding either way.
+    // The diagonal's reciprocals come from rsqrtf and the triangular solves multiply by them instead
+    // of dividing: the FP64 refinement step below removes the FP32 solve's rounding either way.
     auto tri = [](int i, int j) { return (i * (i + 1)) / 2 + j; };
-    float L[28], Li[NQ];  // the factor and the reciprocals of its diagonal
+    float L[28], Li[NQ];  // the factor below the diagonal, the reciprocals of its diagonal
 #pragma unroll
     for (int j = 0; j < NQ; ++j) {
         float d = M[tri(j, j)];
 #pragma unroll
         for (int k = 0; k < NQ; ++k)
             if (k < j) d = fmaf(-L[tri(j, k)], L[tri(j, k)], d);
-        const float ljj = sqrtf(d), inv = 1.f / ljj;
-        L[tri(j, j)] = ljj;
+        const float inv = rsqrtf(d);  // 1 / L_jj
         Li[j] = inv;
 #pragma unroll
         for (int i = 0; i < NQ; ++i) {
